@@ -1,0 +1,568 @@
+/*
+ * hplai_oracle.c -- CPU oracle for the HPL-AI solver hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker, never the product:
+ * only tests/, __graft_entry__.smoke() and bench.py (its cpu_baseline leg and
+ * its `--impl reference` arm) may load liboracle.so.  The CUDA library
+ * (libhplai.so) does not link, load or call anything here.
+ *
+ * It restates, in plain C, the reference's algorithm (RIKEN-RCCS/hpl-ai) for
+ * the single-process collapse of its 2D block-cyclic grid:
+ *   - the 64-bit LCG matrix generator            hpl_rand.hpp:8-123, matgen.hpp:7-22,193-225
+ *   - the no-pivot blocked LU, FP32 panels and an FP16-input / FP32-accumulate
+ *     Schur update (the `-not -r` path, no lazy init)
+ *                                                 panel_trf.hpp:434-633, getrf_nopiv.hpp:30-160,
+ *                                                 fp16sim.hpp:216-233, kernels/avx2.cpp:195-302
+ *   - FP64 iterative refinement with the matrix regenerated on the fly
+ *                                                 iterative_refinement.hpp:18-57,
+ *                                                 panel_gemv.hpp:16-180, otf_gemv.cpp:5-131,
+ *                                                 panel_trsv.hpp:115-285,310-758,
+ *                                                 panel_norm.hpp:8-41,78-84
+ *
+ * Arithmetic follows the reference's operation order, with every
+ * `a = b*c + a` that the reference's x86 build (g++ -O2 -march=native, whose
+ * default -ffp-contract=fast fuses them) turns into one FMA written here as an
+ * explicit fma()/fmaf().  The file itself is compiled with
+ * -ffp-contract=off so that nothing else is fused behind our back.
+ *
+ * The BLAS routines the reference calls (strsm_, sgemm_) are restated in the
+ * netlib reference-BLAS order; the reference's own BLAS is unpinned
+ * (un-vendored, version not recorded), so LU factors agree with it to FP32
+ * rounding, not bit for bit.  The generator, the right-hand side and the
+ * diagonal are integer/sequential and therefore bit-exact.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include <float.h>
+
+#define ORC_EXPORT __attribute__((visibility("default")))
+
+/* ------------------------------------------------------------------ */
+/* LCG: x <- a*x + c (mod 2^64)                hpl_rand.hpp:8-57       */
+/* ------------------------------------------------------------------ */
+typedef struct { uint64_t a, c; } orc_coeff;
+
+static orc_coeff coeff_default(void) { orc_coeff r = {6364136223846793005ULL, 1ULL}; return r; }
+
+/* (l * r)(x) = l(r(x))                         hpl_rand.hpp:16-18 */
+static orc_coeff coeff_mul(orc_coeff l, orc_coeff r)
+{
+	orc_coeff o;
+	o.a = l.a * r.a;
+	o.c = l.a * r.c + l.c;
+	return o;
+}
+
+/* x^n by recursive squaring                    hpl_rand.hpp:20-32 */
+static orc_coeff coeff_pow(orc_coeff x, uint64_t n)
+{
+	if (n == 0) { orc_coeff one = {1ULL, 0ULL}; return one; }
+	orc_coeff t = coeff_pow(x, n / 2);
+	t = coeff_mul(t, t);
+	return (n & 1ULL) ? coeff_mul(t, x) : t;
+}
+
+static uint64_t coeff_apply(orc_coeff c, uint64_t x) { return c.a * x + c.c; }
+
+/* state_0 = a*seed + c                         hpl_rand.hpp:38-43 */
+static uint64_t state_initial(uint64_t seed) { return coeff_apply(coeff_default(), seed); }
+
+/* value = int64(x) * (1-2^-53) * 2^-64 in [-0.5, 0.5)   hpl_rand.hpp:50-52 */
+static double state_value(uint64_t x) { return (double)(int64_t)x * 0x1.fffffffffffffP-65; }
+
+/* state of element (i,j): linear index i + n*j from state_0 */
+static uint64_t state_at(int n, int64_t i, int64_t j, uint64_t seed)
+{
+	orc_coeff jump = coeff_pow(coeff_default(), (uint64_t)i + (uint64_t)n * (uint64_t)j);
+	return coeff_apply(jump, state_initial(seed));
+}
+
+ORC_EXPORT uint64_t orc_state_at(int n, int64_t i, int64_t j, uint64_t seed) { return state_at(n, i, j, seed); }
+ORC_EXPORT double orc_elem(int n, int64_t i, int64_t j, uint64_t seed) { return state_value(state_at(n, i, j, seed)); }
+
+/* Jump coefficients (a, c) of inc1^m, exported so tests can compare the
+ * device's jump-ahead tables.                                            */
+ORC_EXPORT void orc_coeff_pow(uint64_t m, uint64_t *a, uint64_t *c)
+{
+	orc_coeff r = coeff_pow(coeff_default(), m);
+	*a = r.a;
+	*c = r.c;
+}
+
+/* diag_i = sum_{j != i} |a_ij| in sequential FP64     hpl_rand.hpp:108-123 */
+ORC_EXPORT double orc_calc_diag(int i, int n, uint64_t seed)
+{
+	orc_coeff inc1 = coeff_default();
+	orc_coeff jumpn = coeff_pow(inc1, (uint64_t)n);
+	uint64_t s = coeff_apply(coeff_pow(inc1, (uint64_t)i), state_initial(seed));
+	double sum = 0.0;
+	for (int j = 0; j < n; j++) {
+		if (i != j) sum += fabs(state_value(s));
+		s = coeff_apply(jumpn, s);
+	}
+	return sum;
+}
+
+/* fill_one_panel_with_rand<float>               hpl_rand.hpp:59-106
+ * Sub-matrix (i0:i0+nrow, j0:j0+ncol) of the n x n matrix, column-major with
+ * lda; on a square diagonal block the diagonal becomes float(row sum).     */
+ORC_EXPORT void orc_fill_panel(int n, int i0, int j0, int nrow, int ncol,
+	float *a, int64_t lda, uint64_t seed, int calc_diag)
+{
+	orc_coeff inc1 = coeff_default();
+	orc_coeff jump_one_col = coeff_pow(inc1, (uint64_t)n);
+	uint64_t s0 = state_at(n, i0, j0, seed);
+	#pragma omp parallel for schedule(static)
+	for (int j = 0; j < ncol; j++) {
+		uint64_t s = coeff_apply(coeff_pow(jump_one_col, (uint64_t)j), s0);
+		for (int i = 0; i < nrow; i++) {
+			a[(int64_t)j * lda + i] = (float)state_value(s);
+			s = coeff_apply(inc1, s);
+		}
+	}
+	if (calc_diag && i0 == j0 && nrow == ncol) {
+		#pragma omp parallel for schedule(dynamic, 16)
+		for (int i = 0; i < nrow; i++)
+			a[lda * i + i] = (float)orc_calc_diag(i0 + i, n, seed);
+	}
+}
+
+/* pmatgen over the whole matrix                 matgen.hpp:7-22 */
+ORC_EXPORT void orc_fill_matrix(int n, float *a, int64_t lda, uint64_t seed)
+{
+	orc_fill_panel(n, 0, 0, n, n, a, lda, seed, 1);
+}
+
+/* pcolvgen: rhs_i = element (i, n), kept in FP64   matgen.hpp:193-207 */
+ORC_EXPORT void orc_gen_rhs(int n, uint64_t seed, double *rhs)
+{
+	uint64_t s = state_at(n, 0, n, seed);
+	orc_coeff inc1 = coeff_default();
+	for (int i = 0; i < n; i++) {
+		rhs[i] = state_value(s);
+		s = coeff_apply(inc1, s);
+	}
+}
+
+/* pdiaggen                                      matgen.hpp:209-225 */
+ORC_EXPORT void orc_gen_diag(int n, uint64_t seed, double *d)
+{
+	#pragma omp parallel for schedule(dynamic, 16)
+	for (int i = 0; i < n; i++) d[i] = orc_calc_diag(i, n, seed);
+}
+
+/* ------------------------------------------------------------------ */
+/* FP32 dense kernels (netlib reference-BLAS order)                    */
+/* ------------------------------------------------------------------ */
+
+/* getrf_nopiv_small                             getrf_nopiv.hpp:30-46 */
+static void getrf_small(int n, float *a, int64_t lda)
+{
+	for (int k = 0; k < n; k++) {
+		float inv = 1.0f / a[lda * k + k];
+		for (int i = k + 1; i < n; ++i) a[k * lda + i] *= inv;
+		for (int j = k + 1; j < n; ++j) {
+			float akj = a[j * lda + k];
+			for (int i = k + 1; i < n; ++i)
+				a[j * lda + i] = fmaf(-a[k * lda + i], akj, a[j * lda + i]);
+		}
+	}
+}
+
+/* strsm_("R","U","N","N"): B(m x n) <- B * U^{-1}, U upper non-unit (n x n)
+ * trsmR                                         getrf_nopiv.hpp:14-18 */
+ORC_EXPORT void orc_trsm_right_upper(int m, int n, const float *u, int64_t ldu, float *b, int64_t ldb)
+{
+	#pragma omp parallel for schedule(static) if (m >= 4096)
+	for (int i0 = 0; i0 < m; i0 += 256) {
+		int i1 = i0 + 256 < m ? i0 + 256 : m;
+		for (int j = 0; j < n; j++) {
+			for (int k = 0; k < j; k++) {
+				float ukj = u[j * ldu + k];
+				if (ukj != 0.0f)
+					for (int i = i0; i < i1; i++) b[j * ldb + i] = fmaf(-ukj, b[k * ldb + i], b[j * ldb + i]);
+			}
+			float t = 1.0f / u[j * ldu + j];
+			for (int i = i0; i < i1; i++) b[j * ldb + i] *= t;
+		}
+	}
+}
+
+/* strsm_("L","L","N","U"): B(m x n) <- L^{-1} B, L unit lower (m x m)
+ * trsmL                                         getrf_nopiv.hpp:24-28 */
+ORC_EXPORT void orc_trsm_left_lower_unit(int m, int n, const float *l, int64_t ldl, float *b, int64_t ldb)
+{
+	#pragma omp parallel for schedule(static) if (n >= 4096)
+	for (int j = 0; j < n; j++) {
+		for (int k = 0; k < m; k++) {
+			float bkj = b[j * ldb + k];
+			if (bkj != 0.0f)
+				for (int i = k + 1; i < m; i++) b[j * ldb + i] = fmaf(-bkj, l[k * ldl + i], b[j * ldb + i]);
+		}
+	}
+}
+
+/* sgemm_("N","N") with alpha = -1, beta = 1      schur_updator.hpp:18-23 */
+static void sgemm_minus(int m, int n, int k, const float *a, int64_t lda,
+	const float *b, int64_t ldb, float *c, int64_t ldc)
+{
+	for (int j = 0; j < n; j++)
+		for (int l = 0; l < k; l++) {
+			float t = -b[j * ldb + l];
+			for (int i = 0; i < m; i++) c[j * ldc + i] = fmaf(t, a[l * lda + i], c[j * ldc + i]);
+		}
+}
+
+/* getrf_nopiv<float>: NSMALL = 16 blocked no-pivot LU
+ *                                               getrf_nopiv.hpp:124-141 */
+ORC_EXPORT void orc_getrf_nopiv(int n, float *a, int64_t lda)
+{
+	const int nsmall = 16;
+	for (int k = 0; k < n; k += nsmall) {
+		int nn = n - k < nsmall ? n - k : nsmall;
+		getrf_small(nn, a + lda * k + k, lda);
+		if (n - k > nn) {
+			orc_trsm_left_lower_unit(nn, n - k - nn, a + lda * k + k, lda, a + lda * (k + nn) + k, lda);
+			orc_trsm_right_upper(n - k - nn, nn, a + lda * k + k, lda, a + lda * k + k + nn, lda);
+			sgemm_minus(n - k - nn, n - k - nn, nn, a + lda * k + k + nn, lda,
+				a + lda * (k + nn) + k, lda, a + lda * (k + nn) + (k + nn), lda);
+		}
+	}
+}
+
+/* FP32 -> FP16 (round to nearest even) and back; _Float16 is IEEE binary16. */
+ORC_EXPORT void orc_f32_to_f16(int64_t count, const float *src, uint16_t *dst)
+{
+	for (int64_t i = 0; i < count; i++) {
+		_Float16 h = (_Float16)src[i];
+		memcpy(dst + i, &h, 2);
+	}
+}
+
+static inline float f16_bits_to_f32(uint16_t b)
+{
+	_Float16 h;
+	memcpy(&h, &b, 2);
+	return (float)h;
+}
+
+/* shgemm_opt with alpha = -1: C(m x n, FP32) -= A(m x k, FP16) * B(k x n, FP16),
+ * FP32 FMA accumulation in k-blocks of 100, each block folded into C with one
+ * rounding (c = fma(-1, s, c))             kernels/avx2.cpp:195-302, fp16sim.hpp:216-233 */
+ORC_EXPORT void orc_shgemm_minus(int m, int n, int k, const uint16_t *a, int64_t lda,
+	const uint16_t *b, int64_t ldb, float *c, int64_t ldc)
+{
+	const int bk = 100;
+	#pragma omp parallel
+	{
+		float *acol = (float *)malloc(sizeof(float) * (size_t)k);
+		float *arow = (float *)malloc(sizeof(float) * (size_t)k * 64);
+		#pragma omp for schedule(dynamic, 1)
+		for (int i0 = 0; i0 < m; i0 += 64) {
+			int ib = m - i0 < 64 ? m - i0 : 64;
+			/* stage A rows i0..i0+ib as FP32 (exact), k-major */
+			for (int i = 0; i < ib; i++)
+				for (int l = 0; l < k; l++) arow[(size_t)i * k + l] = f16_bits_to_f32(a[l * lda + i0 + i]);
+			for (int j = 0; j < n; j++) {
+				for (int l = 0; l < k; l++) acol[l] = f16_bits_to_f32(b[j * ldb + l]);
+				for (int i = 0; i < ib; i++) {
+					const float *ar = arow + (size_t)i * k;
+					float cij = c[j * ldc + i0 + i];
+					for (int l0 = 0; l0 < k; l0 += bk) {
+						int l1 = l0 + bk < k ? l0 + bk : k;
+						float s = 0.0f;
+						for (int l = l0; l < l1; l++) s = fmaf(ar[l], acol[l], s);
+						cij = fmaf(-1.0f, s, cij);
+					}
+					c[j * ldc + i0 + i] = cij;
+				}
+			}
+		}
+		free(acol);
+		free(arow);
+	}
+}
+
+/* ------------------------------------------------------------------ */
+/* The blocked right-looking no-pivot LU, single-process collapse of    */
+/* panel_lu_async / RDMAPanelLU::run (panel_trf.hpp:434-633, 703-856)  */
+/* ------------------------------------------------------------------ */
+/* On return `a` holds unit-L strictly below the diagonal and U on and
+ * above it (FP32), exactly like the reference's Panels after the LU.
+ * scalea/scaleb are the FP16 down-cast scales (1 without lazy init,
+ * panel_trf.hpp:446-447).                                              */
+ORC_EXPORT int orc_lu(int n, int b, float *a, int64_t lda)
+{
+	if (n <= 0 || b <= 0 || n % b) return -1;
+	int nb = n / b;
+	uint16_t *lh = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)n * b);
+	uint16_t *uh = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)n * b);
+	if (!lh || !uh) { free(lh); free(uh); return -2; }
+	for (int k = 0; k < nb; k++) {
+		int64_t kb = (int64_t)k * b;
+		float *lu = a + kb * lda + kb;
+		/* diagonal block: getrf_nopiv (copy-first variant computes the same
+		 * numbers in a copy, getrf_nopiv.hpp:143-160)                       */
+		orc_getrf_nopiv(b, lu, lda);
+		if (k == nb - 1) break;
+		int64_t rem = n - kb - b;
+		/* update_left_panels: L = A_col * U^{-1}   panel_trf.hpp:143-157 */
+		orc_trsm_right_upper((int)rem, b, lu, lda, lu + b, lda);
+		/* update_right_panels: U = L^{-1} * A_row  panel_trf.hpp:158-171 */
+		orc_trsm_left_lower_unit(b, (int)rem, lu, lda, lu + (int64_t)b * lda, lda);
+		/* convert_left/right_panels with scale 1   panel_trf.hpp:173-233 */
+		for (int j = 0; j < b; j++)
+			orc_f32_to_f16(rem, lu + b + (int64_t)j * lda, lh + (size_t)j * rem);
+		for (int64_t j = 0; j < rem; j++)
+			orc_f32_to_f16(b, lu + (b + j) * lda, uh + (size_t)j * b);
+		/* Schur update of the trailing matrix       schur_updator.hpp:50-106 */
+		orc_shgemm_minus((int)rem, (int)rem, b, lh, rem, uh, b, lu + (int64_t)b * lda + b, lda);
+	}
+	free(lh);
+	free(uh);
+	return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* On-the-fly FP64 GEMV                                                */
+/* ------------------------------------------------------------------ */
+
+/* otf_gemv_kernel: y(0:mb) += alpha * A(0:mb, 0:nb) x with A regenerated;
+ * `seed` is the LCG state of element (0,0) of the sub-block.  Per row the
+ * reference sums even columns and odd columns in two FMA chains, folds an
+ * odd last column into the even chain, adds the chains and applies the
+ * scaled alpha with one FMA.                     otf_gemv.cpp:5-131       */
+static void otf_kernel(int64_t n, int mb, int nb, double alpha, const double *x, double *y, uint64_t s00)
+{
+	orc_coeff inc1 = coeff_default();
+	orc_coeff cn = coeff_pow(inc1, (uint64_t)n);
+	double a2 = alpha * 0x1.fffffffffffffP-65;
+	uint64_t si = s00;
+	for (int i = 0; i < mb; i++) {
+		double y0 = 0.0, y1 = 0.0;
+		uint64_t s = si;
+		int j = 0;
+		for (; j + 1 < nb; j += 2) {
+			y0 = fma((double)(int64_t)s, x[j], y0);
+			s = coeff_apply(cn, s);
+			y1 = fma((double)(int64_t)s, x[j + 1], y1);
+			s = coeff_apply(cn, s);
+		}
+		if (nb & 1) y0 = fma((double)(int64_t)s, x[nb - 1], y0);
+		y[i] = fma(y0 + y1, a2, y[i]);
+		si = coeff_apply(inc1, si);
+	}
+}
+
+/* otf_gemv_kernel_diag, with otf_gemv_small (the 64 x 64 diagonal
+ * micro-block, d on the diagonal) inlined     panel_gemv.hpp:16-55 */
+static void otf_kernel_diag(int64_t n, int b, double alpha, const double *x, double *y,
+	const double *diag, uint64_t s00)
+{
+	const int microb = 64;
+	orc_coeff inc1 = coeff_default();
+	orc_coeff jumpn = coeff_pow(inc1, (uint64_t)n);
+	orc_coeff jumpmb = coeff_pow(inc1, microb);
+	orc_coeff jumpmbn = coeff_pow(jumpn, microb);
+	orc_coeff jumppi = coeff_pow(jumpn, 0);
+	for (int pi = 0; pi < b; pi += microb) {
+		uint64_t sj = s00;
+		int bi = b - pi < microb ? b - pi : microb;
+		if (pi) {
+			otf_kernel(n, bi, pi, alpha, x, y + pi, sj);
+			sj = coeff_apply(jumppi, sj);
+		}
+		/* otf_gemv_small: rows pi..pi+bi, columns pi..pi+bi */
+		{
+			uint64_t srow = sj;
+			for (int i = 0; i < bi; ++i) {
+				uint64_t s = srow;
+				double d = diag[pi + i];
+				double t = 0.0;
+				for (int j = 0; j < bi; ++j) {
+					double aij = (i == j ? d : state_value(s));
+					t = fma(aij, x[pi + j], t);
+					s = coeff_apply(jumpn, s);
+				}
+				y[pi + i] = fma(alpha, t, y[pi + i]);
+				srow = coeff_apply(inc1, srow);
+			}
+		}
+		if (b > pi + microb) {
+			sj = coeff_apply(jumpmbn, sj);
+			otf_kernel(n, bi, b - pi - microb, alpha, x + pi + microb, y + pi, sj);
+		}
+		s00 = coeff_apply(jumpmb, s00);
+		jumppi = coeff_mul(jumppi, jumpmbn);
+	}
+}
+
+/* panel_gemv with beta = 1 on a q-column process grid collapsed into one
+ * address space: y += alpha * A x.            panel_gemv.hpp:57-83,110-180
+ * Block row pi accumulates its block columns in increasing order, split by
+ * process column (pj % q); the part on the process column that owns the
+ * diagonal starts from y, the others from zero, and the parts are then
+ * summed (MPI_Allreduce over the row, panel_gemv.hpp:178).  q = 1 is the
+ * plain sequential order; q = 2 is the grid the reference's published
+ * example ran on (README:26).                                             */
+ORC_EXPORT void orc_otf_gemv(int n, int b, int q, double alpha, const double *x, double *y,
+	uint64_t seed, const double *diag)
+{
+	int nb = n / b;
+	if (q < 1) q = 1;
+	uint64_t st0 = state_initial(seed);
+	#pragma omp parallel for schedule(dynamic, 1)
+	for (int pi = 0; pi < nb; pi++) {
+		double *part = (double *)calloc((size_t)q * b, sizeof(double));
+		int own = pi % q;
+		for (int i = 0; i < b; i++) part[(size_t)own * b + i] = y[(int64_t)pi * b + i];
+		for (int pj = 0; pj < nb; pj++) {
+			int c = pj % q;
+			orc_coeff jump = coeff_pow(coeff_default(), (uint64_t)b * pi + (uint64_t)n * b * pj);
+			uint64_t s00 = coeff_apply(jump, st0);
+			if (pi != pj)
+				otf_kernel(n, b, b, alpha, x + (int64_t)b * pj, part + (size_t)c * b, s00);
+			else
+				otf_kernel_diag(n, b, alpha, x + (int64_t)b * pj, part + (size_t)c * b,
+					diag + (int64_t)b * pi, s00);
+		}
+		for (int i = 0; i < b; i++) {
+			double s = part[(size_t)own * b + i];
+			for (int c = 0; c < q; c++) if (c != own) s = s + part[(size_t)c * b + i];
+			y[(int64_t)pi * b + i] = s;
+		}
+		free(part);
+	}
+}
+
+/* ------------------------------------------------------------------ */
+/* Triangular solves with FP32 factors and an FP64 vector               */
+/* ------------------------------------------------------------------ */
+
+/* panel_trsvL collapsed: x <- L^{-1} x, L unit lower (FP32), block size b.
+ * Per block column: subtract the accumulated partial sums of the earlier
+ * block columns, solve the diagonal block (tttrsvL), then form each lower
+ * block's partial product from zero (ttgemv_compute) and add it to that
+ * block row's running sum.               panel_trsv.hpp:115-124,207-240,310-535 */
+ORC_EXPORT void orc_trsv_lower(int n, int b, const float *a, int64_t lda, double *x)
+{
+	int nb = n / b;
+	double *w = (double *)calloc((size_t)n, sizeof(double));
+	for (int pj = 0; pj < nb; pj++) {
+		int64_t j0 = (int64_t)pj * b;
+		for (int i = 0; i < b; i++) x[j0 + i] -= w[j0 + i];
+		const float *d = a + j0 * lda + j0;
+		for (int j = 0; j + 1 < b; ++j) {
+			double al = x[j0 + j];
+			for (int i = j + 1; i < b; ++i) x[j0 + i] = fma(-al, (double)d[i + j * lda], x[j0 + i]);
+		}
+		#pragma omp parallel for schedule(static) if (n >= 8192)
+		for (int pi = pj + 1; pi < nb; pi++) {
+			int64_t i0 = (int64_t)pi * b;
+			for (int i = 0; i < b; i++) {
+				double t = 0.0;
+				for (int j = 0; j < b; j++) t = fma((double)a[(j0 + j) * lda + i0 + i], x[j0 + j], t);
+				w[i0 + i] += t;
+			}
+		}
+	}
+	free(w);
+}
+
+/* panel_trsvU collapsed: x <- U^{-1} x, U upper non-unit (FP32), sweeping
+ * block columns from the last.       panel_trsv.hpp:126-140,207-240,537-758 */
+ORC_EXPORT void orc_trsv_upper(int n, int b, const float *a, int64_t lda, double *x)
+{
+	int nb = n / b;
+	double *w = (double *)calloc((size_t)n, sizeof(double));
+	for (int pj = nb - 1; pj >= 0; pj--) {
+		int64_t j0 = (int64_t)pj * b;
+		for (int i = 0; i < b; i++) x[j0 + i] -= w[j0 + i];
+		const float *d = a + j0 * lda + j0;
+		for (int jj = b - 1; jj >= 0; --jj) {
+			x[j0 + jj] /= (double)d[jj * lda + jj];
+			double al = x[j0 + jj];
+			for (int ii = 0; ii < jj; ++ii) x[j0 + ii] = fma(-al, (double)d[jj * lda + ii], x[j0 + ii]);
+		}
+		#pragma omp parallel for schedule(static) if (n >= 8192)
+		for (int pi = 0; pi < pj; pi++) {
+			int64_t i0 = (int64_t)pi * b;
+			for (int i = 0; i < b; i++) {
+				double t = 0.0;
+				for (int j = 0; j < b; j++) t = fma((double)a[(j0 + j) * lda + i0 + i], x[j0 + j], t);
+				w[i0 + i] += t;
+			}
+		}
+	}
+	free(w);
+}
+
+/* calc_infnorm                                  panel_norm.hpp:8-19 */
+ORC_EXPORT double orc_infnorm(int n, const double *x)
+{
+	double norm = 0.0;
+	for (int i = 0; i < n; ++i) {
+		double t = x[i] >= 0.0 ? x[i] : -x[i];
+		norm = norm >= t ? norm : t;
+	}
+	return norm;
+}
+
+/* ------------------------------------------------------------------ */
+/* Iterative refinement                  iterative_refinement.hpp:18-57 */
+/* ------------------------------------------------------------------ */
+/* Returns the IRErrors pair through resid/harness ({-1,-1} when maxit
+ * steps do not reach hpl-harness < 16).  steps_resid/steps_harness (may be
+ * NULL, length >= maxit) receive the per-step log the reference prints
+ * (iterative_refinement.hpp:45).                                          */
+ORC_EXPORT int orc_refine(int n, int b, int q, const float *lu, int64_t lda, uint64_t seed,
+	const double *rhs, const double *d, int maxit, double *x,
+	double *steps_resid, double *steps_harness, int *nsteps, double *resid, double *harness)
+{
+	double *r = (double *)malloc(sizeof(double) * (size_t)n);
+	double normb = orc_infnorm(n, rhs);
+	double norma = 2.0 * orc_infnorm(n, d);      /* hpl_infnorm, panel_norm.hpp:78-84 */
+	for (int i = 0; i < n; i++) x[i] = rhs[i] / d[i];  /* x_0 = b ./ diag(A) */
+	*resid = -1.0;
+	*harness = -1.0;
+	if (nsteps) *nsteps = 0;
+	for (int it = 0; it < maxit; ++it) {
+		memcpy(r, rhs, sizeof(double) * (size_t)n);
+		double normx = orc_infnorm(n, x);
+		orc_otf_gemv(n, b, q, -1.0, x, r, seed, d);
+		double normr = orc_infnorm(n, r);
+		double hpl = normr / fma(norma, normx, normb) * 1. / (n * DBL_EPSILON / 2);
+		if (steps_resid) steps_resid[it] = normr;
+		if (steps_harness) steps_harness[it] = hpl;
+		if (nsteps) *nsteps = it + 1;
+		if (hpl < 16.) { *resid = normr; *harness = hpl; free(r); return 0; }
+		orc_trsv_lower(n, b, lu, lda, r);
+		orc_trsv_upper(n, b, lu, lda, r);
+		for (int i = 0; i < n; i++) x[i] += r[i];
+	}
+	free(r);
+	return 1;
+}
+
+/* Generate, factor and refine: the timed body of main.cpp:255-441 on one
+ * process.  Returns 0 on convergence.                                      */
+ORC_EXPORT int orc_solve(int n, int b, int q, uint64_t seed, int maxit, double *x,
+	double *steps_resid, double *steps_harness, int *nsteps, double *resid, double *harness)
+{
+	if (n <= 0 || b <= 0 || n % b) return -1;
+	int64_t lda = n;
+	float *a = (float *)malloc(sizeof(float) * (size_t)n * n);
+	double *rhs = (double *)malloc(sizeof(double) * (size_t)n);
+	double *d = (double *)malloc(sizeof(double) * (size_t)n);
+	orc_fill_matrix(n, a, lda, seed);
+	orc_gen_rhs(n, seed, rhs);
+	orc_gen_diag(n, seed, d);
+	orc_lu(n, b, a, lda);
+	int rc = orc_refine(n, b, q, a, lda, seed, rhs, d, maxit, x, steps_resid, steps_harness, nsteps, resid, harness);
+	free(a);
+	free(rhs);
+	free(d);
+	return rc;
+}
