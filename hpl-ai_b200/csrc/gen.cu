@@ -1,0 +1,166 @@
+// gen.cu -- on-device HPL-AI matrix generator, bit-exact with the reference.
+//
+// Element (i, j) of the n x n matrix is the LCG state at linear index
+// i + n*j after state_0 = a*seed + c, mapped to int64(x) * (1-2^-53)*2^-64
+// (hpl_rand.hpp:35-106).  The diagonal is replaced by the sequential FP64
+// sum of |a_ij| over j != i (hpl_rand.hpp:108-123); the right-hand side is
+// column n of the same stream (matgen.hpp:193-207).  All arithmetic here is
+// integer or explicitly rounded (__dmul_rn, __dadd_rn) so no contraction
+// can change a bit.
+#include "common.cuh"
+#include "internal.h"
+
+namespace hplai {
+
+// inc1^(2^k) for k < 64, passed by value as a kernel parameter.
+struct JumpTable {
+	Coeff p[64];
+};
+
+static JumpTable make_jump_table()
+{
+	JumpTable t;
+	Coeff p{kLcgA, kLcgC};
+	for (int k = 0; k < 64; ++k) {
+		t.p[k] = p;
+		p = coeff_mul(p, p);
+	}
+	return t;
+}
+
+static const JumpTable &jump_table()
+{
+	static const JumpTable t = make_jump_table();
+	return t;
+}
+
+__device__ __forceinline__ Coeff jump_of(const JumpTable &t, uint64_t m)
+{
+	Coeff r{1ULL, 0ULL};
+	for (int k = 0; m; ++k, m >>= 1)
+		if (m & 1ULL) r = coeff_mul(r, t.p[k]);
+	return r;
+}
+
+constexpr int kFillRows = 256;  // rows per CTA (one per thread)
+constexpr int kFillCols = 32;   // columns per CTA
+
+// a(i, j) for i in [0,nrow), j in [0,ncol) of the sub-matrix at (i0, j0).
+__global__ void __launch_bounds__(kFillRows) fill_kernel(int n, int i0, int j0, int nrow, int ncol, float *a,
+	int64_t lda, uint64_t seed, JumpTable tab)
+{
+	const int r = blockIdx.x * kFillRows + threadIdx.x;
+	const int c0 = blockIdx.y * kFillCols;
+	if (r >= nrow) return;
+	const Coeff jn = jump_of(tab, static_cast<uint64_t>(n));
+	uint64_t s = coeff_apply(jump_of(tab, static_cast<uint64_t>(i0 + r) +
+	                                          static_cast<uint64_t>(n) * static_cast<uint64_t>(j0 + c0)),
+		state_initial(seed));
+	const int c1 = min(c0 + kFillCols, ncol);
+	float *col = a + static_cast<int64_t>(c0) * lda + r;
+	for (int c = c0; c < c1; ++c) {
+		*col = __double2float_rn(state_value(s));
+		col += lda;
+		s = coeff_apply(jn, s);
+	}
+}
+
+// d_k = sum_{j != i} |a_ij| for i = i0 + k, summed in j order in FP64.
+// Four interleaved LCG chains break the state dependency; the sum stays one
+// sequential chain so the rounding matches hpl_rand.hpp:117-121 exactly.
+// Writes the FP64 value to d (if non-null) and/or its FP32 rounding to the
+// matrix diagonal a[(i - i0)*(lda+1)] (if non-null).
+__global__ void __launch_bounds__(128) diag_kernel(int n, int i0, int count, double *d, float *adiag, int64_t lda,
+	uint64_t seed, JumpTable tab)
+{
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= count) return;
+	const int i = i0 + k;
+	const Coeff jn = jump_of(tab, static_cast<uint64_t>(n));
+	const Coeff jn4 = coeff_mul(coeff_mul(jn, jn), coeff_mul(jn, jn));
+	uint64_t s0 = coeff_apply(jump_of(tab, static_cast<uint64_t>(i)), state_initial(seed));
+	uint64_t s1 = coeff_apply(jn, s0);
+	uint64_t s2 = coeff_apply(jn, s1);
+	uint64_t s3 = coeff_apply(jn, s2);
+	double sum = 0.0;
+	int j = 0;
+	for (; j + 3 < n; j += 4) {
+		const double v0 = fabs(state_value(s0));
+		const double v1 = fabs(state_value(s1));
+		const double v2 = fabs(state_value(s2));
+		const double v3 = fabs(state_value(s3));
+		if (j != i) sum = __dadd_rn(sum, v0);
+		if (j + 1 != i) sum = __dadd_rn(sum, v1);
+		if (j + 2 != i) sum = __dadd_rn(sum, v2);
+		if (j + 3 != i) sum = __dadd_rn(sum, v3);
+		s0 = coeff_apply(jn4, s0);
+		s1 = coeff_apply(jn4, s1);
+		s2 = coeff_apply(jn4, s2);
+		s3 = coeff_apply(jn4, s3);
+	}
+	for (; j < n; ++j) {
+		if (j != i) sum = __dadd_rn(sum, fabs(state_value(s0)));
+		s0 = coeff_apply(jn, s0);
+	}
+	if (d) d[k] = sum;
+	if (adiag) adiag[static_cast<int64_t>(k) * (lda + 1)] = __double2float_rn(sum);
+}
+
+// rhs_k = element (i0 + k, n) in FP64.
+__global__ void rhs_kernel(int n, int count, double *rhs, uint64_t seed, JumpTable tab)
+{
+	const int k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k >= count) return;
+	const uint64_t idx = static_cast<uint64_t>(k) + static_cast<uint64_t>(n) * static_cast<uint64_t>(n);
+	rhs[k] = state_value(coeff_apply(jump_of(tab, idx), state_initial(seed)));
+}
+
+int launch_fill(int n, int i0, int j0, int nrow, int ncol, float *a, int64_t lda, uint64_t seed, int calc_diag,
+	cudaStream_t st)
+{
+	if (nrow <= 0 || ncol <= 0) return HPLAI_OK;
+	dim3 grid((nrow + kFillRows - 1) / kFillRows, (ncol + kFillCols - 1) / kFillCols);
+	fill_kernel<<<grid, kFillRows, 0, st>>>(n, i0, j0, nrow, ncol, a, lda, seed, jump_table());
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	if (calc_diag && i0 == j0 && nrow == ncol) {
+		diag_kernel<<<(nrow + 127) / 128, 128, 0, st>>>(n, i0, nrow, nullptr, a, lda, seed, jump_table());
+		HPLAI_CUDA_TRY(cudaGetLastError());
+	}
+	return HPLAI_OK;
+}
+
+int launch_diag(int n, int i0, int count, double *d, float *adiag, int64_t lda, uint64_t seed, cudaStream_t st)
+{
+	if (count <= 0) return HPLAI_OK;
+	diag_kernel<<<(count + 127) / 128, 128, 0, st>>>(n, i0, count, d, adiag, lda, seed, jump_table());
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+int launch_rhs(int n, double *rhs, uint64_t seed, cudaStream_t st)
+{
+	rhs_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, n, rhs, seed, jump_table());
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+} // namespace hplai
+
+extern "C" int hplai_fill_panel(int n, int i0, int j0, int nrow, int ncol, float *a, int64_t lda, uint64_t seed,
+	int calc_diag, void *stream)
+{
+	if (n <= 0 || i0 < 0 || j0 < 0 || nrow < 0 || ncol < 0 || !a || lda < nrow) return HPLAI_EINVAL;
+	return hplai::launch_fill(n, i0, j0, nrow, ncol, a, lda, seed, calc_diag, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hplai_gen_rhs(int n, uint64_t seed, double *rhs, void *stream)
+{
+	if (n <= 0 || !rhs) return HPLAI_EINVAL;
+	return hplai::launch_rhs(n, rhs, seed, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hplai_gen_diag(int n, uint64_t seed, int i0, int count, double *d, void *stream)
+{
+	if (n <= 0 || i0 < 0 || count < 0 || i0 + count > n || !d) return HPLAI_EINVAL;
+	return hplai::launch_diag(n, i0, count, d, nullptr, 0, seed, static_cast<cudaStream_t>(stream));
+}

@@ -1,0 +1,57 @@
+// internal.h -- launch functions shared between the translation units of
+// libhplai.  Every function enqueues work on `st` and returns an
+// hplai_status; none of them allocates device memory.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <cuda_runtime.h>
+
+namespace hplai {
+
+// gen.cu
+int launch_fill(int n, int i0, int j0, int nrow, int ncol, float *a, int64_t lda, uint64_t seed, int calc_diag,
+	cudaStream_t st);
+int launch_diag(int n, int i0, int count, double *d, float *adiag, int64_t lda, uint64_t seed, cudaStream_t st);
+int launch_rhs(int n, double *rhs, uint64_t seed, cudaStream_t st);
+
+// panel.cu
+int launch_getrf(int b, float *a, int64_t lda, cudaStream_t st);
+int launch_trsm_right_upper(int m, int b, const float *u, int64_t ldu, float *a, int64_t lda, uint16_t *lh,
+	int64_t ldh, float scale, cudaStream_t st);
+int launch_trsm_left_lower(int b, int ncols, const float *l, int64_t ldl, float *a, int64_t lda, uint16_t *uh,
+	int64_t ldh, float scale, cudaStream_t st);
+
+// schur.cu
+// Tensor maps for the FP16 panel buffers are built once per buffer and
+// reused for every step; `SchurMaps` is opaque storage for two CUtensorMap.
+struct SchurMaps {
+	alignas(64) unsigned char lmap[128];
+	alignas(64) unsigned char umap[128];
+	int k;       // inner dimension (panel width)
+};
+// L: lrows x k FP16, row-major with ldl; U: urows x k FP16 (row j = column j
+// of U), ldu.  Rows beyond lrows/urows read as zero.
+int schur_make_maps(SchurMaps *m, const uint16_t *lh, int lrows, int64_t ldl, const uint16_t *uh, int urows,
+	int64_t ldu, int k);
+// C (m x n, ldc) -= L[lrow0 : lrow0+m, 0:k] * U[urow0 : urow0+n, 0:k]^T
+int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc,
+	cudaStream_t st);
+int schur_status();          // HPLAI_ETIMEOUT if a device wait ran out since the last reset
+void schur_status_reset();
+
+// refine.cu
+size_t otf_gemv_workspace(int n);
+int launch_otf_gemv(int n, double alpha, const double *x, double beta, double *y, uint64_t seed,
+	const double *diag, void *work, size_t work_bytes, cudaStream_t st);
+int launch_otf_gemv_block(int64_t n, int mb, int nb, double alpha, const double *x, double *y, uint64_t state00,
+	void *work, size_t work_bytes, cudaStream_t st);
+size_t trsv_workspace(int n);
+int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes,
+	cudaStream_t st);
+int trsv_status(void *work, cudaStream_t st, int *status);
+int launch_infnorm(int n, const double *x, double *out, cudaStream_t st);
+int launch_div(int n, const double *num, const double *den, double *out, cudaStream_t st);
+int launch_axpy1(int n, const double *x, double *y, cudaStream_t st);
+
+} // namespace hplai

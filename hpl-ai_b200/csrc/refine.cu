@@ -1,0 +1,447 @@
+// refine.cu -- FP64 kernels of the iterative refinement.
+//
+//  otf_gemv        y <- beta*y + alpha*A x with A regenerated from the LCG in
+//                  FP64 (panel_gemv.hpp:57-180, otf_gemv.cpp:5-131); the
+//                  diagonal comes from the FP64 diagonal vector.
+//  trsv            x <- L^{-1} x or U^{-1} x with the FP32 LU factors and an
+//                  FP64 vector (panel_trsv.hpp:310-758), one persistent
+//                  cooperative launch with block-row flags.
+//  infnorm, div, axpy   the vector helpers of panel_norm.hpp / panel.hpp.
+#include "common.cuh"
+#include "internal.h"
+
+namespace hplai {
+
+namespace {
+
+struct JumpTable64 {
+	Coeff p[64];
+};
+
+JumpTable64 make_table()
+{
+	JumpTable64 t;
+	Coeff p{kLcgA, kLcgC};
+	for (int k = 0; k < 64; ++k) {
+		t.p[k] = p;
+		p = coeff_mul(p, p);
+	}
+	return t;
+}
+
+const JumpTable64 &table()
+{
+	static const JumpTable64 t = make_table();
+	return t;
+}
+
+__device__ __forceinline__ Coeff jump_of(const JumpTable64 &t, uint64_t m)
+{
+	Coeff r{1ULL, 0ULL};
+	for (int k = 0; m; ++k, m >>= 1)
+		if (m & 1ULL) r = coeff_mul(r, t.p[k]);
+	return r;
+}
+
+// ---------------------------------------------------------------------------
+// On-the-fly GEMV.  CTA = 256 rows x GEMV_COLS columns; each thread walks
+// its row across the column chunk with four interleaved LCG chains
+// (state jumps by n per column) and two FP64 accumulators.  Partial sums
+// go to the workspace and a second kernel folds them in a fixed order, so
+// the result does not depend on scheduling.
+// ---------------------------------------------------------------------------
+constexpr int GEMV_ROWS = 256;
+constexpr int GEMV_COLS = 2048;
+
+__global__ void __launch_bounds__(GEMV_ROWS) otf_partial_kernel(int64_t n, int mb, int nb, double alpha,
+	const double *__restrict__ x, uint64_t state00, int with_diag, const double *__restrict__ diag,
+	double *__restrict__ part, JumpTable64 tab)
+{
+	__shared__ double xs[GEMV_COLS];
+	const int j0 = blockIdx.y * GEMV_COLS;
+	const int j1 = min(j0 + GEMV_COLS, nb);
+	for (int j = threadIdx.x; j < j1 - j0; j += GEMV_ROWS) xs[j] = x[j0 + j];
+	__syncthreads();
+	const int i = blockIdx.x * GEMV_ROWS + threadIdx.x;
+	if (i >= mb) return;
+	const Coeff jn = jump_of(tab, static_cast<uint64_t>(n));
+	const Coeff jn4 = coeff_mul(coeff_mul(jn, jn), coeff_mul(jn, jn));
+	uint64_t s0 = coeff_apply(jump_of(tab, static_cast<uint64_t>(i) + static_cast<uint64_t>(n) * j0), state00);
+	uint64_t s1 = coeff_apply(jn, s0);
+	uint64_t s2 = coeff_apply(jn, s1);
+	uint64_t s3 = coeff_apply(jn, s2);
+	double a0 = 0.0, a1 = 0.0;
+	const int len = j1 - j0;
+	const int dj = (with_diag && i >= j0 && i < j1) ? i - j0 : -1;   // diagonal column inside the chunk
+	int j = 0;
+	for (; j + 3 < len; j += 4) {
+		double v0 = __ll2double_rn(static_cast<long long>(s0));
+		double v1 = __ll2double_rn(static_cast<long long>(s1));
+		double v2 = __ll2double_rn(static_cast<long long>(s2));
+		double v3 = __ll2double_rn(static_cast<long long>(s3));
+		if (dj >= j && dj < j + 4) {
+			if (dj == j) v0 = 0.0;
+			if (dj == j + 1) v1 = 0.0;
+			if (dj == j + 2) v2 = 0.0;
+			if (dj == j + 3) v3 = 0.0;
+		}
+		a0 = fma(v0, xs[j], a0);
+		a1 = fma(v1, xs[j + 1], a1);
+		a0 = fma(v2, xs[j + 2], a0);
+		a1 = fma(v3, xs[j + 3], a1);
+		s0 = coeff_apply(jn4, s0);
+		s1 = coeff_apply(jn4, s1);
+		s2 = coeff_apply(jn4, s2);
+		s3 = coeff_apply(jn4, s3);
+	}
+	for (; j < len; ++j) {
+		const double v = (j == dj) ? 0.0 : __ll2double_rn(static_cast<long long>(s0));
+		a0 = fma(v, xs[j], a0);
+		s0 = coeff_apply(jn, s0);
+	}
+	double r = (a0 + a1) * (alpha * kValueScale);
+	if (dj >= 0) r = fma(alpha * diag[i], xs[dj], r);
+	part[static_cast<int64_t>(blockIdx.y) * mb + i] = r;
+}
+
+__global__ void otf_reduce_kernel(int mb, int nchunks, double beta, const double *__restrict__ part, double *y,
+	int overwrite)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= mb) return;
+	double s = 0.0;
+	for (int c = 0; c < nchunks; ++c) s += part[static_cast<int64_t>(c) * mb + i];
+	y[i] = overwrite ? s : fma(beta, y[i], s);
+}
+
+int otf_launch(int64_t n, int mb, int nb, double alpha, const double *x, double beta, double *y,
+	uint64_t state00, int with_diag, const double *diag, void *work, size_t work_bytes, cudaStream_t st)
+{
+	if (mb <= 0) return HPLAI_OK;
+	const int nchunks = (nb + GEMV_COLS - 1) / GEMV_COLS;
+	if (work_bytes < static_cast<size_t>(nchunks) * mb * sizeof(double)) return HPLAI_EINVAL;
+	double *part = static_cast<double *>(work);
+	if (nb > 0) {
+		dim3 grid((mb + GEMV_ROWS - 1) / GEMV_ROWS, nchunks);
+		otf_partial_kernel<<<grid, GEMV_ROWS, 0, st>>>(n, mb, nb, alpha, x, state00, with_diag, diag, part, table());
+		HPLAI_CUDA_TRY(cudaGetLastError());
+	}
+	otf_reduce_kernel<<<(mb + 255) / 256, 256, 0, st>>>(mb, nb > 0 ? nchunks : 0, beta, part, y,
+		beta == 0.0 ? 1 : 0);
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Triangular solves.  Block rows of TB; CTA c handles block rows c, c+G, ...
+// in solve order, accumulating the off-diagonal products as the block
+// columns it depends on are published (flag[cb] == epoch), then solving its
+// diagonal block with warp shuffles and publishing x for that block.
+// Progress is guaranteed because every CTA is resident (cooperative launch)
+// and each works through its rows in dependency order.  Every spin is
+// bounded; a timeout sets the status word and the kernel returns.
+// ---------------------------------------------------------------------------
+constexpr int TB = 128;
+constexpr int TRSV_THREADS = 256;
+
+struct TrsvWork {
+	uint32_t epoch;
+	uint32_t status;
+	uint32_t pad[2];
+	// followed by flags[nbt]
+};
+
+__global__ void trsv_epoch_kernel(TrsvWork *w)
+{
+	w->epoch += 1;
+	w->status = 0;
+}
+
+__global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, const float *__restrict__ a,
+	int64_t lda, double *x, TrsvWork *w)
+{
+	extern __shared__ float dyn_smem[];
+	float (*dblk)[TB + 1] = reinterpret_cast<float (*)[TB + 1]>(dyn_smem);   // dblk[i][j] = A[r0+i][r0+j]
+	__shared__ double xs[TB];            // x of the block column being applied
+	__shared__ double part[2][TB];       // partial sums of the two column halves
+	__shared__ double rhs[TB];
+	__shared__ int ready_upto;
+	__shared__ int abort_flag;
+
+	uint32_t *flags = reinterpret_cast<uint32_t *>(w + 1);
+	const uint32_t epoch = *reinterpret_cast<volatile uint32_t *>(&w->epoch);
+	const int nbt = (n + TB - 1) / TB;
+	const int t = threadIdx.x;
+	const int lr = t % TB, grp = t / TB;   // row within the block, column half
+
+	if (t == 0) abort_flag = 0;
+	for (int idx = blockIdx.x; idx < nbt; idx += gridDim.x) {
+		const int r = lower ? idx : nbt - 1 - idx;
+		const int r0 = r * TB;
+		const int rows = min(TB, n - r0);
+		// Stage the diagonal block (independent of other CTAs).
+		for (int e = t; e < TB * TB; e += TRSV_THREADS) {
+			const int i = e % TB, j = e / TB;
+			dblk[i][j] = (i < rows && j < rows) ? a[static_cast<int64_t>(r0 + j) * lda + r0 + i] : 0.f;
+		}
+		if (t == 0) ready_upto = lower ? 0 : nbt - 1;
+		double acc = 0.0;
+		__syncthreads();
+		// Off-diagonal block columns in dependency order.
+		const int nblk = lower ? r : nbt - 1 - r;
+		for (int q = 0; q < nblk; ++q) {
+			const int cb = lower ? q : nbt - 1 - q;
+			if (t < 32) {
+				// Learn how far the published prefix reaches, 32 flags at a time.
+				bool have = lower ? (cb < ready_upto) : (cb > ready_upto);
+				if (!have) {
+					const uint64_t t0 = global_ns();
+					while (true) {
+						const int probe = lower ? cb + t : cb - t;
+						const bool inb = lower ? (probe < r) : (probe > r);
+						const bool rdy = inb && ld_acquire_u32(&flags[probe]) == epoch;
+						const unsigned m = __ballot_sync(0xffffffffu, rdy);
+						const int cnt = __ffs(~m) - 1;   // leading ready flags
+						const int c = (m == 0xffffffffu) ? 32 : cnt;
+						if (c > 0) {
+							if (t == 0) ready_upto = lower ? cb + c : cb - c;
+							break;
+						}
+						// the decision to give up is taken by the whole warp at once
+						if (__ballot_sync(0xffffffffu, global_ns() - t0 > kWaitLimitNs)) {
+							if (t == 0) abort_flag = 1;
+							break;
+						}
+						__nanosleep(200);
+					}
+				}
+			}
+			__syncthreads();
+			if (abort_flag) break;
+			if (t < TB) {
+				const int j = cb * TB + t;
+				xs[t] = (j < n) ? __ldcg(&x[j]) : 0.0;   // published by another CTA: bypass L1
+			}
+			__syncthreads();
+			if (lr < rows) {
+				const float *col = a + static_cast<int64_t>(cb * TB) * lda + r0 + lr;
+				const int cols = min(TB, n - cb * TB);
+				const int jb = grp * (TB / 2), je = min(jb + TB / 2, cols);
+#pragma unroll 8
+				for (int j = jb; j < je; ++j) acc = fma(static_cast<double>(col[static_cast<int64_t>(j) * lda]), xs[j], acc);
+			}
+			__syncthreads();
+		}
+		if (abort_flag) break;
+		part[grp][lr] = acc;
+		__syncthreads();
+		if (t < TB) rhs[t] = (t < rows) ? x[r0 + t] - (part[0][t] + part[1][t]) : 0.0;
+		__syncthreads();
+		// Diagonal block: 32-row sub-blocks solved by warp 0 with shuffles,
+		// the remaining rows updated by all threads.
+		const int nsb = (rows + 31) / 32;
+		for (int s = 0; s < nsb; ++s) {
+			const int sb = lower ? s : nsb - 1 - s;
+			const int base = sb * 32;
+			if (t < 32) {
+				const int i = base + t;
+				double v = (i < rows) ? rhs[i] : 0.0;
+				if (lower) {
+					for (int j = 0; j < 32; ++j) {
+						const double xj = __shfl_sync(0xffffffffu, v, j);
+						if (t > j && base + j < rows) v = fma(-static_cast<double>(dblk[i][base + j]), xj, v);
+					}
+				} else {
+					for (int j = 31; j >= 0; --j) {
+						if (t == j && i < rows) v = v / static_cast<double>(dblk[i][i]);
+						const double xj = __shfl_sync(0xffffffffu, v, j);
+						if (t < j && base + j < rows) v = fma(-static_cast<double>(dblk[i][base + j]), xj, v);
+					}
+				}
+				if (i < rows) rhs[i] = v;
+			}
+			__syncthreads();
+			// rows still to solve: below (lower) or above (upper) this sub-block
+			const int lo = lower ? base + 32 : 0;
+			const int hi = lower ? rows : base;
+			for (int i = lo + t; i < hi; i += TRSV_THREADS) {
+				double v = rhs[i];
+				for (int j = 0; j < 32 && base + j < rows; ++j) v = fma(-static_cast<double>(dblk[i][base + j]), rhs[base + j], v);
+				rhs[i] = v;
+			}
+			__syncthreads();
+		}
+		if (t < rows) x[r0 + t] = rhs[t];
+		__threadfence();
+		__syncthreads();
+		if (t == 0) st_release_u32(&flags[r], epoch);
+	}
+	if (t == 0 && abort_flag) atomicOr(&w->status, 1u);
+}
+
+// ---------------------------------------------------------------------------
+// Vector helpers.
+// ---------------------------------------------------------------------------
+__global__ void infnorm_kernel(int n, const double *__restrict__ x, unsigned long long *out)
+{
+	// max that propagates NaN, so a diverged vector cannot report a finite norm
+	auto vmax = [](double p, double q) { return (q != q || q > p) ? q : p; };
+	double m = 0.0;
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = vmax(m, fabs(x[i]));
+	for (int o = 16; o; o >>= 1) m = vmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+	__shared__ double wm[32];
+	if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+	__syncthreads();
+	if (threadIdx.x < 32) {
+		m = (threadIdx.x < (blockDim.x + 31) / 32) ? wm[threadIdx.x] : 0.0;
+		for (int o = 16; o; o >>= 1) m = vmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+		// non-negative doubles order like their bit patterns
+		if (threadIdx.x == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(m)));
+	}
+}
+
+__global__ void div_kernel(int n, const double *__restrict__ num, const double *__restrict__ den, double *out)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) out[i] = num[i] / den[i];
+}
+
+__global__ void axpy1_kernel(int n, const double *__restrict__ x, double *y)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) y[i] += x[i];
+}
+
+} // namespace
+
+size_t otf_gemv_workspace(int n)
+{
+	if (n <= 0) return 0;
+	const size_t nchunks = (static_cast<size_t>(n) + GEMV_COLS - 1) / GEMV_COLS;
+	return nchunks * static_cast<size_t>(n) * sizeof(double);
+}
+
+int launch_otf_gemv(int n, double alpha, const double *x, double beta, double *y, uint64_t seed, const double *diag,
+	void *work, size_t work_bytes, cudaStream_t st)
+{
+	return otf_launch(n, n, n, alpha, x, beta, y, state_initial(seed), 1, diag, work, work_bytes, st);
+}
+
+int launch_otf_gemv_block(int64_t n, int mb, int nb, double alpha, const double *x, double *y, uint64_t state00,
+	void *work, size_t work_bytes, cudaStream_t st)
+{
+	return otf_launch(n, mb, nb, alpha, x, 1.0, y, state00, 0, nullptr, work, work_bytes, st);
+}
+
+size_t trsv_workspace(int n)
+{
+	const size_t nbt = (static_cast<size_t>(n) + TB - 1) / TB;
+	return sizeof(TrsvWork) + nbt * sizeof(uint32_t);
+}
+
+int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes,
+	cudaStream_t st)
+{
+	if (n <= 0) return HPLAI_OK;
+	if (!work || work_bytes < trsv_workspace(n)) return HPLAI_EINVAL;
+	constexpr size_t dsmem = sizeof(float) * TB * (TB + 1);
+	static int max_blocks = 0;
+	if (!max_blocks) {
+		int per_sm = 0, dev = 0, sms = 0;
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(dsmem)));
+		HPLAI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_kernel, TRSV_THREADS, dsmem));
+		HPLAI_CUDA_TRY(cudaGetDevice(&dev));
+		HPLAI_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+		max_blocks = per_sm * sms;
+		if (max_blocks <= 0) return HPLAI_EUNSUPPORTED;
+	}
+	TrsvWork *w = static_cast<TrsvWork *>(work);
+	trsv_epoch_kernel<<<1, 1, 0, st>>>(w);
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	const int nbt = (n + TB - 1) / TB;
+	const int grid = nbt < max_blocks ? nbt : max_blocks;
+	int lw = lower ? 1 : 0;
+	void *args[] = {(void *)&lw, (void *)&n, (void *)&a, (void *)&lda, (void *)&x, (void *)&w};
+	HPLAI_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(trsv_kernel), dim3(grid), dim3(TRSV_THREADS),
+		args, dsmem, st));
+	return HPLAI_OK;
+}
+
+int trsv_status(void *work, cudaStream_t st, int *status)
+{
+	uint32_t v = 0;
+	TrsvWork *w = static_cast<TrsvWork *>(work);
+	HPLAI_CUDA_TRY(cudaMemcpyAsync(&v, &w->status, sizeof(v), cudaMemcpyDeviceToHost, st));
+	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
+	*status = v ? HPLAI_ETIMEOUT : HPLAI_OK;
+	return HPLAI_OK;
+}
+
+int launch_infnorm(int n, const double *x, double *out, cudaStream_t st)
+{
+	HPLAI_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double), st));
+	if (n <= 0) return HPLAI_OK;
+	int blocks = (n + 255) / 256;
+	if (blocks > 1184) blocks = 1184;
+	infnorm_kernel<<<blocks, 256, 0, st>>>(n, x, reinterpret_cast<unsigned long long *>(out));
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+int launch_div(int n, const double *num, const double *den, double *out, cudaStream_t st)
+{
+	if (n <= 0) return HPLAI_OK;
+	div_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, num, den, out);
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+int launch_axpy1(int n, const double *x, double *y, cudaStream_t st)
+{
+	if (n <= 0) return HPLAI_OK;
+	axpy1_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, x, y);
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+} // namespace hplai
+
+extern "C" size_t hplai_otf_gemv_workspace(int n) { return hplai::otf_gemv_workspace(n); }
+
+extern "C" int hplai_otf_gemv(int n, double alpha, const double *x, double beta, double *y, uint64_t seed,
+	const double *diag, void *work, size_t work_bytes, void *stream)
+{
+	if (n <= 0 || !x || !y || !diag || !work) return HPLAI_EINVAL;
+	return hplai::launch_otf_gemv(n, alpha, x, beta, y, seed, diag, work, work_bytes, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hplai_otf_gemv_block(int64_t n, int mb, int nb, double alpha, const double *x, double *y,
+	uint64_t state00, void *work, size_t work_bytes, void *stream)
+{
+	if (n <= 0 || mb < 0 || nb < 0 || !x || !y || !work) return HPLAI_EINVAL;
+	return hplai::launch_otf_gemv_block(n, mb, nb, alpha, x, y, state00, work, work_bytes,
+		static_cast<cudaStream_t>(stream));
+}
+
+extern "C" size_t hplai_trsv_workspace(int n) { return hplai::trsv_workspace(n); }
+
+extern "C" int hplai_trsv_lower(int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes,
+	void *stream)
+{
+	if (n <= 0 || !a || !x || lda < n) return HPLAI_EINVAL;
+	return hplai::launch_trsv(true, n, a, lda, x, work, work_bytes, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hplai_trsv_upper(int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes,
+	void *stream)
+{
+	if (n <= 0 || !a || !x || lda < n) return HPLAI_EINVAL;
+	return hplai::launch_trsv(false, n, a, lda, x, work, work_bytes, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hplai_infnorm(int n, const double *x, double *out, void *stream)
+{
+	if (n < 0 || (!x && n) || !out) return HPLAI_EINVAL;
+	return hplai::launch_infnorm(n, x, out, static_cast<cudaStream_t>(stream));
+}

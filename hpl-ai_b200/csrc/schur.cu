@@ -1,0 +1,346 @@
+// schur.cu -- the Schur complement update C -= L * U on tcgen05 tensor cores.
+//
+// The reference's gemmschur -> shgemm (schur_updator.hpp:24-31,
+// fp16sim.hpp:216-233, kernels/avx2.cpp:249-302) multiplies FP16 panels
+// and accumulates in FP32 into the FP32 trailing matrix.  Here one
+// persistent, warp-specialised kernel does the same on sm_100a:
+//
+//   warp 0      TMA producer: 128x64 (L) and 256x64 (U) FP16 tiles, 128B
+//               swizzle, into a 4-stage shared-memory ring; also prefetches
+//               the C tile into L2 ahead of its epilogue.
+//   warp 1      allocates 512 TMEM columns (two 128x256 FP32 accumulators)
+//               and one elected thread issues tcgen05.mma (M=128, N=256,
+//               K=16, kind::f16); tcgen05.commit releases ring stages and
+//               publishes finished accumulators.
+//   warps 2-5   epilogue: tcgen05.ld of the accumulator (lane = row),
+//               C[row, col] = C[row, col] - acc in FP32, coalesced per warp.
+//
+// The accumulator is double buffered so the epilogue of tile i overlaps
+// the MMAs of tile i+1.  Every wait is bounded; a timeout sets the status
+// word and the kernel drains and frees TMEM before returning.
+#include "common.cuh"
+#include "internal.h"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cstring>
+
+namespace hplai {
+
+namespace {
+
+constexpr int BM = 128;
+constexpr int BN = 256;
+constexpr int BK = 64;                 // one 128-byte swizzle row of FP16
+constexpr int STAGES = 4;
+constexpr int A_BYTES = BM * BK * 2;   // 16 KB
+constexpr int B_BYTES = BN * BK * 2;   // 32 KB
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int EPI_WARPS = 4;
+constexpr int THREADS = (2 + EPI_WARPS) * 32;
+constexpr uint32_t TMEM_COLS = 2 * BN;
+constexpr size_t SMEM_BYTES = static_cast<size_t>(STAGES) * STAGE_BYTES + 1024 + 256;
+
+static_assert(TMEM_COLS <= 512, "two accumulators must fit in TMEM");
+
+struct Params {
+	float *c;
+	int64_t ldc;
+	int m, n;
+	int num_kc;       // K chunks of BK
+	int lrow0, urow0; // first L row / first U row (= C column) in the panel buffers
+	int tiles_m, tiles_n;
+};
+
+__device__ unsigned int g_status;
+
+__device__ __forceinline__ void prefetch_c_tile(const Params &p, int tm, int tn, int lane)
+{
+	// 16-byte aligned runs of each column of the tile, 8 columns per lane.
+	const int row0 = tm * BM;
+	const int nrows = min(BM, p.m - row0);
+	for (int cc = lane; cc < BN; cc += 32) {
+		const int col = tn * BN + cc;
+		if (col >= p.n) break;
+		const uintptr_t beg = reinterpret_cast<uintptr_t>(p.c + row0 + static_cast<int64_t>(col) * p.ldc);
+		const uintptr_t end = beg + static_cast<uintptr_t>(nrows) * sizeof(float);
+		const uintptr_t abeg = beg & ~static_cast<uintptr_t>(15);
+		const uintptr_t aend = end & ~static_cast<uintptr_t>(15);
+		if (aend > abeg)
+			asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(abeg), "r"(static_cast<uint32_t>(aend - abeg))
+				: "memory");
+	}
+}
+
+__global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant__ CUtensorMap lmap,
+	const __grid_constant__ CUtensorMap umap, const Params p)
+{
+	extern __shared__ uint8_t smem_raw[];
+	const uint32_t raw_addr = smem_u32(smem_raw);
+	uint8_t *smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
+	uint8_t *sA = smem;
+	uint8_t *sB = smem + STAGES * A_BYTES;
+	uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+	uint64_t *full = bars;
+	uint64_t *empty = bars + STAGES;
+	uint64_t *accf = bars + 2 * STAGES;
+	uint64_t *acce = accf + 2;
+	uint64_t *drain = acce + 2;
+	uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(drain + 1);
+	int *consumed = reinterpret_cast<int *>(tmem_holder + 1);   // stages the MMA warp consumed
+
+	const int warp = threadIdx.x >> 5;
+	const int lane = threadIdx.x & 31;
+
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < STAGES; ++s) {
+			mbar_init(&full[s], 1);
+			mbar_init(&empty[s], 1);
+		}
+		for (int a = 0; a < 2; ++a) {
+			mbar_init(&accf[a], 1);
+			mbar_init(&acce[a], EPI_WARPS * 32);
+		}
+		mbar_init(drain, 1);
+		*consumed = 0;
+		fence_mbar_init();
+	}
+	if (warp == 1) {
+		tmem_alloc(tmem_holder, TMEM_COLS);
+		tmem_relinquish();
+	}
+	if (warp == 0 && lane == 0) {
+		tma_prefetch_desc(&lmap);
+		tma_prefetch_desc(&umap);
+	}
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem_base = *tmem_holder;
+
+	const int total = p.tiles_m * p.tiles_n;
+	int issued = 0;   // producer: stages issued
+
+	if (warp == 0) {
+		// ---------------- TMA producer ----------------
+		bool ok = true;
+		int stage = 0;
+		uint32_t phase = 0;
+		for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
+			const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+			prefetch_c_tile(p, tm, tn, lane);
+			if (lane == 0) {
+				for (int kc = 0; kc < p.num_kc; ++kc) {
+					if (!mbar_wait(&empty[stage], phase ^ 1u)) { ok = false; break; }
+					mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+					tma_load_2d(sA + stage * A_BYTES, &lmap, &full[stage], kc * BK, p.lrow0 + tm * BM);
+					tma_load_2d(sB + stage * B_BYTES, &umap, &full[stage], kc * BK, p.urow0 + tn * BN);
+					++issued;
+					if (++stage == STAGES) { stage = 0; phase ^= 1u; }
+				}
+			}
+			ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+		}
+		if (lane == 0 && !ok) atomicOr(&g_status, 1u);
+	} else if (warp == 1) {
+		// ---------------- MMA issuer ----------------
+		if (lane == 0) {
+			bool ok = true;
+			int stage = 0;
+			uint32_t phase = 0;
+			int acc = 0;
+			uint32_t acc_phase = 0;
+			int used = 0;
+			const uint32_t idesc = umma_idesc_f16(BM, BN);
+			for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
+				if (!mbar_wait(&acce[acc], acc_phase ^ 1u)) { ok = false; break; }
+				tc_fence_after();
+				const uint32_t d_tmem = tmem_base + static_cast<uint32_t>(acc * BN);
+				for (int kc = 0; kc < p.num_kc; ++kc) {
+					if (!mbar_wait(&full[stage], phase)) { ok = false; break; }
+					tc_fence_after();
+					const uint64_t adesc = umma_desc_k_sw128(smem_u32(sA + stage * A_BYTES));
+					const uint64_t bdesc = umma_desc_k_sw128(smem_u32(sB + stage * B_BYTES));
+#pragma unroll
+					for (int kk = 0; kk < BK / 16; ++kk) {
+						// advance 16 FP16 = 32 bytes (2 units of 16 B) along K inside the swizzle row
+						umma_f16(d_tmem, adesc + 2u * kk, bdesc + 2u * kk, idesc, (kc | kk) != 0 ? 1u : 0u);
+					}
+					umma_commit(&empty[stage]);
+					++used;
+					if (++stage == STAGES) { stage = 0; phase ^= 1u; }
+				}
+				if (!ok) break;
+				umma_commit(&accf[acc]);
+				if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+			}
+			// Every MMA of this thread completes before TMEM is released.
+			umma_commit(drain);
+			if (!mbar_wait(drain, 0)) ok = false;
+			*consumed = used;
+			if (!ok) atomicOr(&g_status, 1u);
+		}
+	} else {
+		// ---------------- epilogue ----------------
+		const int q = warp & 3;   // TMEM lane quarter this warp may access
+		bool ok = true;
+		int acc = 0;
+		uint32_t acc_phase = 0;
+		for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
+			const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+			const bool mine = mbar_wait(&accf[acc], acc_phase);
+			ok = __all_sync(0xffffffffu, mine) != 0;
+			if (!ok) break;
+			tc_fence_after();
+			const int row = tm * BM + q * 32 + lane;
+			const bool rok = row < p.m;
+			float *crow = p.c + row;
+			const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * BN);
+#pragma unroll 1
+			for (int ch = 0; ch < BN / 32; ++ch) {
+				uint32_t r[32];
+				tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(ch * 32), r);
+				tmem_ld_wait();
+				const int col0 = tn * BN + ch * 32;
+				if (rok) {
+					float cv[32];
+#pragma unroll
+					for (int j = 0; j < 32; ++j)
+						if (col0 + j < p.n) cv[j] = crow[static_cast<int64_t>(col0 + j) * p.ldc];
+#pragma unroll
+					for (int j = 0; j < 32; ++j)
+						if (col0 + j < p.n) crow[static_cast<int64_t>(col0 + j) * p.ldc] = cv[j] - __uint_as_float(r[j]);
+				}
+			}
+			tc_fence_before();
+			mbar_arrive(&acce[acc]);
+			if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+		}
+		if (lane == 0 && !ok) atomicOr(&g_status, 1u);
+	}
+
+	tc_fence_before();
+	__syncthreads();
+	if (warp == 0 && lane == 0) {
+		// Loads issued but never consumed (only after a timeout) land before exit.
+		int left = issued - *consumed;
+		for (int s = 0; left > 0 && s < STAGES; ++s, --left) {
+			(void)mbar_wait(&full[(*consumed + s) % STAGES], static_cast<uint32_t>(((*consumed + s) / STAGES) & 1));
+		}
+	}
+	if (warp == 1) {
+		tc_fence_after();
+		tmem_dealloc(tmem_base, TMEM_COLS);
+	}
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	if (!fn) {
+		void *ptr = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+			q == cudaDriverEntryPointSuccess)
+			fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+	}
+	return fn;
+}
+
+int make_map_f16(void *out, const void *base, uint64_t inner, uint64_t outer, uint64_t ld_elems, uint32_t box_inner,
+	uint32_t box_outer)
+{
+	auto fn = encode_fn();
+	if (!fn) return HPLAI_ECUDA;
+	if ((reinterpret_cast<uintptr_t>(base) & 15u) || ((ld_elems * 2) & 15u)) return HPLAI_EINVAL;
+	CUtensorMap m;
+	cuuint64_t dims[2] = {inner, outer};
+	cuuint64_t strides[1] = {ld_elems * 2};
+	cuuint32_t box[2] = {box_inner, box_outer};
+	cuuint32_t estr[2] = {1, 1};
+	CUresult r = fn(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+		CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+		CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	if (r != CUDA_SUCCESS) return HPLAI_EINVAL;
+	std::memcpy(out, &m, sizeof(m));
+	return HPLAI_OK;
+}
+
+int num_sms()
+{
+	int dev = 0, sms = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+	if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) return 148;
+	return sms;
+}
+
+} // namespace
+
+static_assert(sizeof(CUtensorMap) <= sizeof(SchurMaps::lmap), "tensor map storage");
+
+int schur_make_maps(SchurMaps *m, const uint16_t *lh, int lrows, int64_t ldl, const uint16_t *uh, int urows,
+	int64_t ldu, int k)
+{
+	if (!m || !lh || !uh || lrows <= 0 || urows <= 0 || k <= 0 || ldl < k || ldu < k || (ldl % 8) || (ldu % 8))
+		return HPLAI_EINVAL;
+	HPLAI_TRY(make_map_f16(m->lmap, lh, static_cast<uint64_t>(k), static_cast<uint64_t>(lrows),
+		static_cast<uint64_t>(ldl), BK, BM));
+	HPLAI_TRY(make_map_f16(m->umap, uh, static_cast<uint64_t>(k), static_cast<uint64_t>(urows),
+		static_cast<uint64_t>(ldu), BK, BN));
+	m->k = k;
+	return HPLAI_OK;
+}
+
+int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, cudaStream_t st)
+{
+	if (m <= 0 || n <= 0) return HPLAI_OK;
+	Params p;
+	p.c = c;
+	p.ldc = ldc;
+	p.m = m;
+	p.n = n;
+	p.num_kc = (maps.k + BK - 1) / BK;
+	p.lrow0 = lrow0;
+	p.urow0 = urow0;
+	p.tiles_m = (m + BM - 1) / BM;
+	p.tiles_n = (n + BN - 1) / BN;
+	const int total = p.tiles_m * p.tiles_n;
+	const int grid = total < num_sms() ? total : num_sms();
+	static bool attr_set = false;
+	if (!attr_set) {
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(SMEM_BYTES)));
+		attr_set = true;
+	}
+	CUtensorMap lm, um;
+	std::memcpy(&lm, maps.lmap, sizeof(lm));
+	std::memcpy(&um, maps.umap, sizeof(um));
+	schur_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(lm, um, p);
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+int schur_status()
+{
+	unsigned int v = 0;
+	if (cudaMemcpyFromSymbol(&v, g_status, sizeof(v)) != cudaSuccess) return HPLAI_ECUDA;
+	return v ? HPLAI_ETIMEOUT : HPLAI_OK;
+}
+
+void schur_status_reset()
+{
+	unsigned int z = 0;
+	(void)cudaMemcpyToSymbol(g_status, &z, sizeof(z));
+}
+
+} // namespace hplai
+
+extern "C" int hplai_shgemm_minus(int m, int n, int k, const uint16_t *lh, int64_t ldlh, const uint16_t *uh,
+	int64_t lduh, float *c, int64_t ldc, void *stream)
+{
+	if (m < 0 || n < 0 || k <= 0 || !lh || !uh || !c || ldc < m || ldlh < k || lduh < k) return HPLAI_EINVAL;
+	if (m == 0 || n == 0) return HPLAI_OK;
+	hplai::SchurMaps maps;
+	HPLAI_TRY(hplai::schur_make_maps(&maps, lh, m, ldlh, uh, n, lduh, k));
+	return hplai::launch_schur(maps, 0, 0, m, n, c, ldc, static_cast<cudaStream_t>(stream));
+}

@@ -1,0 +1,221 @@
+"""ctypes binding of libhplai (include/hplai.h) for tests and benchmarks.
+
+The product is the C ABI in libhplai.so plus the C++ driver (driver.out);
+this module only marshals arguments.  It loads the in-tree shared library
+and raises ImportError when it is missing: there is no fallback path.
+
+Names follow the reference (RIKEN-RCCS/hpl-ai): `iterative_refinement`
+returns IRErrors {residual, hpl_harness} = {-1, -1} on failure
+(iterative_refinement.hpp:13-57) instead of raising.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhplai.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"libhplai.so not built at {LIB_PATH}; run `make -C {_HERE}`")
+
+_lib = ctypes.CDLL(LIB_PATH)
+
+HPLAI_OK, HPLAI_EINVAL, HPLAI_ENOMEM, HPLAI_ECUDA, HPLAI_ENOTCONV, HPLAI_ETIMEOUT, HPLAI_ESTATE, \
+    HPLAI_EUNSUPPORTED = range(8)
+F32_F16, F32_F8 = 0, 1
+IR, GMRES = 0, 1
+PHASES = ("DIAG_LU", "TRSM_L", "TRSM_R", "GEMM_UPDATE", "IR_GEMV", "IR_TRSV", "TOTAL")
+
+_c_int, _c_i64, _c_u64, _c_dbl, _c_flt, _c_sz, _vp = (
+    ctypes.c_int, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double, ctypes.c_float, ctypes.c_size_t,
+    ctypes.c_void_p)
+
+
+class IRErrors(ctypes.Structure):
+    _fields_ = [("residual", ctypes.c_double), ("hpl_harness", ctypes.c_double)]
+
+
+def _proto(name, restype, *argtypes):
+    f = getattr(_lib, name)
+    f.restype = restype
+    f.argtypes = list(argtypes)
+    return f
+
+
+_status_string = _proto("hplai_status_string", ctypes.c_char_p, _c_int)
+_last_error = _proto("hplai_last_error", _c_int, ctypes.c_char_p, _c_sz)
+version = _proto("hplai_version", _c_int)
+_create = _proto("hplai_create", _c_int, ctypes.POINTER(_vp), _c_int, _c_int, _c_int, ctypes.c_uint)
+_destroy = _proto("hplai_destroy", _c_int, _vp)
+_generate = _proto("hplai_generate", _c_int, _vp, _c_u64)
+_upload = _proto("hplai_upload", _c_int, _vp, _vp, _c_i64, _vp, _vp, _c_u64)
+_factor = _proto("hplai_factor", _c_int, _vp)
+_refine = _proto("hplai_refine", _c_int, _vp, _c_int, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
+_get_x = _proto("hplai_get_x", _c_int, _vp, _vp)
+_get_lu = _proto("hplai_get_lu", _c_int, _vp, _vp, _c_i64)
+_get_rhs = _proto("hplai_get_rhs", _c_int, _vp, _vp)
+_get_diag = _proto("hplai_get_diag", _c_int, _vp, _vp)
+_get_ir_log = _proto("hplai_get_ir_log", _c_int, _vp, _vp, _vp, _c_int, ctypes.POINTER(_c_int))
+_get_phase_ms = _proto("hplai_get_phase_ms", _c_int, _vp, _vp, _c_int)
+_get_norms = _proto("hplai_get_norms", _c_int, _vp, ctypes.POINTER(_c_dbl), ctypes.POINTER(_c_dbl))
+_solve_host = _proto("hplai_solve_host", _c_int, _vp, _vp, _c_i64, _vp, _vp, _c_u64, _c_int, _vp,
+                     ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
+_format_report = _proto("hplai_format_report", _c_int, _c_int, _c_dbl, IRErrors, ctypes.c_char_p, _c_sz)
+
+fill_panel = _proto("hplai_fill_panel", _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _c_i64, _c_u64,
+                    _c_int, _vp)
+gen_rhs = _proto("hplai_gen_rhs", _c_int, _c_int, _c_u64, _vp, _vp)
+gen_diag = _proto("hplai_gen_diag", _c_int, _c_int, _c_u64, _c_int, _c_int, _vp, _vp)
+getrf_nopiv = _proto("hplai_getrf_nopiv", _c_int, _c_int, _vp, _c_i64, _vp)
+trsm_right_upper = _proto("hplai_trsm_right_upper", _c_int, _c_int, _c_int, _vp, _c_i64, _vp, _c_i64, _vp, _c_i64,
+                          _c_flt, _vp)
+trsm_left_lower = _proto("hplai_trsm_left_lower", _c_int, _c_int, _c_int, _vp, _c_i64, _vp, _c_i64, _vp, _c_i64,
+                         _c_flt, _vp)
+shgemm_minus = _proto("hplai_shgemm_minus", _c_int, _c_int, _c_int, _c_int, _vp, _c_i64, _vp, _c_i64, _vp, _c_i64,
+                      _vp)
+otf_gemv_workspace = _proto("hplai_otf_gemv_workspace", _c_sz, _c_int)
+otf_gemv = _proto("hplai_otf_gemv", _c_int, _c_int, _c_dbl, _vp, _c_dbl, _vp, _c_u64, _vp, _vp, _c_sz, _vp)
+otf_gemv_block = _proto("hplai_otf_gemv_block", _c_int, _c_i64, _c_int, _c_int, _c_dbl, _vp, _vp, _c_u64, _vp,
+                        _c_sz, _vp)
+trsv_workspace = _proto("hplai_trsv_workspace", _c_sz, _c_int)
+trsv_lower = _proto("hplai_trsv_lower", _c_int, _c_int, _vp, _c_i64, _vp, _vp, _c_sz, _vp)
+trsv_upper = _proto("hplai_trsv_upper", _c_int, _c_int, _vp, _c_i64, _vp, _vp, _c_sz, _vp)
+infnorm = _proto("hplai_infnorm", _c_int, _c_int, _vp, _vp, _vp)
+
+
+class HplaiError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        buf = ctypes.create_string_buffer(512)
+        _last_error(buf, 512)
+        detail = buf.value.decode(errors="replace")
+        super().__init__(f"{what}: {status_string(status)}" + (f" [{detail}]" if detail else ""))
+        self.status = status
+
+
+def status_string(status: int) -> str:
+    return _status_string(status).decode()
+
+
+def check(status: int, what: str = "hplai") -> int:
+    if status != HPLAI_OK:
+        raise HplaiError(status, what)
+    return status
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def format_report(n: int, seconds: float, residual: float, harness: float) -> str:
+    buf = ctypes.create_string_buffer(256)
+    check(_format_report(n, seconds, IRErrors(residual, harness), buf, 256), "hplai_format_report")
+    return buf.value.decode()
+
+
+@dataclass
+class RefineResult:
+    residual: float
+    hpl_harness: float
+    iters: int
+    status: int
+
+
+class Solver:
+    """One solve context: the single-GPU collapse of the reference driver."""
+
+    def __init__(self, n: int, b: int, precision: int = F32_F16, flags: int = 0):
+        h = _vp()
+        check(_create(ctypes.byref(h), n, b, precision, flags), f"hplai_create(n={n}, b={b})")
+        self._h = h
+        self.n, self.b = n, b
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def generate(self, seed: int = 42):
+        check(_generate(self._h, seed), "hplai_generate")
+
+    def upload(self, a: np.ndarray, rhs: np.ndarray, diag: np.ndarray, seed: int = 42):
+        a = np.asfortranarray(a, dtype=np.float32)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        diag = np.ascontiguousarray(diag, dtype=np.float64)
+        check(_upload(self._h, _ptr(a), a.shape[0], _ptr(rhs), _ptr(diag), seed), "hplai_upload")
+
+    def factor(self):
+        check(_factor(self._h), "hplai_factor")
+
+    def iterative_refinement(self, maxit: int = 50, mode: int = IR) -> RefineResult:
+        e = IRErrors()
+        it = _c_int()
+        s = _refine(self._h, mode, maxit, ctypes.byref(e), ctypes.byref(it))
+        if s not in (HPLAI_OK, HPLAI_ENOTCONV):
+            check(s, "hplai_refine")
+        return RefineResult(e.residual, e.hpl_harness, it.value, s)
+
+    def solve_host(self, a, rhs, diag, seed=42, maxit=50):
+        a = np.asfortranarray(a, dtype=np.float32)
+        x = np.empty(self.n, dtype=np.float64)
+        e = IRErrors()
+        it = _c_int()
+        s = _solve_host(self._h, _ptr(a), a.shape[0], _ptr(rhs), _ptr(diag), seed, maxit, _ptr(x), ctypes.byref(e),
+                        ctypes.byref(it))
+        if s not in (HPLAI_OK, HPLAI_ENOTCONV):
+            check(s, "hplai_solve_host")
+        return x, RefineResult(e.residual, e.hpl_harness, it.value, s)
+
+    def x(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.float64)
+        check(_get_x(self._h, _ptr(out)), "hplai_get_x")
+        return out
+
+    def lu(self) -> np.ndarray:
+        out = np.empty((self.n, self.n), dtype=np.float32, order="F")
+        check(_get_lu(self._h, _ptr(out), self.n), "hplai_get_lu")
+        return out
+
+    def rhs(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.float64)
+        check(_get_rhs(self._h, _ptr(out)), "hplai_get_rhs")
+        return out
+
+    def diag(self) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.float64)
+        check(_get_diag(self._h, _ptr(out)), "hplai_get_diag")
+        return out
+
+    def ir_log(self):
+        cap = 64
+        r = np.zeros(cap)
+        h = np.zeros(cap)
+        cnt = _c_int()
+        check(_get_ir_log(self._h, _ptr(r), _ptr(h), cap, ctypes.byref(cnt)), "hplai_get_ir_log")
+        m = min(cnt.value, cap)
+        return list(zip(r[:m].tolist(), h[:m].tolist()))
+
+    def phase_ms(self) -> dict:
+        out = np.zeros(len(PHASES))
+        check(_get_phase_ms(self._h, _ptr(out), len(PHASES)), "hplai_get_phase_ms")
+        return dict(zip(PHASES, out.tolist()))
+
+    def norms(self):
+        a, b = _c_dbl(), _c_dbl()
+        check(_get_norms(self._h, ctypes.byref(a), ctypes.byref(b)), "hplai_get_norms")
+        return a.value, b.value

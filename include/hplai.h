@@ -1,0 +1,225 @@
+/*
+ * hplai.h -- C ABI of libhplai, a single-GPU B200 (sm_100a) HPL-AI solver.
+ *
+ * The library solves A x = b for the HPL-AI matrix (the 64-bit LCG matrix of
+ * RIKEN-RCCS/hpl-ai with a row-sum diagonal) by a no-pivot blocked LU with
+ * FP32 panels and an FP16-input / FP32-accumulate Schur update on tcgen05
+ * tensor cores, followed by FP64 iterative refinement that regenerates A on
+ * the fly.  Every entry point is extern "C" with plain pointers and sizes.
+ *
+ * Conventions (the reference's, panel.hpp:20-35 and otf_gemv.cpp:5-7):
+ *   - matrices are column-major with an explicit leading dimension;
+ *   - caller-owned buffers: the leaf kernels below never allocate device
+ *     memory, they take a caller-provided workspace where they need one;
+ *   - every function returns an hplai_status (0 = success), never aborts;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy stream);
+ *     leaf kernels are asynchronous on that stream;
+ *   - a context is not thread-safe; distinct contexts are independent.
+ */
+#ifndef HPLAI_H
+#define HPLAI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The library is built with hidden visibility; everything declared here is
+ * exported. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define HPLAI_VERSION 100
+
+typedef enum hplai_status {
+	HPLAI_OK = 0,
+	HPLAI_EINVAL = 1,        /* bad argument (e.g. n % b != 0, main.cpp:181 / panel.hpp:142) */
+	HPLAI_ENOMEM = 2,        /* device or pinned-host allocation failed */
+	HPLAI_ECUDA = 3,         /* a CUDA runtime call failed */
+	HPLAI_ENOTCONV = 4,      /* refinement did not reach hpl-harness < 16 (IRErrors {-1,-1}) */
+	HPLAI_ETIMEOUT = 5,      /* a device-side bounded wait ran out; the context stays usable */
+	HPLAI_ESTATE = 6,        /* call out of order (e.g. refine before factor) */
+	HPLAI_EUNSUPPORTED = 7   /* configuration outside what this build implements */
+} hplai_status;
+
+/* FHIGH / FLOW precision pair (main.cpp:27-31): the panel precision is FP32,
+ * the Schur-update input precision is FP16 (the reference default) or FP8. */
+typedef enum hplai_precision {
+	HPLAI_F32_F16 = 0,
+	HPLAI_F32_F8 = 1
+} hplai_precision;
+
+/* Refinement flavour. */
+typedef enum hplai_refine_mode {
+	HPLAI_IR = 0,            /* classical refinement, iterative_refinement.hpp:18-57 */
+	HPLAI_GMRES = 1          /* FP64 GMRES-IR preconditioned by the LU (no reference counterpart) */
+} hplai_refine_mode;
+
+/* IRErrors (iterative_refinement.hpp:13-16): {residual, hpl_harness}, or
+ * {-1, -1} when refinement fails to converge. */
+typedef struct hplai_ir_errors {
+	double residual;
+	double hpl_harness;
+} hplai_ir_errors;
+
+/* Phase timers, named after the reference's Timer items (timer.hpp:58-84). */
+typedef enum hplai_phase {
+	HPLAI_PH_DIAG_LU = 0,
+	HPLAI_PH_TRSM_L = 1,
+	HPLAI_PH_TRSM_R = 2,
+	HPLAI_PH_GEMM_UPDATE = 3,
+	HPLAI_PH_IR_GEMV = 4,
+	HPLAI_PH_IR_TRSV = 5,
+	HPLAI_PH_TOTAL = 6,
+	HPLAI_PH_COUNT = 7
+} hplai_phase;
+
+typedef struct hplai_ctx hplai_ctx;
+
+/* ---------------------------------------------------------------------- */
+/* Whole-solve context: the single-GPU collapse of main.cpp:185-488.       */
+/* ---------------------------------------------------------------------- */
+
+const char *hplai_status_string(int status);
+/* Text of the last CUDA error the library saw (thread-shared). */
+int hplai_last_error(char *buf, size_t len);
+int hplai_version(void);
+
+/* build_panels (panel.hpp:135-268) + the driver's vector allocations
+ * (main.cpp:196-213).  Requires n % b == 0 and 16 <= b <= 1024.  Allocates
+ * every device buffer of the solve on the current CUDA device.  `flags` is
+ * reserved (pass 0). */
+int hplai_create(hplai_ctx **ctx, int n, int b, int precision, unsigned flags);
+int hplai_destroy(hplai_ctx *ctx);
+
+/* Matrix, right-hand side and diagonal from the LCG seed on the device:
+ * pmatgen + pcolvgen + pdiaggen (matgen.hpp:7-22,193-225, main.cpp:255-270)
+ * and the norms (main.cpp:273-276).  Bit-exact with the reference.  The
+ * reference driver uses seed 42 (main.cpp:174). */
+int hplai_generate(hplai_ctx *ctx, uint64_t seed);
+
+/* Host-supplied inputs: FP32 matrix (lda >= n), FP64 right-hand side and
+ * FP64 diagonal, plus the LCG seed they came from (refinement regenerates
+ * A in FP64 from it, as Matgen<double> does, main.cpp:257).  Copies
+ * host -> device on the context stream and waits. */
+int hplai_upload(hplai_ctx *ctx, const float *a, int64_t lda, const double *rhs,
+	const double *diag, uint64_t seed);
+
+/* The LU in place: RDMAPanelLU::run / panel_lu_async (panel_trf.hpp:434-858)
+ * collapsed to one GPU.  Unit-L below and U on/above the diagonal, FP32. */
+int hplai_factor(hplai_ctx *ctx);
+
+/* iterative_refinement (iterative_refinement.hpp:18-57) with maxit steps
+ * (the driver uses 50).  Fills *err ({-1,-1} on failure) and *iters (the
+ * number of residual evaluations).  Returns HPLAI_ENOTCONV on failure. */
+int hplai_refine(hplai_ctx *ctx, int mode, int maxit, hplai_ir_errors *err, int *iters);
+
+/* Copies of the results. */
+int hplai_get_x(hplai_ctx *ctx, double *x);                      /* n doubles */
+int hplai_get_lu(hplai_ctx *ctx, float *a, int64_t lda);           /* n x n FP32 */
+int hplai_get_rhs(hplai_ctx *ctx, double *rhs);
+int hplai_get_diag(hplai_ctx *ctx, double *diag);
+/* The per-step refinement log the reference prints (iterative_refinement.hpp:45):
+ * up to `cap` entries; returns the number of steps through *count. */
+int hplai_get_ir_log(hplai_ctx *ctx, double *residual, double *harness, int cap, int *count);
+/* Accumulated milliseconds per hplai_phase since the last hplai_factor. */
+int hplai_get_phase_ms(hplai_ctx *ctx, double *ms, int count);
+/* ||A||_inf (= 2 max diag, panel_norm.hpp:78-84) and ||b||_inf. */
+int hplai_get_norms(hplai_ctx *ctx, double *norma, double *normb);
+
+/* One end-to-end solve through host buffers: upload, factor, refine and
+ * copy x back (the whole of main.cpp's timed region plus the transfers). */
+int hplai_solve_host(hplai_ctx *ctx, const float *a, int64_t lda, const double *rhs,
+	const double *diag, uint64_t seed, int maxit, double *x, hplai_ir_errors *err, int *iters);
+
+/* The reference's report line (main.cpp:451-452) into buf:
+ * "%.9f sec. %.9f GFlop/s resid = %20.15e hpl-harness = %.9f". */
+int hplai_format_report(int n, double seconds, hplai_ir_errors err, char *buf, size_t len);
+
+/* ---------------------------------------------------------------------- */
+/* Leaf kernels on caller-owned device buffers.                            */
+/* ---------------------------------------------------------------------- */
+
+/* fill_one_panel_with_rand<float> (hpl_rand.hpp:59-106): the sub-matrix
+ * (i0:i0+nrow, j0:j0+ncol) of the n x n HPL-AI matrix into `a` (FP32,
+ * column-major, lda).  With calc_diag on a square diagonal block the
+ * diagonal is float(sum_{j != i} |a_ij|) summed sequentially in FP64. */
+int hplai_fill_panel(int n, int i0, int j0, int nrow, int ncol, float *a, int64_t lda,
+	uint64_t seed, int calc_diag, void *stream);
+
+/* pcolvgen (matgen.hpp:193-207): rhs_i = element (i, n) in FP64, i < n. */
+int hplai_gen_rhs(int n, uint64_t seed, double *rhs, void *stream);
+
+/* pdiaggen / calc_diag (matgen.hpp:209-225, hpl_rand.hpp:108-123):
+ * d_i for i in [i0, i0+count). */
+int hplai_gen_diag(int n, uint64_t seed, int i0, int count, double *d, void *stream);
+
+/* getrf_nopiv<float> (getrf_nopiv.hpp:124-141): b x b no-pivot LU in place,
+ * b <= 1024. */
+int hplai_getrf_nopiv(int b, float *a, int64_t lda, void *stream);
+
+/* update_left_panels + convert_left_panels (panel_trf.hpp:143-157,182-207):
+ * a (m x b, lda) <- a * U^{-1} with U the upper triangle of u (b x b, ldu,
+ * non-unit), then lh[i*ldh + k] = half(scale * a[i, k]) (row-major FP16
+ * copy, the layout the Schur GEMM reads).  lh may be NULL. */
+int hplai_trsm_right_upper(int m, int b, const float *u, int64_t ldu, float *a, int64_t lda,
+	uint16_t *lh, int64_t ldh, float scale, void *stream);
+
+/* update_right_panels + convert_right_panels (panel_trf.hpp:158-171,208-233):
+ * a (b x ncols, lda) <- L^{-1} a with L the unit lower triangle of l
+ * (b x b, ldl), then uh[j*ldh + k] = half(scale * a[k, j]).  uh may be NULL. */
+int hplai_trsm_left_lower(int b, int ncols, const float *l, int64_t ldl, float *a, int64_t lda,
+	uint16_t *uh, int64_t ldh, float scale, void *stream);
+
+/* gemmschur -> shgemm with alpha = -1, beta = 1 (schur_updator.hpp:24-31,
+ * fp16sim.hpp:216-233):  C (m x n FP32, ldc) -= L * U, FP32 accumulation,
+ * on tcgen05 tensor cores.  L is m x k FP16 stored row-major
+ * (lh[i*ldlh + p]), U is k x n FP16 stored column-major (uh[j*lduh + p]);
+ * ldlh and lduh are multiples of 8 and the buffers 16-byte aligned. */
+int hplai_shgemm_minus(int m, int n, int k, const uint16_t *lh, int64_t ldlh,
+	const uint16_t *uh, int64_t lduh, float *c, int64_t ldc, void *stream);
+
+/* Workspace bytes for hplai_otf_gemv at order n. */
+size_t hplai_otf_gemv_workspace(int n);
+
+/* panel_gemv / otf_gemv (panel_gemv.hpp:57-180, otf_gemv.cpp:5-131) over the
+ * whole matrix:  y <- beta*y + alpha * A x, A(i,j) regenerated in FP64 from
+ * the LCG (seed) for i != j and A(i,i) = diag[i].  `work` holds at least
+ * hplai_otf_gemv_workspace(n) bytes. */
+int hplai_otf_gemv(int n, double alpha, const double *x, double beta, double *y,
+	uint64_t seed, const double *diag, void *work, size_t work_bytes, void *stream);
+
+/* otf_gemv_kernel (otf_gemv.cpp:5-7) on one off-diagonal sub-block:
+ * y(0:mb) += alpha * A_sub x(0:nb) where `state00` is the LCG state of the
+ * sub-block's (0,0) element and n the order of the whole matrix.  The
+ * sub-block must not contain diagonal elements (otf_gemv.cpp:12-13).
+ * `work` holds at least hplai_otf_gemv_workspace(max(mb,nb)) bytes. */
+int hplai_otf_gemv_block(int64_t n, int mb, int nb, double alpha, const double *x, double *y,
+	uint64_t state00, void *work, size_t work_bytes, void *stream);
+
+/* Workspace bytes for the triangular solves at order n. */
+size_t hplai_trsv_workspace(int n);
+
+/* panel_trsvL / panel_trsvU (panel_trsv.hpp:310-758): x <- L^{-1} x with L
+ * the unit lower triangle of a, or x <- U^{-1} x with U the upper triangle
+ * of a (FP32 factors, FP64 vector).  `work` holds at least
+ * hplai_trsv_workspace(n) bytes and must be zeroed before its first use. */
+int hplai_trsv_lower(int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes, void *stream);
+int hplai_trsv_upper(int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes, void *stream);
+
+/* colv_infnorm / calc_infnorm (panel_norm.hpp:8-41): *out = max_i |x_i|
+ * written to device memory. */
+int hplai_infnorm(int n, const double *x, double *out, void *stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPLAI_H */

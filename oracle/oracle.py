@@ -1,0 +1,198 @@
+"""ctypes binding of the CPU oracle (liboracle.so, built from hplai_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py (cpu_baseline and the reference arm).  The product never imports
+this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+
+def build() -> str:
+    """Compile liboracle.so with the Makefile next to this file (gcc, seconds)."""
+    src = os.path.join(HERE, "hplai_oracle.c")
+    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+build()
+_lib = ctypes.CDLL(LIB_PATH)
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_i64, _u64, _int, _dbl, _vp = ctypes.c_int64, ctypes.c_uint64, ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+
+
+def _proto(name, restype, *argtypes):
+    f = getattr(_lib, name)
+    f.restype = restype
+    f.argtypes = list(argtypes)
+    return f
+
+
+state_at = _proto("orc_state_at", _u64, _int, _i64, _i64, _u64)
+elem = _proto("orc_elem", _dbl, _int, _i64, _i64, _u64)
+_coeff_pow = _proto("orc_coeff_pow", None, _u64, ctypes.POINTER(_u64), ctypes.POINTER(_u64))
+calc_diag = _proto("orc_calc_diag", _dbl, _int, _int, _u64)
+_fill_panel = _proto("orc_fill_panel", None, _int, _int, _int, _int, _int, _vp, _i64, _u64, _int)
+_gen_rhs = _proto("orc_gen_rhs", None, _int, _u64, _vp)
+_gen_diag = _proto("orc_gen_diag", None, _int, _u64, _vp)
+_getrf = _proto("orc_getrf_nopiv", None, _int, _vp, _i64)
+_trsm_ru = _proto("orc_trsm_right_upper", None, _int, _int, _vp, _i64, _vp, _i64)
+_trsm_ll = _proto("orc_trsm_left_lower_unit", None, _int, _int, _vp, _i64, _vp, _i64)
+_shgemm = _proto("orc_shgemm_minus", None, _int, _int, _int, _vp, _i64, _vp, _i64, _vp, _i64)
+_lu = _proto("orc_lu", _int, _int, _int, _vp, _i64)
+_otf_gemv = _proto("orc_otf_gemv", None, _int, _int, _int, _dbl, _vp, _vp, _u64, _vp)
+_trsv_l = _proto("orc_trsv_lower", None, _int, _int, _vp, _i64, _vp)
+_trsv_u = _proto("orc_trsv_upper", None, _int, _int, _vp, _i64, _vp)
+_refine = _proto("orc_refine", _int, _int, _int, _int, _vp, _i64, _u64, _vp, _vp, _int, _vp, _vp, _vp,
+                 ctypes.POINTER(_int), _dp, _dp)
+_solve = _proto("orc_solve", _int, _int, _int, _int, _u64, _int, _vp, _vp, _vp, ctypes.POINTER(_int), _dp, _dp)
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def coeff_pow(m: int):
+    a, c = _u64(), _u64()
+    _coeff_pow(m, ctypes.byref(a), ctypes.byref(c))
+    return a.value, c.value
+
+
+def fill_panel(n, i0, j0, nrow, ncol, seed=42, calc_diag=True) -> np.ndarray:
+    a = np.zeros((nrow, ncol), dtype=np.float32, order="F")
+    _fill_panel(n, i0, j0, nrow, ncol, _p(a), max(nrow, 1), seed, 1 if calc_diag else 0)
+    return a
+
+
+def matrix(n, seed=42) -> np.ndarray:
+    return fill_panel(n, 0, 0, n, n, seed, True)
+
+
+def rhs(n, seed=42) -> np.ndarray:
+    out = np.zeros(n)
+    _gen_rhs(n, seed, _p(out))
+    return out
+
+
+def diag(n, seed=42) -> np.ndarray:
+    out = np.zeros(n)
+    _gen_diag(n, seed, _p(out))
+    return out
+
+
+def getrf_nopiv(a: np.ndarray) -> np.ndarray:
+    a = np.array(a, dtype=np.float32, order="F", copy=True)
+    _getrf(a.shape[0], _p(a), a.shape[0])
+    return a
+
+
+def trsm_right_upper(u: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """B <- B * U^{-1}, U upper non-unit (netlib strsm R,U,N,N order)."""
+    u = np.asfortranarray(u, dtype=np.float32)
+    b = np.array(b, dtype=np.float32, order="F", copy=True)
+    _trsm_ru(b.shape[0], b.shape[1], _p(u), u.shape[0], _p(b), b.shape[0])
+    return b
+
+
+def trsm_left_lower_unit(l: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """B <- L^{-1} B, L unit lower (netlib strsm L,L,N,U order)."""
+    l = np.asfortranarray(l, dtype=np.float32)
+    b = np.array(b, dtype=np.float32, order="F", copy=True)
+    _trsm_ll(b.shape[0], b.shape[1], _p(l), l.shape[0], _p(b), b.shape[0])
+    return b
+
+
+def shgemm_minus(c: np.ndarray, l16: np.ndarray, u16: np.ndarray) -> np.ndarray:
+    """C - L*U with FP16 inputs, FP32 accumulation in k-blocks of 100."""
+    c = np.array(c, dtype=np.float32, order="F", copy=True)
+    l16 = np.asfortranarray(l16, dtype=np.float16).view(np.uint16)
+    u16 = np.asfortranarray(u16, dtype=np.float16).view(np.uint16)
+    m, k = l16.shape
+    n = u16.shape[1]
+    _shgemm(m, n, k, _p(l16), m, _p(u16), k, _p(c), m)
+    return c
+
+
+def lu(a: np.ndarray, b: int) -> np.ndarray:
+    a = np.array(a, dtype=np.float32, order="F", copy=True)
+    rc = _lu(a.shape[0], b, _p(a), a.shape[0])
+    if rc:
+        raise ValueError(f"orc_lu: {rc}")
+    return a
+
+
+def otf_gemv(n, b, alpha, x, y, seed, d, q=1) -> np.ndarray:
+    y = np.array(y, dtype=np.float64, copy=True)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    d = np.ascontiguousarray(d, dtype=np.float64)
+    _otf_gemv(n, b, q, alpha, _p(x), _p(y), seed, _p(d))
+    return y
+
+
+def trsv_lower(lu_f32: np.ndarray, x: np.ndarray, b: int) -> np.ndarray:
+    x = np.array(x, dtype=np.float64, copy=True)
+    a = np.asfortranarray(lu_f32, dtype=np.float32)
+    _trsv_l(a.shape[0], b, _p(a), a.shape[0], _p(x))
+    return x
+
+
+def trsv_upper(lu_f32: np.ndarray, x: np.ndarray, b: int) -> np.ndarray:
+    x = np.array(x, dtype=np.float64, copy=True)
+    a = np.asfortranarray(lu_f32, dtype=np.float32)
+    _trsv_u(a.shape[0], b, _p(a), a.shape[0], _p(x))
+    return x
+
+
+def refine(lu_f32, b, seed, rhs_v, d, maxit=50, q=1):
+    n = lu_f32.shape[0]
+    a = np.asfortranarray(lu_f32, dtype=np.float32)
+    x = np.zeros(n)
+    sr, sh = np.zeros(max(maxit, 1)), np.zeros(max(maxit, 1))
+    ns = _int()
+    res, har = _dbl(), _dbl()
+    rc = _refine(n, b, q, _p(a), n, seed, _p(np.ascontiguousarray(rhs_v)), _p(np.ascontiguousarray(d)), maxit, _p(x),
+                 _p(sr), _p(sh), ctypes.byref(ns), ctypes.byref(res), ctypes.byref(har))
+    steps = list(zip(sr[:ns.value].tolist(), sh[:ns.value].tolist()))
+    return rc, x, res.value, har.value, steps
+
+
+def solve(n, b, seed=42, maxit=50, q=1):
+    """Generate, factor and refine on the CPU; returns (rc, x, resid, harness, steps)."""
+    x = np.zeros(n)
+    sr, sh = np.zeros(max(maxit, 1)), np.zeros(max(maxit, 1))
+    ns = _int()
+    res, har = _dbl(), _dbl()
+    rc = _solve(n, b, q, seed, maxit, _p(x), _p(sr), _p(sh), ctypes.byref(ns), ctypes.byref(res), ctypes.byref(har))
+    steps = list(zip(sr[:ns.value].tolist(), sh[:ns.value].tolist()))
+    return rc, x, res.value, har.value, steps
+
+
+def dense_matrix_f64(n, seed=42) -> np.ndarray:
+    """The FP64 HPL-AI matrix (off-diagonal generator values, FP64 row-sum
+    diagonal), as Matgen<double> defines it for the residual.  Vectorised
+    over rows: column j+1's states are column j's advanced by inc1^n."""
+    scale = float.fromhex("0x1.fffffffffffffp-65")
+    col = np.empty(n, dtype=np.uint64)
+    s = state_at(n, 0, 0, seed)
+    for i in range(n):
+        col[i] = s
+        s = (s * 6364136223846793005 + 1) & ((1 << 64) - 1)
+    an, cn = coeff_pow(n)
+    an, cn = np.uint64(an), np.uint64(cn)
+    a = np.empty((n, n), order="F")
+    with np.errstate(over="ignore"):
+        for j in range(n):
+            a[:, j] = col.view(np.int64).astype(np.float64) * scale
+            col = col * an + cn
+    a[np.arange(n), np.arange(n)] = diag(n, seed)
+    return a
