@@ -1,0 +1,370 @@
+#!/usr/bin/env python3
+"""HPL-AI GFLOP/s of the single-GPU B200 solver (one JSON line on rank 0).
+
+One step = one solve of the HPL-AI system on the GPU: the blocked no-pivot
+LU (FP32 panels, FP16 tcgen05 Schur update) followed by FP64 iterative
+refinement to hpl-harness < 16 -- the reference's timed region
+(main.cpp:283-441).  The matrix is regenerated on the device before every
+step, outside the timed window, as the reference generates it before its
+timer starts (the LU overwrites A).  Work per step: 2/3 n^3 + 3/2 n^2 flops
+(main.cpp:441).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (under torchrun, one rank per GPU) runs N independent replicas: a
+single solve does not shard on this build ("replicas only").  `value` is
+the flops of all ranks over the slowest rank's time.
+
+--impl reference times the reference algorithm on the host cores: the
+reference's own code built from its sources (oracle/_ref) when present,
+else the CPU restatement in oracle/ -- on a bounded sample of the workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hpl-ai_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "HPL-AI GFLOP/s to hpl-harness<16: FP8-Schur+GMRES-IR vs plain; % tensor peak"
+UNIT = "GFLOP/s"
+DEFAULT_N, DEFAULT_B = 65536, 512
+CPU_SAMPLE = (2400, 120)           # bounded CPU sample of the same workload
+
+
+def hpl_flops(n):
+    return 2.0 / 3.0 * n * n * n + 3.0 / 2.0 * n * n
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained", 1400.0), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_solve_gflops(n, b, threads):
+    """One CPU solve of the sample: the reference build if present, else the oracle."""
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "ref_driver.out")
+    if os.path.exists(ref_bin):
+        env = dict(os.environ, OMP_NUM_THREADS=str(max(1, threads // 4)), TMPI_NP="4")
+        t0 = time.perf_counter()
+        out = subprocess.run([ref_bin, str(n), str(b), "2", "-not", "-r"], capture_output=True, text=True, env=env,
+                             timeout=600)
+        wall = time.perf_counter() - t0
+        for ln in out.stdout.splitlines():
+            if "GFlop/s" in ln and "sec." in ln:
+                f = ln.split()
+                secs, harness = float(f[0]), float(f[-1])
+                return hpl_flops(n) / secs / 1e9, secs, harness, "reference", threads
+        raise RuntimeError(f"reference build printed no report line ({wall:.1f}s): {out.stdout[-400:]}")
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    import oracle
+    t0 = time.perf_counter()
+    rc, x, res, har, steps = oracle.solve(n, b, q=1)
+    secs = time.perf_counter() - t0
+    if rc != 0:
+        raise RuntimeError("oracle solve did not converge")
+    return hpl_flops(n) / secs / 1e9, secs, har, "port", threads
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    n, b = CPU_SAMPLE
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_solve_gflops(n, b, threads)
+    vals, secs = [], []
+    for _ in range(args.steps):
+        g, s, har, kind, cores = cpu_solve_gflops(n, b, threads)
+        vals.append(g)
+        secs.append(s)
+    value = len(vals) * hpl_flops(n) / sum(secs) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp16/fp32/fp64",
+        "data": "synthetic (the reference's own LCG matrix, seed 42)",
+        "config": {"workload": f"HPL-AI plain solve, bounded CPU sample n={n} b={b} of the n={args.n} b={args.b} "
+                               f"workload", "n": n, "b": b},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"full solve (LU + IR) at n={n} b={b}, {args.steps} steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def schur_algorithmic(n, b):
+    """Flops and bytes of all Schur launches of one factorisation.
+    Per launch k: C is (n-(k+1)b)^2 FP32 read and written (8 B/elem), the
+    FP16 L and U panels are read once (2*rem*b*2 B), flops 2*rem^2*b."""
+    flops = byts = 0.0
+    launches = 0
+    for k in range(n // b - 1):
+        rem = n - (k + 1) * b
+        flops += 2.0 * rem * rem * b
+        byts += 8.0 * rem * rem + 4.0 * rem * b
+        launches += 1
+    return flops, byts, launches
+
+
+def schur_traffic_per_launch(n, b):
+    """DRAM bytes per average launch from the committed ncu summary, scaled
+    by C elements (traffic grows with rem^2)."""
+    p = os.path.join(ROOT, "profiles", "schur_kernel_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    per_elem = d.get("dram_bytes_per_c_element")
+    if not per_elem:
+        return None
+    _, _, launches = schur_algorithmic(n, b)
+    elems = sum((n - (k + 1) * b) ** 2 for k in range(n // b - 1))
+    return per_elem * elems / launches
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    import hplai
+
+    n, b, seed, maxit = args.n, args.b, 42, 50
+    dev = torch.cuda.current_device()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+
+    s = hplai.Solver(n, b)
+    ext = torch.cuda.ExternalStream(s.stream())
+    results = []
+
+    def one_step(timed):
+        s.generate(seed)
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(ext)
+        s.factor()
+        r = s.iterative_refinement(maxit)
+        ev1.record(ext)
+        ev1.synchronize()
+        barrier()
+        if r.status != hplai.HPLAI_OK:
+            raise RuntimeError(f"solve did not converge: {r}")
+        if timed:
+            results.append((ev0.elapsed_time(ev1), r, s.phase_ms()))
+
+    for _ in range(args.warmup):
+        one_step(False)
+    sampler = ClockSampler(dev)
+    sampler.start()
+    l0 = hplai.launch_count()
+    for _ in range(args.steps):
+        one_step(True)
+    launches = hplai.launch_count() - l0
+    clocks = sampler.stop()
+
+    total_ms = sum(r[0] for r in results)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * args.steps * hpl_flops(n) / (max_ms * 1e-3) / 1e9
+
+    # Roofline of the dominant kernel (the Schur GEMM), timed inside the
+    # library with CUDA events around each launch on its stream.
+    hbm, tc_burst, tc_sus, peak_kind = load_peaks()
+    sflops, sbytes, slaunch = schur_algorithmic(n, b)
+    gemm_ms = statistics.mean(r[2]["GEMM_UPDATE"] for r in results)
+    avg_launch_s = gemm_ms * 1e-3 / slaunch
+    ach_gbs = sbytes / slaunch / avg_launch_s / 1e9
+    ach_tf = sflops / slaunch / avg_launch_s / 1e12
+    ridge = tc_sus * 1e12 / (hbm * 1e9)
+    intensity = sflops / sbytes
+    bound = "tensor" if intensity >= ridge else "hbm"
+    traffic = schur_traffic_per_launch(n, b)
+    if bound == "hbm":
+        roof = {"bound": "hbm", "achieved": ach_gbs, "peak": hbm, "unit": "GB/s", "frac": ach_gbs / hbm}
+    else:
+        roof = {"bound": "tensor", "achieved": ach_tf, "peak": tc_sus, "unit": "TFLOP/s", "frac": ach_tf / tc_sus}
+    roof.update({"traffic": traffic, "kernel": "schur_kernel (tcgen05 FP16 x FP16 -> FP32, C -= L*U)",
+                 "launches_per_step": slaunch, "avg_launch_ms": avg_launch_s * 1e3,
+                 "algorithmic_bytes_per_launch": sbytes / slaunch, "algorithmic_flops_per_launch": sflops / slaunch,
+                 "intensity_flop_per_byte": intensity, "ridge_flop_per_byte": ridge,
+                 "tensor_achieved_tflops": ach_tf, "tensor_peak_tflops": tc_sus,
+                 "tensor_frac": ach_tf / tc_sus, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json: hbm_gbs, "
+                                                               f"bf16_tflops_sustained)"})
+    phases = {k: statistics.mean(r[2][k] for r in results) for k in results[0][2]}
+
+    # End to end through the public C API with host buffers: pinned FP32 A,
+    # FP64 rhs and diagonal copied in, x copied out, every step.
+    e2e = None
+    if not args.no_e2e:
+        s.generate(seed)
+        torch.cuda.synchronize()
+        try:
+            a_h = torch.empty(n * n, dtype=torch.float32, pin_memory=True)
+            pinned = True
+        except RuntimeError:
+            a_h = torch.empty(n * n, dtype=torch.float32)
+            pinned = False
+        import numpy as np
+        hplai.check(hplai._get_lu(s._h, a_h.data_ptr(), n), "hplai_get_lu")
+        rhs_h = torch.from_numpy(s.rhs()).pin_memory() if pinned else torch.from_numpy(s.rhs())
+        d_h = torch.from_numpy(s.diag()).pin_memory() if pinned else torch.from_numpy(s.diag())
+        x_h = torch.empty(n, dtype=torch.float64, pin_memory=pinned)
+        ets = []
+        for i in range(args.e2e_warmup + args.steps):
+            barrier()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(ext)
+            r = s.solve_host_ptrs(a_h.data_ptr(), n, rhs_h.data_ptr(), d_h.data_ptr(), seed, maxit, x_h.data_ptr())
+            ev1.record(ext)
+            ev1.synchronize()
+            barrier()
+            if r.status != hplai.HPLAI_OK:
+                raise RuntimeError(f"e2e solve did not converge: {r}")
+            if i >= args.e2e_warmup:
+                ets.append(ev0.elapsed_time(ev1))
+        te = torch.tensor([sum(ets)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+        e2e = {"value": world * len(ets) * hpl_flops(n) / (float(te.item()) * 1e-3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": n * n * 4 + 2 * n * 8, "d2h_bytes_per_step": n * 8,
+               "host_memory": "pinned" if pinned else "pageable", "ms_per_step": float(te.item()) / len(ets)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        nb_, bb_ = CPU_SAMPLE
+        threads = os.cpu_count() or 1
+        reps, tot = 0, 0.0
+        kind = "port"
+        while tot < 10.0 and reps < 5:
+            g, secs, har, kind, cores = cpu_solve_gflops(nb_, bb_, threads)
+            reps += 1
+            tot += secs
+        cpu = {"value": reps * hpl_flops(nb_) / tot / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"{reps} full solve(s) (LU + IR) at n={nb_} b={bb_} on the host CPU, {tot:.1f} s"}
+
+    last = results[-1][1]
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp16/fp32/fp64",
+            "data": "synthetic (the reference's own LCG matrix, seed 42, regenerated on the device before each step)",
+            "config": {"workload": f"HPL-AI plain solve n={n} b={b}: FP32 panels, FP16 tcgen05 Schur update, "
+                                   f"FP64 iterative refinement", "n": n, "b": b, "form": "plain (F32_F16 + IR)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": f"inputs {n * n * 4 / 1e9:.1f} GB FP32 > 126 MB L2, rewritten between steps"},
+            "hpl_harness": last.hpl_harness, "resid": last.residual, "ir_steps": last.iters,
+            "phases_ms": phases, "roofline": roof, "gpu_launches": int(launches),
+            "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=DEFAULT_N)
+    ap.add_argument("--b", type=int, default=DEFAULT_B)
+    ap.add_argument("--e2e-warmup", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -21,7 +22,10 @@ namespace hplai {
 namespace {
 std::mutex g_err_mu;
 std::string g_err;
+std::atomic<unsigned long long> g_launches{0};
 } // namespace
+
+void count_launches(int k) { g_launches.fetch_add(static_cast<unsigned long long>(k), std::memory_order_relaxed); }
 
 void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int line)
 {
@@ -147,6 +151,8 @@ extern "C" const char *hplai_status_string(int status)
 }
 
 extern "C" int hplai_version(void) { return HPLAI_VERSION; }
+
+extern "C" unsigned long long hplai_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 extern "C" int hplai_last_error(char *buf, size_t len)
 {
@@ -382,6 +388,8 @@ extern "C" int hplai_get_phase_ms(hplai_ctx *c, double *ms, int count)
 	for (int i = 0; i < count && i < HPLAI_PH_COUNT; ++i) ms[i] = (i == HPLAI_PH_TOTAL) ? total : c->phase_ms[i];
 	return HPLAI_OK;
 }
+
+extern "C" void *hplai_get_stream(hplai_ctx *c) { return c ? static_cast<void *>(c->st) : nullptr; }
 
 extern "C" int hplai_get_norms(hplai_ctx *c, double *norma, double *normb)
 {

@@ -121,9 +121,11 @@ int launch_fill(int n, int i0, int j0, int nrow, int ncol, float *a, int64_t lda
 	if (nrow <= 0 || ncol <= 0) return HPLAI_OK;
 	dim3 grid((nrow + kFillRows - 1) / kFillRows, (ncol + kFillCols - 1) / kFillCols);
 	fill_kernel<<<grid, kFillRows, 0, st>>>(n, i0, j0, nrow, ncol, a, lda, seed, jump_table());
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	if (calc_diag && i0 == j0 && nrow == ncol) {
 		diag_kernel<<<(nrow + 127) / 128, 128, 0, st>>>(n, i0, nrow, nullptr, a, lda, seed, jump_table());
+		count_launches();
 		HPLAI_CUDA_TRY(cudaGetLastError());
 	}
 	return HPLAI_OK;
@@ -133,6 +135,7 @@ int launch_diag(int n, int i0, int count, double *d, float *adiag, int64_t lda, 
 {
 	if (count <= 0) return HPLAI_OK;
 	diag_kernel<<<(count + 127) / 128, 128, 0, st>>>(n, i0, count, d, adiag, lda, seed, jump_table());
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
 }
@@ -140,6 +143,7 @@ int launch_diag(int n, int i0, int count, double *d, float *adiag, int64_t lda, 
 int launch_rhs(int n, double *rhs, uint64_t seed, cudaStream_t st)
 {
 	rhs_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, n, rhs, seed, jump_table());
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
 }

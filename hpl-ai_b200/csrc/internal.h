@@ -9,6 +9,10 @@
 
 namespace hplai {
 
+// Number of kernel launches the library has enqueued (all launch paths
+// below add to it); read through hplai_launch_count().
+void count_launches(int k = 1);
+
 // gen.cu
 int launch_fill(int n, int i0, int j0, int nrow, int ncol, float *a, int64_t lda, uint64_t seed, int calc_diag,
 	cudaStream_t st);

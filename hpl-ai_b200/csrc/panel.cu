@@ -146,6 +146,7 @@ static int getrf_launch(int b, float *a, int64_t lda, cudaStream_t st)
 	HPLAI_CUDA_TRY(cudaFuncSetAttribute(getrf_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(smem)));
 	getrf_kernel<NB><<<1, kGetrfThreads, smem, st>>>(b, a, lda);
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
 }
@@ -270,6 +271,7 @@ static int trsm_ru_launch(int m, int b, const float *u, int64_t ldu, float *a, i
 		static_cast<int>(smem)));
 	trsm_ru_kernel<R><<<(m + R - 1) / R, kTrsmThreads, smem, st>>>(m, b, u, ldu, a, lda,
 		reinterpret_cast<__half *>(lh), ldh, scale);
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
 }
@@ -384,6 +386,7 @@ static int trsm_ll_launch(int b, int ncols, const float *l, int64_t ldl, float *
 		static_cast<int>(smem)));
 	trsm_ll_kernel<C><<<(ncols + C - 1) / C, kTrsmThreads, smem, st>>>(b, ncols, l, ldl, a, lda,
 		reinterpret_cast<__half *>(uh), ldh, scale);
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
 }

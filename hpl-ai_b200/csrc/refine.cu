@@ -124,10 +124,12 @@ int otf_launch(int64_t n, int mb, int nb, double alpha, const double *x, double 
 	if (nb > 0) {
 		dim3 grid((mb + GEMV_ROWS - 1) / GEMV_ROWS, nchunks);
 		otf_partial_kernel<<<grid, GEMV_ROWS, 0, st>>>(n, mb, nb, alpha, x, state00, with_diag, diag, part, table());
+		count_launches();
 		HPLAI_CUDA_TRY(cudaGetLastError());
 	}
 	otf_reduce_kernel<<<(mb + 255) / 256, 256, 0, st>>>(mb, nb > 0 ? nchunks : 0, beta, part, y,
 		beta == 0.0 ? 1 : 0);
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
 }
@@ -358,6 +360,7 @@ int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void 
 	}
 	TrsvWork *w = static_cast<TrsvWork *>(work);
 	trsv_epoch_kernel<<<1, 1, 0, st>>>(w);
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	const int nbt = (n + TB - 1) / TB;
 	const int grid = nbt < max_blocks ? nbt : max_blocks;
@@ -365,6 +368,7 @@ int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void 
 	void *args[] = {(void *)&lw, (void *)&n, (void *)&a, (void *)&lda, (void *)&x, (void *)&w};
 	HPLAI_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(trsv_kernel), dim3(grid), dim3(TRSV_THREADS),
 		args, dsmem, st));
+	count_launches();
 	return HPLAI_OK;
 }
 
@@ -385,6 +389,7 @@ int launch_infnorm(int n, const double *x, double *out, cudaStream_t st)
 	int blocks = (n + 255) / 256;
 	if (blocks > 1184) blocks = 1184;
 	infnorm_kernel<<<blocks, 256, 0, st>>>(n, x, reinterpret_cast<unsigned long long *>(out));
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
 }
@@ -393,6 +398,7 @@ int launch_div(int n, const double *num, const double *den, double *out, cudaStr
 {
 	if (n <= 0) return HPLAI_OK;
 	div_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, num, den, out);
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
 }
@@ -401,6 +407,7 @@ int launch_axpy1(int n, const double *x, double *y, cudaStream_t st)
 {
 	if (n <= 0) return HPLAI_OK;
 	axpy1_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, x, y);
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
 }

@@ -316,6 +316,7 @@ int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, floa
 	std::memcpy(&lm, maps.lmap, sizeof(lm));
 	std::memcpy(&um, maps.umap, sizeof(um));
 	schur_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(lm, um, p);
+	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
 }

@@ -61,6 +61,8 @@ _get_rhs = _proto("hplai_get_rhs", _c_int, _vp, _vp)
 _get_diag = _proto("hplai_get_diag", _c_int, _vp, _vp)
 _get_ir_log = _proto("hplai_get_ir_log", _c_int, _vp, _vp, _vp, _c_int, ctypes.POINTER(_c_int))
 _get_phase_ms = _proto("hplai_get_phase_ms", _c_int, _vp, _vp, _c_int)
+_get_stream = _proto("hplai_get_stream", _vp, _vp)
+launch_count = _proto("hplai_launch_count", ctypes.c_ulonglong)
 _get_norms = _proto("hplai_get_norms", _c_int, _vp, ctypes.POINTER(_c_dbl), ctypes.POINTER(_c_dbl))
 _solve_host = _proto("hplai_solve_host", _c_int, _vp, _vp, _c_i64, _vp, _vp, _c_u64, _c_int, _vp,
                      ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
@@ -214,6 +216,20 @@ class Solver:
         out = np.zeros(len(PHASES))
         check(_get_phase_ms(self._h, _ptr(out), len(PHASES)), "hplai_get_phase_ms")
         return dict(zip(PHASES, out.tolist()))
+
+    def stream(self) -> int:
+        """cudaStream_t of this context as an integer handle."""
+        return _get_stream(self._h) or 0
+
+    def solve_host_ptrs(self, a_ptr: int, lda: int, rhs_ptr: int, diag_ptr: int, seed: int, maxit: int,
+                        x_ptr: int) -> RefineResult:
+        """hplai_solve_host on raw host pointers (e.g. pinned torch tensors)."""
+        e = IRErrors()
+        it = _c_int()
+        s = _solve_host(self._h, a_ptr, lda, rhs_ptr, diag_ptr, seed, maxit, x_ptr, ctypes.byref(e), ctypes.byref(it))
+        if s not in (HPLAI_OK, HPLAI_ENOTCONV):
+            check(s, "hplai_solve_host")
+        return RefineResult(e.residual, e.hpl_harness, it.value, s)
 
     def norms(self):
         a, b = _c_dbl(), _c_dbl()

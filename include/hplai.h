@@ -87,6 +87,9 @@ const char *hplai_status_string(int status);
 /* Text of the last CUDA error the library saw (thread-shared). */
 int hplai_last_error(char *buf, size_t len);
 int hplai_version(void);
+/* Kernel launches enqueued by this library since it was loaded (all
+ * contexts and leaf calls). */
+unsigned long long hplai_launch_count(void);
 
 /* build_panels (panel.hpp:135-268) + the driver's vector allocations
  * (main.cpp:196-213).  Requires n % b == 0 and 16 <= b <= 1024.  Allocates
@@ -127,6 +130,9 @@ int hplai_get_diag(hplai_ctx *ctx, double *diag);
 int hplai_get_ir_log(hplai_ctx *ctx, double *residual, double *harness, int cap, int *count);
 /* Accumulated milliseconds per hplai_phase since the last hplai_factor. */
 int hplai_get_phase_ms(hplai_ctx *ctx, double *ms, int count);
+/* The CUDA stream (cudaStream_t) every operation of this context runs on,
+ * for callers that time or order work against it. */
+void *hplai_get_stream(hplai_ctx *ctx);
 /* ||A||_inf (= 2 max diag, panel_norm.hpp:78-84) and ||b||_inf. */
 int hplai_get_norms(hplai_ctx *ctx, double *norma, double *normb);
 
