@@ -35,6 +35,12 @@ void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int 
 	g_err = buf;
 }
 
+void set_last_error_message(const char *msg)
+{
+	std::lock_guard<std::mutex> lk(g_err_mu);
+	g_err = msg;
+}
+
 static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
 } // namespace hplai

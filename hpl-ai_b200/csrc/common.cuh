@@ -32,6 +32,7 @@
 namespace hplai {
 
 void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int line);
+void set_last_error_message(const char *msg);
 
 // ---------------------------------------------------------------------------
 // LCG x <- a*x + c mod 2^64 (hpl_rand.hpp:8-57).

@@ -10,6 +10,8 @@
 #include "common.cuh"
 #include "internal.h"
 
+#include <mutex>
+
 namespace hplai {
 
 namespace {
@@ -412,6 +414,50 @@ int launch_axpy1(int n, const double *x, double *y, cudaStream_t st)
 	return HPLAI_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free on-the-fly GEMV.
+//
+// Callers that cannot allocate device memory (code that is handed every
+// device buffer by another runtime's allocator and has none of its own, or a
+// solve loop that must not call cudaMalloc because it can synchronise the
+// device) get the GEMV's partial-sum scratch from this fixed array instead
+// of a caller workspace.  It is part of the library image: every GPU that
+// loads libhplai holds its 4 MiB until the process exits.  It covers orders
+// up to kNoAllocMaxN (ceil(n/2048) * n doubles).  All calls share it.
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocMaxN = 32768;
+constexpr size_t kNoAllocScratchDoubles =
+	static_cast<size_t>((kNoAllocMaxN + GEMV_COLS - 1) / GEMV_COLS) * kNoAllocMaxN;
+static __device__ __align__(256) double g_gemv_noalloc_scratch[kNoAllocScratchDoubles];
+
+namespace {
+std::mutex g_noalloc_mu;
+constexpr int kMaxDevices = 64;
+void *g_noalloc_addr[kMaxDevices] = {};
+} // namespace
+
+// Device address of the scratch array on the current device.  In host code
+// the array's name is only a host-side handle, so the address is looked up
+// once per device (with that device current) and cached.
+static int noalloc_scratch(void **out)
+{
+	int dev = 0;
+	HPLAI_CUDA_TRY(cudaGetDevice(&dev));
+	if (dev < 0 || dev >= kMaxDevices) return HPLAI_EUNSUPPORTED;
+	std::lock_guard<std::mutex> lk(g_noalloc_mu);
+	if (!g_noalloc_addr[dev]) {
+		void *p = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress(&p, g_gemv_noalloc_scratch);
+		if (e != cudaSuccess) {
+			set_last_cuda_error(e, "cudaGetSymbolAddress(g_gemv_noalloc_scratch)", __FILE__, __LINE__);
+			return HPLAI_ECUDA;
+		}
+		g_noalloc_addr[dev] = p;
+	}
+	*out = g_noalloc_addr[dev];
+	return HPLAI_OK;
+}
+
 } // namespace hplai
 
 extern "C" size_t hplai_otf_gemv_workspace(int n) { return hplai::otf_gemv_workspace(n); }
@@ -451,4 +497,20 @@ extern "C" int hplai_infnorm(int n, const double *x, double *out, void *stream)
 {
 	if (n < 0 || (!x && n) || !out) return HPLAI_EINVAL;
 	return hplai::launch_infnorm(n, x, out, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hplai_otf_gemv_noalloc(int n, double alpha, const double *x, double beta, double *y, uint64_t seed,
+	const double *diag, void *stream)
+{
+	if (n <= 0 || !x || !y || !diag) return HPLAI_EINVAL;
+	if (n > hplai::kNoAllocMaxN) {
+		hplai::set_last_error_message("hplai_otf_gemv_noalloc: n exceeds HPLAI_OTF_GEMV_NOALLOC_MAX_N (32768)");
+		return HPLAI_EINVAL;
+	}
+	void *scratch = nullptr;
+	HPLAI_TRY(hplai::noalloc_scratch(&scratch));
+	// Every partial sum the fold reads is written by this call's first
+	// kernel, so the shared array needs no clearing between calls.
+	return hplai::launch_otf_gemv(n, alpha, x, beta, y, seed, diag, scratch,
+		hplai::kNoAllocScratchDoubles * sizeof(double), static_cast<cudaStream_t>(stream));
 }

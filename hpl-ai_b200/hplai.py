@@ -81,6 +81,8 @@ shgemm_minus = _proto("hplai_shgemm_minus", _c_int, _c_int, _c_int, _c_int, _vp,
                       _vp)
 otf_gemv_workspace = _proto("hplai_otf_gemv_workspace", _c_sz, _c_int)
 otf_gemv = _proto("hplai_otf_gemv", _c_int, _c_int, _c_dbl, _vp, _c_dbl, _vp, _c_u64, _vp, _vp, _c_sz, _vp)
+otf_gemv_noalloc = _proto("hplai_otf_gemv_noalloc", _c_int, _c_int, _c_dbl, _vp, _c_dbl, _vp, _c_u64, _vp, _vp)
+OTF_GEMV_NOALLOC_MAX_N = 32768
 otf_gemv_block = _proto("hplai_otf_gemv_block", _c_int, _c_i64, _c_int, _c_int, _c_dbl, _vp, _vp, _c_u64, _vp,
                         _c_sz, _vp)
 trsv_workspace = _proto("hplai_trsv_workspace", _c_sz, _c_int)

@@ -206,6 +206,22 @@ int hplai_otf_gemv(int n, double alpha, const double *x, double beta, double *y,
 int hplai_otf_gemv_block(int64_t n, int mb, int nb, double alpha, const double *x, double *y,
 	uint64_t state00, void *work, size_t work_bytes, void *stream);
 
+/* Allocation-free variant of hplai_otf_gemv (no counterpart in the
+ * reference): same arguments and result, minus the workspace.  For callers
+ * that cannot allocate device memory -- code that only receives device
+ * buffers from another runtime's allocator, or a solve loop that must not
+ * call cudaMalloc because it can synchronise the device.  The partial sums go
+ * to a scratch array compiled into the library (4 MiB on every GPU that
+ * loads it, held until the process exits), so n <= HPLAI_OTF_GEMV_NOALLOC_MAX_N;
+ * larger n returns HPLAI_EINVAL.  It allocates nothing.  The first call on
+ * each device looks the array's device address up with that device current;
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (other streams, other host threads on
+ * the same device) race on it -- serialise them. */
+#define HPLAI_OTF_GEMV_NOALLOC_MAX_N 32768
+int hplai_otf_gemv_noalloc(int n, double alpha, const double *x, double beta, double *y,
+	uint64_t seed, const double *diag, void *stream);
+
 /* Workspace bytes for the triangular solves at order n. */
 size_t hplai_trsv_workspace(int n);
 
