@@ -54,6 +54,8 @@ struct hplai_ctx {
 	float *A = nullptr;
 	uint16_t *Lh = nullptr, *Uh = nullptr;
 	SchurMaps maps;
+	TcPanels tc;
+	float *tcbuf = nullptr;   // phi, plo (n x ldp) and the four b x ldp inverse buffers
 	double *rhs = nullptr, *d = nullptr, *x = nullptr, *r = nullptr, *scal = nullptr;
 	void *gemv_work = nullptr;
 	size_t gemv_bytes = 0;
@@ -75,6 +77,7 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->A);
 	cudaFree(c->Lh);
 	cudaFree(c->Uh);
+	cudaFree(c->tcbuf);
 	cudaFree(c->rhs);
 	cudaFree(c->d);
 	cudaFree(c->x);
@@ -190,6 +193,9 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	CTX_ALLOC(c->A, sizeof(float) * static_cast<size_t>(c->lda) * n);
 	CTX_ALLOC(c->Lh, sizeof(uint16_t) * static_cast<size_t>(c->ldh) * n);
 	CTX_ALLOC(c->Uh, sizeof(uint16_t) * static_cast<size_t>(c->ldh) * n);
+	const int64_t ldp = round_up(b, 32);
+	const size_t tc_elems = static_cast<size_t>(ldp) * (2 * static_cast<size_t>(n) + 4 * static_cast<size_t>(b));
+	CTX_ALLOC(c->tcbuf, sizeof(float) * tc_elems);
 	CTX_ALLOC(c->rhs, sizeof(double) * n);
 	CTX_ALLOC(c->d, sizeof(double) * n);
 	CTX_ALLOC(c->x, sizeof(double) * n);
@@ -204,6 +210,13 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		return HPLAI_ECUDA;
 	}
 	int s = schur_make_maps(&c->maps, c->Lh, n, c->ldh, c->Uh, n, c->ldh, b);
+	if (s == HPLAI_OK) s = schur_set_cmap(&c->maps, c->A, n, n, c->lda);
+	if (s == HPLAI_OK) {
+		float *base = c->tcbuf;
+		const size_t pn = static_cast<size_t>(ldp) * n, pb = static_cast<size_t>(ldp) * b;
+		s = tc_panels_make(&c->tc, n, b, base, base + pn, ldp, base + 2 * pn, base + 2 * pn + pb,
+			base + 2 * pn + 2 * pb, base + 2 * pn + 3 * pb);
+	}
 	if (s != HPLAI_OK) {
 		ctx_free(c);
 		return s;
@@ -254,6 +267,8 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	const int64_t lda = c->lda, ldh = c->ldh;
 	cudaStream_t st = c->st;
 	schur_status_reset();
+	tc_status_reset();
+	const bool simt = (c->flags & HPLAI_FLAG_SIMT_PANELS) != 0;
 	for (double &v : c->phase_ms) v = 0.0;
 	PhaseEvents pe;
 	// Right-looking blocked LU without pivoting, one panel per step
@@ -268,20 +283,31 @@ extern "C" int hplai_factor(hplai_ctx *c)
 		if (k == nb - 1) break;
 		const int rem = n - static_cast<int>(kb) - b;
 		HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_L));
-		HPLAI_TRY(launch_trsm_right_upper(rem, b, diag, lda, diag + b, lda, c->Lh + (kb + b) * ldh, ldh, 1.0f, st));
+		if (simt) {
+			HPLAI_TRY(launch_trsm_right_upper(rem, b, diag, lda, diag + b, lda, c->Lh + (kb + b) * ldh, ldh, 1.0f, st));
+		} else {
+			HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st));
+			HPLAI_TRY(launch_lpanel_tc(c->tc, rem, diag + b, lda, c->Lh + (kb + b) * ldh, ldh, 1.0f, 0, st));
+		}
 		HPLAI_TRY(pe.end(st));
 		HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_R));
-		HPLAI_TRY(launch_trsm_left_lower(b, rem, diag, lda, diag + static_cast<int64_t>(b) * lda, lda,
-			c->Uh + (kb + b) * ldh, ldh, 1.0f, st));
+		if (simt) {
+			HPLAI_TRY(launch_trsm_left_lower(b, rem, diag, lda, diag + static_cast<int64_t>(b) * lda, lda,
+				c->Uh + (kb + b) * ldh, ldh, 1.0f, st));
+		} else {
+			HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, c->Uh + (kb + b) * ldh,
+				ldh, 1.0f, 0, st));
+		}
 		HPLAI_TRY(pe.end(st));
 		HPLAI_TRY(pe.record(st, HPLAI_PH_GEMM_UPDATE));
 		HPLAI_TRY(launch_schur(c->maps, static_cast<int>(kb) + b, static_cast<int>(kb) + b, rem, rem,
-			diag + b + static_cast<int64_t>(b) * lda, lda, st));
+			diag + b + static_cast<int64_t>(b) * lda, lda, static_cast<int>(kb) + b, static_cast<int>(kb) + b, st));
 		HPLAI_TRY(pe.end(st));
 	}
 	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
 	pe.collect(c->phase_ms);
 	HPLAI_TRY(schur_status());
+	HPLAI_TRY(tc_status());
 	c->factored = true;
 	return HPLAI_OK;
 }

@@ -32,17 +32,51 @@ int launch_trsm_left_lower(int b, int ncols, const float *l, int64_t ldl, float 
 struct SchurMaps {
 	alignas(64) unsigned char lmap[128];
 	alignas(64) unsigned char umap[128];
-	int k;       // inner dimension (panel width)
+	alignas(64) unsigned char cmap[128];   // FP32 C (the trailing matrix), for the reduce epilogue
+	int k;         // inner dimension (panel width)
+	bool has_cmap;
 };
 // L: lrows x k FP16, row-major with ldl; U: urows x k FP16 (row j = column j
 // of U), ldu.  Rows beyond lrows/urows read as zero.
 int schur_make_maps(SchurMaps *m, const uint16_t *lh, int lrows, int64_t ldl, const uint16_t *uh, int urows,
 	int64_t ldu, int k);
-// C (m x n, ldc) -= L[lrow0 : lrow0+m, 0:k] * U[urow0 : urow0+n, 0:k]^T
-int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc,
-	cudaStream_t st);
+// FP32 map over C (rows x cols, ldc) used by the TMA reduce-add epilogue; left
+// unset (plain epilogue) when c or ldc is not 16-byte aligned.
+int schur_set_cmap(SchurMaps *m, const float *c, int rows, int cols, int64_t ldc);
+// C (m x n, ldc) -= L[lrow0 : lrow0+m, 0:k] * U[urow0 : urow0+n, 0:k]^T.  C(0,0)
+// sits at (crow0, ccol0) of the C map.
+int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
+	int ccol0, cudaStream_t st);
 int schur_status();          // HPLAI_ETIMEOUT if a device wait ran out since the last reset
 void schur_status_reset();
+
+// tcpanel.cu
+// Panel TRSMs on tensor cores (3xTF32): triangular inverses of the diagonal
+// block and the two panel products.  Buffers are caller-owned; the tensor
+// maps are built once per context.
+struct TcPanels {
+	alignas(64) unsigned char m_phi[128];
+	alignas(64) unsigned char m_plo[128];
+	alignas(64) unsigned char m_uhi[128];
+	alignas(64) unsigned char m_ulo[128];
+	alignas(64) unsigned char m_lhi[128];
+	alignas(64) unsigned char m_llo[128];
+	int n, b;
+	int64_t ldp;                     // row pitch of every buffer below, a multiple of 32 floats
+	float *phi, *plo;                // n x ldp: K-major hi/lo copy of the current panel
+	float *uhi, *ulo, *lhi, *llo;    // b x ldp: hi/lo of U11^{-1} and L11^{-1}
+};
+int tc_panels_make(TcPanels *t, int n, int b, float *phi, float *plo, int64_t ldp, float *uhi, float *ulo,
+	float *lhi, float *llo);
+int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStream_t st);
+// A_col (rem x b) <- A_col U11^{-1}; lh row i = half(scale * A_col row i)
+int launch_lpanel_tc(const TcPanels &t, int rem, float *acol, int64_t lda, uint16_t *lh, int64_t ldh, float scale,
+	int max_ctas, cudaStream_t st);
+// A_row (b x rem) <- L11^{-1} A_row; uh row j = half(scale * A_row column j)
+int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint16_t *uh, int64_t ldh, float scale,
+	int max_ctas, cudaStream_t st);
+int tc_status();
+void tc_status_reset();
 
 // refine.cu
 size_t otf_gemv_workspace(int n);

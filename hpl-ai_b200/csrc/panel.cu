@@ -1,9 +1,10 @@
 // panel.cu -- FP32 panel factorisation kernels for the blocked no-pivot LU.
 //
 //  getrf_kernel     : b x b diagonal block LU in one CTA (getrf_nopiv.hpp:30-141)
-//  trsm_ru_kernel   : L panel  A_col <- A_col * U^{-1}, plus its FP16 copy
+//  trsm_kernel      : L panel  A_col <- A_col * U^{-1}, plus its FP16 copy
 //                     (update_left_panels + convert_left_panels, panel_trf.hpp:143-157,182-207)
-//  trsm_ll_kernel   : U panel  A_row <- L^{-1} * A_row, plus its FP16 copy
+//                     U panel  A_row <- L^{-1} * A_row, plus its FP16 copy, as the
+//                     same solve on the transpose
 //                     (update_right_panels + convert_right_panels, panel_trf.hpp:158-171,208-233)
 //
 // Every element receives its updates a_ij <- fma(-l_ik, u_kj, a_ij) in
@@ -17,17 +18,19 @@
 namespace hplai {
 
 // ---------------------------------------------------------------------------
-// Diagonal block LU.
+// Diagonal block LU.  One CTA of 512 threads; each thread owns up to two rows
+// of the current column panel, so b <= 1024.
 // ---------------------------------------------------------------------------
-constexpr int kGetrfThreads = 1024;
+constexpr int kGetrfThreads = 512;
 
 template <int NB>
 __global__ void __launch_bounds__(kGetrfThreads, 1) getrf_kernel(int b, float *__restrict__ a, int64_t lda)
 {
 	extern __shared__ float sm[];
+	const int ldu = (b + 3) & ~3;  // U12 row stride, a multiple of 4 for float4 reads
 	float *Lp = sm;                // panel, column-major: Lp[c*b + r], r relative to kb
-	float *Up = sm + b * NB;       // U12 rows: Up[i*b + c], c relative to kb+w
-	float *prow = Up + NB * b;     // two pivot-row buffers of NB floats
+	float *Up = sm + b * NB;       // U12 rows: Up[i*ldu + c], c relative to kb+w
+	float *prow = Up + NB * ldu;   // two pivot-row buffers of NB floats
 	const int t = threadIdx.x;
 
 	for (int kb = 0; kb < b; kb += NB) {
@@ -35,37 +38,50 @@ __global__ void __launch_bounds__(kGetrfThreads, 1) getrf_kernel(int b, float *_
 		const int mrows = b - kb;
 		const int rem = mrows - w;
 
-		// Phase 1: factor the (b-kb) x w column panel, one row per thread.
-		float p[NB];
-		const bool own = t < mrows;
+		// Phase 1: factor the (b-kb) x w column panel; rows t and t+512.
+		float p0[NB], p1[NB];
+		const bool own0 = t < mrows, own1 = t + kGetrfThreads < mrows;
 #pragma unroll
-		for (int c = 0; c < NB; ++c)
-			p[c] = (own && c < w) ? a[static_cast<int64_t>(kb + c) * lda + kb + t] : 0.f;
+		for (int c = 0; c < NB; ++c) {
+			p0[c] = (own0 && c < w) ? a[static_cast<int64_t>(kb + c) * lda + kb + t] : 0.f;
+			p1[c] = (own1 && c < w) ? a[static_cast<int64_t>(kb + c) * lda + kb + t + kGetrfThreads] : 0.f;
+		}
 #pragma unroll
 		for (int j = 0; j < NB; ++j) {
 			if (j < w) {
 				float *pr = prow + (j & 1) * NB;
 				if (t == j) {
 #pragma unroll
-					for (int c = 0; c < NB; ++c) pr[c] = p[c];
+					for (int c = 0; c < NB; ++c) pr[c] = p0[c];
 				}
 				__syncthreads();
-				if (own && t > j) {
-					const float inv = 1.0f / pr[j];
-					const float l = p[j] * inv;
-					p[j] = l;
+				const float inv = 1.0f / pr[j];
+				if (own0 && t > j) {
+					const float l = p0[j] * inv;
+					p0[j] = l;
 #pragma unroll
 					for (int c = j + 1; c < NB; ++c)
-						if (c < w) p[c] = fmaf(-l, pr[c], p[c]);
+						if (c < w) p0[c] = fmaf(-l, pr[c], p0[c]);
+				}
+				if (own1) {
+					const float l = p1[j] * inv;
+					p1[j] = l;
+#pragma unroll
+					for (int c = j + 1; c < NB; ++c)
+						if (c < w) p1[c] = fmaf(-l, pr[c], p1[c]);
 				}
 			}
 		}
-		if (own) {
 #pragma unroll
-			for (int c = 0; c < NB; ++c) {
-				if (c < w) {
-					a[static_cast<int64_t>(kb + c) * lda + kb + t] = p[c];
-					Lp[c * b + t] = p[c];
+		for (int c = 0; c < NB; ++c) {
+			if (c < w) {
+				if (own0) {
+					a[static_cast<int64_t>(kb + c) * lda + kb + t] = p0[c];
+					Lp[c * b + t] = p0[c];
+				}
+				if (own1) {
+					a[static_cast<int64_t>(kb + c) * lda + kb + t + kGetrfThreads] = p1[c];
+					Lp[c * b + t + kGetrfThreads] = p1[c];
 				}
 			}
 		}
@@ -73,9 +89,9 @@ __global__ void __launch_bounds__(kGetrfThreads, 1) getrf_kernel(int b, float *_
 		if (rem <= 0) break;
 
 		// Phase 2: U12 = L11^{-1} A12 (unit lower), one column per thread.
-		if (t < rem) {
+		for (int cc = t; cc < rem; cc += kGetrfThreads) {
 			float q[NB];
-			float *colp = a + static_cast<int64_t>(kb + w + t) * lda + kb;
+			float *colp = a + static_cast<int64_t>(kb + w + cc) * lda + kb;
 #pragma unroll
 			for (int i = 0; i < NB; ++i) q[i] = (i < w) ? colp[i] : 0.f;
 #pragma unroll
@@ -88,7 +104,7 @@ __global__ void __launch_bounds__(kGetrfThreads, 1) getrf_kernel(int b, float *_
 			for (int i = 0; i < NB; ++i) {
 				if (i < w) {
 					colp[i] = q[i];
-					Up[i * b + t] = q[i];
+					Up[i * ldu + cc] = q[i];
 				}
 			}
 		}
@@ -100,6 +116,7 @@ __global__ void __launch_bounds__(kGetrfThreads, 1) getrf_kernel(int b, float *_
 			const int warp = t >> 5, lane = t & 31;
 			const int rblocks = (rem + 255) / 256;
 			const int cblocks = (rem + 3) / 4;
+			const bool vec = (ldu % 4 == 0);
 			for (int item = warp; item < rblocks * cblocks; item += kGetrfThreads / 32) {
 				const int rb = item % rblocks, cbk = item / rblocks;
 				const int r0 = rb * 256 + lane, c0 = cbk * 4;
@@ -119,8 +136,13 @@ __global__ void __launch_bounds__(kGetrfThreads, 1) getrf_kernel(int b, float *_
 						const int r = r0 + 32 * i;
 						lv[i] = (r < rem) ? Lp[pp * b + w + r] : 0.f;
 					}
+					if (vec) {
+						const float4 u4 = *reinterpret_cast<const float4 *>(&Up[pp * ldu + c0]);
+						uv[0] = u4.x; uv[1] = u4.y; uv[2] = u4.z; uv[3] = u4.w;
+					} else {
 #pragma unroll
-					for (int j = 0; j < 4; ++j) uv[j] = (c0 + j < rem) ? Up[pp * b + c0 + j] : 0.f;
+						for (int j = 0; j < 4; ++j) uv[j] = Up[pp * ldu + c0 + j];
+					}
 #pragma unroll
 					for (int i = 0; i < 8; ++i)
 #pragma unroll
@@ -142,7 +164,8 @@ __global__ void __launch_bounds__(kGetrfThreads, 1) getrf_kernel(int b, float *_
 template <int NB>
 static int getrf_launch(int b, float *a, int64_t lda, cudaStream_t st)
 {
-	const size_t smem = (static_cast<size_t>(2) * b * NB + 2 * NB) * sizeof(float);
+	const int ldu = (b + 3) & ~3;
+	const size_t smem = (static_cast<size_t>(b) * NB + static_cast<size_t>(NB) * ldu + 2 * NB) * sizeof(float);
 	HPLAI_CUDA_TRY(cudaFuncSetAttribute(getrf_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(smem)));
 	getrf_kernel<NB><<<1, kGetrfThreads, smem, st>>>(b, a, lda);
@@ -159,67 +182,91 @@ int launch_getrf(int b, float *a, int64_t lda, cudaStream_t st)
 }
 
 // ---------------------------------------------------------------------------
-// L panel: X (m x b) <- X * U^{-1}, U upper non-unit; lh = half(scale * X),
-// row-major.  A CTA owns R rows of X in shared memory (Xs[j*R + r]).
+// Panel TRSM + FP16 copy, one kernel for both panels.
+//
+// X (m x b) <- X * T^{-1} with T upper triangular (b x b).  A CTA owns R rows
+// of X in shared memory (Xs[j*LDX + r]).
+//   L panel (update_left_panels):  X = A_col (column-major, X[r][j] at
+//            a[j*lda + r]), T = U11 (T[p][j] at t[j*ldt + p]), non-unit.
+//   U panel (update_right_panels): L^{-1} A_row = (A_row^T L^{-T})^T, so
+//            X = A_row^T (row-major, X[r][j] at a[r*lda + j]) and T = L11^T
+//            (T[p][j] = L[j][p] at t[p*ldt + j]), unit diagonal.
+// Element (r, j) receives x -= T[p][j] * x[r][p] for p = 0..j-1 in
+// increasing p, then x *= 1/T[j][j] when non-unit: netlib strsm's order for
+// both (R,U,N,N) and (L,L,N,U), so the result is bit-exact with it.
+// hc[(row0 + r)*ldh + j] = half(scale * X[r][j]) in both cases (the L copy is
+// row-major; the U copy stores column j of U as row j).
 // ---------------------------------------------------------------------------
 constexpr int kTrsmThreads = 256;
 
-template <int R>
-__global__ void __launch_bounds__(kTrsmThreads) trsm_ru_kernel(int m, int b, const float *__restrict__ u,
-	int64_t ldu, float *__restrict__ a, int64_t lda, __half *__restrict__ lh, int64_t ldh, float scale)
+template <int R, bool ROWX, bool TRANS_T>
+__global__ void __launch_bounds__(kTrsmThreads) trsm_kernel(int m, int b, const float *__restrict__ t,
+	int64_t ldt, float *__restrict__ a, int64_t lda, __half *__restrict__ hc, int64_t ldh, float scale)
 {
 	constexpr int CW = 4 * 4 * kTrsmThreads / R;   // update chunk width (4x4 tiles, one per thread)
 	constexpr int LDX = R + 4;                     // padded so row-wise reads spread over banks
 	constexpr int LDU = CW + 1;
+	constexpr bool UNIT = TRANS_T;                 // L11^T has a unit diagonal
 	extern __shared__ float sm[];
-	float *Xs = sm;                                  // b x LDX, Xs[j*LDX + r]
-	float *Us = Xs + static_cast<size_t>(b) * LDX;   // 32 x LDU, Us[p*LDU + cc] = U[jb+p][c0+cc]
-	float *Ud = Us + 32 * LDU;                       // 32 x 33,  Ud[p*33 + j]  = U[jb+p][jb+j]
+	float *Xs = sm;                                  // b x LDX
+	float *Us = Xs + static_cast<size_t>(b) * LDX;   // 32 x LDU, Us[p*LDU + cc] = T[jb+p][c0+cc]
+	float *Ud = Us + 32 * LDU;                       // 32 x 33,  Ud[p*33 + j]  = T[jb+p][jb+j]
 	float *inv = Ud + 32 * 33;                       // 32 reciprocals
-	const int t = threadIdx.x;
+	const int tid = threadIdx.x;
 	const int row0 = blockIdx.x * R;
 	const int rows = min(R, m - row0);
+	auto tval = [&](int p, int j) -> float {
+		return TRANS_T ? t[static_cast<int64_t>(p) * ldt + j] : t[static_cast<int64_t>(j) * ldt + p];
+	};
 
-	for (int idx = t; idx < R * b; idx += kTrsmThreads) {
-		const int r = idx % R, j = idx / R;
-		Xs[j * LDX + r] = (r < rows) ? a[static_cast<int64_t>(j) * lda + row0 + r] : 0.f;
+	if (ROWX) {
+		for (int idx = tid; idx < R * b; idx += kTrsmThreads) {
+			const int r = idx / b, j = idx - r * b;
+			Xs[j * LDX + r] = (r < rows) ? a[static_cast<int64_t>(row0 + r) * lda + j] : 0.f;
+		}
+	} else {
+		for (int idx = tid; idx < R * b; idx += kTrsmThreads) {
+			const int r = idx % R, j = idx / R;
+			Xs[j * LDX + r] = (r < rows) ? a[static_cast<int64_t>(j) * lda + row0 + r] : 0.f;
+		}
 	}
 
 	for (int jb = 0; jb < b; jb += 32) {
 		const int jw = min(32, b - jb);
-		for (int idx = t; idx < 32 * 32; idx += kTrsmThreads) {
-			const int p = idx & 31, j = idx >> 5;
-			Ud[p * 33 + j] = (p < jw && j < jw) ? u[static_cast<int64_t>(jb + j) * ldu + jb + p] : 0.f;
+		for (int idx = tid; idx < 32 * 32; idx += kTrsmThreads) {
+			const int p = TRANS_T ? (idx >> 5) : (idx & 31), j = TRANS_T ? (idx & 31) : (idx >> 5);
+			Ud[p * 33 + j] = (p < jw && j < jw) ? tval(jb + p, jb + j) : 0.f;
 		}
-		if (t < jw) inv[t] = 1.0f / u[static_cast<int64_t>(jb + t) * ldu + jb + t];
+		if (!UNIT && tid < jw) inv[tid] = 1.0f / tval(jb + tid, jb + tid);
 		__syncthreads();
 		// Triangular 32-column block: one row per thread.
-		if (t < R) {
+		if (tid < R) {
 			float x[32];
 #pragma unroll
-			for (int j = 0; j < 32; ++j) x[j] = (j < jw) ? Xs[(jb + j) * LDX + t] : 0.f;
+			for (int j = 0; j < 32; ++j) x[j] = (j < jw) ? Xs[(jb + j) * LDX + tid] : 0.f;
 #pragma unroll
 			for (int j = 0; j < 32; ++j) {
 				if (j < jw) {
 #pragma unroll
 					for (int p = 0; p < j; ++p) x[j] = fmaf(-Ud[p * 33 + j], x[p], x[j]);
-					x[j] *= inv[j];
+					if (!UNIT) x[j] *= inv[j];
 				}
 			}
 #pragma unroll
 			for (int j = 0; j < 32; ++j)
-				if (j < jw) Xs[(jb + j) * LDX + t] = x[j];
+				if (j < jw) Xs[(jb + j) * LDX + tid] = x[j];
 		}
 		__syncthreads();
 		// Update the columns right of the block, CW at a time.
 		for (int c0 = jb + jw; c0 < b; c0 += CW) {
 			const int cw = min(CW, b - c0);
-			for (int idx = t; idx < 32 * CW; idx += kTrsmThreads) {
-				const int p = idx & 31, cc = idx >> 5;
-				Us[p * LDU + cc] = (p < jw && cc < cw) ? u[static_cast<int64_t>(c0 + cc) * ldu + jb + p] : 0.f;
+			for (int idx = tid; idx < 32 * CW; idx += kTrsmThreads) {
+				// coalesced along the contiguous index of T's storage
+				const int p = TRANS_T ? (idx / CW) : (idx & 31), cc = TRANS_T ? (idx % CW) : (idx >> 5);
+				Us[p * LDU + cc] = (p < jw && cc < cw) ? tval(jb + p, c0 + cc) : 0.f;
 			}
 			__syncthreads();
-			const int rt = t % (R / 4), ct = t / (R / 4);
+			const int rt = tid % (R / 4), ct = tid / (R / 4);
 			const int r0 = rt * 4, cc0 = ct * 4;
 			if (cc0 < cw) {
 				float acc[4][4];
@@ -249,155 +296,73 @@ __global__ void __launch_bounds__(kTrsmThreads) trsm_ru_kernel(int m, int b, con
 		}
 	}
 
-	for (int idx = t; idx < R * b; idx += kTrsmThreads) {
-		const int r = idx % R, j = idx / R;
-		if (r < rows) a[static_cast<int64_t>(j) * lda + row0 + r] = Xs[j * LDX + r];
+	if (ROWX) {
+		for (int idx = tid; idx < R * b; idx += kTrsmThreads) {
+			const int r = idx / b, j = idx - r * b;
+			if (r < rows) a[static_cast<int64_t>(row0 + r) * lda + j] = Xs[j * LDX + r];
+		}
+	} else {
+		for (int idx = tid; idx < R * b; idx += kTrsmThreads) {
+			const int r = idx % R, j = idx / R;
+			if (r < rows) a[static_cast<int64_t>(j) * lda + row0 + r] = Xs[j * LDX + r];
+		}
 	}
-	if (lh) {
-		for (int idx = t; idx < R * b; idx += kTrsmThreads) {
-			const int r = idx / b, j = idx % b;
-			if (r < rows) lh[static_cast<int64_t>(row0 + r) * ldh + j] = __float2half_rn(scale * Xs[j * LDX + r]);
+	if (hc) {
+		// 8 consecutive halves per thread (16-byte store), rows across lanes.
+		const int b8 = b / 8;
+		for (int idx = tid; idx < R * b8; idx += kTrsmThreads) {
+			const int r = idx % R, q = idx / R;
+			if (r < rows) {
+				__align__(16) __half h[8];
+#pragma unroll
+				for (int e = 0; e < 8; ++e) h[e] = __float2half_rn(scale * Xs[(8 * q + e) * LDX + r]);
+				*reinterpret_cast<uint4 *>(hc + static_cast<int64_t>(row0 + r) * ldh + 8 * q) =
+					*reinterpret_cast<const uint4 *>(h);
+			}
+		}
+		for (int idx = tid; idx < R * (b - 8 * b8); idx += kTrsmThreads) {
+			const int r = idx % R, j = 8 * b8 + idx / R;
+			if (r < rows) hc[static_cast<int64_t>(row0 + r) * ldh + j] = __float2half_rn(scale * Xs[j * LDX + r]);
 		}
 	}
 }
 
-template <int R>
-static int trsm_ru_launch(int m, int b, const float *u, int64_t ldu, float *a, int64_t lda, uint16_t *lh,
-	int64_t ldh, float scale, cudaStream_t st)
+template <int R, bool ROWX, bool TRANS_T>
+static int trsm_launch(int m, int b, const float *t, int64_t ldt, float *a, int64_t lda, uint16_t *hc, int64_t ldh,
+	float scale, cudaStream_t st)
 {
 	constexpr int CW = 4 * 4 * kTrsmThreads / R;
 	const size_t smem = (static_cast<size_t>(b) * (R + 4) + 32 * (CW + 1) + 32 * 33 + 32) * sizeof(float);
-	HPLAI_CUDA_TRY(cudaFuncSetAttribute(trsm_ru_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	HPLAI_CUDA_TRY(cudaFuncSetAttribute(trsm_kernel<R, ROWX, TRANS_T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(smem)));
-	trsm_ru_kernel<R><<<(m + R - 1) / R, kTrsmThreads, smem, st>>>(m, b, u, ldu, a, lda,
-		reinterpret_cast<__half *>(lh), ldh, scale);
+	trsm_kernel<R, ROWX, TRANS_T><<<(m + R - 1) / R, kTrsmThreads, smem, st>>>(m, b, t, ldt, a, lda,
+		reinterpret_cast<__half *>(hc), ldh, scale);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
+}
+
+static bool vec_ok(const uint16_t *hc, int64_t ldh)
+{
+	return !hc || ((reinterpret_cast<uintptr_t>(hc) & 15u) == 0 && ldh % 8 == 0);
 }
 
 int launch_trsm_right_upper(int m, int b, const float *u, int64_t ldu, float *a, int64_t lda, uint16_t *lh,
 	int64_t ldh, float scale, cudaStream_t st)
 {
 	if (m <= 0) return HPLAI_OK;
-	if (b <= 0 || b > 1024) return HPLAI_EINVAL;
-	if (b <= 512) return trsm_ru_launch<64>(m, b, u, ldu, a, lda, lh, ldh, scale, st);
-	return trsm_ru_launch<32>(m, b, u, ldu, a, lda, lh, ldh, scale, st);
-}
-
-// ---------------------------------------------------------------------------
-// U panel: Y (b x ncols) <- L^{-1} Y, L unit lower; uh[j*ldh + k] =
-// half(scale * Y[k][j]).  A CTA owns C columns (Ys[i*LDY + c]).
-// ---------------------------------------------------------------------------
-template <int C>
-__global__ void __launch_bounds__(kTrsmThreads) trsm_ll_kernel(int b, int ncols, const float *__restrict__ l,
-	int64_t ldl, float *__restrict__ a, int64_t lda, __half *__restrict__ uh, int64_t ldh, float scale)
-{
-	constexpr int LDY = C + 1;
-	constexpr int RW = 4 * 4 * kTrsmThreads / C;   // update chunk height (rows)
-	extern __shared__ float sm[];
-	float *Ys = sm;                                  // b x LDY
-	float *Ls = Ys + static_cast<size_t>(b) * LDY;   // RW x 33  (rows of L, 32 columns)
-	float *Ld = Ls + RW * 33;                        // 32 x 33 diagonal block Ld[i*33 + k]
-	const int t = threadIdx.x;
-	const int col0 = blockIdx.x * C;
-	const int cols = min(C, ncols - col0);
-
-	for (int idx = t; idx < C * b; idx += kTrsmThreads) {
-		const int i = idx % b, c = idx / b;
-		Ys[i * LDY + c] = (c < cols) ? a[static_cast<int64_t>(col0 + c) * lda + i] : 0.f;
-	}
-
-	for (int kb = 0; kb < b; kb += 32) {
-		const int kw = min(32, b - kb);
-		for (int idx = t; idx < 32 * 32; idx += kTrsmThreads) {
-			const int i = idx & 31, k = idx >> 5;
-			Ld[i * 33 + k] = (i < kw && k < kw) ? l[static_cast<int64_t>(kb + k) * ldl + kb + i] : 0.f;
-		}
-		__syncthreads();
-		if (t < C) {
-			float y[32];
-#pragma unroll
-			for (int i = 0; i < 32; ++i) y[i] = (i < kw) ? Ys[(kb + i) * LDY + t] : 0.f;
-#pragma unroll
-			for (int k = 0; k < 32; ++k) {
-#pragma unroll
-				for (int i = k + 1; i < 32; ++i)
-					if (i < kw) y[i] = fmaf(-y[k], Ld[i * 33 + k], y[i]);
-			}
-#pragma unroll
-			for (int i = 0; i < 32; ++i)
-				if (i < kw) Ys[(kb + i) * LDY + t] = y[i];
-		}
-		__syncthreads();
-		for (int i0 = kb + kw; i0 < b; i0 += RW) {
-			const int rw = min(RW, b - i0);
-			for (int idx = t; idx < RW * 32; idx += kTrsmThreads) {
-				const int ii = idx % RW, k = idx / RW;
-				Ls[ii * 33 + k] = (ii < rw && k < kw) ? l[static_cast<int64_t>(kb + k) * ldl + i0 + ii] : 0.f;
-			}
-			__syncthreads();
-			const int ct = t % (C / 4), rt = t / (C / 4);
-			const int cc0 = ct * 4, ii0 = rt * 4;
-			if (ii0 < rw) {
-				float acc[4][4];
-#pragma unroll
-				for (int i = 0; i < 4; ++i)
-#pragma unroll
-					for (int j = 0; j < 4; ++j) acc[i][j] = (ii0 + i < rw) ? Ys[(i0 + ii0 + i) * LDY + cc0 + j] : 0.f;
-				for (int k = 0; k < kw; ++k) {
-					float yv[4], lv[4];
-#pragma unroll
-					for (int j = 0; j < 4; ++j) yv[j] = Ys[(kb + k) * LDY + cc0 + j];
-#pragma unroll
-					for (int i = 0; i < 4; ++i) lv[i] = Ls[(ii0 + i) * 33 + k];
-#pragma unroll
-					for (int i = 0; i < 4; ++i)
-#pragma unroll
-						for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(-yv[j], lv[i], acc[i][j]);
-				}
-#pragma unroll
-				for (int i = 0; i < 4; ++i)
-#pragma unroll
-					for (int j = 0; j < 4; ++j)
-						if (ii0 + i < rw) Ys[(i0 + ii0 + i) * LDY + cc0 + j] = acc[i][j];
-			}
-			__syncthreads();
-		}
-	}
-
-	for (int idx = t; idx < C * b; idx += kTrsmThreads) {
-		const int i = idx % b, c = idx / b;
-		if (c < cols) {
-			const float v = Ys[i * LDY + c];
-			a[static_cast<int64_t>(col0 + c) * lda + i] = v;
-			if (uh) uh[static_cast<int64_t>(col0 + c) * ldh + i] = __float2half_rn(scale * v);
-		}
-	}
-}
-
-template <int C>
-static int trsm_ll_launch(int b, int ncols, const float *l, int64_t ldl, float *a, int64_t lda, uint16_t *uh,
-	int64_t ldh, float scale, cudaStream_t st)
-{
-	constexpr int RW = 4 * 4 * kTrsmThreads / C;
-	const size_t smem = (static_cast<size_t>(b) * (C + 1) + RW * 33 + 32 * 33) * sizeof(float);
-	HPLAI_CUDA_TRY(cudaFuncSetAttribute(trsm_ll_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		static_cast<int>(smem)));
-	trsm_ll_kernel<C><<<(ncols + C - 1) / C, kTrsmThreads, smem, st>>>(b, ncols, l, ldl, a, lda,
-		reinterpret_cast<__half *>(uh), ldh, scale);
-	count_launches();
-	HPLAI_CUDA_TRY(cudaGetLastError());
-	return HPLAI_OK;
+	if (b <= 0 || b > 1024 || !vec_ok(lh, ldh)) return HPLAI_EINVAL;
+	if (b <= 512) return trsm_launch<64, false, false>(m, b, u, ldu, a, lda, lh, ldh, scale, st);
+	return trsm_launch<32, false, false>(m, b, u, ldu, a, lda, lh, ldh, scale, st);
 }
 
 int launch_trsm_left_lower(int b, int ncols, const float *l, int64_t ldl, float *a, int64_t lda, uint16_t *uh,
 	int64_t ldh, float scale, cudaStream_t st)
 {
 	if (ncols <= 0) return HPLAI_OK;
-	if (b <= 0 || b > 1024) return HPLAI_EINVAL;
-	if (b <= 512) return trsm_ll_launch<64>(b, ncols, l, ldl, a, lda, uh, ldh, scale, st);
-	return trsm_ll_launch<32>(b, ncols, l, ldl, a, lda, uh, ldh, scale, st);
+	if (b <= 0 || b > 1024 || !vec_ok(uh, ldh)) return HPLAI_EINVAL;
+	if (b <= 512) return trsm_launch<64, true, true>(ncols, b, l, ldl, a, lda, uh, ldh, scale, st);
+	return trsm_launch<32, true, true>(ncols, b, l, ldl, a, lda, uh, ldh, scale, st);
 }
 
 } // namespace hplai

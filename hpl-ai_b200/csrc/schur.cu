@@ -6,14 +6,16 @@
 // persistent, warp-specialised kernel does the same on sm_100a:
 //
 //   warp 0      TMA producer: 128x64 (L) and 256x64 (U) FP16 tiles, 128B
-//               swizzle, into a 4-stage shared-memory ring; also prefetches
-//               the C tile into L2 ahead of its epilogue.
+//               swizzle, into a 4-stage shared-memory ring.  (An L2 prefetch
+//               of the C tile ahead of its epilogue measured 34-42% slower.)
 //   warp 1      allocates 512 TMEM columns (two 128x256 FP32 accumulators)
 //               and one elected thread issues tcgen05.mma (M=128, N=256,
 //               K=16, kind::f16); tcgen05.commit releases ring stages and
 //               publishes finished accumulators.
-//   warps 2-5   epilogue: tcgen05.ld of the accumulator (lane = row),
-//               C[row, col] = C[row, col] - acc in FP32, coalesced per warp.
+//   warps 2-5   epilogue: tcgen05.ld of the accumulator (lane = row), -acc
+//               to shared memory and a TMA reduce-add into C (FP32, in L2);
+//               when C's rows are not 16-byte aligned, C = C - acc with
+//               coalesced loads and stores instead.
 //
 // The accumulator is double buffered so the epilogue of tile i overlaps
 // the MMAs of tile i+1.  Every wait is bounded; a timeout sets the status
@@ -39,7 +41,10 @@ constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int EPI_WARPS = 4;
 constexpr int THREADS = (2 + EPI_WARPS) * 32;
 constexpr uint32_t TMEM_COLS = 2 * BN;
-constexpr size_t SMEM_BYTES = static_cast<size_t>(STAGES) * STAGE_BYTES + 1024 + 256;
+constexpr int EPI_CHUNK = 32;                       // columns per epilogue chunk
+constexpr int EPI_BUF_BYTES = 32 * EPI_CHUNK * 4;   // one warp's 32 rows x 32 columns FP32
+constexpr size_t RED_BYTES = static_cast<size_t>(EPI_WARPS) * 2 * EPI_BUF_BYTES;
+constexpr size_t smem_bytes(bool red) { return static_cast<size_t>(STAGES) * STAGE_BYTES + (red ? RED_BYTES : 0) + 1024 + 256; }
 
 static_assert(TMEM_COLS <= 512, "two accumulators must fit in TMEM");
 
@@ -50,37 +55,32 @@ struct Params {
 	int num_kc;       // K chunks of BK
 	int lrow0, urow0; // first L row / first U row (= C column) in the panel buffers
 	int tiles_m, tiles_n;
+	int crow0, ccol0; // coordinates of C(0,0) in the C tensor map (reduce epilogue)
 };
 
 __device__ unsigned int g_status;
 
-__device__ __forceinline__ void prefetch_c_tile(const Params &p, int tm, int tn, int lane)
+__device__ __forceinline__ void tma_reduce_add_2d(const void *map, const void *smem_src, int x, int y)
 {
-	// 16-byte aligned runs of each column of the tile, 8 columns per lane.
-	const int row0 = tm * BM;
-	const int nrows = min(BM, p.m - row0);
-	for (int cc = lane; cc < BN; cc += 32) {
-		const int col = tn * BN + cc;
-		if (col >= p.n) break;
-		const uintptr_t beg = reinterpret_cast<uintptr_t>(p.c + row0 + static_cast<int64_t>(col) * p.ldc);
-		const uintptr_t end = beg + static_cast<uintptr_t>(nrows) * sizeof(float);
-		const uintptr_t abeg = beg & ~static_cast<uintptr_t>(15);
-		const uintptr_t aend = end & ~static_cast<uintptr_t>(15);
-		if (aend > abeg)
-			asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(abeg), "r"(static_cast<uint32_t>(aend - abeg))
-				: "memory");
-	}
+	asm volatile("cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.bulk_group [%0, {%2, %3}], [%1];"
+		::"l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(smem_src)), "r"(x), "r"(y)
+		: "memory");
 }
 
+// RED: the epilogue writes -acc to shared memory and a TMA reduce-add folds
+// it into C in L2 (C never passes through the SM); otherwise the epilogue
+// loads C, subtracts and stores with plain coalesced accesses.
+template <bool RED>
 __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant__ CUtensorMap lmap,
-	const __grid_constant__ CUtensorMap umap, const Params p)
+	const __grid_constant__ CUtensorMap umap, const __grid_constant__ CUtensorMap cmap, const Params p)
 {
 	extern __shared__ uint8_t smem_raw[];
 	const uint32_t raw_addr = smem_u32(smem_raw);
 	uint8_t *smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
 	uint8_t *sA = smem;
 	uint8_t *sB = smem + STAGES * A_BYTES;
-	uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+	float *sEpi = reinterpret_cast<float *>(smem + STAGES * STAGE_BYTES);   // RED staging
+	uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES + (RED ? RED_BYTES : 0));
 	uint64_t *full = bars;
 	uint64_t *empty = bars + STAGES;
 	uint64_t *accf = bars + 2 * STAGES;
@@ -128,7 +128,6 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 		uint32_t phase = 0;
 		for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
 			const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
-			prefetch_c_tile(p, tm, tn, lane);
 			if (lane == 0) {
 				for (int kc = 0; kc < p.num_kc; ++kc) {
 					if (!mbar_wait(&empty[stage], phase ^ 1u)) { ok = false; break; }
@@ -186,36 +185,63 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 		bool ok = true;
 		int acc = 0;
 		uint32_t acc_phase = 0;
+		int epi_buf = 0;
 		for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
 			const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
 			const bool mine = mbar_wait(&accf[acc], acc_phase);
 			ok = __all_sync(0xffffffffu, mine) != 0;
 			if (!ok) break;
 			tc_fence_after();
-			const int row = tm * BM + q * 32 + lane;
-			const bool rok = row < p.m;
-			float *crow = p.c + row;
 			const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * BN);
+			if (RED) {
+				float *mybuf = sEpi + (warp - 2) * 2 * (EPI_BUF_BYTES / 4);
+				const int gx = p.crow0 + tm * BM + q * 32;   // tensor-map row of this warp's lane 0
 #pragma unroll 1
-			for (int ch = 0; ch < BN / 32; ++ch) {
-				uint32_t r[32];
-				tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(ch * 32), r);
-				tmem_ld_wait();
-				const int col0 = tn * BN + ch * 32;
-				if (rok) {
-					float cv[32];
+				for (int ch = 0; ch < BN / EPI_CHUNK; ++ch) {
+					uint32_t r[32];
+					tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(ch * EPI_CHUNK), r);
+					tmem_ld_wait();
+					float *sb = mybuf + (epi_buf & 1) * (EPI_BUF_BYTES / 4);
+					// the reduce issued two chunks ago read this buffer; let it finish
+					if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+					__syncwarp();
 #pragma unroll
-					for (int j = 0; j < 32; ++j)
-						if (col0 + j < p.n) cv[j] = crow[static_cast<int64_t>(col0 + j) * p.ldc];
+					for (int j = 0; j < 32; ++j) sb[j * 32 + lane] = -__uint_as_float(r[j]);
+					asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+					__syncwarp();
+					if (lane == 0) {
+						tma_reduce_add_2d(&cmap, sb, gx, p.ccol0 + tn * BN + ch * EPI_CHUNK);
+						asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+					}
+					++epi_buf;
+				}
+			} else {
+				const int row = tm * BM + q * 32 + lane;
+				const bool rok = row < p.m;
+				float *crow = p.c + row;
+#pragma unroll 1
+				for (int ch = 0; ch < BN / 32; ++ch) {
+					uint32_t r[32];
+					tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(ch * 32), r);
+					tmem_ld_wait();
+					const int col0 = tn * BN + ch * 32;
+					if (rok) {
+						float cv[32];
 #pragma unroll
-					for (int j = 0; j < 32; ++j)
-						if (col0 + j < p.n) crow[static_cast<int64_t>(col0 + j) * p.ldc] = cv[j] - __uint_as_float(r[j]);
+						for (int j = 0; j < 32; ++j)
+							if (col0 + j < p.n) cv[j] = crow[static_cast<int64_t>(col0 + j) * p.ldc];
+#pragma unroll
+						for (int j = 0; j < 32; ++j)
+							if (col0 + j < p.n) crow[static_cast<int64_t>(col0 + j) * p.ldc] = cv[j] - __uint_as_float(r[j]);
+					}
 				}
 			}
 			tc_fence_before();
 			mbar_arrive(&acce[acc]);
 			if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
 		}
+		// all reduces of this warp complete before the CTA exits
+		if (RED && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 		if (lane == 0 && !ok) atomicOr(&g_status, 1u);
 	}
 
@@ -247,23 +273,29 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 	return fn;
 }
 
-int make_map_f16(void *out, const void *base, uint64_t inner, uint64_t outer, uint64_t ld_elems, uint32_t box_inner,
-	uint32_t box_outer)
+int make_map_2d(void *out, CUtensorMapDataType dt, int esize, const void *base, uint64_t inner, uint64_t outer,
+	uint64_t ld_elems, uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle swz)
 {
 	auto fn = encode_fn();
 	if (!fn) return HPLAI_ECUDA;
-	if ((reinterpret_cast<uintptr_t>(base) & 15u) || ((ld_elems * 2) & 15u)) return HPLAI_EINVAL;
+	if ((reinterpret_cast<uintptr_t>(base) & 15u) || ((ld_elems * esize) & 15u)) return HPLAI_EINVAL;
 	CUtensorMap m;
 	cuuint64_t dims[2] = {inner, outer};
-	cuuint64_t strides[1] = {ld_elems * 2};
+	cuuint64_t strides[1] = {ld_elems * esize};
 	cuuint32_t box[2] = {box_inner, box_outer};
 	cuuint32_t estr[2] = {1, 1};
-	CUresult r = fn(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
-		CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-		CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	CUresult r = fn(&m, dt, 2, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+		CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 	if (r != CUDA_SUCCESS) return HPLAI_EINVAL;
 	std::memcpy(out, &m, sizeof(m));
 	return HPLAI_OK;
+}
+
+int make_map_f16(void *out, const void *base, uint64_t inner, uint64_t outer, uint64_t ld_elems, uint32_t box_inner,
+	uint32_t box_outer)
+{
+	return make_map_2d(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, base, inner, outer, ld_elems, box_inner, box_outer,
+		CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
 int num_sms()
@@ -288,10 +320,22 @@ int schur_make_maps(SchurMaps *m, const uint16_t *lh, int lrows, int64_t ldl, co
 	HPLAI_TRY(make_map_f16(m->umap, uh, static_cast<uint64_t>(k), static_cast<uint64_t>(urows),
 		static_cast<uint64_t>(ldu), BK, BN));
 	m->k = k;
+	m->has_cmap = false;
 	return HPLAI_OK;
 }
 
-int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, cudaStream_t st)
+int schur_set_cmap(SchurMaps *m, const float *c, int rows, int cols, int64_t ldc)
+{
+	m->has_cmap = false;
+	if (!c || rows <= 0 || cols <= 0 || (reinterpret_cast<uintptr_t>(c) & 15u) || (ldc % 4)) return HPLAI_OK;
+	if (make_map_2d(m->cmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c, static_cast<uint64_t>(rows),
+			static_cast<uint64_t>(cols), static_cast<uint64_t>(ldc), 32, EPI_CHUNK, CU_TENSOR_MAP_SWIZZLE_NONE) == HPLAI_OK)
+		m->has_cmap = true;
+	return HPLAI_OK;
+}
+
+int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
+	int ccol0, cudaStream_t st)
 {
 	if (m <= 0 || n <= 0) return HPLAI_OK;
 	Params p;
@@ -304,18 +348,28 @@ int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, floa
 	p.urow0 = urow0;
 	p.tiles_m = (m + BM - 1) / BM;
 	p.tiles_n = (n + BN - 1) / BN;
+	p.crow0 = crow0;
+	p.ccol0 = ccol0;
 	const int total = p.tiles_m * p.tiles_n;
 	const int grid = total < num_sms() ? total : num_sms();
+	// The reduce epilogue needs each warp's first row 16-byte aligned in the map.
+	const bool red = maps.has_cmap && (crow0 % 4 == 0);
 	static bool attr_set = false;
 	if (!attr_set) {
-		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			static_cast<int>(SMEM_BYTES)));
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(smem_bytes(false))));
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(smem_bytes(true))));
 		attr_set = true;
 	}
-	CUtensorMap lm, um;
+	CUtensorMap lm, um, cm;
 	std::memcpy(&lm, maps.lmap, sizeof(lm));
 	std::memcpy(&um, maps.umap, sizeof(um));
-	schur_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(lm, um, p);
+	std::memcpy(&cm, red ? maps.cmap : maps.lmap, sizeof(cm));
+	if (red)
+		schur_kernel<true><<<grid, THREADS, smem_bytes(true), st>>>(lm, um, cm, p);
+	else
+		schur_kernel<false><<<grid, THREADS, smem_bytes(false), st>>>(lm, um, cm, p);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
@@ -343,5 +397,6 @@ extern "C" int hplai_shgemm_minus(int m, int n, int k, const uint16_t *lh, int64
 	if (m == 0 || n == 0) return HPLAI_OK;
 	hplai::SchurMaps maps;
 	HPLAI_TRY(hplai::schur_make_maps(&maps, lh, m, ldlh, uh, n, lduh, k));
-	return hplai::launch_schur(maps, 0, 0, m, n, c, ldc, static_cast<cudaStream_t>(stream));
+	HPLAI_TRY(hplai::schur_set_cmap(&maps, c, m, n, ldc));
+	return hplai::launch_schur(maps, 0, 0, m, n, c, ldc, 0, 0, static_cast<cudaStream_t>(stream));
 }

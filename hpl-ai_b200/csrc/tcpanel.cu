@@ -1,0 +1,523 @@
+// tcpanel.cu -- panel TRSMs of the blocked LU on tensor cores.
+//
+// update_left_panels / update_right_panels (panel_trf.hpp:143-171) solve
+// A_col <- A_col U11^{-1} and A_row <- L11^{-1} A_row with the b x b
+// triangles of the freshly factored diagonal block.  Here the two triangles
+// are inverted once per step (tri_inv_kernel, FP32) and the panels are
+// multiplied by the inverses on tcgen05 in "3xTF32": each FP32 operand x is
+// split into hi = x with the low 13 mantissa bits cleared (exact in TF32)
+// and lo = x - hi (exact in FP32), and
+//     X = A_hi B_hi + A_hi B_lo + A_lo B_hi
+// is accumulated in FP32 in TMEM (the dropped A_lo B_lo and the TF32
+// rounding of the lo parts are ~2^-21 relative), so the panels keep FP32
+// accuracy.  The epilogue writes the FP32 panel back into A and its FP16
+// copy (convert_left/right_panels, panel_trf.hpp:173-233) for the Schur GEMM.
+//
+// Kernels: split_kernel (FP32 panel -> K-major hi/lo copies), tri_inv_kernel
+// (triangular inverse, hi/lo), tf32x3_kernel (persistent, warp-specialised:
+// TMA producer, one MMA-issuing thread, four epilogue warps; bounded waits).
+#include "common.cuh"
+#include "internal.h"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cstring>
+
+namespace hplai {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// hi/lo split
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+
+// Row-major K-major copies P[r*ldp + k] (hi and lo) of an FP32 panel.
+//   TRANS = true : source element (r, k) at src[k*lds + r] (column-major A_col)
+//   TRANS = false: source element (r, k) at src[r*lds + k] (A_row seen by columns)
+// k in [0, kdim), r in [0, rows); columns kdim..ldp-1 are zeroed.
+template <bool TRANS>
+__global__ void __launch_bounds__(256) split_kernel(int rows, int kdim, const float *__restrict__ src, int64_t lds,
+	float *__restrict__ phi, float *__restrict__ plo, int64_t ldp)
+{
+	__shared__ float tile[32][33];
+	const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+	const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
+	if (TRANS) {
+		for (int i = ty; i < 32; i += 8) {
+			const int k = k0 + i, r = r0 + tx;
+			tile[i][tx] = (k < kdim && r < rows) ? src[static_cast<int64_t>(k) * lds + r] : 0.f;
+		}
+		__syncthreads();
+		for (int i = ty; i < 32; i += 8) {
+			const int r = r0 + i, k = k0 + tx;
+			if (r < rows && k < ldp) {
+				const float x = tile[tx][i];
+				const float h = tf32_hi(x);
+				phi[static_cast<int64_t>(r) * ldp + k] = h;
+				plo[static_cast<int64_t>(r) * ldp + k] = x - h;
+			}
+		}
+	} else {
+		for (int i = ty; i < 32; i += 8) {
+			const int r = r0 + i, k = k0 + tx;
+			if (r < rows && k < ldp) {
+				const float x = (k < kdim) ? src[static_cast<int64_t>(r) * lds + k] : 0.f;
+				const float h = tf32_hi(x);
+				phi[static_cast<int64_t>(r) * ldp + k] = h;
+				plo[static_cast<int64_t>(r) * ldp + k] = x - h;
+			}
+		}
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Triangular inverse.  X = T^{-1}, T upper triangular b x b:
+//   TRANS_T = false: T = U11, T[p][j] at t[j*ldt + p], non-unit diagonal
+//   TRANS_T = true : T = L11^T, T[p][j] = L[j][p] at t[p*ldt + j], unit diagonal
+// CTA G computes the 32-column block X[:, 32G:32G+32] by block back
+// substitution X[I,G] = T_II^{-1} (E[I,G] - sum_{J>I} T[I,J] X[J,G]), and
+// writes it column-major (X[row][col] at x*[col*ldx + row]) as hi/lo.
+// ---------------------------------------------------------------------------
+template <bool TRANS_T>
+__global__ void __launch_bounds__(256) tri_inv_kernel(int b, const float *__restrict__ t, int64_t ldt,
+	float *__restrict__ xhi, float *__restrict__ xlo, int64_t ldx)
+{
+	extern __shared__ float sm[];
+	float(*Xs)[33] = reinterpret_cast<float(*)[33]>(sm);       // rows 0..32G+31 of the column block
+	float(*Tb)[33] = reinterpret_cast<float(*)[33]>(sm + static_cast<size_t>(b + 32) * 33);   // 32 x 32 block
+	float(*Sb)[33] = Tb + 32;                                   // 32 x 32 right-hand side
+	const int G = blockIdx.x;
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	auto tval = [&](int p, int j) -> float {
+		if (p >= b || j >= b) return (p == j) ? 1.f : 0.f;       // identity padding
+		if (TRANS_T) return (p == j) ? 1.f : t[static_cast<int64_t>(p) * ldt + j];
+		return t[static_cast<int64_t>(j) * ldt + p];
+	};
+	for (int I = G; I >= 0; --I) {
+		// S = E[I,G] - sum_{J=I+1..G} T[I,J] X[J,G]; thread: column lane, rows warp + 8r
+		float acc[4];
+#pragma unroll
+		for (int r = 0; r < 4; ++r) acc[r] = (I == G && warp + 8 * r == lane) ? 1.f : 0.f;
+		for (int J = I + 1; J <= G; ++J) {
+			__syncthreads();
+			for (int e = tid; e < 1024; e += 256) {
+				const int i = TRANS_T ? (e >> 5) : (e & 31), p = TRANS_T ? (e & 31) : (e >> 5);
+				Tb[i][p] = tval(32 * I + i, 32 * J + p);
+			}
+			__syncthreads();
+#pragma unroll 4
+			for (int p = 0; p < 32; ++p) {
+				const float xv = Xs[32 * J + p][lane];
+#pragma unroll
+				for (int r = 0; r < 4; ++r) acc[r] = fmaf(-Tb[warp + 8 * r][p], xv, acc[r]);
+			}
+		}
+		__syncthreads();
+#pragma unroll
+		for (int r = 0; r < 4; ++r) Sb[warp + 8 * r][lane] = acc[r];
+		for (int e = tid; e < 1024; e += 256) {
+			const int i = TRANS_T ? (e >> 5) : (e & 31), p = TRANS_T ? (e & 31) : (e >> 5);
+			Tb[i][p] = tval(32 * I + i, 32 * I + p);
+		}
+		__syncthreads();
+		// X[I,G] = T_II^{-1} S by back substitution, one column per lane of warp 0.
+		if (warp == 0) {
+			float x[32];
+#pragma unroll
+			for (int i = 31; i >= 0; --i) {
+				float v = Sb[i][lane];
+#pragma unroll
+				for (int p = i + 1; p < 32; ++p) v = fmaf(-Tb[i][p], x[p], v);
+				x[i] = TRANS_T ? v : v / Tb[i][i];
+			}
+#pragma unroll
+			for (int i = 0; i < 32; ++i) Xs[32 * I + i][lane] = x[i];
+		}
+		__syncthreads();
+	}
+	// Write the column block: rows 0..b-1, zero below the diagonal.
+	for (int e = tid; e < 32 * b; e += 256) {
+		const int row = e % b, c = e / b;
+		const int col = 32 * G + c;
+		if (col >= b) continue;
+		const float v = (row <= 32 * G + 31 && row <= col) ? Xs[row][c] : 0.f;
+		const float h = tf32_hi(v);
+		xhi[static_cast<int64_t>(col) * ldx + row] = h;
+		xlo[static_cast<int64_t>(col) * ldx + row] = v - h;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// 3xTF32 GEMM: D (M x N) = A (M x K) B (N x K)^T, K-major hi/lo operands.
+// Output: out32[m*s32m + n*s32n] = D, out16[m*s16m + n*s16n] = half(scale*D).
+// ---------------------------------------------------------------------------
+constexpr int TBM = 128, TBN = 128, TBK = 32;          // TBK FP32 = one 128-byte swizzle row
+constexpr int TSTAGES = 3;
+constexpr int TILE_BYTES = TBM * TBK * 4;              // 16 KB per operand tile (M and N both 128)
+constexpr int TSTAGE_BYTES = 4 * TILE_BYTES;           // A hi/lo, B hi/lo
+constexpr int TEPI_WARPS = 4;
+constexpr int TTHREADS = (2 + TEPI_WARPS) * 32;
+constexpr uint32_t TTMEM_COLS = 2 * TBN;
+constexpr size_t TSMEM_BYTES = static_cast<size_t>(TSTAGES) * TSTAGE_BYTES + 1024 + 256;
+
+struct TParams {
+	int m, n, num_kc, tiles_m, tiles_n;
+	int arow0, brow0;   // first rows of A and B in their maps
+	float *out32;
+	int64_t s32m, s32n;
+	__half *out16;
+	int64_t s16m, s16n;
+	float scale;
+};
+
+__device__ unsigned int g_tstatus;
+
+// kind::tf32 instruction descriptor: FP32 accumulator, A/B TF32 (format 2), K-major.
+__host__ __device__ constexpr uint32_t idesc_tf32(int m, int n)
+{
+	return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
+	       (static_cast<uint32_t>(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+	uint32_t accumulate)
+{
+	asm volatile(
+		"{\n\t.reg .pred p;\n\t"
+		"setp.ne.b32 p, %4, 0;\n\t"
+		"tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+		::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+		: "memory");
+}
+
+__global__ void __launch_bounds__(TTHREADS, 1) tf32x3_kernel(const __grid_constant__ CUtensorMap ahi,
+	const __grid_constant__ CUtensorMap alo, const __grid_constant__ CUtensorMap bhi,
+	const __grid_constant__ CUtensorMap blo, const TParams p)
+{
+	extern __shared__ uint8_t smem_raw[];
+	const uint32_t raw_addr = smem_u32(smem_raw);
+	uint8_t *smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
+	uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TSTAGES * TSTAGE_BYTES);
+	uint64_t *full = bars;
+	uint64_t *empty = bars + TSTAGES;
+	uint64_t *accf = bars + 2 * TSTAGES;
+	uint64_t *acce = accf + 2;
+	uint64_t *drain = acce + 2;
+	uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(drain + 1);
+	int *consumed = reinterpret_cast<int *>(tmem_holder + 1);
+
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < TSTAGES; ++s) {
+			mbar_init(&full[s], 1);
+			mbar_init(&empty[s], 1);
+		}
+		for (int a = 0; a < 2; ++a) {
+			mbar_init(&accf[a], 1);
+			mbar_init(&acce[a], TEPI_WARPS * 32);
+		}
+		mbar_init(drain, 1);
+		*consumed = 0;
+		fence_mbar_init();
+	}
+	if (warp == 1) {
+		tmem_alloc(tmem_holder, TTMEM_COLS);
+		tmem_relinquish();
+	}
+	if (warp == 0 && lane == 0) {
+		tma_prefetch_desc(&ahi);
+		tma_prefetch_desc(&alo);
+		tma_prefetch_desc(&bhi);
+		tma_prefetch_desc(&blo);
+	}
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem_base = *tmem_holder;
+	const int total = p.tiles_m * p.tiles_n;
+	int issued = 0;
+
+	if (warp == 0) {
+		if (lane == 0) {
+			bool ok = true;
+			int stage = 0;
+			uint32_t phase = 0;
+			for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
+				const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+				for (int kc = 0; kc < p.num_kc; ++kc) {
+					if (!mbar_wait(&empty[stage], phase ^ 1u)) { ok = false; break; }
+					mbar_arrive_expect_tx(&full[stage], TSTAGE_BYTES);
+					uint8_t *st = smem + stage * TSTAGE_BYTES;
+					tma_load_2d(st, &ahi, &full[stage], kc * TBK, p.arow0 + tm * TBM);
+					tma_load_2d(st + TILE_BYTES, &alo, &full[stage], kc * TBK, p.arow0 + tm * TBM);
+					tma_load_2d(st + 2 * TILE_BYTES, &bhi, &full[stage], kc * TBK, p.brow0 + tn * TBN);
+					tma_load_2d(st + 3 * TILE_BYTES, &blo, &full[stage], kc * TBK, p.brow0 + tn * TBN);
+					++issued;
+					if (++stage == TSTAGES) { stage = 0; phase ^= 1u; }
+				}
+			}
+			if (!ok) atomicOr(&g_tstatus, 1u);
+		}
+	} else if (warp == 1) {
+		if (lane == 0) {
+			bool ok = true;
+			int stage = 0, acc = 0, used = 0;
+			uint32_t phase = 0, acc_phase = 0;
+			const uint32_t idesc = idesc_tf32(TBM, TBN);
+			for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
+				if (!mbar_wait(&acce[acc], acc_phase ^ 1u)) { ok = false; break; }
+				tc_fence_after();
+				const uint32_t d = tmem_base + static_cast<uint32_t>(acc * TBN);
+				for (int kc = 0; kc < p.num_kc; ++kc) {
+					if (!mbar_wait(&full[stage], phase)) { ok = false; break; }
+					tc_fence_after();
+					const uint32_t st = smem_u32(smem + stage * TSTAGE_BYTES);
+					const uint64_t dah = umma_desc_k_sw128(st), dal = umma_desc_k_sw128(st + TILE_BYTES);
+					const uint64_t dbh = umma_desc_k_sw128(st + 2 * TILE_BYTES), dbl = umma_desc_k_sw128(st + 3 * TILE_BYTES);
+#pragma unroll
+					for (int kk = 0; kk < TBK / 8; ++kk) {
+						// 8 FP32 = 32 bytes = 2 units of 16 B along K inside the swizzle row
+						const uint32_t o = 2u * kk;
+						umma_tf32(d, dah + o, dbh + o, idesc, (kc | kk) != 0 ? 1u : 0u);
+						umma_tf32(d, dah + o, dbl + o, idesc, 1u);
+						umma_tf32(d, dal + o, dbh + o, idesc, 1u);
+					}
+					umma_commit(&empty[stage]);
+					++used;
+					if (++stage == TSTAGES) { stage = 0; phase ^= 1u; }
+				}
+				if (!ok) break;
+				umma_commit(&accf[acc]);
+				if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+			}
+			umma_commit(drain);
+			if (!mbar_wait(drain, 0)) ok = false;
+			*consumed = used;
+			if (!ok) atomicOr(&g_tstatus, 1u);
+		}
+	} else {
+		const int q = warp & 3;
+		bool ok = true;
+		int acc = 0;
+		uint32_t acc_phase = 0;
+		for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
+			const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+			const bool mine = mbar_wait(&accf[acc], acc_phase);
+			ok = __all_sync(0xffffffffu, mine) != 0;
+			if (!ok) break;
+			tc_fence_after();
+			const int row = tm * TBM + q * 32 + lane;
+			const bool rok = row < p.m;
+			const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * TBN);
+#pragma unroll 1
+			for (int ch = 0; ch < TBN / 32; ++ch) {
+				uint32_t r[32];
+				tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(ch * 32), r);
+				tmem_ld_wait();
+				const int col0 = tn * TBN + ch * 32;
+				if (rok) {
+#pragma unroll
+					for (int j = 0; j < 32; ++j) {
+						const int col = col0 + j;
+						if (col < p.n) {
+							const float v = __uint_as_float(r[j]);
+							p.out32[row * p.s32m + col * p.s32n] = v;
+							p.out16[row * p.s16m + col * p.s16n] = __float2half_rn(p.scale * v);
+						}
+					}
+				}
+			}
+			tc_fence_before();
+			mbar_arrive(&acce[acc]);
+			if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+		}
+		if (lane == 0 && !ok) atomicOr(&g_tstatus, 1u);
+	}
+
+	tc_fence_before();
+	__syncthreads();
+	if (warp == 0 && lane == 0) {
+		int left = issued - *consumed;
+		for (int s = 0; left > 0 && s < TSTAGES; ++s, --left)
+			(void)mbar_wait(&full[(*consumed + s) % TSTAGES], static_cast<uint32_t>(((*consumed + s) / TSTAGES) & 1));
+	}
+	if (warp == 1) {
+		tc_fence_after();
+		tmem_dealloc(tmem_base, TTMEM_COLS);
+	}
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn_tc()
+{
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	if (!fn) {
+		void *ptr = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+			q == cudaDriverEntryPointSuccess)
+			fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+	}
+	return fn;
+}
+
+// FP32 K-major operand map: rows x kdim, row pitch ldp floats, box TBK x 128, 128B swizzle.
+int make_f32_kmajor(void *out, const float *base, int rows, int kdim, int64_t ldp)
+{
+	auto fn = encode_fn_tc();
+	if (!fn) return HPLAI_ECUDA;
+	if ((reinterpret_cast<uintptr_t>(base) & 15u) || ((ldp * 4) & 15u)) return HPLAI_EINVAL;
+	CUtensorMap m;
+	cuuint64_t dims[2] = {static_cast<cuuint64_t>(kdim), static_cast<cuuint64_t>(rows)};
+	cuuint64_t strides[1] = {static_cast<cuuint64_t>(ldp * 4)};
+	cuuint32_t box[2] = {TBK, 128};
+	cuuint32_t estr[2] = {1, 1};
+	CUresult r = fn(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides, box, estr,
+		CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+		CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	if (r != CUDA_SUCCESS) return HPLAI_EINVAL;
+	std::memcpy(out, &m, sizeof(m));
+	return HPLAI_OK;
+}
+
+int sm_count()
+{
+	int dev = 0, sms = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+	if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) return 148;
+	return sms;
+}
+
+int launch_tf32x3(const unsigned char *m_ahi, const unsigned char *m_alo, const unsigned char *m_bhi,
+	const unsigned char *m_blo, int arow0, int brow0, int M, int N, int K, float *out32, int64_t s32m, int64_t s32n,
+	__half *out16, int64_t s16m, int64_t s16n, float scale, int max_ctas, cudaStream_t st)
+{
+	if (M <= 0 || N <= 0) return HPLAI_OK;
+	TParams p;
+	p.m = M;
+	p.n = N;
+	p.num_kc = (K + TBK - 1) / TBK;
+	p.tiles_m = (M + TBM - 1) / TBM;
+	p.tiles_n = (N + TBN - 1) / TBN;
+	p.arow0 = arow0;
+	p.brow0 = brow0;
+	p.out32 = out32;
+	p.s32m = s32m;
+	p.s32n = s32n;
+	p.out16 = out16;
+	p.s16m = s16m;
+	p.s16n = s16n;
+	p.scale = scale;
+	static bool attr = false;
+	if (!attr) {
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(TSMEM_BYTES)));
+		attr = true;
+	}
+	const int total = p.tiles_m * p.tiles_n;
+	int grid = max_ctas > 0 ? max_ctas : sm_count();
+	if (grid > total) grid = total;
+	CUtensorMap a0, a1, b0, b1;
+	std::memcpy(&a0, m_ahi, sizeof(a0));
+	std::memcpy(&a1, m_alo, sizeof(a1));
+	std::memcpy(&b0, m_bhi, sizeof(b0));
+	std::memcpy(&b1, m_blo, sizeof(b1));
+	tf32x3_kernel<<<grid, TTHREADS, TSMEM_BYTES, st>>>(a0, a1, b0, b1, p);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+} // namespace
+
+static_assert(sizeof(CUtensorMap) <= 128, "tensor map storage");
+
+int tc_panels_make(TcPanels *t, int n, int b, float *phi, float *plo, int64_t ldp, float *uhi, float *ulo,
+	float *lhi, float *llo)
+{
+	if (!t || n <= 0 || b <= 0 || ldp < b || (ldp % 32)) return HPLAI_EINVAL;
+	t->n = n;
+	t->b = b;
+	t->ldp = ldp;
+	t->phi = phi;
+	t->plo = plo;
+	t->uhi = uhi;
+	t->ulo = ulo;
+	t->lhi = lhi;
+	t->llo = llo;
+	HPLAI_TRY(make_f32_kmajor(t->m_phi, phi, n, b, ldp));
+	HPLAI_TRY(make_f32_kmajor(t->m_plo, plo, n, b, ldp));
+	HPLAI_TRY(make_f32_kmajor(t->m_uhi, uhi, b, b, ldp));
+	HPLAI_TRY(make_f32_kmajor(t->m_ulo, ulo, b, b, ldp));
+	HPLAI_TRY(make_f32_kmajor(t->m_lhi, lhi, b, b, ldp));
+	HPLAI_TRY(make_f32_kmajor(t->m_llo, llo, b, b, ldp));
+	return HPLAI_OK;
+}
+
+int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStream_t st)
+{
+	const int b = t.b;
+	const int groups = (b + 31) / 32;
+	const size_t smem = (static_cast<size_t>(b + 32) * 33 + 2 * 32 * 33) * sizeof(float);
+	static bool attr = false;
+	if (!attr) {
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(tri_inv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>((1024 + 32) * 33 * 4 + 2 * 32 * 33 * 4)));
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(tri_inv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>((1024 + 32) * 33 * 4 + 2 * 32 * 33 * 4)));
+		attr = true;
+	}
+	// U11^{-1} column-major = the B operand of the L-panel product (row n = column n of U^{-1}).
+	tri_inv_kernel<false><<<groups, 256, smem, st>>>(b, lu, lda, t.uhi, t.ulo, t.ldp);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	// (L11^T)^{-1} column-major = L11^{-1} row-major = the A operand of the U-panel product.
+	tri_inv_kernel<true><<<groups, 256, smem, st>>>(b, lu, lda, t.lhi, t.llo, t.ldp);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+int launch_lpanel_tc(const TcPanels &t, int rem, float *acol, int64_t lda, uint16_t *lh, int64_t ldh, float scale,
+	int max_ctas, cudaStream_t st)
+{
+	if (rem <= 0) return HPLAI_OK;
+	const int b = t.b;
+	dim3 g((rem + 31) / 32, static_cast<unsigned>(t.ldp / 32));
+	split_kernel<true><<<g, 256, 0, st>>>(rem, b, acol, lda, t.phi, t.plo, t.ldp);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	// X (rem x b) = A_col U^{-1}: out32 column-major in A, out16 row-major (Lh row = panel row)
+	return launch_tf32x3(t.m_phi, t.m_plo, t.m_uhi, t.m_ulo, 0, 0, rem, b, b, acol, 1, lda,
+		reinterpret_cast<__half *>(lh), ldh, 1, scale, max_ctas, st);
+}
+
+int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint16_t *uh, int64_t ldh, float scale,
+	int max_ctas, cudaStream_t st)
+{
+	if (rem <= 0) return HPLAI_OK;
+	const int b = t.b;
+	dim3 g((rem + 31) / 32, static_cast<unsigned>(t.ldp / 32));
+	// B operand row j = column j of A_row (b contiguous floats, stride lda)
+	split_kernel<false><<<g, 256, 0, st>>>(rem, b, arow, lda, t.phi, t.plo, t.ldp);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	// Y (b x rem) = L^{-1} A_row: out32 column-major in A, out16 with column j of U as row j of Uh
+	return launch_tf32x3(t.m_lhi, t.m_llo, t.m_phi, t.m_plo, 0, 0, b, rem, b, arow, 1, lda,
+		reinterpret_cast<__half *>(uh), 1, ldh, scale, max_ctas, st);
+}
+
+int tc_status()
+{
+	unsigned int v = 0;
+	if (cudaMemcpyFromSymbol(&v, g_tstatus, sizeof(v)) != cudaSuccess) return HPLAI_ECUDA;
+	return v ? HPLAI_ETIMEOUT : HPLAI_OK;
+}
+
+void tc_status_reset()
+{
+	unsigned int z = 0;
+	(void)cudaMemcpyToSymbol(g_tstatus, &z, sizeof(z));
+}
+
+} // namespace hplai

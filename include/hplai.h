@@ -77,6 +77,12 @@ typedef enum hplai_phase {
 	HPLAI_PH_COUNT = 7
 } hplai_phase;
 
+/* hplai_create flags. */
+/* Panel TRSMs on CUDA cores in netlib strsm order -- bit-exact with the
+ * reference's substitution -- instead of the default tensor-core path
+ * (triangular inverses of the diagonal block applied in 3xTF32). */
+#define HPLAI_FLAG_SIMT_PANELS 1u
+
 typedef struct hplai_ctx hplai_ctx;
 
 /* ---------------------------------------------------------------------- */
@@ -93,8 +99,8 @@ unsigned long long hplai_launch_count(void);
 
 /* build_panels (panel.hpp:135-268) + the driver's vector allocations
  * (main.cpp:196-213).  Requires n % b == 0 and 16 <= b <= 1024.  Allocates
- * every device buffer of the solve on the current CUDA device.  `flags` is
- * reserved (pass 0). */
+ * every device buffer of the solve on the current CUDA device.  `flags` is a
+ * combination of HPLAI_FLAG_* (0 for the defaults). */
 int hplai_create(hplai_ctx **ctx, int n, int b, int precision, unsigned flags);
 int hplai_destroy(hplai_ctx *ctx);
 

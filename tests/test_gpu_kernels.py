@@ -142,10 +142,11 @@ def test_trsm_left_lower_bit_exact(hplai, oracle, torch_cuda, b, nc):
 
 
 @pytest.mark.parametrize("m,n,k", [(1140, 1140, 60), (1000, 777, 100), (128, 256, 64), (4096, 4096, 512),
-                                   (300, 5000, 1024), (2500, 129, 16)])
+                                   (300, 5000, 1024), (2500, 129, 16), (1001, 777, 60), (333, 1200, 200)])
 def test_shgemm_minus_vs_torch_fp32(hplai, oracle, torch_cuda, m, n, k):
     """C - L*U on tcgen05 vs a PyTorch FP32 reference of the same op on the
-    same FP16 inputs.  Tolerance per element: 2^-19 * sum_k |l||u| + 2^-22 |C|.
+    same FP16 inputs (m % 4 != 0 exercises the plain epilogue, the others the
+    TMA reduce-add epilogue).  Tolerance per element: 2^-19 * sum_k |l||u| + 2^-22 |C|.
     Both sides accumulate in FP32 but in different orders, and the tensor
     core's FP32 accumulation is not a sequence of IEEE round-to-nearest adds;
     measured on B200 the worst element sits near 2^-20.7 * sum|l||u|."""

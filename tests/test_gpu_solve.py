@@ -36,19 +36,66 @@ def test_c1_solve_matches_reference_and_oracle(hplai, oracle, torch_cuda):
     assert norma == 2 * oracle.diag(n).max() and normb == np.abs(oracle.rhs(n)).max()
 
 
-def test_c1_factors_close_to_oracle(hplai, oracle, torch_cuda):
-    """LU factors: the first panel step is bit-exact, the rest differs only by
-    the Schur update's FP32 summation order."""
-    n, b = 1200, 60
-    with hplai.Solver(n, b) as s:
+@pytest.mark.parametrize("flags", [0, 1])
+def test_block_size_not_multiple_of_four(hplai, oracle, torch_cuda, flags):
+    """b = 50 (as in the reference's sweep, tests/test.py) takes the plain
+    Schur epilogue; the solve still converges to the oracle's x."""
+    n, b = 1200, 50
+    with hplai.Solver(n, b, flags=flags) as s:
         s.generate(42)
         s.factor()
-        lu = s.lu()
-    ref = oracle.lu(oracle.matrix(n), b)
-    assert np.array_equal(lu[:, :b].view(np.uint32), ref[:, :b].view(np.uint32))
-    assert np.array_equal(lu[:b, :].view(np.uint32), ref[:b, :].view(np.uint32))
-    rel = np.abs(lu.astype(np.float64) - ref) / (np.abs(ref) + 1e-3 * np.abs(ref).max())
-    assert rel.max() < 1e-3
+        r = s.iterative_refinement(50)
+        x = s.x()
+    assert r.status == hplai.HPLAI_OK and 0 <= r.hpl_harness < 16
+    rc, xo, _, _, _ = oracle.solve(n, b, q=1)
+    assert rc == 0 and np.abs(x - xo).max() <= 1e-12 * np.abs(xo).max()
+
+
+def _first_panels(hplai, n, b, flags):
+    with hplai.Solver(n, b, flags=flags) as s:
+        s.generate(42)
+        s.factor()
+        return s.lu()
+
+
+@pytest.mark.parametrize("n,b", [(1200, 60), (4096, 512), (3072, 1024)])
+def test_simt_panels_bit_exact_first_step(hplai, oracle, torch_cuda, n, b):
+    """With HPLAI_FLAG_SIMT_PANELS the first step's diagonal block and both
+    panels (final after step 0) equal the oracle's netlib-order TRSMs bit for
+    bit; the rest differs only by the Schur update's summation order."""
+    lu = _first_panels(hplai, n, b, hplai.FLAG_SIMT_PANELS)
+    a = oracle.matrix(n)
+    f = a[:b, :b].copy(order="F")
+    d = oracle.getrf_nopiv(f)
+    lcol = oracle.trsm_right_upper(np.triu(d), a[b:, :b])
+    urow = oracle.trsm_left_lower_unit(np.tril(d, -1) + np.eye(b, dtype=np.float32), a[:b, b:])
+    assert np.array_equal(lu[:b, :b].view(np.uint32), d.view(np.uint32))
+    assert np.array_equal(lu[b:, :b].view(np.uint32), lcol.view(np.uint32))
+    assert np.array_equal(lu[:b, b:].view(np.uint32), urow.view(np.uint32))
+    if n <= 1200:
+        ref = oracle.lu(a, b)
+        rel = np.abs(lu.astype(np.float64) - ref) / (np.abs(ref) + 1e-3 * np.abs(ref).max())
+        assert rel.max() < 1e-3
+
+
+@pytest.mark.parametrize("n,b", [(1200, 60), (4096, 512), (3072, 1024)])
+def test_tensor_core_panels_fp32_accurate(hplai, oracle, torch_cuda, n, b):
+    """Default path: the panels come from the diagonal block's triangular
+    inverses applied in 3xTF32 on tcgen05.  Against the FP64 products of the
+    same (bit-exact) diagonal factors, every element is within
+    2^-18 * (|A| |T^-1|) -- FP32-level, far below the FP16 of the Schur update."""
+    lu = _first_panels(hplai, n, b, 0)
+    a = oracle.matrix(n).astype(np.float64)
+    d = oracle.getrf_nopiv(a[:b, :b].astype(np.float32)).astype(np.float64)
+    assert np.array_equal(lu[:b, :b], d.astype(np.float32))
+    uinv = np.linalg.inv(np.triu(d))
+    linv = np.linalg.inv(np.tril(d, -1) + np.eye(b))
+    lcol = a[b:, :b] @ uinv
+    urow = linv @ a[:b, b:]
+    bl = np.abs(a[b:, :b]) @ np.abs(uinv) * 2.0 ** -18
+    bu = np.abs(linv) @ np.abs(a[:b, b:]) * 2.0 ** -18
+    assert np.all(np.abs(lu[b:, :b] - lcol) <= bl + 1e-30)
+    assert np.all(np.abs(lu[:b, b:] - urow) <= bu + 1e-30)
 
 
 @pytest.mark.parametrize("n,b", [(2048, 64), (3000, 100), (8192, 256), (16384, 512)])
