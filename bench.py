@@ -168,15 +168,18 @@ def run_reference(args):
 
 def schur_algorithmic(n, b):
     """Flops and bytes of all Schur launches of one factorisation.
-    Per launch k: C is (n-(k+1)b)^2 FP32 read and written (8 B/elem), the
-    FP16 L and U panels are read once (2*rem*b*2 B), flops 2*rem^2*b."""
+    Step k updates C = (n-(k+1)b)^2 FP32 elements (read and written, 8 B
+    each), reads the FP16 L and U panels (2*rem*b*2 B) and does 2*rem^2*b
+    flops, in three launches (the next panel's block column and block row,
+    then the rest of the trailing matrix; the last step has no rest)."""
     flops = byts = 0.0
     launches = 0
-    for k in range(n // b - 1):
+    nb = n // b
+    for k in range(nb - 1):
         rem = n - (k + 1) * b
         flops += 2.0 * rem * rem * b
         byts += 8.0 * rem * rem + 4.0 * rem * b
-        launches += 1
+        launches += 3 if k < nb - 2 else 2   # next block column, next block row, rest
     return flops, byts, launches
 
 

@@ -52,8 +52,11 @@ struct hplai_ctx {
 	unsigned flags = 0;
 	int64_t lda = 0, ldh = 0;
 	float *A = nullptr;
-	uint16_t *Lh = nullptr, *Uh = nullptr;
-	SchurMaps maps;
+	// FP16 panel copies, double buffered: the panels of step k+1 are formed
+	// on the side stream while the main stream's update of step k still
+	// reads those of step k (the reference's nbuf = 2 rotating buffers).
+	uint16_t *Lh[2] = {nullptr, nullptr}, *Uh[2] = {nullptr, nullptr};
+	SchurMaps maps[2];
 	TcPanels tc;
 	float *tcbuf = nullptr;   // phi, plo (n x ldp) and the four b x ldp inverse buffers
 	double *rhs = nullptr, *d = nullptr, *x = nullptr, *r = nullptr, *scal = nullptr;
@@ -61,7 +64,9 @@ struct hplai_ctx {
 	size_t gemv_bytes = 0;
 	void *trsv_work = nullptr;
 	size_t trsv_bytes = 0;
-	cudaStream_t st = nullptr;
+	cudaStream_t st = nullptr;    // main stream: Schur updates, refinement, everything else
+	cudaStream_t st2 = nullptr;   // side stream (high priority): diagonal block + panels
+	cudaEvent_t ev_panel = nullptr, ev_next = nullptr;
 	uint64_t seed = 0;
 	bool have_inputs = false, factored = false;
 	double norma = 0.0, normb = 0.0;
@@ -75,8 +80,10 @@ int ctx_free(hplai_ctx *c)
 {
 	if (!c) return HPLAI_OK;
 	cudaFree(c->A);
-	cudaFree(c->Lh);
-	cudaFree(c->Uh);
+	for (int i = 0; i < 2; ++i) {
+		cudaFree(c->Lh[i]);
+		cudaFree(c->Uh[i]);
+	}
 	cudaFree(c->tcbuf);
 	cudaFree(c->rhs);
 	cudaFree(c->d);
@@ -85,7 +92,10 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->scal);
 	cudaFree(c->gemv_work);
 	cudaFree(c->trsv_work);
+	if (c->ev_panel) cudaEventDestroy(c->ev_panel);
+	if (c->ev_next) cudaEventDestroy(c->ev_next);
 	if (c->st) cudaStreamDestroy(c->st);
+	if (c->st2) cudaStreamDestroy(c->st2);
 	delete c;
 	return HPLAI_OK;
 }
@@ -189,10 +199,26 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	// power-of-two stride (the reference's calc_lda_c, panel.hpp:10-18, for HBM).
 	c->lda = round_up(n, 64) + 64;
 	c->ldh = round_up(b, 64);
-	HPLAI_CUDA_TRY(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+	{
+		int lo = 0, hi = 0;
+		const cudaError_t e[5] = {cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking),
+			cudaDeviceGetStreamPriorityRange(&lo, &hi),
+			cudaStreamCreateWithPriority(&c->st2, cudaStreamNonBlocking, hi),
+			cudaEventCreateWithFlags(&c->ev_panel, cudaEventDisableTiming),
+			cudaEventCreateWithFlags(&c->ev_next, cudaEventDisableTiming)};
+		for (cudaError_t ei : e) {
+			if (ei != cudaSuccess) {
+				set_last_cuda_error(ei, "stream/event creation", __FILE__, __LINE__);
+				ctx_free(c);
+				return HPLAI_ECUDA;
+			}
+		}
+	}
 	CTX_ALLOC(c->A, sizeof(float) * static_cast<size_t>(c->lda) * n);
-	CTX_ALLOC(c->Lh, sizeof(uint16_t) * static_cast<size_t>(c->ldh) * n);
-	CTX_ALLOC(c->Uh, sizeof(uint16_t) * static_cast<size_t>(c->ldh) * n);
+	for (int i = 0; i < 2; ++i) {
+		CTX_ALLOC(c->Lh[i], sizeof(uint16_t) * static_cast<size_t>(c->ldh) * n);
+		CTX_ALLOC(c->Uh[i], sizeof(uint16_t) * static_cast<size_t>(c->ldh) * n);
+	}
 	const int64_t ldp = round_up(b, 32);
 	const size_t tc_elems = static_cast<size_t>(ldp) * (2 * static_cast<size_t>(n) + 4 * static_cast<size_t>(b));
 	CTX_ALLOC(c->tcbuf, sizeof(float) * tc_elems);
@@ -209,8 +235,11 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		ctx_free(c);
 		return HPLAI_ECUDA;
 	}
-	int s = schur_make_maps(&c->maps, c->Lh, n, c->ldh, c->Uh, n, c->ldh, b);
-	if (s == HPLAI_OK) s = schur_set_cmap(&c->maps, c->A, n, n, c->lda);
+	int s = HPLAI_OK;
+	for (int i = 0; i < 2 && s == HPLAI_OK; ++i) {
+		s = schur_make_maps(&c->maps[i], c->Lh[i], n, c->ldh, c->Uh[i], n, c->ldh, b);
+		if (s == HPLAI_OK) s = schur_set_cmap(&c->maps[i], c->A, n, n, c->lda);
+	}
 	if (s == HPLAI_OK) {
 		float *base = c->tcbuf;
 		const size_t pn = static_cast<size_t>(ldp) * n, pb = static_cast<size_t>(ldp) * b;
@@ -259,51 +288,104 @@ extern "C" int hplai_upload(hplai_ctx *c, const float *a, int64_t lda, const dou
 	return HPLAI_OK;
 }
 
+namespace {
+
+// Factor the diagonal block of step k and form its two panels with their
+// FP16 copies in buffer `buf` (getrf_nopiv + update_left/right_panels +
+// convert_left/right_panels, panel_trf.hpp:143-233).
+int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStream_t st, PhaseEvents &pe)
+{
+	const int n = c->n, b = c->b;
+	const int64_t lda = c->lda, ldh = c->ldh;
+	const int64_t kb = static_cast<int64_t>(k) * b;
+	float *diag = c->A + kb + kb * lda;
+	HPLAI_TRY(pe.record(st, HPLAI_PH_DIAG_LU));
+	HPLAI_TRY(launch_getrf(b, diag, lda, st));
+	HPLAI_TRY(pe.end(st));
+	if (k == c->nb - 1) return HPLAI_OK;
+	const int rem = n - static_cast<int>(kb) - b;
+	HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_L));
+	if (simt) {
+		HPLAI_TRY(launch_trsm_right_upper(rem, b, diag, lda, diag + b, lda, c->Lh[buf] + (kb + b) * ldh, ldh, 1.0f, st));
+	} else {
+		HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st));
+		HPLAI_TRY(launch_lpanel_tc(c->tc, rem, diag + b, lda, c->Lh[buf] + (kb + b) * ldh, ldh, 1.0f, side_ctas, st));
+	}
+	HPLAI_TRY(pe.end(st));
+	HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_R));
+	if (simt) {
+		HPLAI_TRY(launch_trsm_left_lower(b, rem, diag, lda, diag + static_cast<int64_t>(b) * lda, lda,
+			c->Uh[buf] + (kb + b) * ldh, ldh, 1.0f, st));
+	} else {
+		HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, c->Uh[buf] + (kb + b) * ldh,
+			ldh, 1.0f, side_ctas, st));
+	}
+	HPLAI_TRY(pe.end(st));
+	return HPLAI_OK;
+}
+
+// C -= L_k U_k on the rectangle of rows [r0, r1) and columns [c0, c1).
+int schur_region(hplai_ctx *c, int buf, int r0, int r1, int c0, int c1, int max_ctas, cudaStream_t st,
+	PhaseEvents &pe)
+{
+	if (r1 <= r0 || c1 <= c0) return HPLAI_OK;
+	HPLAI_TRY(pe.record(st, HPLAI_PH_GEMM_UPDATE));
+	HPLAI_TRY(launch_schur(c->maps[buf], r0, c0, r1 - r0, c1 - c0, c->A + r0 + static_cast<int64_t>(c0) * c->lda,
+		c->lda, r0, c0, max_ctas, st));
+	HPLAI_TRY(pe.end(st));
+	return HPLAI_OK;
+}
+
+} // namespace
+
 extern "C" int hplai_factor(hplai_ctx *c)
 {
 	if (!c) return HPLAI_EINVAL;
 	if (!c->have_inputs) return HPLAI_ESTATE;
 	const int n = c->n, b = c->b, nb = c->nb;
-	const int64_t lda = c->lda, ldh = c->ldh;
-	cudaStream_t st = c->st;
 	schur_status_reset();
 	tc_status_reset();
 	const bool simt = (c->flags & HPLAI_FLAG_SIMT_PANELS) != 0;
+	const bool serial = (c->flags & HPLAI_FLAG_LOOKAHEAD) == 0;
 	for (double &v : c->phase_ms) v = 0.0;
 	PhaseEvents pe;
-	// Right-looking blocked LU without pivoting, one panel per step
-	// (panel_lu, panel_trf.hpp:329-432, with GemmControl's pieces fused
-	// into one trailing update per step).
-	for (int k = 0; k < nb; ++k) {
-		const int64_t kb = static_cast<int64_t>(k) * b;
-		float *diag = c->A + kb + kb * lda;
-		HPLAI_TRY(pe.record(st, HPLAI_PH_DIAG_LU));
-		HPLAI_TRY(launch_getrf(b, diag, lda, st));
-		HPLAI_TRY(pe.end(st));
-		if (k == nb - 1) break;
-		const int rem = n - static_cast<int>(kb) - b;
-		HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_L));
-		if (simt) {
-			HPLAI_TRY(launch_trsm_right_upper(rem, b, diag, lda, diag + b, lda, c->Lh + (kb + b) * ldh, ldh, 1.0f, st));
-		} else {
-			HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st));
-			HPLAI_TRY(launch_lpanel_tc(c->tc, rem, diag + b, lda, c->Lh + (kb + b) * ldh, ldh, 1.0f, 0, st));
-		}
-		HPLAI_TRY(pe.end(st));
-		HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_R));
-		if (simt) {
-			HPLAI_TRY(launch_trsm_left_lower(b, rem, diag, lda, diag + static_cast<int64_t>(b) * lda, lda,
-				c->Uh + (kb + b) * ldh, ldh, 1.0f, st));
-		} else {
-			HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, c->Uh + (kb + b) * ldh,
-				ldh, 1.0f, 0, st));
-		}
-		HPLAI_TRY(pe.end(st));
-		HPLAI_TRY(pe.record(st, HPLAI_PH_GEMM_UPDATE));
-		HPLAI_TRY(launch_schur(c->maps, static_cast<int>(kb) + b, static_cast<int>(kb) + b, rem, rem,
-			diag + b + static_cast<int64_t>(b) * lda, lda, static_cast<int>(kb) + b, static_cast<int>(kb) + b, st));
-		HPLAI_TRY(pe.end(st));
+	// Right-looking blocked LU without pivoting with one-step look-ahead
+	// (panel_lu_async / RDMAPanelLU::run, panel_trf.hpp:434-858).  The update
+	// of step k is split into the next panel's block column and block row
+	// (first) and the rest of the trailing matrix (after).  With
+	// HPLAI_FLAG_LOOKAHEAD step k+1's diagonal block and panels are formed on
+	// the side stream as soon as the first part is done, overlapping the
+	// second, which then leaves kSideSms SMs to the side stream; otherwise
+	// everything runs in the same order on one stream.
+	constexpr int kSideSms = 20;
+	cudaStream_t st = c->st, sd = serial ? c->st : c->st2;
+	const int side_ctas = serial ? 0 : kSideSms;
+	int sms = 148;
+	{
+		int dev = 0;
+		if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	}
+	const int main_ctas = (serial || sms <= 2 * kSideSms) ? 0 : sms - kSideSms;
+	// the side stream starts from the generated matrix
+	HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));
+	HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_next, 0));
+	HPLAI_TRY(panel_step(c, 0, 0, simt, side_ctas, sd, pe));
+	for (int k = 0; k + 1 < nb; ++k) {
+		const int buf = k & 1;
+		const int r1 = (k + 1) * b, r2 = (k + 2) * b;
+		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_panel, sd));
+		HPLAI_CUDA_TRY(cudaStreamWaitEvent(st, c->ev_panel, 0));
+		// the next panel's block column (rows r1..n) and block row (columns r2..n)
+		HPLAI_TRY(schur_region(c, buf, r1, n, r1, r2, 0, st, pe));
+		HPLAI_TRY(schur_region(c, buf, r1, r2, r2, n, 0, st, pe));
+		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));
+		HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_next, 0));
+		HPLAI_TRY(panel_step(c, k + 1, buf ^ 1, simt, side_ctas, sd, pe));
+		// the rest of the trailing matrix
+		HPLAI_TRY(schur_region(c, buf, r2, n, r2, n, main_ctas, st, pe));
+	}
+	HPLAI_CUDA_TRY(cudaEventRecord(c->ev_panel, sd));
+	HPLAI_CUDA_TRY(cudaStreamWaitEvent(st, c->ev_panel, 0));
 	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
 	pe.collect(c->phase_ms);
 	HPLAI_TRY(schur_status());

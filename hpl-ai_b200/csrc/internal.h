@@ -32,21 +32,26 @@ int launch_trsm_left_lower(int b, int ncols, const float *l, int64_t ldl, float 
 struct SchurMaps {
 	alignas(64) unsigned char lmap[128];
 	alignas(64) unsigned char umap[128];
-	alignas(64) unsigned char cmap[128];   // FP32 C (the trailing matrix), for the reduce epilogue
 	int k;         // inner dimension (panel width)
-	bool has_cmap;
+	// FP32 matrix holding C, for the TMA reduce-add epilogue (a map clipped to
+	// each launch's region is encoded per launch).
+	float *cbase = nullptr;
+	int64_t cld = 0;
+	bool has_cmap = false;
 };
 // L: lrows x k FP16, row-major with ldl; U: urows x k FP16 (row j = column j
 // of U), ldu.  Rows beyond lrows/urows read as zero.
 int schur_make_maps(SchurMaps *m, const uint16_t *lh, int lrows, int64_t ldl, const uint16_t *uh, int urows,
 	int64_t ldu, int k);
-// FP32 map over C (rows x cols, ldc) used by the TMA reduce-add epilogue; left
-// unset (plain epilogue) when c or ldc is not 16-byte aligned.
+// Matrix holding C for the TMA reduce-add epilogue; left unset (plain
+// epilogue) when c or ldc is not 16-byte aligned.
 int schur_set_cmap(SchurMaps *m, const float *c, int rows, int cols, int64_t ldc);
 // C (m x n, ldc) -= L[lrow0 : lrow0+m, 0:k] * U[urow0 : urow0+n, 0:k]^T.  C(0,0)
-// sits at (crow0, ccol0) of the C map.
+// sits at (crow0, ccol0) of the matrix given to schur_set_cmap.  At most
+// max_ctas persistent CTAs (0 = one per SM), so that concurrent work on
+// another stream keeps some SMs.
 int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
-	int ccol0, cudaStream_t st);
+	int ccol0, int max_ctas, cudaStream_t st);
 int schur_status();          // HPLAI_ETIMEOUT if a device wait ran out since the last reset
 void schur_status_reset();
 

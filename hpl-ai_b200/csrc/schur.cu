@@ -328,14 +328,14 @@ int schur_set_cmap(SchurMaps *m, const float *c, int rows, int cols, int64_t ldc
 {
 	m->has_cmap = false;
 	if (!c || rows <= 0 || cols <= 0 || (reinterpret_cast<uintptr_t>(c) & 15u) || (ldc % 4)) return HPLAI_OK;
-	if (make_map_2d(m->cmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c, static_cast<uint64_t>(rows),
-			static_cast<uint64_t>(cols), static_cast<uint64_t>(ldc), 32, EPI_CHUNK, CU_TENSOR_MAP_SWIZZLE_NONE) == HPLAI_OK)
-		m->has_cmap = true;
+	m->cbase = const_cast<float *>(c);
+	m->cld = ldc;
+	m->has_cmap = true;
 	return HPLAI_OK;
 }
 
 int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
-	int ccol0, cudaStream_t st)
+	int ccol0, int max_ctas, cudaStream_t st)
 {
 	if (m <= 0 || n <= 0) return HPLAI_OK;
 	Params p;
@@ -351,9 +351,18 @@ int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, floa
 	p.crow0 = crow0;
 	p.ccol0 = ccol0;
 	const int total = p.tiles_m * p.tiles_n;
-	const int grid = total < num_sms() ? total : num_sms();
+	int grid = (max_ctas > 0 && max_ctas < num_sms()) ? max_ctas : num_sms();
+	if (grid > total) grid = total;
 	// The reduce epilogue needs each warp's first row 16-byte aligned in the map.
-	const bool red = maps.has_cmap && (crow0 % 4 == 0);
+	// Its map ends at the region's last row and column: a TMA reduce clips
+	// only at the tensor's extent, and a tile reaching past a region that
+	// does not end at the matrix edge must not touch the neighbouring blocks.
+	bool red = maps.has_cmap && (crow0 % 4 == 0);
+	alignas(64) unsigned char cmap[128];
+	if (red && make_map_2d(cmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, maps.cbase, static_cast<uint64_t>(crow0 + m),
+			static_cast<uint64_t>(ccol0 + n), static_cast<uint64_t>(maps.cld), 32, EPI_CHUNK,
+			CU_TENSOR_MAP_SWIZZLE_NONE) != HPLAI_OK)
+		red = false;
 	static bool attr_set = false;
 	if (!attr_set) {
 		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -365,7 +374,7 @@ int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, floa
 	CUtensorMap lm, um, cm;
 	std::memcpy(&lm, maps.lmap, sizeof(lm));
 	std::memcpy(&um, maps.umap, sizeof(um));
-	std::memcpy(&cm, red ? maps.cmap : maps.lmap, sizeof(cm));
+	std::memcpy(&cm, red ? cmap : maps.lmap, sizeof(cm));
 	if (red)
 		schur_kernel<true><<<grid, THREADS, smem_bytes(true), st>>>(lm, um, cm, p);
 	else
@@ -398,5 +407,5 @@ extern "C" int hplai_shgemm_minus(int m, int n, int k, const uint16_t *lh, int64
 	hplai::SchurMaps maps;
 	HPLAI_TRY(hplai::schur_make_maps(&maps, lh, m, ldlh, uh, n, lduh, k));
 	HPLAI_TRY(hplai::schur_set_cmap(&maps, c, m, n, ldc));
-	return hplai::launch_schur(maps, 0, 0, m, n, c, ldc, 0, 0, static_cast<cudaStream_t>(stream));
+	return hplai::launch_schur(maps, 0, 0, m, n, c, ldc, 0, 0, 0, static_cast<cudaStream_t>(stream));
 }

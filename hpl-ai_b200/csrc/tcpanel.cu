@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256) split_kernel(int rows, int kdim, const fl
 // writes it column-major (X[row][col] at x*[col*ldx + row]) as hi/lo.
 // ---------------------------------------------------------------------------
 template <bool TRANS_T>
-__global__ void __launch_bounds__(256) tri_inv_kernel(int b, const float *__restrict__ t, int64_t ldt,
+__device__ __forceinline__ void tri_inv_body(int b, const float *__restrict__ t, int64_t ldt,
 	float *__restrict__ xhi, float *__restrict__ xlo, int64_t ldx)
 {
 	extern __shared__ float sm[];
@@ -146,6 +146,16 @@ __global__ void __launch_bounds__(256) tri_inv_kernel(int b, const float *__rest
 		xhi[static_cast<int64_t>(col) * ldx + row] = h;
 		xlo[static_cast<int64_t>(col) * ldx + row] = v - h;
 	}
+}
+
+// blockIdx.y = 0: U11^{-1} from the upper triangle; 1: (L11^T)^{-1} from the unit lower one.
+__global__ void __launch_bounds__(256) tri_inv_kernel(int b, const float *__restrict__ t, int64_t ldt,
+	float *__restrict__ uhi, float *__restrict__ ulo, float *__restrict__ lhi, float *__restrict__ llo, int64_t ldx)
+{
+	if (blockIdx.y == 0)
+		tri_inv_body<false>(b, t, ldt, uhi, ulo, ldx);
+	else
+		tri_inv_body<true>(b, t, ldt, lhi, llo, ldx);
 }
 
 // ---------------------------------------------------------------------------
@@ -461,18 +471,13 @@ int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStr
 	const size_t smem = (static_cast<size_t>(b + 32) * 33 + 2 * 32 * 33) * sizeof(float);
 	static bool attr = false;
 	if (!attr) {
-		HPLAI_CUDA_TRY(cudaFuncSetAttribute(tri_inv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			static_cast<int>((1024 + 32) * 33 * 4 + 2 * 32 * 33 * 4)));
-		HPLAI_CUDA_TRY(cudaFuncSetAttribute(tri_inv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(tri_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			static_cast<int>((1024 + 32) * 33 * 4 + 2 * 32 * 33 * 4)));
 		attr = true;
 	}
-	// U11^{-1} column-major = the B operand of the L-panel product (row n = column n of U^{-1}).
-	tri_inv_kernel<false><<<groups, 256, smem, st>>>(b, lu, lda, t.uhi, t.ulo, t.ldp);
-	count_launches();
-	HPLAI_CUDA_TRY(cudaGetLastError());
-	// (L11^T)^{-1} column-major = L11^{-1} row-major = the A operand of the U-panel product.
-	tri_inv_kernel<true><<<groups, 256, smem, st>>>(b, lu, lda, t.lhi, t.llo, t.ldp);
+	// y = 0: U11^{-1} column-major = the B operand of the L-panel product (row n = column n of U^{-1});
+	// y = 1: (L11^T)^{-1} column-major = L11^{-1} row-major = the A operand of the U-panel product.
+	tri_inv_kernel<<<dim3(groups, 2), 256, smem, st>>>(b, lu, lda, t.uhi, t.ulo, t.lhi, t.llo, t.ldp);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;

@@ -82,6 +82,12 @@ typedef enum hplai_phase {
  * reference's substitution -- instead of the default tensor-core path
  * (triangular inverses of the diagonal block applied in 3xTF32). */
 #define HPLAI_FLAG_SIMT_PANELS 1u
+/* One-step look-ahead on two streams: the next diagonal block and panels are
+ * formed on a high-priority side stream while the main stream applies the
+ * rest of the trailing update (which then leaves 20 SMs free).  Off by
+ * default: on B200 the diagonal-block kernels slow down more under the
+ * concurrent update than the overlap saves.  Results are bit-identical. */
+#define HPLAI_FLAG_LOOKAHEAD 2u
 
 typedef struct hplai_ctx hplai_ctx;
 

@@ -166,6 +166,34 @@ def test_shgemm_minus_vs_torch_fp32(hplai, oracle, torch_cuda, m, n, k):
     assert bool((err <= bound).all()), float((err / bound).max())
 
 
+@pytest.mark.parametrize("m,n,k", [(60, 300, 60), (200, 60, 60), (1000, 500, 512), (4, 4, 16)])
+def test_shgemm_subregion_leaves_rest(hplai, torch_cuda, m, n, k):
+    """C is an interior m x n block of a larger matrix: the update must touch
+    exactly that block, even where a tensor-core tile reaches past its edge
+    into the rest of the matrix (the trailing update is applied region by
+    region)."""
+    torch = torch_cuda
+    g = torch.Generator(device="cuda").manual_seed(m + n + k)
+    ldh = (k + 63) // 64 * 64
+    l16 = (torch.rand(m, ldh, device="cuda", generator=g) - 0.5).half()
+    u16 = (torch.rand(n, ldh, device="cuda", generator=g) - 0.5).half()
+    big_rows, big_cols = m + 300, n + 300
+    big = torch.rand(big_cols, big_rows, device="cuda", generator=g)   # column-major, ld = big_rows
+    big0 = big.clone()
+    r0, c0 = 36, 20                                                     # interior offset, 16-byte aligned rows
+    cptr = big.data_ptr() + 4 * (r0 + c0 * big_rows)
+    hplai.check(hplai.shgemm_minus(m, n, k, l16.data_ptr(), ldh, u16.data_ptr(), ldh, cptr, big_rows, None))
+    torch.cuda.synchronize()
+    ref = big0.clone()
+    lf, uf = l16[:, :k].float(), u16[:, :k].float()
+    ref[c0:c0 + n, r0:r0 + m] -= uf @ lf.T
+    mask = torch.ones_like(big, dtype=torch.bool)
+    mask[c0:c0 + n, r0:r0 + m] = False
+    assert torch.equal(big[mask], big0[mask])
+    bound = (uf.abs() @ lf.abs().T) * 2.0 ** -19 + big0[c0:c0 + n, r0:r0 + m].abs() * 2.0 ** -22
+    assert bool(((big[c0:c0 + n, r0:r0 + m] - ref[c0:c0 + n, r0:r0 + m]).abs() <= bound).all())
+
+
 def test_shgemm_matches_oracle_at_c1_step(hplai, oracle, torch_cuda):
     """First C1 trailing update against the oracle's own Schur kernel."""
     torch = torch_cuda

@@ -98,6 +98,22 @@ def test_tensor_core_panels_fp32_accurate(hplai, oracle, torch_cuda, n, b):
     assert np.all(np.abs(lu[:b, b:] - urow) <= bu + 1e-30)
 
 
+@pytest.mark.parametrize("n,b,flags", [(1200, 60, 0), (8192, 512, 0), (6144, 1024, 0), (4096, 256, 1), (1200, 50, 0)])
+def test_lookahead_matches_serial_schedule(hplai, torch_cuda, n, b, flags):
+    """The two-stream look-ahead (next panel formed on the side stream while
+    the main stream updates the rest) computes exactly what the one-stream
+    schedule computes: every element sees the same kernels in the same
+    order, so the factors must be bit-identical."""
+    def lu(f):
+        with hplai.Solver(n, b, flags=f) as s:
+            s.generate(42)
+            s.factor()
+            return s.lu()
+    a = lu(flags | hplai.FLAG_LOOKAHEAD)
+    z = lu(flags)
+    assert np.array_equal(a.view(np.uint32), z.view(np.uint32))
+
+
 @pytest.mark.parametrize("n,b", [(2048, 64), (3000, 100), (8192, 256), (16384, 512)])
 def test_larger_solves_converge(hplai, oracle, torch_cuda, n, b):
     """Size-independent checks: hpl-harness < 16 (the FP64 backward-error
