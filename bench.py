@@ -166,19 +166,20 @@ def run_reference(args):
     return 0
 
 
-def schur_algorithmic(n, b):
+def schur_algorithmic(n, b, panel_bytes=2):
     """Flops and bytes of all Schur launches of one factorisation.
     Step k updates C = (n-(k+1)b)^2 FP32 elements (read and written, 8 B
-    each), reads the FP16 L and U panels (2*rem*b*2 B) and does 2*rem^2*b
-    flops, in three launches (the next panel's block column and block row,
-    then the rest of the trailing matrix; the last step has no rest)."""
+    each), reads the L and U panels (2*rem*b elements of panel_bytes: 2 for
+    FP16, 1 for e4m3) and does 2*rem^2*b flops, in three launches (the next
+    panel's block column and block row, then the rest of the trailing
+    matrix; the last step has no rest)."""
     flops = byts = 0.0
     launches = 0
     nb = n // b
     for k in range(nb - 1):
         rem = n - (k + 1) * b
         flops += 2.0 * rem * rem * b
-        byts += 8.0 * rem * rem + 4.0 * rem * b
+        byts += 8.0 * rem * rem + 2.0 * panel_bytes * rem * b
         launches += 3 if k < nb - 2 else 2   # next block column, next block row, rest
     return flops, byts, launches
 
@@ -213,13 +214,18 @@ def run_ours(args):
 
     n, b, seed, maxit = args.n, args.b, 42, 50
     dev = torch.cuda.current_device()
+    prec = hplai.F32_F8 if args.precision == "f8" else hplai.F32_F16
+    refine = args.refine or ("gmres" if args.precision == "f8" else "ir")
+    mode = hplai.GMRES if refine == "gmres" else hplai.IR
+    form = ("precision (F32_F8 e4m3 Schur" if prec == hplai.F32_F8 else "plain (F32_F16") + \
+        (" + GMRES-IR)" if mode == hplai.GMRES else " + IR)")
 
     def barrier():
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
 
-    s = hplai.Solver(n, b)
+    s = hplai.Solver(n, b, precision=prec)
     ext = torch.cuda.ExternalStream(s.stream())
     results = []
 
@@ -229,14 +235,14 @@ def run_ours(args):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(ext)
         s.factor()
-        r = s.iterative_refinement(maxit)
+        r = s.iterative_refinement(maxit, mode=mode)
         ev1.record(ext)
         ev1.synchronize()
         barrier()
         if r.status != hplai.HPLAI_OK:
             raise RuntimeError(f"solve did not converge: {r}")
         if timed:
-            results.append((ev0.elapsed_time(ev1), r, s.phase_ms()))
+            results.append((ev0.elapsed_time(ev1), r, s.phase_ms(), s.refine_counts()))
 
     for _ in range(args.warmup):
         one_step(False)
@@ -258,7 +264,12 @@ def run_ours(args):
     # Roofline of the dominant kernel (the Schur GEMM), timed inside the
     # library with CUDA events around each launch on its stream.
     hbm, tc_burst, tc_sus, peak_kind = load_peaks()
-    sflops, sbytes, slaunch = schur_algorithmic(n, b)
+    peak_note = f"{peak_kind} (MEASURED_PEAKS.json: hbm_gbs, bf16_tflops_sustained)"
+    if prec == hplai.F32_F8:
+        # no measured e4m3 peak: the dense e4m3 rate is twice the FP16/BF16 rate
+        tc_sus *= 2.0
+        peak_note += " x 2 for e4m3 (nominal e4m3:bf16 ratio; no measured e4m3 peak)"
+    sflops, sbytes, slaunch = schur_algorithmic(n, b, 1 if prec == hplai.F32_F8 else 2)
     gemm_ms = statistics.mean(r[2]["GEMM_UPDATE"] for r in results)
     avg_launch_s = gemm_ms * 1e-3 / slaunch
     ach_gbs = sbytes / slaunch / avg_launch_s / 1e9
@@ -271,13 +282,14 @@ def run_ours(args):
         roof = {"bound": "hbm", "achieved": ach_gbs, "peak": hbm, "unit": "GB/s", "frac": ach_gbs / hbm}
     else:
         roof = {"bound": "tensor", "achieved": ach_tf, "peak": tc_sus, "unit": "TFLOP/s", "frac": ach_tf / tc_sus}
-    roof.update({"traffic": traffic, "kernel": "schur_kernel (tcgen05 FP16 x FP16 -> FP32, C -= L*U)",
+    kname = "schur_kernel (tcgen05 e4m3 x e4m3 -> FP32, C -= sl*L*U*su)" if prec == hplai.F32_F8 else \
+        "schur_kernel (tcgen05 FP16 x FP16 -> FP32, C -= L*U)"
+    roof.update({"traffic": traffic if prec == hplai.F32_F16 else None, "kernel": kname,
                  "launches_per_step": slaunch, "avg_launch_ms": avg_launch_s * 1e3,
                  "algorithmic_bytes_per_launch": sbytes / slaunch, "algorithmic_flops_per_launch": sflops / slaunch,
                  "intensity_flop_per_byte": intensity, "ridge_flop_per_byte": ridge,
                  "tensor_achieved_tflops": ach_tf, "tensor_peak_tflops": tc_sus,
-                 "tensor_frac": ach_tf / tc_sus, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json: hbm_gbs, "
-                                                               f"bf16_tflops_sustained)"})
+                 "tensor_frac": ach_tf / tc_sus, "peak_source": peak_note})
     phases = {k: statistics.mean(r[2][k] for r in results) for k in results[0][2]}
 
     # End to end through the public C API with host buffers: pinned FP32 A,
@@ -335,13 +347,17 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp16/fp32/fp64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "e4m3/fp32/fp64" if prec == hplai.F32_F8 else "fp16/fp32/fp64",
             "data": "synthetic (the reference's own LCG matrix, seed 42, regenerated on the device before each step)",
-            "config": {"workload": f"HPL-AI plain solve n={n} b={b}: FP32 panels, FP16 tcgen05 Schur update, "
-                                   f"FP64 iterative refinement", "n": n, "b": b, "form": "plain (F32_F16 + IR)",
+            "config": {"workload": f"HPL-AI solve n={n} b={b}: FP32 panels, "
+                                   f"{'e4m3' if prec == hplai.F32_F8 else 'FP16'} tcgen05 Schur update, "
+                                   f"FP64 {'GMRES-IR' if mode == hplai.GMRES else 'iterative refinement'}",
+                       "n": n, "b": b, "form": form,
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": f"inputs {n * n * 4 / 1e9:.1f} GB FP32 > 126 MB L2, rewritten between steps"},
             "hpl_harness": last.hpl_harness, "resid": last.residual, "ir_steps": last.iters,
+            "gmres_inner_steps": results[-1][3][1] if mode == hplai.GMRES else None,
             "phases_ms": phases, "roofline": roof, "gpu_launches": int(launches),
             "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
         }
@@ -363,6 +379,10 @@ def main():
     ap.add_argument("--e2e-warmup", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", choices=("f16", "f8"), default="f16",
+                    help="Schur update operands: FP16 (plain form) or e4m3 with per-128 factors")
+    ap.add_argument("--refine", choices=("ir", "gmres"), default=None,
+                    help="correction: classical IR or GMRES (default: ir for f16, gmres for f8)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -57,6 +57,12 @@ struct hplai_ctx {
 	// reads those of step k (the reference's nbuf = 2 rotating buffers).
 	uint16_t *Lh[2] = {nullptr, nullptr}, *Uh[2] = {nullptr, nullptr};
 	SchurMaps maps[2];
+	// precision form: e4m3 panel copies with per-128-row/column factors
+	uint8_t *L8[2] = {nullptr, nullptr}, *U8[2] = {nullptr, nullptr};
+	float *sl[2] = {nullptr, nullptr}, *su[2] = {nullptr, nullptr};
+	unsigned *qbits = nullptr;
+	int64_t ld8 = 0;
+	SchurMaps maps8[2];
 	TcPanels tc;
 	float *tcbuf = nullptr;   // phi, plo (n x ldp) and the four b x ldp inverse buffers
 	double *rhs = nullptr, *d = nullptr, *x = nullptr, *r = nullptr, *scal = nullptr;
@@ -72,6 +78,16 @@ struct hplai_ctx {
 	double norma = 0.0, normb = 0.0;
 	std::vector<double> log_resid, log_harness;
 	double phase_ms[HPLAI_PH_COUNT] = {};
+	// GMRES correction: restart length, relative tolerance on the
+	// preconditioned residual, basis and scratch (allocated on first use)
+	int gm_restart = 30;
+	double gm_tol = 1e-12;
+	double *gm_v = nullptr;     // n x (gm_restart + 1), ld = gm_ldv
+	double *gm_w = nullptr;     // n
+	double *gm_small = nullptr; // part (kDotBlocks x kMaxBasis), H (kMaxBasis^2), tmp, y
+	int64_t gm_ldv = 0;
+	int gm_cap = 0;             // restart length gm_v was sized for
+	int gm_inner = 0;           // inner steps of the last hplai_refine
 };
 
 namespace {
@@ -83,7 +99,12 @@ int ctx_free(hplai_ctx *c)
 	for (int i = 0; i < 2; ++i) {
 		cudaFree(c->Lh[i]);
 		cudaFree(c->Uh[i]);
+		cudaFree(c->L8[i]);
+		cudaFree(c->U8[i]);
+		cudaFree(c->sl[i]);
+		cudaFree(c->su[i]);
 	}
+	cudaFree(c->qbits);
 	cudaFree(c->tcbuf);
 	cudaFree(c->rhs);
 	cudaFree(c->d);
@@ -92,6 +113,9 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->scal);
 	cudaFree(c->gemv_work);
 	cudaFree(c->trsv_work);
+	cudaFree(c->gm_v);
+	cudaFree(c->gm_w);
+	cudaFree(c->gm_small);
 	if (c->ev_panel) cudaEventDestroy(c->ev_panel);
 	if (c->ev_next) cudaEventDestroy(c->ev_next);
 	if (c->st) cudaStreamDestroy(c->st);
@@ -188,7 +212,7 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	if (!out) return HPLAI_EINVAL;
 	*out = nullptr;
 	if (n <= 0 || b < 16 || b > 1024 || n % b) return HPLAI_EINVAL;
-	if (precision != HPLAI_F32_F16) return HPLAI_EUNSUPPORTED;
+	if (precision != HPLAI_F32_F16 && precision != HPLAI_F32_F8) return HPLAI_EUNSUPPORTED;
 	hplai_ctx *c = new hplai_ctx;
 	c->n = n;
 	c->b = b;
@@ -219,6 +243,17 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		CTX_ALLOC(c->Lh[i], sizeof(uint16_t) * static_cast<size_t>(c->ldh) * n);
 		CTX_ALLOC(c->Uh[i], sizeof(uint16_t) * static_cast<size_t>(c->ldh) * n);
 	}
+	const int nblk128 = n / 128 + 2;
+	if (precision == HPLAI_F32_F8) {
+		c->ld8 = round_up(b, 128);
+		for (int i = 0; i < 2; ++i) {
+			CTX_ALLOC(c->L8[i], static_cast<size_t>(c->ld8) * n);
+			CTX_ALLOC(c->U8[i], static_cast<size_t>(c->ld8) * n);
+			CTX_ALLOC(c->sl[i], sizeof(float) * nblk128);
+			CTX_ALLOC(c->su[i], sizeof(float) * nblk128);
+		}
+		CTX_ALLOC(c->qbits, sizeof(unsigned) * nblk128);
+	}
 	const int64_t ldp = round_up(b, 32);
 	const size_t tc_elems = static_cast<size_t>(ldp) * (2 * static_cast<size_t>(n) + 4 * static_cast<size_t>(b));
 	CTX_ALLOC(c->tcbuf, sizeof(float) * tc_elems);
@@ -239,6 +274,10 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	for (int i = 0; i < 2 && s == HPLAI_OK; ++i) {
 		s = schur_make_maps(&c->maps[i], c->Lh[i], n, c->ldh, c->Uh[i], n, c->ldh, b);
 		if (s == HPLAI_OK) s = schur_set_cmap(&c->maps[i], c->A, n, n, c->lda);
+		if (s == HPLAI_OK && precision == HPLAI_F32_F8) {
+			s = schur_make_maps_fp8(&c->maps8[i], c->L8[i], n, c->ld8, c->U8[i], n, c->ld8, b);
+			if (s == HPLAI_OK) s = schur_set_cmap(&c->maps8[i], c->A, n, n, c->lda);
+		}
 	}
 	if (s == HPLAI_OK) {
 		float *base = c->tcbuf;
@@ -320,18 +359,29 @@ int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStrea
 		HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, c->Uh[buf] + (kb + b) * ldh,
 			ldh, 1.0f, side_ctas, st));
 	}
+	if (c->precision == HPLAI_F32_F8) {
+		HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, c->qbits, c->L8[buf] + (kb + b) * c->ld8, c->ld8,
+			c->sl[buf], st));
+		HPLAI_TRY(launch_quantize_upanel(rem, b, diag + static_cast<int64_t>(b) * lda, lda, c->qbits,
+			c->U8[buf] + (kb + b) * c->ld8, c->ld8, c->su[buf], st));
+	}
 	HPLAI_TRY(pe.end(st));
 	return HPLAI_OK;
 }
 
-// C -= L_k U_k on the rectangle of rows [r0, r1) and columns [c0, c1).
-int schur_region(hplai_ctx *c, int buf, int r0, int r1, int c0, int c1, int max_ctas, cudaStream_t st,
+// C -= L_k U_k on the rectangle of rows [r0, r1) and columns [c0, c1); the
+// step's panels start at row/column p0.
+int schur_region(hplai_ctx *c, int buf, int p0, int r0, int r1, int c0, int c1, int max_ctas, cudaStream_t st,
 	PhaseEvents &pe)
 {
 	if (r1 <= r0 || c1 <= c0) return HPLAI_OK;
 	HPLAI_TRY(pe.record(st, HPLAI_PH_GEMM_UPDATE));
-	HPLAI_TRY(launch_schur(c->maps[buf], r0, c0, r1 - r0, c1 - c0, c->A + r0 + static_cast<int64_t>(c0) * c->lda,
-		c->lda, r0, c0, max_ctas, st));
+	float *cp = c->A + r0 + static_cast<int64_t>(c0) * c->lda;
+	if (c->precision == HPLAI_F32_F8)
+		HPLAI_TRY(launch_schur_fp8(c->maps8[buf], c->sl[buf], p0, c->su[buf], p0, r0, c0, r1 - r0, c1 - c0, cp, c->lda,
+			r0, c0, max_ctas, st));
+	else
+		HPLAI_TRY(launch_schur(c->maps[buf], r0, c0, r1 - r0, c1 - c0, cp, c->lda, r0, c0, max_ctas, st));
 	HPLAI_TRY(pe.end(st));
 	return HPLAI_OK;
 }
@@ -376,13 +426,13 @@ extern "C" int hplai_factor(hplai_ctx *c)
 		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_panel, sd));
 		HPLAI_CUDA_TRY(cudaStreamWaitEvent(st, c->ev_panel, 0));
 		// the next panel's block column (rows r1..n) and block row (columns r2..n)
-		HPLAI_TRY(schur_region(c, buf, r1, n, r1, r2, 0, st, pe));
-		HPLAI_TRY(schur_region(c, buf, r1, r2, r2, n, 0, st, pe));
+		HPLAI_TRY(schur_region(c, buf, r1, r1, n, r1, r2, 0, st, pe));
+		HPLAI_TRY(schur_region(c, buf, r1, r1, r2, r2, n, 0, st, pe));
 		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));
 		HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_next, 0));
 		HPLAI_TRY(panel_step(c, k + 1, buf ^ 1, simt, side_ctas, sd, pe));
 		// the rest of the trailing matrix
-		HPLAI_TRY(schur_region(c, buf, r2, n, r2, n, main_ctas, st, pe));
+		HPLAI_TRY(schur_region(c, buf, r1, r2, n, r2, n, main_ctas, st, pe));
 	}
 	HPLAI_CUDA_TRY(cudaEventRecord(c->ev_panel, sd));
 	HPLAI_CUDA_TRY(cudaStreamWaitEvent(st, c->ev_panel, 0));
@@ -394,17 +444,147 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	return HPLAI_OK;
 }
 
+namespace {
+
+int ensure_gmres_buffers(hplai_ctx *c)
+{
+	const int m = c->gm_restart;
+	if (c->gm_v && c->gm_cap >= m) return HPLAI_OK;
+	cudaFree(c->gm_v);
+	cudaFree(c->gm_w);
+	cudaFree(c->gm_small);
+	c->gm_v = c->gm_w = c->gm_small = nullptr;
+	c->gm_ldv = round_up(c->n, 32);
+	HPLAI_CUDA_TRY(cudaMalloc(&c->gm_v, sizeof(double) * c->gm_ldv * (m + 1)));
+	HPLAI_CUDA_TRY(cudaMalloc(&c->gm_w, sizeof(double) * c->gm_ldv));
+	HPLAI_CUDA_TRY(cudaMalloc(&c->gm_small, sizeof(double) * (kDotBlocks * kMaxBasis + kMaxBasis * kMaxBasis +
+		2 * kMaxBasis)));
+	c->gm_cap = m;
+	return HPLAI_OK;
+}
+
+// r <- M^{-1} r with M = L U, the FP32 factors applied to an FP64 vector
+// (panel_trsvL / panel_trsvU, panel_trsv.hpp:310-758).
+int apply_lu_inverse(hplai_ctx *c, double *v, PhaseEvents &pe)
+{
+	cudaStream_t st = c->st;
+	HPLAI_TRY(pe.record(st, HPLAI_PH_IR_TRSV));
+	HPLAI_TRY(launch_trsv(true, c->n, c->A, c->lda, v, c->trsv_work, c->trsv_bytes, st));
+	HPLAI_TRY(launch_trsv(false, c->n, c->A, c->lda, v, c->trsv_work, c->trsv_bytes, st));
+	HPLAI_TRY(pe.end(st));
+	return HPLAI_OK;
+}
+
+// The classical correction: x += U^{-1} L^{-1} r (iterative_refinement.hpp:50-53).
+int correct_ir(hplai_ctx *c, PhaseEvents &pe)
+{
+	HPLAI_TRY(apply_lu_inverse(c, c->r, pe));
+	HPLAI_TRY(launch_axpy1(c->n, c->r, c->x, c->st));
+	return HPLAI_OK;
+}
+
+// The GMRES correction: one cycle of left-preconditioned GMRES(m) on
+// M^{-1} A d = M^{-1} r from d = 0, x += d.  CGS2 orthogonalisation on the
+// device, Givens rotations and the small triangular solve on the host.
+// Stops at |g_{j+1}| <= tol * ||M^{-1} r||_2 or after m steps.
+int correct_gmres(hplai_ctx *c, PhaseEvents &pe, int *inner)
+{
+	const int n = c->n, m = c->gm_restart;
+	const int64_t ldv = c->gm_ldv;
+	cudaStream_t st = c->st;
+	double *part = c->gm_small, *H = part + kDotBlocks * kMaxBasis, *tmp = H + kMaxBasis * kMaxBasis,
+	       *yd = tmp + kMaxBasis;
+	double *V = c->gm_v, *w = c->gm_w;
+	*inner = 0;
+	// z = M^{-1} r, beta = ||z||, v_0 = z / beta
+	HPLAI_TRY(apply_lu_inverse(c, c->r, pe));
+	HPLAI_TRY(launch_dots(n, 1, c->r, ldv, c->r, part, tmp, 2, st));
+	HPLAI_TRY(launch_scale(n, c->r, tmp, V, st));
+	double beta = 0.0;
+	HPLAI_CUDA_TRY(cudaMemcpyAsync(&beta, tmp, sizeof beta, cudaMemcpyDeviceToHost, st));
+	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
+	if (!(beta > 0.0) || !std::isfinite(beta)) return beta == 0.0 ? HPLAI_OK : HPLAI_ENOTCONV;
+	std::vector<double> R(static_cast<size_t>(m) * m, 0.0), cs(m), sn(m), g(m + 1, 0.0), h(m + 1);
+	g[0] = beta;
+	int k = 0;
+	for (int j = 0; j < m; ++j) {
+		double *vj = V + j * ldv, *vn = V + (j + 1) * ldv, *hc = H + j * kMaxBasis;
+		// w = M^{-1} A v_j, A regenerated in FP64
+		HPLAI_TRY(pe.record(st, HPLAI_PH_IR_GEMV));
+		HPLAI_TRY(launch_otf_gemv(n, 1.0, vj, 0.0, w, c->seed, c->d, c->gemv_work, c->gemv_bytes, st));
+		HPLAI_TRY(pe.end(st));
+		HPLAI_TRY(apply_lu_inverse(c, w, pe));
+		// two Gram-Schmidt sweeps against v_0..v_j; ||w|| after the second
+		HPLAI_TRY(launch_dots(n, j + 1, V, ldv, w, part, hc, 0, st));
+		HPLAI_TRY(launch_gs_update(n, j + 1, V, ldv, hc, w, part, nullptr, st));
+		HPLAI_TRY(launch_dots(n, j + 1, V, ldv, w, part, tmp, 0, st));
+		HPLAI_TRY(launch_gs_update(n, j + 1, V, ldv, tmp, w, part, hc + j + 1, st));
+		HPLAI_TRY(launch_add_small(j + 1, tmp, hc, st));
+		HPLAI_TRY(launch_scale(n, w, hc + j + 1, vn, st));
+		HPLAI_CUDA_TRY(cudaMemcpyAsync(h.data(), hc, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, st));
+		HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
+		++*inner;
+		for (int i = 0; i < j; ++i) {
+			const double t = cs[i] * h[i] + sn[i] * h[i + 1];
+			h[i + 1] = -sn[i] * h[i] + cs[i] * h[i + 1];
+			h[i] = t;
+		}
+		const double rho = std::hypot(h[j], h[j + 1]);
+		if (!(rho > 0.0) || !std::isfinite(rho)) break;
+		cs[j] = h[j] / rho;
+		sn[j] = h[j + 1] / rho;
+		h[j] = rho;
+		g[j + 1] = -sn[j] * g[j];
+		g[j] = cs[j] * g[j];
+		for (int i = 0; i <= j; ++i) R[static_cast<size_t>(j) * m + i] = h[i];
+		k = j + 1;
+		if (std::fabs(g[j + 1]) <= c->gm_tol * beta) break;
+	}
+	if (k == 0) return HPLAI_ENOTCONV;
+	// R y = g, R upper triangular (column j at R[j*m])
+	std::vector<double> y(k);
+	for (int i = k - 1; i >= 0; --i) {
+		double s = g[i];
+		for (int j = i + 1; j < k; ++j) s -= R[static_cast<size_t>(j) * m + i] * y[j];
+		y[i] = s / R[static_cast<size_t>(i) * m + i];
+	}
+	HPLAI_CUDA_TRY(cudaMemcpyAsync(yd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
+	HPLAI_TRY(launch_combine(n, k, V, ldv, yd, c->x, st));
+	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
+	return HPLAI_OK;
+}
+
+} // namespace
+
+extern "C" int hplai_set_gmres(hplai_ctx *c, int restart, double tol)
+{
+	if (!c || restart < 1 || restart > kMaxBasis - 1 || !(tol > 0.0) || !(tol < 1.0)) return HPLAI_EINVAL;
+	c->gm_restart = restart;
+	c->gm_tol = tol;
+	return HPLAI_OK;
+}
+
+extern "C" int hplai_get_refine_counts(hplai_ctx *c, int *outer, int *inner)
+{
+	if (!c) return HPLAI_EINVAL;
+	if (outer) *outer = static_cast<int>(c->log_resid.size());
+	if (inner) *inner = c->gm_inner;
+	return HPLAI_OK;
+}
+
 extern "C" int hplai_refine(hplai_ctx *c, int mode, int maxit, hplai_ir_errors *err, int *iters)
 {
 	if (!c || maxit < 0) return HPLAI_EINVAL;
 	if (!c->factored) return HPLAI_ESTATE;
-	if (mode != HPLAI_IR) return HPLAI_EUNSUPPORTED;
+	if (mode != HPLAI_IR && mode != HPLAI_GMRES) return HPLAI_EUNSUPPORTED;
 	const int n = c->n;
 	cudaStream_t st = c->st;
 	c->log_resid.clear();
 	c->log_harness.clear();
+	c->gm_inner = 0;
 	if (err) *err = hplai_ir_errors{-1.0, -1.0};
 	if (iters) *iters = 0;
+	if (mode == HPLAI_GMRES) HPLAI_TRY(ensure_gmres_buffers(c));
 	PhaseEvents pe;
 	// x_0 = b ./ diag(A)   (iterative_refinement.hpp:31-34)
 	HPLAI_TRY(launch_div(n, c->rhs, c->d, c->x, st));
@@ -431,12 +611,15 @@ extern "C" int hplai_refine(hplai_ctx *c, int mode, int maxit, hplai_ir_errors *
 			rc = HPLAI_OK;
 			break;
 		}
-		// x += U^{-1} L^{-1} r   (iterative_refinement.hpp:50-53)
-		HPLAI_TRY(pe.record(st, HPLAI_PH_IR_TRSV));
-		HPLAI_TRY(launch_trsv(true, n, c->A, c->lda, c->r, c->trsv_work, c->trsv_bytes, st));
-		HPLAI_TRY(launch_trsv(false, n, c->A, c->lda, c->r, c->trsv_work, c->trsv_bytes, st));
-		HPLAI_TRY(pe.end(st));
-		HPLAI_TRY(launch_axpy1(n, c->r, c->x, st));
+		if (!std::isfinite(hpl)) break;
+		if (mode == HPLAI_IR) {
+			HPLAI_TRY(correct_ir(c, pe));
+		} else {
+			int in = 0;
+			const int gr = correct_gmres(c, pe, &in);
+			c->gm_inner += in;
+			if (gr != HPLAI_OK) break;
+		}
 		int ts = HPLAI_OK;
 		HPLAI_TRY(trsv_status(c->trsv_work, st, &ts));
 		if (ts != HPLAI_OK) return ts;
@@ -518,7 +701,7 @@ extern "C" int hplai_solve_host(hplai_ctx *c, const float *a, int64_t lda, const
 {
 	HPLAI_TRY(hplai_upload(c, a, lda, rhs, diag, seed));
 	HPLAI_TRY(hplai_factor(c));
-	const int rc = hplai_refine(c, HPLAI_IR, maxit, err, iters);
+	const int rc = hplai_refine(c, c->precision == HPLAI_F32_F8 ? HPLAI_GMRES : HPLAI_IR, maxit, err, iters);
 	if (rc != HPLAI_OK && rc != HPLAI_ENOTCONV) return rc;
 	HPLAI_TRY(hplai_get_x(c, x));
 	return rc;

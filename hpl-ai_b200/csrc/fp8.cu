@@ -1,0 +1,138 @@
+// fp8.cu -- FP8 (e4m3) copies of the L and U panels for the precision form.
+//
+// The reference down-casts its FP32 panels to FLOW with one scale factor
+// (convert_left/right_panels, panel_trf.hpp:173-233, scalea = n^0.75 under
+// lazy init).  With e4m3 (3 mantissa bits, |x| <= 448) one global factor
+// cannot cover the panels' dynamic range, so here every block of 128 panel
+// rows (128 rows of L, 128 columns of U) gets its own power-of-two factor
+// 2^e chosen so that the block's largest magnitude maps just below 448.  The
+// Schur GEMM multiplies each accumulator element by the two blocks' factors
+// (exact, powers of two) before the update.
+//
+// amax_kernel: per-block max |x| (atomicMax on the float bits, which order
+// like the values for x >= 0).  cast8_kernel: x * 2^-e rounded to e4m3 (RN,
+// saturating), row-major with K contiguous, plus the factor 2^e per block.
+#include "common.cuh"
+#include "internal.h"
+
+#include <cuda_fp8.h>
+
+namespace hplai {
+
+namespace {
+
+constexpr float kE4M3Max = 448.f;
+
+// X (rows x kdim), element (r, k) at src[r + k*ld] (RCONTIG, column-major L
+// panel) or at src[k + r*ld] (the U panel read by columns).
+template <bool RCONTIG>
+__global__ void __launch_bounds__(256) amax_kernel(int rows, int kdim, const float *__restrict__ src, int64_t ld,
+	unsigned *__restrict__ bits)
+{
+	const int r0 = blockIdx.x * 128, k0 = blockIdx.y * 64;
+	float m = 0.f;
+	for (int e = threadIdx.x; e < 128 * 64; e += 256) {
+		const int r = RCONTIG ? (e & 127) : (e >> 6), k = RCONTIG ? (e >> 7) : (e & 63);
+		if (r0 + r < rows && k0 + k < kdim) {
+			const float v = RCONTIG ? src[static_cast<int64_t>(k0 + k) * ld + r0 + r]
+			                        : src[static_cast<int64_t>(r0 + r) * ld + k0 + k];
+			m = fmaxf(m, fabsf(v));
+		}
+	}
+	for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+	__shared__ float wm[8];
+	if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (int w = 1; w < 8; ++w) m = fmaxf(m, wm[w]);
+		atomicMax(&bits[blockIdx.x], __float_as_uint(m));
+	}
+}
+
+__device__ __forceinline__ int block_exponent(unsigned amax_bits)
+{
+	const float amax = __uint_as_float(amax_bits);
+	if (!(amax > 0.f)) return 0;
+	int e;
+	frexpf(amax / kE4M3Max, &e);   // amax/448 = f 2^e, f in [0.5, 1): amax 2^-e < 448
+	return e;
+}
+
+// Tile of 32 rows x 128 k: load (coalesced along the source's contiguous
+// index), then write 4 e4m3 bytes per thread along k.
+template <bool RCONTIG>
+__global__ void __launch_bounds__(256) cast8_kernel(int rows, int kdim, const float *__restrict__ src, int64_t ld,
+	const unsigned *__restrict__ bits, uint8_t *__restrict__ dst, int64_t ld8, float *__restrict__ scale)
+{
+	__shared__ float tile[32][129];
+	const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 128;
+	for (int e = threadIdx.x; e < 32 * 128; e += 256) {
+		const int r = RCONTIG ? (e & 31) : (e >> 7), k = RCONTIG ? (e >> 5) : (e & 127);
+		float v = 0.f;
+		if (r0 + r < rows && k0 + k < kdim)
+			v = RCONTIG ? src[static_cast<int64_t>(k0 + k) * ld + r0 + r] : src[static_cast<int64_t>(r0 + r) * ld + k0 + k];
+		tile[r][k] = v;
+	}
+	__syncthreads();
+	for (int e = threadIdx.x; e < 32 * 32; e += 256) {
+		const int r = e >> 5, w = e & 31;
+		const int row = r0 + r;
+		if (row >= rows) continue;
+		const int ex = block_exponent(bits[row >> 7]);
+		const float inv = ldexpf(1.f, -ex);
+		uint32_t packed = 0;
+#pragma unroll
+		for (int q = 0; q < 4; ++q) {
+			const __nv_fp8_storage_t b8 = __nv_cvt_float_to_fp8(tile[r][4 * w + q] * inv, __NV_SATFINITE, __NV_E4M3);
+			packed |= static_cast<uint32_t>(b8) << (8 * q);
+		}
+		if (k0 + 4 * w < ld8) *reinterpret_cast<uint32_t *>(dst + static_cast<int64_t>(row) * ld8 + k0 + 4 * w) = packed;
+		if ((row & 127) == 0 && k0 == 0 && w == 0) scale[row >> 7] = ldexpf(1.f, ex);
+	}
+}
+
+template <bool RCONTIG>
+int quantize(int rows, int kdim, const float *src, int64_t ld, unsigned *bits, uint8_t *dst, int64_t ld8,
+	float *scale, cudaStream_t st)
+{
+	if (rows <= 0) return HPLAI_OK;
+	const int nblk = (rows + 127) / 128;
+	HPLAI_CUDA_TRY(cudaMemsetAsync(bits, 0, sizeof(unsigned) * nblk, st));
+	amax_kernel<RCONTIG><<<dim3(nblk, (kdim + 63) / 64), 256, 0, st>>>(rows, kdim, src, ld, bits);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	cast8_kernel<RCONTIG><<<dim3((rows + 31) / 32, static_cast<unsigned>((ld8 + 127) / 128)), 256, 0, st>>>(rows, kdim,
+		src, ld, bits, dst, ld8, scale);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+} // namespace
+
+int launch_quantize_lpanel(int rows, int b, const float *acol, int64_t lda, unsigned *bits, uint8_t *l8, int64_t ld8,
+	float *scale, cudaStream_t st)
+{
+	if (ld8 % 128) return HPLAI_EINVAL;
+	return quantize<true>(rows, b, acol, lda, bits, l8, ld8, scale, st);
+}
+
+int launch_quantize_upanel(int cols, int b, const float *arow, int64_t lda, unsigned *bits, uint8_t *u8, int64_t ld8,
+	float *scale, cudaStream_t st)
+{
+	if (ld8 % 128) return HPLAI_EINVAL;
+	return quantize<false>(cols, b, arow, lda, bits, u8, ld8, scale, st);
+}
+
+} // namespace hplai
+
+extern "C" int hplai_quantize_e4m3(int rows, int k, const float *src, int64_t lds, int col_major, uint8_t *dst,
+	int64_t ld8, float *scale, unsigned *bits, void *stream)
+{
+	if (rows < 0 || k <= 0 || k > ld8 || !src || !dst || !scale || !bits || (ld8 % 128)) return HPLAI_EINVAL;
+	if (reinterpret_cast<uintptr_t>(dst) % 16) return HPLAI_EINVAL;   // rows are written as 4-byte words
+	if (col_major ? lds < rows : lds < k) return HPLAI_EINVAL;
+	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	return col_major ? hplai::launch_quantize_lpanel(rows, k, src, lds, bits, dst, ld8, scale, st)
+	                 : hplai::launch_quantize_upanel(rows, k, src, lds, bits, dst, ld8, scale, st);
+}

@@ -52,6 +52,15 @@ int schur_set_cmap(SchurMaps *m, const float *c, int rows, int cols, int64_t ldc
 // another stream keeps some SMs.
 int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
 	int ccol0, int max_ctas, cudaStream_t st);
+// FP8 (e4m3) panels: L8 lrows x k bytes (row-major, ldl), U8 urows x k; maps
+// for the same kernel with kind::f8f6f4.  The C matrix is set with
+// schur_set_cmap as for FP16.
+int schur_make_maps_fp8(SchurMaps *m, const uint8_t *l8, int lrows, int64_t ldl, const uint8_t *u8, int urows,
+	int64_t ldu, int k);
+// C -= (sl x L8)(su x U8)^T with one power-of-two factor per 128 rows of L8
+// (sl[(row - sl0) / 128]) and per 128 rows of U8 (su[(row - su0) / 128]).
+int launch_schur_fp8(const SchurMaps &maps8, const float *sl, int sl0, const float *su, int su0, int lrow0, int urow0,
+	int m, int n, float *c, int64_t ldc, int crow0, int ccol0, int max_ctas, cudaStream_t st);
 int schur_status();          // HPLAI_ETIMEOUT if a device wait ran out since the last reset
 void schur_status_reset();
 
@@ -83,6 +92,16 @@ int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint1
 int tc_status();
 void tc_status_reset();
 
+// fp8.cu
+// e4m3 copies of the L panel (rows x b, column-major FP32 source) and of the
+// U panel (read by columns), row-major with K contiguous (ld8 a multiple of
+// 128 bytes), and one power-of-two factor per 128 rows/columns in `scale`
+// (block 0 = the first row).  `bits` is rows/128 + 1 words of scratch.
+int launch_quantize_lpanel(int rows, int b, const float *acol, int64_t lda, unsigned *bits, uint8_t *l8, int64_t ld8,
+	float *scale, cudaStream_t st);
+int launch_quantize_upanel(int cols, int b, const float *arow, int64_t lda, unsigned *bits, uint8_t *u8, int64_t ld8,
+	float *scale, cudaStream_t st);
+
 // refine.cu
 size_t otf_gemv_workspace(int n);
 int launch_otf_gemv(int n, double alpha, const double *x, double beta, double *y, uint64_t seed,
@@ -96,5 +115,20 @@ int trsv_status(void *work, cudaStream_t st, int *status);
 int launch_infnorm(int n, const double *x, double *out, cudaStream_t st);
 int launch_div(int n, const double *num, const double *den, double *out, cudaStream_t st);
 int launch_axpy1(int n, const double *x, double *y, cudaStream_t st);
+
+// krylov.cu -- GMRES vector kernels.  `part` holds kDotBlocks x kMaxBasis
+// doubles.  V is column-major n x nv with leading dimension ldv.
+constexpr int kMaxBasis = 32;
+constexpr int kDotBlocks = 296;
+// out[0..nv) (op 0: =, 1: +=) V^T w
+int launch_dots(int n, int nv, const double *v, int64_t ldv, const double *w, double *part, double *out, int op,
+	cudaStream_t st);
+// w -= V h; if norm_out, *norm_out = ||w||_2 afterwards
+int launch_gs_update(int n, int nv, const double *v, int64_t ldv, const double *h, double *w, double *part,
+	double *norm_out, cudaStream_t st);
+int launch_add_small(int nv, const double *a, double *b, cudaStream_t st);
+int launch_scale(int n, const double *w, const double *den, double *out, cudaStream_t st);
+// x += V y
+int launch_combine(int n, int nv, const double *v, int64_t ldv, const double *y, double *x, cudaStream_t st);
 
 } // namespace hplai

@@ -33,7 +33,7 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BN = 256;
-constexpr int BK = 64;                 // one 128-byte swizzle row of FP16
+constexpr int BK = 64;                 // one 128-byte swizzle row of FP16 (128 FP8 values)
 constexpr int STAGES = 4;
 constexpr int A_BYTES = BM * BK * 2;   // 16 KB
 constexpr int B_BYTES = BN * BK * 2;   // 32 KB
@@ -56,6 +56,10 @@ struct Params {
 	int lrow0, urow0; // first L row / first U row (= C column) in the panel buffers
 	int tiles_m, tiles_n;
 	int crow0, ccol0; // coordinates of C(0,0) in the C tensor map (reduce epilogue)
+	// FP8 operands: power-of-two dequantisation factors per 128 rows of L
+	// (sl, block 0 starting at L row sl0) and per 128 columns of U (su, su0).
+	const float *sl, *su;
+	int sl0, su0;
 };
 
 __device__ unsigned int g_status;
@@ -70,7 +74,10 @@ __device__ __forceinline__ void tma_reduce_add_2d(const void *map, const void *s
 // RED: the epilogue writes -acc to shared memory and a TMA reduce-add folds
 // it into C in L2 (C never passes through the SM); otherwise the epilogue
 // loads C, subtracts and stores with plain coalesced accesses.
-template <bool RED>
+// FP8: e4m3 operands (kind::f8f6f4, K = 32 per MMA, 128 per 128-byte row)
+// with the accumulator multiplied by the two blocks' power-of-two factors
+// in the epilogue (exact); otherwise FP16 operands (kind::f16).
+template <bool RED, bool FP8>
 __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant__ CUtensorMap lmap,
 	const __grid_constant__ CUtensorMap umap, const __grid_constant__ CUtensorMap cmap, const Params p)
 {
@@ -132,8 +139,10 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 				for (int kc = 0; kc < p.num_kc; ++kc) {
 					if (!mbar_wait(&empty[stage], phase ^ 1u)) { ok = false; break; }
 					mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
-					tma_load_2d(sA + stage * A_BYTES, &lmap, &full[stage], kc * BK, p.lrow0 + tm * BM);
-					tma_load_2d(sB + stage * B_BYTES, &umap, &full[stage], kc * BK, p.urow0 + tn * BN);
+					// K offset of this stage in elements: 64 FP16 or 128 FP8 per 128-byte row
+					const int kx = kc * (FP8 ? 2 * BK : BK);
+					tma_load_2d(sA + stage * A_BYTES, &lmap, &full[stage], kx, p.lrow0 + tm * BM);
+					tma_load_2d(sB + stage * B_BYTES, &umap, &full[stage], kx, p.urow0 + tn * BN);
 					++issued;
 					if (++stage == STAGES) { stage = 0; phase ^= 1u; }
 				}
@@ -161,9 +170,13 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 					const uint64_t adesc = umma_desc_k_sw128(smem_u32(sA + stage * A_BYTES));
 					const uint64_t bdesc = umma_desc_k_sw128(smem_u32(sB + stage * B_BYTES));
 #pragma unroll
-					for (int kk = 0; kk < BK / 16; ++kk) {
-						// advance 16 FP16 = 32 bytes (2 units of 16 B) along K inside the swizzle row
-						umma_f16(d_tmem, adesc + 2u * kk, bdesc + 2u * kk, idesc, (kc | kk) != 0 ? 1u : 0u);
+					for (int kk = 0; kk < 4; ++kk) {
+						// advance 32 bytes (2 units of 16 B) along K inside the 128-byte swizzle row:
+						// 16 FP16 or 32 FP8 values per MMA
+						if (FP8)
+							umma_f8(d_tmem, adesc + 2u * kk, bdesc + 2u * kk, idesc, (kc | kk) != 0 ? 1u : 0u);
+						else
+							umma_f16(d_tmem, adesc + 2u * kk, bdesc + 2u * kk, idesc, (kc | kk) != 0 ? 1u : 0u);
 					}
 					umma_commit(&empty[stage]);
 					++used;
@@ -193,6 +206,12 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 			if (!ok) break;
 			tc_fence_after();
 			const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * BN);
+			// FP8: this lane's row factor (rows past the panel end read block 0; never stored)
+			float rs = 1.f;
+			if (FP8) {
+				const int lr = p.lrow0 + tm * BM + q * 32 + lane - p.sl0;
+				rs = (tm * BM + q * 32 + lane < p.m) ? p.sl[lr >> 7] : 0.f;
+			}
 			if (RED) {
 				float *mybuf = sEpi + (warp - 2) * 2 * (EPI_BUF_BYTES / 4);
 				const int gx = p.crow0 + tm * BM + q * 32;   // tensor-map row of this warp's lane 0
@@ -205,8 +224,18 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 					// the reduce issued two chunks ago read this buffer; let it finish
 					if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
 					__syncwarp();
+					if (FP8) {
+						const int cb = p.urow0 + tn * BN + ch * EPI_CHUNK - p.su0;
 #pragma unroll
-					for (int j = 0; j < 32; ++j) sb[j * 32 + lane] = -__uint_as_float(r[j]);
+						for (int j = 0; j < 32; ++j) {
+							const int cj = cb + j;
+							const float cs = (tn * BN + ch * EPI_CHUNK + j < p.n) ? __ldg(&p.su[cj >> 7]) : 0.f;
+							sb[j * 32 + lane] = -(__uint_as_float(r[j]) * (rs * cs));
+						}
+					} else {
+#pragma unroll
+						for (int j = 0; j < 32; ++j) sb[j * 32 + lane] = -__uint_as_float(r[j]);
+					}
 					asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 					__syncwarp();
 					if (lane == 0) {
@@ -231,8 +260,13 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 						for (int j = 0; j < 32; ++j)
 							if (col0 + j < p.n) cv[j] = crow[static_cast<int64_t>(col0 + j) * p.ldc];
 #pragma unroll
-						for (int j = 0; j < 32; ++j)
-							if (col0 + j < p.n) crow[static_cast<int64_t>(col0 + j) * p.ldc] = cv[j] - __uint_as_float(r[j]);
+						for (int j = 0; j < 32; ++j) {
+							if (col0 + j < p.n) {
+								float v = __uint_as_float(r[j]);
+								if (FP8) v *= rs * __ldg(&p.su[(p.urow0 + col0 + j - p.su0) >> 7]);
+								crow[static_cast<int64_t>(col0 + j) * p.ldc] = cv[j] - v;
+							}
+						}
 					}
 				}
 			}
@@ -334,8 +368,8 @@ int schur_set_cmap(SchurMaps *m, const float *c, int rows, int cols, int64_t ldc
 	return HPLAI_OK;
 }
 
-int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
-	int ccol0, int max_ctas, cudaStream_t st)
+static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, int sl0, const float *su, int su0,
+	int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0, int ccol0, int max_ctas, cudaStream_t st)
 {
 	if (m <= 0 || n <= 0) return HPLAI_OK;
 	Params p;
@@ -343,13 +377,17 @@ int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, floa
 	p.ldc = ldc;
 	p.m = m;
 	p.n = n;
-	p.num_kc = (maps.k + BK - 1) / BK;
+	p.num_kc = fp8 ? (maps.k + 127) / 128 : (maps.k + BK - 1) / BK;
 	p.lrow0 = lrow0;
 	p.urow0 = urow0;
 	p.tiles_m = (m + BM - 1) / BM;
 	p.tiles_n = (n + BN - 1) / BN;
 	p.crow0 = crow0;
 	p.ccol0 = ccol0;
+	p.sl = sl;
+	p.su = su;
+	p.sl0 = sl0;
+	p.su0 = su0;
 	const int total = p.tiles_m * p.tiles_n;
 	int grid = (max_ctas > 0 && max_ctas < num_sms()) ? max_ctas : num_sms();
 	if (grid > total) grid = total;
@@ -365,9 +403,13 @@ int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, floa
 		red = false;
 	static bool attr_set = false;
 	if (!attr_set) {
-		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			static_cast<int>(smem_bytes(false))));
-		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(smem_bytes(true))));
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(smem_bytes(false))));
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			static_cast<int>(smem_bytes(true))));
 		attr_set = true;
 	}
@@ -375,12 +417,42 @@ int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, floa
 	std::memcpy(&lm, maps.lmap, sizeof(lm));
 	std::memcpy(&um, maps.umap, sizeof(um));
 	std::memcpy(&cm, red ? cmap : maps.lmap, sizeof(cm));
-	if (red)
-		schur_kernel<true><<<grid, THREADS, smem_bytes(true), st>>>(lm, um, cm, p);
+	if (red && fp8)
+		schur_kernel<true, true><<<grid, THREADS, smem_bytes(true), st>>>(lm, um, cm, p);
+	else if (red)
+		schur_kernel<true, false><<<grid, THREADS, smem_bytes(true), st>>>(lm, um, cm, p);
+	else if (fp8)
+		schur_kernel<false, true><<<grid, THREADS, smem_bytes(false), st>>>(lm, um, cm, p);
 	else
-		schur_kernel<false><<<grid, THREADS, smem_bytes(false), st>>>(lm, um, cm, p);
+		schur_kernel<false, false><<<grid, THREADS, smem_bytes(false), st>>>(lm, um, cm, p);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
+	int ccol0, int max_ctas, cudaStream_t st)
+{
+	return launch_schur_any(maps, false, nullptr, 0, nullptr, 0, lrow0, urow0, m, n, c, ldc, crow0, ccol0, max_ctas, st);
+}
+
+int launch_schur_fp8(const SchurMaps &maps8, const float *sl, int sl0, const float *su, int su0, int lrow0, int urow0,
+	int m, int n, float *c, int64_t ldc, int crow0, int ccol0, int max_ctas, cudaStream_t st)
+{
+	return launch_schur_any(maps8, true, sl, sl0, su, su0, lrow0, urow0, m, n, c, ldc, crow0, ccol0, max_ctas, st);
+}
+
+int schur_make_maps_fp8(SchurMaps *m, const uint8_t *l8, int lrows, int64_t ldl, const uint8_t *u8, int urows,
+	int64_t ldu, int k)
+{
+	if (!m || !l8 || !u8 || lrows <= 0 || urows <= 0 || k <= 0 || ldl < k || ldu < k || (ldl % 16) || (ldu % 16))
+		return HPLAI_EINVAL;
+	HPLAI_TRY(make_map_2d(m->lmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, l8, static_cast<uint64_t>(k),
+		static_cast<uint64_t>(lrows), static_cast<uint64_t>(ldl), 128, BM, CU_TENSOR_MAP_SWIZZLE_128B));
+	HPLAI_TRY(make_map_2d(m->umap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, u8, static_cast<uint64_t>(k),
+		static_cast<uint64_t>(urows), static_cast<uint64_t>(ldu), 128, BN, CU_TENSOR_MAP_SWIZZLE_128B));
+	m->k = k;
+	m->has_cmap = false;
 	return HPLAI_OK;
 }
 
@@ -408,4 +480,15 @@ extern "C" int hplai_shgemm_minus(int m, int n, int k, const uint16_t *lh, int64
 	HPLAI_TRY(hplai::schur_make_maps(&maps, lh, m, ldlh, uh, n, lduh, k));
 	HPLAI_TRY(hplai::schur_set_cmap(&maps, c, m, n, ldc));
 	return hplai::launch_schur(maps, 0, 0, m, n, c, ldc, 0, 0, 0, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hplai_f8gemm_minus(int m, int n, int k, const uint8_t *l8, int64_t ldl, const float *sl,
+	const uint8_t *u8, int64_t ldu, const float *su, float *c, int64_t ldc, void *stream)
+{
+	if (m < 0 || n < 0 || k <= 0 || !l8 || !u8 || !sl || !su || !c || ldc < m || ldl < k || ldu < k) return HPLAI_EINVAL;
+	if (m == 0 || n == 0) return HPLAI_OK;
+	hplai::SchurMaps maps;
+	HPLAI_TRY(hplai::schur_make_maps_fp8(&maps, l8, m, ldl, u8, n, ldu, k));
+	HPLAI_TRY(hplai::schur_set_cmap(&maps, c, m, n, ldc));
+	return hplai::launch_schur_fp8(maps, sl, 0, su, 0, 0, 0, m, n, c, ldc, 0, 0, 0, static_cast<cudaStream_t>(stream));
 }

@@ -65,6 +65,8 @@ _get_ir_log = _proto("hplai_get_ir_log", _c_int, _vp, _vp, _vp, _c_int, ctypes.P
 _get_phase_ms = _proto("hplai_get_phase_ms", _c_int, _vp, _vp, _c_int)
 _get_stream = _proto("hplai_get_stream", _vp, _vp)
 launch_count = _proto("hplai_launch_count", ctypes.c_ulonglong)
+_set_gmres = _proto("hplai_set_gmres", _c_int, _vp, _c_int, _c_dbl)
+_get_refine_counts = _proto("hplai_get_refine_counts", _c_int, _vp, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int))
 _get_norms = _proto("hplai_get_norms", _c_int, _vp, ctypes.POINTER(_c_dbl), ctypes.POINTER(_c_dbl))
 _solve_host = _proto("hplai_solve_host", _c_int, _vp, _vp, _c_i64, _vp, _vp, _c_u64, _c_int, _vp,
                      ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
@@ -81,6 +83,10 @@ trsm_left_lower = _proto("hplai_trsm_left_lower", _c_int, _c_int, _c_int, _vp, _
                          _c_flt, _vp)
 shgemm_minus = _proto("hplai_shgemm_minus", _c_int, _c_int, _c_int, _c_int, _vp, _c_i64, _vp, _c_i64, _vp, _c_i64,
                       _vp)
+quantize_e4m3 = _proto("hplai_quantize_e4m3", _c_int, _c_int, _c_int, _vp, _c_i64, _c_int, _vp, _c_i64, _vp, _vp,
+                       _vp)
+f8gemm_minus = _proto("hplai_f8gemm_minus", _c_int, _c_int, _c_int, _c_int, _vp, _c_i64, _vp, _vp, _c_i64, _vp, _vp,
+                      _c_i64, _vp)
 otf_gemv_workspace = _proto("hplai_otf_gemv_workspace", _c_sz, _c_int)
 otf_gemv = _proto("hplai_otf_gemv", _c_int, _c_int, _c_dbl, _vp, _c_dbl, _vp, _c_u64, _vp, _vp, _c_sz, _vp)
 otf_gemv_noalloc = _proto("hplai_otf_gemv_noalloc", _c_int, _c_int, _c_dbl, _vp, _c_dbl, _vp, _c_u64, _vp, _vp)
@@ -175,6 +181,15 @@ class Solver:
         if s not in (HPLAI_OK, HPLAI_ENOTCONV):
             check(s, "hplai_refine")
         return RefineResult(e.residual, e.hpl_harness, it.value, s)
+
+    def set_gmres(self, restart: int = 30, tol: float = 1e-12):
+        check(_set_gmres(self._h, restart, tol), "hplai_set_gmres")
+
+    def refine_counts(self):
+        """(residual evaluations, GMRES inner steps) of the last refinement."""
+        o, i = _c_int(), _c_int()
+        check(_get_refine_counts(self._h, ctypes.byref(o), ctypes.byref(i)), "hplai_get_refine_counts")
+        return o.value, i.value
 
     def solve_host(self, a, rhs, diag, seed=42, maxit=50):
         a = np.asfortranarray(a, dtype=np.float32)

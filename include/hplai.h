@@ -129,8 +129,16 @@ int hplai_factor(hplai_ctx *ctx);
 
 /* iterative_refinement (iterative_refinement.hpp:18-57) with maxit steps
  * (the driver uses 50).  Fills *err ({-1,-1} on failure) and *iters (the
- * number of residual evaluations).  Returns HPLAI_ENOTCONV on failure. */
+ * number of residual evaluations).  Returns HPLAI_ENOTCONV on failure.
+ * mode HPLAI_IR corrects with x += U^{-1} L^{-1} r as the reference does;
+ * HPLAI_GMRES corrects with one cycle of FP64 GMRES(restart) on
+ * (LU)^{-1} A d = (LU)^{-1} r, same residual, harness and stopping test. */
 int hplai_refine(hplai_ctx *ctx, int mode, int maxit, hplai_ir_errors *err, int *iters);
+/* GMRES parameters: restart length (1..31, default 30) and the relative
+ * reduction of the preconditioned residual that ends a cycle (default 1e-12). */
+int hplai_set_gmres(hplai_ctx *ctx, int restart, double tol);
+/* Residual evaluations and GMRES inner steps of the last hplai_refine. */
+int hplai_get_refine_counts(hplai_ctx *ctx, int *outer, int *inner);
 
 /* Copies of the results. */
 int hplai_get_x(hplai_ctx *ctx, double *x);                      /* n doubles */
@@ -149,7 +157,8 @@ void *hplai_get_stream(hplai_ctx *ctx);
 int hplai_get_norms(hplai_ctx *ctx, double *norma, double *normb);
 
 /* One end-to-end solve through host buffers: upload, factor, refine and
- * copy x back (the whole of main.cpp's timed region plus the transfers). */
+ * copy x back (the whole of main.cpp's timed region plus the transfers).
+ * Refines with HPLAI_IR, or HPLAI_GMRES for an HPLAI_F32_F8 context. */
 int hplai_solve_host(hplai_ctx *ctx, const float *a, int64_t lda, const double *rhs,
 	const double *diag, uint64_t seed, int maxit, double *x, hplai_ir_errors *err, int *iters);
 
@@ -199,6 +208,25 @@ int hplai_trsm_left_lower(int b, int ncols, const float *l, int64_t ldl, float *
  * ldlh and lduh are multiples of 8 and the buffers 16-byte aligned. */
 int hplai_shgemm_minus(int m, int n, int k, const uint16_t *lh, int64_t ldlh,
 	const uint16_t *uh, int64_t lduh, float *c, int64_t ldc, void *stream);
+
+/* Precision form (no reference counterpart; the down-cast follows
+ * convert_left/right_panels, panel_trf.hpp:173-233, with one factor per 128
+ * rows instead of one global factor).  X is rows x k FP32, element (r, p) at
+ * src[r + p*lds] (col_major, an L panel) or src[p + r*lds] (a U panel read
+ * by columns).  For each block of 128 rows, e = the exponent with
+ * max|X_blk| = f 2^e, f in [0.5, 1) after dividing by 448; then
+ * dst[r*ld8 + p] = e4m3_rn(X[r,p] 2^(-e)) (bytes k..ld8 of a row zero) and
+ * scale[r/128] = 2^e.  ld8 is a multiple of 128; `bits` is scratch for
+ * rows/128 + 1 words. */
+int hplai_quantize_e4m3(int rows, int k, const float *src, int64_t lds, int col_major, uint8_t *dst,
+	int64_t ld8, float *scale, unsigned *bits, void *stream);
+
+/* C (m x n FP32, ldc) -= diag(sl) L8 U8^T diag(su): e4m3 operands row-major
+ * with K contiguous (l8[i*ldl + p], u8[j*ldu + p]), exact products
+ * accumulated in FP32 on tcgen05 (kind::f8f6f4) and scaled by the
+ * power-of-two factors sl[i/128] su[j/128] before the update. */
+int hplai_f8gemm_minus(int m, int n, int k, const uint8_t *l8, int64_t ldl, const float *sl,
+	const uint8_t *u8, int64_t ldu, const float *su, float *c, int64_t ldc, void *stream);
 
 /* Workspace bytes for hplai_otf_gemv at order n. */
 size_t hplai_otf_gemv_workspace(int n);

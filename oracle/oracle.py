@@ -18,8 +18,8 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 
 def build() -> str:
     """Compile liboracle.so with the Makefile next to this file (gcc, seconds)."""
-    src = os.path.join(HERE, "hplai_oracle.c")
-    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    srcs = [os.path.join(HERE, f) for f in ("hplai_oracle.c", "hplai_oracle_f8.c", "Makefile")]
+    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(os.path.getmtime(s) for s in srcs):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 
@@ -56,6 +56,10 @@ _trsv_u = _proto("orc_trsv_upper", None, _int, _int, _vp, _i64, _vp)
 _refine = _proto("orc_refine", _int, _int, _int, _int, _vp, _i64, _u64, _vp, _vp, _int, _vp, _vp, _vp,
                  ctypes.POINTER(_int), _dp, _dp)
 _solve = _proto("orc_solve", _int, _int, _int, _int, _u64, _int, _vp, _vp, _vp, ctypes.POINTER(_int), _dp, _dp)
+_e4m3_rn = _proto("orc_e4m3_rn", ctypes.c_uint8, ctypes.c_float)
+_e4m3_to_f32 = _proto("orc_e4m3_to_f32", ctypes.c_float, ctypes.c_uint8)
+_quantize_e4m3 = _proto("orc_quantize_e4m3", None, _int, _int, _vp, _i64, _int, _vp, _i64, _vp)
+_f8gemm = _proto("orc_f8gemm_minus", None, _int, _int, _int, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _i64)
 
 
 def _p(a: np.ndarray) -> int:
@@ -196,3 +200,42 @@ def dense_matrix_f64(n, seed=42) -> np.ndarray:
             col = col * an + cn
     a[np.arange(n), np.arange(n)] = diag(n, seed)
     return a
+
+
+def e4m3_rn(x: float) -> int:
+    return int(_e4m3_rn(x))
+
+
+def e4m3_to_f32(b: int) -> float:
+    return float(_e4m3_to_f32(b))
+
+
+def quantize_e4m3(x: np.ndarray, col_major: bool, ld8: int = None):
+    """e4m3 copy of the rows x k panel X with one power-of-two factor per 128
+    rows.  col_major: X given as an (rows, k) array read down columns (an L
+    panel); else X given as (rows, k) with k contiguous in memory.  Returns
+    (bytes (rows, ld8) uint8, scale (ceil(rows/128),) float32)."""
+    x = np.asarray(x, dtype=np.float32)
+    rows, k = x.shape
+    ld8 = ld8 or (k + 127) // 128 * 128
+    if col_major:
+        src = np.asfortranarray(x)
+        lds = max(rows, 1)
+    else:
+        src = np.ascontiguousarray(x)
+        lds = k
+    dst = np.zeros((rows, ld8), dtype=np.uint8)
+    scale = np.zeros((rows + 127) // 128, dtype=np.float32)
+    _quantize_e4m3(rows, k, _p(src), lds, 1 if col_major else 0, _p(dst), ld8, _p(scale))
+    return dst, scale
+
+
+def f8gemm_minus(c: np.ndarray, l8: np.ndarray, sl: np.ndarray, u8: np.ndarray, su: np.ndarray, k: int) -> np.ndarray:
+    """C - diag(sl) L8 U8^T diag(su), FP64 sums of the exact e4m3 products."""
+    c = np.array(c, dtype=np.float32, order="F", copy=True)
+    l8 = np.ascontiguousarray(l8, dtype=np.uint8)
+    u8 = np.ascontiguousarray(u8, dtype=np.uint8)
+    m, n = c.shape
+    _f8gemm(m, n, k, _p(l8), l8.shape[1], _p(np.ascontiguousarray(sl, dtype=np.float32)), _p(u8), u8.shape[1],
+            _p(np.ascontiguousarray(su, dtype=np.float32)), _p(c), m)
+    return c

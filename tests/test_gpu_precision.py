@@ -1,0 +1,158 @@
+"""The precision form (e4m3 Schur update) and GMRES refinement on the B200.
+
+The e4m3 down-cast is integer-exact work (a power-of-two factor per 128
+rows, then round-to-nearest-even), so the device bytes and factors must
+equal the oracle's restatement bit for bit.  The e4m3 GEMM forms exact
+products and sums them in FP32 on the tensor cores, so it is checked
+against FP64 sums of the same products with a stated tolerance.  Whole
+solves have no reference counterpart: they must reach hpl-harness < 16 and
+agree with a dense FP64 solve of the same matrix.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def panel_values(rng, rows, k):
+    """Panel-like values whose magnitude changes from one 128-row block to the
+    next (one block all zero, one tiny enough to reach e4m3 subnormals)."""
+    x = rng.uniform(-1.0, 1.0, (rows, k)).astype(np.float32)
+    for blk in range((rows + 127) // 128):
+        x[blk * 128:(blk + 1) * 128] *= np.float32(2.0) ** int(rng.integers(-20, 6))
+    if rows > 256:
+        x[128:256] = 0.0
+    x[::37, ::5] *= np.float32(1e-4)   # values far below the block maximum
+    return x
+
+
+@pytest.mark.parametrize("rows,k", [(1000, 60), (777, 512), (300, 1024), (128, 128)])
+@pytest.mark.parametrize("col_major", [True, False])
+def test_quantize_e4m3_bit_exact(hplai, oracle, torch_cuda, rows, k, col_major):
+    torch = torch_cuda
+    rng = np.random.default_rng(rows * 7 + k)
+    x = panel_values(rng, rows, k)
+    ld8 = (k + 127) // 128 * 128
+    if col_major:
+        src = torch.from_numpy(np.ascontiguousarray(x.T)).cuda()     # column p of x contiguous, ld = rows
+        lds = rows
+    else:
+        src = torch.from_numpy(np.ascontiguousarray(x)).cuda()       # row r contiguous, ld = k
+        lds = k
+    dst = torch.full((rows, ld8), 0xAB, dtype=torch.uint8, device="cuda")
+    scale = torch.zeros((rows + 127) // 128, dtype=torch.float32, device="cuda")
+    bits = torch.zeros((rows + 127) // 128 + 1, dtype=torch.int32, device="cuda")
+    hplai.check(hplai.quantize_e4m3(rows, k, src.data_ptr(), lds, 1 if col_major else 0, dst.data_ptr(), ld8,
+                                    scale.data_ptr(), bits.data_ptr(), None))
+    torch.cuda.synchronize()
+    ref8, refs = oracle.quantize_e4m3(x, col_major=True, ld8=ld8)
+    assert np.array_equal(scale.cpu().numpy(), refs)
+    got = dst.cpu().numpy()
+    assert np.array_equal(got, ref8), f"{np.count_nonzero(got != ref8)} bytes differ"
+
+
+def test_quantize_e4m3_rejects_bad_ld(hplai):
+    assert hplai.quantize_e4m3(10, 60, 0, 10, 1, 0, 100, 0, 0, None) == hplai.HPLAI_EINVAL
+
+
+@pytest.mark.parametrize("m,n,k", [(700, 500, 256), (1000, 1000, 60), (256, 384, 1024), (129, 131, 512)])
+def test_f8gemm_minus_vs_fp64_products(hplai, oracle, torch_cuda, m, n, k):
+    torch = torch_cuda
+    rng = np.random.default_rng(m + n + k)
+    l8, sl = oracle.quantize_e4m3(panel_values(rng, m, k), col_major=True)
+    u8, su = oracle.quantize_e4m3(panel_values(rng, n, k), col_major=False)
+    c = np.asfortranarray(rng.uniform(-1, 1, (m, n)).astype(np.float32))
+    cd = torch.from_numpy(np.ascontiguousarray(c.T)).cuda()
+    l8d, u8d = torch.from_numpy(l8).cuda(), torch.from_numpy(u8).cuda()
+    sld, sud = torch.from_numpy(sl).cuda(), torch.from_numpy(su).cuda()
+    hplai.check(hplai.f8gemm_minus(m, n, k, l8d.data_ptr(), l8.shape[1], sld.data_ptr(), u8d.data_ptr(), u8.shape[1],
+                                   sud.data_ptr(), cd.data_ptr(), m, None))
+    torch.cuda.synchronize()
+    got = np.asfortranarray(cd.cpu().numpy().T)
+    ref = oracle.f8gemm_minus(c, l8, sl, u8, su, k)
+    # bound: FP32 summation of k exact products, then one rounding of the update
+    lv = np.vectorize(oracle.e4m3_to_f32)(l8[:, :k]).astype(np.float64) * np.repeat(sl, 128)[:m, None]
+    uv = np.vectorize(oracle.e4m3_to_f32)(u8[:, :k]).astype(np.float64) * np.repeat(su, 128)[:n, None]
+    mag = np.abs(lv) @ np.abs(uv).T
+    tol = 2.0 ** -19 * mag + 2.0 ** -22 * np.abs(ref)
+    err = np.abs(got.astype(np.float64) - ref)
+    assert np.all(err <= tol), f"max err/tol {np.max(err / np.maximum(tol, 1e-300)):.3g}"
+
+
+def dense_solution(oracle, n, seed=42):
+    a = oracle.dense_matrix_f64(n, seed)
+    return np.linalg.solve(a, oracle.rhs(n, seed))
+
+
+@pytest.mark.parametrize("precision,mode", [(1, 1), (0, 1)])
+def test_c1_solve_precision_and_mode(hplai, oracle, torch_cuda, precision, mode):
+    n, b = 1200, 60
+    with hplai.Solver(n, b, precision=precision) as s:
+        s.generate(42)
+        s.factor()
+        res = s.iterative_refinement(50, mode=mode)
+        outer, inner = s.refine_counts()
+        x = s.x()
+    assert res.status == hplai.HPLAI_OK and res.hpl_harness < 16.0, (res, outer, inner)
+    assert inner >= 1 and outer <= 4
+    xs = dense_solution(oracle, n)
+    rel = np.max(np.abs(x - xs)) / np.max(np.abs(xs))
+    assert rel < 1e-11, rel
+
+
+@pytest.mark.parametrize("n,b", [(8192, 512), (4096, 1024), (6144, 256)])
+def test_fp8_gmres_converges(hplai, torch_cuda, n, b):
+    with hplai.Solver(n, b, precision=hplai.F32_F8) as s:
+        s.generate(42)
+        s.factor()
+        res = s.iterative_refinement(50, mode=hplai.GMRES)
+        outer, inner = s.refine_counts()
+        log = s.ir_log()
+    assert res.status == hplai.HPLAI_OK and res.hpl_harness < 16.0, (res, log)
+    # one GMRES cycle per residual evaluation; a few residual evaluations in all
+    assert outer <= 4 and inner <= 30 * (outer - 1), (outer, inner)
+
+
+def test_fp8_classical_ir_still_terminates(hplai, torch_cuda):
+    """The e4m3 factor with the reference's classical correction: either it
+    converges or it stops with {-1,-1} (never a hang or an error)."""
+    with hplai.Solver(4096, 512, precision=hplai.F32_F8) as s:
+        s.generate(42)
+        s.factor()
+        res = s.iterative_refinement(50, mode=hplai.IR)
+    assert res.status in (hplai.HPLAI_OK, hplai.HPLAI_ENOTCONV)
+    if res.status == hplai.HPLAI_OK:
+        assert res.hpl_harness < 16.0
+    else:
+        assert (res.residual, res.hpl_harness) == (-1.0, -1.0)
+
+
+def test_fp8_factor_close_to_fp16_factor(hplai, torch_cuda):
+    """Each e4m3 rounding moves a panel value by at most 2^-4 relative, so the
+    two factors of the same matrix differ by a few percent of the Schur
+    contribution, far below the diagonal."""
+    n, b = 2048, 256
+    lus = []
+    for prec in (hplai.F32_F16, hplai.F32_F8):
+        with hplai.Solver(n, b, precision=prec) as s:
+            s.generate(42)
+            s.factor()
+            lus.append(s.lu().astype(np.float64))
+    d = np.abs(lus[0] - lus[1])
+    assert np.max(d) < 0.05, np.max(d)
+    assert np.all(np.isfinite(lus[1]))
+
+
+def test_gmres_parameters_validated(hplai, torch_cuda):
+    with hplai.Solver(512, 128) as s:
+        with pytest.raises(hplai.HplaiError):
+            s.set_gmres(0, 1e-12)
+        with pytest.raises(hplai.HplaiError):
+            s.set_gmres(32, 1e-12)
+        with pytest.raises(hplai.HplaiError):
+            s.set_gmres(10, 0.0)
+        s.set_gmres(5, 1e-10)
+        s.generate(42)
+        s.factor()
+        res = s.iterative_refinement(50, mode=hplai.GMRES)
+        assert res.status == hplai.HPLAI_OK

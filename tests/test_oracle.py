@@ -161,3 +161,37 @@ def test_nonconvergence_reports_minus_one(oracle):
     bad = np.eye(n, dtype=np.float32, order="F") * 1e-3
     rc, x, res, har, steps = oracle.refine(bad, b, 42, oracle.rhs(n), oracle.diag(n), maxit=3)
     assert rc == 1 and res == -1.0 and har == -1.0 and len(steps) == 3
+
+
+def test_e4m3_restatement_matches_torch_conversion(oracle):
+    """The oracle's e4m3 rounding (restated from the format definition) agrees
+    with torch's independent float -> float8_e4m3fn conversion on a dense sweep
+    of the finite range and on random values across 20 binades."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(1)
+    xs = np.concatenate([np.linspace(-448, 448, 100001, dtype=np.float32),
+                         (rng.standard_normal(100000) * np.float32(2.0) ** rng.integers(-14, 8, 100000))
+                         .astype(np.float32)])
+    xs = np.clip(xs, -448, 448)
+    mine = np.fromiter((oracle.e4m3_rn(float(v)) for v in xs), dtype=np.uint8, count=len(xs))
+    ref = torch.from_numpy(xs.copy()).to(torch.float8_e4m3fn).view(torch.uint8).numpy()
+    assert np.array_equal(mine, ref)
+    for b in range(256):
+        if (b & 0x7F) != 0x7F:
+            assert oracle.e4m3_rn(oracle.e4m3_to_f32(b)) == b
+
+
+def test_quantize_e4m3_block_factors(oracle):
+    """One power-of-two factor per 128 rows; the scaled block maximum lies in
+    [224, 448]; an all-zero block gets factor 1 and zero bytes."""
+    rng = np.random.default_rng(5)
+    x = rng.uniform(-1, 1, (300, 60)).astype(np.float32)
+    x[:128] *= 1e-3
+    x[128:256] = 0
+    q, s = oracle.quantize_e4m3(x, col_major=True)
+    assert q.shape == (300, 128) and s.shape == (3,)
+    assert s[1] == 1.0 and not q[128:256].any() and not q[:, 60:].any()
+    for blk in (0, 2):
+        amax = np.abs(x[blk * 128:(blk + 1) * 128]).max() / s[blk]
+        assert 224.0 <= amax < 448.0
+        assert np.log2(s[blk]) == int(np.log2(s[blk]))
