@@ -64,12 +64,14 @@ struct hplai_ctx {
 	int64_t ld8 = 0;
 	SchurMaps maps8[2];
 	TcPanels tc;
-	float *tcbuf = nullptr;   // phi, plo (n x ldp) and the four b x ldp inverse buffers
+	float *tcbuf = nullptr;   // phi, plo (n x ldp), the four b x ldp inverse buffers, the inversion work
 	double *rhs = nullptr, *d = nullptr, *x = nullptr, *r = nullptr, *scal = nullptr;
 	void *gemv_work = nullptr;
 	size_t gemv_bytes = 0;
 	void *trsv_work = nullptr;
 	size_t trsv_bytes = 0;
+	void *getrf_work = nullptr;   // tile flags of the diagonal block LU
+	uint32_t getrf_epoch = 0;
 	cudaStream_t st = nullptr;    // main stream: Schur updates, refinement, everything else
 	cudaStream_t st2 = nullptr;   // side stream (high priority): diagonal block + panels
 	cudaEvent_t ev_panel = nullptr, ev_next = nullptr;
@@ -113,6 +115,7 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->scal);
 	cudaFree(c->gemv_work);
 	cudaFree(c->trsv_work);
+	cudaFree(c->getrf_work);
 	cudaFree(c->gm_v);
 	cudaFree(c->gm_w);
 	cudaFree(c->gm_small);
@@ -255,7 +258,8 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		CTX_ALLOC(c->qbits, sizeof(unsigned) * nblk128);
 	}
 	const int64_t ldp = round_up(b, 32);
-	const size_t tc_elems = static_cast<size_t>(ldp) * (2 * static_cast<size_t>(n) + 4 * static_cast<size_t>(b));
+	const size_t tc_elems = static_cast<size_t>(ldp) * (2 * static_cast<size_t>(n) + 4 * static_cast<size_t>(b)) +
+		tc_inverse_work_elems(ldp);
 	CTX_ALLOC(c->tcbuf, sizeof(float) * tc_elems);
 	CTX_ALLOC(c->rhs, sizeof(double) * n);
 	CTX_ALLOC(c->d, sizeof(double) * n);
@@ -266,7 +270,10 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	CTX_ALLOC(c->gemv_work, c->gemv_bytes);
 	c->trsv_bytes = trsv_workspace(n);
 	CTX_ALLOC(c->trsv_work, c->trsv_bytes);
-	if (cudaMemset(c->trsv_work, 0, c->trsv_bytes) != cudaSuccess) {
+	CTX_ALLOC(c->getrf_work, getrf_workspace());
+	if (cudaMemset(c->trsv_work, 0, c->trsv_bytes) != cudaSuccess ||
+		cudaMemset(c->getrf_work, 0, getrf_workspace()) != cudaSuccess ||
+		cudaMemset(c->tcbuf, 0, sizeof(float) * tc_elems) != cudaSuccess) {
 		ctx_free(c);
 		return HPLAI_ECUDA;
 	}
@@ -283,7 +290,7 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		float *base = c->tcbuf;
 		const size_t pn = static_cast<size_t>(ldp) * n, pb = static_cast<size_t>(ldp) * b;
 		s = tc_panels_make(&c->tc, n, b, base, base + pn, ldp, base + 2 * pn, base + 2 * pn + pb,
-			base + 2 * pn + 2 * pb, base + 2 * pn + 3 * pb);
+			base + 2 * pn + 2 * pb, base + 2 * pn + 3 * pb, base + 2 * pn + 4 * pb);
 	}
 	if (s != HPLAI_OK) {
 		ctx_free(c);
@@ -339,7 +346,7 @@ int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStrea
 	const int64_t kb = static_cast<int64_t>(k) * b;
 	float *diag = c->A + kb + kb * lda;
 	HPLAI_TRY(pe.record(st, HPLAI_PH_DIAG_LU));
-	HPLAI_TRY(launch_getrf(b, diag, lda, st));
+	HPLAI_TRY(launch_getrf_tiles(b, diag, lda, c->getrf_work, &c->getrf_epoch, side_ctas, st));
 	HPLAI_TRY(pe.end(st));
 	if (k == c->nb - 1) return HPLAI_OK;
 	const int rem = n - static_cast<int>(kb) - b;
@@ -395,6 +402,7 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	const int n = c->n, b = c->b, nb = c->nb;
 	schur_status_reset();
 	tc_status_reset();
+	HPLAI_CUDA_TRY(cudaMemsetAsync(c->getrf_work, 0, sizeof(uint32_t), c->st));   // its status word
 	const bool simt = (c->flags & HPLAI_FLAG_SIMT_PANELS) != 0;
 	const bool serial = (c->flags & HPLAI_FLAG_LOOKAHEAD) == 0;
 	for (double &v : c->phase_ms) v = 0.0;
@@ -440,6 +448,11 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	pe.collect(c->phase_ms);
 	HPLAI_TRY(schur_status());
 	HPLAI_TRY(tc_status());
+	{
+		int gs = HPLAI_OK;
+		HPLAI_TRY(getrf_status(c->getrf_work, st, &gs));
+		HPLAI_TRY(gs);
+	}
 	c->factored = true;
 	return HPLAI_OK;
 }

@@ -20,6 +20,14 @@ int launch_diag(int n, int i0, int count, double *d, float *adiag, int64_t lda, 
 int launch_rhs(int n, double *rhs, uint64_t seed, cudaStream_t st);
 
 // panel.cu
+// getrf.cu: tile-parallel diagonal block LU (bit-exact with the sequential
+// order).  `work` holds getrf_workspace() bytes, zeroed once; `epoch` is
+// the host-side launch counter that goes with it.  launch_getrf is the
+// leaf entry point's form on a library-owned workspace (it waits for the
+// result and returns the kernel's status).
+size_t getrf_workspace();
+int launch_getrf_tiles(int b, float *a, int64_t lda, void *work, uint32_t *epoch, int max_ctas, cudaStream_t st);
+int getrf_status(void *work, cudaStream_t st, int *status);
 int launch_getrf(int b, float *a, int64_t lda, cudaStream_t st);
 int launch_trsm_right_upper(int m, int b, const float *u, int64_t ldu, float *a, int64_t lda, uint16_t *lh,
 	int64_t ldh, float scale, cudaStream_t st);
@@ -79,9 +87,12 @@ struct TcPanels {
 	int64_t ldp;                     // row pitch of every buffer below, a multiple of 32 floats
 	float *phi, *plo;                // n x ldp: K-major hi/lo copy of the current panel
 	float *uhi, *ulo, *lhi, *llo;    // b x ldp: hi/lo of U11^{-1} and L11^{-1}
+	float *xu, *xl, *wu, *wl;        // ldp x ldp FP32 work of the inversion (zeroed once)
 };
+// `work` holds tc_inverse_work_elems(ldp) floats, zeroed before first use.
+inline size_t tc_inverse_work_elems(int64_t ldp) { return 4 * static_cast<size_t>(ldp) * static_cast<size_t>(ldp); }
 int tc_panels_make(TcPanels *t, int n, int b, float *phi, float *plo, int64_t ldp, float *uhi, float *ulo,
-	float *lhi, float *llo);
+	float *lhi, float *llo, float *work);
 int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStream_t st);
 // A_col (rem x b) <- A_col U11^{-1}; lh row i = half(scale * A_col row i)
 int launch_lpanel_tc(const TcPanels &t, int rem, float *acol, int64_t lda, uint16_t *lh, int64_t ldh, float scale,

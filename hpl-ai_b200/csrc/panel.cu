@@ -1,6 +1,5 @@
 // panel.cu -- FP32 panel factorisation kernels for the blocked no-pivot LU.
 //
-//  getrf_kernel     : b x b diagonal block LU in one CTA (getrf_nopiv.hpp:30-141)
 //  trsm_kernel      : L panel  A_col <- A_col * U^{-1}, plus its FP16 copy
 //                     (update_left_panels + convert_left_panels, panel_trf.hpp:143-157,182-207)
 //                     U panel  A_row <- L^{-1} * A_row, plus its FP16 copy, as the
@@ -17,169 +16,6 @@
 
 namespace hplai {
 
-// ---------------------------------------------------------------------------
-// Diagonal block LU.  One CTA of 512 threads; each thread owns up to two rows
-// of the current column panel, so b <= 1024.
-// ---------------------------------------------------------------------------
-constexpr int kGetrfThreads = 512;
-
-template <int NB>
-__global__ void __launch_bounds__(kGetrfThreads, 1) getrf_kernel(int b, float *__restrict__ a, int64_t lda)
-{
-	extern __shared__ float sm[];
-	const int ldu = (b + 3) & ~3;  // U12 row stride, a multiple of 4 for float4 reads
-	float *Lp = sm;                // panel, column-major: Lp[c*b + r], r relative to kb
-	float *Up = sm + b * NB;       // U12 rows: Up[i*ldu + c], c relative to kb+w
-	float *prow = Up + NB * ldu;   // two pivot-row buffers of NB floats
-	const int t = threadIdx.x;
-
-	for (int kb = 0; kb < b; kb += NB) {
-		const int w = min(NB, b - kb);
-		const int mrows = b - kb;
-		const int rem = mrows - w;
-
-		// Phase 1: factor the (b-kb) x w column panel; rows t and t+512.
-		float p0[NB], p1[NB];
-		const bool own0 = t < mrows, own1 = t + kGetrfThreads < mrows;
-#pragma unroll
-		for (int c = 0; c < NB; ++c) {
-			p0[c] = (own0 && c < w) ? a[static_cast<int64_t>(kb + c) * lda + kb + t] : 0.f;
-			p1[c] = (own1 && c < w) ? a[static_cast<int64_t>(kb + c) * lda + kb + t + kGetrfThreads] : 0.f;
-		}
-#pragma unroll
-		for (int j = 0; j < NB; ++j) {
-			if (j < w) {
-				float *pr = prow + (j & 1) * NB;
-				if (t == j) {
-#pragma unroll
-					for (int c = 0; c < NB; ++c) pr[c] = p0[c];
-				}
-				__syncthreads();
-				const float inv = 1.0f / pr[j];
-				if (own0 && t > j) {
-					const float l = p0[j] * inv;
-					p0[j] = l;
-#pragma unroll
-					for (int c = j + 1; c < NB; ++c)
-						if (c < w) p0[c] = fmaf(-l, pr[c], p0[c]);
-				}
-				if (own1) {
-					const float l = p1[j] * inv;
-					p1[j] = l;
-#pragma unroll
-					for (int c = j + 1; c < NB; ++c)
-						if (c < w) p1[c] = fmaf(-l, pr[c], p1[c]);
-				}
-			}
-		}
-#pragma unroll
-		for (int c = 0; c < NB; ++c) {
-			if (c < w) {
-				if (own0) {
-					a[static_cast<int64_t>(kb + c) * lda + kb + t] = p0[c];
-					Lp[c * b + t] = p0[c];
-				}
-				if (own1) {
-					a[static_cast<int64_t>(kb + c) * lda + kb + t + kGetrfThreads] = p1[c];
-					Lp[c * b + t + kGetrfThreads] = p1[c];
-				}
-			}
-		}
-		__syncthreads();
-		if (rem <= 0) break;
-
-		// Phase 2: U12 = L11^{-1} A12 (unit lower), one column per thread.
-		for (int cc = t; cc < rem; cc += kGetrfThreads) {
-			float q[NB];
-			float *colp = a + static_cast<int64_t>(kb + w + cc) * lda + kb;
-#pragma unroll
-			for (int i = 0; i < NB; ++i) q[i] = (i < w) ? colp[i] : 0.f;
-#pragma unroll
-			for (int k = 0; k < NB; ++k) {
-#pragma unroll
-				for (int i = k + 1; i < NB; ++i)
-					if (i < w) q[i] = fmaf(-q[k], Lp[k * b + i], q[i]);
-			}
-#pragma unroll
-			for (int i = 0; i < NB; ++i) {
-				if (i < w) {
-					colp[i] = q[i];
-					Up[i * ldu + cc] = q[i];
-				}
-			}
-		}
-		__syncthreads();
-
-		// Phase 3: A22 -= L21 * U12.  Warp items of 256 rows x 4 columns;
-		// lane owns rows lane + 32*i.  Each element is updated in increasing p.
-		{
-			const int warp = t >> 5, lane = t & 31;
-			const int rblocks = (rem + 255) / 256;
-			const int cblocks = (rem + 3) / 4;
-			const bool vec = (ldu % 4 == 0);
-			for (int item = warp; item < rblocks * cblocks; item += kGetrfThreads / 32) {
-				const int rb = item % rblocks, cbk = item / rblocks;
-				const int r0 = rb * 256 + lane, c0 = cbk * 4;
-				float acc[8][4];
-#pragma unroll
-				for (int i = 0; i < 8; ++i)
-#pragma unroll
-					for (int j = 0; j < 4; ++j) {
-						const int r = r0 + 32 * i, c = c0 + j;
-						acc[i][j] = (r < rem && c < rem)
-							? a[static_cast<int64_t>(kb + w + c) * lda + kb + w + r] : 0.f;
-					}
-				for (int pp = 0; pp < w; ++pp) {
-					float lv[8], uv[4];
-#pragma unroll
-					for (int i = 0; i < 8; ++i) {
-						const int r = r0 + 32 * i;
-						lv[i] = (r < rem) ? Lp[pp * b + w + r] : 0.f;
-					}
-					if (vec) {
-						const float4 u4 = *reinterpret_cast<const float4 *>(&Up[pp * ldu + c0]);
-						uv[0] = u4.x; uv[1] = u4.y; uv[2] = u4.z; uv[3] = u4.w;
-					} else {
-#pragma unroll
-						for (int j = 0; j < 4; ++j) uv[j] = Up[pp * ldu + c0 + j];
-					}
-#pragma unroll
-					for (int i = 0; i < 8; ++i)
-#pragma unroll
-						for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(-lv[i], uv[j], acc[i][j]);
-				}
-#pragma unroll
-				for (int i = 0; i < 8; ++i)
-#pragma unroll
-					for (int j = 0; j < 4; ++j) {
-						const int r = r0 + 32 * i, c = c0 + j;
-						if (r < rem && c < rem) a[static_cast<int64_t>(kb + w + c) * lda + kb + w + r] = acc[i][j];
-					}
-			}
-		}
-		__syncthreads();
-	}
-}
-
-template <int NB>
-static int getrf_launch(int b, float *a, int64_t lda, cudaStream_t st)
-{
-	const int ldu = (b + 3) & ~3;
-	const size_t smem = (static_cast<size_t>(b) * NB + static_cast<size_t>(NB) * ldu + 2 * NB) * sizeof(float);
-	HPLAI_CUDA_TRY(cudaFuncSetAttribute(getrf_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		static_cast<int>(smem)));
-	getrf_kernel<NB><<<1, kGetrfThreads, smem, st>>>(b, a, lda);
-	count_launches();
-	HPLAI_CUDA_TRY(cudaGetLastError());
-	return HPLAI_OK;
-}
-
-int launch_getrf(int b, float *a, int64_t lda, cudaStream_t st)
-{
-	if (b <= 0 || b > 1024) return HPLAI_EINVAL;
-	if (b <= 640) return getrf_launch<32>(b, a, lda, st);
-	return getrf_launch<16>(b, a, lda, st);
-}
 
 // ---------------------------------------------------------------------------
 // Panel TRSM + FP16 copy, one kernel for both panels.

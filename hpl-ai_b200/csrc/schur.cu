@@ -34,16 +34,43 @@ namespace {
 constexpr int BM = 128;
 constexpr int BN = 256;
 constexpr int BK = 64;                 // one 128-byte swizzle row of FP16 (128 FP8 values)
-constexpr int STAGES = 4;
+// Pipeline shape (build-time tunables): operand stages, epilogue warps (4,
+// or 8 = two per TMEM lane quarter, each taking half of the tile's
+// columns) and staging buffers per epilogue warp.
+#ifndef HPLAI_SCHUR_STAGES
+#define HPLAI_SCHUR_STAGES 4
+#endif
+#ifndef HPLAI_SCHUR_EPI_WARPS
+#define HPLAI_SCHUR_EPI_WARPS 4
+#endif
+#ifndef HPLAI_SCHUR_EPI_BUFS
+#define HPLAI_SCHUR_EPI_BUFS 2
+#endif
+// Reduce box: 32 rows (one warp's TMEM quarter) or the tile's full 128 rows
+// (the four epilogue warps stage one chunk together; 512-byte column runs).
+#ifndef HPLAI_SCHUR_TALL_BOX
+#define HPLAI_SCHUR_TALL_BOX 1
+#endif
+#ifndef HPLAI_SCHUR_EPI_CHUNK
+#define HPLAI_SCHUR_EPI_CHUNK 32
+#endif
+constexpr int STAGES = HPLAI_SCHUR_STAGES;
 constexpr int A_BYTES = BM * BK * 2;   // 16 KB
 constexpr int B_BYTES = BN * BK * 2;   // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-constexpr int EPI_WARPS = 4;
+constexpr int EPI_WARPS = HPLAI_SCHUR_EPI_WARPS;
+constexpr int EPI_BUFS = HPLAI_SCHUR_EPI_BUFS;
+constexpr int EPI_SPLIT = EPI_WARPS / 4;            // warps per TMEM lane quarter
+constexpr int EPI_COLS = BN / EPI_SPLIT;            // accumulator columns per epilogue warp
 constexpr int THREADS = (2 + EPI_WARPS) * 32;
+static_assert(EPI_WARPS == 4 || EPI_WARPS == 8, "one or two epilogue warps per lane quarter");
 constexpr uint32_t TMEM_COLS = 2 * BN;
-constexpr int EPI_CHUNK = 32;                       // columns per epilogue chunk
-constexpr int EPI_BUF_BYTES = 32 * EPI_CHUNK * 4;   // one warp's 32 rows x 32 columns FP32
-constexpr size_t RED_BYTES = static_cast<size_t>(EPI_WARPS) * 2 * EPI_BUF_BYTES;
+constexpr bool TALL = HPLAI_SCHUR_TALL_BOX != 0;
+constexpr int EPI_CHUNK = HPLAI_SCHUR_EPI_CHUNK;    // columns per epilogue chunk
+constexpr int EPI_BUF_BYTES = 32 * EPI_CHUNK * 4;   // one warp's 32 rows x EPI_CHUNK columns FP32
+static_assert(!TALL || EPI_WARPS == 4, "the tall box is staged by the four lane-quarter warps");
+static_assert(TALL || EPI_CHUNK == 32, "per-warp boxes are 32 x 32");
+constexpr size_t RED_BYTES = static_cast<size_t>(EPI_WARPS) * EPI_BUFS * EPI_BUF_BYTES;   // = BM x EPI_CHUNK x EPI_BUFS when tall
 constexpr size_t smem_bytes(bool red) { return static_cast<size_t>(STAGES) * STAGE_BYTES + (red ? RED_BYTES : 0) + 1024 + 256; }
 
 static_assert(TMEM_COLS <= 512, "two accumulators must fit in TMEM");
@@ -63,6 +90,24 @@ struct Params {
 };
 
 __device__ unsigned int g_status;
+
+// Tile order: groups of kGroupM tile rows, each group swept column by column
+// (tile rows fastest).  The CTAs in flight then share a few U blocks and the
+// group's L blocks stay in L2 while the group crosses all tile columns, so
+// each panel is read from HBM about once per group instead of once per tile
+// column (the L panel alone is 256 MB at n = 131072, b = 1024).
+constexpr int kGroupM = 32;
+
+__device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, int &tm, int &tn)
+{
+	const int per_group = kGroupM * tiles_n;
+	const int g = tile / per_group;
+	const int first = g * kGroupM;
+	const int gm = min(kGroupM, tiles_m - first);
+	const int in = tile - g * per_group;
+	tm = first + in % gm;
+	tn = in / gm;
+}
 
 __device__ __forceinline__ void tma_reduce_add_2d(const void *map, const void *smem_src, int x, int y)
 {
@@ -134,7 +179,8 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 		int stage = 0;
 		uint32_t phase = 0;
 		for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
-			const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+			int tm, tn;
+			tile_coords(tile, p.tiles_m, p.tiles_n, tm, tn);
 			if (lane == 0) {
 				for (int kc = 0; kc < p.num_kc; ++kc) {
 					if (!mbar_wait(&empty[stage], phase ^ 1u)) { ok = false; break; }
@@ -195,14 +241,21 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 	} else {
 		// ---------------- epilogue ----------------
 		const int q = warp & 3;   // TMEM lane quarter this warp may access
+		const int cbase = ((warp - 2) / 4) * EPI_COLS;   // first accumulator column of this warp
 		bool ok = true;
 		int acc = 0;
 		uint32_t acc_phase = 0;
 		int epi_buf = 0;
 		for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
-			const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
+			int tm, tn;
+			tile_coords(tile, p.tiles_m, p.tiles_n, tm, tn);
 			const bool mine = mbar_wait(&accf[acc], acc_phase);
-			ok = __all_sync(0xffffffffu, mine) != 0;
+			// the epilogue warps decide together (their named barriers must not split)
+			int all_ok;
+			asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\t"
+			             "bar.red.and.pred q, 1, %2, p;\n\tselp.s32 %0, 1, 0, q;\n\t}"
+			             : "=r"(all_ok) : "r"(mine ? 1 : 0), "n"(EPI_WARPS * 32) : "memory");
+			ok = all_ok != 0;
 			if (!ok) break;
 			tc_fence_after();
 			const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * BN);
@@ -212,24 +265,59 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 				const int lr = p.lrow0 + tm * BM + q * 32 + lane - p.sl0;
 				rs = (tm * BM + q * 32 + lane < p.m) ? p.sl[lr >> 7] : 0.f;
 			}
-			if (RED) {
-				float *mybuf = sEpi + (warp - 2) * 2 * (EPI_BUF_BYTES / 4);
-				const int gx = p.crow0 + tm * BM + q * 32;   // tensor-map row of this warp's lane 0
+			if (RED && TALL) {
+				const bool issuer = (warp == 2 && lane == 0);
 #pragma unroll 1
 				for (int ch = 0; ch < BN / EPI_CHUNK; ++ch) {
+					const int cc = ch * EPI_CHUNK;
+					float *sb = sEpi + (epi_buf % EPI_BUFS) * (BM * EPI_CHUNK);
+					// the reduce issued EPI_BUFS chunks ago read this buffer; let it finish
+					if (issuer) asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(EPI_BUFS - 1) : "memory");
+					asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+#pragma unroll
+					for (int half = 0; half < EPI_CHUNK / 32; ++half) {
+						uint32_t r[32];
+						tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(cc + 32 * half), r);
+						tmem_ld_wait();
+						if (FP8) {
+							const int cb = p.urow0 + tn * BN + cc + 32 * half - p.su0;
+#pragma unroll
+							for (int j = 0; j < 32; ++j) {
+								const float cs = (tn * BN + cc + 32 * half + j < p.n) ? __ldg(&p.su[(cb + j) >> 7]) : 0.f;
+								sb[(32 * half + j) * BM + q * 32 + lane] = -(__uint_as_float(r[j]) * (rs * cs));
+							}
+						} else {
+#pragma unroll
+							for (int j = 0; j < 32; ++j) sb[(32 * half + j) * BM + q * 32 + lane] = -__uint_as_float(r[j]);
+						}
+					}
+					asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+					asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+					if (issuer) {
+						tma_reduce_add_2d(&cmap, sb, p.crow0 + tm * BM, p.ccol0 + tn * BN + cc);
+						asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+					}
+					++epi_buf;
+				}
+			} else if (RED) {
+				float *mybuf = sEpi + (warp - 2) * EPI_BUFS * (EPI_BUF_BYTES / 4);
+				const int gx = p.crow0 + tm * BM + q * 32;   // tensor-map row of this warp's lane 0
+#pragma unroll 1
+				for (int ch = 0; ch < EPI_COLS / EPI_CHUNK; ++ch) {
+					const int cc = cbase + ch * EPI_CHUNK;   // accumulator column of the chunk
 					uint32_t r[32];
-					tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(ch * EPI_CHUNK), r);
+					tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(cc), r);
 					tmem_ld_wait();
-					float *sb = mybuf + (epi_buf & 1) * (EPI_BUF_BYTES / 4);
-					// the reduce issued two chunks ago read this buffer; let it finish
-					if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+					float *sb = mybuf + (epi_buf % EPI_BUFS) * (EPI_BUF_BYTES / 4);
+					// the reduce issued EPI_BUFS chunks ago read this buffer; let it finish
+					if (lane == 0) asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(EPI_BUFS - 1) : "memory");
 					__syncwarp();
 					if (FP8) {
-						const int cb = p.urow0 + tn * BN + ch * EPI_CHUNK - p.su0;
+						const int cb = p.urow0 + tn * BN + cc - p.su0;
 #pragma unroll
 						for (int j = 0; j < 32; ++j) {
 							const int cj = cb + j;
-							const float cs = (tn * BN + ch * EPI_CHUNK + j < p.n) ? __ldg(&p.su[cj >> 7]) : 0.f;
+							const float cs = (tn * BN + cc + j < p.n) ? __ldg(&p.su[cj >> 7]) : 0.f;
 							sb[j * 32 + lane] = -(__uint_as_float(r[j]) * (rs * cs));
 						}
 					} else {
@@ -239,7 +327,7 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 					asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 					__syncwarp();
 					if (lane == 0) {
-						tma_reduce_add_2d(&cmap, sb, gx, p.ccol0 + tn * BN + ch * EPI_CHUNK);
+						tma_reduce_add_2d(&cmap, sb, gx, p.ccol0 + tn * BN + cc);
 						asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 					}
 					++epi_buf;
@@ -249,11 +337,11 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 				const bool rok = row < p.m;
 				float *crow = p.c + row;
 #pragma unroll 1
-				for (int ch = 0; ch < BN / 32; ++ch) {
+				for (int ch = 0; ch < EPI_COLS / 32; ++ch) {
 					uint32_t r[32];
-					tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(ch * 32), r);
+					tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(cbase + ch * 32), r);
 					tmem_ld_wait();
-					const int col0 = tn * BN + ch * 32;
+					const int col0 = tn * BN + cbase + ch * 32;
 					if (rok) {
 						float cv[32];
 #pragma unroll
@@ -398,7 +486,7 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 	bool red = maps.has_cmap && (crow0 % 4 == 0);
 	alignas(64) unsigned char cmap[128];
 	if (red && make_map_2d(cmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, maps.cbase, static_cast<uint64_t>(crow0 + m),
-			static_cast<uint64_t>(ccol0 + n), static_cast<uint64_t>(maps.cld), 32, EPI_CHUNK,
+			static_cast<uint64_t>(ccol0 + n), static_cast<uint64_t>(maps.cld), TALL ? BM : 32, EPI_CHUNK,
 			CU_TENSOR_MAP_SWIZZLE_NONE) != HPLAI_OK)
 		red = false;
 	static bool attr_set = false;

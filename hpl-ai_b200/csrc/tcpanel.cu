@@ -72,90 +72,153 @@ __global__ void __launch_bounds__(256) split_kernel(int rows, int kdim, const fl
 }
 
 // ---------------------------------------------------------------------------
-// Triangular inverse.  X = T^{-1}, T upper triangular b x b:
-//   TRANS_T = false: T = U11, T[p][j] at t[j*ldt + p], non-unit diagonal
-//   TRANS_T = true : T = L11^T, T[p][j] = L[j][p] at t[p*ldt + j], unit diagonal
-// CTA G computes the 32-column block X[:, 32G:32G+32] by block back
-// substitution X[I,G] = T_II^{-1} (E[I,G] - sum_{J>I} T[I,J] X[J,G]), and
-// writes it column-major (X[row][col] at x*[col*ldx + row]) as hi/lo.
+// Triangular inverses by recursive doubling.  X = T^{-1}, T upper triangular
+// and padded with the identity to bp = ldp rows/columns:
+//   TRANS_T = false: T = U11, T[p][j] at lu[j*lda + p], non-unit diagonal
+//   TRANS_T = true : T = L11^T, T[p][j] = L[j][p] at lu[p*lda + j], unit diagonal
+// Level 0 inverts the 32 x 32 diagonal tiles (one warp each, back
+// substitution).  Level l joins pairs of inverted blocks of h = 32 * 2^(l-1):
+//   [A B; 0 C]^{-1} = [A^{-1}, -A^{-1} (B C^{-1}); 0, C^{-1}]
+// as two FP32 products W = B C^{-1}, then -A^{-1} W, each an upper-triangular
+// operand whose zero blocks the tiles skip.  X (work, column-major, ld = ldp)
+// is built in place; its strictly lower part is never written and stays zero.
+// A final pass writes the hi/lo TF32 split of X for the tensor-core panels.
 // ---------------------------------------------------------------------------
 template <bool TRANS_T>
-__device__ __forceinline__ void tri_inv_body(int b, const float *__restrict__ t, int64_t ldt,
-	float *__restrict__ xhi, float *__restrict__ xlo, int64_t ldx)
+__device__ __forceinline__ float tri_t(const float *lu, int64_t lda, int b, int p, int j)
 {
-	extern __shared__ float sm[];
-	float(*Xs)[33] = reinterpret_cast<float(*)[33]>(sm);       // rows 0..32G+31 of the column block
-	float(*Tb)[33] = reinterpret_cast<float(*)[33]>(sm + static_cast<size_t>(b + 32) * 33);   // 32 x 32 block
-	float(*Sb)[33] = Tb + 32;                                   // 32 x 32 right-hand side
-	const int G = blockIdx.x;
-	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	auto tval = [&](int p, int j) -> float {
-		if (p >= b || j >= b) return (p == j) ? 1.f : 0.f;       // identity padding
-		if (TRANS_T) return (p == j) ? 1.f : t[static_cast<int64_t>(p) * ldt + j];
-		return t[static_cast<int64_t>(j) * ldt + p];
-	};
-	for (int I = G; I >= 0; --I) {
-		// S = E[I,G] - sum_{J=I+1..G} T[I,J] X[J,G]; thread: column lane, rows warp + 8r
-		float acc[4];
+	if (p >= b || j >= b) return (p == j) ? 1.f : 0.f;
+	if (p > j) return 0.f;
+	if (TRANS_T) return (p == j) ? 1.f : lu[static_cast<int64_t>(p) * lda + j];
+	return lu[static_cast<int64_t>(j) * lda + p];
+}
+
+// grid (tiles, 2): blockIdx.y = 0 -> U11, 1 -> L11^T; one warp per tile.
+__global__ void __launch_bounds__(32) tri_diag_kernel(int b, const float *__restrict__ lu, int64_t lda,
+	float *__restrict__ xu, float *__restrict__ xl, int64_t ldp)
+{
+	__shared__ float Tb[32][33];
+	const bool lower = blockIdx.y != 0;
+	float *x = lower ? xl : xu;
+	const int o = blockIdx.x * 32, lane = threadIdx.x;
+	for (int i = 0; i < 32; ++i)
+		Tb[i][lane] = lower ? tri_t<true>(lu, lda, b, o + i, o + lane) : tri_t<false>(lu, lda, b, o + i, o + lane);
+	__syncwarp();
+	// column `lane` of the tile's inverse
+	float v[32];
 #pragma unroll
-		for (int r = 0; r < 4; ++r) acc[r] = (I == G && warp + 8 * r == lane) ? 1.f : 0.f;
-		for (int J = I + 1; J <= G; ++J) {
-			__syncthreads();
-			for (int e = tid; e < 1024; e += 256) {
-				const int i = TRANS_T ? (e >> 5) : (e & 31), p = TRANS_T ? (e & 31) : (e >> 5);
-				Tb[i][p] = tval(32 * I + i, 32 * J + p);
-			}
-			__syncthreads();
-#pragma unroll 4
-			for (int p = 0; p < 32; ++p) {
-				const float xv = Xs[32 * J + p][lane];
+	for (int i = 31; i >= 0; --i) {
+		float a = (i == lane) ? 1.f : 0.f;
 #pragma unroll
-				for (int r = 0; r < 4; ++r) acc[r] = fmaf(-Tb[warp + 8 * r][p], xv, acc[r]);
+		for (int p = i + 1; p < 32; ++p) a = fmaf(-Tb[i][p], v[p], a);
+		v[i] = lower ? a : a / Tb[i][i];
+	}
+#pragma unroll
+	for (int i = 0; i < 32; ++i) x[static_cast<int64_t>(o + lane) * ldp + o + i] = v[i];
+}
+
+// One level's products for every pair and both triangles.  grid.x = 64 x 64
+// output tiles of an h x h block (clipped), grid.y = pair, grid.z = triangle.
+//   STEP 0: W[o:o+h, o+h:o+h+h2] = T[o:o+h, o+h:..] X[o+h:.., o+h:..]
+//   STEP 1: X[o:o+h, o+h:..]     = -X[o:o+h, o:o+h] W[o:o+h, o+h:..]
+template <int STEP>
+__global__ void __launch_bounds__(256) tri_level_kernel(int b, int bp, int h, const float *__restrict__ lu, int64_t lda,
+	float *__restrict__ xu, float *__restrict__ xl, float *__restrict__ wu, float *__restrict__ wl, int64_t ldp)
+{
+	__shared__ float As[16][64 + 1];
+	__shared__ float Bs[16][64 + 1];
+	const bool lower = blockIdx.z != 0;
+	float *x = lower ? xl : xu;
+	float *w = lower ? wl : wu;
+	const int o = blockIdx.y * 2 * h;
+	const int h2 = min(h, bp - o - h);   // width of the second half
+	if (h2 <= 0) return;
+	const int tiles_n = (h2 + 63) / 64;
+	const int tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
+	if (tm * 64 >= h) return;
+	const int row0 = o + tm * 64, col0 = o + h + tn * 64;   // output block position in X / W
+	const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+	// K range with nonzero contributions: STEP 0 rows of X_C up to the
+	// tile's last column; STEP 1 columns of X_A from the tile's first row
+	int k_begin, k_end;
+	if (STEP == 0) {
+		k_begin = o + h;
+		k_end = min(o + h + h2, col0 + 64);
+	} else {
+		k_begin = row0;
+		k_end = o + h;
+	}
+	// A element (row, k) is contiguous along rows except for L11^T (along k);
+	// B element (k, col) is contiguous along k.  Consecutive threads take the
+	// contiguous index so every load is coalesced.
+	const bool a_k_fast = (STEP == 0) && lower;
+	float acc[4][4] = {};
+	for (int k0 = k_begin; k0 < k_end; k0 += 16) {
+		for (int e = tid; e < 64 * 16; e += 256) {
+			const int r = a_k_fast ? (e >> 4) : (e & 63), kk = a_k_fast ? (e & 15) : (e >> 6);
+			const int k = k0 + kk, row = row0 + r;
+			float av = 0.f;
+			if (k < k_end && row < o + h) {
+				if (STEP == 0)
+					av = lower ? tri_t<true>(lu, lda, b, row, k) : tri_t<false>(lu, lda, b, row, k);
+				else
+					av = x[static_cast<int64_t>(k) * ldp + row];
 			}
+			As[kk][r] = av;
+			const int kb = e & 15, cc = e >> 4;
+			const int kq = k0 + kb, col = col0 + cc;
+			float bv = 0.f;
+			if (kq < k_end && col < o + h + h2)
+				bv = (STEP == 0) ? x[static_cast<int64_t>(col) * ldp + kq] : w[static_cast<int64_t>(col) * ldp + kq];
+			Bs[kb][cc] = bv;
 		}
 		__syncthreads();
 #pragma unroll
-		for (int r = 0; r < 4; ++r) Sb[warp + 8 * r][lane] = acc[r];
-		for (int e = tid; e < 1024; e += 256) {
-			const int i = TRANS_T ? (e >> 5) : (e & 31), p = TRANS_T ? (e & 31) : (e >> 5);
-			Tb[i][p] = tval(32 * I + i, 32 * I + p);
-		}
-		__syncthreads();
-		// X[I,G] = T_II^{-1} S by back substitution, one column per lane of warp 0.
-		if (warp == 0) {
-			float x[32];
+		for (int kk = 0; kk < 16; ++kk) {
+			float a[4], bb[4];
 #pragma unroll
-			for (int i = 31; i >= 0; --i) {
-				float v = Sb[i][lane];
-#pragma unroll
-				for (int p = i + 1; p < 32; ++p) v = fmaf(-Tb[i][p], x[p], v);
-				x[i] = TRANS_T ? v : v / Tb[i][i];
+			for (int q = 0; q < 4; ++q) {
+				a[q] = As[kk][ty + 16 * q];
+				bb[q] = Bs[kk][tx + 16 * q];
 			}
 #pragma unroll
-			for (int i = 0; i < 32; ++i) Xs[32 * I + i][lane] = x[i];
+			for (int q = 0; q < 4; ++q)
+#pragma unroll
+				for (int u = 0; u < 4; ++u) acc[q][u] = fmaf(a[q], bb[u], acc[q][u]);
 		}
 		__syncthreads();
 	}
-	// Write the column block: rows 0..b-1, zero below the diagonal.
-	for (int e = tid; e < 32 * b; e += 256) {
-		const int row = e % b, c = e / b;
-		const int col = 32 * G + c;
-		if (col >= b) continue;
-		const float v = (row <= 32 * G + 31 && row <= col) ? Xs[row][c] : 0.f;
-		const float h = tf32_hi(v);
-		xhi[static_cast<int64_t>(col) * ldx + row] = h;
-		xlo[static_cast<int64_t>(col) * ldx + row] = v - h;
+	float *out = (STEP == 0) ? w : x;
+	const float sgn = (STEP == 0) ? 1.f : -1.f;
+#pragma unroll
+	for (int q = 0; q < 4; ++q) {
+		const int row = row0 + ty + 16 * q;
+		if (row >= o + h) continue;
+#pragma unroll
+		for (int u = 0; u < 4; ++u) {
+			const int col = col0 + tx + 16 * u;
+			if (col < o + h + h2) out[static_cast<int64_t>(col) * ldp + row] = sgn * acc[q][u];
+		}
 	}
 }
 
-// blockIdx.y = 0: U11^{-1} from the upper triangle; 1: (L11^T)^{-1} from the unit lower one.
-__global__ void __launch_bounds__(256) tri_inv_kernel(int b, const float *__restrict__ t, int64_t ldt,
-	float *__restrict__ uhi, float *__restrict__ ulo, float *__restrict__ lhi, float *__restrict__ llo, int64_t ldx)
+// X (work, ldp x ldp) -> hi/lo copies: column col < b is map row col of
+// the K-major operand, rows 0..ldp-1 with zeros below the diagonal.
+__global__ void __launch_bounds__(256) tri_split_kernel(int b, const float *__restrict__ xu,
+	const float *__restrict__ xl, float *__restrict__ uhi, float *__restrict__ ulo, float *__restrict__ lhi,
+	float *__restrict__ llo, int64_t ldp)
 {
-	if (blockIdx.y == 0)
-		tri_inv_body<false>(b, t, ldt, uhi, ulo, ldx);
-	else
-		tri_inv_body<true>(b, t, ldt, lhi, llo, ldx);
+	const bool lower = blockIdx.y != 0;
+	const float *x = lower ? xl : xu;
+	float *hi = lower ? lhi : uhi, *lo = lower ? llo : ulo;
+	const int64_t total = static_cast<int64_t>(b) * ldp;
+	for (int64_t e = blockIdx.x * 256 + threadIdx.x; e < total; e += static_cast<int64_t>(gridDim.x) * 256) {
+		const int row = static_cast<int>(e % ldp), col = static_cast<int>(e / ldp);
+		const float v = (row <= col) ? x[e] : 0.f;
+		const float hv = tf32_hi(v);
+		hi[e] = hv;
+		lo[e] = v - hv;
+	}
 }
 
 // ---------------------------------------------------------------------------
@@ -443,9 +506,14 @@ int launch_tf32x3(const unsigned char *m_ahi, const unsigned char *m_alo, const 
 static_assert(sizeof(CUtensorMap) <= 128, "tensor map storage");
 
 int tc_panels_make(TcPanels *t, int n, int b, float *phi, float *plo, int64_t ldp, float *uhi, float *ulo,
-	float *lhi, float *llo)
+	float *lhi, float *llo, float *work)
 {
-	if (!t || n <= 0 || b <= 0 || ldp < b || (ldp % 32)) return HPLAI_EINVAL;
+	if (!t || n <= 0 || b <= 0 || ldp < b || (ldp % 32) || !work) return HPLAI_EINVAL;
+	const size_t sq = static_cast<size_t>(ldp) * ldp;
+	t->xu = work;
+	t->xl = work + sq;
+	t->wu = work + 2 * sq;
+	t->wl = work + 3 * sq;
 	t->n = n;
 	t->b = b;
 	t->ldp = ldp;
@@ -467,17 +535,26 @@ int tc_panels_make(TcPanels *t, int n, int b, float *phi, float *plo, int64_t ld
 int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStream_t st)
 {
 	const int b = t.b;
-	const int groups = (b + 31) / 32;
-	const size_t smem = (static_cast<size_t>(b + 32) * 33 + 2 * 32 * 33) * sizeof(float);
-	static bool attr = false;
-	if (!attr) {
-		HPLAI_CUDA_TRY(cudaFuncSetAttribute(tri_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			static_cast<int>((1024 + 32) * 33 * 4 + 2 * 32 * 33 * 4)));
-		attr = true;
+	const int bp = static_cast<int>(t.ldp);
+	const int nt = bp / 32;
+	tri_diag_kernel<<<dim3(nt, 2), 32, 0, st>>>(b, lu, lda, t.xu, t.xl, t.ldp);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	for (int h = 32; h < bp; h *= 2) {
+		const int pairs = (bp + 2 * h - 1) / (2 * h);
+		const int tiles = ((h + 63) / 64) * ((h + 63) / 64);
+		const dim3 g(tiles, pairs, 2);
+		tri_level_kernel<0><<<g, 256, 0, st>>>(b, bp, h, lu, lda, t.xu, t.xl, t.wu, t.wl, t.ldp);
+		count_launches();
+		HPLAI_CUDA_TRY(cudaGetLastError());
+		tri_level_kernel<1><<<g, 256, 0, st>>>(b, bp, h, lu, lda, t.xu, t.xl, t.wu, t.wl, t.ldp);
+		count_launches();
+		HPLAI_CUDA_TRY(cudaGetLastError());
 	}
-	// y = 0: U11^{-1} column-major = the B operand of the L-panel product (row n = column n of U^{-1});
-	// y = 1: (L11^T)^{-1} column-major = L11^{-1} row-major = the A operand of the U-panel product.
-	tri_inv_kernel<<<dim3(groups, 2), 256, smem, st>>>(b, lu, lda, t.uhi, t.ulo, t.lhi, t.llo, t.ldp);
+	// U11^{-1} column-major = the B operand of the L-panel product (row n = column n of U^{-1});
+	// (L11^T)^{-1} column-major = L11^{-1} row-major = the A operand of the U-panel product.
+	tri_split_kernel<<<dim3((b * bp + 255) / 256 < 1184 ? (b * bp + 255) / 256 : 1184, 2), 256, 0, st>>>(b, t.xu,
+		t.xl, t.uhi, t.ulo, t.lhi, t.llo, t.ldp);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
