@@ -225,7 +225,8 @@ def run_ours(args):
         if world > 1:
             torch.distributed.barrier()
 
-    s = hplai.Solver(n, b, precision=prec)
+    flags = hplai.FLAG_LOOKAHEAD if args.lookahead else 0
+    s = hplai.Solver(n, b, precision=prec, flags=flags)
     ext = torch.cuda.ExternalStream(s.stream())
     results = []
 
@@ -353,7 +354,7 @@ def run_ours(args):
             "config": {"workload": f"HPL-AI solve n={n} b={b}: FP32 panels, "
                                    f"{'e4m3' if prec == hplai.F32_F8 else 'FP16'} tcgen05 Schur update, "
                                    f"FP64 {'GMRES-IR' if mode == hplai.GMRES else 'iterative refinement'}",
-                       "n": n, "b": b, "form": form,
+                       "n": n, "b": b, "form": form, "lookahead": bool(args.lookahead),
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": f"inputs {n * n * 4 / 1e9:.1f} GB FP32 > 126 MB L2, rewritten between steps"},
             "hpl_harness": last.hpl_harness, "resid": last.residual, "ir_steps": last.iters,
@@ -381,6 +382,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--precision", choices=("f16", "f8"), default="f16",
                     help="Schur update operands: FP16 (plain form) or e4m3 with per-128 factors")
+    ap.add_argument("--lookahead", action="store_true",
+                    help="form the next step's diagonal block and panels on a side stream (HPLAI_FLAG_LOOKAHEAD)")
     ap.add_argument("--refine", choices=("ir", "gmres"), default=None,
                     help="correction: classical IR or GMRES (default: ir for f16, gmres for f8)")
     args = ap.parse_args()

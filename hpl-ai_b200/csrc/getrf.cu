@@ -1,20 +1,27 @@
 // getrf.cu -- b x b diagonal block LU without pivoting, spread over the GPU.
 //
 // getrf_nopiv (getrf_nopiv.hpp:30-141) on the diagonal block of each step.
-// The block is cut into 32 x 32 tiles; every tile is owned by one warp and
-// goes through the steps of a right-looking LU:
+// The block is cut into 32 x 32 tiles that go through the steps of a
+// right-looking LU:
 //   step r < min(ti, tj):  X -= L(ti, r) U(r, tj)              (trailing update)
 //   step r = ti = tj:      X <- LU of X                        (tile factor)
 //   step r = tj < ti:      X <- X U(r, r)^{-1}                 (L tile)
 //   step r = ti < tj:      X <- L(r, r)^{-1} X  (unit lower)   (U tile)
-// A tile that is final publishes a per-tile flag; consumers wait on the
-// flags of the tiles they read.  All warps are resident (cooperative
-// launch) and each walks its tiles step by step, within a step first the
-// diagonal tile, then panel tiles, then trailing updates, so no warp can
-// wait on work it has not yet reached and the dataflow always completes; it
-// also runs the next step's tile factor as soon as its inputs exist (a
-// look-ahead for free).  Every wait is bounded; a timeout sets the status
-// word and the warp stops.
+// Each tile publishes a progress word, epoch * 64 + (steps applied), where a
+// tile with min(ti, tj) = r is final at r + 1; consumers wait for the value
+// they need.
+//
+// The diagonal is the critical chain, so one warp (CTA 0) does nothing
+// else: at step r it takes L(r+1, r) and U(r, r+1) once their owners have
+// applied their first r updates, solves them with the factored tile (r, r)
+// it still holds, publishes them, applies the last update to tile
+// (r+1, r+1) and factors it.  There is no flag hop between two diagonal
+// tiles, and its code stays hot in its SM's instruction cache.  Worker
+// warps (the other CTAs) own every other tile and walk them step by step,
+// panel tiles before updates.  Every wait is on work the producer reaches
+// without waiting on the waiter, so the dataflow always completes (all
+// warps are resident: cooperative launch); every wait is bounded, and a
+// timeout sets the status word and the warp stops.
 //
 // Each element receives a_ij <- fmaf(-l_ik, u_kj, a_ij) in increasing k,
 // multipliers are a_ik * (1/u_kk) and the U tiles use the same unit-lower
@@ -31,177 +38,357 @@ namespace hplai {
 namespace {
 
 constexpr int T = 32;
-constexpr int kWarps = 8;
+constexpr int kWarps = 8;       // worker warps per CTA
 constexpr int kMaxTiles = 32;   // b <= 1024
+
+// One progress word per 128-byte line, so that polling warps and publishing
+// warps do not queue on a few L2 lines.
+constexpr int kFlagStride = 32;
 
 struct GetrfWork {
 	uint32_t status;
 	uint32_t pad[31];
-	uint32_t flags[kMaxTiles * kMaxTiles];
+	uint32_t prog[kMaxTiles * kMaxTiles * kFlagStride];
 };
 
-// Wait until *f == epoch; every lane polls, the warp gives up together.
-__device__ __forceinline__ bool wait_tile(const uint32_t *f, uint32_t epoch)
+// Wait until *f >= target (values of earlier launches are below every target
+// of this one).  Lane 0 reads the word; the whole warp stays in the loop
+// and learns the outcome through a shuffle, so the warp never diverges
+// around a wait (a warp left split after a long divergent spin runs the
+// following shuffles many times slower).
+__device__ __forceinline__ bool wait_prog(const uint32_t *f, uint32_t target)
 {
-	if (ld_acquire_u32(f) == epoch) return true;
-	const uint64_t t0 = global_ns();
-	while (true) {
-		if (__all_sync(0xffffffffu, ld_acquire_u32(f) == epoch)) return true;
-		if (__any_sync(0xffffffffu, global_ns() - t0 > kWaitLimitNs)) return false;
+	const bool lead = (threadIdx.x & 31) == 0;
+	uint64_t t0 = 0;
+	for (int it = 0;; ++it) {
+		int ready = lead ? (ld_acquire_u32(f) >= target) : 0;
+		ready = __shfl_sync(0xffffffffu, ready, 0);
+		if (ready) return true;
+		if (it == 0) t0 = global_ns();
+		else if (global_ns() - t0 > kWaitLimitNs) return false;
+		__nanosleep(32);
 	}
 }
 
-__device__ __forceinline__ void publish(uint32_t *f, uint32_t epoch)
+__device__ __forceinline__ void publish(uint32_t *f, uint32_t v)
 {
 	__syncwarp();
 	if ((threadIdx.x & 31) == 0) {
 		__threadfence();
-		st_release_u32(f, epoch);
+		st_release_u32(f, v);
 	}
 }
 
-// Tile (rows r0.., cols c0..) -> S[i][j] (rows >= rv or cols >= cv read as 0).
-__device__ __forceinline__ void load_tile(float (*S)[T + 1], const float *a, int64_t lda, int r0, int c0, int rv,
-	int cv, int lane)
+// A staged tile: column-major, element (i, j) at t[j * kLd + i]; rows of 16
+// bytes so that cp.async can fill it.  Lane i works on row i (conflict-free
+// along a column); all lanes reading one element is a broadcast.
+constexpr int kLd = 36;
+constexpr int kTileFloats = T * kLd;
+
+// Tile (rows r0.., cols c0..) -> t, rows >= rv and columns >= cv zero.
+// vec: a, lda and r0 allow 16-byte copies (cp.async.cg, L2 only); otherwise
+// 4-byte loads through L2.  The caller waits with stage_wait().
+__device__ __forceinline__ void stage_tile(float *t, const float *a, int64_t lda, int r0, int c0, int rv, int cv,
+	bool vec, int lane)
 {
-#pragma unroll 8
-	for (int j = 0; j < T; ++j)
-		S[lane][j] = (lane < rv && j < cv) ? __ldcg(&a[static_cast<int64_t>(c0 + j) * lda + r0 + lane]) : 0.f;
+	if (vec) {
+#pragma unroll 1
+		for (int q = 0; q < 8; ++q) {
+			const int e = lane + 32 * q, j = e >> 3, g = (e & 7) * 4;
+			int bytes = (j < cv) ? (rv - g) * 4 : 0;
+			bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
+			const float *src = a + static_cast<int64_t>(c0 + (j < cv ? j : 0)) * lda + r0 + (bytes ? g : 0);
+			asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(t + j * kLd + g)), "l"(src),
+				"r"(bytes) : "memory");
+		}
+		asm volatile("cp.async.commit_group;" ::: "memory");
+	} else {
+#pragma unroll 4
+		for (int j = 0; j < T; ++j)
+			t[j * kLd + lane] = (lane < rv && j < cv) ? __ldcg(&a[static_cast<int64_t>(c0 + j) * lda + r0 + lane]) : 0.f;
+	}
 }
 
-__device__ __forceinline__ void store_tile(const float (*S)[T + 1], float *a, int64_t lda, int r0, int c0, int rv,
-	int cv, int lane)
+__device__ __forceinline__ void stage_wait()
+{
+	asm volatile("cp.async.wait_all;" ::: "memory");
+	__syncwarp();
+}
+
+__device__ __forceinline__ void store_tile(const float *t, float *a, int64_t lda, int r0, int c0, int rv, int cv,
+	int lane)
 {
 	if (lane < rv) {
-#pragma unroll 8
-		for (int j = 0; j < T; ++j)
-			if (j < cv) a[static_cast<int64_t>(c0 + j) * lda + r0 + lane] = S[lane][j];
+#pragma unroll 4
+		for (int j = 0; j < cv; ++j) a[static_cast<int64_t>(c0 + j) * lda + r0 + lane] = t[j * kLd + lane];
 	}
+}
+
+// Tile operations on staged tiles.  Each keeps a row (or column) of its tile
+// in registers and walks the pivots with a runtime loop: the element of the
+// current pivot column is always v[0] and the row shifts left by one after
+// each step, so every register index is static while the loop body stays a
+// few hundred bytes of code (instruction-cache resident; a fully unrolled
+// 32-step elimination is tens of KB and runs from L2 once per step).
+
+// Unblocked LU (getrf_nopiv_small order) of the kv x kv tile x; row `lane`
+// in registers, the pivot row broadcast from its lane.
+__device__ __noinline__ void op_factor(float *x, int kv)
+{
+	const int lane = threadIdx.x & 31;
+	float v[T];
+#pragma unroll
+	for (int j = 0; j < T; ++j) v[j] = x[j * kLd + lane];
+#pragma unroll 1
+	for (int k = 0; k < kv; ++k) {
+		// v[t] = element (lane, k + t)
+		const float inv = 1.0f / __shfl_sync(0xffffffffu, v[0], k);
+		const bool below = lane > k;
+		const float lik = v[0] * inv;
+		if (below) v[0] = lik;
+#pragma unroll
+		for (int t = 1; t < T; ++t) {
+			const float ukj = __shfl_sync(0xffffffffu, v[t], k);
+			if (below) v[t] = fmaf(-lik, ukj, v[t]);
+		}
+		x[k * kLd + lane] = v[0];   // column k of row `lane` is final
+#pragma unroll
+		for (int t = 0; t < T - 1; ++t) v[t] = v[t + 1];
+		v[T - 1] = 0.f;
+	}
+	__syncwarp();
+}
+
+// L tile x <- x U^{-1}, U = upper part of the factored tile d (kv x kv); row `lane`.
+__device__ __noinline__ void op_solve_l(float *x, const float *d, int kv)
+{
+	const int lane = threadIdx.x & 31;
+	float v[T];
+#pragma unroll
+	for (int j = 0; j < T; ++j) v[j] = x[j * kLd + lane];
+#pragma unroll 1
+	for (int j = 0; j < kv; ++j) {
+		// v[t] = element (lane, j + t); U(j, j + t) at d[(j + t) * kLd + j]
+		v[0] *= 1.0f / d[j * kLd + j];
+		const float *urow = d + j * kLd + j;
+#pragma unroll
+		for (int t = 1; t < T; ++t)
+			if (j + t < T) v[t] = fmaf(-v[0], urow[t * kLd], v[t]);
+		x[j * kLd + lane] = v[0];
+#pragma unroll
+		for (int t = 0; t < T - 1; ++t) v[t] = v[t + 1];
+		v[T - 1] = 0.f;
+	}
+	__syncwarp();
+}
+
+// U tile x <- L^{-1} x, L = unit lower part of d (kv x kv); column `lane`.
+__device__ __noinline__ void op_solve_u(float *x, const float *d, int kv)
+{
+	const int lane = threadIdx.x & 31;
+	float v[T];
+	float *col = x + lane * kLd;
+#pragma unroll
+	for (int q = 0; q < T / 4; ++q) {
+		const float4 c = reinterpret_cast<const float4 *>(col)[q];
+		v[4 * q] = c.x;
+		v[4 * q + 1] = c.y;
+		v[4 * q + 2] = c.z;
+		v[4 * q + 3] = c.w;
+	}
+#pragma unroll 1
+	for (int k = 0; k < kv; ++k) {
+		// v[t] = element (k + t, lane); L(k + t, k) at d[k * kLd + k + t]
+		const float *lcol = d + k * kLd + k;
+#pragma unroll
+		for (int t = 1; t < T; ++t)
+			if (k + t < T) v[t] = fmaf(-v[0], lcol[t], v[t]);
+		col[k] = v[0];
+#pragma unroll
+		for (int t = 0; t < T - 1; ++t) v[t] = v[t + 1];
+		v[T - 1] = 0.f;
+	}
+	__syncwarp();
+}
+
+// x -= l u (K = T); row `lane` of x in registers.
+__device__ __noinline__ void op_update(float *x, const float *l, const float *u)
+{
+	const int lane = threadIdx.x & 31;
+	float v[T];
+#pragma unroll
+	for (int j = 0; j < T; ++j) v[j] = x[j * kLd + lane];
+#pragma unroll 1
+	for (int k = 0; k < T; ++k) {
+		const float lk = l[k * kLd + lane];
+#pragma unroll
+		for (int j = 0; j < T; ++j) v[j] = fmaf(-lk, u[j * kLd + k], v[j]);
+	}
+#pragma unroll
+	for (int j = 0; j < T; ++j) x[j * kLd + lane] = v[j];
+	__syncwarp();
+}
+
+constexpr int kDiagWarps = 4;
+
+// Barrier and AND-vote of the diagonal CTA's warps (named barrier 1).
+__device__ __forceinline__ void diag_sync()
+{
+	asm volatile("bar.sync 1, %0;" ::"n"(kDiagWarps * 32) : "memory");
+}
+
+__device__ __forceinline__ bool diag_all(bool p)
+{
+	int r;
+	asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\tbar.red.and.pred q, 1, %2, p;\n\t"
+	             "selp.s32 %0, 1, 0, q;\n\t}"
+	             : "=r"(r) : "r"(p ? 1 : 0), "n"(kDiagWarps * 32) : "memory");
+	return r != 0;
+}
+
+// Columns c0 .. c0 + T/kDiagWarps - 1 of x -= l u (K = T); row `lane`.
+__device__ __noinline__ void op_update_cols(float *x, const float *l, const float *u, int c0)
+{
+	constexpr int C = T / kDiagWarps;
+	const int lane = threadIdx.x & 31;
+	float v[C];
+#pragma unroll
+	for (int j = 0; j < C; ++j) v[j] = x[(c0 + j) * kLd + lane];
+#pragma unroll 4
+	for (int k = 0; k < T; ++k) {
+		const float lk = l[k * kLd + lane];
+#pragma unroll
+		for (int j = 0; j < C; ++j) v[j] = fmaf(-lk, u[(c0 + j) * kLd + k], v[j]);
+	}
+#pragma unroll
+	for (int j = 0; j < C; ++j) x[(c0 + j) * kLd + lane] = v[j];
 }
 
 __global__ void __launch_bounds__(kWarps * 32) getrf_tiles_kernel(int b, float *a, int64_t lda, GetrfWork *w,
 	uint32_t epoch)
 {
-	__shared__ float stage[kWarps][T][T + 1];
+	extern __shared__ __align__(16) float dyn[];
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	// this warp's staging tile: its own tile (factor, U tile transpose) or the
-	// tile it reads (U(r, tj) of an update, the factored diagonal tile)
-	float (*S)[T + 1] = stage[warp];
-	float (*D)[T + 1] = stage[warp];
-	const int wid = blockIdx.x * kWarps + warp, nwarps = gridDim.x * kWarps;
+	float *X = dyn + warp * 4 * kTileFloats;   // this warp's tile
+	float *D = X + kTileFloats;                // the factored diagonal tile it reads
+	float *Lt = X + 2 * kTileFloats;           // an L tile it reads
+	float *Ut = X + 3 * kTileFloats;           // a U tile it reads
 	const int nt = (b + T - 1) / T, ntiles = nt * nt;
-	uint32_t *flags = w->flags;
+	const uint32_t base = epoch * 64u;
+	uint32_t *prog = w->prog;
+	auto pidx = [nt](int ti, int tj) { return (ti + nt * tj) * kFlagStride; };
+	const bool vec = ((reinterpret_cast<uintptr_t>(a) & 15u) == 0) && ((lda & 3) == 0);
 	bool ok = true;
 
+	if (blockIdx.x == 0) {
+		// ---------------- the diagonal chain (4 warps) ----------------
+		// warp 0 solves L(r+1, r) while warp 1 solves U(r, r+1); the four
+		// warps share the update of tile (r+1, r+1), 8 columns each; warp 0
+		// factors it.  Their tiles are warp 0's four staging buffers.
+		if (warp >= kDiagWarps) return;
+		float *Dd = dyn, *Xd = dyn + kTileFloats, *Ld = dyn + 2 * kTileFloats, *Ud = dyn + 3 * kTileFloats;
+		if (warp == 0) {
+			const int kv = min(T, b);
+			stage_tile(Dd, a, lda, 0, 0, kv, kv, vec, lane);
+			stage_wait();
+			op_factor(Dd, kv);
+			store_tile(Dd, a, lda, 0, 0, kv, kv, lane);
+			publish(&prog[0], base + 1);
+		}
+		diag_sync();
+		for (int r = 0; r + 1 < nt && ok; ++r) {
+			const int k0 = r * T, r1 = k0 + T, v1 = min(T, b - r1);
+			bool mine = true;
+			if (r > 0 && warp < 3) {
+				const int f = warp == 0 ? pidx(r + 1, r) : (warp == 1 ? pidx(r, r + 1) : pidx(r + 1, r + 1));
+				mine = wait_prog(&prog[f], base + r);
+			}
+			ok = diag_all(mine);
+			if (!ok) break;
+			if (warp == 0) stage_tile(Ld, a, lda, r1, k0, v1, T, vec, lane);   // L(r+1, r) before its solve
+			if (warp == 1) stage_tile(Ud, a, lda, k0, r1, T, v1, vec, lane);   // U(r, r+1) before its solve
+			if (warp == 2) stage_tile(Xd, a, lda, r1, r1, v1, v1, vec, lane);  // tile (r+1, r+1)
+			stage_wait();
+			if (warp == 0) {
+				op_solve_l(Ld, Dd, T);
+				store_tile(Ld, a, lda, r1, k0, v1, T, lane);
+			} else if (warp == 1) {
+				op_solve_u(Ud, Dd, T);
+				store_tile(Ud, a, lda, k0, r1, T, v1, lane);
+			}
+			__threadfence();
+			diag_sync();
+			if (warp == 0 && lane == 0) {
+				st_release_u32(&prog[pidx(r + 1, r)], base + r + 1);
+				st_release_u32(&prog[pidx(r, r + 1)], base + r + 1);
+			}
+			op_update_cols(Xd, Ld, Ud, warp * (T / kDiagWarps));
+			diag_sync();
+			if (warp == 0) {
+				op_factor(Xd, v1);
+				store_tile(Xd, a, lda, r1, r1, v1, v1, lane);
+				publish(&prog[pidx(r + 1, r + 1)], base + r + 2);
+			}
+			diag_sync();
+			// the new diagonal tile is the next step's factor
+			for (int e = threadIdx.x; e < kTileFloats; e += kDiagWarps * 32) Dd[e] = Xd[e];
+			diag_sync();
+		}
+		if (!ok && threadIdx.x == 0) atomicOr(&w->status, 1u);
+		return;
+	}
+
+	// ---------------- worker warps ----------------
+	const int wid = (blockIdx.x - 1) * kWarps + warp, nwarps = (gridDim.x - 1) * kWarps;
 	for (int r = 0; r < nt && ok; ++r) {
 		const int k0 = r * T, kv = min(T, b - k0);
-		for (int pass = 0; pass < 3 && ok; ++pass) {
+		const uint32_t diag_final = base + r + 1;
+		// pass 0: panel tiles of step r; pass 1: trailing updates
+		for (int pass = 0; pass < 2 && ok; ++pass) {
 			for (int t = wid; t < ntiles && ok; t += nwarps) {
 				const int ti = t % nt, tj = t / nt;
 				const int mn = min(ti, tj);
-				if (mn < r) continue;
-				const int kind = (ti == r && tj == r) ? 0 : (mn == r ? 1 : 2);
-				if (kind != pass) continue;
+				if (mn < r || ti == tj && ti <= r + 1) continue;                     // done, or the diagonal warp's
+				if ((ti == r + 1 && tj == r) || (ti == r && tj == r + 1)) continue;  // the diagonal warp's
+				if ((mn == r ? 0 : 1) != pass) continue;
 				const int r0 = ti * T, c0 = tj * T;
 				const int rv = min(T, b - r0), cv = min(T, b - c0);
-				if (kind == 2) {
-					// X -= L(ti, r) U(r, tj): row `lane` of X and of L in registers, U staged
-					if (!wait_tile(&flags[ti + nt * r], epoch) || !wait_tile(&flags[r + nt * tj], epoch)) {
-						ok = false;
-						break;
-					}
-					float x[T], l[T];
-#pragma unroll
-					for (int j = 0; j < T; ++j) {
-						x[j] = (lane < rv && j < cv) ? __ldcg(&a[static_cast<int64_t>(c0 + j) * lda + r0 + lane]) : 0.f;
-						l[j] = (lane < rv) ? __ldcg(&a[static_cast<int64_t>(k0 + j) * lda + r0 + lane]) : 0.f;
-					}
-					load_tile(D, a, lda, k0, c0, T, cv, lane);
-					__syncwarp();
-#pragma unroll
-					for (int k = 0; k < T; ++k)
-#pragma unroll
-						for (int j = 0; j < T; ++j) x[j] = fmaf(-l[k], D[k][j], x[j]);
-					if (lane < rv) {
-#pragma unroll
-						for (int j = 0; j < T; ++j)
-							if (j < cv) a[static_cast<int64_t>(c0 + j) * lda + r0 + lane] = x[j];
-					}
-					__syncwarp();
-				} else if (kind == 0) {
-					// unblocked LU of the diagonal tile (getrf_nopiv_small order)
-					load_tile(S, a, lda, r0, c0, rv, cv, lane);
-					__syncwarp();
-					for (int k = 0; k < kv; ++k) {
-						const float inv = 1.0f / S[k][k];
-						if (lane > k && lane < kv) {
-							const float lik = S[lane][k] * inv;
-							S[lane][k] = lik;
-							for (int j = k + 1; j < kv; ++j) S[lane][j] = fmaf(-lik, S[k][j], S[lane][j]);
-						}
-						__syncwarp();
-					}
-					store_tile(S, a, lda, r0, c0, rv, cv, lane);
-					publish(&flags[t], epoch);
-				} else if (tj == r) {
-					// L tile: X <- X U(r,r)^{-1}, row `lane` of X in registers
-					float x[T];
-#pragma unroll
-					for (int j = 0; j < T; ++j)
-						x[j] = (lane < rv && j < kv) ? __ldcg(&a[static_cast<int64_t>(c0 + j) * lda + r0 + lane]) : 0.f;
-					if (!wait_tile(&flags[r + nt * r], epoch)) {
-						ok = false;
-						break;
-					}
-					load_tile(D, a, lda, k0, k0, kv, kv, lane);
-					__syncwarp();
-#pragma unroll
-					for (int j = 0; j < T; ++j) {
-						if (j < kv) {
-							x[j] *= 1.0f / D[j][j];
-#pragma unroll
-							for (int q = j + 1; q < T; ++q) x[q] = fmaf(-x[j], D[j][q], x[q]);
-						}
-					}
-					if (lane < rv) {
-#pragma unroll
-						for (int j = 0; j < T; ++j)
-							if (j < kv) a[static_cast<int64_t>(c0 + j) * lda + r0 + lane] = x[j];
-					}
-					publish(&flags[t], epoch);
+				if (pass == 0) {
+					// L tile X <- X U(r,r)^{-1}, or U tile X <- L(r,r)^{-1} X
+					stage_tile(X, a, lda, r0, c0, rv, cv, vec, lane);
+					if (!wait_prog(&prog[pidx(r, r)], diag_final)) { ok = false; break; }
+					stage_tile(D, a, lda, k0, k0, kv, kv, vec, lane);
+					stage_wait();
+					if (tj == r)
+						op_solve_l(X, D, kv);
+					else
+						op_solve_u(X, D, kv);
+					store_tile(X, a, lda, r0, c0, rv, cv, lane);
+					publish(&prog[t * kFlagStride], base + r + 1);
 				} else {
-					// U tile: X <- L(r,r)^{-1} X, column `lane` of X in registers
-					load_tile(S, a, lda, r0, c0, kv, cv, lane);
-					__syncwarp();
-					float y[T];
-#pragma unroll
-					for (int i = 0; i < T; ++i) y[i] = S[i][lane];
-					__syncwarp();
-					if (!wait_tile(&flags[r + nt * r], epoch)) {
+					// X -= L(ti, r) U(r, tj)
+					if (!wait_prog(&prog[pidx(ti, r)], base + r + 1) || !wait_prog(&prog[pidx(r, tj)], base + r + 1)) {
 						ok = false;
 						break;
 					}
-					load_tile(D, a, lda, k0, k0, kv, kv, lane);
-					__syncwarp();
-#pragma unroll
-					for (int k = 0; k < T; ++k) {
-						if (k < kv) {
-#pragma unroll
-							for (int i = k + 1; i < T; ++i) y[i] = fmaf(-y[k], D[i][k], y[i]);
-						}
-					}
-					__syncwarp();
-#pragma unroll
-					for (int i = 0; i < T; ++i) S[i][lane] = y[i];
-					__syncwarp();
-					store_tile(S, a, lda, r0, c0, kv, cv, lane);
-					publish(&flags[t], epoch);
+					stage_tile(X, a, lda, r0, c0, rv, cv, vec, lane);
+					stage_tile(Lt, a, lda, r0, k0, rv, T, vec, lane);
+					stage_tile(Ut, a, lda, k0, c0, T, cv, vec, lane);
+					stage_wait();
+					op_update(X, Lt, Ut);
+					store_tile(X, a, lda, r0, c0, rv, cv, lane);
+					// the next step's panel tiles, and the diagonal tile after next, announce
+					// that they hold r + 1 updates
+					if (mn == r + 1 || (ti == tj && ti == r + 2)) publish(&prog[t * kFlagStride], base + r + 1);
 				}
+				__syncwarp();   // this warp's staging tiles are free again
 			}
 		}
 	}
 	if (!ok && lane == 0) atomicOr(&w->status, 1u);
 }
+
+constexpr size_t kSmemBytes = static_cast<size_t>(kWarps) * 4 * kTileFloats * sizeof(float);
 
 std::mutex g_static_mu;
 __device__ GetrfWork g_static_work;
@@ -212,7 +399,10 @@ int max_coresident_ctas()
 	static int cached = 0;
 	if (!cached) {
 		int per_sm = 0, dev = 0, sms = 0;
-		HPLAI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, getrf_tiles_kernel, kWarps * 32, 0));
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(getrf_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(kSmemBytes)));
+		HPLAI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, getrf_tiles_kernel, kWarps * 32,
+			kSmemBytes));
 		HPLAI_CUDA_TRY(cudaGetDevice(&dev));
 		HPLAI_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
 		cached = per_sm * sms;
@@ -229,17 +419,20 @@ int launch_getrf_tiles(int b, float *a, int64_t lda, void *work, uint32_t *epoch
 	if (b <= 0) return HPLAI_OK;
 	if (b > T * kMaxTiles || !a || lda < b || !work || !epoch) return HPLAI_EINVAL;
 	const int nt = (b + T - 1) / T;
-	int grid = (nt * nt + kWarps - 1) / kWarps;
+	// CTA 0: the diagonal warp; then enough worker CTAs for one tile per warp
+	int grid = 1 + (nt > 1 ? (nt * nt + kWarps - 1) / kWarps : 0);
 	const int cap = max_coresident_ctas();
-	if (cap <= 0) return HPLAI_EUNSUPPORTED;
+	if (cap < 2) return HPLAI_EUNSUPPORTED;
 	if (grid > cap) grid = cap;
-	if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
+	if (max_ctas > 0 && grid > max_ctas) grid = max_ctas < 2 ? 2 : max_ctas;
+	if (nt > 1 && grid < 2) grid = 2;
 	GetrfWork *w = static_cast<GetrfWork *>(work);
+	// progress words are epoch * 64 + steps (< 64): epochs stay below 2^26
 	uint32_t ep = ++*epoch;
-	if (ep == 0) ep = ++*epoch;   // flags start zeroed: never wait for 0
+	if (ep >= (1u << 26)) return HPLAI_EUNSUPPORTED;
 	void *args[] = {(void *)&b, (void *)&a, (void *)&lda, (void *)&w, (void *)&ep};
 	HPLAI_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(getrf_tiles_kernel), dim3(grid),
-		dim3(kWarps * 32), args, 0, st));
+		dim3(kWarps * 32), args, kSmemBytes, st));
 	count_launches();
 	return HPLAI_OK;
 }
