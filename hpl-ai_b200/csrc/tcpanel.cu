@@ -117,88 +117,104 @@ __global__ void __launch_bounds__(32) tri_diag_kernel(int b, const float *__rest
 	for (int i = 0; i < 32; ++i) x[static_cast<int64_t>(o + lane) * ldp + o + i] = v[i];
 }
 
-// One level's products for every pair and both triangles.  grid.x = 64 x 64
+// One level's products for every pair and both triangles.  grid.x = 32 x 32
 // output tiles of an h x h block (clipped), grid.y = pair, grid.z = triangle.
 //   STEP 0: W[o:o+h, o+h:o+h+h2] = T[o:o+h, o+h:..] X[o+h:.., o+h:..]
 //   STEP 1: X[o:o+h, o+h:..]     = -X[o:o+h, o:o+h] W[o:o+h, o+h:..]
+// K runs in chunks of 32; the next chunk is loaded into registers while the
+// current one is multiplied from shared memory.
 template <int STEP>
-__global__ void __launch_bounds__(256) tri_level_kernel(int b, int bp, int h, const float *__restrict__ lu, int64_t lda,
+__global__ void __launch_bounds__(128) tri_level_kernel(int b, int bp, int h, const float *__restrict__ lu, int64_t lda,
 	float *__restrict__ xu, float *__restrict__ xl, float *__restrict__ wu, float *__restrict__ wl, int64_t ldp)
 {
-	__shared__ float As[16][64 + 1];
-	__shared__ float Bs[16][64 + 1];
+	__shared__ float As[2][32][33];   // [buffer][k][row]
+	__shared__ float Bs[2][32][33];   // [buffer][k][col]
 	const bool lower = blockIdx.z != 0;
 	float *x = lower ? xl : xu;
 	float *w = lower ? wl : wu;
 	const int o = blockIdx.y * 2 * h;
 	const int h2 = min(h, bp - o - h);   // width of the second half
 	if (h2 <= 0) return;
-	const int tiles_n = (h2 + 63) / 64;
+	const int tiles_n = (h2 + 31) / 32;
 	const int tm = blockIdx.x / tiles_n, tn = blockIdx.x % tiles_n;
-	if (tm * 64 >= h) return;
-	const int row0 = o + tm * 64, col0 = o + h + tn * 64;   // output block position in X / W
-	const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+	if (tm * 32 >= h) return;
+	const int row0 = o + tm * 32, col0 = o + h + tn * 32;   // output tile position in X / W
+	const int rend = o + h, cend = o + h + h2;
+	const int tid = threadIdx.x;
 	// K range with nonzero contributions: STEP 0 rows of X_C up to the
 	// tile's last column; STEP 1 columns of X_A from the tile's first row
-	int k_begin, k_end;
-	if (STEP == 0) {
-		k_begin = o + h;
-		k_end = min(o + h + h2, col0 + 64);
-	} else {
-		k_begin = row0;
-		k_end = o + h;
-	}
+	const int k_begin = (STEP == 0) ? o + h : row0;
+	const int k_end = (STEP == 0) ? min(cend, col0 + 32) : rend;
 	// A element (row, k) is contiguous along rows except for L11^T (along k);
 	// B element (k, col) is contiguous along k.  Consecutive threads take the
 	// contiguous index so every load is coalesced.
 	const bool a_k_fast = (STEP == 0) && lower;
-	float acc[4][4] = {};
-	for (int k0 = k_begin; k0 < k_end; k0 += 16) {
-		for (int e = tid; e < 64 * 16; e += 256) {
-			const int r = a_k_fast ? (e >> 4) : (e & 63), kk = a_k_fast ? (e & 15) : (e >> 6);
+	float ra[8], rb[8];
+	auto load = [&](int k0) {
+#pragma unroll
+		for (int q = 0; q < 8; ++q) {
+			const int e = tid + 128 * q;
+			const int r = a_k_fast ? (e >> 5) : (e & 31), kk = a_k_fast ? (e & 31) : (e >> 5);
 			const int k = k0 + kk, row = row0 + r;
 			float av = 0.f;
-			if (k < k_end && row < o + h) {
+			if (k < k_end && row < rend) {
 				if (STEP == 0)
 					av = lower ? tri_t<true>(lu, lda, b, row, k) : tri_t<false>(lu, lda, b, row, k);
 				else
 					av = x[static_cast<int64_t>(k) * ldp + row];
 			}
-			As[kk][r] = av;
-			const int kb = e & 15, cc = e >> 4;
+			ra[q] = av;
+			const int kb = e & 31, cc = e >> 5;
 			const int kq = k0 + kb, col = col0 + cc;
 			float bv = 0.f;
-			if (kq < k_end && col < o + h + h2)
+			if (kq < k_end && col < cend)
 				bv = (STEP == 0) ? x[static_cast<int64_t>(col) * ldp + kq] : w[static_cast<int64_t>(col) * ldp + kq];
-			Bs[kb][cc] = bv;
+			rb[q] = bv;
 		}
-		__syncthreads();
+	};
+	auto stash = [&](int buf) {
 #pragma unroll
-		for (int kk = 0; kk < 16; ++kk) {
-			float a[4], bb[4];
-#pragma unroll
-			for (int q = 0; q < 4; ++q) {
-				a[q] = As[kk][ty + 16 * q];
-				bb[q] = Bs[kk][tx + 16 * q];
-			}
-#pragma unroll
-			for (int q = 0; q < 4; ++q)
-#pragma unroll
-				for (int u = 0; u < 4; ++u) acc[q][u] = fmaf(a[q], bb[u], acc[q][u]);
+		for (int q = 0; q < 8; ++q) {
+			const int e = tid + 128 * q;
+			const int r = a_k_fast ? (e >> 5) : (e & 31), kk = a_k_fast ? (e & 31) : (e >> 5);
+			As[buf][kk][r] = ra[q];
+			Bs[buf][e & 31][e >> 5] = rb[q];
 		}
-		__syncthreads();
+	};
+	// thread: output column `c`, rows 8g .. 8g+7
+	const int c = tid & 31, g = tid >> 5;
+	float acc[8] = {};
+	int buf = 0;
+	if (k_begin < k_end) {
+		load(k_begin);
+		stash(0);
 	}
+	__syncthreads();
+	for (int k0 = k_begin; k0 < k_end; k0 += 32) {
+		const bool more = k0 + 32 < k_end;
+		if (more) load(k0 + 32);
+#pragma unroll
+		for (int kk = 0; kk < 32; ++kk) {
+			const float bv = Bs[buf][kk][c];
+#pragma unroll
+			for (int i = 0; i < 8; ++i) acc[i] = fmaf(As[buf][kk][8 * g + i], bv, acc[i]);
+		}
+		if (more) stash(buf ^ 1);
+		__syncthreads();
+		buf ^= 1;
+	}
+	// write through shared memory so the stores run along the rows
 	float *out = (STEP == 0) ? w : x;
 	const float sgn = (STEP == 0) ? 1.f : -1.f;
 #pragma unroll
-	for (int q = 0; q < 4; ++q) {
-		const int row = row0 + ty + 16 * q;
-		if (row >= o + h) continue;
+	for (int i = 0; i < 8; ++i) As[0][c][8 * g + i] = sgn * acc[i];
+	__syncthreads();
 #pragma unroll
-		for (int u = 0; u < 4; ++u) {
-			const int col = col0 + tx + 16 * u;
-			if (col < o + h + h2) out[static_cast<int64_t>(col) * ldp + row] = sgn * acc[q][u];
-		}
+	for (int q = 0; q < 8; ++q) {
+		const int e = tid + 128 * q;
+		const int r = e & 31, cc = e >> 5;
+		const int row = row0 + r, col = col0 + cc;
+		if (row < rend && col < cend) out[static_cast<int64_t>(col) * ldp + row] = As[0][cc][r];
 	}
 }
 
@@ -390,13 +406,29 @@ __global__ void __launch_bounds__(TTHREADS, 1) tf32x3_kernel(const __grid_consta
 				tmem_ld_wait();
 				const int col0 = tn * TBN + ch * 32;
 				if (rok) {
+					__half *o16 = p.out16 + row * p.s16m + col0 * p.s16n;
+					// a row-major FP16 copy gets this thread's 32 columns as four 16-byte stores
+					const bool vec16 = p.s16n == 1 && col0 + 32 <= p.n && (reinterpret_cast<uintptr_t>(o16) & 15u) == 0;
 #pragma unroll
 					for (int j = 0; j < 32; ++j) {
 						const int col = col0 + j;
 						if (col < p.n) {
 							const float v = __uint_as_float(r[j]);
 							p.out32[row * p.s32m + col * p.s32n] = v;
-							p.out16[row * p.s16m + col * p.s16n] = __float2half_rn(p.scale * v);
+							if (!vec16) p.out16[row * p.s16m + col * p.s16n] = __float2half_rn(p.scale * v);
+						}
+					}
+					if (vec16) {
+#pragma unroll
+						for (int q = 0; q < 4; ++q) {
+							uint32_t w4[4];
+#pragma unroll
+							for (int e = 0; e < 4; ++e) {
+								const __half2 h2 = __floats2half2_rn(p.scale * __uint_as_float(r[8 * q + 2 * e]),
+									p.scale * __uint_as_float(r[8 * q + 2 * e + 1]));
+								w4[e] = *reinterpret_cast<const uint32_t *>(&h2);
+							}
+							*reinterpret_cast<uint4 *>(o16 + 8 * q) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
 						}
 					}
 				}
@@ -542,12 +574,12 @@ int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStr
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	for (int h = 32; h < bp; h *= 2) {
 		const int pairs = (bp + 2 * h - 1) / (2 * h);
-		const int tiles = ((h + 63) / 64) * ((h + 63) / 64);
+		const int tiles = ((h + 31) / 32) * ((h + 31) / 32);
 		const dim3 g(tiles, pairs, 2);
-		tri_level_kernel<0><<<g, 256, 0, st>>>(b, bp, h, lu, lda, t.xu, t.xl, t.wu, t.wl, t.ldp);
+		tri_level_kernel<0><<<g, 128, 0, st>>>(b, bp, h, lu, lda, t.xu, t.xl, t.wu, t.wl, t.ldp);
 		count_launches();
 		HPLAI_CUDA_TRY(cudaGetLastError());
-		tri_level_kernel<1><<<g, 256, 0, st>>>(b, bp, h, lu, lda, t.xu, t.xl, t.wu, t.wl, t.ldp);
+		tri_level_kernel<1><<<g, 128, 0, st>>>(b, bp, h, lu, lda, t.xu, t.xl, t.wu, t.wl, t.ldp);
 		count_launches();
 		HPLAI_CUDA_TRY(cudaGetLastError());
 	}
