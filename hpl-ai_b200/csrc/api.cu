@@ -87,6 +87,7 @@ struct hplai_ctx {
 	double *gm_v = nullptr;     // n x (gm_restart + 1), ld = gm_ldv
 	double *gm_w = nullptr;     // n
 	double *gm_small = nullptr; // part (kDotBlocks x kMaxBasis), H (kMaxBasis^2), tmp, y
+	double *rhs2 = nullptr, *x2 = nullptr;   // caller right-hand sides (hplai_solve_rhs / _transpose)
 	int64_t gm_ldv = 0;
 	int gm_cap = 0;             // restart length gm_v was sized for
 	int gm_inner = 0;           // inner steps of the last hplai_refine
@@ -119,6 +120,8 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->gm_v);
 	cudaFree(c->gm_w);
 	cudaFree(c->gm_small);
+	cudaFree(c->rhs2);
+	cudaFree(c->x2);
 	if (c->ev_panel) cudaEventDestroy(c->ev_panel);
 	if (c->ev_next) cudaEventDestroy(c->ev_next);
 	if (c->st) cudaStreamDestroy(c->st);
@@ -477,22 +480,23 @@ int ensure_gmres_buffers(hplai_ctx *c)
 }
 
 // r <- M^{-1} r with M = L U, the FP32 factors applied to an FP64 vector
-// (panel_trsvL / panel_trsvU, panel_trsv.hpp:310-758).
-int apply_lu_inverse(hplai_ctx *c, double *v, PhaseEvents &pe)
+// (panel_trsvL / panel_trsvU, panel_trsv.hpp:310-758); trans: r <- M^{-T} r,
+// U^T first, then L^T.
+int apply_lu_inverse(hplai_ctx *c, double *v, PhaseEvents &pe, bool trans)
 {
 	cudaStream_t st = c->st;
 	HPLAI_TRY(pe.record(st, HPLAI_PH_IR_TRSV));
-	HPLAI_TRY(launch_trsv(true, c->n, c->A, c->lda, v, c->trsv_work, c->trsv_bytes, st));
-	HPLAI_TRY(launch_trsv(false, c->n, c->A, c->lda, v, c->trsv_work, c->trsv_bytes, st));
+	HPLAI_TRY(launch_trsv(true, c->n, c->A, c->lda, v, c->trsv_work, c->trsv_bytes, st, trans));
+	HPLAI_TRY(launch_trsv(false, c->n, c->A, c->lda, v, c->trsv_work, c->trsv_bytes, st, trans));
 	HPLAI_TRY(pe.end(st));
 	return HPLAI_OK;
 }
 
 // The classical correction: x += U^{-1} L^{-1} r (iterative_refinement.hpp:50-53).
-int correct_ir(hplai_ctx *c, PhaseEvents &pe)
+int correct_ir(hplai_ctx *c, double *x, PhaseEvents &pe, bool trans)
 {
-	HPLAI_TRY(apply_lu_inverse(c, c->r, pe));
-	HPLAI_TRY(launch_axpy1(c->n, c->r, c->x, c->st));
+	HPLAI_TRY(apply_lu_inverse(c, c->r, pe, trans));
+	HPLAI_TRY(launch_axpy1(c->n, c->r, x, c->st));
 	return HPLAI_OK;
 }
 
@@ -500,7 +504,7 @@ int correct_ir(hplai_ctx *c, PhaseEvents &pe)
 // M^{-1} A d = M^{-1} r from d = 0, x += d.  CGS2 orthogonalisation on the
 // device, Givens rotations and the small triangular solve on the host.
 // Stops at |g_{j+1}| <= tol * ||M^{-1} r||_2 or after m steps.
-int correct_gmres(hplai_ctx *c, PhaseEvents &pe, int *inner)
+int correct_gmres(hplai_ctx *c, double *x, PhaseEvents &pe, int *inner, bool trans)
 {
 	const int n = c->n, m = c->gm_restart;
 	const int64_t ldv = c->gm_ldv;
@@ -510,7 +514,7 @@ int correct_gmres(hplai_ctx *c, PhaseEvents &pe, int *inner)
 	double *V = c->gm_v, *w = c->gm_w;
 	*inner = 0;
 	// z = M^{-1} r, beta = ||z||, v_0 = z / beta
-	HPLAI_TRY(apply_lu_inverse(c, c->r, pe));
+	HPLAI_TRY(apply_lu_inverse(c, c->r, pe, trans));
 	HPLAI_TRY(launch_dots(n, 1, c->r, ldv, c->r, part, tmp, 2, st));
 	HPLAI_TRY(launch_scale(n, c->r, tmp, V, st));
 	double beta = 0.0;
@@ -524,9 +528,9 @@ int correct_gmres(hplai_ctx *c, PhaseEvents &pe, int *inner)
 		double *vj = V + j * ldv, *vn = V + (j + 1) * ldv, *hc = H + j * kMaxBasis;
 		// w = M^{-1} A v_j, A regenerated in FP64
 		HPLAI_TRY(pe.record(st, HPLAI_PH_IR_GEMV));
-		HPLAI_TRY(launch_otf_gemv(n, 1.0, vj, 0.0, w, c->seed, c->d, c->gemv_work, c->gemv_bytes, st));
+		HPLAI_TRY(launch_otf_gemv(n, 1.0, vj, 0.0, w, c->seed, c->d, c->gemv_work, c->gemv_bytes, st, trans));
 		HPLAI_TRY(pe.end(st));
-		HPLAI_TRY(apply_lu_inverse(c, w, pe));
+		HPLAI_TRY(apply_lu_inverse(c, w, pe, trans));
 		// two Gram-Schmidt sweeps against v_0..v_j; ||w|| after the second
 		HPLAI_TRY(launch_dots(n, j + 1, V, ldv, w, part, hc, 0, st));
 		HPLAI_TRY(launch_gs_update(n, j + 1, V, ldv, hc, w, part, nullptr, st));
@@ -562,7 +566,7 @@ int correct_gmres(hplai_ctx *c, PhaseEvents &pe, int *inner)
 		y[i] = s / R[static_cast<size_t>(i) * m + i];
 	}
 	HPLAI_CUDA_TRY(cudaMemcpyAsync(yd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
-	HPLAI_TRY(launch_combine(n, k, V, ldv, yd, c->x, st));
+	HPLAI_TRY(launch_combine(n, k, V, ldv, yd, x, st));
 	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
 	return HPLAI_OK;
 }
@@ -585,11 +589,16 @@ extern "C" int hplai_get_refine_counts(hplai_ctx *c, int *outer, int *inner)
 	return HPLAI_OK;
 }
 
-extern "C" int hplai_refine(hplai_ctx *c, int mode, int maxit, hplai_ir_errors *err, int *iters)
+namespace {
+
+// Iterative refinement of op(A) x = rhs (op = identity or transpose) with
+// the context's factors: x_0 = rhs ./ diag(A), then residuals with A
+// regenerated in FP64 and classical or GMRES corrections until the
+// hpl-harness (scaled by ||A||_inf and ||rhs||_inf) is below 16
+// (iterative_refinement.hpp:18-57).
+int refine_core(hplai_ctx *c, int mode, bool trans, const double *rhs, double normb, double *x, int maxit,
+	hplai_ir_errors *err, int *iters)
 {
-	if (!c || maxit < 0) return HPLAI_EINVAL;
-	if (!c->factored) return HPLAI_ESTATE;
-	if (mode != HPLAI_IR && mode != HPLAI_GMRES) return HPLAI_EUNSUPPORTED;
 	const int n = c->n;
 	cudaStream_t st = c->st;
 	c->log_resid.clear();
@@ -600,14 +609,14 @@ extern "C" int hplai_refine(hplai_ctx *c, int mode, int maxit, hplai_ir_errors *
 	if (mode == HPLAI_GMRES) HPLAI_TRY(ensure_gmres_buffers(c));
 	PhaseEvents pe;
 	// x_0 = b ./ diag(A)   (iterative_refinement.hpp:31-34)
-	HPLAI_TRY(launch_div(n, c->rhs, c->d, c->x, st));
+	HPLAI_TRY(launch_div(n, rhs, c->d, x, st));
 	int rc = HPLAI_ENOTCONV;
 	for (int it = 0; it < maxit; ++it) {
-		HPLAI_CUDA_TRY(cudaMemcpyAsync(c->r, c->rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-		HPLAI_TRY(launch_infnorm(n, c->x, c->scal + 2, st));
+		HPLAI_CUDA_TRY(cudaMemcpyAsync(c->r, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+		HPLAI_TRY(launch_infnorm(n, x, c->scal + 2, st));
 		// r = b - A x with A regenerated in FP64 (panel_gemv(-1, ..., 1, r))
 		HPLAI_TRY(pe.record(st, HPLAI_PH_IR_GEMV));
-		HPLAI_TRY(launch_otf_gemv(n, -1.0, c->x, 1.0, c->r, c->seed, c->d, c->gemv_work, c->gemv_bytes, st));
+		HPLAI_TRY(launch_otf_gemv(n, -1.0, x, 1.0, c->r, c->seed, c->d, c->gemv_work, c->gemv_bytes, st, trans));
 		HPLAI_TRY(pe.end(st));
 		HPLAI_TRY(launch_infnorm(n, c->r, c->scal + 3, st));
 		double h[2];
@@ -615,7 +624,7 @@ extern "C" int hplai_refine(hplai_ctx *c, int mode, int maxit, hplai_ir_errors *
 		HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
 		const double normx = h[0], normr = h[1];
 		// iterative_refinement.hpp:43
-		const double hpl = normr / std::fma(c->norma, normx, c->normb) * 1. / (n * DBL_EPSILON / 2);
+		const double hpl = normr / std::fma(c->norma, normx, normb) * 1. / (n * DBL_EPSILON / 2);
 		c->log_resid.push_back(normr);
 		c->log_harness.push_back(hpl);
 		if (iters) *iters = it + 1;
@@ -626,10 +635,10 @@ extern "C" int hplai_refine(hplai_ctx *c, int mode, int maxit, hplai_ir_errors *
 		}
 		if (!std::isfinite(hpl)) break;
 		if (mode == HPLAI_IR) {
-			HPLAI_TRY(correct_ir(c, pe));
+			HPLAI_TRY(correct_ir(c, x, pe, trans));
 		} else {
 			int in = 0;
-			const int gr = correct_gmres(c, pe, &in);
+			const int gr = correct_gmres(c, x, pe, &in, trans);
 			c->gm_inner += in;
 			if (gr != HPLAI_OK) break;
 		}
@@ -643,6 +652,53 @@ extern "C" int hplai_refine(hplai_ctx *c, int mode, int maxit, hplai_ir_errors *
 	c->phase_ms[HPLAI_PH_IR_GEMV] = tmp[HPLAI_PH_IR_GEMV];
 	c->phase_ms[HPLAI_PH_IR_TRSV] = tmp[HPLAI_PH_IR_TRSV];
 	return rc;
+}
+
+// A solve with a caller's right-hand side (host vectors): rhs -> device,
+// refine, x -> host.  Uses the scratch vectors rhs2/x2, not the context's
+// own rhs and x.
+int solve_vector(hplai_ctx *c, bool trans, const double *b, double *x, int maxit, hplai_ir_errors *err, int *iters)
+{
+	if (!c || !b || !x || maxit < 0) return HPLAI_EINVAL;
+	if (!c->factored) return HPLAI_ESTATE;
+	const int n = c->n;
+	cudaStream_t st = c->st;
+	if (!c->rhs2) {
+		HPLAI_CUDA_TRY(cudaMalloc(&c->rhs2, sizeof(double) * n));
+		HPLAI_CUDA_TRY(cudaMalloc(&c->x2, sizeof(double) * n));
+	}
+	HPLAI_CUDA_TRY(cudaMemcpyAsync(c->rhs2, b, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+	HPLAI_TRY(launch_infnorm(n, c->rhs2, c->scal + 4, st));
+	double normb = 0.0;
+	HPLAI_CUDA_TRY(cudaMemcpyAsync(&normb, c->scal + 4, sizeof normb, cudaMemcpyDeviceToHost, st));
+	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
+	const int mode = c->precision == HPLAI_F32_F8 ? HPLAI_GMRES : HPLAI_IR;
+	const int rc = refine_core(c, mode, trans, c->rhs2, normb, c->x2, maxit, err, iters);
+	if (rc != HPLAI_OK && rc != HPLAI_ENOTCONV) return rc;
+	HPLAI_CUDA_TRY(cudaMemcpyAsync(x, c->x2, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
+	return rc;
+}
+
+} // namespace
+
+extern "C" int hplai_refine(hplai_ctx *c, int mode, int maxit, hplai_ir_errors *err, int *iters)
+{
+	if (!c || maxit < 0) return HPLAI_EINVAL;
+	if (!c->factored) return HPLAI_ESTATE;
+	if (mode != HPLAI_IR && mode != HPLAI_GMRES) return HPLAI_EUNSUPPORTED;
+	return refine_core(c, mode, false, c->rhs, c->normb, c->x, maxit, err, iters);
+}
+
+extern "C" int hplai_solve_rhs(hplai_ctx *c, const double *b, double *x, int maxit, hplai_ir_errors *err, int *iters)
+{
+	return solve_vector(c, false, b, x, maxit, err, iters);
+}
+
+extern "C" int hplai_solve_transpose(hplai_ctx *c, const double *g, double *lambda, int maxit, hplai_ir_errors *err,
+	int *iters)
+{
+	return solve_vector(c, true, g, lambda, maxit, err, iters);
 }
 
 extern "C" int hplai_get_x(hplai_ctx *c, double *x)

@@ -115,13 +115,16 @@ int launch_quantize_upanel(int cols, int b, const float *arow, int64_t lda, unsi
 
 // refine.cu
 size_t otf_gemv_workspace(int n);
+// trans: y <- beta*y + alpha*A^T x
 int launch_otf_gemv(int n, double alpha, const double *x, double beta, double *y, uint64_t seed,
-	const double *diag, void *work, size_t work_bytes, cudaStream_t st);
+	const double *diag, void *work, size_t work_bytes, cudaStream_t st, bool trans = false);
 int launch_otf_gemv_block(int64_t n, int mb, int nb, double alpha, const double *x, double *y, uint64_t state00,
 	void *work, size_t work_bytes, cudaStream_t st);
 size_t trsv_workspace(int n);
+// trans: solve with the transpose of the stored triangle (lower = U^T non-unit,
+// upper = L^T unit); otherwise lower = L (unit), upper = U (non-unit).
 int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes,
-	cudaStream_t st);
+	cudaStream_t st, bool trans = false);
 int trsv_status(void *work, cudaStream_t st, int *status);
 int launch_infnorm(int n, const double *x, double *out, cudaStream_t st);
 int launch_div(int n, const double *num, const double *den, double *out, cudaStream_t st);

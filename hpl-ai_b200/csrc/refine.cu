@@ -55,6 +55,9 @@ __device__ __forceinline__ Coeff jump_of(const JumpTable64 &t, uint64_t m)
 constexpr int GEMV_ROWS = 256;
 constexpr int GEMV_COLS = 2048;
 
+// TRANS: y = A^T x, output i walks column i of A (element (j, i) is state
+// j + n*i, so the chain steps by 1 instead of n).
+template <bool TRANS>
 __global__ void __launch_bounds__(GEMV_ROWS) otf_partial_kernel(int64_t n, int mb, int nb, double alpha,
 	const double *__restrict__ x, uint64_t state00, int with_diag, const double *__restrict__ diag,
 	double *__restrict__ part, JumpTable64 tab)
@@ -66,9 +69,11 @@ __global__ void __launch_bounds__(GEMV_ROWS) otf_partial_kernel(int64_t n, int m
 	__syncthreads();
 	const int i = blockIdx.x * GEMV_ROWS + threadIdx.x;
 	if (i >= mb) return;
-	const Coeff jn = jump_of(tab, static_cast<uint64_t>(n));
+	const Coeff jn = jump_of(tab, TRANS ? 1ULL : static_cast<uint64_t>(n));
 	const Coeff jn4 = coeff_mul(coeff_mul(jn, jn), coeff_mul(jn, jn));
-	uint64_t s0 = coeff_apply(jump_of(tab, static_cast<uint64_t>(i) + static_cast<uint64_t>(n) * j0), state00);
+	const uint64_t idx0 = TRANS ? static_cast<uint64_t>(j0) + static_cast<uint64_t>(n) * static_cast<uint64_t>(i)
+	                            : static_cast<uint64_t>(i) + static_cast<uint64_t>(n) * j0;
+	uint64_t s0 = coeff_apply(jump_of(tab, idx0), state00);
 	uint64_t s1 = coeff_apply(jn, s0);
 	uint64_t s2 = coeff_apply(jn, s1);
 	uint64_t s3 = coeff_apply(jn, s2);
@@ -117,7 +122,8 @@ __global__ void otf_reduce_kernel(int mb, int nchunks, double beta, const double
 }
 
 int otf_launch(int64_t n, int mb, int nb, double alpha, const double *x, double beta, double *y,
-	uint64_t state00, int with_diag, const double *diag, void *work, size_t work_bytes, cudaStream_t st)
+	uint64_t state00, int with_diag, const double *diag, void *work, size_t work_bytes, cudaStream_t st,
+	bool trans = false)
 {
 	if (mb <= 0) return HPLAI_OK;
 	const int nchunks = (nb + GEMV_COLS - 1) / GEMV_COLS;
@@ -125,7 +131,12 @@ int otf_launch(int64_t n, int mb, int nb, double alpha, const double *x, double 
 	double *part = static_cast<double *>(work);
 	if (nb > 0) {
 		dim3 grid((mb + GEMV_ROWS - 1) / GEMV_ROWS, nchunks);
-		otf_partial_kernel<<<grid, GEMV_ROWS, 0, st>>>(n, mb, nb, alpha, x, state00, with_diag, diag, part, table());
+		if (trans)
+			otf_partial_kernel<true><<<grid, GEMV_ROWS, 0, st>>>(n, mb, nb, alpha, x, state00, with_diag, diag, part,
+				table());
+		else
+			otf_partial_kernel<false><<<grid, GEMV_ROWS, 0, st>>>(n, mb, nb, alpha, x, state00, with_diag, diag, part,
+				table());
 		count_launches();
 		HPLAI_CUDA_TRY(cudaGetLastError());
 	}
@@ -161,11 +172,16 @@ __global__ void trsv_epoch_kernel(TrsvWork *w)
 	w->status = 0;
 }
 
+// TRANS: the triangle solved is the transpose of the stored one, M[i][j] =
+// a[i*lda + j]: lower = U^T (non-unit), upper = L^T (unit).  Otherwise
+// M[i][j] = a[j*lda + i]: lower = L (unit), upper = U (non-unit).
+template <bool TRANS>
 __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, const float *__restrict__ a,
 	int64_t lda, double *x, TrsvWork *w)
 {
 	extern __shared__ float dyn_smem[];
-	float (*dblk)[TB + 1] = reinterpret_cast<float (*)[TB + 1]>(dyn_smem);   // dblk[i][j] = A[r0+i][r0+j]
+	float (*dblk)[TB + 1] = reinterpret_cast<float (*)[TB + 1]>(dyn_smem);   // dblk[i][j] = M[r0+i][r0+j]
+	const bool unit = TRANS ? !lower : lower;
 	__shared__ double xs[TB];            // x of the block column being applied
 	__shared__ double part[2][TB];       // partial sums of the two column halves
 	__shared__ double rhs[TB];
@@ -185,11 +201,17 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 		const int rows = min(TB, n - r0);
 		// Stage the diagonal block (independent of other CTAs).
 		for (int e = t; e < TB * TB; e += TRSV_THREADS) {
-			const int i = e % TB, j = e / TB;
-			dblk[i][j] = (i < rows && j < rows) ? a[static_cast<int64_t>(r0 + j) * lda + r0 + i] : 0.f;
+			// consecutive threads take the contiguous index of the stored matrix
+			const int i = TRANS ? e / TB : e % TB, j = TRANS ? e % TB : e / TB;
+			const int64_t off = TRANS ? static_cast<int64_t>(r0 + i) * lda + r0 + j : static_cast<int64_t>(r0 + j) * lda + r0 + i;
+			dblk[i][j] = (i < rows && j < rows) ? a[off] : 0.f;
 		}
 		if (t == 0) ready_upto = lower ? 0 : nbt - 1;
 		double acc = 0.0;
+		// TRANS: warp `grp8` takes rows grp8, grp8 + 8, ...; lane takes 4 columns
+		double tacc[TB / 8];
+#pragma unroll
+		for (int q = 0; q < TB / 8; ++q) tacc[q] = 0.0;
 		__syncthreads();
 		// Off-diagonal block columns in dependency order.
 		const int nblk = lower ? r : nbt - 1 - r;
@@ -227,7 +249,33 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 				xs[t] = (j < n) ? __ldcg(&x[j]) : 0.0;   // published by another CTA: bypass L1
 			}
 			__syncthreads();
-			if (lr < rows) {
+			if (TRANS) {
+				const int wv = t >> 5, ln = t & 31;
+				const int cols = min(TB, n - cb * TB);
+				const int j = 4 * ln;
+				if (j < cols) {
+					const double x0 = xs[j], x1 = xs[j + 1], x2 = xs[j + 2], x3 = xs[j + 3];
+#pragma unroll
+					for (int q = 0; q < TB / 8; ++q) {
+						const int i = wv + 8 * q;
+						if (i < rows) {
+							const float *rowp = a + static_cast<int64_t>(r0 + i) * lda + cb * TB + j;
+							if (j + 3 < cols) {
+								const float4 v = *reinterpret_cast<const float4 *>(rowp);
+								double s4 = tacc[q];
+								s4 = fma(static_cast<double>(v.x), x0, s4);
+								s4 = fma(static_cast<double>(v.y), x1, s4);
+								s4 = fma(static_cast<double>(v.z), x2, s4);
+								s4 = fma(static_cast<double>(v.w), x3, s4);
+								tacc[q] = s4;
+							} else {
+								for (int e = 0; e < 4 && j + e < cols; ++e)
+									tacc[q] = fma(static_cast<double>(rowp[e]), xs[j + e], tacc[q]);
+							}
+						}
+					}
+				}
+			} else if (lr < rows) {
 				const float *col = a + static_cast<int64_t>(cb * TB) * lda + r0 + lr;
 				const int cols = min(TB, n - cb * TB);
 				const int jb = grp * (TB / 2), je = min(jb + TB / 2, cols);
@@ -237,7 +285,21 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 			__syncthreads();
 		}
 		if (abort_flag) break;
-		part[grp][lr] = acc;
+		if (TRANS) {
+			// fold the lanes' partial sums of each row in a fixed order
+			const int wv = t >> 5, ln = t & 31;
+#pragma unroll
+			for (int q = 0; q < TB / 8; ++q) {
+				double v = tacc[q];
+				for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+				if (ln == 0) {
+					part[0][wv + 8 * q] = v;
+					part[1][wv + 8 * q] = 0.0;
+				}
+			}
+		} else {
+			part[grp][lr] = acc;
+		}
 		__syncthreads();
 		if (t < TB) rhs[t] = (t < rows) ? x[r0 + t] - (part[0][t] + part[1][t]) : 0.0;
 		__syncthreads();
@@ -252,12 +314,13 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 				double v = (i < rows) ? rhs[i] : 0.0;
 				if (lower) {
 					for (int j = 0; j < 32; ++j) {
+						if (!unit && t == j && i < rows) v = v / static_cast<double>(dblk[i][i]);
 						const double xj = __shfl_sync(0xffffffffu, v, j);
 						if (t > j && base + j < rows) v = fma(-static_cast<double>(dblk[i][base + j]), xj, v);
 					}
 				} else {
 					for (int j = 31; j >= 0; --j) {
-						if (t == j && i < rows) v = v / static_cast<double>(dblk[i][i]);
+						if (!unit && t == j && i < rows) v = v / static_cast<double>(dblk[i][i]);
 						const double xj = __shfl_sync(0xffffffffu, v, j);
 						if (t < j && base + j < rows) v = fma(-static_cast<double>(dblk[i][base + j]), xj, v);
 					}
@@ -326,9 +389,9 @@ size_t otf_gemv_workspace(int n)
 }
 
 int launch_otf_gemv(int n, double alpha, const double *x, double beta, double *y, uint64_t seed, const double *diag,
-	void *work, size_t work_bytes, cudaStream_t st)
+	void *work, size_t work_bytes, cudaStream_t st, bool trans)
 {
-	return otf_launch(n, n, n, alpha, x, beta, y, state_initial(seed), 1, diag, work, work_bytes, st);
+	return otf_launch(n, n, n, alpha, x, beta, y, state_initial(seed), 1, diag, work, work_bytes, st, trans);
 }
 
 int launch_otf_gemv_block(int64_t n, int mb, int nb, double alpha, const double *x, double *y, uint64_t state00,
@@ -344,22 +407,27 @@ size_t trsv_workspace(int n)
 }
 
 int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes,
-	cudaStream_t st)
+	cudaStream_t st, bool trans)
 {
 	if (n <= 0) return HPLAI_OK;
 	if (!work || work_bytes < trsv_workspace(n)) return HPLAI_EINVAL;
 	constexpr size_t dsmem = sizeof(float) * TB * (TB + 1);
 	static int max_blocks = 0;
 	if (!max_blocks) {
-		int per_sm = 0, dev = 0, sms = 0;
-		HPLAI_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		int per_sm = 0, per_sm_t = 0, dev = 0, sms = 0;
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			static_cast<int>(dsmem)));
-		HPLAI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_kernel, TRSV_THREADS, dsmem));
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(dsmem)));
+		HPLAI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_kernel<false>, TRSV_THREADS, dsmem));
+		HPLAI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, trsv_kernel<true>, TRSV_THREADS, dsmem));
 		HPLAI_CUDA_TRY(cudaGetDevice(&dev));
 		HPLAI_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-		max_blocks = per_sm * sms;
+		max_blocks = (per_sm < per_sm_t ? per_sm : per_sm_t) * sms;
 		if (max_blocks <= 0) return HPLAI_EUNSUPPORTED;
 	}
+	// the transposed solve reads rows of the stored matrix as float4
+	if (trans && ((reinterpret_cast<uintptr_t>(a) & 15u) || (lda & 3))) return HPLAI_EINVAL;
 	TrsvWork *w = static_cast<TrsvWork *>(work);
 	trsv_epoch_kernel<<<1, 1, 0, st>>>(w);
 	count_launches();
@@ -368,8 +436,8 @@ int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void 
 	const int grid = nbt < max_blocks ? nbt : max_blocks;
 	int lw = lower ? 1 : 0;
 	void *args[] = {(void *)&lw, (void *)&n, (void *)&a, (void *)&lda, (void *)&x, (void *)&w};
-	HPLAI_CUDA_TRY(cudaLaunchCooperativeKernel(reinterpret_cast<void *>(trsv_kernel), dim3(grid), dim3(TRSV_THREADS),
-		args, dsmem, st));
+	void *fn = trans ? reinterpret_cast<void *>(trsv_kernel<true>) : reinterpret_cast<void *>(trsv_kernel<false>);
+	HPLAI_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(TRSV_THREADS), args, dsmem, st));
 	count_launches();
 	return HPLAI_OK;
 }

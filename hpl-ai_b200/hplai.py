@@ -65,6 +65,9 @@ _get_ir_log = _proto("hplai_get_ir_log", _c_int, _vp, _vp, _vp, _c_int, ctypes.P
 _get_phase_ms = _proto("hplai_get_phase_ms", _c_int, _vp, _vp, _c_int)
 _get_stream = _proto("hplai_get_stream", _vp, _vp)
 launch_count = _proto("hplai_launch_count", ctypes.c_ulonglong)
+_solve_rhs = _proto("hplai_solve_rhs", _c_int, _vp, _vp, _vp, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
+_solve_transpose = _proto("hplai_solve_transpose", _c_int, _vp, _vp, _vp, _c_int, ctypes.POINTER(IRErrors),
+                          ctypes.POINTER(_c_int))
 _set_gmres = _proto("hplai_set_gmres", _c_int, _vp, _c_int, _c_dbl)
 _get_refine_counts = _proto("hplai_get_refine_counts", _c_int, _vp, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int))
 _get_norms = _proto("hplai_get_norms", _c_int, _vp, ctypes.POINTER(_c_dbl), ctypes.POINTER(_c_dbl))
@@ -181,6 +184,26 @@ class Solver:
         if s not in (HPLAI_OK, HPLAI_ENOTCONV):
             check(s, "hplai_refine")
         return RefineResult(e.residual, e.hpl_harness, it.value, s)
+
+    def _solve_vec(self, fn, name, v, maxit):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        if v.shape != (self.n,):
+            raise ValueError(f"{name}: expected a vector of {self.n} doubles")
+        out = np.empty(self.n, dtype=np.float64)
+        e = IRErrors()
+        it = _c_int()
+        s = fn(self._h, _ptr(v), _ptr(out), maxit, ctypes.byref(e), ctypes.byref(it))
+        if s not in (HPLAI_OK, HPLAI_ENOTCONV):
+            check(s, name)
+        return out, RefineResult(e.residual, e.hpl_harness, it.value, s)
+
+    def solve_rhs(self, b, maxit: int = 50):
+        """x = A^{-1} b for a caller's right-hand side (the factors of the last factor())."""
+        return self._solve_vec(_solve_rhs, "hplai_solve_rhs", b, maxit)
+
+    def solve_transpose(self, g, maxit: int = 50):
+        """lambda = A^{-T} g: the adjoint solve."""
+        return self._solve_vec(_solve_transpose, "hplai_solve_transpose", g, maxit)
 
     def set_gmres(self, restart: int = 30, tol: float = 1e-12):
         check(_set_gmres(self._h, restart, tol), "hplai_set_gmres")

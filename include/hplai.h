@@ -134,6 +134,17 @@ int hplai_factor(hplai_ctx *ctx);
  * HPLAI_GMRES corrects with one cycle of FP64 GMRES(restart) on
  * (LU)^{-1} A d = (LU)^{-1} r, same residual, harness and stopping test. */
 int hplai_refine(hplai_ctx *ctx, int mode, int maxit, hplai_ir_errors *err, int *iters);
+/* Solves with the context's factors for a caller's right-hand side (host
+ * vectors of n doubles): A x = b, or the adjoint system A^T lambda = g
+ * (U^T and L^T solves, A^T regenerated as element (j, i) = state j + n*i).
+ * Same refinement, harness and stopping test as hplai_refine (the harness
+ * is scaled by ||A||_inf and ||b||_inf); HPLAI_GMRES corrections for an
+ * HPLAI_F32_F8 context, HPLAI_IR otherwise.  The context's own rhs and x
+ * are left untouched; the refinement log is replaced.  No reference
+ * counterpart: these serve the adjoint (gradient) of the solve. */
+int hplai_solve_rhs(hplai_ctx *ctx, const double *b, double *x, int maxit, hplai_ir_errors *err, int *iters);
+int hplai_solve_transpose(hplai_ctx *ctx, const double *g, double *lambda, int maxit, hplai_ir_errors *err,
+	int *iters);
 /* GMRES parameters: restart length (1..31, default 30) and the relative
  * reduction of the preconditioned residual that ends a cycle (default 1e-12). */
 int hplai_set_gmres(hplai_ctx *ctx, int restart, double tol);
