@@ -71,6 +71,7 @@ struct hplai_ctx {
 	void *trsv_work = nullptr;
 	size_t trsv_bytes = 0;
 	void *getrf_work = nullptr;   // tile flags of the diagonal block LU
+	unsigned *kstatus = nullptr;  // timeout words of this context's Schur [0] and panel [1] kernels
 	uint32_t getrf_epoch = 0;
 	cudaStream_t st = nullptr;    // main stream: Schur updates, refinement, everything else
 	cudaStream_t st2 = nullptr;   // side stream (high priority): diagonal block + panels
@@ -117,6 +118,7 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->gemv_work);
 	cudaFree(c->trsv_work);
 	cudaFree(c->getrf_work);
+	cudaFree(c->kstatus);
 	cudaFree(c->gm_v);
 	cudaFree(c->gm_w);
 	cudaFree(c->gm_small);
@@ -274,8 +276,10 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	c->trsv_bytes = trsv_workspace(n);
 	CTX_ALLOC(c->trsv_work, c->trsv_bytes);
 	CTX_ALLOC(c->getrf_work, getrf_workspace());
+	CTX_ALLOC(c->kstatus, 2 * sizeof(unsigned));
 	if (cudaMemset(c->trsv_work, 0, c->trsv_bytes) != cudaSuccess ||
 		cudaMemset(c->getrf_work, 0, getrf_workspace()) != cudaSuccess ||
+		cudaMemset(c->kstatus, 0, 2 * sizeof(unsigned)) != cudaSuccess ||
 		cudaMemset(c->tcbuf, 0, sizeof(float) * tc_elems) != cudaSuccess) {
 		ctx_free(c);
 		return HPLAI_ECUDA;
@@ -284,9 +288,11 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	for (int i = 0; i < 2 && s == HPLAI_OK; ++i) {
 		s = schur_make_maps(&c->maps[i], c->Lh[i], n, c->ldh, c->Uh[i], n, c->ldh, b);
 		if (s == HPLAI_OK) s = schur_set_cmap(&c->maps[i], c->A, n, n, c->lda);
+		c->maps[i].status = c->kstatus;
 		if (s == HPLAI_OK && precision == HPLAI_F32_F8) {
 			s = schur_make_maps_fp8(&c->maps8[i], c->L8[i], n, c->ld8, c->U8[i], n, c->ld8, b);
 			if (s == HPLAI_OK) s = schur_set_cmap(&c->maps8[i], c->A, n, n, c->lda);
+			c->maps8[i].status = c->kstatus;
 		}
 	}
 	if (s == HPLAI_OK) {
@@ -294,6 +300,7 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		const size_t pn = static_cast<size_t>(ldp) * n, pb = static_cast<size_t>(ldp) * b;
 		s = tc_panels_make(&c->tc, n, b, base, base + pn, ldp, base + 2 * pn, base + 2 * pn + pb,
 			base + 2 * pn + 2 * pb, base + 2 * pn + 3 * pb, base + 2 * pn + 4 * pb);
+		c->tc.status = c->kstatus + 1;
 	}
 	if (s != HPLAI_OK) {
 		ctx_free(c);
@@ -403,8 +410,7 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	if (!c) return HPLAI_EINVAL;
 	if (!c->have_inputs) return HPLAI_ESTATE;
 	const int n = c->n, b = c->b, nb = c->nb;
-	schur_status_reset();
-	tc_status_reset();
+	HPLAI_CUDA_TRY(cudaMemsetAsync(c->kstatus, 0, 2 * sizeof(unsigned), c->st));
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->getrf_work, 0, sizeof(uint32_t), c->st));   // its status word
 	const bool simt = (c->flags & HPLAI_FLAG_SIMT_PANELS) != 0;
 	const bool serial = (c->flags & HPLAI_FLAG_LOOKAHEAD) == 0;
@@ -449,8 +455,12 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	HPLAI_CUDA_TRY(cudaStreamWaitEvent(st, c->ev_panel, 0));
 	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
 	pe.collect(c->phase_ms);
-	HPLAI_TRY(schur_status());
-	HPLAI_TRY(tc_status());
+	{
+		unsigned ks[2] = {0, 0};
+		HPLAI_CUDA_TRY(cudaMemcpyAsync(ks, c->kstatus, sizeof ks, cudaMemcpyDeviceToHost, st));
+		HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
+		if (ks[0] || ks[1]) return HPLAI_ETIMEOUT;
+	}
 	{
 		int gs = HPLAI_OK;
 		HPLAI_TRY(getrf_status(c->getrf_work, st, &gs));
@@ -681,6 +691,35 @@ int solve_vector(hplai_ctx *c, bool trans, const double *b, double *x, int maxit
 }
 
 } // namespace
+
+// Right-hand side `col` of the stream (column n + col), solved with the
+// context's factors into x (host, n doubles).  For the batched solver.
+int hplai_ctx_solve_stream_rhs(hplai_ctx *c, int col, double *x, int maxit, hplai_ir_errors *err, int *iters)
+{
+	if (!c || !x || col < 0 || maxit < 0) return HPLAI_EINVAL;
+	if (!c->factored) return HPLAI_ESTATE;
+	const int n = c->n;
+	cudaStream_t st = c->st;
+	if (!c->rhs2) {
+		HPLAI_CUDA_TRY(cudaMalloc(&c->rhs2, sizeof(double) * n));
+		HPLAI_CUDA_TRY(cudaMalloc(&c->x2, sizeof(double) * n));
+	}
+	const double *rhs = c->rhs;
+	double normb = c->normb;
+	if (col > 0) {
+		HPLAI_TRY(launch_rhs_cols(n, col, 1, c->rhs2, c->seed, st));
+		HPLAI_TRY(launch_infnorm(n, c->rhs2, c->scal + 4, st));
+		HPLAI_CUDA_TRY(cudaMemcpyAsync(&normb, c->scal + 4, sizeof normb, cudaMemcpyDeviceToHost, st));
+		HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
+		rhs = c->rhs2;
+	}
+	const int mode = c->precision == HPLAI_F32_F8 ? HPLAI_GMRES : HPLAI_IR;
+	const int rc = refine_core(c, mode, false, rhs, normb, c->x2, maxit, err, iters);
+	if (rc != HPLAI_OK && rc != HPLAI_ENOTCONV) return rc;
+	HPLAI_CUDA_TRY(cudaMemcpyAsync(x, c->x2, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
+	return rc;
+}
 
 extern "C" int hplai_refine(hplai_ctx *c, int mode, int maxit, hplai_ir_errors *err, int *iters)
 {

@@ -106,13 +106,20 @@ __global__ void __launch_bounds__(128) diag_kernel(int n, int i0, int count, dou
 	if (adiag) adiag[static_cast<int64_t>(k) * (lda + 1)] = __double2float_rn(sum);
 }
 
-// rhs_k = element (i0 + k, n) in FP64.
-__global__ void rhs_kernel(int n, int count, double *rhs, uint64_t seed, JumpTable tab)
+// out[k + r*n] = element (k, n + col0 + r) in FP64: column n of the stream is
+// the right-hand side (pcolvgen), columns n+1, n+2, ... further ones.
+__global__ void rhs_kernel(int n, int col0, int ncols, double *out, uint64_t seed, JumpTable tab)
 {
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= count) return;
-	const uint64_t idx = static_cast<uint64_t>(k) + static_cast<uint64_t>(n) * static_cast<uint64_t>(n);
-	rhs[k] = state_value(coeff_apply(jump_of(tab, idx), state_initial(seed)));
+	if (k >= n) return;
+	const Coeff jn = jump_of(tab, static_cast<uint64_t>(n));
+	uint64_t s = coeff_apply(jump_of(tab, static_cast<uint64_t>(k) +
+	                                          static_cast<uint64_t>(n) * (static_cast<uint64_t>(n) + col0)),
+		state_initial(seed));
+	for (int r = 0; r < ncols; ++r) {
+		out[k + static_cast<int64_t>(r) * n] = state_value(s);
+		s = coeff_apply(jn, s);
+	}
 }
 
 int launch_fill(int n, int i0, int j0, int nrow, int ncol, float *a, int64_t lda, uint64_t seed, int calc_diag,
@@ -142,7 +149,13 @@ int launch_diag(int n, int i0, int count, double *d, float *adiag, int64_t lda, 
 
 int launch_rhs(int n, double *rhs, uint64_t seed, cudaStream_t st)
 {
-	rhs_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, n, rhs, seed, jump_table());
+	return launch_rhs_cols(n, 0, 1, rhs, seed, st);
+}
+
+int launch_rhs_cols(int n, int col0, int ncols, double *out, uint64_t seed, cudaStream_t st)
+{
+	if (n <= 0 || ncols <= 0) return HPLAI_OK;
+	rhs_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, col0, ncols, out, seed, jump_table());
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
@@ -161,6 +174,12 @@ extern "C" int hplai_gen_rhs(int n, uint64_t seed, double *rhs, void *stream)
 {
 	if (n <= 0 || !rhs) return HPLAI_EINVAL;
 	return hplai::launch_rhs(n, rhs, seed, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hplai_gen_rhs_cols(int n, uint64_t seed, int first, int count, double *out, void *stream)
+{
+	if (n <= 0 || first < 0 || count < 0 || !out) return HPLAI_EINVAL;
+	return hplai::launch_rhs_cols(n, first, count, out, seed, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int hplai_gen_diag(int n, uint64_t seed, int i0, int count, double *d, void *stream)

@@ -18,6 +18,8 @@ int launch_fill(int n, int i0, int j0, int nrow, int ncol, float *a, int64_t lda
 	cudaStream_t st);
 int launch_diag(int n, int i0, int count, double *d, float *adiag, int64_t lda, uint64_t seed, cudaStream_t st);
 int launch_rhs(int n, double *rhs, uint64_t seed, cudaStream_t st);
+// columns n + col0 .. n + col0 + ncols - 1 of the stream, column-major with ld n
+int launch_rhs_cols(int n, int col0, int ncols, double *out, uint64_t seed, cudaStream_t st);
 
 // panel.cu
 // getrf.cu: tile-parallel diagonal block LU (bit-exact with the sequential
@@ -46,6 +48,7 @@ struct SchurMaps {
 	float *cbase = nullptr;
 	int64_t cld = 0;
 	bool has_cmap = false;
+	unsigned *status = nullptr;   // device word set on a wait timeout (null: the library's own)
 };
 // L: lrows x k FP16, row-major with ldl; U: urows x k FP16 (row j = column j
 // of U), ldu.  Rows beyond lrows/urows read as zero.
@@ -69,7 +72,7 @@ int schur_make_maps_fp8(SchurMaps *m, const uint8_t *l8, int lrows, int64_t ldl,
 // (sl[(row - sl0) / 128]) and per 128 rows of U8 (su[(row - su0) / 128]).
 int launch_schur_fp8(const SchurMaps &maps8, const float *sl, int sl0, const float *su, int su0, int lrow0, int urow0,
 	int m, int n, float *c, int64_t ldc, int crow0, int ccol0, int max_ctas, cudaStream_t st);
-int schur_status();          // HPLAI_ETIMEOUT if a device wait ran out since the last reset
+int schur_status();          // the library's word: HPLAI_ETIMEOUT if a device wait ran out since the last reset
 void schur_status_reset();
 
 // tcpanel.cu
@@ -88,6 +91,7 @@ struct TcPanels {
 	float *phi, *plo;                // n x ldp: K-major hi/lo copy of the current panel
 	float *uhi, *ulo, *lhi, *llo;    // b x ldp: hi/lo of U11^{-1} and L11^{-1}
 	float *xu, *xl, *wu, *wl;        // ldp x ldp FP32 work of the inversion (zeroed once)
+	unsigned *status = nullptr;      // device word set on a wait timeout (null: the library's own)
 };
 // `work` holds tc_inverse_work_elems(ldp) floats, zeroed before first use.
 inline size_t tc_inverse_work_elems(int64_t ldp) { return 4 * static_cast<size_t>(ldp) * static_cast<size_t>(ldp); }
@@ -146,3 +150,9 @@ int launch_scale(int n, const double *w, const double *den, double *out, cudaStr
 int launch_combine(int n, int nv, const double *v, int64_t ldv, const double *y, double *x, cudaStream_t st);
 
 } // namespace hplai
+
+// api.cu, for the batched solver: right-hand side column n + col of the
+// context's stream, solved with its factors into host memory.
+struct hplai_ctx;
+struct hplai_ir_errors;
+int hplai_ctx_solve_stream_rhs(hplai_ctx *c, int col, double *x, int maxit, hplai_ir_errors *err, int *iters);

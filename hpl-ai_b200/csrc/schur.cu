@@ -87,6 +87,7 @@ struct Params {
 	// (sl, block 0 starting at L row sl0) and per 128 columns of U (su, su0).
 	const float *sl, *su;
 	int sl0, su0;
+	unsigned *status;   // set to 1 on a wait timeout
 };
 
 __device__ unsigned int g_status;
@@ -195,7 +196,7 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 			}
 			ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
 		}
-		if (lane == 0 && !ok) atomicOr(&g_status, 1u);
+		if (lane == 0 && !ok) atomicOr(p.status, 1u);
 	} else if (warp == 1) {
 		// ---------------- MMA issuer ----------------
 		if (lane == 0) {
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 			umma_commit(drain);
 			if (!mbar_wait(drain, 0)) ok = false;
 			*consumed = used;
-			if (!ok) atomicOr(&g_status, 1u);
+			if (!ok) atomicOr(p.status, 1u);
 		}
 	} else {
 		// ---------------- epilogue ----------------
@@ -364,7 +365,7 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 		}
 		// all reduces of this warp complete before the CTA exits
 		if (RED && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-		if (lane == 0 && !ok) atomicOr(&g_status, 1u);
+		if (lane == 0 && !ok) atomicOr(p.status, 1u);
 	}
 
 	tc_fence_before();
@@ -476,6 +477,12 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 	p.su = su;
 	p.sl0 = sl0;
 	p.su0 = su0;
+	p.status = maps.status;
+	if (!p.status) {
+		void *g = nullptr;
+		HPLAI_CUDA_TRY(cudaGetSymbolAddress(&g, g_status));
+		p.status = static_cast<unsigned *>(g);
+	}
 	const int total = p.tiles_m * p.tiles_n;
 	int grid = (max_ctas > 0 && max_ctas < num_sms()) ? max_ctas : num_sms();
 	if (grid > total) grid = total;

@@ -258,6 +258,7 @@ struct TParams {
 	__half *out16;
 	int64_t s16m, s16n;
 	float scale;
+	unsigned *status;   // set to 1 on a wait timeout
 };
 
 __device__ unsigned int g_tstatus;
@@ -346,7 +347,7 @@ __global__ void __launch_bounds__(TTHREADS, 1) tf32x3_kernel(const __grid_consta
 					if (++stage == TSTAGES) { stage = 0; phase ^= 1u; }
 				}
 			}
-			if (!ok) atomicOr(&g_tstatus, 1u);
+			if (!ok) atomicOr(p.status, 1u);
 		}
 	} else if (warp == 1) {
 		if (lane == 0) {
@@ -383,7 +384,7 @@ __global__ void __launch_bounds__(TTHREADS, 1) tf32x3_kernel(const __grid_consta
 			umma_commit(drain);
 			if (!mbar_wait(drain, 0)) ok = false;
 			*consumed = used;
-			if (!ok) atomicOr(&g_tstatus, 1u);
+			if (!ok) atomicOr(p.status, 1u);
 		}
 	} else {
 		const int q = warp & 3;
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(TTHREADS, 1) tf32x3_kernel(const __grid_consta
 			mbar_arrive(&acce[acc]);
 			if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
 		}
-		if (lane == 0 && !ok) atomicOr(&g_tstatus, 1u);
+		if (lane == 0 && !ok) atomicOr(p.status, 1u);
 	}
 
 	tc_fence_before();
@@ -495,10 +496,16 @@ int sm_count()
 
 int launch_tf32x3(const unsigned char *m_ahi, const unsigned char *m_alo, const unsigned char *m_bhi,
 	const unsigned char *m_blo, int arow0, int brow0, int M, int N, int K, float *out32, int64_t s32m, int64_t s32n,
-	__half *out16, int64_t s16m, int64_t s16n, float scale, int max_ctas, cudaStream_t st)
+	__half *out16, int64_t s16m, int64_t s16n, float scale, int max_ctas, cudaStream_t st, unsigned *status)
 {
 	if (M <= 0 || N <= 0) return HPLAI_OK;
 	TParams p;
+	p.status = status;
+	if (!p.status) {
+		void *g = nullptr;
+		HPLAI_CUDA_TRY(cudaGetSymbolAddress(&g, g_tstatus));
+		p.status = static_cast<unsigned *>(g);
+	}
 	p.m = M;
 	p.n = N;
 	p.num_kc = (K + TBK - 1) / TBK;
@@ -603,7 +610,7 @@ int launch_lpanel_tc(const TcPanels &t, int rem, float *acol, int64_t lda, uint1
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// X (rem x b) = A_col U^{-1}: out32 column-major in A, out16 row-major (Lh row = panel row)
 	return launch_tf32x3(t.m_phi, t.m_plo, t.m_uhi, t.m_ulo, 0, 0, rem, b, b, acol, 1, lda,
-		reinterpret_cast<__half *>(lh), ldh, 1, scale, max_ctas, st);
+		reinterpret_cast<__half *>(lh), ldh, 1, scale, max_ctas, st, t.status);
 }
 
 int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint16_t *uh, int64_t ldh, float scale,
@@ -618,7 +625,7 @@ int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint1
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// Y (b x rem) = L^{-1} A_row: out32 column-major in A, out16 with column j of U as row j of Uh
 	return launch_tf32x3(t.m_lhi, t.m_llo, t.m_phi, t.m_plo, 0, 0, b, rem, b, arow, 1, lda,
-		reinterpret_cast<__half *>(uh), 1, ldh, scale, max_ctas, st);
+		reinterpret_cast<__half *>(uh), 1, ldh, scale, max_ctas, st, t.status);
 }
 
 int tc_status()

@@ -102,6 +102,17 @@ trsv_upper = _proto("hplai_trsv_upper", _c_int, _c_int, _vp, _c_i64, _vp, _vp, _
 infnorm = _proto("hplai_infnorm", _c_int, _c_int, _vp, _vp, _vp)
 
 
+gen_rhs_cols = _proto("hplai_gen_rhs_cols", _c_int, _c_int, _c_u64, _c_int, _c_int, _vp, _vp)
+_batch_create = _proto("hplai_batch_create", _c_int, ctypes.POINTER(_vp), _c_int, _vp, _vp, _vp, _c_int, ctypes.c_uint,
+                       _c_int)
+_batch_destroy = _proto("hplai_batch_destroy", _c_int, _vp)
+_batch_solve = _proto("hplai_batch_solve", _c_int, _vp, _c_int)
+_batch_result = _proto("hplai_batch_result", _c_int, _vp, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int),
+                       ctypes.POINTER(_c_int))
+_batch_get_x = _proto("hplai_batch_get_x", _c_int, _vp, _c_int, _vp, _c_i64)
+_batch_block = _proto("hplai_batch_block", _c_int, _vp, _c_int)
+
+
 class HplaiError(RuntimeError):
     def __init__(self, status: int, what: str):
         buf = ctypes.create_string_buffer(512)
@@ -277,3 +288,65 @@ class Solver:
         a, b = _c_dbl(), _c_dbl()
         check(_get_norms(self._h, ctypes.byref(a), ctypes.byref(b)), "hplai_get_norms")
         return a.value, b.value
+
+
+class Batch:
+    """Many independent systems (sizes n[s], nrhs[s] right-hand sides, seeds[s])."""
+
+    def __init__(self, n, nrhs, seeds, precision: int = F32_F16, flags: int = 0, workers: int = 0):
+        self.n = np.ascontiguousarray(n, dtype=np.int32)
+        self.nrhs = np.ascontiguousarray(nrhs, dtype=np.int32)
+        self.seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+        if not (len(self.n) == len(self.nrhs) == len(self.seeds)):
+            raise ValueError("n, nrhs and seeds must have the same length")
+        h = _vp()
+        check(_batch_create(ctypes.byref(h), len(self.n), _ptr(self.n), _ptr(self.nrhs), _ptr(self.seeds), precision,
+                            flags, workers), "hplai_batch_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def solve(self, maxit: int = 50) -> int:
+        s = _batch_solve(self._h, maxit)
+        if s not in (HPLAI_OK, HPLAI_ENOTCONV):
+            check(s, "hplai_batch_solve")
+        return s
+
+    def result(self, s: int) -> RefineResult:
+        e = IRErrors()
+        it, st = _c_int(), _c_int()
+        check(_batch_result(self._h, s, ctypes.byref(e), ctypes.byref(it), ctypes.byref(st)), "hplai_batch_result")
+        return RefineResult(e.residual, e.hpl_harness, it.value, st.value)
+
+    def x(self, s: int) -> np.ndarray:
+        out = np.empty((int(self.nrhs[s]), int(self.n[s])), dtype=np.float64)   # rows = columns of x
+        check(_batch_get_x(self._h, s, _ptr(out), int(self.n[s])), "hplai_batch_get_x")
+        return out.T
+
+    def block(self, s: int) -> int:
+        return _batch_block(self._h, s)
+
+
+def batch_sizes(count: int = 512, rng_seed: int = 20240611, lo: int = 256, hi: int = 4096):
+    """System orders n_s = round64(exp(U(ln lo, ln hi))) and right-hand-side
+    counts U{1..8} from a fixed host generator (numpy PCG64, rng_seed)."""
+    rng = np.random.default_rng(rng_seed)
+    n = np.exp(rng.uniform(np.log(lo), np.log(hi), count))
+    n = np.clip(np.rint(n / 64).astype(np.int64) * 64, lo, hi).astype(np.int32)
+    nrhs = rng.integers(1, 9, count).astype(np.int32)
+    return n, nrhs

@@ -178,6 +178,32 @@ int hplai_solve_host(hplai_ctx *ctx, const float *a, int64_t lda, const double *
 int hplai_format_report(int n, double seconds, hplai_ir_errors err, char *buf, size_t len);
 
 /* ---------------------------------------------------------------------- */
+/* Batched solver (no reference counterpart: the reference solves one      */
+/* system per run).                                                        */
+/* ---------------------------------------------------------------------- */
+typedef struct hplai_batch hplai_batch;
+
+/* `count` independent systems: system s is the HPL-AI matrix of order n[s]
+ * from seeds[s] (as hplai_generate) with nrhs[s] >= 1 right-hand sides,
+ * columns n[s], n[s]+1, ... of its stream.  The block size of each system is
+ * the largest of 256, 128, 64, 32, 16 dividing n[s].  `workers` host
+ * threads (0: 8) feed the GPU; every system gets its own context. */
+int hplai_batch_create(hplai_batch **batch, int count, const int *n, const int *nrhs, const uint64_t *seeds,
+	int precision, unsigned flags, int workers);
+int hplai_batch_destroy(hplai_batch *batch);
+/* Generate, factor and refine every right-hand side of every system
+ * (largest systems first).  HPLAI_ENOTCONV if any right-hand side missed
+ * hpl-harness < 16 within maxit steps. */
+int hplai_batch_solve(hplai_batch *batch, int maxit);
+/* System s: the largest hpl-harness over its right-hand sides ({-1,-1} on
+ * failure), the most refinement steps any took, and its status. */
+int hplai_batch_result(hplai_batch *batch, int s, hplai_ir_errors *worst, int *iters, int *status);
+/* System s's solutions, n[s] x nrhs[s] column-major with leading dimension ldx. */
+int hplai_batch_get_x(hplai_batch *batch, int s, double *x, int64_t ldx);
+/* The block size chosen for system s. */
+int hplai_batch_block(hplai_batch *batch, int s);
+
+/* ---------------------------------------------------------------------- */
 /* Leaf kernels on caller-owned device buffers.                            */
 /* ---------------------------------------------------------------------- */
 
@@ -190,6 +216,8 @@ int hplai_fill_panel(int n, int i0, int j0, int nrow, int ncol, float *a, int64_
 
 /* pcolvgen (matgen.hpp:193-207): rhs_i = element (i, n) in FP64, i < n. */
 int hplai_gen_rhs(int n, uint64_t seed, double *rhs, void *stream);
+/* pcolvgen extended: out[i + r*n] = element (i, n + first + r), r < count. */
+int hplai_gen_rhs_cols(int n, uint64_t seed, int first, int count, double *out, void *stream);
 
 /* pdiaggen / calc_diag (matgen.hpp:209-225, hpl_rand.hpp:108-123):
  * d_i for i in [i0, i0+count). */
