@@ -369,6 +369,113 @@ def run_ours(args):
     return 0
 
 
+def run_batch(args):
+    """Many independent systems on one GPU (log-uniform orders 256..4096,
+    1..8 right-hand sides, system s seeded with s), through the batched C API."""
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local if world > 1 else 0)
+    import hplai
+    count = args.batch_count
+    n, nrhs = hplai.batch_sizes(count, rng_seed=args.batch_seed)
+    seeds = [rank * count + s for s in range(count)]
+    flops = float(sum(2.0 / 3.0 * float(v) ** 3 + 1.5 * float(v) ** 2 * int(r) for v, r in zip(n, nrhs)))
+    dev = torch.cuda.current_device()
+    t0 = time.perf_counter()
+    bt = hplai.Batch(n, nrhs, seeds, workers=args.batch_workers)
+    create_s = time.perf_counter() - t0
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        if bt.solve() != hplai.HPLAI_OK:
+            raise RuntimeError("batch did not converge")
+    sampler = ClockSampler(dev)
+    sampler.start()
+    l0 = hplai.launch_count()
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = bt.solve()
+        e1.record(stream)
+        e1.synchronize()
+        if rc != hplai.HPLAI_OK:
+            raise RuntimeError("batch did not converge")
+        times.append(e0.elapsed_time(e1))
+    launches = hplai.launch_count() - l0
+    clocks = sampler.stop()
+    worst = max(bt.result(s).hpl_harness for s in range(count))
+    bt.close()
+    total_ms = sum(times)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    value = world * args.steps * flops / (float(t.item()) * 1e-3) / 1e9
+    if rank == 0:
+        xbytes = int(sum(int(v) * int(r) * 8 for v, r in zip(n, nrhs)))
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": float(t.item()) / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp16/fp32/fp64",
+            "data": f"synthetic (LCG matrices, system s seeded with s; sizes from host generator seed {args.batch_seed})",
+            "config": {"workload": f"batched: {count} systems, n log-uniform 256..4096 (round 64), 1..8 "
+                                   f"right-hand sides each, plain form + IR", "systems": count,
+                       "n_total": int(n.sum()), "rhs_total": int(nrhs.sum()), "workers": args.batch_workers,
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "worst_hpl_harness": worst, "context_create_s": create_s, "gpu_launches": int(launches),
+            "clocks": clocks,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(count * 16),
+                    "d2h_bytes_per_step": xbytes,
+                    "note": "the batched call itself: sizes and seeds in, every solution vector out"},
+        }), flush=True)
+    return 0
+
+
+def run_adjoint(args):
+    """Forward solve and adjoint (transposed) solve of one system, n = 8192,
+    b = 256 by default: factor + A x = b + A^T lambda = g."""
+    import torch
+    import numpy as np
+    torch.cuda.set_device(0)
+    import hplai
+    n, b = args.n, args.b
+    rng = np.random.default_rng(2024)
+    bvec = rng.uniform(-1, 1, n)
+    g = rng.uniform(-1, 1, n)
+    s = hplai.Solver(n, b)
+    ext = torch.cuda.ExternalStream(s.stream())
+    res = []
+    for i in range(args.warmup + args.steps):
+        s.generate(42)
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record(ext)
+        s.factor()
+        e[1].record(ext)
+        x, r1 = s.solve_rhs(bvec)
+        e[2].record(ext)
+        lam, r2 = s.solve_transpose(g)
+        e[3].record(ext)
+        e[3].synchronize()
+        if r1.status != hplai.HPLAI_OK or r2.status != hplai.HPLAI_OK:
+            raise RuntimeError("adjoint solve did not converge")
+        if i >= args.warmup:
+            res.append([e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), e[2].elapsed_time(e[3]), r2.hpl_harness])
+    s.close()
+    arr = np.array(res)
+    fl = hpl_flops(n)
+    print(json.dumps({
+        "metric": METRIC, "value": fl / (arr[:, 0].sum() + arr[:, 1].sum()) * len(res) * 1e-6, "unit": UNIT,
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": float(arr[:, :3].sum(1).mean()), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp16/fp32/fp64", "data": "synthetic (LCG matrix seed 42; b, g ~ U[-1,1) seed 2024)",
+        "config": {"workload": f"adjoint: factor, A x = b and A^T lambda = g at n={n} b={b}", "n": n, "b": b},
+        "factor_ms": float(arr[:, 0].mean()), "forward_solve_ms": float(arr[:, 1].mean()),
+        "adjoint_solve_ms": float(arr[:, 2].mean()), "adjoint_hpl_harness": float(arr[-1, 3]),
+    }), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -382,6 +489,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--precision", choices=("f16", "f8"), default="f16",
                     help="Schur update operands: FP16 (plain form) or e4m3 with per-128 factors")
+    ap.add_argument("--workload", choices=("solve", "batch", "adjoint"), default="solve",
+                    help="solve: one system (default n=65536 b=512); batch: many systems; adjoint: forward + "
+                         "transposed solves")
+    ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--batch-seed", type=int, default=20240611)
+    ap.add_argument("--batch-workers", type=int, default=8)
     ap.add_argument("--lookahead", action="store_true",
                     help="form the next step's diagonal block and panels on a side stream (HPLAI_FLAG_LOOKAHEAD)")
     ap.add_argument("--refine", choices=("ir", "gmres"), default=None,
@@ -389,6 +502,10 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     return run_ours(args)
 
 

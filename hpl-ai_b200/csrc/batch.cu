@@ -34,9 +34,11 @@ struct hplai_batch {
 
 namespace {
 
+// The largest block size <= 512 that is a multiple of 16 and divides n:
+// fewer, larger steps (each step costs a fixed number of launches).
 int pick_block(int n)
 {
-	for (int b : {256, 128, 64, 32, 16})
+	for (int b = 512; b >= 16; b -= 16)
 		if (n % b == 0 && n >= b) return b;
 	return 0;
 }

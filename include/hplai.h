@@ -186,7 +186,7 @@ typedef struct hplai_batch hplai_batch;
 /* `count` independent systems: system s is the HPL-AI matrix of order n[s]
  * from seeds[s] (as hplai_generate) with nrhs[s] >= 1 right-hand sides,
  * columns n[s], n[s]+1, ... of its stream.  The block size of each system is
- * the largest of 256, 128, 64, 32, 16 dividing n[s].  `workers` host
+ * the largest multiple of 16 up to 512 dividing n[s].  `workers` host
  * threads (0: 8) feed the GPU; every system gets its own context. */
 int hplai_batch_create(hplai_batch **batch, int count, const int *n, const int *nrhs, const uint64_t *seeds,
 	int precision, unsigned flags, int workers);

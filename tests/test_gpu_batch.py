@@ -48,7 +48,7 @@ def test_small_batch_vs_dense(hplai, oracle, torch_cuda):
 
 def test_batch_rejects_bad_sizes(hplai):
     with pytest.raises(hplai.HplaiError):
-        hplai.Batch([100], [1], [1])          # no block size in {256, 128, 64, 32, 16} divides 100
+        hplai.Batch([100], [1], [1])          # no multiple of 16 divides 100
     with pytest.raises(hplai.HplaiError):
         hplai.Batch([256], [0], [1])
 
