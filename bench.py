@@ -112,6 +112,26 @@ def dist_setup():
     return world, rank, local
 
 
+def replica_value(total_ms, units, world, device=None):
+    """Whole-job throughput over `world` replicas: the units of all ranks over
+    the slowest rank's time (max over ranks), in units/s / 1e9.  Every rank
+    takes the same two collectives."""
+    import torch
+    t = torch.tensor([float(total_ms)], dtype=torch.float64, device=device)
+    u = torch.tensor([float(units)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    max_ms = float(t.item())
+    return float(u.item()) / (max_ms * 1e-3) / 1e9, max_ms
+
+
+def batch_seeds(rank, count):
+    """Seeds of rank `rank`'s systems: replicas solve disjoint systems."""
+    return [rank * count + s for s in range(count)]
+
+
 def cpu_solve_gflops(n, b, threads):
     """One CPU solve of the sample: the reference build if present, else the oracle."""
     ref_bin = os.path.join(ROOT, "oracle", "_ref", "ref_driver.out")
@@ -256,11 +276,7 @@ def run_ours(args):
     clocks = sampler.stop()
 
     total_ms = sum(r[0] for r in results)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * args.steps * hpl_flops(n) / (max_ms * 1e-3) / 1e9
+    value, max_ms = replica_value(total_ms, args.steps * hpl_flops(n), world, device="cuda")
 
     # Roofline of the dominant kernel (the Schur GEMM), timed inside the
     # library with CUDA events around each launch on its stream.
@@ -378,7 +394,7 @@ def run_batch(args):
     import hplai
     count = args.batch_count
     n, nrhs = hplai.batch_sizes(count, rng_seed=args.batch_seed)
-    seeds = [rank * count + s for s in range(count)]
+    seeds = batch_seeds(rank, count)
     flops = float(sum(2.0 / 3.0 * float(v) ** 3 + 1.5 * float(v) ** 2 * int(r) for v, r in zip(n, nrhs)))
     dev = torch.cuda.current_device()
     t0 = time.perf_counter()
@@ -407,15 +423,12 @@ def run_batch(args):
     worst = max(bt.result(s).hpl_harness for s in range(count))
     bt.close()
     total_ms = sum(times)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    value = world * args.steps * flops / (float(t.item()) * 1e-3) / 1e9
+    value, max_ms = replica_value(total_ms, args.steps * flops, world, device="cuda")
     if rank == 0:
         xbytes = int(sum(int(v) * int(r) * 8 for v, r in zip(n, nrhs)))
         print(json.dumps({
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": float(t.item()) / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp16/fp32/fp64",
             "data": f"synthetic (LCG matrices, system s seeded with s; sizes from host generator seed {args.batch_seed})",
             "config": {"workload": f"batched: {count} systems, n log-uniform 256..4096 (round 64), 1..8 "
@@ -476,6 +489,51 @@ def run_adjoint(args):
     return 0
 
 
+def run_gemm(args):
+    """The Schur GEMM alone through its leaf entry point: C (m x n FP32) -= L U
+    with FP16 (or e4m3) panels of width k, C larger than L2."""
+    import torch
+    torch.cuda.set_device(0)
+    import hplai
+    m, n, k = args.m, args.n_cols, args.k
+    fp8 = args.precision == "f8"
+    torch.manual_seed(0)
+    c = torch.zeros(n, m, dtype=torch.float32, device="cuda")
+    if fp8:
+        ld = (k + 127) // 128 * 128
+        lp = (torch.rand(m, ld, device="cuda") * 4).to(torch.float8_e4m3fn).view(torch.uint8)
+        up = (torch.rand(n, ld, device="cuda") * 4).to(torch.float8_e4m3fn).view(torch.uint8)
+        sl = torch.ones((m + 127) // 128, device="cuda")
+        su = torch.ones((n + 127) // 128, device="cuda")
+
+        def call():
+            hplai.check(hplai.f8gemm_minus(m, n, k, lp.data_ptr(), ld, sl.data_ptr(), up.data_ptr(), ld, su.data_ptr(),
+                                           c.data_ptr(), m, None))
+    else:
+        ld = (k + 63) // 64 * 64
+        lp = torch.rand(m, ld, device="cuda").half()
+        up = torch.rand(n, ld, device="cuda").half()
+
+        def call():
+            hplai.check(hplai.shgemm_minus(m, n, k, lp.data_ptr(), ld, up.data_ptr(), ld, c.data_ptr(), m, None))
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        call()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    flops = 2.0 * m * n * k
+    byts = 8.0 * m * n + (m + n) * k * (1 if fp8 else 2)
+    print(json.dumps({"workload": f"schur GEMM leaf m={m} n={n} k={k} {'e4m3' if fp8 else 'fp16'}",
+                      "ms_per_launch": ms, "tflops": flops / ms / 1e9, "gbs": byts / ms / 1e6,
+                      "algorithmic_bytes": byts, "flops": flops}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -489,9 +547,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--precision", choices=("f16", "f8"), default="f16",
                     help="Schur update operands: FP16 (plain form) or e4m3 with per-128 factors")
-    ap.add_argument("--workload", choices=("solve", "batch", "adjoint"), default="solve",
+    ap.add_argument("--workload", choices=("solve", "batch", "adjoint", "gemm"), default="solve",
                     help="solve: one system (default n=65536 b=512); batch: many systems; adjoint: forward + "
                          "transposed solves")
+    ap.add_argument("--m", type=int, default=16384, help="gemm workload: rows of C")
+    ap.add_argument("--n-cols", type=int, default=16384, help="gemm workload: columns of C")
+    ap.add_argument("--k", type=int, default=512, help="gemm workload: panel width")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-seed", type=int, default=20240611)
     ap.add_argument("--batch-workers", type=int, default=8)
@@ -506,6 +567,8 @@ def main():
         return run_batch(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "gemm":
+        return run_gemm(args)
     return run_ours(args)
 
 
