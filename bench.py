@@ -498,7 +498,8 @@ def run_gemm(args):
     m, n, k = args.m, args.n_cols, args.k
     fp8 = args.precision == "f8"
     torch.manual_seed(0)
-    c = torch.zeros(n, m, dtype=torch.float32, device="cuda")
+    ldc = (m + 63) // 64 * 64 + 64   # the solver's padded leading dimension (no power-of-two stride)
+    c = torch.zeros(n, ldc, dtype=torch.float32, device="cuda")
     if fp8:
         ld = (k + 127) // 128 * 128
         lp = (torch.rand(m, ld, device="cuda") * 4).to(torch.float8_e4m3fn).view(torch.uint8)
@@ -508,14 +509,14 @@ def run_gemm(args):
 
         def call():
             hplai.check(hplai.f8gemm_minus(m, n, k, lp.data_ptr(), ld, sl.data_ptr(), up.data_ptr(), ld, su.data_ptr(),
-                                           c.data_ptr(), m, None))
+                                           c.data_ptr(), ldc, None))
     else:
         ld = (k + 63) // 64 * 64
         lp = torch.rand(m, ld, device="cuda").half()
         up = torch.rand(n, ld, device="cuda").half()
 
         def call():
-            hplai.check(hplai.shgemm_minus(m, n, k, lp.data_ptr(), ld, up.data_ptr(), ld, c.data_ptr(), m, None))
+            hplai.check(hplai.shgemm_minus(m, n, k, lp.data_ptr(), ld, up.data_ptr(), ld, c.data_ptr(), ldc, None))
     for _ in range(args.warmup):
         call()
     torch.cuda.synchronize()
