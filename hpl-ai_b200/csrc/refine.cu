@@ -172,16 +172,57 @@ __global__ void trsv_epoch_kernel(TrsvWork *w)
 	w->status = 0;
 }
 
+// Copy block (rows r0.., cols c0..) of M into shared memory with cp.async:
+// TRANS (M[i][j] = a[i*lda + j]) as blk[i*TB + j], otherwise
+// (M[i][j] = a[j*lda + i]) as blk[j*TB + i]; rows >= rows / cols >= cols
+// are zero.  vec: 16-byte copies through L2 (a 16-byte aligned, lda % 4 == 0),
+// else 4-byte copies.  The matrix is read-only for the whole solve.
+template <bool TRANS>
+__device__ __forceinline__ void stage_block(float *blk, const float *a, int64_t lda, int r0, int c0, int rows,
+	int cols, bool vec)
+{
+	const int t = threadIdx.x;
+	// contiguous index of the stored matrix: rows for M = stored, columns for M^T
+	const int ncont = TRANS ? cols : rows, nline = TRANS ? rows : cols;
+	if (vec) {
+		for (int e = t; e < TB * TB / 4; e += TRSV_THREADS) {
+			const int line = e / (TB / 4), g = (e % (TB / 4)) * 4;
+			int bytes = (line < nline) ? (ncont - g) * 4 : 0;
+			bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
+			const float *src = TRANS ? a + static_cast<int64_t>(r0 + (bytes ? line : 0)) * lda + c0 + (bytes ? g : 0)
+			                         : a + static_cast<int64_t>(c0 + (bytes ? line : 0)) * lda + r0 + (bytes ? g : 0);
+			asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(blk + line * TB + g)),
+				"l"(src), "r"(bytes) : "memory");
+		}
+	} else {
+		for (int e = t; e < TB * TB; e += TRSV_THREADS) {
+			const int line = e / TB, g = e % TB;
+			const bool in = line < nline && g < ncont;
+			const float *src = TRANS ? a + static_cast<int64_t>(r0 + (in ? line : 0)) * lda + c0 + (in ? g : 0)
+			                         : a + static_cast<int64_t>(c0 + (in ? line : 0)) * lda + r0 + (in ? g : 0);
+			asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(blk + line * TB + g)), "l"(src),
+				"r"(in ? 4 : 0) : "memory");
+		}
+	}
+	asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
 // TRANS: the triangle solved is the transpose of the stored one, M[i][j] =
 // a[i*lda + j]: lower = U^T (non-unit), upper = L^T (unit).  Otherwise
 // M[i][j] = a[j*lda + i]: lower = L (unit), upper = U (non-unit).
+// The off-diagonal blocks of a block row stream through two shared-memory
+// buffers: block q+1 is being copied while block q waits for its x and is
+// applied, so the latency of the factor reads leaves the dependency chain.
 template <bool TRANS>
 __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, const float *__restrict__ a,
 	int64_t lda, double *x, TrsvWork *w)
 {
-	extern __shared__ float dyn_smem[];
+	extern __shared__ __align__(16) float dyn_smem[];
 	float (*dblk)[TB + 1] = reinterpret_cast<float (*)[TB + 1]>(dyn_smem);   // dblk[i][j] = M[r0+i][r0+j]
+	float *bufs = dyn_smem + TB * (TB + 1) + 3;   // two TB x TB blocks, 16-byte aligned
+	bufs = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(bufs) + 15) & ~static_cast<uintptr_t>(15));
 	const bool unit = TRANS ? !lower : lower;
+	const bool vec = ((reinterpret_cast<uintptr_t>(a) & 15u) == 0) && ((lda & 3) == 0);
 	__shared__ double xs[TB];            // x of the block column being applied
 	__shared__ double part[2][TB];       // partial sums of the two column halves
 	__shared__ double rhs[TB];
@@ -199,24 +240,35 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 		const int r = lower ? idx : nbt - 1 - idx;
 		const int r0 = r * TB;
 		const int rows = min(TB, n - r0);
+		const int nblk = lower ? r : nbt - 1 - r;
+		// first off-diagonal block in flight before anything waits
+		if (nblk > 0) {
+			const int cb0 = lower ? 0 : nbt - 1;
+			stage_block<TRANS>(bufs, a, lda, r0, cb0 * TB, rows, min(TB, n - cb0 * TB), vec);
+		}
 		// Stage the diagonal block (independent of other CTAs).
 		for (int e = t; e < TB * TB; e += TRSV_THREADS) {
 			// consecutive threads take the contiguous index of the stored matrix
-			const int i = TRANS ? e / TB : e % TB, j = TRANS ? e % TB : e / TB;
-			const int64_t off = TRANS ? static_cast<int64_t>(r0 + i) * lda + r0 + j : static_cast<int64_t>(r0 + j) * lda + r0 + i;
-			dblk[i][j] = (i < rows && j < rows) ? a[off] : 0.f;
+			const int i = TRANS ? e / TB : e % TB, jj = TRANS ? e % TB : e / TB;
+			const int64_t off = TRANS ? static_cast<int64_t>(r0 + i) * lda + r0 + jj : static_cast<int64_t>(r0 + jj) * lda + r0 + i;
+			dblk[i][jj] = (i < rows && jj < rows) ? a[off] : 0.f;
 		}
 		if (t == 0) ready_upto = lower ? 0 : nbt - 1;
 		double acc = 0.0;
-		// TRANS: warp `grp8` takes rows grp8, grp8 + 8, ...; lane takes 4 columns
+		// TRANS: warp `wv` takes rows wv, wv + 8, ...; lane takes 4 columns
 		double tacc[TB / 8];
 #pragma unroll
 		for (int q = 0; q < TB / 8; ++q) tacc[q] = 0.0;
 		__syncthreads();
 		// Off-diagonal block columns in dependency order.
-		const int nblk = lower ? r : nbt - 1 - r;
 		for (int q = 0; q < nblk; ++q) {
 			const int cb = lower ? q : nbt - 1 - q;
+			const int cols = min(TB, n - cb * TB);
+			float *cur = bufs + (q & 1) * TB * TB;
+			if (q + 1 < nblk) {
+				const int cn = lower ? q + 1 : nbt - 2 - q;
+				stage_block<TRANS>(bufs + ((q + 1) & 1) * TB * TB, a, lda, r0, cn * TB, rows, min(TB, n - cn * TB), vec);
+			}
 			if (t < 32) {
 				// Learn how far the published prefix reaches, 32 flags at a time.
 				bool have = lower ? (cb < ready_upto) : (cb > ready_upto);
@@ -238,7 +290,7 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 							if (t == 0) abort_flag = 1;
 							break;
 						}
-						__nanosleep(200);
+						__nanosleep(100);
 					}
 				}
 			}
@@ -248,53 +300,47 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 				const int j = cb * TB + t;
 				xs[t] = (j < n) ? __ldcg(&x[j]) : 0.0;   // published by another CTA: bypass L1
 			}
+			// block q has landed (block q+1 may still be in flight)
+			if (q + 1 < nblk)
+				asm volatile("cp.async.wait_group 1;" ::: "memory");
+			else
+				asm volatile("cp.async.wait_group 0;" ::: "memory");
 			__syncthreads();
 			if (TRANS) {
 				const int wv = t >> 5, ln = t & 31;
-				const int cols = min(TB, n - cb * TB);
 				const int j = 4 * ln;
 				if (j < cols) {
 					const double x0 = xs[j], x1 = xs[j + 1], x2 = xs[j + 2], x3 = xs[j + 3];
 #pragma unroll
-					for (int q = 0; q < TB / 8; ++q) {
-						const int i = wv + 8 * q;
-						if (i < rows) {
-							const float *rowp = a + static_cast<int64_t>(r0 + i) * lda + cb * TB + j;
-							if (j + 3 < cols) {
-								const float4 v = *reinterpret_cast<const float4 *>(rowp);
-								double s4 = tacc[q];
-								s4 = fma(static_cast<double>(v.x), x0, s4);
-								s4 = fma(static_cast<double>(v.y), x1, s4);
-								s4 = fma(static_cast<double>(v.z), x2, s4);
-								s4 = fma(static_cast<double>(v.w), x3, s4);
-								tacc[q] = s4;
-							} else {
-								for (int e = 0; e < 4 && j + e < cols; ++e)
-									tacc[q] = fma(static_cast<double>(rowp[e]), xs[j + e], tacc[q]);
-							}
-						}
+					for (int qq = 0; qq < TB / 8; ++qq) {
+						const int i = wv + 8 * qq;
+						const float4 v = *reinterpret_cast<const float4 *>(cur + i * TB + j);
+						double s4 = tacc[qq];
+						s4 = fma(static_cast<double>(v.x), x0, s4);
+						s4 = fma(static_cast<double>(v.y), x1, s4);
+						s4 = fma(static_cast<double>(v.z), x2, s4);
+						s4 = fma(static_cast<double>(v.w), x3, s4);
+						tacc[qq] = s4;
 					}
 				}
 			} else if (lr < rows) {
-				const float *col = a + static_cast<int64_t>(cb * TB) * lda + r0 + lr;
-				const int cols = min(TB, n - cb * TB);
 				const int jb = grp * (TB / 2), je = min(jb + TB / 2, cols);
 #pragma unroll 8
-				for (int j = jb; j < je; ++j) acc = fma(static_cast<double>(col[static_cast<int64_t>(j) * lda]), xs[j], acc);
+				for (int j = jb; j < je; ++j) acc = fma(static_cast<double>(cur[j * TB + lr]), xs[j], acc);
 			}
-			__syncthreads();
+			__syncthreads();   // this buffer is refilled two blocks later
 		}
 		if (abort_flag) break;
 		if (TRANS) {
 			// fold the lanes' partial sums of each row in a fixed order
 			const int wv = t >> 5, ln = t & 31;
 #pragma unroll
-			for (int q = 0; q < TB / 8; ++q) {
-				double v = tacc[q];
+			for (int qq = 0; qq < TB / 8; ++qq) {
+				double v = tacc[qq];
 				for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
 				if (ln == 0) {
-					part[0][wv + 8 * q] = v;
-					part[1][wv + 8 * q] = 0.0;
+					part[0][wv + 8 * qq] = v;
+					part[1][wv + 8 * qq] = 0.0;
 				}
 			}
 		} else {
@@ -306,23 +352,23 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 		// Diagonal block: 32-row sub-blocks solved by warp 0 with shuffles,
 		// the remaining rows updated by all threads.
 		const int nsb = (rows + 31) / 32;
-		for (int s = 0; s < nsb; ++s) {
-			const int sb = lower ? s : nsb - 1 - s;
+		for (int sblk = 0; sblk < nsb; ++sblk) {
+			const int sb = lower ? sblk : nsb - 1 - sblk;
 			const int base = sb * 32;
 			if (t < 32) {
 				const int i = base + t;
 				double v = (i < rows) ? rhs[i] : 0.0;
 				if (lower) {
-					for (int j = 0; j < 32; ++j) {
-						if (!unit && t == j && i < rows) v = v / static_cast<double>(dblk[i][i]);
-						const double xj = __shfl_sync(0xffffffffu, v, j);
-						if (t > j && base + j < rows) v = fma(-static_cast<double>(dblk[i][base + j]), xj, v);
+					for (int jj = 0; jj < 32; ++jj) {
+						if (!unit && t == jj && i < rows) v = v / static_cast<double>(dblk[i][i]);
+						const double xj = __shfl_sync(0xffffffffu, v, jj);
+						if (t > jj && base + jj < rows) v = fma(-static_cast<double>(dblk[i][base + jj]), xj, v);
 					}
 				} else {
-					for (int j = 31; j >= 0; --j) {
-						if (!unit && t == j && i < rows) v = v / static_cast<double>(dblk[i][i]);
-						const double xj = __shfl_sync(0xffffffffu, v, j);
-						if (t < j && base + j < rows) v = fma(-static_cast<double>(dblk[i][base + j]), xj, v);
+					for (int jj = 31; jj >= 0; --jj) {
+						if (!unit && t == jj && i < rows) v = v / static_cast<double>(dblk[i][i]);
+						const double xj = __shfl_sync(0xffffffffu, v, jj);
+						if (t < jj && base + jj < rows) v = fma(-static_cast<double>(dblk[i][base + jj]), xj, v);
 					}
 				}
 				if (i < rows) rhs[i] = v;
@@ -333,7 +379,7 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 			const int hi = lower ? rows : base;
 			for (int i = lo + t; i < hi; i += TRSV_THREADS) {
 				double v = rhs[i];
-				for (int j = 0; j < 32 && base + j < rows; ++j) v = fma(-static_cast<double>(dblk[i][base + j]), rhs[base + j], v);
+				for (int jj = 0; jj < 32 && base + jj < rows; ++jj) v = fma(-static_cast<double>(dblk[i][base + jj]), rhs[base + jj], v);
 				rhs[i] = v;
 			}
 			__syncthreads();
@@ -343,6 +389,8 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 		__syncthreads();
 		if (t == 0) st_release_u32(&flags[r], epoch);
 	}
+	// copies still in flight after a timeout land before the CTA exits
+	asm volatile("cp.async.wait_all;" ::: "memory");
 	if (t == 0 && abort_flag) atomicOr(&w->status, 1u);
 }
 
@@ -411,7 +459,7 @@ int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void 
 {
 	if (n <= 0) return HPLAI_OK;
 	if (!work || work_bytes < trsv_workspace(n)) return HPLAI_EINVAL;
-	constexpr size_t dsmem = sizeof(float) * TB * (TB + 1);
+	constexpr size_t dsmem = sizeof(float) * (TB * (TB + 1) + 3 + 4 + 2 * TB * TB);
 	static int max_blocks = 0;
 	if (!max_blocks) {
 		int per_sm = 0, per_sm_t = 0, dev = 0, sms = 0;
