@@ -71,6 +71,7 @@ struct hplai_ctx {
 	void *trsv_work = nullptr;
 	size_t trsv_bytes = 0;
 	void *getrf_work = nullptr;   // tile flags of the diagonal block LU
+	double *dinv = nullptr;       // FP64 inverses of the factors' 128 x 128 diagonal blocks
 	unsigned *kstatus = nullptr;  // timeout words of this context's Schur [0] and panel [1] kernels
 	uint32_t getrf_epoch = 0;
 	cudaStream_t st = nullptr;    // main stream: Schur updates, refinement, everything else
@@ -118,6 +119,7 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->gemv_work);
 	cudaFree(c->trsv_work);
 	cudaFree(c->getrf_work);
+	cudaFree(c->dinv);
 	cudaFree(c->kstatus);
 	cudaFree(c->gm_v);
 	cudaFree(c->gm_w);
@@ -276,6 +278,7 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	c->trsv_bytes = trsv_workspace(n);
 	CTX_ALLOC(c->trsv_work, c->trsv_bytes);
 	CTX_ALLOC(c->getrf_work, getrf_workspace());
+	CTX_ALLOC(c->dinv, sizeof(double) * trsv_dinv_doubles(n));
 	CTX_ALLOC(c->kstatus, 2 * sizeof(unsigned));
 	if (cudaMemset(c->trsv_work, 0, c->trsv_bytes) != cudaSuccess ||
 		cudaMemset(c->getrf_work, 0, getrf_workspace()) != cudaSuccess ||
@@ -453,6 +456,10 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	}
 	HPLAI_CUDA_TRY(cudaEventRecord(c->ev_panel, sd));
 	HPLAI_CUDA_TRY(cudaStreamWaitEvent(st, c->ev_panel, 0));
+	// inverses of the factors' 128 x 128 diagonal blocks for the refinement's solves
+	HPLAI_TRY(pe.record(st, HPLAI_PH_IR_TRSV));
+	HPLAI_TRY(launch_trsv_dinv(n, c->A, c->lda, c->dinv, st));
+	HPLAI_TRY(pe.end(st));
 	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
 	pe.collect(c->phase_ms);
 	{
@@ -496,8 +503,8 @@ int apply_lu_inverse(hplai_ctx *c, double *v, PhaseEvents &pe, bool trans)
 {
 	cudaStream_t st = c->st;
 	HPLAI_TRY(pe.record(st, HPLAI_PH_IR_TRSV));
-	HPLAI_TRY(launch_trsv(true, c->n, c->A, c->lda, v, c->trsv_work, c->trsv_bytes, st, trans));
-	HPLAI_TRY(launch_trsv(false, c->n, c->A, c->lda, v, c->trsv_work, c->trsv_bytes, st, trans));
+	HPLAI_TRY(launch_trsv(true, c->n, c->A, c->lda, v, c->trsv_work, c->trsv_bytes, st, trans, c->dinv));
+	HPLAI_TRY(launch_trsv(false, c->n, c->A, c->lda, v, c->trsv_work, c->trsv_bytes, st, trans, c->dinv));
 	HPLAI_TRY(pe.end(st));
 	return HPLAI_OK;
 }

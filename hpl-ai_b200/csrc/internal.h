@@ -127,8 +127,12 @@ int launch_otf_gemv_block(int64_t n, int mb, int nb, double alpha, const double 
 size_t trsv_workspace(int n);
 // trans: solve with the transpose of the stored triangle (lower = U^T non-unit,
 // upper = L^T unit); otherwise lower = L (unit), upper = U (non-unit).
+// dinv (optional): FP64 inverses of the 128 x 128 diagonal blocks of both
+// factors (launch_trsv_dinv), applied as products instead of substitution.
 int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes,
-	cudaStream_t st, bool trans = false);
+	cudaStream_t st, bool trans = false, const double *dinv = nullptr);
+size_t trsv_dinv_doubles(int n);
+int launch_trsv_dinv(int n, const float *a, int64_t lda, double *dinv, cudaStream_t st);
 int trsv_status(void *work, cudaStream_t st, int *status);
 int launch_infnorm(int n, const double *x, double *out, cudaStream_t st);
 int launch_div(int n, const double *num, const double *den, double *out, cudaStream_t st);

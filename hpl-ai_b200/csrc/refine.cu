@@ -172,6 +172,46 @@ __global__ void trsv_epoch_kernel(TrsvWork *w)
 	w->status = 0;
 }
 
+// FP64 inverses of the TB x TB diagonal blocks of the stored factors:
+// dinv[(2*r + 0) * TB*TB + c*TB + i] = (L_rr^{-1})[i][c] (unit lower) and
+// dinv[(2*r + 1) * TB*TB + c*TB + i] = (U_rr^{-1})[i][c], rows/columns past
+// n padded with the identity.  Thread c solves T x = e_c by substitution in
+// FP64 (the FP32 factor entries convert exactly).  Computed once per
+// factorisation; the triangular solves then apply a block as one product.
+__global__ void __launch_bounds__(TB) trsv_dinv_kernel(int n, const float *__restrict__ a, int64_t lda,
+	double *__restrict__ dinv)
+{
+	extern __shared__ __align__(16) float dyn_smem[];
+	float (*tb)[TB + 1] = reinterpret_cast<float (*)[TB + 1]>(dyn_smem);                 // tb[i][j] = A[r0+i][r0+j]
+	double *xc = reinterpret_cast<double *>(dyn_smem + TB * (TB + 1) + 1);             // xc[i * TB + c], 8-aligned
+	xc = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(xc) + 7) & ~static_cast<uintptr_t>(7));
+	const int r = blockIdx.x, upper = blockIdx.y;
+	const int r0 = r * TB, rows = min(TB, n - r0);
+	const int c = threadIdx.x;
+	for (int e = c; e < TB * TB; e += TB) {
+		const int i = e % TB, j = e / TB;
+		tb[i][j] = (i < rows && j < rows) ? a[static_cast<int64_t>(r0 + j) * lda + r0 + i] : (i == j ? 1.f : 0.f);
+	}
+	__syncthreads();
+	if (!upper) {
+		for (int i = 0; i < TB; ++i) {
+			double v = (i == c) ? 1.0 : 0.0;
+			if (i > c)
+				for (int j = c; j < i; ++j) v = fma(-static_cast<double>(tb[i][j]), xc[j * TB + c], v);
+			xc[i * TB + c] = v;
+		}
+	} else {
+		for (int i = TB - 1; i >= 0; --i) {
+			double v = (i == c) ? 1.0 : 0.0;
+			if (i < c)
+				for (int j = i + 1; j <= c; ++j) v = fma(-static_cast<double>(tb[i][j]), xc[j * TB + c], v);
+			xc[i * TB + c] = (i <= c) ? v / static_cast<double>(tb[i][i]) : 0.0;
+		}
+	}
+	double *out = dinv + (static_cast<int64_t>(2 * r + upper) * TB) * TB;
+	for (int i = 0; i < TB; ++i) out[static_cast<int64_t>(c) * TB + i] = xc[i * TB + c];
+}
+
 // Copy block (rows r0.., cols c0..) of M into shared memory with cp.async:
 // TRANS (M[i][j] = a[i*lda + j]) as blk[i*TB + j], otherwise
 // (M[i][j] = a[j*lda + i]) as blk[j*TB + i]; rows >= rows / cols >= cols
@@ -213,9 +253,12 @@ __device__ __forceinline__ void stage_block(float *blk, const float *a, int64_t 
 // The off-diagonal blocks of a block row stream through two shared-memory
 // buffers: block q+1 is being copied while block q waits for its x and is
 // applied, so the latency of the factor reads leaves the dependency chain.
+// With dinv (the FP64 inverses of the diagonal blocks, trsv_dinv_kernel) a
+// diagonal block is applied as one product instead of 128 dependent
+// substitution steps.
 template <bool TRANS>
 __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, const float *__restrict__ a,
-	int64_t lda, double *x, TrsvWork *w)
+	int64_t lda, double *x, TrsvWork *w, const double *__restrict__ dinv)
 {
 	extern __shared__ __align__(16) float dyn_smem[];
 	float (*dblk)[TB + 1] = reinterpret_cast<float (*)[TB + 1]>(dyn_smem);   // dblk[i][j] = M[r0+i][r0+j]
@@ -246,8 +289,17 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 			const int cb0 = lower ? 0 : nbt - 1;
 			stage_block<TRANS>(bufs, a, lda, r0, cb0 * TB, rows, min(TB, n - cb0 * TB), vec);
 		}
+		// the diagonal block's inverse (M^{-1} = T^{-1} or its transpose) into L2
+		const double *dblock = nullptr;
+		if (dinv) {
+			const int tri = (lower != 0) == !TRANS ? 0 : 1;   // L for lower / L^T, U for upper / U^T
+			dblock = dinv + (static_cast<int64_t>(2 * r + tri) * TB) * TB;
+			if (t < 8)
+				asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(dblock + t * (TB * TB / 8)),
+					"r"(static_cast<unsigned>(sizeof(double) * TB * TB / 8)) : "memory");
+		}
 		// Stage the diagonal block (independent of other CTAs).
-		for (int e = t; e < TB * TB; e += TRSV_THREADS) {
+		for (int e = t; !dinv && e < TB * TB; e += TRSV_THREADS) {
 			// consecutive threads take the contiguous index of the stored matrix
 			const int i = TRANS ? e / TB : e % TB, jj = TRANS ? e % TB : e / TB;
 			const int64_t off = TRANS ? static_cast<int64_t>(r0 + i) * lda + r0 + jj : static_cast<int64_t>(r0 + jj) * lda + r0 + i;
@@ -349,9 +401,39 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 		__syncthreads();
 		if (t < TB) rhs[t] = (t < rows) ? x[r0 + t] - (part[0][t] + part[1][t]) : 0.0;
 		__syncthreads();
+		if (dinv) {
+			// x_r = M_rr^{-1} rhs: element (i, j) of M^{-1} is dblock[j*TB + i], or
+			// dblock[i*TB + j] for the transpose
+			if (TRANS) {
+				const int wv = t >> 5, ln = t & 31;
+#pragma unroll 4
+				for (int qq = 0; qq < TB / 8; ++qq) {
+					const int i = wv + 8 * qq;
+					const double *row = dblock + static_cast<int64_t>(i) * TB + 4 * ln;
+					double v = row[0] * rhs[4 * ln];
+					v = fma(row[1], rhs[4 * ln + 1], v);
+					v = fma(row[2], rhs[4 * ln + 2], v);
+					v = fma(row[3], rhs[4 * ln + 3], v);
+					for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+					if (ln == 0) {
+						part[0][i] = v;
+						part[1][i] = 0.0;
+					}
+				}
+			} else {
+				const int jb = grp * (TB / 2);
+				double v = 0.0;
+#pragma unroll 16
+				for (int jj = jb; jj < jb + TB / 2; ++jj) v = fma(dblock[static_cast<int64_t>(jj) * TB + lr], rhs[jj], v);
+				part[grp][lr] = v;
+			}
+			__syncthreads();
+			if (t < rows) rhs[t] = part[0][t] + part[1][t];
+			__syncthreads();
+		}
 		// Diagonal block: 32-row sub-blocks solved by warp 0 with shuffles,
 		// the remaining rows updated by all threads.
-		const int nsb = (rows + 31) / 32;
+		const int nsb = dinv ? 0 : (rows + 31) / 32;
 		for (int sblk = 0; sblk < nsb; ++sblk) {
 			const int sb = lower ? sblk : nsb - 1 - sblk;
 			const int base = sb * 32;
@@ -455,7 +537,7 @@ size_t trsv_workspace(int n)
 }
 
 int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes,
-	cudaStream_t st, bool trans)
+	cudaStream_t st, bool trans, const double *dinv)
 {
 	if (n <= 0) return HPLAI_OK;
 	if (!work || work_bytes < trsv_workspace(n)) return HPLAI_EINVAL;
@@ -483,10 +565,32 @@ int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void 
 	const int nbt = (n + TB - 1) / TB;
 	const int grid = nbt < max_blocks ? nbt : max_blocks;
 	int lw = lower ? 1 : 0;
-	void *args[] = {(void *)&lw, (void *)&n, (void *)&a, (void *)&lda, (void *)&x, (void *)&w};
+	void *args[] = {(void *)&lw, (void *)&n, (void *)&a, (void *)&lda, (void *)&x, (void *)&w, (void *)&dinv};
 	void *fn = trans ? reinterpret_cast<void *>(trsv_kernel<true>) : reinterpret_cast<void *>(trsv_kernel<false>);
 	HPLAI_CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(TRSV_THREADS), args, dsmem, st));
 	count_launches();
+	return HPLAI_OK;
+}
+
+size_t trsv_dinv_doubles(int n)
+{
+	const size_t nbt = (static_cast<size_t>(n) + TB - 1) / TB;
+	return 2 * nbt * TB * TB;
+}
+
+int launch_trsv_dinv(int n, const float *a, int64_t lda, double *dinv, cudaStream_t st)
+{
+	if (n <= 0) return HPLAI_OK;
+	constexpr size_t smem = sizeof(float) * (TB * (TB + 1) + 3) + sizeof(double) * TB * TB;
+	static bool attr = false;
+	if (!attr) {
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(trsv_dinv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(smem)));
+		attr = true;
+	}
+	trsv_dinv_kernel<<<dim3((n + TB - 1) / TB, 2), TB, smem, st>>>(n, a, lda, dinv);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
 }
 
