@@ -186,20 +186,21 @@ def run_reference(args):
     return 0
 
 
-def schur_algorithmic(n, b, panel_bytes=2):
+def schur_algorithmic(n, b, panel_bytes=2, c_bytes=8):
     """Flops and bytes of all Schur launches of one factorisation.
     Step k updates C = (n-(k+1)b)^2 FP32 elements (read and written, 8 B
     each), reads the L and U panels (2*rem*b elements of panel_bytes: 2 for
     FP16, 1 for e4m3) and does 2*rem^2*b flops, in three launches (the next
     panel's block column and block row, then the rest of the trailing
-    matrix; the last step has no rest)."""
+    matrix; the last step has no rest).  c_bytes: 8 for the FP32 trailing
+    matrix read + write, 4 for the FP16 deck."""
     flops = byts = 0.0
     launches = 0
     nb = n // b
     for k in range(nb - 1):
         rem = n - (k + 1) * b
         flops += 2.0 * rem * rem * b
-        byts += 8.0 * rem * rem + 2.0 * panel_bytes * rem * b
+        byts += float(c_bytes) * rem * rem + 2.0 * panel_bytes * rem * b
         launches += 3 if k < nb - 2 else 2   # next block column, next block row, rest
     return flops, byts, launches
 
@@ -246,6 +247,9 @@ def run_ours(args):
             torch.distributed.barrier()
 
     flags = hplai.FLAG_LOOKAHEAD if args.lookahead else 0
+    deck = args.deck == "on"
+    if deck:
+        flags |= hplai.FLAG_FP16_DECK
     s = hplai.Solver(n, b, precision=prec, flags=flags)
     ext = torch.cuda.ExternalStream(s.stream())
     results = []
@@ -286,7 +290,7 @@ def run_ours(args):
         # no measured e4m3 peak: the dense e4m3 rate is twice the FP16/BF16 rate
         tc_sus *= 2.0
         peak_note += " x 2 for e4m3 (nominal e4m3:bf16 ratio; no measured e4m3 peak)"
-    sflops, sbytes, slaunch = schur_algorithmic(n, b, 1 if prec == hplai.F32_F8 else 2)
+    sflops, sbytes, slaunch = schur_algorithmic(n, b, 1 if prec == hplai.F32_F8 else 2, 4 if deck else 8)
     gemm_ms = statistics.mean(r[2]["GEMM_UPDATE"] for r in results)
     avg_launch_s = gemm_ms * 1e-3 / slaunch
     ach_gbs = sbytes / slaunch / avg_launch_s / 1e9
@@ -301,7 +305,7 @@ def run_ours(args):
         roof = {"bound": "tensor", "achieved": ach_tf, "peak": tc_sus, "unit": "TFLOP/s", "frac": ach_tf / tc_sus}
     kname = "schur_kernel (tcgen05 e4m3 x e4m3 -> FP32, C -= sl*L*U*su)" if prec == hplai.F32_F8 else \
         "schur_kernel (tcgen05 FP16 x FP16 -> FP32, C -= L*U)"
-    roof.update({"traffic": traffic if prec == hplai.F32_F16 else None, "kernel": kname,
+    roof.update({"traffic": traffic if (prec == hplai.F32_F16 and not deck) else None, "kernel": kname,
                  "launches_per_step": slaunch, "avg_launch_ms": avg_launch_s * 1e3,
                  "algorithmic_bytes_per_launch": sbytes / slaunch, "algorithmic_flops_per_launch": sflops / slaunch,
                  "intensity_flop_per_byte": intensity, "ridge_flop_per_byte": ridge,
@@ -371,6 +375,7 @@ def run_ours(args):
                                    f"{'e4m3' if prec == hplai.F32_F8 else 'FP16'} tcgen05 Schur update, "
                                    f"FP64 {'GMRES-IR' if mode == hplai.GMRES else 'iterative refinement'}",
                        "n": n, "b": b, "form": form, "lookahead": bool(args.lookahead),
+                       "trailing_matrix": "FP16 deck (updates in FP16, applied per panel)" if deck else "FP32",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": f"inputs {n * n * 4 / 1e9:.1f} GB FP32 > 126 MB L2, rewritten between steps"},
             "hpl_harness": last.hpl_harness, "resid": last.residual, "ir_steps": last.iters,
@@ -557,6 +562,8 @@ def main():
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-seed", type=int, default=20240611)
     ap.add_argument("--batch-workers", type=int, default=8)
+    ap.add_argument("--deck", choices=("on", "off"), default="off",
+                    help="FP16 trailing-update deck (HPLAI_FLAG_FP16_DECK)")
     ap.add_argument("--lookahead", action="store_true",
                     help="form the next step's diagonal block and panels on a side stream (HPLAI_FLAG_LOOKAHEAD)")
     ap.add_argument("--refine", choices=("ir", "gmres"), default=None,

@@ -62,6 +62,10 @@ struct hplai_ctx {
 	float *sl[2] = {nullptr, nullptr}, *su[2] = {nullptr, nullptr};
 	unsigned *qbits = nullptr;
 	int64_t ld8 = 0;
+	// HPLAI_FLAG_FP16_DECK: FP16 trailing-update deck (n x lda halves), holding
+	// dscale x (accumulated update)
+	uint16_t *deck = nullptr;
+	float dscale = 1.f;
 	SchurMaps maps8[2];
 	TcPanels tc;
 	float *tcbuf = nullptr;   // phi, plo (n x ldp), the four b x ldp inverse buffers, the inversion work
@@ -110,6 +114,7 @@ int ctx_free(hplai_ctx *c)
 		cudaFree(c->su[i]);
 	}
 	cudaFree(c->qbits);
+	cudaFree(c->deck);
 	cudaFree(c->tcbuf);
 	cudaFree(c->rhs);
 	cudaFree(c->d);
@@ -223,6 +228,7 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	*out = nullptr;
 	if (n <= 0 || b < 16 || b > 1024 || n % b) return HPLAI_EINVAL;
 	if (precision != HPLAI_F32_F16 && precision != HPLAI_F32_F8) return HPLAI_EUNSUPPORTED;
+	if ((flags & HPLAI_FLAG_FP16_DECK) && (b % 8)) return HPLAI_EINVAL;
 	hplai_ctx *c = new hplai_ctx;
 	c->n = n;
 	c->b = b;
@@ -264,6 +270,11 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		}
 		CTX_ALLOC(c->qbits, sizeof(unsigned) * nblk128);
 	}
+	if (flags & HPLAI_FLAG_FP16_DECK) {
+		CTX_ALLOC(c->deck, sizeof(uint16_t) * static_cast<size_t>(c->lda) * n);
+		// a power of two near n^0.75, the reference's scalea (hpl_rand.hpp:154)
+		c->dscale = std::ldexp(1.0f, static_cast<int>(std::lround(0.75 * std::log2(static_cast<double>(n)))));
+	}
 	const int64_t ldp = round_up(b, 32);
 	const size_t tc_elems = static_cast<size_t>(ldp) * (2 * static_cast<size_t>(n) + 4 * static_cast<size_t>(b)) +
 		tc_inverse_work_elems(ldp);
@@ -292,10 +303,14 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		s = schur_make_maps(&c->maps[i], c->Lh[i], n, c->ldh, c->Uh[i], n, c->ldh, b);
 		if (s == HPLAI_OK) s = schur_set_cmap(&c->maps[i], c->A, n, n, c->lda);
 		c->maps[i].status = c->kstatus;
+		c->maps[i].deck_base = c->deck;
+		c->maps[i].deck_ld = c->lda;
 		if (s == HPLAI_OK && precision == HPLAI_F32_F8) {
 			s = schur_make_maps_fp8(&c->maps8[i], c->L8[i], n, c->ld8, c->U8[i], n, c->ld8, b);
 			if (s == HPLAI_OK) s = schur_set_cmap(&c->maps8[i], c->A, n, n, c->lda);
 			c->maps8[i].status = c->kstatus;
+			c->maps8[i].deck_base = c->deck;
+			c->maps8[i].deck_ld = c->lda;
 		}
 	}
 	if (s == HPLAI_OK) {
@@ -397,7 +412,11 @@ int schur_region(hplai_ctx *c, int buf, int p0, int r0, int r1, int c0, int c1, 
 	if (r1 <= r0 || c1 <= c0) return HPLAI_OK;
 	HPLAI_TRY(pe.record(st, HPLAI_PH_GEMM_UPDATE));
 	float *cp = c->A + r0 + static_cast<int64_t>(c0) * c->lda;
-	if (c->precision == HPLAI_F32_F8)
+	if (c->deck)
+		HPLAI_TRY(launch_schur_deck(c->precision == HPLAI_F32_F8 ? c->maps8[buf] : c->maps[buf],
+			c->precision == HPLAI_F32_F8, c->sl[buf], p0, c->su[buf], p0, r0, c0, r1 - r0, c1 - c0, r0, c0, c->dscale,
+			max_ctas, st));
+	else if (c->precision == HPLAI_F32_F8)
 		HPLAI_TRY(launch_schur_fp8(c->maps8[buf], c->sl[buf], p0, c->su[buf], p0, r0, c0, r1 - r0, c1 - c0, cp, c->lda,
 			r0, c0, max_ctas, st));
 	else
@@ -414,6 +433,7 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	if (!c->have_inputs) return HPLAI_ESTATE;
 	const int n = c->n, b = c->b, nb = c->nb;
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->kstatus, 0, 2 * sizeof(unsigned), c->st));
+	if (c->deck) HPLAI_CUDA_TRY(cudaMemsetAsync(c->deck, 0, sizeof(uint16_t) * static_cast<size_t>(c->lda) * n, c->st));
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->getrf_work, 0, sizeof(uint32_t), c->st));   // its status word
 	const bool simt = (c->flags & HPLAI_FLAG_SIMT_PANELS) != 0;
 	const bool serial = (c->flags & HPLAI_FLAG_LOOKAHEAD) == 0;
@@ -448,6 +468,13 @@ extern "C" int hplai_factor(hplai_ctx *c)
 		// the next panel's block column (rows r1..n) and block row (columns r2..n)
 		HPLAI_TRY(schur_region(c, buf, r1, r1, n, r1, r2, 0, st, pe));
 		HPLAI_TRY(schur_region(c, buf, r1, r1, r2, r2, n, 0, st, pe));
+		if (c->deck) {
+			// the next block column and block row become A + deck / dscale
+			HPLAI_TRY(pe.record(st, HPLAI_PH_GEMM_UPDATE));
+			HPLAI_TRY(launch_deck_apply(r1, n, r1, r2, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
+			HPLAI_TRY(launch_deck_apply(r1, r2, r2, n, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
+			HPLAI_TRY(pe.end(st));
+		}
 		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));
 		HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_next, 0));
 		HPLAI_TRY(panel_step(c, k + 1, buf ^ 1, simt, side_ctas, sd, pe));

@@ -124,6 +124,38 @@ int launch_quantize_upanel(int cols, int b, const float *arow, int64_t lda, unsi
 	return quantize<false>(cols, b, arow, lda, bits, u8, ld8, scale, st);
 }
 
+namespace {
+
+// A[i][j] += deck[i][j] * inv_scale over rows [r0, r1) x cols [c0, c1).
+__global__ void __launch_bounds__(256) deck_apply_kernel(int r0, int r1, int c0, int c1, float *__restrict__ a,
+	int64_t lda, const __half *__restrict__ deck, int64_t ldd, float inv_scale)
+{
+	const int rows = r1 - r0;
+	const int64_t total = static_cast<int64_t>(rows) * (c1 - c0);
+	for (int64_t e = static_cast<int64_t>(blockIdx.x) * 256 + threadIdx.x; e < total;
+		e += static_cast<int64_t>(gridDim.x) * 256) {
+		const int i = r0 + static_cast<int>(e % rows), j = c0 + static_cast<int>(e / rows);
+		const int64_t ia = static_cast<int64_t>(j) * lda + i, id = static_cast<int64_t>(j) * ldd + i;
+		a[ia] = fmaf(__half2float(deck[id]), inv_scale, a[ia]);
+	}
+}
+
+} // namespace
+
+int launch_deck_apply(int r0, int r1, int c0, int c1, float *a, int64_t lda, const void *deck, int64_t ldd,
+	float inv_scale, cudaStream_t st)
+{
+	if (r1 <= r0 || c1 <= c0) return HPLAI_OK;
+	const int64_t total = static_cast<int64_t>(r1 - r0) * (c1 - c0);
+	int64_t blocks = (total + 255) / 256;
+	if (blocks > 148 * 16) blocks = 148 * 16;
+	deck_apply_kernel<<<static_cast<unsigned>(blocks), 256, 0, st>>>(r0, r1, c0, c1, a, lda,
+		static_cast<const __half *>(deck), ldd, inv_scale);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
 } // namespace hplai
 
 extern "C" int hplai_quantize_e4m3(int rows, int k, const float *src, int64_t lds, int col_major, uint8_t *dst,

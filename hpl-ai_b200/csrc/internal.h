@@ -49,6 +49,10 @@ struct SchurMaps {
 	int64_t cld = 0;
 	bool has_cmap = false;
 	unsigned *status = nullptr;   // device word set on a wait timeout (null: the library's own)
+	// FP16 deck (trailing-matrix updates of the lazy form): base and leading
+	// dimension in halves
+	void *deck_base = nullptr;
+	int64_t deck_ld = 0;
 };
 // L: lrows x k FP16, row-major with ldl; U: urows x k FP16 (row j = column j
 // of U), ldu.  Rows beyond lrows/urows read as zero.
@@ -72,6 +76,10 @@ int schur_make_maps_fp8(SchurMaps *m, const uint8_t *l8, int lrows, int64_t ldl,
 // (sl[(row - sl0) / 128]) and per 128 rows of U8 (su[(row - su0) / 128]).
 int launch_schur_fp8(const SchurMaps &maps8, const float *sl, int sl0, const float *su, int su0, int lrow0, int urow0,
 	int m, int n, float *c, int64_t ldc, int crow0, int ccol0, int max_ctas, cudaStream_t st);
+// deck -= dscale * L U on the FP16 deck of `maps` (rows crow0.., cols ccol0..;
+// crow0 a multiple of 8), FP16 (fp8 = false) or e4m3 operands.
+int launch_schur_deck(const SchurMaps &maps, bool fp8, const float *sl, int sl0, const float *su, int su0, int lrow0,
+	int urow0, int m, int n, int crow0, int ccol0, float dscale, int max_ctas, cudaStream_t st);
 int schur_status();          // the library's word: HPLAI_ETIMEOUT if a device wait ran out since the last reset
 void schur_status_reset();
 
@@ -116,6 +124,10 @@ int launch_quantize_lpanel(int rows, int b, const float *acol, int64_t lda, unsi
 	float *scale, cudaStream_t st);
 int launch_quantize_upanel(int cols, int b, const float *arow, int64_t lda, unsigned *bits, uint8_t *u8, int64_t ld8,
 	float *scale, cudaStream_t st);
+
+// A[i][j] += deck[i][j] * inv_scale on rows [r0, r1) x cols [c0, c1) (FP16 deck, ld ldd)
+int launch_deck_apply(int r0, int r1, int c0, int c1, float *a, int64_t lda, const void *deck, int64_t ldd,
+	float inv_scale, cudaStream_t st);
 
 // refine.cu
 size_t otf_gemv_workspace(int n);

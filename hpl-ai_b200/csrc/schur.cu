@@ -71,7 +71,22 @@ constexpr int EPI_BUF_BYTES = 32 * EPI_CHUNK * 4;   // one warp's 32 rows x EPI_
 static_assert(!TALL || EPI_WARPS == 4, "the tall box is staged by the four lane-quarter warps");
 static_assert(TALL || EPI_CHUNK == 32, "per-warp boxes are 32 x 32");
 constexpr size_t RED_BYTES = static_cast<size_t>(EPI_WARPS) * EPI_BUFS * EPI_BUF_BYTES;   // = BM x EPI_CHUNK x EPI_BUFS when tall
-constexpr size_t smem_bytes(bool red) { return static_cast<size_t>(STAGES) * STAGE_BYTES + (red ? RED_BYTES : 0) + 1024 + 256; }
+// DECK epilogue: FP16 trailing matrix, chunks of 128 rows x 32 columns loaded
+// by TMA into a ring of DECK_BUFS buffers, updated and stored back.
+constexpr int DECK_CH = 32;
+constexpr int DECK_BUFS = 10;      // DECK_BUFS - 1 chunk loads in flight per SM
+constexpr int DECK_STAGES = 3;     // operand stages of the deck kernel (its chunk ring takes the rest)
+constexpr uint32_t DECK_CHUNK_BYTES = BM * DECK_CH * 2;
+constexpr size_t DECK_BYTES = static_cast<size_t>(DECK_BUFS) * DECK_CHUNK_BYTES;
+// epilogue kinds: 0 direct (plain loads/stores of FP32 C), 1 TMA reduce-add
+// into FP32 C, 2 FP16 deck (load, update, store)
+__host__ __device__ constexpr size_t epi_bytes(int epi) { return epi == 1 ? RED_BYTES : (epi == 2 ? DECK_BYTES : 0); }
+__host__ __device__ constexpr int stages_for(int epi) { return epi == 2 ? DECK_STAGES : STAGES; }
+constexpr size_t smem_bytes(int epi)
+{
+	return static_cast<size_t>(stages_for(epi)) * STAGE_BYTES + epi_bytes(epi) + 1024 + 256;
+}
+static_assert(smem_bytes(2) <= 232448 && smem_bytes(1) <= 232448, "shared memory per CTA");
 
 static_assert(TMEM_COLS <= 512, "two accumulators must fit in TMEM");
 
@@ -88,6 +103,7 @@ struct Params {
 	const float *sl, *su;
 	int sl0, su0;
 	unsigned *status;   // set to 1 on a wait timeout
+	float dscale;       // DECK: the deck holds dscale x (accumulated update)
 };
 
 __device__ unsigned int g_status;
@@ -110,6 +126,23 @@ __device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, 
 	tn = in / gm;
 }
 
+__device__ __forceinline__ void tma_store_2d(const void *map, const void *smem_src, int x, int y)
+{
+	asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];"
+		::"l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(smem_src)), "r"(x), "r"(y)
+		: "memory");
+}
+
+// AND over the epilogue warps (named barrier 1), so that they take the same branch.
+__device__ __forceinline__ bool epi_all(bool mine)
+{
+	int all_ok;
+	asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\t"
+	             "bar.red.and.pred q, 1, %2, p;\n\tselp.s32 %0, 1, 0, q;\n\t}"
+	             : "=r"(all_ok) : "r"(mine ? 1 : 0), "n"(EPI_WARPS * 32) : "memory");
+	return all_ok != 0;
+}
+
 __device__ __forceinline__ void tma_reduce_add_2d(const void *map, const void *smem_src, int x, int y)
 {
 	asm volatile("cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.bulk_group [%0, {%2, %3}], [%1];"
@@ -123,30 +156,36 @@ __device__ __forceinline__ void tma_reduce_add_2d(const void *map, const void *s
 // FP8: e4m3 operands (kind::f8f6f4, K = 32 per MMA, 128 per 128-byte row)
 // with the accumulator multiplied by the two blocks' power-of-two factors
 // in the epilogue (exact); otherwise FP16 operands (kind::f16).
-template <bool RED, bool FP8>
+// DECK: C is an FP16 deck holding dscale x (the accumulated update); each
+// chunk is loaded by TMA, deck - dscale * acc is rounded to FP16 once and
+// stored back by TMA (the precision form's trailing matrix, half the bytes).
+template <int EPI, bool FP8>
 __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant__ CUtensorMap lmap,
 	const __grid_constant__ CUtensorMap umap, const __grid_constant__ CUtensorMap cmap, const Params p)
 {
+	constexpr bool RED = EPI == 1, DECK = EPI == 2;
+	constexpr int NST = stages_for(EPI);   // operand ring stages
 	extern __shared__ uint8_t smem_raw[];
 	const uint32_t raw_addr = smem_u32(smem_raw);
 	uint8_t *smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
 	uint8_t *sA = smem;
-	uint8_t *sB = smem + STAGES * A_BYTES;
-	float *sEpi = reinterpret_cast<float *>(smem + STAGES * STAGE_BYTES);   // RED staging
-	uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES + (RED ? RED_BYTES : 0));
+	uint8_t *sB = smem + NST * A_BYTES;
+	float *sEpi = reinterpret_cast<float *>(smem + NST * STAGE_BYTES);   // RED staging / DECK chunks
+	uint64_t *bars = reinterpret_cast<uint64_t *>(smem + NST * STAGE_BYTES + epi_bytes(EPI));
 	uint64_t *full = bars;
-	uint64_t *empty = bars + STAGES;
-	uint64_t *accf = bars + 2 * STAGES;
+	uint64_t *empty = bars + NST;
+	uint64_t *accf = bars + 2 * NST;
 	uint64_t *acce = accf + 2;
 	uint64_t *drain = acce + 2;
-	uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(drain + 1);
+	uint64_t *dbar = drain + 1;   // DECK chunk loads
+	uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(dbar + DECK_BUFS);
 	int *consumed = reinterpret_cast<int *>(tmem_holder + 1);   // stages the MMA warp consumed
 
 	const int warp = threadIdx.x >> 5;
 	const int lane = threadIdx.x & 31;
 
 	if (threadIdx.x == 0) {
-		for (int s = 0; s < STAGES; ++s) {
+		for (int s = 0; s < NST; ++s) {
 			mbar_init(&full[s], 1);
 			mbar_init(&empty[s], 1);
 		}
@@ -155,6 +194,7 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 			mbar_init(&acce[a], EPI_WARPS * 32);
 		}
 		mbar_init(drain, 1);
+		for (int b = 0; b < DECK_BUFS; ++b) mbar_init(&dbar[b], 1);
 		*consumed = 0;
 		fence_mbar_init();
 	}
@@ -191,7 +231,7 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 					tma_load_2d(sA + stage * A_BYTES, &lmap, &full[stage], kx, p.lrow0 + tm * BM);
 					tma_load_2d(sB + stage * B_BYTES, &umap, &full[stage], kx, p.urow0 + tn * BN);
 					++issued;
-					if (++stage == STAGES) { stage = 0; phase ^= 1u; }
+					if (++stage == NST) { stage = 0; phase ^= 1u; }
 				}
 			}
 			ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
@@ -227,7 +267,7 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 					}
 					umma_commit(&empty[stage]);
 					++used;
-					if (++stage == STAGES) { stage = 0; phase ^= 1u; }
+					if (++stage == NST) { stage = 0; phase ^= 1u; }
 				}
 				if (!ok) break;
 				umma_commit(&accf[acc]);
@@ -239,6 +279,95 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 			*consumed = used;
 			if (!ok) atomicOr(p.status, 1u);
 		}
+	} else if (DECK) {
+		// ---------------- FP16 deck epilogue ----------------
+		// A rolling pipeline over this CTA's chunk sequence (its tiles in order,
+		// BN / DECK_CH chunks each): warp 2's lane 0 keeps DECK_BUFS loads ahead.
+		constexpr int CPT = BN / DECK_CH;
+		const int q = warp & 3;
+		__half *dbuf = reinterpret_cast<__half *>(sEpi);
+		const bool lead = (warp == 2 && lane == 0);
+		const int my_tiles = (blockIdx.x < total) ? (total - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+		const int nseq = my_tiles * CPT;
+		auto chunk_xy = [&](int sidx, int &x, int &y) {
+			int tm, tn;
+			tile_coords(blockIdx.x + (sidx / CPT) * gridDim.x, p.tiles_m, p.tiles_n, tm, tn);
+			x = p.crow0 + tm * BM;
+			y = p.ccol0 + tn * BN + (sidx % CPT) * DECK_CH;
+		};
+		int issued = 0;
+		if (lead) {
+			for (; issued < DECK_BUFS - 1 && issued < nseq; ++issued) {
+				int x, y;
+				chunk_xy(issued, x, y);
+				mbar_arrive_expect_tx(&dbar[issued % DECK_BUFS], DECK_CHUNK_BYTES);
+				tma_load_2d(dbuf + (issued % DECK_BUFS) * (BM * DECK_CH), &cmap, &dbar[issued % DECK_BUFS], x, y);
+			}
+		}
+		bool ok = true;
+		int acc = 0;
+		uint32_t acc_phase = 0;
+		int sidx = 0;
+		for (int it = 0; it < my_tiles && ok; ++it) {
+			int tm, tn;
+			tile_coords(blockIdx.x + it * gridDim.x, p.tiles_m, p.tiles_n, tm, tn);
+			ok = epi_all(mbar_wait(&accf[acc], acc_phase));
+			if (!ok) break;
+			tc_fence_after();
+			const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * BN);
+			float rs = 1.f;
+			if (FP8) {
+				const int lr = p.lrow0 + tm * BM + q * 32 + lane - p.sl0;
+				rs = (tm * BM + q * 32 + lane < p.m) ? p.sl[lr >> 7] : 0.f;
+			}
+#pragma unroll 1
+			for (int ch = 0; ch < CPT; ++ch, ++sidx) {
+				const int bi = sidx % DECK_BUFS;
+				ok = epi_all(mbar_wait(&dbar[bi], static_cast<uint32_t>((sidx / DECK_BUFS) & 1)));
+				if (!ok) break;
+				uint32_t r[32];
+				tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(ch * DECK_CH), r);
+				tmem_ld_wait();
+				__half *sb = dbuf + bi * (BM * DECK_CH) + q * 32 + lane;   // element (row, j) at j * BM + row
+				const int cb = p.urow0 + tn * BN + ch * DECK_CH - p.su0;
+#pragma unroll
+				for (int j = 0; j < 32; ++j) {
+					float f = p.dscale;
+					if (FP8) f *= rs * ((tn * BN + ch * DECK_CH + j < p.n) ? __ldg(&p.su[(cb + j) >> 7]) : 0.f);
+					const float v = __half2float(sb[j * BM]) - __uint_as_float(r[j]) * f;
+					sb[j * BM] = __float2half_rn(v);
+				}
+				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+				asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+				if (lead) {
+					int x, y;
+					chunk_xy(sidx, x, y);
+					tma_store_2d(&cmap, dbuf + bi * (BM * DECK_CH), x, y);
+					asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+					if (issued < nseq) {
+						// chunk sidx + DECK_BUFS - 1 goes into the buffer of chunk sidx - 1,
+						// whose store (one group back) has read it
+						const int nb2 = issued % DECK_BUFS;
+						asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+						chunk_xy(issued, x, y);
+						mbar_arrive_expect_tx(&dbar[nb2], DECK_CHUNK_BYTES);
+						tma_load_2d(dbuf + nb2 * (BM * DECK_CH), &cmap, &dbar[nb2], x, y);
+						++issued;
+					}
+				}
+			}
+			if (!ok) break;
+			tc_fence_before();
+			mbar_arrive(&acce[acc]);
+			if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+		}
+		if (lead) {
+			asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+			// loads issued but never consumed (only after a timeout) land before exit
+			for (int s2 = sidx; s2 < issued; ++s2)
+				(void)mbar_wait(&dbar[s2 % DECK_BUFS], static_cast<uint32_t>((s2 / DECK_BUFS) & 1));
+		}
+		if (lane == 0 && !ok) atomicOr(p.status, 1u);
 	} else {
 		// ---------------- epilogue ----------------
 		const int q = warp & 3;   // TMEM lane quarter this warp may access
@@ -250,13 +379,8 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 		for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
 			int tm, tn;
 			tile_coords(tile, p.tiles_m, p.tiles_n, tm, tn);
-			const bool mine = mbar_wait(&accf[acc], acc_phase);
 			// the epilogue warps decide together (their named barriers must not split)
-			int all_ok;
-			asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\t"
-			             "bar.red.and.pred q, 1, %2, p;\n\tselp.s32 %0, 1, 0, q;\n\t}"
-			             : "=r"(all_ok) : "r"(mine ? 1 : 0), "n"(EPI_WARPS * 32) : "memory");
-			ok = all_ok != 0;
+			ok = epi_all(mbar_wait(&accf[acc], acc_phase));
 			if (!ok) break;
 			tc_fence_after();
 			const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * BN);
@@ -373,8 +497,8 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 	if (warp == 0 && lane == 0) {
 		// Loads issued but never consumed (only after a timeout) land before exit.
 		int left = issued - *consumed;
-		for (int s = 0; left > 0 && s < STAGES; ++s, --left) {
-			(void)mbar_wait(&full[(*consumed + s) % STAGES], static_cast<uint32_t>(((*consumed + s) / STAGES) & 1));
+		for (int s = 0; left > 0 && s < NST; ++s, --left) {
+			(void)mbar_wait(&full[(*consumed + s) % NST], static_cast<uint32_t>(((*consumed + s) / NST) & 1));
 		}
 	}
 	if (warp == 1) {
@@ -457,12 +581,23 @@ int schur_set_cmap(SchurMaps *m, const float *c, int rows, int cols, int64_t ldc
 	return HPLAI_OK;
 }
 
+template <int EPI, bool FP8>
+int set_smem_attr()
+{
+	HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<EPI, FP8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(smem_bytes(EPI))));
+	return HPLAI_OK;
+}
+
+// deck: C is the FP16 deck (c = its base, ldc its leading dimension in
+// halves) updated as deck - dscale * acc; otherwise FP32 C.
 static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, int sl0, const float *su, int su0,
-	int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0, int ccol0, int max_ctas, cudaStream_t st)
+	int lrow0, int urow0, int m, int n, void *c, int64_t ldc, int crow0, int ccol0, bool deck, float dscale,
+	int max_ctas, cudaStream_t st)
 {
 	if (m <= 0 || n <= 0) return HPLAI_OK;
 	Params p;
-	p.c = c;
+	p.c = static_cast<float *>(c);
 	p.ldc = ldc;
 	p.m = m;
 	p.n = n;
@@ -477,6 +612,7 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 	p.su = su;
 	p.sl0 = sl0;
 	p.su0 = su0;
+	p.dscale = dscale;
 	p.status = maps.status;
 	if (!p.status) {
 		void *g = nullptr;
@@ -490,36 +626,46 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 	// Its map ends at the region's last row and column: a TMA reduce clips
 	// only at the tensor's extent, and a tile reaching past a region that
 	// does not end at the matrix edge must not touch the neighbouring blocks.
-	bool red = maps.has_cmap && (crow0 % 4 == 0);
+	// The deck's loads and stores use a map clipped the same way (FP16: rows
+	// start on multiples of 8).
+	int epi = 0;
 	alignas(64) unsigned char cmap[128];
-	if (red && make_map_2d(cmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, maps.cbase, static_cast<uint64_t>(crow0 + m),
+	if (deck) {
+		if (crow0 % 8 || !maps.deck_base) return HPLAI_EINVAL;
+		HPLAI_TRY(make_map_2d(cmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, maps.deck_base,
+			static_cast<uint64_t>(crow0 + m), static_cast<uint64_t>(ccol0 + n), static_cast<uint64_t>(maps.deck_ld), BM,
+			DECK_CH, CU_TENSOR_MAP_SWIZZLE_NONE));
+		epi = 2;
+	} else if (maps.has_cmap && (crow0 % 4 == 0) &&
+		make_map_2d(cmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, maps.cbase, static_cast<uint64_t>(crow0 + m),
 			static_cast<uint64_t>(ccol0 + n), static_cast<uint64_t>(maps.cld), TALL ? BM : 32, EPI_CHUNK,
-			CU_TENSOR_MAP_SWIZZLE_NONE) != HPLAI_OK)
-		red = false;
+			CU_TENSOR_MAP_SWIZZLE_NONE) == HPLAI_OK) {
+		epi = 1;
+	}
 	static bool attr_set = false;
 	if (!attr_set) {
-		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			static_cast<int>(smem_bytes(false))));
-		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			static_cast<int>(smem_bytes(true))));
-		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			static_cast<int>(smem_bytes(false))));
-		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			static_cast<int>(smem_bytes(true))));
+		HPLAI_TRY((set_smem_attr<0, false>()));
+		HPLAI_TRY((set_smem_attr<1, false>()));
+		HPLAI_TRY((set_smem_attr<2, false>()));
+		HPLAI_TRY((set_smem_attr<0, true>()));
+		HPLAI_TRY((set_smem_attr<1, true>()));
+		HPLAI_TRY((set_smem_attr<2, true>()));
 		attr_set = true;
 	}
 	CUtensorMap lm, um, cm;
 	std::memcpy(&lm, maps.lmap, sizeof(lm));
 	std::memcpy(&um, maps.umap, sizeof(um));
-	std::memcpy(&cm, red ? cmap : maps.lmap, sizeof(cm));
-	if (red && fp8)
-		schur_kernel<true, true><<<grid, THREADS, smem_bytes(true), st>>>(lm, um, cm, p);
-	else if (red)
-		schur_kernel<true, false><<<grid, THREADS, smem_bytes(true), st>>>(lm, um, cm, p);
-	else if (fp8)
-		schur_kernel<false, true><<<grid, THREADS, smem_bytes(false), st>>>(lm, um, cm, p);
-	else
-		schur_kernel<false, false><<<grid, THREADS, smem_bytes(false), st>>>(lm, um, cm, p);
+	std::memcpy(&cm, epi ? cmap : maps.lmap, sizeof(cm));
+	const size_t sm = smem_bytes(epi);
+	if (fp8) {
+		if (epi == 2) schur_kernel<2, true><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
+		else if (epi == 1) schur_kernel<1, true><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
+		else schur_kernel<0, true><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
+	} else {
+		if (epi == 2) schur_kernel<2, false><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
+		else if (epi == 1) schur_kernel<1, false><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
+		else schur_kernel<0, false><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
+	}
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
@@ -528,13 +674,22 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 int launch_schur(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
 	int ccol0, int max_ctas, cudaStream_t st)
 {
-	return launch_schur_any(maps, false, nullptr, 0, nullptr, 0, lrow0, urow0, m, n, c, ldc, crow0, ccol0, max_ctas, st);
+	return launch_schur_any(maps, false, nullptr, 0, nullptr, 0, lrow0, urow0, m, n, c, ldc, crow0, ccol0, false, 0.f,
+		max_ctas, st);
 }
 
 int launch_schur_fp8(const SchurMaps &maps8, const float *sl, int sl0, const float *su, int su0, int lrow0, int urow0,
 	int m, int n, float *c, int64_t ldc, int crow0, int ccol0, int max_ctas, cudaStream_t st)
 {
-	return launch_schur_any(maps8, true, sl, sl0, su, su0, lrow0, urow0, m, n, c, ldc, crow0, ccol0, max_ctas, st);
+	return launch_schur_any(maps8, true, sl, sl0, su, su0, lrow0, urow0, m, n, c, ldc, crow0, ccol0, false, 0.f,
+		max_ctas, st);
+}
+
+int launch_schur_deck(const SchurMaps &maps, bool fp8, const float *sl, int sl0, const float *su, int su0, int lrow0,
+	int urow0, int m, int n, int crow0, int ccol0, float dscale, int max_ctas, cudaStream_t st)
+{
+	return launch_schur_any(maps, fp8, sl, sl0, su, su0, lrow0, urow0, m, n, maps.deck_base, maps.deck_ld, crow0, ccol0,
+		true, dscale, max_ctas, st);
 }
 
 int schur_make_maps_fp8(SchurMaps *m, const uint8_t *l8, int lrows, int64_t ldl, const uint8_t *u8, int urows,

@@ -29,6 +29,7 @@ HPLAI_OK, HPLAI_EINVAL, HPLAI_ENOMEM, HPLAI_ECUDA, HPLAI_ENOTCONV, HPLAI_ETIMEOU
 F32_F16, F32_F8 = 0, 1
 FLAG_SIMT_PANELS = 1
 FLAG_LOOKAHEAD = 2
+FLAG_FP16_DECK = 4
 IR, GMRES = 0, 1
 PHASES = ("DIAG_LU", "TRSM_L", "TRSM_R", "GEMM_UPDATE", "IR_GEMV", "IR_TRSV", "TOTAL")
 

@@ -88,6 +88,14 @@ typedef enum hplai_phase {
  * default: on B200 the diagonal-block kernels slow down more under the
  * concurrent update than the overlap saves.  Results are bit-identical. */
 #define HPLAI_FLAG_LOOKAHEAD 2u
+/* The trailing matrix's updates accumulate in an FP16 "deck" (the
+ * double-decker lazy form, lazy_init.hpp:92-227): each step adds
+ * -s L U (FP32 accumulation, one FP16 rounding per step, s a power of two
+ * near n^0.75 as scalea, lazy_init.hpp / hpl_rand.hpp:154), and a block
+ * column/row becomes A + deck / s just before it is factored.  Halves the
+ * Schur update's memory traffic; the FP32 matrix keeps the original
+ * entries and receives the factors.  Requires b % 8 == 0. */
+#define HPLAI_FLAG_FP16_DECK 4u
 
 typedef struct hplai_ctx hplai_ctx;
 

@@ -156,3 +156,39 @@ def test_gmres_parameters_validated(hplai, torch_cuda):
         s.factor()
         res = s.iterative_refinement(50, mode=hplai.GMRES)
         assert res.status == hplai.HPLAI_OK
+
+
+# ---------------------------------------------------------------------------
+# FP16 deck (HPLAI_FLAG_FP16_DECK): the trailing updates accumulate in FP16
+# and are applied to a block column/row just before it is factored.
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("precision,mode,n,b", [(0, 0, 2048, 256), (0, 0, 1536, 128), (1, 1, 4096, 512),
+                                               (1, 1, 8192, 1024)])
+def test_deck_solves_converge(hplai, oracle, torch_cuda, precision, mode, n, b):
+    with hplai.Solver(n, b, precision=precision, flags=hplai.FLAG_FP16_DECK) as s:
+        s.generate(42)
+        s.factor()
+        res = s.iterative_refinement(50, mode=mode)
+        x = s.x()
+    assert res.status == hplai.HPLAI_OK and res.hpl_harness < 16.0, res
+    if n <= 4096:
+        xs = dense_solution(oracle, n)
+        assert np.max(np.abs(x - xs)) / np.max(np.abs(xs)) < 1e-11
+
+
+def test_deck_factor_close_to_fp32_trailing(hplai, torch_cuda):
+    """FP16 accumulation of the updates moves each factor entry by far less
+    than the FP16 operands already do."""
+    n, b = 2048, 256
+    lus = []
+    for flags in (0, hplai.FLAG_FP16_DECK):
+        with hplai.Solver(n, b, flags=flags) as s:
+            s.generate(42)
+            s.factor()
+            lus.append(s.lu().astype(np.float64))
+    assert np.max(np.abs(lus[0] - lus[1])) < 1e-2
+
+
+def test_deck_needs_block_multiple_of_8(hplai):
+    with pytest.raises(hplai.HplaiError):
+        hplai.Solver(1200, 60, flags=hplai.FLAG_FP16_DECK)
