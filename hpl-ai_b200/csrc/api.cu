@@ -319,6 +319,8 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		s = tc_panels_make(&c->tc, n, b, base, base + pn, ldp, base + 2 * pn, base + 2 * pn + pb,
 			base + 2 * pn + 2 * pb, base + 2 * pn + 3 * pb, base + 2 * pn + 4 * pb);
 		c->tc.status = c->kstatus + 1;
+		// the precision form's panels only need TF32 accuracy: its Schur operands are e4m3
+		if (precision == HPLAI_F32_F8) c->tc.terms = 1;
 	}
 	if (s != HPLAI_OK) {
 		ctx_free(c);
@@ -383,7 +385,9 @@ int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStrea
 		HPLAI_TRY(launch_trsm_right_upper(rem, b, diag, lda, diag + b, lda, c->Lh[buf] + (kb + b) * ldh, ldh, 1.0f, st));
 	} else {
 		HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st));
-		HPLAI_TRY(launch_lpanel_tc(c->tc, rem, diag + b, lda, c->Lh[buf] + (kb + b) * ldh, ldh, 1.0f, side_ctas, st));
+		// the precision form's Schur update reads the e4m3 copies only: no FP16 copy
+		uint16_t *lh = c->precision == HPLAI_F32_F8 ? nullptr : c->Lh[buf] + (kb + b) * ldh;
+		HPLAI_TRY(launch_lpanel_tc(c->tc, rem, diag + b, lda, lh, ldh, 1.0f, side_ctas, st));
 	}
 	HPLAI_TRY(pe.end(st));
 	HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_R));
@@ -391,8 +395,8 @@ int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStrea
 		HPLAI_TRY(launch_trsm_left_lower(b, rem, diag, lda, diag + static_cast<int64_t>(b) * lda, lda,
 			c->Uh[buf] + (kb + b) * ldh, ldh, 1.0f, st));
 	} else {
-		HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, c->Uh[buf] + (kb + b) * ldh,
-			ldh, 1.0f, side_ctas, st));
+		uint16_t *uh = c->precision == HPLAI_F32_F8 ? nullptr : c->Uh[buf] + (kb + b) * ldh;
+		HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, uh, ldh, 1.0f, side_ctas, st));
 	}
 	if (c->precision == HPLAI_F32_F8) {
 		HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, c->qbits, c->L8[buf] + (kb + b) * c->ld8, c->ld8,

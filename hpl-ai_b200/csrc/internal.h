@@ -100,6 +100,7 @@ struct TcPanels {
 	float *uhi, *ulo, *lhi, *llo;    // b x ldp: hi/lo of U11^{-1} and L11^{-1}
 	float *xu, *xl, *wu, *wl;        // ldp x ldp FP32 work of the inversion (zeroed once)
 	unsigned *status = nullptr;      // device word set on a wait timeout (null: the library's own)
+	int terms = 3;                   // 3xTF32 (FP32 accuracy) or 1 (TF32, for the precision form)
 };
 // `work` holds tc_inverse_work_elems(ldp) floats, zeroed before first use.
 inline size_t tc_inverse_work_elems(int64_t ldp) { return 4 * static_cast<size_t>(ldp) * static_cast<size_t>(ldp); }

@@ -36,6 +36,7 @@ __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__flo
 //   TRANS = true : source element (r, k) at src[k*lds + r] (column-major A_col)
 //   TRANS = false: source element (r, k) at src[r*lds + k] (A_row seen by columns)
 // k in [0, kdim), r in [0, rows); columns kdim..ldp-1 are zeroed.
+// plo == nullptr: the hi part only (single-term TF32 products).
 template <bool TRANS>
 __global__ void __launch_bounds__(256) split_kernel(int rows, int kdim, const float *__restrict__ src, int64_t lds,
 	float *__restrict__ phi, float *__restrict__ plo, int64_t ldp)
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(256) split_kernel(int rows, int kdim, const fl
 				const float x = tile[tx][i];
 				const float h = tf32_hi(x);
 				phi[static_cast<int64_t>(r) * ldp + k] = h;
-				plo[static_cast<int64_t>(r) * ldp + k] = x - h;
+				if (plo) plo[static_cast<int64_t>(r) * ldp + k] = x - h;
 			}
 		}
 	} else {
@@ -65,7 +66,7 @@ __global__ void __launch_bounds__(256) split_kernel(int rows, int kdim, const fl
 				const float x = (k < kdim) ? src[static_cast<int64_t>(r) * lds + k] : 0.f;
 				const float h = tf32_hi(x);
 				phi[static_cast<int64_t>(r) * ldp + k] = h;
-				plo[static_cast<int64_t>(r) * ldp + k] = x - h;
+				if (plo) plo[static_cast<int64_t>(r) * ldp + k] = x - h;
 			}
 		}
 	}
@@ -259,6 +260,7 @@ struct TParams {
 	int64_t s16m, s16n;
 	float scale;
 	unsigned *status;   // set to 1 on a wait timeout
+	int terms;          // 3: hi*hi + hi*lo + lo*hi (FP32 accuracy); 1: hi*hi only (TF32)
 };
 
 __device__ unsigned int g_tstatus;
@@ -337,12 +339,12 @@ __global__ void __launch_bounds__(TTHREADS, 1) tf32x3_kernel(const __grid_consta
 				const int tm = tile % p.tiles_m, tn = tile / p.tiles_m;
 				for (int kc = 0; kc < p.num_kc; ++kc) {
 					if (!mbar_wait(&empty[stage], phase ^ 1u)) { ok = false; break; }
-					mbar_arrive_expect_tx(&full[stage], TSTAGE_BYTES);
+					mbar_arrive_expect_tx(&full[stage], p.terms == 1 ? 2 * TILE_BYTES : TSTAGE_BYTES);
 					uint8_t *st = smem + stage * TSTAGE_BYTES;
 					tma_load_2d(st, &ahi, &full[stage], kc * TBK, p.arow0 + tm * TBM);
-					tma_load_2d(st + TILE_BYTES, &alo, &full[stage], kc * TBK, p.arow0 + tm * TBM);
+					if (p.terms != 1) tma_load_2d(st + TILE_BYTES, &alo, &full[stage], kc * TBK, p.arow0 + tm * TBM);
 					tma_load_2d(st + 2 * TILE_BYTES, &bhi, &full[stage], kc * TBK, p.brow0 + tn * TBN);
-					tma_load_2d(st + 3 * TILE_BYTES, &blo, &full[stage], kc * TBK, p.brow0 + tn * TBN);
+					if (p.terms != 1) tma_load_2d(st + 3 * TILE_BYTES, &blo, &full[stage], kc * TBK, p.brow0 + tn * TBN);
 					++issued;
 					if (++stage == TSTAGES) { stage = 0; phase ^= 1u; }
 				}
@@ -370,8 +372,10 @@ __global__ void __launch_bounds__(TTHREADS, 1) tf32x3_kernel(const __grid_consta
 						// 8 FP32 = 32 bytes = 2 units of 16 B along K inside the swizzle row
 						const uint32_t o = 2u * kk;
 						umma_tf32(d, dah + o, dbh + o, idesc, (kc | kk) != 0 ? 1u : 0u);
-						umma_tf32(d, dah + o, dbl + o, idesc, 1u);
-						umma_tf32(d, dal + o, dbh + o, idesc, 1u);
+						if (p.terms != 1) {
+							umma_tf32(d, dah + o, dbl + o, idesc, 1u);
+							umma_tf32(d, dal + o, dbh + o, idesc, 1u);
+						}
 					}
 					umma_commit(&empty[stage]);
 					++used;
@@ -407,16 +411,16 @@ __global__ void __launch_bounds__(TTHREADS, 1) tf32x3_kernel(const __grid_consta
 				tmem_ld_wait();
 				const int col0 = tn * TBN + ch * 32;
 				if (rok) {
-					__half *o16 = p.out16 + row * p.s16m + col0 * p.s16n;
+					__half *o16 = p.out16 ? p.out16 + row * p.s16m + col0 * p.s16n : nullptr;
 					// a row-major FP16 copy gets this thread's 32 columns as four 16-byte stores
-					const bool vec16 = p.s16n == 1 && col0 + 32 <= p.n && (reinterpret_cast<uintptr_t>(o16) & 15u) == 0;
+					const bool vec16 = o16 && p.s16n == 1 && col0 + 32 <= p.n && (reinterpret_cast<uintptr_t>(o16) & 15u) == 0;
 #pragma unroll
 					for (int j = 0; j < 32; ++j) {
 						const int col = col0 + j;
 						if (col < p.n) {
 							const float v = __uint_as_float(r[j]);
 							p.out32[row * p.s32m + col * p.s32n] = v;
-							if (!vec16) p.out16[row * p.s16m + col * p.s16n] = __float2half_rn(p.scale * v);
+							if (o16 && !vec16) p.out16[row * p.s16m + col * p.s16n] = __float2half_rn(p.scale * v);
 						}
 					}
 					if (vec16) {
@@ -496,10 +500,11 @@ int sm_count()
 
 int launch_tf32x3(const unsigned char *m_ahi, const unsigned char *m_alo, const unsigned char *m_bhi,
 	const unsigned char *m_blo, int arow0, int brow0, int M, int N, int K, float *out32, int64_t s32m, int64_t s32n,
-	__half *out16, int64_t s16m, int64_t s16n, float scale, int max_ctas, cudaStream_t st, unsigned *status)
+	__half *out16, int64_t s16m, int64_t s16n, float scale, int max_ctas, cudaStream_t st, unsigned *status, int terms)
 {
 	if (M <= 0 || N <= 0) return HPLAI_OK;
 	TParams p;
+	p.terms = terms;
 	p.status = status;
 	if (!p.status) {
 		void *g = nullptr;
@@ -605,12 +610,12 @@ int launch_lpanel_tc(const TcPanels &t, int rem, float *acol, int64_t lda, uint1
 	if (rem <= 0) return HPLAI_OK;
 	const int b = t.b;
 	dim3 g((rem + 31) / 32, static_cast<unsigned>(t.ldp / 32));
-	split_kernel<true><<<g, 256, 0, st>>>(rem, b, acol, lda, t.phi, t.plo, t.ldp);
+	split_kernel<true><<<g, 256, 0, st>>>(rem, b, acol, lda, t.phi, t.terms == 1 ? nullptr : t.plo, t.ldp);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// X (rem x b) = A_col U^{-1}: out32 column-major in A, out16 row-major (Lh row = panel row)
 	return launch_tf32x3(t.m_phi, t.m_plo, t.m_uhi, t.m_ulo, 0, 0, rem, b, b, acol, 1, lda,
-		reinterpret_cast<__half *>(lh), ldh, 1, scale, max_ctas, st, t.status);
+		reinterpret_cast<__half *>(lh), ldh, 1, scale, max_ctas, st, t.status, t.terms);
 }
 
 int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint16_t *uh, int64_t ldh, float scale,
@@ -620,12 +625,12 @@ int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint1
 	const int b = t.b;
 	dim3 g((rem + 31) / 32, static_cast<unsigned>(t.ldp / 32));
 	// B operand row j = column j of A_row (b contiguous floats, stride lda)
-	split_kernel<false><<<g, 256, 0, st>>>(rem, b, arow, lda, t.phi, t.plo, t.ldp);
+	split_kernel<false><<<g, 256, 0, st>>>(rem, b, arow, lda, t.phi, t.terms == 1 ? nullptr : t.plo, t.ldp);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// Y (b x rem) = L^{-1} A_row: out32 column-major in A, out16 with column j of U as row j of Uh
 	return launch_tf32x3(t.m_lhi, t.m_llo, t.m_phi, t.m_plo, 0, 0, b, rem, b, arow, 1, lda,
-		reinterpret_cast<__half *>(uh), 1, ldh, scale, max_ctas, st, t.status);
+		reinterpret_cast<__half *>(uh), 1, ldh, scale, max_ctas, st, t.status, t.terms);
 }
 
 int tc_status()
