@@ -7,8 +7,11 @@
 // refinement timed as one region, then
 //   "%.9f sec. %.9f GFlop/s resid = %20.15e hpl-harness = %.9f".
 // P (the process-grid rows) is accepted and ignored: the whole matrix lives
-// on one GPU.  The reference's layout/transport flags (-not, -r, -m, --pack,
-// --numa, --nbuf, ...) are accepted and reported as not applicable.
+// on one GPU.  `-d`/`-l` (the double-decker layout with lazy
+// initialisation, main.cpp:52-53) select the FP16 trailing-update deck; `--fp8` the
+// precision form (e4m3 Schur update, GMRES-IR); `--gmres` GMRES-IR.  The
+// reference's layout/transport flags (-not, -r, -m, --pack, --numa, --nbuf,
+// ...) are accepted and reported as not applicable.
 #include "../../include/hplai.h"
 
 #include <chrono>
@@ -36,8 +39,13 @@ static int usage()
 		"   P                       Process-grid rows of the distributed reference; ignored.\n"
 		"   --maxit <k>             Refinement steps before giving up (default 50).\n"
 		"   --seed <s>              LCG seed (default 42, as the reference).\n"
+		"   -d, -l, --delayed, --lazy-init\n"
+		"                           Keep the trailing updates in an FP16 deck (double-decker form).\n"
+		"   --fp8                   e4m3 Schur update with GMRES refinement.\n"
+		"   --gmres                 GMRES refinement instead of the classical correction.\n"
+		"   --lookahead             Factor the next panel while the trailing update runs.\n"
 		"   --help or -h            Print this message.\n"
-		"Layout and transport flags of the distributed reference (-not, -d, -r, -m, -w, --pack,\n"
+		"Layout and transport flags of the distributed reference (-not, -r, -m, -w, --pack,\n"
 		"--numa, --numa-map, --nbuf, --job-id, --checksum, --l1est, --highammat, --pwrtune)\n"
 		"are accepted and ignored.\n");
 	return 0;
@@ -47,12 +55,20 @@ int main(int argc, char **argv)
 {
 	int n = 120, b = 30, maxit = 50;
 	unsigned long long seed = 42;
+	int precision = HPLAI_F32_F16, mode = HPLAI_IR;
+	unsigned flags = 0;
 	if (argc > 1) n = std::atoi(argv[1]);
 	if (argc > 2) b = std::atoi(argv[2]);
 	for (int i = 4; i < argc; ++i) {
 		if (!std::strcmp(argv[i], "--help") || !std::strcmp(argv[i], "-h")) return usage();
 		else if (!std::strcmp(argv[i], "--maxit") && i + 1 < argc) maxit = std::atoi(argv[++i]);
 		else if (!std::strcmp(argv[i], "--seed") && i + 1 < argc) seed = std::strtoull(argv[++i], nullptr, 10);
+		else if (!std::strcmp(argv[i], "-d") || !std::strcmp(argv[i], "--delayed") || !std::strcmp(argv[i], "-l") ||
+			!std::strcmp(argv[i], "--lazy-init"))
+			flags |= HPLAI_FLAG_FP16_DECK;
+		else if (!std::strcmp(argv[i], "--fp8")) { precision = HPLAI_F32_F8; mode = HPLAI_GMRES; }
+		else if (!std::strcmp(argv[i], "--gmres")) mode = HPLAI_GMRES;
+		else if (!std::strcmp(argv[i], "--lookahead")) flags |= HPLAI_FLAG_LOOKAHEAD;
 		else if (!std::strcmp(argv[i], "--numa") || !std::strcmp(argv[i], "--numa-map") ||
 			!std::strcmp(argv[i], "--nbuf") || !std::strcmp(argv[i], "--job-id")) ++i;
 		else if (argv[i][0] == '-') std::printf("Ignoring option not applicable on one GPU: %s\n", argv[i]);
@@ -61,26 +77,27 @@ int main(int argc, char **argv)
 	if (argc > 1 && (!std::strcmp(argv[1], "-h") || !std::strcmp(argv[1], "--help"))) return usage();
 
 	std::printf("n=%d b=%d r=1 c=1\n", n, b);
-	std::printf("1gpu precomp full fp32/fp16 ddmat\n");
+	std::printf("1gpu precomp full fp32/%s%s\n", precision == HPLAI_F32_F8 ? "e4m3" : "fp16",
+		(flags & HPLAI_FLAG_FP16_DECK) ? " fp16-deck" : " ddmat");
 
 	// Warm-up on a small system with the same block size so that every kernel
 	// is loaded before the timed region (the reference warms BLAS up the same
 	// way, getrf_nopiv.hpp:161-167 / main.cpp:281).
 	{
 		hplai_ctx *w = nullptr;
-		int rc = hplai_create(&w, 2 * b, b, HPLAI_F32_F16, 0);
+		int rc = hplai_create(&w, 2 * b, b, precision, flags);
 		if (rc == HPLAI_OK) {
 			hplai_ir_errors e;
 			int it;
 			hplai_generate(w, seed);
 			hplai_factor(w);
-			hplai_refine(w, HPLAI_IR, maxit, &e, &it);
+			hplai_refine(w, mode, maxit, &e, &it);
 			hplai_destroy(w);
 		}
 	}
 
 	hplai_ctx *ctx = nullptr;
-	int rc = hplai_create(&ctx, n, b, HPLAI_F32_F16, 0);
+	int rc = hplai_create(&ctx, n, b, precision, flags);
 	if (rc != HPLAI_OK) {
 		std::fprintf(stderr, "hplai_create(n=%d, b=%d): %s\n", n, b, hplai_status_string(rc));
 		return 1;
@@ -102,7 +119,7 @@ int main(int argc, char **argv)
 	auto t0 = std::chrono::steady_clock::now();
 	rc = hplai_factor(ctx);
 	int rr = HPLAI_OK;
-	if (rc == HPLAI_OK) rr = hplai_refine(ctx, HPLAI_IR, maxit, &er, &iters);
+	if (rc == HPLAI_OK) rr = hplai_refine(ctx, mode, maxit, &er, &iters);
 	auto t1 = std::chrono::steady_clock::now();
 	if (rc != HPLAI_OK) {
 		std::fprintf(stderr, "hplai_factor: %s\n", hplai_status_string(rc));

@@ -71,11 +71,24 @@ constexpr int EPI_BUF_BYTES = 32 * EPI_CHUNK * 4;   // one warp's 32 rows x EPI_
 static_assert(!TALL || EPI_WARPS == 4, "the tall box is staged by the four lane-quarter warps");
 static_assert(TALL || EPI_CHUNK == 32, "per-warp boxes are 32 x 32");
 constexpr size_t RED_BYTES = static_cast<size_t>(EPI_WARPS) * EPI_BUFS * EPI_BUF_BYTES;   // = BM x EPI_CHUNK x EPI_BUFS when tall
-// DECK epilogue: FP16 trailing matrix, chunks of 128 rows x 32 columns loaded
-// by TMA into a ring of DECK_BUFS buffers, updated and stored back.
-constexpr int DECK_CH = 32;
-constexpr int DECK_BUFS = 10;      // DECK_BUFS - 1 chunk loads in flight per SM
-constexpr int DECK_STAGES = 3;     // operand stages of the deck kernel (its chunk ring takes the rest)
+// DECK epilogue: FP16 trailing matrix, chunks of 128 rows x DECK_CH columns
+// loaded by TMA into a ring of DECK_BUFS buffers, updated and stored back.
+// 64-column chunks with five buffers and three operand stages measured
+// fastest at n = 65536, b = 512 (trailing update 220 ms against 280 ms for
+// 32-column chunks with ten buffers).
+#ifndef HPLAI_DECK_CH
+#define HPLAI_DECK_CH 64
+#endif
+#ifndef HPLAI_DECK_BUFS
+#define HPLAI_DECK_BUFS 5
+#endif
+#ifndef HPLAI_DECK_STAGES
+#define HPLAI_DECK_STAGES 3
+#endif
+constexpr int DECK_CH = HPLAI_DECK_CH;
+constexpr int DECK_BUFS = HPLAI_DECK_BUFS;      // DECK_BUFS - 1 chunk loads in flight per SM
+constexpr int DECK_STAGES = HPLAI_DECK_STAGES;  // operand stages of the deck kernel (its chunk ring takes the rest)
+static_assert(DECK_CH % 32 == 0 && BN % DECK_CH == 0, "deck chunks are whole 32-column TMEM loads");
 constexpr uint32_t DECK_CHUNK_BYTES = BM * DECK_CH * 2;
 constexpr size_t DECK_BYTES = static_cast<size_t>(DECK_BUFS) * DECK_CHUNK_BYTES;
 // epilogue kinds: 0 direct (plain loads/stores of FP32 C), 1 TMA reduce-add
@@ -325,17 +338,21 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 				const int bi = sidx % DECK_BUFS;
 				ok = epi_all(mbar_wait(&dbar[bi], static_cast<uint32_t>((sidx / DECK_BUFS) & 1)));
 				if (!ok) break;
-				uint32_t r[32];
-				tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(ch * DECK_CH), r);
-				tmem_ld_wait();
-				__half *sb = dbuf + bi * (BM * DECK_CH) + q * 32 + lane;   // element (row, j) at j * BM + row
-				const int cb = p.urow0 + tn * BN + ch * DECK_CH - p.su0;
 #pragma unroll
-				for (int j = 0; j < 32; ++j) {
-					float f = p.dscale;
-					if (FP8) f *= rs * ((tn * BN + ch * DECK_CH + j < p.n) ? __ldg(&p.su[(cb + j) >> 7]) : 0.f);
-					const float v = __half2float(sb[j * BM]) - __uint_as_float(r[j]) * f;
-					sb[j * BM] = __float2half_rn(v);
+				for (int h = 0; h < DECK_CH / 32; ++h) {
+					uint32_t r[32];
+					tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(ch * DECK_CH + 32 * h), r);
+					tmem_ld_wait();
+					// element (row, j) of the chunk at j * BM + row
+					__half *sb = dbuf + bi * (BM * DECK_CH) + 32 * h * BM + q * 32 + lane;
+					const int cb = p.urow0 + tn * BN + ch * DECK_CH + 32 * h - p.su0;
+#pragma unroll
+					for (int j = 0; j < 32; ++j) {
+						float f = p.dscale;
+						if (FP8) f *= rs * ((tn * BN + ch * DECK_CH + 32 * h + j < p.n) ? __ldg(&p.su[(cb + j) >> 7]) : 0.f);
+						const float v = __half2float(sb[j * BM]) - __uint_as_float(r[j]) * f;
+						sb[j * BM] = __float2half_rn(v);
+					}
 				}
 				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 				asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
