@@ -496,7 +496,8 @@ def run_adjoint(args):
 
 def run_gemm(args):
     """The Schur GEMM alone through its leaf entry point: C (m x n FP32) -= L U
-    with FP16 (or e4m3) panels of width k, C larger than L2."""
+    with FP16 (or e4m3) panels of width k, C larger than L2; with --deck on,
+    the FP16 deck form deck -= dscale L U."""
     import torch
     torch.cuda.set_device(0)
     import hplai
@@ -504,7 +505,10 @@ def run_gemm(args):
     fp8 = args.precision == "f8"
     torch.manual_seed(0)
     ldc = (m + 63) // 64 * 64 + 64   # the solver's padded leading dimension (no power-of-two stride)
-    c = torch.zeros(n, ldc, dtype=torch.float32, device="cuda")
+    deck = args.deck == "on"
+    # FP32 C, or the FP16 deck of the lazy form (updated as deck - dscale * L U)
+    c = torch.zeros(n, ldc, dtype=torch.float16 if deck else torch.float32, device="cuda")
+    dscale = 2.0 ** -8
     if fp8:
         ld = (k + 127) // 128 * 128
         lp = (torch.rand(m, ld, device="cuda") * 4).to(torch.float8_e4m3fn).view(torch.uint8)
@@ -513,15 +517,24 @@ def run_gemm(args):
         su = torch.ones((n + 127) // 128, device="cuda")
 
         def call():
-            hplai.check(hplai.f8gemm_minus(m, n, k, lp.data_ptr(), ld, sl.data_ptr(), up.data_ptr(), ld, su.data_ptr(),
-                                           c.data_ptr(), ldc, None))
+            if deck:
+                hplai.check(hplai.f8gemm_deck_minus(m, n, k, lp.data_ptr(), ld, sl.data_ptr(), up.data_ptr(), ld,
+                                                    su.data_ptr(), c.data_ptr(), ldc, dscale, None))
+            else:
+                hplai.check(hplai.f8gemm_minus(m, n, k, lp.data_ptr(), ld, sl.data_ptr(), up.data_ptr(), ld,
+                                               su.data_ptr(), c.data_ptr(), ldc, None))
     else:
         ld = (k + 63) // 64 * 64
         lp = torch.rand(m, ld, device="cuda").half()
         up = torch.rand(n, ld, device="cuda").half()
 
         def call():
-            hplai.check(hplai.shgemm_minus(m, n, k, lp.data_ptr(), ld, up.data_ptr(), ld, c.data_ptr(), ldc, None))
+            if deck:
+                hplai.check(hplai.shgemm_deck_minus(m, n, k, lp.data_ptr(), ld, up.data_ptr(), ld, c.data_ptr(), ldc,
+                                                    dscale, None))
+            else:
+                hplai.check(hplai.shgemm_minus(m, n, k, lp.data_ptr(), ld, up.data_ptr(), ld, c.data_ptr(), ldc,
+                                               None))
     for _ in range(args.warmup):
         call()
     torch.cuda.synchronize()
@@ -533,8 +546,9 @@ def run_gemm(args):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     flops = 2.0 * m * n * k
-    byts = 8.0 * m * n + (m + n) * k * (1 if fp8 else 2)
-    print(json.dumps({"workload": f"schur GEMM leaf m={m} n={n} k={k} {'e4m3' if fp8 else 'fp16'}",
+    byts = (4.0 if deck else 8.0) * m * n + (m + n) * k * (1 if fp8 else 2)
+    cform = "FP16 deck" if deck else "FP32 C"
+    print(json.dumps({"workload": f"schur GEMM leaf m={m} n={n} k={k} {'e4m3' if fp8 else 'fp16'} {cform}",
                       "ms_per_launch": ms, "tflops": flops / ms / 1e9, "gbs": byts / ms / 1e6,
                       "algorithmic_bytes": byts, "flops": flops}), flush=True)
     return 0

@@ -62,7 +62,6 @@ constexpr int EPI_WARPS = HPLAI_SCHUR_EPI_WARPS;
 constexpr int EPI_BUFS = HPLAI_SCHUR_EPI_BUFS;
 constexpr int EPI_SPLIT = EPI_WARPS / 4;            // warps per TMEM lane quarter
 constexpr int EPI_COLS = BN / EPI_SPLIT;            // accumulator columns per epilogue warp
-constexpr int THREADS = (2 + EPI_WARPS) * 32;
 static_assert(EPI_WARPS == 4 || EPI_WARPS == 8, "one or two epilogue warps per lane quarter");
 constexpr uint32_t TMEM_COLS = 2 * BN;
 constexpr bool TALL = HPLAI_SCHUR_TALL_BOX != 0;
@@ -85,16 +84,29 @@ constexpr size_t RED_BYTES = static_cast<size_t>(EPI_WARPS) * EPI_BUFS * EPI_BUF
 #ifndef HPLAI_DECK_STAGES
 #define HPLAI_DECK_STAGES 3
 #endif
+// Epilogue warps of the deck kernel: 8 = two per TMEM lane quarter, each
+// taking half of every chunk's columns (the update is a few instructions per
+// element, so one warp per SM sub-partition cannot keep up with the MMAs:
+// 8 warps took the e4m3 trailing update at n = 131072, b = 1024 from 1.39 s
+// to 0.98 s).
+#ifndef HPLAI_DECK_EPI_WARPS
+#define HPLAI_DECK_EPI_WARPS 8
+#endif
 constexpr int DECK_CH = HPLAI_DECK_CH;
 constexpr int DECK_BUFS = HPLAI_DECK_BUFS;      // DECK_BUFS - 1 chunk loads in flight per SM
 constexpr int DECK_STAGES = HPLAI_DECK_STAGES;  // operand stages of the deck kernel (its chunk ring takes the rest)
-static_assert(DECK_CH % 32 == 0 && BN % DECK_CH == 0, "deck chunks are whole 32-column TMEM loads");
+constexpr int DECK_EPI_WARPS = HPLAI_DECK_EPI_WARPS;
+constexpr int DECK_CW = DECK_CH / (DECK_EPI_WARPS / 4);   // chunk columns per deck epilogue warp
+static_assert(DECK_EPI_WARPS == 4 || DECK_EPI_WARPS == 8, "one or two deck epilogue warps per lane quarter");
+static_assert(DECK_CW % 32 == 0 && BN % DECK_CH == 0, "deck chunks are whole 32-column TMEM loads per warp");
 constexpr uint32_t DECK_CHUNK_BYTES = BM * DECK_CH * 2;
 constexpr size_t DECK_BYTES = static_cast<size_t>(DECK_BUFS) * DECK_CHUNK_BYTES;
 // epilogue kinds: 0 direct (plain loads/stores of FP32 C), 1 TMA reduce-add
 // into FP32 C, 2 FP16 deck (load, update, store)
 __host__ __device__ constexpr size_t epi_bytes(int epi) { return epi == 1 ? RED_BYTES : (epi == 2 ? DECK_BYTES : 0); }
 __host__ __device__ constexpr int stages_for(int epi) { return epi == 2 ? DECK_STAGES : STAGES; }
+__host__ __device__ constexpr int epi_warps_for(int epi) { return epi == 2 ? DECK_EPI_WARPS : EPI_WARPS; }
+__host__ __device__ constexpr int threads_for(int epi) { return (2 + epi_warps_for(epi)) * 32; }
 constexpr size_t smem_bytes(int epi)
 {
 	return static_cast<size_t>(stages_for(epi)) * STAGE_BYTES + epi_bytes(epi) + 1024 + 256;
@@ -146,14 +158,33 @@ __device__ __forceinline__ void tma_store_2d(const void *map, const void *smem_s
 		: "memory");
 }
 
-// AND over the epilogue warps (named barrier 1), so that they take the same branch.
+// AND over the NW epilogue warps (named barrier 1), so that they take the same branch.
+template <int NW = EPI_WARPS>
 __device__ __forceinline__ bool epi_all(bool mine)
 {
 	int all_ok;
 	asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\t"
 	             "bar.red.and.pred q, 1, %2, p;\n\tselp.s32 %0, 1, 0, q;\n\t}"
-	             : "=r"(all_ok) : "r"(mine ? 1 : 0), "n"(EPI_WARPS * 32) : "memory");
+	             : "=r"(all_ok) : "r"(mine ? 1 : 0), "n"(NW * 32) : "memory");
 	return all_ok != 0;
+}
+
+// FP8: dequantisation factors of the 32 C columns c0 .. c0 + 31 of this
+// launch (U rows urow0 + c0 ..).  When they share one 128-row block of U
+// (always, for panels whose blocks start on a multiple of 32) the factor is
+// returned in `uni` with true; otherwise lane j's `mine` is column c0 + j's
+// factor.  Columns past n take the last column's block: the clipped C maps
+// never store them.
+__device__ __forceinline__ bool col_factors(const Params &p, int c0, int lane, float &uni, float &mine)
+{
+	const int a = (p.urow0 + min(c0, p.n - 1) - p.su0) >> 7;
+	const int b = (p.urow0 + min(c0 + 31, p.n - 1) - p.su0) >> 7;
+	if (a == b) {
+		uni = __ldg(&p.su[a]);
+		return true;
+	}
+	mine = __ldg(&p.su[(p.urow0 + min(c0 + lane, p.n - 1) - p.su0) >> 7]);
+	return false;
 }
 
 __device__ __forceinline__ void tma_reduce_add_2d(const void *map, const void *smem_src, int x, int y)
@@ -173,11 +204,12 @@ __device__ __forceinline__ void tma_reduce_add_2d(const void *map, const void *s
 // chunk is loaded by TMA, deck - dscale * acc is rounded to FP16 once and
 // stored back by TMA (the precision form's trailing matrix, half the bytes).
 template <int EPI, bool FP8>
-__global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant__ CUtensorMap lmap,
+__global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid_constant__ CUtensorMap lmap,
 	const __grid_constant__ CUtensorMap umap, const __grid_constant__ CUtensorMap cmap, const Params p)
 {
 	constexpr bool RED = EPI == 1, DECK = EPI == 2;
 	constexpr int NST = stages_for(EPI);   // operand ring stages
+	constexpr int NW = epi_warps_for(EPI); // epilogue warps
 	extern __shared__ uint8_t smem_raw[];
 	const uint32_t raw_addr = smem_u32(smem_raw);
 	uint8_t *smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
@@ -204,7 +236,7 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 		}
 		for (int a = 0; a < 2; ++a) {
 			mbar_init(&accf[a], 1);
-			mbar_init(&acce[a], EPI_WARPS * 32);
+			mbar_init(&acce[a], NW * 32);
 		}
 		mbar_init(drain, 1);
 		for (int b = 0; b < DECK_BUFS; ++b) mbar_init(&dbar[b], 1);
@@ -296,8 +328,11 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 		// ---------------- FP16 deck epilogue ----------------
 		// A rolling pipeline over this CTA's chunk sequence (its tiles in order,
 		// BN / DECK_CH chunks each): warp 2's lane 0 keeps DECK_BUFS loads ahead.
+		// Warp w updates TMEM lane quarter w & 3 (rows) and, with 8 warps, one
+		// half of each chunk's columns.
 		constexpr int CPT = BN / DECK_CH;
 		const int q = warp & 3;
+		const int cw0 = ((warp - 2) >> 2) * DECK_CW;   // first chunk column of this warp
 		__half *dbuf = reinterpret_cast<__half *>(sEpi);
 		const bool lead = (warp == 2 && lane == 0);
 		const int my_tiles = (blockIdx.x < total) ? (total - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
@@ -324,38 +359,47 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 		for (int it = 0; it < my_tiles && ok; ++it) {
 			int tm, tn;
 			tile_coords(blockIdx.x + it * gridDim.x, p.tiles_m, p.tiles_n, tm, tn);
-			ok = epi_all(mbar_wait(&accf[acc], acc_phase));
+			ok = epi_all<NW>(mbar_wait(&accf[acc], acc_phase));
 			if (!ok) break;
 			tc_fence_after();
 			const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * BN);
-			float rs = 1.f;
-			if (FP8) {
-				const int lr = p.lrow0 + tm * BM + q * 32 + lane - p.sl0;
-				rs = (tm * BM + q * 32 + lane < p.m) ? p.sl[lr >> 7] : 0.f;
-			}
+			// this lane's row factor: dscale, times the row block's factor for FP8
+			// (rows past m read the last row's block; never stored)
+			float rf = p.dscale;
+			if (FP8) rf *= p.sl[(p.lrow0 + min(tm * BM + q * 32 + lane, p.m - 1) - p.sl0) >> 7];
 #pragma unroll 1
 			for (int ch = 0; ch < CPT; ++ch, ++sidx) {
 				const int bi = sidx % DECK_BUFS;
-				ok = epi_all(mbar_wait(&dbar[bi], static_cast<uint32_t>((sidx / DECK_BUFS) & 1)));
+				ok = epi_all<NW>(mbar_wait(&dbar[bi], static_cast<uint32_t>((sidx / DECK_BUFS) & 1)));
 				if (!ok) break;
 #pragma unroll
-				for (int h = 0; h < DECK_CH / 32; ++h) {
+				for (int g = 0; g < DECK_CW / 32; ++g) {
+					const int cc = ch * DECK_CH + cw0 + 32 * g;   // tile column of this group
 					uint32_t r[32];
-					tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(ch * DECK_CH + 32 * h), r);
-					tmem_ld_wait();
-					// element (row, j) of the chunk at j * BM + row
-					__half *sb = dbuf + bi * (BM * DECK_CH) + 32 * h * BM + q * 32 + lane;
-					const int cb = p.urow0 + tn * BN + ch * DECK_CH + 32 * h - p.su0;
+					tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(cc), r);
+					// element (row, j) of the chunk at j * BM + row; the deck values are
+					// read while the accumulator load is in flight
+					__half *sb = dbuf + bi * (BM * DECK_CH) + (cw0 + 32 * g) * BM + q * 32 + lane;
+					float d[32];
 #pragma unroll
-					for (int j = 0; j < 32; ++j) {
-						float f = p.dscale;
-						if (FP8) f *= rs * ((tn * BN + ch * DECK_CH + 32 * h + j < p.n) ? __ldg(&p.su[(cb + j) >> 7]) : 0.f);
-						const float v = __half2float(sb[j * BM]) - __uint_as_float(r[j]) * f;
-						sb[j * BM] = __float2half_rn(v);
+					for (int j = 0; j < 32; ++j) d[j] = __half2float(sb[j * BM]);
+					float fu = rf, fl = 0.f;
+					const bool uni = FP8 ? col_factors(p, tn * BN + cc, lane, fu, fl) : true;
+					if (FP8 && uni) fu *= rf;
+					tmem_ld_wait();
+					if (uni) {
+#pragma unroll
+						for (int j = 0; j < 32; ++j) sb[j * BM] = __float2half_rn(d[j] - __uint_as_float(r[j]) * fu);
+					} else {
+#pragma unroll
+						for (int j = 0; j < 32; ++j) {
+							const float f = rf * __shfl_sync(0xffffffffu, fl, j);
+							sb[j * BM] = __float2half_rn(d[j] - __uint_as_float(r[j]) * f);
+						}
 					}
 				}
 				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-				asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
+				asm volatile("bar.sync 1, %0;" ::"n"(NW * 32) : "memory");
 				if (lead) {
 					int x, y;
 					chunk_xy(sidx, x, y);
@@ -422,11 +466,16 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 						tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(cc + 32 * half), r);
 						tmem_ld_wait();
 						if (FP8) {
-							const int cb = p.urow0 + tn * BN + cc + 32 * half - p.su0;
+							float fu = 0.f, fl = 0.f;
+							if (col_factors(p, tn * BN + cc + 32 * half, lane, fu, fl)) {
+								fu *= rs;
 #pragma unroll
-							for (int j = 0; j < 32; ++j) {
-								const float cs = (tn * BN + cc + 32 * half + j < p.n) ? __ldg(&p.su[(cb + j) >> 7]) : 0.f;
-								sb[(32 * half + j) * BM + q * 32 + lane] = -(__uint_as_float(r[j]) * (rs * cs));
+								for (int j = 0; j < 32; ++j) sb[(32 * half + j) * BM + q * 32 + lane] = -(__uint_as_float(r[j]) * fu);
+							} else {
+#pragma unroll
+								for (int j = 0; j < 32; ++j)
+									sb[(32 * half + j) * BM + q * 32 + lane] =
+										-(__uint_as_float(r[j]) * (rs * __shfl_sync(0xffffffffu, fl, j)));
 							}
 						} else {
 #pragma unroll
@@ -455,12 +504,15 @@ __global__ void __launch_bounds__(THREADS, 1) schur_kernel(const __grid_constant
 					if (lane == 0) asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(EPI_BUFS - 1) : "memory");
 					__syncwarp();
 					if (FP8) {
-						const int cb = p.urow0 + tn * BN + cc - p.su0;
+						float fu = 0.f, fl = 0.f;
+						if (col_factors(p, tn * BN + cc, lane, fu, fl)) {
+							fu *= rs;
 #pragma unroll
-						for (int j = 0; j < 32; ++j) {
-							const int cj = cb + j;
-							const float cs = (tn * BN + cc + j < p.n) ? __ldg(&p.su[cj >> 7]) : 0.f;
-							sb[j * 32 + lane] = -(__uint_as_float(r[j]) * (rs * cs));
+							for (int j = 0; j < 32; ++j) sb[j * 32 + lane] = -(__uint_as_float(r[j]) * fu);
+						} else {
+#pragma unroll
+							for (int j = 0; j < 32; ++j)
+								sb[j * 32 + lane] = -(__uint_as_float(r[j]) * (rs * __shfl_sync(0xffffffffu, fl, j)));
 						}
 					} else {
 #pragma unroll
@@ -643,12 +695,14 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 	// Its map ends at the region's last row and column: a TMA reduce clips
 	// only at the tensor's extent, and a tile reaching past a region that
 	// does not end at the matrix edge must not touch the neighbouring blocks.
-	// The deck's loads and stores use a map clipped the same way (FP16: rows
-	// start on multiples of 8).
+	// The deck's loads and stores use a map clipped the same way; its rows
+	// start and end on multiples of 8 (a TMA store clips a column in whole
+	// 16-byte units, so a region ending inside one would overwrite the rows
+	// after it with the out-of-range fill).
 	int epi = 0;
 	alignas(64) unsigned char cmap[128];
 	if (deck) {
-		if (crow0 % 8 || !maps.deck_base) return HPLAI_EINVAL;
+		if (crow0 % 8 || m % 8 || !maps.deck_base) return HPLAI_EINVAL;
 		HPLAI_TRY(make_map_2d(cmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, maps.deck_base,
 			static_cast<uint64_t>(crow0 + m), static_cast<uint64_t>(ccol0 + n), static_cast<uint64_t>(maps.deck_ld), BM,
 			DECK_CH, CU_TENSOR_MAP_SWIZZLE_NONE));
@@ -675,13 +729,13 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 	std::memcpy(&cm, epi ? cmap : maps.lmap, sizeof(cm));
 	const size_t sm = smem_bytes(epi);
 	if (fp8) {
-		if (epi == 2) schur_kernel<2, true><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
-		else if (epi == 1) schur_kernel<1, true><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
-		else schur_kernel<0, true><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
+		if (epi == 2) schur_kernel<2, true><<<grid, threads_for(2), sm, st>>>(lm, um, cm, p);
+		else if (epi == 1) schur_kernel<1, true><<<grid, threads_for(1), sm, st>>>(lm, um, cm, p);
+		else schur_kernel<0, true><<<grid, threads_for(0), sm, st>>>(lm, um, cm, p);
 	} else {
-		if (epi == 2) schur_kernel<2, false><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
-		else if (epi == 1) schur_kernel<1, false><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
-		else schur_kernel<0, false><<<grid, THREADS, sm, st>>>(lm, um, cm, p);
+		if (epi == 2) schur_kernel<2, false><<<grid, threads_for(2), sm, st>>>(lm, um, cm, p);
+		else if (epi == 1) schur_kernel<1, false><<<grid, threads_for(1), sm, st>>>(lm, um, cm, p);
+		else schur_kernel<0, false><<<grid, threads_for(0), sm, st>>>(lm, um, cm, p);
 	}
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
@@ -758,4 +812,35 @@ extern "C" int hplai_f8gemm_minus(int m, int n, int k, const uint8_t *l8, int64_
 	HPLAI_TRY(hplai::schur_make_maps_fp8(&maps, l8, m, ldl, u8, n, ldu, k));
 	HPLAI_TRY(hplai::schur_set_cmap(&maps, c, m, n, ldc));
 	return hplai::launch_schur_fp8(maps, sl, 0, su, 0, 0, 0, m, n, c, ldc, 0, 0, 0, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hplai_shgemm_deck_minus(int m, int n, int k, const uint16_t *lh, int64_t ldlh, const uint16_t *uh,
+	int64_t lduh, uint16_t *deck, int64_t ldd, float dscale, void *stream)
+{
+	if (m < 0 || n < 0 || k <= 0 || !lh || !uh || !deck || ldd < m || (ldd % 8) || (m % 8) || ldlh < k || lduh < k ||
+		(reinterpret_cast<uintptr_t>(deck) & 15))
+		return HPLAI_EINVAL;
+	if (m == 0 || n == 0) return HPLAI_OK;
+	hplai::SchurMaps maps;
+	HPLAI_TRY(hplai::schur_make_maps(&maps, lh, m, ldlh, uh, n, lduh, k));
+	maps.deck_base = deck;
+	maps.deck_ld = ldd;
+	return hplai::launch_schur_deck(maps, false, nullptr, 0, nullptr, 0, 0, 0, m, n, 0, 0, dscale, 0,
+		static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hplai_f8gemm_deck_minus(int m, int n, int k, const uint8_t *l8, int64_t ldl, const float *sl,
+	const uint8_t *u8, int64_t ldu, const float *su, uint16_t *deck, int64_t ldd, float dscale, void *stream)
+{
+	if (m < 0 || n < 0 || k <= 0 || !l8 || !u8 || !sl || !su || !deck || ldd < m || (ldd % 8) || (m % 8) || ldl < k ||
+		ldu < k ||
+		(reinterpret_cast<uintptr_t>(deck) & 15))
+		return HPLAI_EINVAL;
+	if (m == 0 || n == 0) return HPLAI_OK;
+	hplai::SchurMaps maps;
+	HPLAI_TRY(hplai::schur_make_maps_fp8(&maps, l8, m, ldl, u8, n, ldu, k));
+	maps.deck_base = deck;
+	maps.deck_ld = ldd;
+	return hplai::launch_schur_deck(maps, true, sl, 0, su, 0, 0, 0, m, n, 0, 0, dscale, 0,
+		static_cast<cudaStream_t>(stream));
 }

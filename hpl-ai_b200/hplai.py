@@ -91,6 +91,10 @@ quantize_e4m3 = _proto("hplai_quantize_e4m3", _c_int, _c_int, _c_int, _vp, _c_i6
                        _vp)
 f8gemm_minus = _proto("hplai_f8gemm_minus", _c_int, _c_int, _c_int, _c_int, _vp, _c_i64, _vp, _vp, _c_i64, _vp, _vp,
                       _c_i64, _vp)
+shgemm_deck_minus = _proto("hplai_shgemm_deck_minus", _c_int, _c_int, _c_int, _c_int, _vp, _c_i64, _vp, _c_i64, _vp,
+                           _c_i64, _c_flt, _vp)
+f8gemm_deck_minus = _proto("hplai_f8gemm_deck_minus", _c_int, _c_int, _c_int, _c_int, _vp, _c_i64, _vp, _vp, _c_i64,
+                           _vp, _vp, _c_i64, _c_flt, _vp)
 otf_gemv_workspace = _proto("hplai_otf_gemv_workspace", _c_sz, _c_int)
 otf_gemv = _proto("hplai_otf_gemv", _c_int, _c_int, _c_dbl, _vp, _c_dbl, _vp, _c_u64, _vp, _vp, _c_sz, _vp)
 otf_gemv_noalloc = _proto("hplai_otf_gemv_noalloc", _c_int, _c_int, _c_dbl, _vp, _c_dbl, _vp, _c_u64, _vp, _vp)

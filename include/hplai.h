@@ -275,6 +275,19 @@ int hplai_quantize_e4m3(int rows, int k, const float *src, int64_t lds, int col_
 int hplai_f8gemm_minus(int m, int n, int k, const uint8_t *l8, int64_t ldl, const float *sl,
 	const uint8_t *u8, int64_t ldu, const float *su, float *c, int64_t ldc, void *stream);
 
+/* The FP16-deck form of the two updates above (the double-decker lower
+ * deck, lazy_init.hpp:92-227): deck (m x n FP16, column-major, ldd) <-
+ * half_rn(deck - dscale * L U) (FP16 operands) or
+ * half_rn(deck - dscale * diag(sl) L8 U8^T diag(su)) (e4m3 operands), the
+ * product accumulated in FP32 and each deck element rounded once.  m and ldd
+ * are multiples of 8 (the deck is stored in 16-byte units) and deck is
+ * 16-byte aligned. */
+int hplai_shgemm_deck_minus(int m, int n, int k, const uint16_t *lh, int64_t ldlh,
+	const uint16_t *uh, int64_t lduh, uint16_t *deck, int64_t ldd, float dscale, void *stream);
+int hplai_f8gemm_deck_minus(int m, int n, int k, const uint8_t *l8, int64_t ldl, const float *sl,
+	const uint8_t *u8, int64_t ldu, const float *su, uint16_t *deck, int64_t ldd, float dscale,
+	void *stream);
+
 /* Workspace bytes for hplai_otf_gemv at order n. */
 size_t hplai_otf_gemv_workspace(int n);
 

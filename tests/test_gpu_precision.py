@@ -192,3 +192,67 @@ def test_deck_factor_close_to_fp32_trailing(hplai, torch_cuda):
 def test_deck_needs_block_multiple_of_8(hplai):
     with pytest.raises(hplai.HplaiError):
         hplai.Solver(1200, 60, flags=hplai.FLAG_FP16_DECK)
+
+
+def _deck_check(got, ref, mag, dscale):
+    """FP32 accumulation of the products (2^-19 of the magnitude sum, as for
+    the FP32 updates), then one FP16 rounding of the deck element."""
+    acc_err = dscale * 2.0 ** -19 * mag
+    tol = acc_err + 2.0 ** -11 * (np.abs(ref) + acc_err) + 2.0 ** -25
+    err = np.abs(got.astype(np.float64) - ref)
+    assert np.all(err <= tol), f"max err/tol {np.max(err / tol):.3g}"
+
+
+@pytest.mark.parametrize("m,n,k", [(704, 500, 256), (136, 131, 512), (1000, 1000, 64), (256, 768, 1024)])
+def test_shgemm_deck_minus_vs_fp64_products(hplai, torch_cuda, m, n, k):
+    """deck <- half(deck - dscale L U) on an FP16 column-major deck (m a
+    multiple of 8, n ragged); the rows between m and ldd and the column
+    after n are not touched."""
+    torch = torch_cuda
+    rng = np.random.default_rng(m * 3 + n + k)
+    ld = (k + 7) // 8 * 8
+    l16 = rng.uniform(-0.5, 0.5, (m, ld)).astype(np.float16)
+    u16 = rng.uniform(-0.5, 0.5, (n, ld)).astype(np.float16)
+    ldd = (m + 7) // 8 * 8 + 8
+    deck0 = rng.uniform(-100, 100, (n + 1, ldd)).astype(np.float16)     # column j at deck0[j]
+    dscale = 64.0
+    dd = torch.from_numpy(deck0.copy()).cuda()
+    ld_, ud = torch.from_numpy(l16).cuda(), torch.from_numpy(u16).cuda()
+    hplai.check(hplai.shgemm_deck_minus(m, n, k, ld_.data_ptr(), ld, ud.data_ptr(), ld, dd.data_ptr(), ldd,
+                                        dscale, None))
+    torch.cuda.synchronize()
+    got = dd.cpu().numpy()
+    lv, uv = l16[:, :k].astype(np.float64), u16[:, :k].astype(np.float64)
+    ref = deck0[:n, :m].astype(np.float64).T - dscale * (lv @ uv.T)
+    _deck_check(got[:n, :m].T, ref, np.abs(lv) @ np.abs(uv).T, dscale)
+    assert np.array_equal(got[:, m:], deck0[:, m:]) and np.array_equal(got[n], deck0[n])
+
+
+@pytest.mark.parametrize("m,n,k", [(704, 500, 256), (136, 131, 512), (256, 384, 1024)])
+def test_f8gemm_deck_minus_vs_fp64_products(hplai, oracle, torch_cuda, m, n, k):
+    torch = torch_cuda
+    rng = np.random.default_rng(m + 5 * n + k)
+    l8, sl = oracle.quantize_e4m3(panel_values(rng, m, k), col_major=True)
+    u8, su = oracle.quantize_e4m3(panel_values(rng, n, k), col_major=False)
+    ldd = (m + 7) // 8 * 8 + 8
+    deck0 = rng.uniform(-100, 100, (n + 1, ldd)).astype(np.float16)
+    dscale = 2.0 ** -8
+    dd = torch.from_numpy(deck0.copy()).cuda()
+    l8d, u8d = torch.from_numpy(l8).cuda(), torch.from_numpy(u8).cuda()
+    sld, sud = torch.from_numpy(sl).cuda(), torch.from_numpy(su).cuda()
+    hplai.check(hplai.f8gemm_deck_minus(m, n, k, l8d.data_ptr(), l8.shape[1], sld.data_ptr(), u8d.data_ptr(),
+                                        u8.shape[1], sud.data_ptr(), dd.data_ptr(), ldd, dscale, None))
+    torch.cuda.synchronize()
+    got = dd.cpu().numpy()
+    lv = np.vectorize(oracle.e4m3_to_f32)(l8[:, :k]).astype(np.float64) * np.repeat(sl, 128)[:m, None]
+    uv = np.vectorize(oracle.e4m3_to_f32)(u8[:, :k]).astype(np.float64) * np.repeat(su, 128)[:n, None]
+    ref = deck0[:n, :m].astype(np.float64).T - dscale * (lv @ uv.T)
+    _deck_check(got[:n, :m].T, ref, np.abs(lv) @ np.abs(uv).T, dscale)
+    assert np.array_equal(got[:, m:], deck0[:, m:]) and np.array_equal(got[n], deck0[n])
+
+
+def test_deck_minus_rejects_bad_layouts(hplai):
+    assert hplai.shgemm_deck_minus(64, 64, 64, 16, 64, 16, 64, 16, 60, 1.0, None) == hplai.HPLAI_EINVAL  # ldd < m
+    assert hplai.shgemm_deck_minus(64, 64, 64, 16, 64, 16, 64, 16, 68, 1.0, None) == hplai.HPLAI_EINVAL  # ldd % 8
+    assert hplai.shgemm_deck_minus(60, 64, 64, 16, 64, 16, 64, 16, 64, 1.0, None) == hplai.HPLAI_EINVAL  # m % 8
+    assert hplai.f8gemm_deck_minus(64, 64, 128, 16, 128, 16, 16, 128, 16, 24, 64, 1.0, None) == hplai.HPLAI_EINVAL
