@@ -3,10 +3,11 @@ system, and the torch.autograd.Function) on the B200.
 
 No reference counterpart: the checks are a dense FP64 solve of the same
 matrix (numpy / torch linalg.solve with autograd), FP64 central differences
-and the hpl-harness of the transposed system.  Tolerances: solutions agree
-with the dense solve to 1e-11 relative (both are converged to a backward
-error near n*eps of a matrix with cond_inf of a few units); gradients to
-1e-9 relative.
+and the hpl-harness of the transposed system.  Tolerances: solutions and
+the adjoint workload's gradients agree with the dense solve to 1e-12
+relative (both are converged to a backward error near n*eps of a matrix
+with cond_inf of a few units); the linear-loss gradients of the small
+system to 1e-9.
 """
 import numpy as np
 import pytest
@@ -36,7 +37,7 @@ def test_solve_rhs_matches_dense(hplai, small):
     b = rng.uniform(-1.0, 1.0, N_SMALL)
     x, res = s.solve_rhs(b)
     assert res.status == hplai.HPLAI_OK and res.hpl_harness < 16.0
-    assert rel(x, np.linalg.solve(a, b)) < 1e-11
+    assert rel(x, np.linalg.solve(a, b)) < 1e-12
 
 
 def test_solve_transpose_matches_dense(hplai, small):
@@ -45,7 +46,7 @@ def test_solve_transpose_matches_dense(hplai, small):
     g = rng.uniform(-1.0, 1.0, N_SMALL)
     lam, res = s.solve_transpose(g)
     assert res.status == hplai.HPLAI_OK and res.hpl_harness < 16.0
-    assert rel(lam, np.linalg.solve(a.T, g)) < 1e-11
+    assert rel(lam, np.linalg.solve(a.T, g)) < 1e-12
 
 
 def test_custom_solves_leave_context_solution(hplai, small):
@@ -73,7 +74,7 @@ def test_autograd_matches_torch_fp64(hplai, small, torch_cuda):
     b2 = torch.tensor(bvec, requires_grad=True)
     x2 = torch.linalg.solve(at, b2)
     (xt * x2).sum().backward()
-    assert rel(x1.detach().numpy(), x2.detach().numpy()) < 1e-11
+    assert rel(x1.detach().numpy(), x2.detach().numpy()) < 1e-12
     assert rel(b1.grad.numpy(), b2.grad.numpy()) < 1e-9
     # sampled matrix gradients dL/dA_ij = -lambda_i x_j
     rows = rng.integers(0, N_SMALL, 256)
@@ -116,3 +117,62 @@ def test_adjoint_workload_n8192(hplai, oracle, torch_cuda):
         norma = np.max(np.sum(np.abs(a), axis=1))
         harness = np.max(np.abs(r)) / (norma * np.max(np.abs(lam)) + np.max(np.abs(g))) / (n * 2.0 ** -53)
         assert harness < 16.0, harness
+
+
+def test_c5_quadratic_loss_gradients(hplai, oracle, torch_cuda):
+    """The adjoint workload: n = 8192, b = 256, L = 0.5 ||x - x_t||^2 with
+    x_t ~ U[-1, 1).  x, grad_b = lambda = A^{-T}(x - x_t) and grad_A = -lambda x^T
+    on 4096 sampled entries agree with torch's FP64 dense solve and its
+    autograd to 1e-12 relative; central differences with step 1e-6 (in b, and
+    in A through the Sherman-Morrison form of the perturbed solve, so that
+    the difference is not lost to cancellation) agree with lambda_k and
+    -lambda_i x_j to 1e-6."""
+    torch = torch_cuda
+    import hplai_torch
+    n, bs = 8192, 256
+    rng = np.random.default_rng(5)
+    xt_np = rng.uniform(-1.0, 1.0, n)
+    with hplai.Solver(n, bs) as s:
+        s.generate(42)
+        s.factor()
+        bvec = s.rhs()
+        b1 = torch.tensor(bvec, requires_grad=True)
+        x1 = hplai_torch.solve(b1, s)
+        xt = torch.from_numpy(xt_np)
+        (0.5 * ((x1 - xt) ** 2).sum()).backward()
+        x, lam = x1.detach().numpy(), b1.grad.numpy()
+        rows = rng.integers(0, n, 4096)
+        cols = rng.integers(0, n, 4096)
+        ga = hplai_torch.matrix_grad_entries(lam, x, rows, cols)
+        # central differences in b: L(b + h e_k) - L(b) = g . dx + 0.5 |dx|^2
+        h = 1e-6
+        g = x - xt_np
+        for k in rng.integers(0, n, 3):
+            def dl(sign):
+                bp = bvec.copy()
+                bp[k] += sign * h
+                dx = s.solve_rhs(bp)[0] - x
+                return g @ dx + 0.5 * dx @ dx
+            fd = (dl(1.0) - dl(-1.0)) / (2 * h)
+            assert abs(fd - lam[k]) <= 1e-6 * np.max(np.abs(lam)), (k, fd, lam[k])
+        # central differences in A_ij: (A + t e_i e_j^T)^{-1} b = x - t x_j u / (1 + t u_j), u = A^{-1} e_i
+        for q in range(3):
+            i, j = int(rows[q]), int(cols[q])
+            e = np.zeros(n)
+            e[i] = 1.0
+            u = s.solve_rhs(e)[0]
+
+            def dla(t):
+                dx = -t * x[j] * u / (1.0 + t * u[j])
+                return g @ dx + 0.5 * dx @ dx
+            fd = (dla(h) - dla(-h)) / (2 * h)
+            assert abs(fd - ga[q]) <= 1e-6 * np.max(np.abs(ga)), (i, j, fd, ga[q])
+    a = oracle.dense_matrix_f64(n, 42)
+    at = torch.tensor(a, device="cuda", requires_grad=True)
+    b2 = torch.tensor(bvec, device="cuda", requires_grad=True)
+    x2 = torch.linalg.solve(at, b2)
+    (0.5 * ((x2 - xt.cuda()) ** 2).sum()).backward()
+    assert rel(x, x2.detach().cpu().numpy()) < 1e-12
+    assert rel(lam, b2.grad.cpu().numpy()) < 1e-12
+    ref = at.grad[torch.from_numpy(rows).cuda(), torch.from_numpy(cols).cuda()].cpu().numpy()
+    assert np.max(np.abs(ga - ref)) / np.max(np.abs(ref)) < 1e-12

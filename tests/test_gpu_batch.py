@@ -4,7 +4,7 @@ System s is the HPL-AI matrix of order n[s] from seed[s], with nrhs[s]
 right-hand sides taken from columns n, n+1, ... of its LCG stream.  The
 extra columns are integer/generator work and must match the oracle bit for
 bit; solutions are compared with a dense FP64 solve of the same system
-(1e-11 relative, converged solutions of a matrix with cond_inf of a few
+(1e-12 relative, converged solutions of a matrix with cond_inf of a few
 units), and every right-hand side must reach hpl-harness < 16.
 """
 import numpy as np
@@ -43,7 +43,7 @@ def test_small_batch_vs_dense(hplai, oracle, torch_cuda):
             rhs = stream_columns(oracle, n[s], seeds[s], 0, nrhs[s])
             ref = np.linalg.solve(a, rhs)
             err = np.max(np.abs(x - ref)) / np.max(np.abs(ref))
-            assert err < 1e-11, (s, err)
+            assert err < 1e-12, (s, err)
 
 
 def test_batch_rejects_bad_sizes(hplai):
