@@ -35,6 +35,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 METRIC = "HPL-AI GFLOP/s to hpl-harness<16: FP8-Schur+GMRES-IR vs plain; % tensor peak"
 UNIT = "GFLOP/s"
 DEFAULT_N, DEFAULT_B = 65536, 512
+ADJOINT_N, ADJOINT_B = 8192, 256
 CPU_SAMPLE = (2400, 120)           # bounded CPU sample of the same workload
 
 
@@ -440,6 +441,7 @@ def run_batch(args):
                                    f"right-hand sides each, plain form + IR", "systems": count,
                        "n_total": int(n.sum()), "rhs_total": int(nrhs.sum()), "workers": args.batch_workers,
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "systems_per_s": world * count * args.steps / (max_ms / 1e3),
             "worst_hpl_harness": worst, "context_create_s": create_s, "gpu_launches": int(launches),
             "clocks": clocks,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(count * 16),
@@ -562,8 +564,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--n", type=int, default=DEFAULT_N)
-    ap.add_argument("--b", type=int, default=DEFAULT_B)
+    ap.add_argument("--n", type=int, default=None, help="order (default 65536; 8192 for the adjoint workload)")
+    ap.add_argument("--b", type=int, default=None, help="block size (default 512; 256 for the adjoint workload)")
     ap.add_argument("--e2e-warmup", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -585,6 +587,10 @@ def main():
     ap.add_argument("--refine", choices=("ir", "gmres"), default=None,
                     help="correction: classical IR or GMRES (default: ir for f16, gmres for f8)")
     args = ap.parse_args()
+    if args.n is None:
+        args.n = ADJOINT_N if args.workload == "adjoint" else DEFAULT_N
+    if args.b is None:
+        args.b = ADJOINT_B if args.workload == "adjoint" else DEFAULT_B
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":
