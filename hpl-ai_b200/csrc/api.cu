@@ -77,6 +77,7 @@ struct hplai_ctx {
 	void *getrf_work = nullptr;   // tile flags of the diagonal block LU
 	double *dinv = nullptr;       // FP64 inverses of the factors' 128 x 128 diagonal blocks
 	unsigned *kstatus = nullptr;  // timeout words of this context's Schur [0] and panel [1] kernels
+	unsigned *f16s = nullptr;     // precision form: triangle maxima [0..1] and inverse scales [2..3]
 	uint32_t getrf_epoch = 0;
 	cudaStream_t st = nullptr;    // main stream: Schur updates, refinement, everything else
 	cudaStream_t st2 = nullptr;   // side stream (high priority): diagonal block + panels
@@ -126,6 +127,7 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->getrf_work);
 	cudaFree(c->dinv);
 	cudaFree(c->kstatus);
+	cudaFree(c->f16s);
 	cudaFree(c->gm_v);
 	cudaFree(c->gm_w);
 	cudaFree(c->gm_small);
@@ -291,6 +293,7 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	CTX_ALLOC(c->getrf_work, getrf_workspace());
 	CTX_ALLOC(c->dinv, sizeof(double) * trsv_dinv_doubles(n));
 	CTX_ALLOC(c->kstatus, 2 * sizeof(unsigned));
+	CTX_ALLOC(c->f16s, 4 * sizeof(unsigned));
 	if (cudaMemset(c->trsv_work, 0, c->trsv_bytes) != cudaSuccess ||
 		cudaMemset(c->getrf_work, 0, getrf_workspace()) != cudaSuccess ||
 		cudaMemset(c->kstatus, 0, 2 * sizeof(unsigned)) != cudaSuccess ||
@@ -319,8 +322,10 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		s = tc_panels_make(&c->tc, n, b, base, base + pn, ldp, base + 2 * pn, base + 2 * pn + pb,
 			base + 2 * pn + 2 * pb, base + 2 * pn + 3 * pb, base + 2 * pn + 4 * pb);
 		c->tc.status = c->kstatus + 1;
-		// the precision form's panels only need TF32 accuracy: its Schur operands are e4m3
+		// the precision form's panels only need FP16 accuracy: its Schur operands are e4m3
 		if (precision == HPLAI_F32_F8) c->tc.terms = 1;
+		c->tc.f16_amax = c->f16s;
+		c->tc.f16_oscale = reinterpret_cast<float *>(c->f16s + 2);
 	}
 	if (s != HPLAI_OK) {
 		ctx_free(c);
@@ -380,9 +385,17 @@ int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStrea
 	HPLAI_TRY(pe.end(st));
 	if (k == c->nb - 1) return HPLAI_OK;
 	const int rem = n - static_cast<int>(kb) - b;
+	// the precision form forms its panels on FP16 tensor cores when the store
+	// epilogue's 16-byte row alignment holds (b a multiple of 4), else in TF32
+	const bool f16_panels = c->precision == HPLAI_F32_F8 && b % 4 == 0;
 	HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_L));
 	if (simt) {
 		HPLAI_TRY(launch_trsm_right_upper(rem, b, diag, lda, diag + b, lda, c->Lh[buf] + (kb + b) * ldh, ldh, 1.0f, st));
+	} else if (f16_panels) {
+		// FP16 panel products (the Schur update reads only the e4m3 copies made below)
+		HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st, false));
+		HPLAI_TRY(launch_lpanel_f16(c->tc, c->maps[buf], static_cast<int>(kb), rem, c->A, lda, c->Lh[buf], c->Uh[buf],
+			ldh, side_ctas, st));
 	} else {
 		HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st));
 		// the precision form's Schur update reads the e4m3 copies only: no FP16 copy
@@ -394,6 +407,9 @@ int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStrea
 	if (simt) {
 		HPLAI_TRY(launch_trsm_left_lower(b, rem, diag, lda, diag + static_cast<int64_t>(b) * lda, lda,
 			c->Uh[buf] + (kb + b) * ldh, ldh, 1.0f, st));
+	} else if (f16_panels) {
+		HPLAI_TRY(launch_upanel_f16(c->tc, c->maps[buf], static_cast<int>(kb), rem, c->A, lda, c->Uh[buf], ldh,
+			side_ctas, st));
 	} else {
 		uint16_t *uh = c->precision == HPLAI_F32_F8 ? nullptr : c->Uh[buf] + (kb + b) * ldh;
 		HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, uh, ldh, 1.0f, side_ctas, st));

@@ -78,6 +78,10 @@ int launch_schur_fp8(const SchurMaps &maps8, const float *sl, int sl0, const flo
 	int m, int n, float *c, int64_t ldc, int crow0, int ccol0, int max_ctas, cudaStream_t st);
 // deck -= dscale * L U on the FP16 deck of `maps` (rows crow0.., cols ccol0..;
 // crow0 a multiple of 8), FP16 (fp8 = false) or e4m3 operands.
+// C (m x n FP32 region of the map's matrix) = (L U) * *oscale, written by TMA
+// store (FP16 operands; crow0 and m multiples of 4).
+int launch_schur_store(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
+	int ccol0, const float *oscale, int max_ctas, cudaStream_t st);
 int launch_schur_deck(const SchurMaps &maps, bool fp8, const float *sl, int sl0, const float *su, int su0, int lrow0,
 	int urow0, int m, int n, int crow0, int ccol0, float dscale, int max_ctas, cudaStream_t st);
 int schur_status();          // the library's word: HPLAI_ETIMEOUT if a device wait ran out since the last reset
@@ -101,12 +105,24 @@ struct TcPanels {
 	float *xu, *xl, *wu, *wl;        // ldp x ldp FP32 work of the inversion (zeroed once)
 	unsigned *status = nullptr;      // device word set on a wait timeout (null: the library's own)
 	int terms = 3;                   // 3xTF32 (FP32 accuracy) or 1 (TF32, for the precision form)
+	unsigned *f16_amax = nullptr;    // FP16 panel products: 2 words of triangle maxima
+	float *f16_oscale = nullptr;     // and the 2 inverse scales of the FP16 triangles
 };
 // `work` holds tc_inverse_work_elems(ldp) floats, zeroed before first use.
 inline size_t tc_inverse_work_elems(int64_t ldp) { return 4 * static_cast<size_t>(ldp) * static_cast<size_t>(ldp); }
 int tc_panels_make(TcPanels *t, int n, int b, float *phi, float *plo, int64_t ldp, float *uhi, float *ulo,
 	float *lhi, float *llo, float *work);
-int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStream_t st);
+int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStream_t st, bool split = true);
+// The precision form's panel products on FP16 tensor cores (after
+// launch_tri_inverses without the split): the triangles are scaled by powers
+// of two into rows kb..kb+b-1 of the FP16 panel buffers lh/uh, the panels are
+// copied to FP16 (rows kb+b..), and A_col <- A_col U11^{-1},
+// A_row <- L11^{-1} A_row are written back into A by the Schur kernel's store
+// form.  `maps` are the FP16 maps over lh/uh with the C map over A.
+int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
+	uint16_t *lh, uint16_t *uh, int64_t ldh, int max_ctas, cudaStream_t st);
+int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
+	uint16_t *uh, int64_t ldh, int max_ctas, cudaStream_t st);
 // A_col (rem x b) <- A_col U11^{-1}; lh row i = half(scale * A_col row i)
 int launch_lpanel_tc(const TcPanels &t, int rem, float *acol, int64_t lda, uint16_t *lh, int64_t ldh, float scale,
 	int max_ctas, cudaStream_t st);

@@ -129,6 +129,9 @@ struct Params {
 	int sl0, su0;
 	unsigned *status;   // set to 1 on a wait timeout
 	float dscale;       // DECK: the deck holds dscale x (accumulated update)
+	// Store form of the reduce epilogue (FP16 operands only): C = acc * *oscale
+	// written by TMA store instead of C -= acc (null: the update)
+	const float *oscale;
 };
 
 __device__ unsigned int g_status;
@@ -477,6 +480,10 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 									sb[(32 * half + j) * BM + q * 32 + lane] =
 										-(__uint_as_float(r[j]) * (rs * __shfl_sync(0xffffffffu, fl, j)));
 							}
+						} else if (p.oscale) {
+							const float os = *p.oscale;
+#pragma unroll
+							for (int j = 0; j < 32; ++j) sb[(32 * half + j) * BM + q * 32 + lane] = __uint_as_float(r[j]) * os;
 						} else {
 #pragma unroll
 							for (int j = 0; j < 32; ++j) sb[(32 * half + j) * BM + q * 32 + lane] = -__uint_as_float(r[j]);
@@ -485,7 +492,10 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 					asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 					asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
 					if (issuer) {
-						tma_reduce_add_2d(&cmap, sb, p.crow0 + tm * BM, p.ccol0 + tn * BN + cc);
+						if (!FP8 && p.oscale)
+							tma_store_2d(&cmap, sb, p.crow0 + tm * BM, p.ccol0 + tn * BN + cc);
+						else
+							tma_reduce_add_2d(&cmap, sb, p.crow0 + tm * BM, p.ccol0 + tn * BN + cc);
 						asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 					}
 					++epi_buf;
@@ -662,7 +672,7 @@ int set_smem_attr()
 // halves) updated as deck - dscale * acc; otherwise FP32 C.
 static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, int sl0, const float *su, int su0,
 	int lrow0, int urow0, int m, int n, void *c, int64_t ldc, int crow0, int ccol0, bool deck, float dscale,
-	int max_ctas, cudaStream_t st)
+	int max_ctas, cudaStream_t st, const float *oscale = nullptr)
 {
 	if (m <= 0 || n <= 0) return HPLAI_OK;
 	Params p;
@@ -682,6 +692,7 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 	p.sl0 = sl0;
 	p.su0 = su0;
 	p.dscale = dscale;
+	p.oscale = oscale;
 	p.status = maps.status;
 	if (!p.status) {
 		void *g = nullptr;
@@ -713,6 +724,9 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 			CU_TENSOR_MAP_SWIZZLE_NONE) == HPLAI_OK) {
 		epi = 1;
 	}
+	// The store form writes whole 16-byte units of a column, so its region
+	// starts and ends on multiples of 4 rows; it needs the tall-box reduce path.
+	if (oscale && (fp8 || deck || epi != 1 || !TALL || (m % 4))) return HPLAI_EINVAL;
 	static bool attr_set = false;
 	if (!attr_set) {
 		HPLAI_TRY((set_smem_attr<0, false>()));
@@ -754,6 +768,14 @@ int launch_schur_fp8(const SchurMaps &maps8, const float *sl, int sl0, const flo
 {
 	return launch_schur_any(maps8, true, sl, sl0, su, su0, lrow0, urow0, m, n, c, ldc, crow0, ccol0, false, 0.f,
 		max_ctas, st);
+}
+
+int launch_schur_store(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
+	int ccol0, const float *oscale, int max_ctas, cudaStream_t st)
+{
+	if (!oscale) return HPLAI_EINVAL;
+	return launch_schur_any(maps, false, nullptr, 0, nullptr, 0, lrow0, urow0, m, n, c, ldc, crow0, ccol0, false, 0.f,
+		max_ctas, st, oscale);
 }
 
 int launch_schur_deck(const SchurMaps &maps, bool fp8, const float *sl, int sl0, const float *su, int su0, int lrow0,

@@ -21,6 +21,7 @@
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <algorithm>
 #include <cstring>
 
 namespace hplai {
@@ -69,6 +70,93 @@ __global__ void __launch_bounds__(256) split_kernel(int rows, int kdim, const fl
 				if (plo) plo[static_cast<int64_t>(r) * ldp + k] = x - h;
 			}
 		}
+	}
+}
+
+// FP16 K-major copy of a panel for the precision form's panel products, with
+// split_kernel's indexing: out[r*ldh + k] = half_rn(x(r, k)), columns
+// kdim..ldh-1 zero.  (The precision form's Schur operands are e4m3, so FP16
+// operands, 11 significant bits, lose nothing that matters and run the panel
+// products at the FP16 tensor rate with half the bytes of TF32.)
+template <bool TRANS>
+__global__ void __launch_bounds__(256) panel_f16_kernel(int rows, int kdim, const float *__restrict__ src,
+	int64_t lds, __half *__restrict__ out, int64_t ldh)
+{
+	__shared__ float tile[32][33];
+	const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+	const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
+	if (TRANS) {
+		for (int i = ty; i < 32; i += 8) {
+			const int k = k0 + i, r = r0 + tx;
+			tile[i][tx] = (k < kdim && r < rows) ? src[static_cast<int64_t>(k) * lds + r] : 0.f;
+		}
+		__syncthreads();
+		for (int i = ty; i < 32; i += 8) {
+			const int r = r0 + i, k = k0 + tx;
+			if (r < rows && k < ldh) out[static_cast<int64_t>(r) * ldh + k] = __float2half_rn(tile[tx][i]);
+		}
+	} else {
+		for (int i = ty; i < 32; i += 8) {
+			const int r = r0 + i, k = k0 + tx;
+			if (r < rows && k < ldh)
+				out[static_cast<int64_t>(r) * ldh + k] =
+					__float2half_rn((k < kdim) ? src[static_cast<int64_t>(r) * lds + k] : 0.f);
+		}
+	}
+}
+
+// Largest |entry| of the two inverted triangles (blockIdx.y: 0 = U11^{-1},
+// 1 = L11^{-1}), as the bits of a non-negative float (ordered like unsigned).
+__global__ void __launch_bounds__(256) tri_amax_kernel(int b, const float *__restrict__ xu,
+	const float *__restrict__ xl, int64_t ldp, unsigned *amax)
+{
+	const float *x = blockIdx.y ? xl : xu;
+	float m = 0.f;
+	const int64_t total = static_cast<int64_t>(b) * ldp;
+	for (int64_t e = blockIdx.x * 256 + threadIdx.x; e < total; e += static_cast<int64_t>(gridDim.x) * 256) {
+		const int pp = static_cast<int>(e % ldp), j = static_cast<int>(e / ldp);
+		if (pp <= j && pp < b) m = fmaxf(m, fabsf(x[e]));
+	}
+	for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+	__shared__ float wm[8];
+	if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		float r = wm[0];
+		for (int w = 1; w < 8; ++w) r = fmaxf(r, wm[w]);
+		atomicMax(&amax[blockIdx.y], __float_as_uint(r));
+	}
+}
+
+// 2^(14 - e) for amax = f 2^e, f in [0.5, 1): the scaled triangle stays below
+// 2^14 (FP16 holds up to 65504) and its small entries stay normal longer.
+__device__ __forceinline__ float f16_tri_scale(unsigned bits)
+{
+	const float a = __uint_as_float(bits);
+	if (!(a > 0.f) || !isfinite(a)) return 1.f;
+	int e = 0;
+	(void)frexpf(a, &e);
+	return ldexpf(1.f, 14 - e);
+}
+
+// The inverted triangles as FP16 Schur operands, scaled by a power of two:
+//   uh[j*ldh + p] = half(s_u U11^{-1}(p, j))   (U operand of A_col U11^{-1})
+//   lh[i*ldh + p] = half(s_l L11^{-1}(i, p))   (L operand of L11^{-1} A_row)
+// and oscale[0..1] = 1/s_u, 1/s_l (exact) for the products' epilogues.
+__global__ void __launch_bounds__(256) tri_f16_kernel(int b, const float *__restrict__ xu,
+	const float *__restrict__ xl, int64_t ldp, const unsigned *__restrict__ amax, __half *__restrict__ uh,
+	__half *__restrict__ lh, int64_t ldh, float *__restrict__ oscale)
+{
+	const bool lower = blockIdx.y != 0;
+	const float *x = lower ? xl : xu;
+	__half *o = lower ? lh : uh;
+	const float sc = f16_tri_scale(amax[blockIdx.y]);
+	if (blockIdx.x == 0 && threadIdx.x == 0) oscale[blockIdx.y] = 1.f / sc;
+	const int64_t total = static_cast<int64_t>(b) * ldh;
+	for (int64_t e = blockIdx.x * 256 + threadIdx.x; e < total; e += static_cast<int64_t>(gridDim.x) * 256) {
+		const int pp = static_cast<int>(e % ldh), j = static_cast<int>(e / ldh);
+		const float v = (pp <= j && pp < b) ? x[static_cast<int64_t>(j) * ldp + pp] * sc : 0.f;
+		o[e] = __float2half_rn(v);
 	}
 }
 
@@ -576,7 +664,7 @@ int tc_panels_make(TcPanels *t, int n, int b, float *phi, float *plo, int64_t ld
 	return HPLAI_OK;
 }
 
-int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStream_t st)
+int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStream_t st, bool split)
 {
 	const int b = t.b;
 	const int bp = static_cast<int>(t.ldp);
@@ -595,6 +683,7 @@ int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStr
 		count_launches();
 		HPLAI_CUDA_TRY(cudaGetLastError());
 	}
+	if (!split) return HPLAI_OK;
 	// U11^{-1} column-major = the B operand of the L-panel product (row n = column n of U^{-1});
 	// (L11^T)^{-1} column-major = L11^{-1} row-major = the A operand of the U-panel product.
 	tri_split_kernel<<<dim3((b * bp + 255) / 256 < 1184 ? (b * bp + 255) / 256 : 1184, 2), 256, 0, st>>>(b, t.xu,
@@ -631,6 +720,52 @@ int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint1
 	// Y (b x rem) = L^{-1} A_row: out32 column-major in A, out16 with column j of U as row j of Uh
 	return launch_tf32x3(t.m_lhi, t.m_llo, t.m_phi, t.m_plo, 0, 0, b, rem, b, arow, 1, lda,
 		reinterpret_cast<__half *>(uh), 1, ldh, scale, max_ctas, st, t.status, t.terms);
+}
+
+int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
+	uint16_t *lh, uint16_t *uh, int64_t ldh, int max_ctas, cudaStream_t st)
+{
+	if (rem <= 0) return HPLAI_OK;
+	if (!t.f16_amax || !t.f16_oscale || ldh % 32) return HPLAI_EINVAL;
+	const int b = t.b;
+	// the inverted triangles into rows kb .. kb+b-1 of the FP16 panel buffers
+	// (rows the step's Schur update never reads)
+	HPLAI_CUDA_TRY(cudaMemsetAsync(t.f16_amax, 0, 2 * sizeof(unsigned), st));
+	const int tb = static_cast<int>(std::min<int64_t>((static_cast<int64_t>(b) * t.ldp + 255) / 256, 592));
+	tri_amax_kernel<<<dim3(tb, 2), 256, 0, st>>>(b, t.xu, t.xl, t.ldp, t.f16_amax);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	tri_f16_kernel<<<dim3(tb, 2), 256, 0, st>>>(b, t.xu, t.xl, t.ldp, t.f16_amax,
+		reinterpret_cast<__half *>(uh) + static_cast<int64_t>(kb) * ldh,
+		reinterpret_cast<__half *>(lh) + static_cast<int64_t>(kb) * ldh, ldh, t.f16_oscale);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	// A_col (rows kb+b.., columns kb..kb+b-1) -> FP16 K-major rows kb+b.. of lh
+	const int64_t kbl = kb;
+	float *acol = a + (kbl + b) + kbl * lda;
+	panel_f16_kernel<true><<<dim3((rem + 31) / 32, static_cast<unsigned>(ldh / 32)), 256, 0, st>>>(rem, b, acol, lda,
+		reinterpret_cast<__half *>(lh) + (kbl + b) * ldh, ldh);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	// A_col = (A_col (s_u U11^{-1})) / s_u
+	return launch_schur_store(maps, kb + b, kb, rem, b, a, lda, kb + b, kb, t.f16_oscale, max_ctas, st);
+}
+
+int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
+	uint16_t *uh, int64_t ldh, int max_ctas, cudaStream_t st)
+{
+	if (rem <= 0) return HPLAI_OK;
+	if (!t.f16_oscale || ldh % 32) return HPLAI_EINVAL;
+	const int b = t.b;
+	const int64_t kbl = kb;
+	// A_row (rows kb..kb+b-1, columns kb+b..): column j -> FP16 row kb+b+j of uh
+	float *arow = a + kbl + (kbl + b) * lda;
+	panel_f16_kernel<false><<<dim3((rem + 31) / 32, static_cast<unsigned>(ldh / 32)), 256, 0, st>>>(rem, b, arow, lda,
+		reinterpret_cast<__half *>(uh) + (kbl + b) * ldh, ldh);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	// A_row = ((s_l L11^{-1}) A_row) / s_l, the triangle in rows kb.. of the L buffer
+	return launch_schur_store(maps, kb, kb + b, b, rem, a, lda, kb, kb + b, t.f16_oscale + 1, max_ctas, st);
 }
 
 int tc_status()
