@@ -371,6 +371,13 @@ extern "C" int hplai_upload(hplai_ctx *c, const float *a, int64_t lda, const dou
 
 namespace {
 
+// The precision form forms its panels on FP16 tensor cores when the store
+// epilogue's 16-byte row alignment holds (b a multiple of 4), else in TF32.
+bool f16_panel_form(const hplai_ctx *c, bool simt)
+{
+	return !simt && c->precision == HPLAI_F32_F8 && c->b % 4 == 0;
+}
+
 // Factor the diagonal block of step k and form its two panels with their
 // FP16 copies in buffer `buf` (getrf_nopiv + update_left/right_panels +
 // convert_left/right_panels, panel_trf.hpp:143-233).
@@ -385,9 +392,9 @@ int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStrea
 	HPLAI_TRY(pe.end(st));
 	if (k == c->nb - 1) return HPLAI_OK;
 	const int rem = n - static_cast<int>(kb) - b;
-	// the precision form forms its panels on FP16 tensor cores when the store
-	// epilogue's 16-byte row alignment holds (b a multiple of 4), else in TF32
-	const bool f16_panels = c->precision == HPLAI_F32_F8 && b % 4 == 0;
+	const bool f16_panels = f16_panel_form(c, simt);
+	const uint16_t *deck = f16_panels ? c->deck : nullptr;   // folded into the FP16 panel copies
+	const float inv_dscale = c->deck ? 1.0f / c->dscale : 0.f;
 	HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_L));
 	if (simt) {
 		HPLAI_TRY(launch_trsm_right_upper(rem, b, diag, lda, diag + b, lda, c->Lh[buf] + (kb + b) * ldh, ldh, 1.0f, st));
@@ -395,7 +402,7 @@ int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStrea
 		// FP16 panel products (the Schur update reads only the e4m3 copies made below)
 		HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st, false));
 		HPLAI_TRY(launch_lpanel_f16(c->tc, c->maps[buf], static_cast<int>(kb), rem, c->A, lda, c->Lh[buf], c->Uh[buf],
-			ldh, side_ctas, st));
+			ldh, deck, inv_dscale, side_ctas, st));
 	} else {
 		HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st));
 		// the precision form's Schur update reads the e4m3 copies only: no FP16 copy
@@ -408,8 +415,8 @@ int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStrea
 		HPLAI_TRY(launch_trsm_left_lower(b, rem, diag, lda, diag + static_cast<int64_t>(b) * lda, lda,
 			c->Uh[buf] + (kb + b) * ldh, ldh, 1.0f, st));
 	} else if (f16_panels) {
-		HPLAI_TRY(launch_upanel_f16(c->tc, c->maps[buf], static_cast<int>(kb), rem, c->A, lda, c->Uh[buf], ldh,
-			side_ctas, st));
+		HPLAI_TRY(launch_upanel_f16(c->tc, c->maps[buf], static_cast<int>(kb), rem, c->A, lda, c->Uh[buf], ldh, deck,
+			inv_dscale, side_ctas, st));
 	} else {
 		uint16_t *uh = c->precision == HPLAI_F32_F8 ? nullptr : c->Uh[buf] + (kb + b) * ldh;
 		HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, uh, ldh, 1.0f, side_ctas, st));
@@ -489,10 +496,15 @@ extern "C" int hplai_factor(hplai_ctx *c)
 		HPLAI_TRY(schur_region(c, buf, r1, r1, n, r1, r2, 0, st, pe));
 		HPLAI_TRY(schur_region(c, buf, r1, r1, r2, r2, n, 0, st, pe));
 		if (c->deck) {
-			// the next block column and block row become A + deck / dscale
+			// the next block column and block row become A + deck / dscale (the
+			// FP16 panel copies fold the deck in themselves: the diagonal block only)
 			HPLAI_TRY(pe.record(st, HPLAI_PH_GEMM_UPDATE));
-			HPLAI_TRY(launch_deck_apply(r1, n, r1, r2, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
-			HPLAI_TRY(launch_deck_apply(r1, r2, r2, n, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
+			if (f16_panel_form(c, simt)) {
+				HPLAI_TRY(launch_deck_apply(r1, r2, r1, r2, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
+			} else {
+				HPLAI_TRY(launch_deck_apply(r1, n, r1, r2, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
+				HPLAI_TRY(launch_deck_apply(r1, r2, r2, n, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
+			}
 			HPLAI_TRY(pe.end(st));
 		}
 		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));

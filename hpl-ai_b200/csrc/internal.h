@@ -118,11 +118,13 @@ int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStr
 // of two into rows kb..kb+b-1 of the FP16 panel buffers lh/uh, the panels are
 // copied to FP16 (rows kb+b..), and A_col <- A_col U11^{-1},
 // A_row <- L11^{-1} A_row are written back into A by the Schur kernel's store
-// form.  `maps` are the FP16 maps over lh/uh with the C map over A.
+// form.  `maps` are the FP16 maps over lh/uh with the C map over A.  With
+// the FP16 deck (same layout as A; null if none) the panels are read as
+// A + deck * inv_dscale, so only the diagonal block needs deck_apply.
 int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
-	uint16_t *lh, uint16_t *uh, int64_t ldh, int max_ctas, cudaStream_t st);
+	uint16_t *lh, uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st);
 int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
-	uint16_t *uh, int64_t ldh, int max_ctas, cudaStream_t st);
+	uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st);
 // A_col (rem x b) <- A_col U11^{-1}; lh row i = half(scale * A_col row i)
 int launch_lpanel_tc(const TcPanels &t, int rem, float *acol, int64_t lda, uint16_t *lh, int64_t ldh, float scale,
 	int max_ctas, cudaStream_t st);

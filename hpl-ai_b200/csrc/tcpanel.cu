@@ -77,10 +77,14 @@ __global__ void __launch_bounds__(256) split_kernel(int rows, int kdim, const fl
 // split_kernel's indexing: out[r*ldh + k] = half_rn(x(r, k)), columns
 // kdim..ldh-1 zero.  (The precision form's Schur operands are e4m3, so FP16
 // operands, 11 significant bits, lose nothing that matters and run the panel
-// products at the FP16 tensor rate with half the bytes of TF32.)
+// products at the FP16 tensor rate with half the bytes of TF32.)  With the
+// FP16 deck, x = fmaf(deck, inv_scale, a) as deck_apply_kernel forms it, the
+// deck element at the same offset from `deck` (leading dimension ldd) as the
+// panel element from `src`.
 template <bool TRANS>
 __global__ void __launch_bounds__(256) panel_f16_kernel(int rows, int kdim, const float *__restrict__ src,
-	int64_t lds, __half *__restrict__ out, int64_t ldh)
+	int64_t lds, const __half *__restrict__ deck, int64_t ldd, float inv_scale, __half *__restrict__ out,
+	int64_t ldh)
 {
 	__shared__ float tile[32][33];
 	const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
@@ -88,7 +92,12 @@ __global__ void __launch_bounds__(256) panel_f16_kernel(int rows, int kdim, cons
 	if (TRANS) {
 		for (int i = ty; i < 32; i += 8) {
 			const int k = k0 + i, r = r0 + tx;
-			tile[i][tx] = (k < kdim && r < rows) ? src[static_cast<int64_t>(k) * lds + r] : 0.f;
+			float x = 0.f;
+			if (k < kdim && r < rows) {
+				x = src[static_cast<int64_t>(k) * lds + r];
+				if (deck) x = fmaf(__half2float(deck[static_cast<int64_t>(k) * ldd + r]), inv_scale, x);
+			}
+			tile[i][tx] = x;
 		}
 		__syncthreads();
 		for (int i = ty; i < 32; i += 8) {
@@ -98,9 +107,14 @@ __global__ void __launch_bounds__(256) panel_f16_kernel(int rows, int kdim, cons
 	} else {
 		for (int i = ty; i < 32; i += 8) {
 			const int r = r0 + i, k = k0 + tx;
-			if (r < rows && k < ldh)
-				out[static_cast<int64_t>(r) * ldh + k] =
-					__float2half_rn((k < kdim) ? src[static_cast<int64_t>(r) * lds + k] : 0.f);
+			if (r < rows && k < ldh) {
+				float x = 0.f;
+				if (k < kdim) {
+					x = src[static_cast<int64_t>(r) * lds + k];
+					if (deck) x = fmaf(__half2float(deck[static_cast<int64_t>(r) * ldd + k]), inv_scale, x);
+				}
+				out[static_cast<int64_t>(r) * ldh + k] = __float2half_rn(x);
+			}
 		}
 	}
 }
@@ -723,7 +737,7 @@ int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint1
 }
 
 int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
-	uint16_t *lh, uint16_t *uh, int64_t ldh, int max_ctas, cudaStream_t st)
+	uint16_t *lh, uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st)
 {
 	if (rem <= 0) return HPLAI_OK;
 	if (!t.f16_amax || !t.f16_oscale || ldh % 32) return HPLAI_EINVAL;
@@ -743,8 +757,9 @@ int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 	// A_col (rows kb+b.., columns kb..kb+b-1) -> FP16 K-major rows kb+b.. of lh
 	const int64_t kbl = kb;
 	float *acol = a + (kbl + b) + kbl * lda;
+	const __half *dcol = deck ? reinterpret_cast<const __half *>(deck) + (kbl + b) + kbl * lda : nullptr;
 	panel_f16_kernel<true><<<dim3((rem + 31) / 32, static_cast<unsigned>(ldh / 32)), 256, 0, st>>>(rem, b, acol, lda,
-		reinterpret_cast<__half *>(lh) + (kbl + b) * ldh, ldh);
+		dcol, lda, inv_dscale, reinterpret_cast<__half *>(lh) + (kbl + b) * ldh, ldh);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// A_col = (A_col (s_u U11^{-1})) / s_u
@@ -752,7 +767,7 @@ int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 }
 
 int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
-	uint16_t *uh, int64_t ldh, int max_ctas, cudaStream_t st)
+	uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st)
 {
 	if (rem <= 0) return HPLAI_OK;
 	if (!t.f16_oscale || ldh % 32) return HPLAI_EINVAL;
@@ -760,8 +775,9 @@ int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 	const int64_t kbl = kb;
 	// A_row (rows kb..kb+b-1, columns kb+b..): column j -> FP16 row kb+b+j of uh
 	float *arow = a + kbl + (kbl + b) * lda;
+	const __half *drow = deck ? reinterpret_cast<const __half *>(deck) + kbl + (kbl + b) * lda : nullptr;
 	panel_f16_kernel<false><<<dim3((rem + 31) / 32, static_cast<unsigned>(ldh / 32)), 256, 0, st>>>(rem, b, arow, lda,
-		reinterpret_cast<__half *>(uh) + (kbl + b) * ldh, ldh);
+		drow, lda, inv_dscale, reinterpret_cast<__half *>(uh) + (kbl + b) * ldh, ldh);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// A_row = ((s_l L11^{-1}) A_row) / s_l, the triangle in rows kb.. of the L buffer
