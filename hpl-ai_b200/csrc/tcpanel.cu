@@ -73,49 +73,82 @@ __global__ void __launch_bounds__(256) split_kernel(int rows, int kdim, const fl
 	}
 }
 
-// FP16 K-major copy of a panel for the precision form's panel products, with
-// split_kernel's indexing: out[r*ldh + k] = half_rn(x(r, k)), columns
-// kdim..ldh-1 zero.  (The precision form's Schur operands are e4m3, so FP16
-// operands, 11 significant bits, lose nothing that matters and run the panel
-// products at the FP16 tensor rate with half the bytes of TF32.)  With the
-// FP16 deck, x = fmaf(deck, inv_scale, a) as deck_apply_kernel forms it, the
-// deck element at the same offset from `deck` (leading dimension ldd) as the
-// panel element from `src`.
-template <bool TRANS>
-__global__ void __launch_bounds__(256) panel_f16_kernel(int rows, int kdim, const float *__restrict__ src,
+// FP16 K-major copies of a panel for the precision form's panel products:
+// out[r*ldh + k] = half_rn(x(r, k)) for k < kdim, zero for kdim <= k < ldh.
+// (The precision form's Schur operands are e4m3, so FP16 operands, 11
+// significant bits, lose nothing that matters and run the panel products at
+// the FP16 tensor rate with half the bytes of TF32.)  With the FP16 deck,
+// x = fmaf(deck, inv_scale, a) as deck_apply_kernel forms it, the deck element
+// at the same offset from `deck` (leading dimension ldd) as the panel element
+// from `src`.  rows, kdim, the offsets and the leading dimensions are
+// multiples of 4 (float4 loads, 4-half deck loads).
+__device__ __forceinline__ float4 load4_deck(const float *src, const __half *deck, float inv_scale)
+{
+	float4 v = *reinterpret_cast<const float4 *>(src);
+	if (deck) {
+		const uint2 d = *reinterpret_cast<const uint2 *>(deck);
+		const float2 d01 = __half22float2(*reinterpret_cast<const __half2 *>(&d.x));
+		const float2 d23 = __half22float2(*reinterpret_cast<const __half2 *>(&d.y));
+		v.x = fmaf(d01.x, inv_scale, v.x);
+		v.y = fmaf(d01.y, inv_scale, v.y);
+		v.z = fmaf(d23.x, inv_scale, v.z);
+		v.w = fmaf(d23.y, inv_scale, v.w);
+	}
+	return v;
+}
+
+// A_col: element (r, k) at src[k*lds + r] (column-major).  64 x 64 tiles
+// through shared memory: float4 loads along r, half2 stores along k.
+__global__ void __launch_bounds__(256) panel_f16_t_kernel(int rows, int kdim, const float *__restrict__ src,
 	int64_t lds, const __half *__restrict__ deck, int64_t ldd, float inv_scale, __half *__restrict__ out,
 	int64_t ldh)
 {
-	__shared__ float tile[32][33];
-	const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
-	const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
-	if (TRANS) {
-		for (int i = ty; i < 32; i += 8) {
-			const int k = k0 + i, r = r0 + tx;
-			float x = 0.f;
-			if (k < kdim && r < rows) {
-				x = src[static_cast<int64_t>(k) * lds + r];
-				if (deck) x = fmaf(__half2float(deck[static_cast<int64_t>(k) * ldd + r]), inv_scale, x);
-			}
-			tile[i][tx] = x;
-		}
-		__syncthreads();
-		for (int i = ty; i < 32; i += 8) {
-			const int r = r0 + i, k = k0 + tx;
-			if (r < rows && k < ldh) out[static_cast<int64_t>(r) * ldh + k] = __float2half_rn(tile[tx][i]);
-		}
-	} else {
-		for (int i = ty; i < 32; i += 8) {
-			const int r = r0 + i, k = k0 + tx;
-			if (r < rows && k < ldh) {
-				float x = 0.f;
-				if (k < kdim) {
-					x = src[static_cast<int64_t>(r) * lds + k];
-					if (deck) x = fmaf(__half2float(deck[static_cast<int64_t>(r) * ldd + k]), inv_scale, x);
-				}
-				out[static_cast<int64_t>(r) * ldh + k] = __float2half_rn(x);
-			}
-		}
+	__shared__ float tile[64][65];   // tile[k][r]
+	const int r0 = blockIdx.x * 64, k0 = blockIdx.y * 64;
+	const int t = threadIdx.x;
+#pragma unroll
+	for (int q = 0; q < 4; ++q) {
+		const int idx = t + 256 * q, kk = idx >> 4, rr = (idx & 15) * 4;
+		const int k = k0 + kk, r = r0 + rr;
+		float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+		if (k < kdim && r < rows)
+			v = load4_deck(src + static_cast<int64_t>(k) * lds + r,
+				deck ? deck + static_cast<int64_t>(k) * ldd + r : nullptr, inv_scale);
+		tile[kk][rr] = v.x;
+		tile[kk][rr + 1] = v.y;
+		tile[kk][rr + 2] = v.z;
+		tile[kk][rr + 3] = v.w;
+	}
+	__syncthreads();
+#pragma unroll
+	for (int q = 0; q < 8; ++q) {
+		const int idx = t + 256 * q, rr = idx >> 5, kp = (idx & 31) * 2;
+		const int r = r0 + rr, k = k0 + kp;
+		if (r < rows && k < ldh)
+			*reinterpret_cast<__half2 *>(out + static_cast<int64_t>(r) * ldh + k) =
+				__floats2half2_rn(tile[kp][rr], tile[kp + 1][rr]);
+	}
+}
+
+// A_row seen by columns: element (r, k) at src[r*lds + k]; no transpose.
+__global__ void __launch_bounds__(256) panel_f16_n_kernel(int rows, int kdim, const float *__restrict__ src,
+	int64_t lds, const __half *__restrict__ deck, int64_t ldd, float inv_scale, __half *__restrict__ out,
+	int64_t ldh)
+{
+	const int groups = static_cast<int>(ldh / 4);
+	const int64_t total = static_cast<int64_t>(rows) * groups;
+	for (int64_t e = static_cast<int64_t>(blockIdx.x) * 256 + threadIdx.x; e < total;
+		e += static_cast<int64_t>(gridDim.x) * 256) {
+		const int r = static_cast<int>(e / groups), k = static_cast<int>(e % groups) * 4;
+		float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+		if (k < kdim)
+			v = load4_deck(src + static_cast<int64_t>(r) * lds + k,
+				deck ? deck + static_cast<int64_t>(r) * ldd + k : nullptr, inv_scale);
+		const __half2 h01 = __floats2half2_rn(v.x, v.y), h23 = __floats2half2_rn(v.z, v.w);
+		uint2 w;
+		w.x = *reinterpret_cast<const uint32_t *>(&h01);
+		w.y = *reinterpret_cast<const uint32_t *>(&h23);
+		*reinterpret_cast<uint2 *>(out + static_cast<int64_t>(r) * ldh + k) = w;
 	}
 }
 
@@ -740,7 +773,7 @@ int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 	uint16_t *lh, uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st)
 {
 	if (rem <= 0) return HPLAI_OK;
-	if (!t.f16_amax || !t.f16_oscale || ldh % 32) return HPLAI_EINVAL;
+	if (!t.f16_amax || !t.f16_oscale || ldh % 64 || t.b % 4 || kb % 4 || rem % 4 || lda % 4) return HPLAI_EINVAL;
 	const int b = t.b;
 	// the inverted triangles into rows kb .. kb+b-1 of the FP16 panel buffers
 	// (rows the step's Schur update never reads)
@@ -758,7 +791,7 @@ int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 	const int64_t kbl = kb;
 	float *acol = a + (kbl + b) + kbl * lda;
 	const __half *dcol = deck ? reinterpret_cast<const __half *>(deck) + (kbl + b) + kbl * lda : nullptr;
-	panel_f16_kernel<true><<<dim3((rem + 31) / 32, static_cast<unsigned>(ldh / 32)), 256, 0, st>>>(rem, b, acol, lda,
+	panel_f16_t_kernel<<<dim3((rem + 63) / 64, static_cast<unsigned>(ldh / 64)), 256, 0, st>>>(rem, b, acol, lda,
 		dcol, lda, inv_dscale, reinterpret_cast<__half *>(lh) + (kbl + b) * ldh, ldh);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
@@ -770,14 +803,18 @@ int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 	uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st)
 {
 	if (rem <= 0) return HPLAI_OK;
-	if (!t.f16_oscale || ldh % 32) return HPLAI_EINVAL;
+	if (!t.f16_oscale || ldh % 64 || t.b % 4 || kb % 4 || rem % 4 || lda % 4) return HPLAI_EINVAL;
 	const int b = t.b;
 	const int64_t kbl = kb;
 	// A_row (rows kb..kb+b-1, columns kb+b..): column j -> FP16 row kb+b+j of uh
 	float *arow = a + kbl + (kbl + b) * lda;
 	const __half *drow = deck ? reinterpret_cast<const __half *>(deck) + kbl + (kbl + b) * lda : nullptr;
-	panel_f16_kernel<false><<<dim3((rem + 31) / 32, static_cast<unsigned>(ldh / 32)), 256, 0, st>>>(rem, b, arow, lda,
-		drow, lda, inv_dscale, reinterpret_cast<__half *>(uh) + (kbl + b) * ldh, ldh);
+	{
+		const int64_t work = static_cast<int64_t>(rem) * (ldh / 4);
+		const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((work + 255) / 256, 148 * 16));
+		panel_f16_n_kernel<<<blocks, 256, 0, st>>>(rem, b, arow, lda, drow, lda, inv_dscale,
+			reinterpret_cast<__half *>(uh) + (kbl + b) * ldh, ldh);
+	}
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// A_row = ((s_l L11^{-1}) A_row) / s_l, the triangle in rows kb.. of the L buffer
