@@ -257,7 +257,7 @@ __device__ __forceinline__ void stage_block(float *blk, const float *a, int64_t 
 // diagonal block is applied as one product instead of 128 dependent
 // substitution steps.
 template <bool TRANS>
-__global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, const float *__restrict__ a,
+__global__ void __launch_bounds__(TRSV_THREADS, 1) trsv_kernel(int lower, int n, const float *__restrict__ a,
 	int64_t lda, double *x, TrsvWork *w, const double *__restrict__ dinv)
 {
 	extern __shared__ __align__(16) float dyn_smem[];
@@ -297,6 +297,15 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 			if (t < 8)
 				asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(dblock + t * (TB * TB / 8)),
 					"r"(static_cast<unsigned>(sizeof(double) * TB * TB / 8)) : "memory");
+		}
+		// Not transposed: this thread's 64 entries of the inverse go to registers
+		// now, while the block row is summed, so that the diagonal step (the
+		// chain's critical path) does not wait on L2.
+		double dv[TB / 2];
+		if (!TRANS && dinv) {
+			const int jb = grp * (TB / 2);
+#pragma unroll
+			for (int q = 0; q < TB / 2; ++q) dv[q] = __ldcg(&dblock[static_cast<int64_t>(jb + q) * TB + lr]);
 		}
 		// Stage the diagonal block (independent of other CTAs).
 		for (int e = t; !dinv && e < TB * TB; e += TRSV_THREADS) {
@@ -423,8 +432,8 @@ __global__ void __launch_bounds__(TRSV_THREADS) trsv_kernel(int lower, int n, co
 			} else {
 				const int jb = grp * (TB / 2);
 				double v = 0.0;
-#pragma unroll 16
-				for (int jj = jb; jj < jb + TB / 2; ++jj) v = fma(dblock[static_cast<int64_t>(jj) * TB + lr], rhs[jj], v);
+#pragma unroll
+				for (int q = 0; q < TB / 2; ++q) v = fma(dv[q], rhs[jb + q], v);
 				part[grp][lr] = v;
 			}
 			__syncthreads();
