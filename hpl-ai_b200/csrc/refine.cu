@@ -301,6 +301,8 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) trsv_kernel(int lower, int n,
 		// Not transposed: this thread's 64 entries of the inverse go to registers
 		// now, while the block row is summed, so that the diagonal step (the
 		// chain's critical path) does not wait on L2.
+		// this block's right-hand side (only this CTA writes it, at the end)
+		const double xr = (t < rows) ? __ldcg(&x[r0 + t]) : 0.0;
 		double dv[TB / 2];
 		if (!TRANS && dinv) {
 			const int jb = grp * (TB / 2);
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) trsv_kernel(int lower, int n,
 			part[grp][lr] = acc;
 		}
 		__syncthreads();
-		if (t < TB) rhs[t] = (t < rows) ? x[r0 + t] - (part[0][t] + part[1][t]) : 0.0;
+		if (t < TB) rhs[t] = (t < rows) ? xr - (part[0][t] + part[1][t]) : 0.0;
 		__syncthreads();
 		if (dinv) {
 			// x_r = M_rr^{-1} rhs: element (i, j) of M^{-1} is dblock[j*TB + i], or

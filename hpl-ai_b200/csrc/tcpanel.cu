@@ -73,6 +73,59 @@ __global__ void __launch_bounds__(256) split_kernel(int rows, int kdim, const fl
 	}
 }
 
+// Vectorised forms of split_kernel for panels whose rows, width and offsets
+// are multiples of 4 (b % 4 == 0): float4 loads, 8- or 16-byte stores.
+// TRANS (A_col, element (r, k) at src[k*lds + r]): 64 x 64 transpose tiles.
+__global__ void __launch_bounds__(256) split_t_kernel(int rows, int kdim, const float *__restrict__ src, int64_t lds,
+	float *__restrict__ phi, float *__restrict__ plo, int64_t ldp)
+{
+	__shared__ float tile[64][65];   // tile[k][r]
+	const int r0 = blockIdx.x * 64, k0 = blockIdx.y * 64;
+	const int t = threadIdx.x;
+#pragma unroll
+	for (int q = 0; q < 4; ++q) {
+		const int idx = t + 256 * q, kk = idx >> 4, rr = (idx & 15) * 4;
+		const int k = k0 + kk, r = r0 + rr;
+		float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+		if (k < kdim && r < rows) v = *reinterpret_cast<const float4 *>(src + static_cast<int64_t>(k) * lds + r);
+		tile[kk][rr] = v.x;
+		tile[kk][rr + 1] = v.y;
+		tile[kk][rr + 2] = v.z;
+		tile[kk][rr + 3] = v.w;
+	}
+	__syncthreads();
+#pragma unroll
+	for (int q = 0; q < 8; ++q) {
+		const int idx = t + 256 * q, rr = idx >> 5, kp = (idx & 31) * 2;
+		const int r = r0 + rr, k = k0 + kp;
+		if (r < rows && k < ldp) {
+			const float x0 = tile[kp][rr], x1 = tile[kp + 1][rr];
+			const float h0 = tf32_hi(x0), h1 = tf32_hi(x1);
+			*reinterpret_cast<float2 *>(phi + static_cast<int64_t>(r) * ldp + k) = make_float2(h0, h1);
+			if (plo) *reinterpret_cast<float2 *>(plo + static_cast<int64_t>(r) * ldp + k) = make_float2(x0 - h0, x1 - h1);
+		}
+	}
+}
+
+// not TRANS (A_row seen by columns, element (r, k) at src[r*lds + k]).
+__global__ void __launch_bounds__(256) split_n_kernel(int rows, int kdim, const float *__restrict__ src, int64_t lds,
+	float *__restrict__ phi, float *__restrict__ plo, int64_t ldp)
+{
+	const int groups = static_cast<int>(ldp / 4);
+	const int64_t total = static_cast<int64_t>(rows) * groups;
+	for (int64_t e = static_cast<int64_t>(blockIdx.x) * 256 + threadIdx.x; e < total;
+		e += static_cast<int64_t>(gridDim.x) * 256) {
+		const int r = static_cast<int>(e / groups), k = static_cast<int>(e % groups) * 4;
+		float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+		if (k < kdim) v = *reinterpret_cast<const float4 *>(src + static_cast<int64_t>(r) * lds + k);
+		const float4 h = make_float4(tf32_hi(v.x), tf32_hi(v.y), tf32_hi(v.z), tf32_hi(v.w));
+		*reinterpret_cast<float4 *>(phi + static_cast<int64_t>(r) * ldp + k) = h;
+		if (plo)
+			*reinterpret_cast<float4 *>(plo + static_cast<int64_t>(r) * ldp + k) =
+				make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+	}
+}
+
 // FP16 K-major copies of a panel for the precision form's panel products:
 // out[r*ldh + k] = half_rn(x(r, k)) for k < kdim, zero for kdim <= k < ldh.
 // (The precision form's Schur operands are e4m3, so FP16 operands, 11
@@ -745,8 +798,15 @@ int launch_lpanel_tc(const TcPanels &t, int rem, float *acol, int64_t lda, uint1
 {
 	if (rem <= 0) return HPLAI_OK;
 	const int b = t.b;
-	dim3 g((rem + 31) / 32, static_cast<unsigned>(t.ldp / 32));
-	split_kernel<true><<<g, 256, 0, st>>>(rem, b, acol, lda, t.phi, t.terms == 1 ? nullptr : t.plo, t.ldp);
+	float *plo = t.terms == 1 ? nullptr : t.plo;
+	const bool vec = b % 4 == 0 && rem % 4 == 0 && lda % 4 == 0 && (reinterpret_cast<uintptr_t>(acol) & 15) == 0;
+	if (vec) {
+		split_t_kernel<<<dim3((rem + 63) / 64, static_cast<unsigned>((t.ldp + 63) / 64)), 256, 0, st>>>(rem, b, acol,
+			lda, t.phi, plo, t.ldp);
+	} else {
+		dim3 g((rem + 31) / 32, static_cast<unsigned>(t.ldp / 32));
+		split_kernel<true><<<g, 256, 0, st>>>(rem, b, acol, lda, t.phi, plo, t.ldp);
+	}
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// X (rem x b) = A_col U^{-1}: out32 column-major in A, out16 row-major (Lh row = panel row)
@@ -759,9 +819,17 @@ int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint1
 {
 	if (rem <= 0) return HPLAI_OK;
 	const int b = t.b;
-	dim3 g((rem + 31) / 32, static_cast<unsigned>(t.ldp / 32));
 	// B operand row j = column j of A_row (b contiguous floats, stride lda)
-	split_kernel<false><<<g, 256, 0, st>>>(rem, b, arow, lda, t.phi, t.terms == 1 ? nullptr : t.plo, t.ldp);
+	float *plo = t.terms == 1 ? nullptr : t.plo;
+	const bool vec = b % 4 == 0 && lda % 4 == 0 && (reinterpret_cast<uintptr_t>(arow) & 15) == 0;
+	if (vec) {
+		const int64_t work = static_cast<int64_t>(rem) * (t.ldp / 4);
+		const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((work + 255) / 256, 148 * 16));
+		split_n_kernel<<<blocks, 256, 0, st>>>(rem, b, arow, lda, t.phi, plo, t.ldp);
+	} else {
+		dim3 g((rem + 31) / 32, static_cast<unsigned>(t.ldp / 32));
+		split_kernel<false><<<g, 256, 0, st>>>(rem, b, arow, lda, t.phi, plo, t.ldp);
+	}
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// Y (b x rem) = L^{-1} A_row: out32 column-major in A, out16 with column j of U as row j of Uh
