@@ -50,6 +50,7 @@ using namespace hplai;
 struct hplai_ctx {
 	int n = 0, b = 0, nb = 0, precision = 0;
 	unsigned flags = 0;
+	int side_sms = 20;   // SMs of the side stream with HPLAI_FLAG_LOOKAHEAD (hplai_autotune sets it)
 	int64_t lda = 0, ldh = 0;
 	float *A = nullptr;
 	// FP16 panel copies, double buffered: the panels of step k+1 are formed
@@ -472,9 +473,9 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	// (first) and the rest of the trailing matrix (after).  With
 	// HPLAI_FLAG_LOOKAHEAD step k+1's diagonal block and panels are formed on
 	// the side stream as soon as the first part is done, overlapping the
-	// second, which then leaves kSideSms SMs to the side stream; otherwise
+	// second, which then leaves side_sms SMs to the side stream; otherwise
 	// everything runs in the same order on one stream.
-	constexpr int kSideSms = 20;
+	const int kSideSms = c->side_sms;
 	cudaStream_t st = c->st, sd = serial ? c->st : c->st2;
 	const int side_ctas = serial ? 0 : kSideSms;
 	int sms = 148;
@@ -785,6 +786,67 @@ int hplai_ctx_solve_stream_rhs(hplai_ctx *c, int col, double *x, int maxit, hpla
 	HPLAI_CUDA_TRY(cudaMemcpyAsync(x, c->x2, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
 	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
 	return rc;
+}
+
+// The project's own tuner in place of lda_tuner (lda_tuner.hpp:9-45, whose
+// call the reference leaves commented out): the factorisation is timed on
+// this context (regenerated from `seed` before each trial) serially and with
+// look-ahead at several side-stream SM counts; the fastest becomes the
+// context's schedule.  Tile shapes are compile-time constants of the kernels
+// (measured sweeps chose them), so the run-time choice is the schedule.
+extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, int *side_sms_out, double *ms_out)
+{
+	if (!c) return HPLAI_EINVAL;
+	int sms = 148;
+	{
+		int dev = 0;
+		if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	}
+	struct Trial {
+		bool lookahead;
+		int side;
+	};
+	const Trial trials[] = {{false, 20}, {true, 16}, {true, 24}, {true, 32}, {true, 48}};
+	const unsigned flags0 = c->flags, base_flags = c->flags & ~HPLAI_FLAG_LOOKAHEAD;
+	const int side0 = c->side_sms;
+	double best = -1.0;
+	Trial pick = trials[0];
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	HPLAI_CUDA_TRY(cudaEventCreate(&e0));
+	HPLAI_CUDA_TRY(cudaEventCreate(&e1));
+	int rc = HPLAI_OK;
+	for (const Trial &t : trials) {
+		if (t.lookahead && sms <= 2 * t.side) continue;
+		c->flags = base_flags | (t.lookahead ? HPLAI_FLAG_LOOKAHEAD : 0u);
+		c->side_sms = t.side;
+		rc = hplai_generate(c, seed);
+		if (rc == HPLAI_OK && cudaEventRecord(e0, c->st) != cudaSuccess) rc = HPLAI_ECUDA;
+		if (rc == HPLAI_OK) rc = hplai_factor(c);
+		if (rc == HPLAI_OK && cudaEventRecord(e1, c->st) != cudaSuccess) rc = HPLAI_ECUDA;
+		if (rc == HPLAI_OK && cudaEventSynchronize(e1) != cudaSuccess) rc = HPLAI_ECUDA;
+		float ms = 0.f;
+		if (rc == HPLAI_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = HPLAI_ECUDA;
+		if (rc != HPLAI_OK) break;
+		if (best < 0.0 || ms < best) {
+			best = ms;
+			pick = t;
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	if (rc != HPLAI_OK) {
+		c->flags = flags0;
+		c->side_sms = side0;
+		return rc;
+	}
+	c->flags = base_flags | (pick.lookahead ? HPLAI_FLAG_LOOKAHEAD : 0u);
+	c->side_sms = pick.side;
+	// the context is left generated and unfactored, as after hplai_generate
+	HPLAI_TRY(hplai_generate(c, seed));
+	if (flags_out) *flags_out = c->flags;
+	if (side_sms_out) *side_sms_out = c->side_sms;
+	if (ms_out) *ms_out = best;
+	return HPLAI_OK;
 }
 
 extern "C" int hplai_refine(hplai_ctx *c, int mode, int maxit, hplai_ir_errors *err, int *iters)

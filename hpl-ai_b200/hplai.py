@@ -57,6 +57,7 @@ _destroy = _proto("hplai_destroy", _c_int, _vp)
 _generate = _proto("hplai_generate", _c_int, _vp, _c_u64)
 _upload = _proto("hplai_upload", _c_int, _vp, _vp, _c_i64, _vp, _vp, _c_u64)
 _factor = _proto("hplai_factor", _c_int, _vp)
+_autotune = _proto("hplai_autotune", _c_int, _vp, _c_u64, _vp, _vp, _vp)
 _refine = _proto("hplai_refine", _c_int, _vp, _c_int, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
 _get_x = _proto("hplai_get_x", _c_int, _vp, _vp)
 _get_lu = _proto("hplai_get_lu", _c_int, _vp, _vp, _c_i64)
@@ -192,6 +193,14 @@ class Solver:
 
     def factor(self):
         check(_factor(self._h), "hplai_factor")
+
+    def autotune(self, seed: int = 42):
+        """Time the factorisation serially and with look-ahead at several
+        side-stream SM counts, keep the fastest schedule; returns
+        (flags, side_sms, best_ms).  The context is left generated from seed."""
+        fl, side, ms = ctypes.c_uint(), _c_int(), ctypes.c_double()
+        check(_autotune(self._h, seed, ctypes.byref(fl), ctypes.byref(side), ctypes.byref(ms)), "hplai_autotune")
+        return fl.value, side.value, ms.value
 
     def iterative_refinement(self, maxit: int = 50, mode: int = IR) -> RefineResult:
         e = IRErrors()

@@ -135,6 +135,14 @@ int hplai_upload(hplai_ctx *ctx, const float *a, int64_t lda, const double *rhs,
  * collapsed to one GPU.  Unit-L below and U on/above the diagonal, FP32. */
 int hplai_factor(hplai_ctx *ctx);
 
+/* Schedule tuner in place of lda_tuner (lda_tuner.hpp:9-45): times
+ * hplai_factor on this context (regenerated from seed before each trial)
+ * serially and with HPLAI_FLAG_LOOKAHEAD at several side-stream SM counts,
+ * keeps the fastest as the context's schedule, and leaves the context
+ * generated and unfactored.  Outputs (may be NULL): the chosen flags, the
+ * side-stream SM count and the best factorisation time in ms. */
+int hplai_autotune(hplai_ctx *ctx, uint64_t seed, unsigned *flags, int *side_sms, double *ms);
+
 /* iterative_refinement (iterative_refinement.hpp:18-57) with maxit steps
  * (the driver uses 50).  Fills *err ({-1,-1} on failure) and *iters (the
  * number of residual evaluations).  Returns HPLAI_ENOTCONV on failure.

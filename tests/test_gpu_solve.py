@@ -156,3 +156,21 @@ def test_call_order_and_nonconvergence(hplai, torch_cuda):
         assert r.status == hplai.HPLAI_ENOTCONV and r.residual == -1 and r.hpl_harness == -1
         r = s.iterative_refinement(50)
         assert r.status == hplai.HPLAI_OK
+
+
+def test_autotune_picks_a_schedule_and_solves(hplai, oracle, torch_cuda):
+    """hplai_autotune leaves a valid schedule (serial, or look-ahead with a
+    side-stream SM count) and a generated, unfactored context; the solve
+    with that schedule converges to the same x as the serial one."""
+    n, b = 4096, 512
+    with hplai.Solver(n, b) as s:
+        flags, side, ms = s.autotune(42)
+        assert ms > 0.0 and side in (16, 20, 24, 32, 48)
+        assert flags & ~hplai.FLAG_LOOKAHEAD == 0
+        s.factor()
+        res = s.iterative_refinement(50)
+        x = s.x()
+    assert res.status == hplai.HPLAI_OK and res.hpl_harness < 16.0
+    a = oracle.dense_matrix_f64(n, 42)
+    xs = np.linalg.solve(a, oracle.rhs(n, 42))
+    assert np.max(np.abs(x - xs)) / np.max(np.abs(xs)) < 1e-12
