@@ -254,6 +254,11 @@ def run_ours(args):
     s = hplai.Solver(n, b, precision=prec, flags=flags)
     ext = torch.cuda.ExternalStream(s.stream())
     results = []
+    tuned = None
+    if args.autotune:
+        # outside the timed region: time the factorisation under each schedule, keep the fastest
+        tflags, tside, tms = s.autotune(seed)
+        tuned = {"lookahead": bool(tflags & hplai.FLAG_LOOKAHEAD), "side_sms": tside, "factor_ms": tms}
 
     def one_step(timed):
         s.generate(seed)
@@ -375,7 +380,7 @@ def run_ours(args):
             "config": {"workload": f"HPL-AI solve n={n} b={b}: FP32 panels, "
                                    f"{'e4m3' if prec == hplai.F32_F8 else 'FP16'} tcgen05 Schur update, "
                                    f"FP64 {'GMRES-IR' if mode == hplai.GMRES else 'iterative refinement'}",
-                       "n": n, "b": b, "form": form, "lookahead": bool(args.lookahead),
+                       "n": n, "b": b, "form": form, "lookahead": bool(args.lookahead), "autotuned": tuned,
                        "trailing_matrix": "FP16 deck (updates in FP16, applied per panel)" if deck else "FP32",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": f"inputs {n * n * 4 / 1e9:.1f} GB FP32 > 126 MB L2, rewritten between steps"},
@@ -582,11 +587,17 @@ def main():
     ap.add_argument("--batch-workers", type=int, default=8)
     ap.add_argument("--deck", choices=("on", "off"), default="off",
                     help="FP16 trailing-update deck (HPLAI_FLAG_FP16_DECK)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="choose the schedule (serial or look-ahead, side-stream SMs) with hplai_autotune first "
+                         "(the default for the solve workload unless --lookahead or --no-autotune is given)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the serial schedule (or --lookahead's)")
     ap.add_argument("--lookahead", action="store_true",
                     help="form the next step's diagonal block and panels on a side stream (HPLAI_FLAG_LOOKAHEAD)")
     ap.add_argument("--refine", choices=("ir", "gmres"), default=None,
                     help="correction: classical IR or GMRES (default: ir for f16, gmres for f8)")
     args = ap.parse_args()
+    if not args.lookahead and not args.no_autotune:
+        args.autotune = True
     if args.n is None:
         args.n = ADJOINT_N if args.workload == "adjoint" else DEFAULT_N
     if args.b is None:
