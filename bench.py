@@ -563,6 +563,40 @@ def run_gemm(args):
     return 0
 
 
+def run_check(args):
+    """The factored-matrix checksum (panel_check.hpp:9-65) alone through its
+    leaf entry point: one read of an n x n FP32 matrix (4 n^2 bytes, larger
+    than L2 at the default n) into three FP64 sums; reports GB/s of that read."""
+    import torch
+    torch.cuda.set_device(0)
+    import hplai
+    n = args.n
+    lda = (n + 63) // 64 * 64 + 64   # the solver's padded leading dimension
+    torch.manual_seed(0)
+    a = torch.rand(n, lda, device="cuda") - 0.5
+    ws = hplai.panel_check_workspace(n)
+    work = torch.empty(ws // 8 + 1, dtype=torch.float64, device="cuda")
+    sig = torch.empty(3, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def call():
+        hplai.check(hplai.panel_check(n, a.data_ptr(), lda, sig.data_ptr(), work.data_ptr(), ws, stream.cuda_stream))
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        call()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    byts = 4.0 * n * n
+    print(json.dumps({"workload": f"panel_check leaf n={n} lda={lda} FP32", "ms_per_launch": ms,
+                      "gbs": byts / ms / 1e6, "algorithmic_bytes": byts}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -576,9 +610,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--precision", choices=("f16", "f8"), default="f16",
                     help="Schur update operands: FP16 (plain form) or e4m3 with per-128 factors")
-    ap.add_argument("--workload", choices=("solve", "batch", "adjoint", "gemm"), default="solve",
+    ap.add_argument("--workload", choices=("solve", "batch", "adjoint", "gemm", "check"), default="solve",
                     help="solve: one system (default n=65536 b=512); batch: many systems; adjoint: forward + "
-                         "transposed solves")
+                         "transposed solves; gemm / check: the Schur GEMM or the factor checksum leaf alone")
     ap.add_argument("--m", type=int, default=16384, help="gemm workload: rows of C")
     ap.add_argument("--n-cols", type=int, default=16384, help="gemm workload: columns of C")
     ap.add_argument("--k", type=int, default=512, help="gemm workload: panel width")
@@ -610,6 +644,8 @@ def main():
         return run_adjoint(args)
     if args.workload == "gemm":
         return run_gemm(args)
+    if args.workload == "check":
+        return run_check(args)
     return run_ours(args)
 
 

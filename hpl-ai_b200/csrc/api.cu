@@ -76,6 +76,7 @@ struct hplai_ctx {
 	void *trsv_work = nullptr;
 	size_t trsv_bytes = 0;
 	void *getrf_work = nullptr;   // tile flags of the diagonal block LU
+	void *check_work = nullptr;   // hplai_checksum: per-CTA partial sums, then the three results
 	double *dinv = nullptr;       // FP64 inverses of the factors' 128 x 128 diagonal blocks
 	unsigned *kstatus = nullptr;  // timeout words of this context's Schur [0] and panel [1] kernels
 	unsigned *f16s = nullptr;     // precision form: triangle maxima [0..1] and inverse scales [2..3]
@@ -126,6 +127,7 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->gemv_work);
 	cudaFree(c->trsv_work);
 	cudaFree(c->getrf_work);
+	cudaFree(c->check_work);
 	cudaFree(c->dinv);
 	cudaFree(c->kstatus);
 	cudaFree(c->f16s);
@@ -292,6 +294,7 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	c->trsv_bytes = trsv_workspace(n);
 	CTX_ALLOC(c->trsv_work, c->trsv_bytes);
 	CTX_ALLOC(c->getrf_work, getrf_workspace());
+	CTX_ALLOC(c->check_work, panel_check_workspace(n) + 3 * sizeof(double));
 	CTX_ALLOC(c->dinv, sizeof(double) * trsv_dinv_doubles(n));
 	CTX_ALLOC(c->kstatus, 2 * sizeof(unsigned));
 	CTX_ALLOC(c->f16s, 4 * sizeof(unsigned));
@@ -881,6 +884,16 @@ extern "C" int hplai_get_lu(hplai_ctx *c, float *a, int64_t lda)
 	if (!c || !a || lda < c->n) return HPLAI_EINVAL;
 	HPLAI_CUDA_TRY(cudaMemcpy2DAsync(a, sizeof(float) * lda, c->A, sizeof(float) * c->lda, sizeof(float) * c->n, c->n,
 		cudaMemcpyDeviceToHost, c->st));
+	HPLAI_CUDA_TRY(cudaStreamSynchronize(c->st));
+	return HPLAI_OK;
+}
+
+extern "C" int hplai_checksum(hplai_ctx *c, double *sigs)
+{
+	if (!c || !sigs) return HPLAI_EINVAL;
+	double *dsig = static_cast<double *>(c->check_work);
+	HPLAI_TRY(launch_panel_check(c->n, c->A, c->lda, dsig, dsig + 3, panel_check_workspace(c->n), c->st));
+	HPLAI_CUDA_TRY(cudaMemcpyAsync(sigs, dsig, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
 	HPLAI_CUDA_TRY(cudaStreamSynchronize(c->st));
 	return HPLAI_OK;
 }

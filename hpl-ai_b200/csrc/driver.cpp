@@ -44,9 +44,10 @@ static int usage()
 		"   --fp8                   e4m3 Schur update with GMRES refinement.\n"
 		"   --gmres                 GMRES refinement instead of the classical correction.\n"
 		"   --lookahead             Factor the next panel while the trailing update runs.\n"
+		"   --checksum              Print sums of |diag|, |upper|, |lower| of the factors after the LU.\n"
 		"   --help or -h            Print this message.\n"
 		"Layout and transport flags of the distributed reference (-not, -r, -m, -w, --pack,\n"
-		"--numa, --numa-map, --nbuf, --job-id, --checksum, --l1est, --highammat, --pwrtune)\n"
+		"--numa, --numa-map, --nbuf, --job-id, --l1est, --highammat, --pwrtune)\n"
 		"are accepted and ignored.\n");
 	return 0;
 }
@@ -57,6 +58,7 @@ int main(int argc, char **argv)
 	unsigned long long seed = 42;
 	int precision = HPLAI_F32_F16, mode = HPLAI_IR;
 	unsigned flags = 0;
+	bool checksum = false;
 	if (argc > 1) n = std::atoi(argv[1]);
 	if (argc > 2) b = std::atoi(argv[2]);
 	for (int i = 4; i < argc; ++i) {
@@ -69,6 +71,7 @@ int main(int argc, char **argv)
 		else if (!std::strcmp(argv[i], "--fp8")) { precision = HPLAI_F32_F8; mode = HPLAI_GMRES; }
 		else if (!std::strcmp(argv[i], "--gmres")) mode = HPLAI_GMRES;
 		else if (!std::strcmp(argv[i], "--lookahead")) flags |= HPLAI_FLAG_LOOKAHEAD;
+		else if (!std::strcmp(argv[i], "--checksum")) checksum = true;
 		else if (!std::strcmp(argv[i], "--numa") || !std::strcmp(argv[i], "--numa-map") ||
 			!std::strcmp(argv[i], "--nbuf") || !std::strcmp(argv[i], "--job-id")) ++i;
 		else if (argv[i][0] == '-') std::printf("Ignoring option not applicable on one GPU: %s\n", argv[i]);
@@ -118,6 +121,13 @@ int main(int argc, char **argv)
 	int iters = 0;
 	auto t0 = std::chrono::steady_clock::now();
 	rc = hplai_factor(ctx);
+	if (rc == HPLAI_OK && checksum) {
+		// inside the timed region, between the LU and the refinement (main.cpp:298-302)
+		double sigs[3];
+		rc = hplai_checksum(ctx, sigs);
+		if (rc == HPLAI_OK) std::printf("check %22.17e %22.17e, %22.17e\n", sigs[0], sigs[1], sigs[2]);
+		std::fflush(stdout);
+	}
 	int rr = HPLAI_OK;
 	if (rc == HPLAI_OK) rr = hplai_refine(ctx, mode, maxit, &er, &iters);
 	auto t1 = std::chrono::steady_clock::now();

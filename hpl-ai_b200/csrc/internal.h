@@ -166,6 +166,11 @@ size_t trsv_dinv_doubles(int n);
 int launch_trsv_dinv(int n, const float *a, int64_t lda, double *dinv, cudaStream_t st);
 int trsv_status(void *work, cudaStream_t st, int *status);
 int launch_infnorm(int n, const double *x, double *out, cudaStream_t st);
+// panel_check: sigs (device, 3 doubles) = FP64 sums of |a_ij| over the
+// diagonal, strict upper and strict lower triangle of a (n x n, lda).
+size_t panel_check_workspace(int n);
+int launch_panel_check(int n, const float *a, int64_t lda, double *sigs, void *work, size_t work_bytes,
+	cudaStream_t st);
 int launch_div(int n, const double *num, const double *den, double *out, cudaStream_t st);
 int launch_axpy1(int n, const double *x, double *y, cudaStream_t st);
 

@@ -508,6 +508,102 @@ __global__ void infnorm_kernel(int n, const double *__restrict__ x, unsigned lon
 	}
 }
 
+// Checksum of the factored matrix (panel_check.hpp:9-65): FP64 sums of
+// |a_ij| over the diagonal, the strict upper and the strict lower triangle.
+// HBM-bound (4 n^2 bytes read once).  One warp per column, grid-stride over
+// columns, two float4 loads in flight per lane where a and lda allow them;
+// each CTA writes its three partial sums and one CTA folds them in a fixed
+// order, so the result depends on n and the matrix only.
+constexpr int kCheckWarps = 8;
+
+int check_blocks(int n)
+{
+	const int need = (n + kCheckWarps - 1) / kCheckWarps;
+	return need < 1184 ? (need > 0 ? need : 1) : 1184;   // 148 SMs x 8 CTAs
+}
+
+__device__ __forceinline__ void check_add(float v, int r, int j, double &sd, double &su, double &sl)
+{
+	const double t = fabs(static_cast<double>(v));
+	if (r < j) su += t;
+	else if (r == j) sd += t;
+	else sl += t;
+}
+
+__global__ void __launch_bounds__(kCheckWarps * 32) check_partial_kernel(int n, const float *__restrict__ a,
+	int64_t lda, int vec, double *__restrict__ part)
+{
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	double sd = 0.0, su = 0.0, sl = 0.0;
+	const int n4 = vec ? (n & ~3) : 0;
+	for (int j = blockIdx.x * kCheckWarps + warp; j < n; j += gridDim.x * kCheckWarps) {
+		const float *col = a + static_cast<int64_t>(j) * lda;
+		int i = lane * 4;
+		for (; i + 128 < n4; i += 256) {
+			const float4 v0 = __ldcs(reinterpret_cast<const float4 *>(col + i));
+			const float4 v1 = __ldcs(reinterpret_cast<const float4 *>(col + i + 128));
+			check_add(v0.x, i, j, sd, su, sl);
+			check_add(v0.y, i + 1, j, sd, su, sl);
+			check_add(v0.z, i + 2, j, sd, su, sl);
+			check_add(v0.w, i + 3, j, sd, su, sl);
+			check_add(v1.x, i + 128, j, sd, su, sl);
+			check_add(v1.y, i + 129, j, sd, su, sl);
+			check_add(v1.z, i + 130, j, sd, su, sl);
+			check_add(v1.w, i + 131, j, sd, su, sl);
+		}
+		if (i < n4) {
+			const float4 v0 = __ldcs(reinterpret_cast<const float4 *>(col + i));
+			check_add(v0.x, i, j, sd, su, sl);
+			check_add(v0.y, i + 1, j, sd, su, sl);
+			check_add(v0.z, i + 2, j, sd, su, sl);
+			check_add(v0.w, i + 3, j, sd, su, sl);
+		}
+		for (int r = n4 + lane; r < n; r += 32) check_add(__ldcs(col + r), r, j, sd, su, sl);
+	}
+	for (int o = 16; o; o >>= 1) {
+		sd += __shfl_xor_sync(0xffffffffu, sd, o);
+		su += __shfl_xor_sync(0xffffffffu, su, o);
+		sl += __shfl_xor_sync(0xffffffffu, sl, o);
+	}
+	__shared__ double ws[3][kCheckWarps];
+	if (lane == 0) {
+		ws[0][warp] = sd;
+		ws[1][warp] = su;
+		ws[2][warp] = sl;
+	}
+	__syncthreads();
+	if (threadIdx.x < 3) {
+		double s = 0.0;
+		for (int w = 0; w < kCheckWarps; ++w) s += ws[threadIdx.x][w];
+		part[3 * blockIdx.x + threadIdx.x] = s;
+	}
+}
+
+__global__ void __launch_bounds__(256) check_fold_kernel(int nparts, const double *__restrict__ part, double *sigs)
+{
+	__shared__ double s[3][256];
+	const int t = threadIdx.x;
+	double d = 0.0, u = 0.0, l = 0.0;
+	for (int p = t; p < nparts; p += 256) {
+		d += part[3 * p];
+		u += part[3 * p + 1];
+		l += part[3 * p + 2];
+	}
+	s[0][t] = d;
+	s[1][t] = u;
+	s[2][t] = l;
+	for (int o = 128; o; o >>= 1) {
+		__syncthreads();
+		if (t < o) {
+			s[0][t] += s[0][t + o];
+			s[1][t] += s[1][t + o];
+			s[2][t] += s[2][t + o];
+		}
+	}
+	__syncthreads();
+	if (t < 3) sigs[t] = s[t][0];
+}
+
 __global__ void div_kernel(int n, const double *__restrict__ num, const double *__restrict__ den, double *out)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -627,6 +723,31 @@ int launch_infnorm(int n, const double *x, double *out, cudaStream_t st)
 	return HPLAI_OK;
 }
 
+size_t panel_check_workspace(int n)
+{
+	return 3 * sizeof(double) * static_cast<size_t>(check_blocks(n));
+}
+
+int launch_panel_check(int n, const float *a, int64_t lda, double *sigs, void *work, size_t work_bytes,
+	cudaStream_t st)
+{
+	if (n <= 0) {
+		HPLAI_CUDA_TRY(cudaMemsetAsync(sigs, 0, 3 * sizeof(double), st));
+		return HPLAI_OK;
+	}
+	if (work_bytes < panel_check_workspace(n)) return HPLAI_EINVAL;
+	const int blocks = check_blocks(n);
+	const int vec = (reinterpret_cast<uintptr_t>(a) % 16 == 0 && lda % 4 == 0) ? 1 : 0;
+	double *part = static_cast<double *>(work);
+	check_partial_kernel<<<blocks, kCheckWarps * 32, 0, st>>>(n, a, lda, vec, part);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	check_fold_kernel<<<1, 256, 0, st>>>(blocks, part, sigs);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
 int launch_div(int n, const double *num, const double *den, double *out, cudaStream_t st)
 {
 	if (n <= 0) return HPLAI_OK;
@@ -728,6 +849,22 @@ extern "C" int hplai_infnorm(int n, const double *x, double *out, void *stream)
 {
 	if (n < 0 || (!x && n) || !out) return HPLAI_EINVAL;
 	return hplai::launch_infnorm(n, x, out, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" size_t hplai_panel_check_workspace(int n)
+{
+	return hplai::panel_check_workspace(n);
+}
+
+extern "C" int hplai_panel_check(int n, const float *a, int64_t lda, double *sigs, void *work, size_t work_bytes,
+	void *stream)
+{
+	if (n < 0 || !sigs || (n > 0 && (!a || lda < n || !work))) return HPLAI_EINVAL;
+	if (n > 0 && work_bytes < hplai::panel_check_workspace(n)) {
+		hplai::set_last_error_message("hplai_panel_check: work is smaller than hplai_panel_check_workspace(n)");
+		return HPLAI_EINVAL;
+	}
+	return hplai::launch_panel_check(n, a, lda, sigs, work, work_bytes, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int hplai_otf_gemv_noalloc(int n, double alpha, const double *x, double beta, double *y, uint64_t seed,

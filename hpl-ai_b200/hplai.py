@@ -61,6 +61,7 @@ _autotune = _proto("hplai_autotune", _c_int, _vp, _c_u64, _vp, _vp, _vp)
 _refine = _proto("hplai_refine", _c_int, _vp, _c_int, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
 _get_x = _proto("hplai_get_x", _c_int, _vp, _vp)
 _get_lu = _proto("hplai_get_lu", _c_int, _vp, _vp, _c_i64)
+_checksum = _proto("hplai_checksum", _c_int, _vp, _vp)
 _get_rhs = _proto("hplai_get_rhs", _c_int, _vp, _vp)
 _get_diag = _proto("hplai_get_diag", _c_int, _vp, _vp)
 _get_ir_log = _proto("hplai_get_ir_log", _c_int, _vp, _vp, _vp, _c_int, ctypes.POINTER(_c_int))
@@ -106,6 +107,8 @@ trsv_workspace = _proto("hplai_trsv_workspace", _c_sz, _c_int)
 trsv_lower = _proto("hplai_trsv_lower", _c_int, _c_int, _vp, _c_i64, _vp, _vp, _c_sz, _vp)
 trsv_upper = _proto("hplai_trsv_upper", _c_int, _c_int, _vp, _c_i64, _vp, _vp, _c_sz, _vp)
 infnorm = _proto("hplai_infnorm", _c_int, _c_int, _vp, _vp, _vp)
+panel_check_workspace = _proto("hplai_panel_check_workspace", _c_sz, _c_int)
+panel_check = _proto("hplai_panel_check", _c_int, _c_int, _vp, _c_i64, _vp, _vp, _c_sz, _vp)
 
 
 gen_rhs_cols = _proto("hplai_gen_rhs_cols", _c_int, _c_int, _c_u64, _c_int, _c_int, _vp, _vp)
@@ -258,6 +261,13 @@ class Solver:
     def lu(self) -> np.ndarray:
         out = np.empty((self.n, self.n), dtype=np.float32, order="F")
         check(_get_lu(self._h, _ptr(out), self.n), "hplai_get_lu")
+        return out
+
+    def checksum(self) -> np.ndarray:
+        """panel_check (panel_check.hpp:9-65): [sum |diag|, sum |strict upper|,
+        sum |strict lower|] of the context's matrix (the factors after factor())."""
+        out = np.empty(3, dtype=np.float64)
+        check(_checksum(self._h, _ptr(out)), "hplai_checksum")
         return out
 
     def rhs(self) -> np.ndarray:

@@ -172,6 +172,12 @@ int hplai_get_x(hplai_ctx *ctx, double *x);                      /* n doubles */
 int hplai_get_lu(hplai_ctx *ctx, float *a, int64_t lda);           /* n x n FP32 */
 int hplai_get_rhs(hplai_ctx *ctx, double *rhs);
 int hplai_get_diag(hplai_ctx *ctx, double *diag);
+/* panel_check (panel_check.hpp:9-65, `--checksum` at main.cpp:298-302):
+ * sigs[0..2] (host) = FP64 sums of |a_ij| over the diagonal, the strict
+ * upper and the strict lower triangle of the context's matrix -- the
+ * factors after hplai_factor.  Deterministic for a given matrix; agrees with
+ * the reference's sequential sums to rounding (the summation order differs). */
+int hplai_checksum(hplai_ctx *ctx, double *sigs);
 /* The per-step refinement log the reference prints (iterative_refinement.hpp:45):
  * up to `cap` entries; returns the number of steps through *count. */
 int hplai_get_ir_log(hplai_ctx *ctx, double *residual, double *harness, int cap, int *count);
@@ -339,6 +345,15 @@ size_t hplai_trsv_workspace(int n);
  * hplai_trsv_workspace(n) bytes and must be zeroed before its first use. */
 int hplai_trsv_lower(int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes, void *stream);
 int hplai_trsv_upper(int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes, void *stream);
+
+/* Workspace bytes for hplai_panel_check at order n (at most 28416). */
+size_t hplai_panel_check_workspace(int n);
+/* panel_check (panel_check.hpp:9-65) on caller buffers: sigs (device, 3
+ * doubles) = FP64 sums of |a_ij| over the diagonal, strict upper and strict
+ * lower triangle of a (n x n FP32, column-major, lda >= n).  `work` holds at
+ * least hplai_panel_check_workspace(n) bytes; no clearing needed. */
+int hplai_panel_check(int n, const float *a, int64_t lda, double *sigs, void *work, size_t work_bytes,
+	void *stream);
 
 /* colv_infnorm / calc_infnorm (panel_norm.hpp:8-41): *out = max_i |x_i|
  * written to device memory. */

@@ -18,6 +18,8 @@
  *                                                 panel_gemv.hpp:16-180, otf_gemv.cpp:5-131,
  *                                                 panel_trsv.hpp:115-285,310-758,
  *                                                 panel_norm.hpp:8-41,78-84
+ *   - the checksum of the factored matrix (`--checksum`)
+ *                                                 panel_check.hpp:9-65
  *
  * Arithmetic follows the reference's operation order, with every
  * `a = b*c + a` that the reference's x86 build (g++ -O2 -march=native, whose
@@ -565,4 +567,35 @@ ORC_EXPORT int orc_solve(int n, int b, int q, uint64_t seed, int maxit, double *
 	free(rhs);
 	free(d);
 	return rc;
+}
+
+/* panel_check (panel_check.hpp:9-65) on a 1x1 grid: FP64 sums of |a_ij| over
+ * the diagonal, the strict upper and the strict lower triangle of the
+ * factored matrix, in the reference's order -- block columns, block rows
+ * within them, then each b x b block column-major (diagonal blocks split at
+ * their own diagonal).  sigs = {diag, upper, lower}.                       */
+ORC_EXPORT void orc_panel_check(int n, int b, const float *a, int64_t lda, double *sigs)
+{
+	double sigd = 0.0, sigu = 0.0, sigl = 0.0;
+	const int nb = n / b;
+	for (int j = 0; j < nb; ++j)
+		for (int i = 0; i < nb; ++i) {
+			const float *blk = a + (int64_t)j * b * lda + (int64_t)i * b;
+			if (i == j) {
+				for (int jj = 0; jj < b; ++jj) {
+					for (int ii = 0; ii < jj; ++ii) sigu += fabs((double)blk[jj * lda + ii]);
+					sigd += fabs((double)blk[jj * lda + jj]);
+					for (int ii = jj + 1; ii < b; ++ii) sigl += fabs((double)blk[jj * lda + ii]);
+				}
+			} else if (i < j) {
+				for (int jj = 0; jj < b; ++jj)
+					for (int ii = 0; ii < b; ++ii) sigu += fabs((double)blk[jj * lda + ii]);
+			} else {
+				for (int jj = 0; jj < b; ++jj)
+					for (int ii = 0; ii < b; ++ii) sigl += fabs((double)blk[jj * lda + ii]);
+			}
+		}
+	sigs[0] = sigd;
+	sigs[1] = sigu;
+	sigs[2] = sigl;
 }

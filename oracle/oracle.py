@@ -59,6 +59,7 @@ _solve = _proto("orc_solve", _int, _int, _int, _int, _u64, _int, _vp, _vp, _vp, 
 _e4m3_rn = _proto("orc_e4m3_rn", ctypes.c_uint8, ctypes.c_float)
 _e4m3_to_f32 = _proto("orc_e4m3_to_f32", ctypes.c_float, ctypes.c_uint8)
 _quantize_e4m3 = _proto("orc_quantize_e4m3", None, _int, _int, _vp, _i64, _int, _vp, _i64, _vp)
+_panel_check = _proto("orc_panel_check", None, _int, _int, _vp, _i64, _vp)
 _f8gemm = _proto("orc_f8gemm_minus", None, _int, _int, _int, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _i64)
 
 
@@ -133,6 +134,18 @@ def lu(a: np.ndarray, b: int) -> np.ndarray:
     if rc:
         raise ValueError(f"orc_lu: {rc}")
     return a
+
+
+def panel_check(lu_f32: np.ndarray, b: int) -> np.ndarray:
+    """panel_check (panel_check.hpp:9-65): [sum |diag|, sum |strict upper|,
+    sum |strict lower|] of the factored matrix, in the reference's order."""
+    a = np.asfortranarray(lu_f32, dtype=np.float32)
+    n = a.shape[0]
+    if n % b:
+        raise ValueError("panel_check: n % b != 0")
+    sigs = np.zeros(3, dtype=np.float64)
+    _panel_check(n, b, _p(a), n, _p(sigs))
+    return sigs
 
 
 def otf_gemv(n, b, alpha, x, y, seed, d, q=1) -> np.ndarray:

@@ -47,3 +47,8 @@ def test_invalid_arguments_rejected_without_gpu(hplai):
     assert e.value.status == hplai.HPLAI_EINVAL
     assert hplai.fill_panel(0, 0, 0, 1, 1, None, 1, 42, 0, None) == hplai.HPLAI_EINVAL
     assert hplai.getrf_nopiv(2048, None, 2048, None) == hplai.HPLAI_EINVAL
+    # panel_check: lda < n, missing output, and work smaller than its workspace
+    assert hplai.panel_check_workspace(1 << 20) == 3 * 8 * 1184
+    assert hplai.panel_check(100, 16, 99, 16, 16, 1 << 20, None) == hplai.HPLAI_EINVAL
+    assert hplai.panel_check(100, 16, 100, None, 16, 1 << 20, None) == hplai.HPLAI_EINVAL
+    assert hplai.panel_check(100, 16, 100, 16, 16, hplai.panel_check_workspace(100) - 1, None) == hplai.HPLAI_EINVAL

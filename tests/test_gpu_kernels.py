@@ -288,3 +288,27 @@ def test_infnorm(hplai, torch_cuda):
     hplai.check(hplai.infnorm(v.numel(), v.data_ptr(), out.data_ptr(), None))
     torch.cuda.synchronize()
     assert np.isnan(out.item())
+
+
+@pytest.mark.parametrize("n,lda,off", [(4096, 4096, 0), (1030, 1032, 0), (1001, 1003, 0), (130, 132, 1), (5, 8, 0)])
+def test_panel_check_leaf(hplai, torch_cuda, n, lda, off):
+    """hplai_panel_check (panel_check.hpp:9-65) vs FP64 sums of |a_ij| over the
+    diagonal and the strict triangles, 1e-13 relative (summation order only):
+    float4 path with and without a row tail, lda not a multiple of 4, and a
+    pointer off the 16-byte boundary (scalar path)."""
+    torch = torch_cuda
+    g = torch.Generator(device="cpu").manual_seed(n)
+    buf = torch.rand(lda * n + off, generator=g, dtype=torch.float32) - 0.5
+    dev = buf.cuda()
+    ws = hplai.panel_check_workspace(n)
+    work = torch.empty(ws // 8 + 1, dtype=torch.float64, device="cuda")
+    sig = torch.empty(3, dtype=torch.float64, device="cuda")
+    hplai.check(hplai.panel_check(n, dev.data_ptr() + 4 * off, lda, sig.data_ptr(), work.data_ptr(), ws, None),
+                "hplai_panel_check")
+    got = sig.cpu().numpy()
+    # column-major: element (i, j) sits at j * lda + i
+    a = np.abs(buf[off:].numpy().reshape(n, lda)[:, :n].astype(np.float64)).T
+    want = np.array([np.trace(a), np.triu(a, 1).sum(), np.tril(a, -1).sum()])
+    assert np.all(np.abs(got - want) <= 1e-13 * want)
+    hplai.check(hplai.panel_check(0, None, 0, sig.data_ptr(), None, 0, None), "hplai_panel_check")
+    assert np.array_equal(sig.cpu().numpy(), np.zeros(3))

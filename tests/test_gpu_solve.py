@@ -174,3 +174,30 @@ def test_autotune_picks_a_schedule_and_solves(hplai, oracle, torch_cuda):
     a = oracle.dense_matrix_f64(n, 42)
     xs = np.linalg.solve(a, oracle.rhs(n, 42))
     assert np.max(np.abs(x - xs)) / np.max(np.abs(xs)) < 1e-12
+
+
+def test_checksum_after_lu_matches_oracle_and_driver(hplai, oracle, torch_cuda):
+    """`--checksum` (panel_check.hpp:9-65, main.cpp:298-302) at n=1200, b=60:
+    hplai_checksum over the factors equals the oracle's sums in the
+    reference's block order to 1e-13 relative, repeats bit for bit, and
+    driver.out prints the same three numbers on its `check` line."""
+    import re
+    import subprocess
+    n, b = 1200, 60
+    with hplai.Solver(n, b) as s:
+        s.generate(42)
+        s.factor()
+        c1 = s.checksum()
+        c2 = s.checksum()
+        lu = s.lu()
+    assert np.array_equal(c1, c2)
+    want = oracle.panel_check(lu, b)
+    assert np.all(np.abs(c1 - want) <= 1e-13 * want)
+    exe = os.path.join(HERE, "..", "hpl-ai_b200", "driver.out")
+    out = subprocess.run([exe, str(n), str(b), "1", "--checksum"], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    m = re.search(r"^check (\S+) (\S+), (\S+)$", out.stdout, re.M)
+    assert m, out.stdout
+    got = np.array([float(v) for v in m.groups()])
+    assert np.all(np.abs(got - c1) <= 1e-15 * c1)
+    assert re.search(r"GFlop/s resid = .* hpl-harness = ", out.stdout), out.stdout

@@ -195,3 +195,17 @@ def test_quantize_e4m3_block_factors(oracle):
         amax = np.abs(x[blk * 128:(blk + 1) * 128]).max() / s[blk]
         assert 224.0 <= amax < 448.0
         assert np.log2(s[blk]) == int(np.log2(s[blk]))
+
+
+def test_panel_check_restatement_matches_triangle_sums(oracle):
+    """panel_check (panel_check.hpp:9-65) in the reference's block order agrees
+    with order-free FP64 sums of the diagonal and the strict triangles of the
+    factored matrix (to 1e-13: only the summation order differs), and the
+    block size changes only the order."""
+    n, b = 360, 60
+    lu = oracle.lu(oracle.matrix(n), b)
+    s = oracle.panel_check(lu, b)
+    a = np.abs(lu.astype(np.float64))
+    want = np.array([np.trace(a), np.triu(a, 1).sum(), np.tril(a, -1).sum()])
+    assert np.all(np.abs(s - want) <= 1e-13 * want)
+    assert np.all(np.abs(oracle.panel_check(lu, 120) - s) <= 1e-13 * s)
