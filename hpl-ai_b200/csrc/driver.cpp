@@ -20,6 +20,55 @@
 #include <cstring>
 #include <ctime>
 #include <vector>
+#include <unistd.h>
+
+// Timer::show / Timer::dump_mp (timer.hpp:174-218) as main.cpp:470-478 calls
+// them on one process: the file Timerdump.<job>.<n>.<b>.<size>.<rank> in the
+// working directory, one line per timer item (seconds, share of TOTAL,
+// accumulated operation count, Gop/s) and the GEMM rate.  Items of the
+// distributed reference that have no work on one GPU (broadcasts, tests,
+// waits, separate down-casts, write-back, communication) read 0; MISC is
+// TOTAL minus the other items, as in the reference.
+static void write_timerdump(int jobid, int n, int b, double total_s, const double *ms, long long matvecs)
+{
+	enum { DIAG_LU = 5, TRSM_L = 6, TRSM_R = 7, GEMM_UPDATE = 10, GEMM_PROGRESS = 11, IR_GEMV = 14, IR_TRSV = 16,
+		TOTAL = 19, MISC = 20, NUM_ITEMS = 21 };
+	static const char *names[NUM_ITEMS] = {"DIAG_BCAST", "LCOL_BCAST", "RROW_BCAST", "TEST", "WAIT", "DIAG_LU",
+		"TRSM_L", "TRSM_R", "CONV_L", "CONV_R", "GEMM_UPDATE", "GEMM_PROGRESS", "LAZY_INIT", "WRITE_BACK", "IR_GEMV",
+		"IR_GEMV_COMM", "IR_TRSV", "IR_TRSV_MV", "IR_TRSV_COMM", "TOTAL", "MISC"};
+	double t[NUM_ITEMS] = {};
+	long long acc[NUM_ITEMS] = {};
+	const long long nb = n / b, bb = b;
+	t[DIAG_LU] = 1e-3 * ms[HPLAI_PH_DIAG_LU];
+	t[TRSM_L] = 1e-3 * ms[HPLAI_PH_TRSM_L];
+	t[TRSM_R] = 1e-3 * ms[HPLAI_PH_TRSM_R];
+	t[GEMM_UPDATE] = 1e-3 * ms[HPLAI_PH_GEMM_UPDATE];
+	t[IR_GEMV] = 1e-3 * ms[HPLAI_PH_IR_GEMV];
+	t[IR_TRSV] = 1e-3 * ms[HPLAI_PH_IR_TRSV];
+	t[TOTAL] = total_s;
+	// operation counts the reference accumulates per item, summed over the
+	// n/b steps (panel_trf.hpp:156,170,457; schur_updator.hpp:394; panel_gemv.hpp:156)
+	acc[DIAG_LU] = nb * (bb * (bb * (4 * bb - 3) + 5) / 6);
+	acc[TRSM_L] = bb * bb * bb * (nb * (nb - 1) / 2);
+	acc[TRSM_R] = acc[TRSM_L];
+	acc[GEMM_UPDATE] = 2 * bb * bb * bb * ((nb - 1) * nb * (2 * nb - 1) / 6);
+	acc[IR_GEMV] = 2LL * n * n * matvecs;
+	t[MISC] = t[TOTAL];
+	for (int i = 0; i < NUM_ITEMS - 2; ++i) t[MISC] -= t[i];
+	char fname[128];
+	std::snprintf(fname, sizeof fname, "Timerdump.%06d.%09d.%04d.%05d.%05d", jobid, n, b, 1, 0);
+	FILE *fp = std::fopen(fname, "w");
+	if (!fp) return;
+	char host[256] = "";
+	gethostname(host, sizeof host - 1);
+	std::fprintf(fp, "# row=%d, col=%d, host=%s\n", 0, 0, host);
+	for (int i = 0; i < NUM_ITEMS; ++i)
+		std::fprintf(fp, " %-12s : %e sec : %6.2f %% : %20lld : %e Gop/s\n", names[i], t[i], 100.0 * t[i] / t[TOTAL],
+			acc[i], 1e-9 * static_cast<double>(acc[i]) / t[i]);
+	const double flops = static_cast<double>(acc[GEMM_UPDATE] + acc[GEMM_PROGRESS]) / (t[GEMM_UPDATE] + t[GEMM_PROGRESS]);
+	std::fprintf(fp, "GEMM_TOTAL: %f Tflops\n", 1.e-12 * flops);
+	std::fclose(fp);
+}
 
 static void print_ctime(const char *msg)
 {
@@ -45,9 +94,10 @@ static int usage()
 		"   --gmres                 GMRES refinement instead of the classical correction.\n"
 		"   --lookahead             Factor the next panel while the trailing update runs.\n"
 		"   --checksum              Print sums of |diag|, |upper|, |lower| of the factors after the LU.\n"
+		"   --job-id <id>           Job number in the name of the Timerdump file (default 0).\n"
 		"   --help or -h            Print this message.\n"
 		"Layout and transport flags of the distributed reference (-not, -r, -m, -w, --pack,\n"
-		"--numa, --numa-map, --nbuf, --job-id, --l1est, --highammat, --pwrtune)\n"
+		"--numa, --numa-map, --nbuf, --l1est, --highammat, --pwrtune)\n"
 		"are accepted and ignored.\n");
 	return 0;
 }
@@ -59,6 +109,7 @@ int main(int argc, char **argv)
 	int precision = HPLAI_F32_F16, mode = HPLAI_IR;
 	unsigned flags = 0;
 	bool checksum = false;
+	int jobid = 0;
 	if (argc > 1) n = std::atoi(argv[1]);
 	if (argc > 2) b = std::atoi(argv[2]);
 	for (int i = 4; i < argc; ++i) {
@@ -73,7 +124,8 @@ int main(int argc, char **argv)
 		else if (!std::strcmp(argv[i], "--lookahead")) flags |= HPLAI_FLAG_LOOKAHEAD;
 		else if (!std::strcmp(argv[i], "--checksum")) checksum = true;
 		else if (!std::strcmp(argv[i], "--numa") || !std::strcmp(argv[i], "--numa-map") ||
-			!std::strcmp(argv[i], "--nbuf") || !std::strcmp(argv[i], "--job-id")) ++i;
+			!std::strcmp(argv[i], "--nbuf")) ++i;
+		else if (!std::strcmp(argv[i], "--job-id") && i + 1 < argc) jobid = std::atoi(argv[++i]);
 		else if (argv[i][0] == '-') std::printf("Ignoring option not applicable on one GPU: %s\n", argv[i]);
 		else std::printf("Ignoring unknown option: %s\n", argv[i]);
 	}
@@ -151,6 +203,9 @@ int main(int argc, char **argv)
 		ms[HPLAI_PH_DIAG_LU], ms[HPLAI_PH_TRSM_L], ms[HPLAI_PH_TRSM_R], ms[HPLAI_PH_GEMM_UPDATE], ms[HPLAI_PH_IR_GEMV],
 		ms[HPLAI_PH_IR_TRSV]);
 	std::fflush(stdout);
+	int outer = 0, inner = 0;
+	hplai_get_refine_counts(ctx, &outer, &inner);
+	write_timerdump(jobid, n, b, secs, ms, static_cast<long long>(outer) + inner);
 	hplai_destroy(ctx);
 	if (rr != HPLAI_OK && rr != HPLAI_ENOTCONV) {
 		std::fprintf(stderr, "hplai_refine: %s\n", hplai_status_string(rr));

@@ -176,11 +176,14 @@ def test_autotune_picks_a_schedule_and_solves(hplai, oracle, torch_cuda):
     assert np.max(np.abs(x - xs)) / np.max(np.abs(xs)) < 1e-12
 
 
-def test_checksum_after_lu_matches_oracle_and_driver(hplai, oracle, torch_cuda):
+def test_checksum_after_lu_matches_oracle_and_driver(hplai, oracle, torch_cuda, tmp_path):
     """`--checksum` (panel_check.hpp:9-65, main.cpp:298-302) at n=1200, b=60:
     hplai_checksum over the factors equals the oracle's sums in the
     reference's block order to 1e-13 relative, repeats bit for bit, and
-    driver.out prints the same three numbers on its `check` line."""
+    driver.out prints the same three numbers on its `check` line.  The driver
+    also writes the reference's Timerdump file (timer.hpp:174-218,
+    main.cpp:470-478): 21 timer items, TOTAL at 100 %, the reference's
+    operation counts, and the GEMM rate line."""
     import re
     import subprocess
     n, b = 1200, 60
@@ -193,11 +196,26 @@ def test_checksum_after_lu_matches_oracle_and_driver(hplai, oracle, torch_cuda):
     assert np.array_equal(c1, c2)
     want = oracle.panel_check(lu, b)
     assert np.all(np.abs(c1 - want) <= 1e-13 * want)
-    exe = os.path.join(HERE, "..", "hpl-ai_b200", "driver.out")
-    out = subprocess.run([exe, str(n), str(b), "1", "--checksum"], capture_output=True, text=True, timeout=300)
+    exe = os.path.abspath(os.path.join(HERE, "..", "hpl-ai_b200", "driver.out"))
+    out = subprocess.run([exe, str(n), str(b), "1", "--checksum", "--job-id", "7"], capture_output=True, text=True,
+                         timeout=300, cwd=tmp_path)
     assert out.returncode == 0, out.stderr
     m = re.search(r"^check (\S+) (\S+), (\S+)$", out.stdout, re.M)
     assert m, out.stdout
     got = np.array([float(v) for v in m.groups()])
     assert np.all(np.abs(got - c1) <= 1e-15 * c1)
     assert re.search(r"GFlop/s resid = .* hpl-harness = ", out.stdout), out.stdout
+    dump = (tmp_path / "Timerdump.000007.000001200.0060.00001.00000").read_text().splitlines()
+    assert dump[0].startswith("# row=0, col=0, host=")
+    items = {}
+    for line in dump[1:22]:
+        name, sec, pct, acc, _ = [f.strip() for f in line.split(":")]
+        items[name] = (float(sec.split()[0]), float(pct.split()[0]), int(acc))
+    assert len(items) == 21 and items["TOTAL"][1] == 100.0
+    nb = n // b
+    assert items["GEMM_UPDATE"][2] == 2 * b ** 3 * sum(k * k for k in range(nb))
+    assert items["DIAG_LU"][2] == nb * (b * (b * (4 * b - 3) + 5) // 6)
+    assert items["TRSM_L"][2] == items["TRSM_R"][2] == b ** 3 * nb * (nb - 1) // 2
+    assert items["IR_GEMV"][2] > 0 and items["IR_GEMV"][2] % (2 * n * n) == 0
+    assert items["GEMM_UPDATE"][0] > 0 and items["DIAG_BCAST"][0] == 0.0
+    assert re.match(r"GEMM_TOTAL: \S+ Tflops$", dump[22])
