@@ -256,3 +256,19 @@ def test_deck_minus_rejects_bad_layouts(hplai):
     assert hplai.shgemm_deck_minus(64, 64, 64, 16, 64, 16, 64, 16, 68, 1.0, None) == hplai.HPLAI_EINVAL  # ldd % 8
     assert hplai.shgemm_deck_minus(60, 64, 64, 16, 64, 16, 64, 16, 64, 1.0, None) == hplai.HPLAI_EINVAL  # m % 8
     assert hplai.f8gemm_deck_minus(64, 64, 128, 16, 128, 16, 16, 128, 16, 24, 64, 1.0, None) == hplai.HPLAI_EINVAL
+
+
+@pytest.mark.parametrize("precision,flags,n,b", [(0, 4, 2048, 256), (1, 0, 4096, 512), (1, 4, 4096, 512)])
+def test_checksum_over_factors_of_every_form(hplai, oracle, torch_cuda, precision, flags, n, b):
+    """hplai_checksum (panel_check.hpp:9-65) reads the FP32 factors the
+    refinement uses in the FP16-deck and e4m3 forms too: it equals the
+    oracle's sums in the reference's block order over hplai_get_lu's copy,
+    to 1e-13 relative."""
+    assert flags in (0, hplai.FLAG_FP16_DECK)
+    with hplai.Solver(n, b, precision=precision, flags=flags) as s:
+        s.generate(42)
+        s.factor()
+        got = s.checksum()
+        lu = s.lu()
+    want = oracle.panel_check(lu, b)
+    assert np.all(np.abs(got - want) <= 1e-13 * want)
