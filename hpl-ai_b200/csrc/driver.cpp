@@ -176,8 +176,12 @@ int main(int argc, char **argv)
 	if (rc == HPLAI_OK && checksum) {
 		// inside the timed region, between the LU and the refinement (main.cpp:298-302)
 		double sigs[3];
-		rc = hplai_checksum(ctx, sigs);
-		if (rc == HPLAI_OK) std::printf("check %22.17e %22.17e, %22.17e\n", sigs[0], sigs[1], sigs[2]);
+		const int rs = hplai_checksum(ctx, sigs);
+		if (rs != HPLAI_OK) {
+			std::fprintf(stderr, "hplai_checksum: %s\n", hplai_status_string(rs));
+			return 1;
+		}
+		std::printf("check %22.17e %22.17e, %22.17e\n", sigs[0], sigs[1], sigs[2]);
 		std::fflush(stdout);
 	}
 	int rr = HPLAI_OK;
