@@ -2,12 +2,21 @@
 """HPL-AI GFLOP/s of the single-GPU B200 solver (one JSON line on rank 0).
 
 One step = one solve of the HPL-AI system on the GPU: the blocked no-pivot
-LU (FP32 panels, FP16 tcgen05 Schur update) followed by FP64 iterative
-refinement to hpl-harness < 16 -- the reference's timed region
-(main.cpp:283-441).  The matrix is regenerated on the device before every
-step, outside the timed window, as the reference generates it before its
-timer starts (the LU overwrites A).  Work per step: 2/3 n^3 + 3/2 n^2 flops
-(main.cpp:441).
+LU followed by FP64 refinement to hpl-harness < 16 -- the reference's timed
+region (main.cpp:283-441).  The matrix is regenerated on the device before
+every step, outside the timed window, as the reference generates it before
+its timer starts (the LU overwrites A).  Work per step: 2/3 n^3 + 3/2 n^2
+flops (main.cpp:441).
+
+By default the workload is n = 131072, b = 1024 in two forms, timed back to
+back on the same GPU:
+  * the precision form (the headline `value`): e4m3 Schur update with
+    per-128 power-of-two factors and FP32 accumulation into the FP16
+    trailing-update deck, FP32 panels, FP64 GMRES-IR;
+  * the plain form (`plain`): FP16 Schur update with FP32 accumulation into
+    the FP32 trailing matrix, FP32 panels, FP64 iterative refinement;
+and `speedup_vs_plain` is the plain form's time per solve over the
+precision form's.  `--n 65536 --b 512` gives the smaller plain-scale case.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -34,9 +43,9 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 METRIC = "HPL-AI GFLOP/s to hpl-harness<16: FP8-Schur+GMRES-IR vs plain; % tensor peak"
 UNIT = "GFLOP/s"
-DEFAULT_N, DEFAULT_B = 65536, 512
+DEFAULT_N, DEFAULT_B = 131072, 1024   # the precision-vs-plain configuration (C3)
 ADJOINT_N, ADJOINT_B = 8192, 256
-CPU_SAMPLE = (2400, 120)           # bounded CPU sample of the same workload
+CPU_SAMPLE = (4800, 120)           # bounded CPU sample of the same workload (seconds per solve)
 
 
 def hpl_flops(n):
@@ -133,21 +142,29 @@ def batch_seeds(rank, count):
     return [rank * count + s for s in range(count)]
 
 
+REF_FLAGS = ["-not", "-d", "-r"]   # the reference command of the north star: mpirun -n 4 driver.out n b 2 -not -d -r
+
+
 def cpu_solve_gflops(n, b, threads):
-    """One CPU solve of the sample: the reference build if present, else the oracle."""
+    """One CPU solve of the sample by the reference's own driver (built from
+    its sources by oracle/build_ref.sh: 4 ranks as threads of one process, a
+    2 x 2 grid, threads // 4 OpenMP threads each, OpenBLAS single-threaded
+    per rank), timed by the driver itself (LU + refinement, main.cpp:283-452);
+    the oracle restatement when that build is absent."""
     ref_bin = os.path.join(ROOT, "oracle", "_ref", "ref_driver.out")
     if os.path.exists(ref_bin):
-        env = dict(os.environ, OMP_NUM_THREADS=str(max(1, threads // 4)), TMPI_NP="4")
-        t0 = time.perf_counter()
-        out = subprocess.run([ref_bin, str(n), str(b), "2", "-not", "-r"], capture_output=True, text=True, env=env,
+        per_rank = max(1, threads // 4)
+        env = dict(os.environ, OMP_NUM_THREADS=str(per_rank), OPENBLAS_NUM_THREADS="1", TMPI_NP="4")
+        out = subprocess.run([ref_bin, str(n), str(b), "2"] + REF_FLAGS, capture_output=True, text=True, env=env,
                              timeout=600)
-        wall = time.perf_counter() - t0
         for ln in out.stdout.splitlines():
             if "GFlop/s" in ln and "sec." in ln:
                 f = ln.split()
                 secs, harness = float(f[0]), float(f[-1])
-                return hpl_flops(n) / secs / 1e9, secs, harness, "reference", threads
-        raise RuntimeError(f"reference build printed no report line ({wall:.1f}s): {out.stdout[-400:]}")
+                if not harness < 16:
+                    raise RuntimeError(f"reference solve did not reach hpl-harness < 16: {ln}")
+                return hpl_flops(n) / secs / 1e9, secs, harness, "reference", 4 * per_rank
+        raise RuntimeError(f"reference build printed no report line (rc {out.returncode}): {out.stdout[-400:]}")
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     import oracle
     t0 = time.perf_counter()
@@ -156,6 +173,14 @@ def cpu_solve_gflops(n, b, threads):
     if rc != 0:
         raise RuntimeError("oracle solve did not converge")
     return hpl_flops(n) / secs / 1e9, secs, har, "port", threads
+
+
+def cpu_sample_note(kind, cores, n, b):
+    if kind == "reference":
+        return (f"the reference's driver.out {n} {b} 2 {' '.join(REF_FLAGS)} built from its sources "
+                f"(oracle/build_ref.sh; 4 ranks as threads, {cores // 4} OpenMP threads each, OpenBLAS 0.3.15 "
+                f"single-threaded per rank), its own LU + IR timer")
+    return f"the oracle's CPU restatement, full solve (LU + IR) at n={n} b={b}"
 
 
 def run_reference(args):
@@ -171,16 +196,19 @@ def run_reference(args):
         g, s, har, kind, cores = cpu_solve_gflops(n, b, threads)
         vals.append(g)
         secs.append(s)
+    sample = cpu_sample_note(kind, cores, n, b)
     value = len(vals) * hpl_flops(n) / sum(secs) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp16/fp32/fp64",
         "data": "synthetic (the reference's own LCG matrix, seed 42)",
-        "config": {"workload": f"HPL-AI plain solve, bounded CPU sample n={n} b={b} of the n={args.n} b={args.b} "
-                               f"workload", "n": n, "b": b},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                         "sample": f"full solve (LU + IR) at n={n} b={b}, {args.steps} steps"},
+        "config": {"workload": f"HPL-AI solve, bounded CPU sample n={n} b={b} of the n={args.n} b={args.b} "
+                               f"workload", "n": n, "b": b,
+                   "command": f"driver.out {n} {b} 2 {' '.join(REF_FLAGS)}" if kind == "reference" else None},
+        "hpl_harness": har,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{sample}; {args.steps} steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -221,6 +249,190 @@ def schur_traffic_per_launch(n, b):
     return per_elem * elems / launches
 
 
+FORMS = {
+    # the precision form: e4m3 Schur update (per-128 power-of-two factors, FP32
+    # accumulation) into the FP16 trailing-update deck, FP64 GMRES-IR
+    "precision": {"precision": "f8", "deck": True, "refine": "gmres",
+                  "label": "precision: e4m3 Schur into the FP16 deck + FP64 GMRES-IR(30)"},
+    # the plain form: FP16 Schur update with FP32 accumulation into the FP32
+    # trailing matrix, FP64 iterative refinement (the reference's no -d form)
+    "plain": {"precision": "f16", "deck": False, "refine": "ir",
+              "label": "plain: FP16 Schur into the FP32 trailing matrix + FP64 IR"},
+}
+
+
+def schur_roofline(hplai, n, b, fp8, deck, gemm_ms):
+    """Roofline of the Schur GEMM over one factorisation: algorithmic flops
+    and bytes per launch (schur_algorithmic) over the average launch time
+    (CUDA events around each launch on its stream, summed by the library)."""
+    hbm, tc_burst, tc_sus, peak_kind = load_peaks()
+    peak_note = f"{peak_kind} (MEASURED_PEAKS.json: hbm_gbs, bf16_tflops_sustained)"
+    if fp8:
+        e4 = load_e4m3_peak()
+        if e4:
+            tc_sus = e4["sustained_tflops"]
+            peak_note = f"measured e4m3 dense (cuBLAS e4m3 8192^3 back to back, {e4['source']})"
+        else:
+            tc_sus *= 2.0
+            peak_note += " x 2 for e4m3 (nominal e4m3:bf16 ratio; no measured e4m3 peak)"
+    sflops, sbytes, slaunch = schur_algorithmic(n, b, 1 if fp8 else 2, 4 if deck else 8)
+    avg_launch_s = gemm_ms * 1e-3 / slaunch
+    ach_gbs = sbytes / slaunch / avg_launch_s / 1e9
+    ach_tf = sflops / slaunch / avg_launch_s / 1e12
+    ridge = tc_sus * 1e12 / (hbm * 1e9)
+    intensity = sflops / sbytes
+    bound = "tensor" if intensity >= ridge else "hbm"
+    if bound == "hbm":
+        roof = {"bound": "hbm", "achieved": ach_gbs, "peak": hbm, "unit": "GB/s", "frac": ach_gbs / hbm}
+    else:
+        roof = {"bound": "tensor", "achieved": ach_tf, "peak": tc_sus, "unit": "TFLOP/s", "frac": ach_tf / tc_sus}
+    cdesc = "FP16 deck, deck -= s*L*U" if deck else "FP32 C, C -= L*U"
+    kname = f"schur_kernel (tcgen05 {'e4m3 x e4m3' if fp8 else 'FP16 x FP16'} -> FP32 accumulator; {cdesc})"
+    traffic = schur_traffic_per_launch(n, b) if (not fp8 and not deck) else None
+    roof.update({"traffic": traffic, "kernel": kname,
+                 "launches_per_step": slaunch, "avg_launch_ms": avg_launch_s * 1e3,
+                 "algorithmic_bytes_per_launch": sbytes / slaunch, "algorithmic_flops_per_launch": sflops / slaunch,
+                 "algorithmic_bytes_note": ("per C element 4 B (FP16 deck read + write)" if deck else
+                                            "per C element 8 B (FP32 read + write)") +
+                 f" + panels {1 if fp8 else 2} B per element",
+                 "intensity_flop_per_byte": intensity, "ridge_flop_per_byte": ridge,
+                 "tensor_achieved_tflops": ach_tf, "tensor_peak_tflops": tc_sus,
+                 "tensor_frac": ach_tf / tc_sus, "hbm_achieved_gbs": ach_gbs, "hbm_frac": ach_gbs / hbm,
+                 "peak_source": peak_note})
+    return roof
+
+
+def load_e4m3_peak():
+    """Measured dense e4m3 rate of this GPU type (bench.py --workload peak),
+    committed as a figure under profiles/."""
+    p = os.path.join(ROOT, "profiles", "tensor_peaks_cublas_8192.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    e4 = d.get("e4m3")
+    if not e4:
+        return None
+    return {"sustained_tflops": e4["sustained_tflops"], "burst_tflops": e4["burst_tflops"],
+            "source": "profiles/tensor_peaks_cublas_8192.json"}
+
+
+class FormRun:
+    """One solver form timed over `steps` solves (factor + refinement to
+    hpl-harness < 16) after `warmup` untimed ones, the matrix regenerated on
+    the device before each solve outside the timed window."""
+
+    def __init__(self, hplai, torch, form, n, b, seed, maxit, autotune, lookahead, barrier):
+        self.hplai, self.torch, self.form = hplai, torch, form
+        self.n, self.b, self.seed, self.maxit = n, b, seed, maxit
+        self.fp8 = form["precision"] == "f8"
+        self.deck = form["deck"]
+        self.mode = hplai.GMRES if form["refine"] == "gmres" else hplai.IR
+        flags = hplai.FLAG_LOOKAHEAD if lookahead else 0
+        if self.deck:
+            flags |= hplai.FLAG_FP16_DECK
+        self.s = hplai.Solver(n, b, precision=hplai.F32_F8 if self.fp8 else hplai.F32_F16, flags=flags)
+        self.ext = torch.cuda.ExternalStream(self.s.stream())
+        self.barrier = barrier
+        self.tuned = None
+        self.schedule = {"lookahead": bool(lookahead), "side_sms": None, "source": "flag" if lookahead else "serial"}
+        if autotune:
+            # outside the timed region: time the factorisation under each schedule, keep the fastest
+            tflags, tside, tms = self.s.autotune(seed)
+            la = bool(tflags & hplai.FLAG_LOOKAHEAD)
+            self.tuned = {"lookahead": la, "side_sms": tside, "factor_ms": tms}
+            self.schedule = {"lookahead": la, "side_sms": tside if la else None, "source": "hplai_autotune"}
+        self.results = []
+
+    def step(self, timed):
+        s, torch = self.s, self.torch
+        s.generate(self.seed)
+        self.barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(self.ext)
+        s.factor()
+        r = s.iterative_refinement(self.maxit, mode=self.mode)
+        ev1.record(self.ext)
+        ev1.synchronize()
+        self.barrier()
+        if r.status != self.hplai.HPLAI_OK:
+            raise RuntimeError(f"solve did not converge: {r}")
+        if timed:
+            self.results.append((ev0.elapsed_time(ev1), r, s.phase_ms(), s.refine_counts()))
+
+    def run(self, steps, warmup):
+        for _ in range(warmup):
+            self.step(False)
+        for _ in range(steps):
+            self.step(True)
+        return self
+
+    def summary(self, world):
+        hplai = self.hplai
+        total_ms = sum(r[0] for r in self.results)
+        steps = len(self.results)
+        value, max_ms = replica_value(total_ms, steps * hpl_flops(self.n), world, device="cuda")
+        phases = {k: statistics.mean(r[2][k] for r in self.results) for k in self.results[0][2]}
+        roof = schur_roofline(hplai, self.n, self.b, self.fp8, self.deck, phases["GEMM_UPDATE"])
+        last = self.results[-1]
+        return {
+            "form": self.form["label"], "value": value, "unit": UNIT, "steps": steps,
+            "ms_per_step": max_ms / steps, "ms_min": min(r[0] for r in self.results),
+            "ms_max": max(r[0] for r in self.results),
+            "schedule": self.schedule, "autotuned": self.tuned,
+            "trailing_matrix": "FP16 deck (updates rounded to FP16 once per step, folded in per panel)"
+            if self.deck else "FP32",
+            "hpl_harness": last[1].hpl_harness, "resid": last[1].residual,
+            "residual_evaluations": last[1].iters,
+            "gmres_inner_steps": last[3][1] if self.mode == hplai.GMRES else None,
+            "phases_ms": phases, "roofline": roof,
+        }
+
+    def close(self):
+        self.s.close()
+
+
+def e2e_run(hplai, torch, fr, steps, warmup, world, barrier):
+    """The same solve through the public C API with host buffers: pinned FP32
+    A, FP64 rhs and diagonal copied in, x copied out, every step
+    (hplai_solve_host)."""
+    s, n, seed = fr.s, fr.n, fr.seed
+    s.generate(seed)
+    torch.cuda.synchronize()
+    try:
+        a_h = torch.empty(n * n, dtype=torch.float32, pin_memory=True)
+        pinned = True
+    except RuntimeError:
+        a_h = torch.empty(n * n, dtype=torch.float32)
+        pinned = False
+    hplai.check(hplai._get_lu(s._h, a_h.data_ptr(), n), "hplai_get_lu")
+    rhs_h = torch.from_numpy(s.rhs())
+    d_h = torch.from_numpy(s.diag())
+    if pinned:
+        rhs_h, d_h = rhs_h.pin_memory(), d_h.pin_memory()
+    x_h = torch.empty(n, dtype=torch.float64, pin_memory=pinned)
+    ets = []
+    for i in range(warmup + steps):
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(fr.ext)
+        r = s.solve_host_ptrs(a_h.data_ptr(), n, rhs_h.data_ptr(), d_h.data_ptr(), seed, fr.maxit, x_h.data_ptr())
+        ev1.record(fr.ext)
+        ev1.synchronize()
+        barrier()
+        if r.status != hplai.HPLAI_OK:
+            raise RuntimeError(f"e2e solve did not converge: {r}")
+        if i >= warmup:
+            ets.append(ev0.elapsed_time(ev1))
+    del a_h
+    te = torch.tensor([sum(ets)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    return {"value": world * len(ets) * hpl_flops(n) / (float(te.item()) * 1e-3) / 1e9, "unit": UNIT,
+            "h2d_bytes_per_step": n * n * 4 + 2 * n * 8, "d2h_bytes_per_step": n * 8,
+            "host_memory": "pinned" if pinned else "pageable", "ms_per_step": float(te.item()) / len(ets),
+            "steps": len(ets), "warmup": warmup, "call": "hplai_solve_host (" + fr.form["label"] + ")"}
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_setup()
@@ -236,161 +448,88 @@ def run_ours(args):
 
     n, b, seed, maxit = args.n, args.b, 42, 50
     dev = torch.cuda.current_device()
-    prec = hplai.F32_F8 if args.precision == "f8" else hplai.F32_F16
-    refine = args.refine or ("gmres" if args.precision == "f8" else "ir")
-    mode = hplai.GMRES if refine == "gmres" else hplai.IR
-    form = ("precision (F32_F8 e4m3 Schur" if prec == hplai.F32_F8 else "plain (F32_F16") + \
-        (" + GMRES-IR)" if mode == hplai.GMRES else " + IR)")
 
     def barrier():
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
 
-    flags = hplai.FLAG_LOOKAHEAD if args.lookahead else 0
-    deck = args.deck == "on"
-    if deck:
-        flags |= hplai.FLAG_FP16_DECK
-    s = hplai.Solver(n, b, precision=prec, flags=flags)
-    ext = torch.cuda.ExternalStream(s.stream())
-    results = []
-    tuned = None
-    if args.autotune:
-        # outside the timed region: time the factorisation under each schedule, keep the fastest
-        tflags, tside, tms = s.autotune(seed)
-        tuned = {"lookahead": bool(tflags & hplai.FLAG_LOOKAHEAD), "side_sms": tside, "factor_ms": tms}
+    if args.forms == "both":
+        head_key, other_key = "precision", "plain"
+    else:
+        head_key, other_key = args.forms, None
+    head_form = dict(FORMS[head_key])
+    if args.precision:
+        head_form["precision"] = args.precision
+    if args.deck:
+        head_form["deck"] = args.deck == "on"
+    if args.refine:
+        head_form["refine"] = args.refine
+    if head_form != FORMS[head_key]:
+        head_form["label"] = (f"{'e4m3' if head_form['precision'] == 'f8' else 'FP16'} Schur into the "
+                              f"{'FP16 deck' if head_form['deck'] else 'FP32 trailing matrix'} + FP64 "
+                              f"{'GMRES-IR' if head_form['refine'] == 'gmres' else 'IR'}")
 
-    def one_step(timed):
-        s.generate(seed)
-        barrier()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(ext)
-        s.factor()
-        r = s.iterative_refinement(maxit, mode=mode)
-        ev1.record(ext)
-        ev1.synchronize()
-        barrier()
-        if r.status != hplai.HPLAI_OK:
-            raise RuntimeError(f"solve did not converge: {r}")
-        if timed:
-            results.append((ev0.elapsed_time(ev1), r, s.phase_ms(), s.refine_counts()))
-
-    for _ in range(args.warmup):
-        one_step(False)
+    # the headline form: exactly `steps` timed solves after `warmup`
+    fr = FormRun(hplai, torch, head_form, n, b, seed, maxit, args.autotune, args.lookahead, barrier)
+    fr.run(0, args.warmup)
     sampler = ClockSampler(dev)
     sampler.start()
     l0 = hplai.launch_count()
-    for _ in range(args.steps):
-        one_step(True)
+    fr.run(args.steps, 0)
     launches = hplai.launch_count() - l0
     clocks = sampler.stop()
-
-    total_ms = sum(r[0] for r in results)
-    value, max_ms = replica_value(total_ms, args.steps * hpl_flops(n), world, device="cuda")
-
-    # Roofline of the dominant kernel (the Schur GEMM), timed inside the
-    # library with CUDA events around each launch on its stream.
-    hbm, tc_burst, tc_sus, peak_kind = load_peaks()
-    peak_note = f"{peak_kind} (MEASURED_PEAKS.json: hbm_gbs, bf16_tflops_sustained)"
-    if prec == hplai.F32_F8:
-        # no measured e4m3 peak: the dense e4m3 rate is twice the FP16/BF16 rate
-        tc_sus *= 2.0
-        peak_note += " x 2 for e4m3 (nominal e4m3:bf16 ratio; no measured e4m3 peak)"
-    sflops, sbytes, slaunch = schur_algorithmic(n, b, 1 if prec == hplai.F32_F8 else 2, 4 if deck else 8)
-    gemm_ms = statistics.mean(r[2]["GEMM_UPDATE"] for r in results)
-    avg_launch_s = gemm_ms * 1e-3 / slaunch
-    ach_gbs = sbytes / slaunch / avg_launch_s / 1e9
-    ach_tf = sflops / slaunch / avg_launch_s / 1e12
-    ridge = tc_sus * 1e12 / (hbm * 1e9)
-    intensity = sflops / sbytes
-    bound = "tensor" if intensity >= ridge else "hbm"
-    traffic = schur_traffic_per_launch(n, b)
-    if bound == "hbm":
-        roof = {"bound": "hbm", "achieved": ach_gbs, "peak": hbm, "unit": "GB/s", "frac": ach_gbs / hbm}
-    else:
-        roof = {"bound": "tensor", "achieved": ach_tf, "peak": tc_sus, "unit": "TFLOP/s", "frac": ach_tf / tc_sus}
-    kname = "schur_kernel (tcgen05 e4m3 x e4m3 -> FP32, C -= sl*L*U*su)" if prec == hplai.F32_F8 else \
-        "schur_kernel (tcgen05 FP16 x FP16 -> FP32, C -= L*U)"
-    roof.update({"traffic": traffic if (prec == hplai.F32_F16 and not deck) else None, "kernel": kname,
-                 "launches_per_step": slaunch, "avg_launch_ms": avg_launch_s * 1e3,
-                 "algorithmic_bytes_per_launch": sbytes / slaunch, "algorithmic_flops_per_launch": sflops / slaunch,
-                 "intensity_flop_per_byte": intensity, "ridge_flop_per_byte": ridge,
-                 "tensor_achieved_tflops": ach_tf, "tensor_peak_tflops": tc_sus,
-                 "tensor_frac": ach_tf / tc_sus, "peak_source": peak_note})
-    phases = {k: statistics.mean(r[2][k] for r in results) for k in results[0][2]}
-
-    # End to end through the public C API with host buffers: pinned FP32 A,
-    # FP64 rhs and diagonal copied in, x copied out, every step.
+    head = fr.summary(world)
     e2e = None
     if not args.no_e2e:
-        s.generate(seed)
-        torch.cuda.synchronize()
-        try:
-            a_h = torch.empty(n * n, dtype=torch.float32, pin_memory=True)
-            pinned = True
-        except RuntimeError:
-            a_h = torch.empty(n * n, dtype=torch.float32)
-            pinned = False
-        import numpy as np
-        hplai.check(hplai._get_lu(s._h, a_h.data_ptr(), n), "hplai_get_lu")
-        rhs_h = torch.from_numpy(s.rhs()).pin_memory() if pinned else torch.from_numpy(s.rhs())
-        d_h = torch.from_numpy(s.diag()).pin_memory() if pinned else torch.from_numpy(s.diag())
-        x_h = torch.empty(n, dtype=torch.float64, pin_memory=pinned)
-        ets = []
-        for i in range(args.e2e_warmup + args.steps):
-            barrier()
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            ev0.record(ext)
-            r = s.solve_host_ptrs(a_h.data_ptr(), n, rhs_h.data_ptr(), d_h.data_ptr(), seed, maxit, x_h.data_ptr())
-            ev1.record(ext)
-            ev1.synchronize()
-            barrier()
-            if r.status != hplai.HPLAI_OK:
-                raise RuntimeError(f"e2e solve did not converge: {r}")
-            if i >= args.e2e_warmup:
-                ets.append(ev0.elapsed_time(ev1))
-        te = torch.tensor([sum(ets)], dtype=torch.float64, device="cuda")
-        if world > 1:
-            torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-        e2e = {"value": world * len(ets) * hpl_flops(n) / (float(te.item()) * 1e-3) / 1e9, "unit": UNIT,
-               "h2d_bytes_per_step": n * n * 4 + 2 * n * 8, "d2h_bytes_per_step": n * 8,
-               "host_memory": "pinned" if pinned else "pageable", "ms_per_step": float(te.item()) / len(ets)}
+        e2e = e2e_run(hplai, torch, fr, min(args.steps, args.e2e_steps), args.e2e_warmup, world, barrier)
+    fr.close()
+
+    # the comparison form, on the same GPU right after (its own context)
+    other = None
+    if other_key:
+        fo = FormRun(hplai, torch, FORMS[other_key], n, b, seed, maxit, args.autotune, args.lookahead, barrier)
+        fo.run(min(args.steps, args.compare_steps), min(args.warmup, args.compare_warmup))
+        other = fo.summary(world)
+        fo.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nb_, bb_ = CPU_SAMPLE
         threads = os.cpu_count() or 1
         reps, tot = 0, 0.0
-        kind = "port"
-        while tot < 10.0 and reps < 5:
+        kind, cores = "port", threads
+        while tot < 10.0 and reps < 8:
             g, secs, har, kind, cores = cpu_solve_gflops(nb_, bb_, threads)
             reps += 1
             tot += secs
-        cpu = {"value": reps * hpl_flops(nb_) / tot / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
-               "sample": f"{reps} full solve(s) (LU + IR) at n={nb_} b={bb_} on the host CPU, {tot:.1f} s"}
+        cpu = {"value": reps * hpl_flops(nb_) / tot / 1e9, "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"{reps} solve(s) by {cpu_sample_note(kind, cores, nb_, bb_)}, {tot:.1f} s"}
 
-    last = results[-1][1]
     if rank == 0:
+        cfg = "C3" if (n, b) == (131072, 1024) else ("C2" if (n, b) == (65536, 512) else "custom")
+        wl = f"HPL-AI solve n={n} b={b} ({cfg}), {head['form']}"
+        if other:
+            wl += f"; compared with the {other['form']}"
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "e4m3/fp32/fp64" if prec == hplai.F32_F8 else "fp16/fp32/fp64",
+            "dtype": "e4m3/fp16/fp32/fp64" if head_form["precision"] == "f8" else "fp16/fp32/fp64",
             "data": "synthetic (the reference's own LCG matrix, seed 42, regenerated on the device before each step)",
-            "config": {"workload": f"HPL-AI solve n={n} b={b}: FP32 panels, "
-                                   f"{'e4m3' if prec == hplai.F32_F8 else 'FP16'} tcgen05 Schur update, "
-                                   f"FP64 {'GMRES-IR' if mode == hplai.GMRES else 'iterative refinement'}",
-                       "n": n, "b": b, "form": form, "lookahead": bool(args.lookahead), "autotuned": tuned,
-                       "trailing_matrix": "FP16 deck (updates in FP16, applied per panel)" if deck else "FP32",
+            "config": {"workload": wl, "n": n, "b": b, "form": head["form"], "schedule": head["schedule"],
+                       "trailing_matrix": head["trailing_matrix"],
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": f"inputs {n * n * 4 / 1e9:.1f} GB FP32 > 126 MB L2, rewritten between steps"},
-            "hpl_harness": last.hpl_harness, "resid": last.residual, "ir_steps": last.iters,
-            "gmres_inner_steps": results[-1][3][1] if mode == hplai.GMRES else None,
-            "phases_ms": phases, "roofline": roof, "gpu_launches": int(launches),
+            "hpl_harness": head["hpl_harness"], "resid": head["resid"],
+            "residual_evaluations": head["residual_evaluations"], "gmres_inner_steps": head["gmres_inner_steps"],
+            "phases_ms": head["phases_ms"], "roofline": head["roofline"], "gpu_launches": int(launches),
             "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
         }
+        if other:
+            line["plain" if other_key == "plain" else other_key] = other
+            line["speedup_vs_" + other_key] = other["ms_per_step"] / head["ms_per_step"]
         print(json.dumps(line), flush=True)
-    s.close()
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
@@ -597,30 +736,85 @@ def run_check(args):
     return 0
 
 
+def run_peak(args):
+    """Dense tensor-core peaks of this GPU as cuBLAS reaches them (torch
+    matmul in bf16, torch._scaled_mm in e4m3 with FP32 scales, bf16 out),
+    M = N = K = 8192: the best of 10 launches (burst) and the mean over 4 s
+    back to back (sustained, under the power cap).  A measurement of the
+    denominator only: no product path calls these."""
+    import torch
+    torch.cuda.set_device(0)
+    m = 8192
+    fl = 2.0 * m * m * m
+    a = torch.randn(m, m, device="cuda").to(torch.bfloat16)
+    bm = torch.randn(m, m, device="cuda").to(torch.bfloat16)
+    a8 = a.to(torch.float8_e4m3fn)
+    b8 = bm.to(torch.float8_e4m3fn).t()   # column-major operand
+    one = torch.ones((), device="cuda")
+    kinds = {"bf16": lambda: torch.matmul(a, bm),
+             "e4m3": lambda: torch._scaled_mm(a8, b8, scale_a=one, scale_b=one, out_dtype=torch.bfloat16)}
+    out = {"gpu": torch.cuda.get_device_name(0), "m": m, "n": m, "k": m}
+    sampler = ClockSampler(0)
+    sampler.start()
+    for name, fn in kinds.items():
+        for _ in range(5):
+            fn()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(10):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        reps, t_end = 0, time.perf_counter() + 4.0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        while time.perf_counter() < t_end:
+            for _ in range(20):
+                fn()
+            reps += 20
+            torch.cuda.synchronize()
+        e1.record()
+        e1.synchronize()
+        out[name] = {"burst_tflops": fl / best / 1e9, "sustained_tflops": fl * reps / e0.elapsed_time(e1) / 1e9,
+                     "sustained_launches": reps}
+    out["clocks"] = sampler.stop()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--n", type=int, default=None, help="order (default 65536; 8192 for the adjoint workload)")
-    ap.add_argument("--b", type=int, default=None, help="block size (default 512; 256 for the adjoint workload)")
+    ap.add_argument("--n", type=int, default=None, help="order (default 131072; 8192 for the adjoint workload)")
+    ap.add_argument("--b", type=int, default=None, help="block size (default 1024; 256 for the adjoint workload)")
     ap.add_argument("--e2e-warmup", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=5, help="end-to-end solves timed (at most --steps)")
+    ap.add_argument("--forms", choices=("both", "precision", "plain"), default="both",
+                    help="solve workload: the precision form (headline) and the plain form back to back, or one")
+    ap.add_argument("--compare-steps", type=int, default=8, help="timed solves of the comparison form (at most --steps)")
+    ap.add_argument("--compare-warmup", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--precision", choices=("f16", "f8"), default="f16",
-                    help="Schur update operands: FP16 (plain form) or e4m3 with per-128 factors")
-    ap.add_argument("--workload", choices=("solve", "batch", "adjoint", "gemm", "check"), default="solve",
-                    help="solve: one system (default n=65536 b=512); batch: many systems; adjoint: forward + "
-                         "transposed solves; gemm / check: the Schur GEMM or the factor checksum leaf alone")
+    ap.add_argument("--precision", choices=("f16", "f8"), default=None,
+                    help="override the headline form's Schur operands: FP16 or e4m3 with per-128 factors")
+    ap.add_argument("--workload", choices=("solve", "batch", "adjoint", "gemm", "check", "peak"), default="solve",
+                    help="solve: one system (default n=131072 b=1024, precision and plain forms); batch: many "
+                         "systems; adjoint: forward + transposed solves; gemm / check: the Schur GEMM or the "
+                         "factor checksum leaf alone; peak: cuBLAS bf16/e4m3 dense rates (the roofline denominators)")
     ap.add_argument("--m", type=int, default=16384, help="gemm workload: rows of C")
     ap.add_argument("--n-cols", type=int, default=16384, help="gemm workload: columns of C")
     ap.add_argument("--k", type=int, default=512, help="gemm workload: panel width")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-seed", type=int, default=20240611)
     ap.add_argument("--batch-workers", type=int, default=8)
-    ap.add_argument("--deck", choices=("on", "off"), default="off",
-                    help="FP16 trailing-update deck (HPLAI_FLAG_FP16_DECK)")
+    ap.add_argument("--deck", choices=("on", "off"), default=None,
+                    help="override the headline form's trailing matrix: FP16 deck (HPLAI_FLAG_FP16_DECK) or FP32")
     ap.add_argument("--autotune", action="store_true",
                     help="choose the schedule (serial or look-ahead, side-stream SMs) with hplai_autotune first "
                          "(the default for the solve workload unless --lookahead or --no-autotune is given)")
@@ -628,7 +822,7 @@ def main():
     ap.add_argument("--lookahead", action="store_true",
                     help="form the next step's diagonal block and panels on a side stream (HPLAI_FLAG_LOOKAHEAD)")
     ap.add_argument("--refine", choices=("ir", "gmres"), default=None,
-                    help="correction: classical IR or GMRES (default: ir for f16, gmres for f8)")
+                    help="override the headline form's correction: classical IR or GMRES")
     args = ap.parse_args()
     if not args.lookahead and not args.no_autotune:
         args.autotune = True
@@ -646,6 +840,8 @@ def main():
         return run_gemm(args)
     if args.workload == "check":
         return run_check(args)
+    if args.workload == "peak":
+        return run_peak(args)
     return run_ours(args)
 
 

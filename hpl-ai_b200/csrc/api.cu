@@ -502,7 +502,7 @@ extern "C" int hplai_factor(hplai_ctx *c)
 		if (c->deck) {
 			// the next block column and block row become A + deck / dscale (the
 			// FP16 panel copies fold the deck in themselves: the diagonal block only)
-			HPLAI_TRY(pe.record(st, HPLAI_PH_GEMM_UPDATE));
+			HPLAI_TRY(pe.record(st, HPLAI_PH_LAZY_INIT));
 			if (f16_panel_form(c, simt)) {
 				HPLAI_TRY(launch_deck_apply(r1, r2, r1, r2, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
 			} else {
@@ -930,7 +930,8 @@ extern "C" int hplai_get_phase_ms(hplai_ctx *c, double *ms, int count)
 {
 	if (!c || !ms) return HPLAI_EINVAL;
 	double total = 0.0;
-	for (int i = 0; i < HPLAI_PH_TOTAL; ++i) total += c->phase_ms[i];
+	for (int i = 0; i < HPLAI_PH_COUNT; ++i)
+		if (i != HPLAI_PH_TOTAL) total += c->phase_ms[i];
 	for (int i = 0; i < count && i < HPLAI_PH_COUNT; ++i) ms[i] = (i == HPLAI_PH_TOTAL) ? total : c->phase_ms[i];
 	return HPLAI_OK;
 }

@@ -73,8 +73,9 @@ typedef enum hplai_phase {
 	HPLAI_PH_GEMM_UPDATE = 3,
 	HPLAI_PH_IR_GEMV = 4,
 	HPLAI_PH_IR_TRSV = 5,
-	HPLAI_PH_TOTAL = 6,
-	HPLAI_PH_COUNT = 7
+	HPLAI_PH_TOTAL = 6,      /* sum of the other items (overlapping side-stream items included) */
+	HPLAI_PH_LAZY_INIT = 7,  /* FP16 deck folded into the next block column/row (lazy_init.hpp:92-227) */
+	HPLAI_PH_COUNT = 8
 } hplai_phase;
 
 /* hplai_create flags. */

@@ -599,3 +599,44 @@ ORC_EXPORT void orc_panel_check(int n, int b, const float *a, int64_t lda, doubl
 	sigs[1] = sigu;
 	sigs[2] = sigl;
 }
+
+/* Residual rows r_i = rhs_i - sum_j A(i,j) x_j of the FP64 matrix the
+ * refinement regenerates (Matgen<double>: off-diagonal generator values,
+ * the sequential row-sum diagonal; iterative_refinement.hpp:36-42 with
+ * panel_gemv.hpp:16-180), for the listed rows only, each summed in long
+ * double (64-bit mantissa on x86) so that the oracle's own rounding is far
+ * below the GPU's.  rhs_col selects the right-hand side: column n + rhs_col
+ * of the stream (0 = the benchmark's b).  n LCG steps per row: cheap at any
+ * n, so large solves can be checked on sampled rows.  trans: rows of A^T. */
+ORC_EXPORT void orc_residual_rows(int n, uint64_t seed, const double *x, int nrows, const int64_t *rows,
+	int trans, int rhs_col, const double *rhs, double *r)
+{
+	orc_coeff inc1 = coeff_default();
+	orc_coeff jumpn = coeff_pow(inc1, (uint64_t)n);
+	#pragma omp parallel for schedule(dynamic, 1)
+	for (int t = 0; t < nrows; t++) {
+		const int64_t i = rows[t];
+		/* A(i, j) at index i + n j (step jumpn per column); A^T(i, j) = A(j, i)
+		 * at index j + n i (step 1 per column) */
+		uint64_t s = trans ? state_at(n, 0, i, seed) : state_at(n, i, 0, seed);
+		const orc_coeff step = trans ? inc1 : jumpn;
+		long double acc = 0.0L;
+		double di = 0.0;
+		for (int64_t j = 0; j < n; j++) {
+			const double v = state_value(s);
+			if (j != i) {
+				acc += (long double)v * (long double)x[j];
+				di += fabs(trans ? 0.0 : v);
+			}
+			s = coeff_apply(step, s);
+		}
+		/* the diagonal entry is the off-diagonal absolute sum of row i of A
+		 * (the same row for A and A^T), summed in sequential FP64 */
+		if (trans) di = orc_calc_diag((int)i, n, seed);
+		acc += (long double)di * (long double)x[i];
+		double bi;
+		if (rhs) bi = rhs[i];
+		else bi = state_value(state_at(n, i, (int64_t)n + rhs_col, seed));
+		r[t] = (double)((long double)bi - acc);
+	}
+}

@@ -60,6 +60,7 @@ _e4m3_rn = _proto("orc_e4m3_rn", ctypes.c_uint8, ctypes.c_float)
 _e4m3_to_f32 = _proto("orc_e4m3_to_f32", ctypes.c_float, ctypes.c_uint8)
 _quantize_e4m3 = _proto("orc_quantize_e4m3", None, _int, _int, _vp, _i64, _int, _vp, _i64, _vp)
 _panel_check = _proto("orc_panel_check", None, _int, _int, _vp, _i64, _vp)
+_residual_rows = _proto("orc_residual_rows", None, _int, _u64, _vp, _int, _vp, _int, _int, _vp, _vp)
 _f8gemm = _proto("orc_f8gemm_minus", None, _int, _int, _int, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _i64)
 
 
@@ -252,3 +253,17 @@ def f8gemm_minus(c: np.ndarray, l8: np.ndarray, sl: np.ndarray, u8: np.ndarray, 
     _f8gemm(m, n, k, _p(l8), l8.shape[1], _p(np.ascontiguousarray(sl, dtype=np.float32)), _p(u8), u8.shape[1],
             _p(np.ascontiguousarray(su, dtype=np.float32)), _p(c), m)
     return c
+
+
+def residual_rows(n, x, rows, seed=42, trans=False, rhs_col=0, rhs_v=None) -> np.ndarray:
+    """r_i = rhs_i - (A x)_i for the listed rows of the FP64 matrix the
+    refinement regenerates (long-double sums; n generator steps per row).
+    rhs_v: the right-hand side (host vector), else column n + rhs_col of the
+    generator stream."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    out = np.zeros(len(rows))
+    rv = None if rhs_v is None else np.ascontiguousarray(rhs_v, dtype=np.float64)
+    _residual_rows(n, seed, _p(x), len(rows), _p(rows), 1 if trans else 0, rhs_col,
+                   None if rv is None else _p(rv), _p(out))
+    return out

@@ -1,0 +1,79 @@
+"""The oracle and the GPU path against the reference's own outputs at C1
+(n = 1200, b = 60, seed 42, 2 x 2 grid), from tests/golden/ref_c1.json
+(written by tests/golden/make_ref_fixtures.py from the reference's CPU driver
+built by oracle/build_ref.sh).
+
+* The oracle's LU is the reference's LU bit for bit when the reference is
+  linked with a netlib-order BLAS (its own BLAS is unpinned): the SHA-256 of
+  the FP32 factors match.
+* The refinement's step-0 residual and harness equal the reference's in every
+  run; step 1 depends on the grid's TRSV summation order (the oracle follows a
+  single process column), so it is compared to 1e-8.
+* Every solution -- the oracle's, the GPU's plain form, the GPU's FP16-deck
+  form, the GPU's precision form -- equals the reference's x from each of its
+  four runs (`-not -r`, `-not -d -r`, netlib and OpenBLAS builds) to FP64
+  relative error 1e-12.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIX = json.load(open(os.path.join(HERE, "golden", "ref_c1.json")))
+N, B = FIX["n"], FIX["b"]
+
+
+def ref_x(run):
+    return np.array([float.fromhex(v) for v in FIX["runs"][run]["x"]])
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def test_oracle_lu_is_the_references_bit_for_bit(oracle):
+    lu = oracle.lu(oracle.matrix(N), B)
+    digest = hashlib.sha256(np.asfortranarray(lu).tobytes(order="F")).hexdigest()
+    assert digest == FIX["runs"]["netlib_not_r"]["lu_sha256"]
+
+
+def test_oracle_refinement_vs_reference_steps(oracle):
+    rc, x, res, har, steps = oracle.solve(N, B, q=2)
+    assert rc == 0
+    for run in FIX["runs"].values():
+        assert steps[0][0] == run["steps"][0]["residual"]
+        assert abs(steps[0][1] - run["steps"][0]["hpl_harness"]) <= 1e-12 * steps[0][1]
+    ref = FIX["runs"]["netlib_not_r"]["steps"]
+    assert len(steps) == len(ref)
+    assert abs(steps[1][0] - ref[1]["residual"]) <= 1e-8 * ref[1]["residual"]
+    assert 0 <= har < 16 and 0 <= FIX["runs"]["netlib_not_r"]["hpl_harness"] < 16
+
+
+@pytest.mark.parametrize("run", sorted(FIX["runs"]))
+def test_oracle_x_matches_reference_x(oracle, run):
+    rc, x, _, _, _ = oracle.solve(N, B, q=2)
+    assert rc == 0
+    assert rel(x, ref_x(run)) <= 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", ["plain", "deck", "precision"])
+def test_gpu_x_matches_reference_x(hplai, torch_cuda, form):
+    """C1's parity bar: x equals the reference's x to FP64 relative 1e-12,
+    against all four of the reference's runs."""
+    prec, flags, mode = hplai.F32_F16, 0, hplai.IR
+    if form == "deck":
+        flags = hplai.FLAG_FP16_DECK
+    elif form == "precision":
+        prec, flags, mode = hplai.F32_F8, hplai.FLAG_FP16_DECK, hplai.GMRES
+    with hplai.Solver(N, B, precision=prec, flags=flags) as s:
+        s.generate(42)
+        s.factor()
+        r = s.iterative_refinement(50, mode=mode)
+        x = s.x()
+    assert r.status == hplai.HPLAI_OK and 0 <= r.hpl_harness < 16
+    for run in FIX["runs"]:
+        assert rel(x, ref_x(run)) <= 1e-12, run
