@@ -215,28 +215,50 @@ def run_reference(args):
     return 0
 
 
-def schur_algorithmic(n, b, panel_bytes=2, c_bytes=8):
-    """Flops and bytes of all Schur launches of one factorisation.
-    Step k updates C = (n-(k+1)b)^2 FP32 elements (read and written, 8 B
-    each), reads the L and U panels (2*rem*b elements of panel_bytes: 2 for
-    FP16, 1 for e4m3) and does 2*rem^2*b flops, in three launches (the next
-    panel's block column and block row, then the rest of the trailing
-    matrix; the last step has no rest).  c_bytes: 8 for the FP32 trailing
-    matrix read + write, 4 for the FP16 deck."""
-    flops = byts = 0.0
-    launches = 0
+def schur_algorithmic(n, b, panel_bytes=2, c_bytes=8, group=1):
+    """Flops, bytes and launches of all Schur updates of one factorisation,
+    in the order hplai_factor issues them.  The update by a group of `group`
+    panels (K = group * b) of the trailing matrix from block e on is split
+    into the next group's block columns, its block rows and the rest; with
+    two-panel groups a group's second block first receives its first panel's
+    update alone (K = b).  A region of m x n C elements with panel width K
+    does 2 m n K flops and moves c_bytes per C element (8: FP32 read +
+    write; 4: the FP16 deck) plus (m + n) K panel elements of panel_bytes
+    (2 for FP16, 1 for e4m3)."""
+    acc = {"flops": 0.0, "bytes": 0.0, "launches": 0}
     nb = n // b
-    for k in range(nb - 1):
-        rem = n - (k + 1) * b
-        flops += 2.0 * rem * rem * b
-        byts += float(c_bytes) * rem * rem + 2.0 * panel_bytes * rem * b
-        launches += 3 if k < nb - 2 else 2   # next block column, next block row, rest
-    return flops, byts, launches
+
+    def region(m, nn, k):
+        if m <= 0 or nn <= 0:
+            return
+        acc["flops"] += 2.0 * m * nn * k
+        acc["bytes"] += float(c_bytes) * m * nn + float(panel_bytes) * (m + nn) * k
+        acc["launches"] += 1
+
+    def first_panel_update(j):
+        region(n - j * b, b, b)
+        region(b, n - (j + 1) * b, b)
+
+    for j in range(1, min(group, nb)):
+        first_panel_update(j)
+    s = 0
+    while s + group < nb:
+        e = s + group
+        ne = min(group, nb - e)
+        r1, r2, k = e * b, (e + ne) * b, group * b
+        region(n - r1, r2 - r1, k)
+        region(r2 - r1, n - r2, k)
+        for j in range(e + 1, e + ne):
+            first_panel_update(j)
+        region(n - r2, n - r2, k)
+        s += group
+    return acc["flops"], acc["bytes"], acc["launches"]
 
 
-def schur_traffic_per_launch(n, b):
-    """DRAM bytes per average launch from the committed ncu summary, scaled
-    by C elements (traffic grows with rem^2)."""
+def schur_traffic_per_launch(n, b, group=1):
+    """DRAM bytes per average launch from the committed ncu summary (DRAM
+    bytes per C element of the FP32-C kernel), times the C elements of one
+    factorisation's launches (traffic grows with the C area), per launch."""
     p = os.path.join(ROOT, "profiles", "schur_kernel_traffic.json")
     if not os.path.exists(p):
         return None
@@ -244,9 +266,8 @@ def schur_traffic_per_launch(n, b):
     per_elem = d.get("dram_bytes_per_c_element")
     if not per_elem:
         return None
-    _, _, launches = schur_algorithmic(n, b)
-    elems = sum((n - (k + 1) * b) ** 2 for k in range(n // b - 1))
-    return per_elem * elems / launches
+    _, byts, launches = schur_algorithmic(n, b, 0, 1, group)   # bytes = C elements
+    return per_elem * byts / launches
 
 
 FORMS = {
@@ -261,7 +282,7 @@ FORMS = {
 }
 
 
-def schur_roofline(hplai, n, b, fp8, deck, gemm_ms):
+def schur_roofline(hplai, n, b, fp8, deck, gemm_ms, group=1):
     """Roofline of the Schur GEMM over one factorisation: algorithmic flops
     and bytes per launch (schur_algorithmic) over the average launch time
     (CUDA events around each launch on its stream, summed by the library)."""
@@ -275,7 +296,7 @@ def schur_roofline(hplai, n, b, fp8, deck, gemm_ms):
         else:
             tc_sus *= 2.0
             peak_note += " x 2 for e4m3 (nominal e4m3:bf16 ratio; no measured e4m3 peak)"
-    sflops, sbytes, slaunch = schur_algorithmic(n, b, 1 if fp8 else 2, 4 if deck else 8)
+    sflops, sbytes, slaunch = schur_algorithmic(n, b, 1 if fp8 else 2, 4 if deck else 8, group)
     avg_launch_s = gemm_ms * 1e-3 / slaunch
     ach_gbs = sbytes / slaunch / avg_launch_s / 1e9
     ach_tf = sflops / slaunch / avg_launch_s / 1e12
@@ -288,7 +309,7 @@ def schur_roofline(hplai, n, b, fp8, deck, gemm_ms):
         roof = {"bound": "tensor", "achieved": ach_tf, "peak": tc_sus, "unit": "TFLOP/s", "frac": ach_tf / tc_sus}
     cdesc = "FP16 deck, deck -= s*L*U" if deck else "FP32 C, C -= L*U"
     kname = f"schur_kernel (tcgen05 {'e4m3 x e4m3' if fp8 else 'FP16 x FP16'} -> FP32 accumulator; {cdesc})"
-    traffic = schur_traffic_per_launch(n, b) if (not fp8 and not deck) else None
+    traffic = schur_traffic_per_launch(n, b, group) if (not fp8 and not deck) else None
     roof.update({"traffic": traffic, "kernel": kname,
                  "launches_per_step": slaunch, "avg_launch_ms": avg_launch_s * 1e3,
                  "algorithmic_bytes_per_launch": sbytes / slaunch, "algorithmic_flops_per_launch": sflops / slaunch,
@@ -298,6 +319,7 @@ def schur_roofline(hplai, n, b, fp8, deck, gemm_ms):
                  "intensity_flop_per_byte": intensity, "ridge_flop_per_byte": ridge,
                  "tensor_achieved_tflops": ach_tf, "tensor_peak_tflops": tc_sus,
                  "tensor_frac": ach_tf / tc_sus, "hbm_achieved_gbs": ach_gbs, "hbm_frac": ach_gbs / hbm,
+                 "panels_per_update": group,
                  "peak_source": peak_note})
     return roof
 
@@ -321,7 +343,7 @@ class FormRun:
     hpl-harness < 16) after `warmup` untimed ones, the matrix regenerated on
     the device before each solve outside the timed window."""
 
-    def __init__(self, hplai, torch, form, n, b, seed, maxit, autotune, lookahead, barrier):
+    def __init__(self, hplai, torch, form, n, b, seed, maxit, autotune, lookahead, barrier, group=1):
         self.hplai, self.torch, self.form = hplai, torch, form
         self.n, self.b, self.seed, self.maxit = n, b, seed, maxit
         self.fp8 = form["precision"] == "f8"
@@ -330,17 +352,26 @@ class FormRun:
         flags = hplai.FLAG_LOOKAHEAD if lookahead else 0
         if self.deck:
             flags |= hplai.FLAG_FP16_DECK
+        if group == 2:
+            flags |= hplai.FLAG_GROUP2
         self.s = hplai.Solver(n, b, precision=hplai.F32_F8 if self.fp8 else hplai.F32_F16, flags=flags)
         self.ext = torch.cuda.ExternalStream(self.s.stream())
         self.barrier = barrier
         self.tuned = None
-        self.schedule = {"lookahead": bool(lookahead), "side_sms": None, "source": "flag" if lookahead else "serial"}
+        self.group = 2 if (flags & hplai.FLAG_GROUP2) else 1
+        self.schedule = {"lookahead": bool(lookahead), "side_sms": None, "panels_per_update": self.group,
+                         "source": "flags"}
         if autotune:
             # outside the timed region: time the factorisation under each schedule, keep the fastest
             tflags, tside, tms = self.s.autotune(seed)
             la = bool(tflags & hplai.FLAG_LOOKAHEAD)
-            self.tuned = {"lookahead": la, "side_sms": tside, "factor_ms": tms}
-            self.schedule = {"lookahead": la, "side_sms": tside if la else None, "source": "hplai_autotune"}
+            self.group = 2 if (tflags & hplai.FLAG_GROUP2) else 1
+            trials = [{"panels_per_update": 2 if (f & hplai.FLAG_GROUP2) else 1,
+                       "lookahead": bool(f & hplai.FLAG_LOOKAHEAD), "side_sms": sd if (f & hplai.FLAG_LOOKAHEAD) else None,
+                       "factor_ms": round(ms, 2)} for f, sd, ms in self.s.autotune_log()]
+            self.tuned = {"factor_ms_median": tms, "trials_warmup_first": trials}
+            self.schedule = {"lookahead": la, "side_sms": tside if la else None, "panels_per_update": self.group,
+                             "source": "hplai_autotune"}
         self.results = []
 
     def step(self, timed):
@@ -372,7 +403,7 @@ class FormRun:
         steps = len(self.results)
         value, max_ms = replica_value(total_ms, steps * hpl_flops(self.n), world, device="cuda")
         phases = {k: statistics.mean(r[2][k] for r in self.results) for k in self.results[0][2]}
-        roof = schur_roofline(hplai, self.n, self.b, self.fp8, self.deck, phases["GEMM_UPDATE"])
+        roof = schur_roofline(hplai, self.n, self.b, self.fp8, self.deck, phases["GEMM_UPDATE"], self.group)
         last = self.results[-1]
         return {
             "form": self.form["label"], "value": value, "unit": UNIT, "steps": steps,
@@ -471,7 +502,7 @@ def run_ours(args):
                               f"{'GMRES-IR' if head_form['refine'] == 'gmres' else 'IR'}")
 
     # the headline form: exactly `steps` timed solves after `warmup`
-    fr = FormRun(hplai, torch, head_form, n, b, seed, maxit, args.autotune, args.lookahead, barrier)
+    fr = FormRun(hplai, torch, head_form, n, b, seed, maxit, args.autotune, args.lookahead, barrier, args.group)
     fr.run(0, args.warmup)
     sampler = ClockSampler(dev)
     sampler.start()
@@ -488,7 +519,8 @@ def run_ours(args):
     # the comparison form, on the same GPU right after (its own context)
     other = None
     if other_key:
-        fo = FormRun(hplai, torch, FORMS[other_key], n, b, seed, maxit, args.autotune, args.lookahead, barrier)
+        fo = FormRun(hplai, torch, FORMS[other_key], n, b, seed, maxit, args.autotune, args.lookahead, barrier,
+                     args.group)
         fo.run(min(args.steps, args.compare_steps), min(args.warmup, args.compare_warmup))
         other = fo.summary(world)
         fo.close()
@@ -819,12 +851,14 @@ def main():
                     help="choose the schedule (serial or look-ahead, side-stream SMs) with hplai_autotune first "
                          "(the default for the solve workload unless --lookahead or --no-autotune is given)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the serial schedule (or --lookahead's)")
+    ap.add_argument("--group", type=int, choices=(1, 2), default=1,
+                    help="panels per trailing update without autotuning (2 = HPLAI_FLAG_GROUP2, b % 128 == 0)")
     ap.add_argument("--lookahead", action="store_true",
                     help="form the next step's diagonal block and panels on a side stream (HPLAI_FLAG_LOOKAHEAD)")
     ap.add_argument("--refine", choices=("ir", "gmres"), default=None,
                     help="override the headline form's correction: classical IR or GMRES")
     args = ap.parse_args()
-    if not args.lookahead and not args.no_autotune:
+    if not args.lookahead and not args.no_autotune and args.group == 1:
         args.autotune = True
     if args.n is None:
         args.n = ADJOINT_N if args.workload == "adjoint" else DEFAULT_N

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <string>
@@ -53,21 +54,37 @@ struct hplai_ctx {
 	int side_sms = 20;   // SMs of the side stream with HPLAI_FLAG_LOOKAHEAD (hplai_autotune sets it)
 	int64_t lda = 0, ldh = 0;
 	float *A = nullptr;
-	// FP16 panel copies, double buffered: the panels of step k+1 are formed
-	// on the side stream while the main stream's update of step k still
-	// reads those of step k (the reference's nbuf = 2 rotating buffers).
+	// Panel copies for the trailing updates.  A group of `group` consecutive
+	// panels (1, or 2 with HPLAI_FLAG_GROUP2) updates the trailing matrix in
+	// one pass with K = group * b (C -= [L_k L_k+1] [U_k; U_k+1]), which halves
+	// the passes over the trailing matrix.  FP16 group buffers, double
+	// buffered (the next group is formed on the side stream while the main
+	// stream's update still reads the current one): row i of Lh[q] holds row i
+	// of the group's L panels side by side (slot h at column h * ldh, row
+	// pitch ldg = gcap * ldh), row j of Uh[q] column j of its U panels (the
+	// reference's nbuf = 2 rotating LRPanels, panel.hpp:236-268).
+	int group = 1, gcap = 1;      // panels per update now / that the buffers hold
+	int64_t ldg = 0;
 	uint16_t *Lh[2] = {nullptr, nullptr}, *Uh[2] = {nullptr, nullptr};
-	SchurMaps maps[2];
-	// precision form: e4m3 panel copies with per-128-row/column factors
+	SchurMaps maps[2][2];         // [buffer][slot]: one panel, K = b
+	SchurMaps mapsg[2];           // [buffer]: both slots, K = 2b (gcap 2)
+	// precision form: e4m3 group copies with one power-of-two factor per 128
+	// rows shared by the group's panels (row pitch ld8g = gcap * ld8), and,
+	// for the update of a group's second block by its first panel alone, an
+	// e4m3 copy of that panel (L8s, U8s)
 	uint8_t *L8[2] = {nullptr, nullptr}, *U8[2] = {nullptr, nullptr};
 	float *sl[2] = {nullptr, nullptr}, *su[2] = {nullptr, nullptr};
+	uint8_t *L8s = nullptr, *U8s = nullptr;
+	float *sls = nullptr, *sus = nullptr;
 	unsigned *qbits = nullptr;
-	int64_t ld8 = 0;
+	int64_t ld8 = 0, ld8g = 0;
 	// HPLAI_FLAG_FP16_DECK: FP16 trailing-update deck (n x lda halves), holding
 	// dscale x (accumulated update)
 	uint16_t *deck = nullptr;
 	float dscale = 1.f;
-	SchurMaps maps8[2];
+	SchurMaps maps8[2];           // [buffer]: K = b
+	SchurMaps maps8g[2];          // [buffer]: K = 2b (gcap 2)
+	SchurMaps maps8s;             // the single panel copy, K = b
 	TcPanels tc;
 	float *tcbuf = nullptr;   // phi, plo (n x ldp), the four b x ldp inverse buffers, the inversion work
 	double *rhs = nullptr, *d = nullptr, *x = nullptr, *r = nullptr, *scal = nullptr;
@@ -89,6 +106,13 @@ struct hplai_ctx {
 	double norma = 0.0, normb = 0.0;
 	std::vector<double> log_resid, log_harness;
 	double phase_ms[HPLAI_PH_COUNT] = {};
+	// hplai_autotune's trials: schedule and factorisation milliseconds
+	struct Trial {
+		unsigned flags;
+		int side_sms;
+		double ms;
+	};
+	std::vector<Trial> tune_log;
 	// GMRES correction: restart length, relative tolerance on the
 	// preconditioned residual, basis and scratch (allocated on first use)
 	int gm_restart = 30;
@@ -116,6 +140,10 @@ int ctx_free(hplai_ctx *c)
 		cudaFree(c->sl[i]);
 		cudaFree(c->su[i]);
 	}
+	cudaFree(c->L8s);
+	cudaFree(c->U8s);
+	cudaFree(c->sls);
+	cudaFree(c->sus);
 	cudaFree(c->qbits);
 	cudaFree(c->deck);
 	cudaFree(c->tcbuf);
@@ -234,6 +262,7 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	if (n <= 0 || b < 16 || b > 1024 || n % b) return HPLAI_EINVAL;
 	if (precision != HPLAI_F32_F16 && precision != HPLAI_F32_F8) return HPLAI_EUNSUPPORTED;
 	if ((flags & HPLAI_FLAG_FP16_DECK) && (b % 8)) return HPLAI_EINVAL;
+	if ((flags & HPLAI_FLAG_GROUP2) && (b % 128)) return HPLAI_EINVAL;
 	hplai_ctx *c = new hplai_ctx;
 	c->n = n;
 	c->b = b;
@@ -244,6 +273,10 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	// power-of-two stride (the reference's calc_lda_c, panel.hpp:10-18, for HBM).
 	c->lda = round_up(n, 64) + 64;
 	c->ldh = round_up(b, 64);
+	// two-panel groups need whole 128-byte e4m3 rows and 64-half FP16 rows per panel
+	c->gcap = (b % 128 == 0) ? 2 : 1;
+	c->group = (flags & HPLAI_FLAG_GROUP2) ? 2 : 1;
+	c->ldg = c->gcap * c->ldh;
 	{
 		int lo = 0, hi = 0;
 		const cudaError_t e[5] = {cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking),
@@ -261,17 +294,24 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	}
 	CTX_ALLOC(c->A, sizeof(float) * static_cast<size_t>(c->lda) * n);
 	for (int i = 0; i < 2; ++i) {
-		CTX_ALLOC(c->Lh[i], sizeof(uint16_t) * static_cast<size_t>(c->ldh) * n);
-		CTX_ALLOC(c->Uh[i], sizeof(uint16_t) * static_cast<size_t>(c->ldh) * n);
+		CTX_ALLOC(c->Lh[i], sizeof(uint16_t) * static_cast<size_t>(c->ldg) * n);
+		CTX_ALLOC(c->Uh[i], sizeof(uint16_t) * static_cast<size_t>(c->ldg) * n);
 	}
 	const int nblk128 = n / 128 + 2;
 	if (precision == HPLAI_F32_F8) {
 		c->ld8 = round_up(b, 128);
+		c->ld8g = c->gcap * c->ld8;
 		for (int i = 0; i < 2; ++i) {
-			CTX_ALLOC(c->L8[i], static_cast<size_t>(c->ld8) * n);
-			CTX_ALLOC(c->U8[i], static_cast<size_t>(c->ld8) * n);
+			CTX_ALLOC(c->L8[i], static_cast<size_t>(c->ld8g) * n);
+			CTX_ALLOC(c->U8[i], static_cast<size_t>(c->ld8g) * n);
 			CTX_ALLOC(c->sl[i], sizeof(float) * nblk128);
 			CTX_ALLOC(c->su[i], sizeof(float) * nblk128);
+		}
+		if (c->gcap == 2) {
+			CTX_ALLOC(c->L8s, static_cast<size_t>(c->ld8) * n);
+			CTX_ALLOC(c->U8s, static_cast<size_t>(c->ld8) * n);
+			CTX_ALLOC(c->sls, sizeof(float) * nblk128);
+			CTX_ALLOC(c->sus, sizeof(float) * nblk128);
 		}
 		CTX_ALLOC(c->qbits, sizeof(unsigned) * nblk128);
 	}
@@ -306,19 +346,33 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		return HPLAI_ECUDA;
 	}
 	int s = HPLAI_OK;
+	auto finish = [&](SchurMaps &m) {
+		if (s == HPLAI_OK) s = schur_set_cmap(&m, c->A, n, n, c->lda);
+		m.status = c->kstatus;
+		m.deck_base = c->deck;
+		m.deck_ld = c->lda;
+	};
 	for (int i = 0; i < 2 && s == HPLAI_OK; ++i) {
-		s = schur_make_maps(&c->maps[i], c->Lh[i], n, c->ldh, c->Uh[i], n, c->ldh, b);
-		if (s == HPLAI_OK) s = schur_set_cmap(&c->maps[i], c->A, n, n, c->lda);
-		c->maps[i].status = c->kstatus;
-		c->maps[i].deck_base = c->deck;
-		c->maps[i].deck_ld = c->lda;
-		if (s == HPLAI_OK && precision == HPLAI_F32_F8) {
-			s = schur_make_maps_fp8(&c->maps8[i], c->L8[i], n, c->ld8, c->U8[i], n, c->ld8, b);
-			if (s == HPLAI_OK) s = schur_set_cmap(&c->maps8[i], c->A, n, n, c->lda);
-			c->maps8[i].status = c->kstatus;
-			c->maps8[i].deck_base = c->deck;
-			c->maps8[i].deck_ld = c->lda;
+		for (int h = 0; h < c->gcap && s == HPLAI_OK; ++h) {
+			s = schur_make_maps(&c->maps[i][h], c->Lh[i] + h * c->ldh, n, c->ldg, c->Uh[i] + h * c->ldh, n, c->ldg, b);
+			finish(c->maps[i][h]);
 		}
+		if (s == HPLAI_OK && c->gcap == 2) {
+			s = schur_make_maps(&c->mapsg[i], c->Lh[i], n, c->ldg, c->Uh[i], n, c->ldg, 2 * b);
+			finish(c->mapsg[i]);
+		}
+		if (s == HPLAI_OK && precision == HPLAI_F32_F8) {
+			s = schur_make_maps_fp8(&c->maps8[i], c->L8[i], n, c->ld8g, c->U8[i], n, c->ld8g, b);
+			finish(c->maps8[i]);
+			if (s == HPLAI_OK && c->gcap == 2) {
+				s = schur_make_maps_fp8(&c->maps8g[i], c->L8[i], n, c->ld8g, c->U8[i], n, c->ld8g, 2 * b);
+				finish(c->maps8g[i]);
+			}
+		}
+	}
+	if (s == HPLAI_OK && precision == HPLAI_F32_F8 && c->gcap == 2) {
+		s = schur_make_maps_fp8(&c->maps8s, c->L8s, n, c->ld8, c->U8s, n, c->ld8, b);
+		finish(c->maps8s);
 	}
 	if (s == HPLAI_OK) {
 		float *base = c->tcbuf;
@@ -383,12 +437,16 @@ bool f16_panel_form(const hplai_ctx *c, bool simt)
 }
 
 // Factor the diagonal block of step k and form its two panels with their
-// FP16 copies in buffer `buf` (getrf_nopiv + update_left/right_panels +
-// convert_left/right_panels, panel_trf.hpp:143-233).
-int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStream_t st, PhaseEvents &pe)
+// FP16 copies in slot `slot` of group buffer `buf` (getrf_nopiv +
+// update_left/right_panels + convert_left/right_panels,
+// panel_trf.hpp:143-233).  Precision form: the e4m3 copies for the next
+// update that reads this panel -- with one-panel groups this panel's own, in
+// a group's first slot the single copy for the update of the group's second
+// block, in its second slot the group's shared copy of both panels.
+int panel_step(hplai_ctx *c, int k, int buf, int slot, bool simt, int side_ctas, cudaStream_t st, PhaseEvents &pe)
 {
 	const int n = c->n, b = c->b;
-	const int64_t lda = c->lda, ldh = c->ldh;
+	const int64_t lda = c->lda, ldg = c->ldg;
 	const int64_t kb = static_cast<int64_t>(k) * b;
 	float *diag = c->A + kb + kb * lda;
 	HPLAI_TRY(pe.record(st, HPLAI_PH_DIAG_LU));
@@ -399,60 +457,143 @@ int panel_step(hplai_ctx *c, int k, int buf, bool simt, int side_ctas, cudaStrea
 	const bool f16_panels = f16_panel_form(c, simt);
 	const uint16_t *deck = f16_panels ? c->deck : nullptr;   // folded into the FP16 panel copies
 	const float inv_dscale = c->deck ? 1.0f / c->dscale : 0.f;
+	uint16_t *lslot = c->Lh[buf] + slot * c->ldh, *uslot = c->Uh[buf] + slot * c->ldh;
 	HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_L));
 	if (simt) {
-		HPLAI_TRY(launch_trsm_right_upper(rem, b, diag, lda, diag + b, lda, c->Lh[buf] + (kb + b) * ldh, ldh, 1.0f, st));
+		HPLAI_TRY(launch_trsm_right_upper(rem, b, diag, lda, diag + b, lda, lslot + (kb + b) * ldg, ldg, 1.0f, st));
 	} else if (f16_panels) {
 		// FP16 panel products (the Schur update reads only the e4m3 copies made below)
 		HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st, false));
-		HPLAI_TRY(launch_lpanel_f16(c->tc, c->maps[buf], static_cast<int>(kb), rem, c->A, lda, c->Lh[buf], c->Uh[buf],
-			ldh, deck, inv_dscale, side_ctas, st));
+		HPLAI_TRY(launch_lpanel_f16(c->tc, c->maps[buf][slot], static_cast<int>(kb), rem, c->A, lda, lslot, uslot, ldg,
+			deck, inv_dscale, side_ctas, st));
 	} else {
 		HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st));
 		// the precision form's Schur update reads the e4m3 copies only: no FP16 copy
-		uint16_t *lh = c->precision == HPLAI_F32_F8 ? nullptr : c->Lh[buf] + (kb + b) * ldh;
-		HPLAI_TRY(launch_lpanel_tc(c->tc, rem, diag + b, lda, lh, ldh, 1.0f, side_ctas, st));
+		uint16_t *lh = c->precision == HPLAI_F32_F8 ? nullptr : lslot + (kb + b) * ldg;
+		HPLAI_TRY(launch_lpanel_tc(c->tc, rem, diag + b, lda, lh, ldg, 1.0f, side_ctas, st));
 	}
 	HPLAI_TRY(pe.end(st));
 	HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_R));
 	if (simt) {
 		HPLAI_TRY(launch_trsm_left_lower(b, rem, diag, lda, diag + static_cast<int64_t>(b) * lda, lda,
-			c->Uh[buf] + (kb + b) * ldh, ldh, 1.0f, st));
+			uslot + (kb + b) * ldg, ldg, 1.0f, st));
 	} else if (f16_panels) {
-		HPLAI_TRY(launch_upanel_f16(c->tc, c->maps[buf], static_cast<int>(kb), rem, c->A, lda, c->Uh[buf], ldh, deck,
+		HPLAI_TRY(launch_upanel_f16(c->tc, c->maps[buf][slot], static_cast<int>(kb), rem, c->A, lda, uslot, ldg, deck,
 			inv_dscale, side_ctas, st));
 	} else {
-		uint16_t *uh = c->precision == HPLAI_F32_F8 ? nullptr : c->Uh[buf] + (kb + b) * ldh;
-		HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, uh, ldh, 1.0f, side_ctas, st));
+		uint16_t *uh = c->precision == HPLAI_F32_F8 ? nullptr : uslot + (kb + b) * ldg;
+		HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, uh, ldg, 1.0f, side_ctas, st));
 	}
 	if (c->precision == HPLAI_F32_F8) {
-		HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, c->qbits, c->L8[buf] + (kb + b) * c->ld8, c->ld8,
-			c->sl[buf], st));
-		HPLAI_TRY(launch_quantize_upanel(rem, b, diag + static_cast<int64_t>(b) * lda, lda, c->qbits,
-			c->U8[buf] + (kb + b) * c->ld8, c->ld8, c->su[buf], st));
+		if (c->group == 1) {
+			HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, c->qbits, c->L8[buf] + (kb + b) * c->ld8g, c->ld8g,
+				c->sl[buf], st));
+			HPLAI_TRY(launch_quantize_upanel(rem, b, diag + static_cast<int64_t>(b) * lda, lda, c->qbits,
+				c->U8[buf] + (kb + b) * c->ld8g, c->ld8g, c->su[buf], st));
+		} else if (slot == 0) {
+			HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, c->qbits, c->L8s + (kb + b) * c->ld8, c->ld8, c->sls,
+				st));
+			HPLAI_TRY(launch_quantize_upanel(rem, b, diag + static_cast<int64_t>(b) * lda, lda, c->qbits,
+				c->U8s + (kb + b) * c->ld8, c->ld8, c->sus, st));
+		} else {
+			// [L_k-1 L_k] (rows kb+b.., A columns kb-b .. kb+b-1) and [U_k-1; U_k]
+			// (A rows kb-b .. kb+b-1, columns kb+b..) with factors over both panels
+			HPLAI_TRY(launch_quantize_lpanel(rem, 2 * b, diag + b - static_cast<int64_t>(b) * lda, lda, c->qbits,
+				c->L8[buf] + (kb + b) * c->ld8g, c->ld8g, c->sl[buf], st));
+			HPLAI_TRY(launch_quantize_upanel(rem, 2 * b, diag - b + static_cast<int64_t>(b) * lda, lda, c->qbits,
+				c->U8[buf] + (kb + b) * c->ld8g, c->ld8g, c->su[buf], st));
+		}
 	}
 	HPLAI_TRY(pe.end(st));
 	return HPLAI_OK;
 }
 
-// C -= L_k U_k on the rectangle of rows [r0, r1) and columns [c0, c1); the
-// step's panels start at row/column p0.
-int schur_region(hplai_ctx *c, int buf, int p0, int r0, int r1, int c0, int c1, int max_ctas, cudaStream_t st,
+// The operands of one trailing update: FP16 maps, or e4m3 maps with their
+// factors (block 0 of sl/su starting at row/column s0).
+struct Operands {
+	const SchurMaps *m = nullptr;
+	bool fp8 = false;
+	const float *sl = nullptr, *su = nullptr;
+	int s0 = 0;
+};
+
+// C -= L U on the rectangle of rows [r0, r1) and columns [c0, c1).
+int schur_region(hplai_ctx *c, const Operands &op, int r0, int r1, int c0, int c1, int max_ctas, cudaStream_t st,
 	PhaseEvents &pe)
 {
 	if (r1 <= r0 || c1 <= c0) return HPLAI_OK;
 	HPLAI_TRY(pe.record(st, HPLAI_PH_GEMM_UPDATE));
 	float *cp = c->A + r0 + static_cast<int64_t>(c0) * c->lda;
 	if (c->deck)
-		HPLAI_TRY(launch_schur_deck(c->precision == HPLAI_F32_F8 ? c->maps8[buf] : c->maps[buf],
-			c->precision == HPLAI_F32_F8, c->sl[buf], p0, c->su[buf], p0, r0, c0, r1 - r0, c1 - c0, r0, c0, c->dscale,
+		HPLAI_TRY(launch_schur_deck(*op.m, op.fp8, op.sl, op.s0, op.su, op.s0, r0, c0, r1 - r0, c1 - c0, r0, c0,
+			c->dscale, max_ctas, st));
+	else if (op.fp8)
+		HPLAI_TRY(launch_schur_fp8(*op.m, op.sl, op.s0, op.su, op.s0, r0, c0, r1 - r0, c1 - c0, cp, c->lda, r0, c0,
 			max_ctas, st));
-	else if (c->precision == HPLAI_F32_F8)
-		HPLAI_TRY(launch_schur_fp8(c->maps8[buf], c->sl[buf], p0, c->su[buf], p0, r0, c0, r1 - r0, c1 - c0, cp, c->lda,
-			r0, c0, max_ctas, st));
 	else
-		HPLAI_TRY(launch_schur(c->maps[buf], r0, c0, r1 - r0, c1 - c0, cp, c->lda, r0, c0, max_ctas, st));
+		HPLAI_TRY(launch_schur(*op.m, r0, c0, r1 - r0, c1 - c0, cp, c->lda, r0, c0, max_ctas, st));
 	HPLAI_TRY(pe.end(st));
+	return HPLAI_OK;
+}
+
+// The operands of the update by the whole group in buffer q whose first
+// trailing row/column is e * b.
+Operands group_operands(const hplai_ctx *c, int q, int e)
+{
+	Operands op;
+	op.fp8 = c->precision == HPLAI_F32_F8;
+	if (op.fp8) {
+		op.m = c->group == 2 ? &c->maps8g[q] : &c->maps8[q];
+		op.sl = c->sl[q];
+		op.su = c->su[q];
+		op.s0 = e * c->b;
+	} else {
+		op.m = c->group == 2 ? &c->mapsg[q] : &c->maps[q][0];
+	}
+	return op;
+}
+
+// The operands of the update of a group's second block by its first panel
+// alone (panel e in slot 0 of buffer q).
+Operands first_panel_operands(const hplai_ctx *c, int q, int e)
+{
+	Operands op;
+	op.fp8 = c->precision == HPLAI_F32_F8;
+	if (op.fp8) {
+		op.m = &c->maps8s;
+		op.sl = c->sls;
+		op.su = c->sus;
+		op.s0 = (e + 1) * c->b;
+	} else {
+		op.m = &c->maps[q][0];
+	}
+	return op;
+}
+
+// Everything block j needs before it is factored, on the side stream: with
+// two-panel groups the update of a group's second block by the group's first
+// panel; then, with the FP16 deck, the deck folded into the block column and
+// row (A + deck / dscale; the FP16 panel copies fold the off-diagonal part
+// themselves, so then only the diagonal block).
+int prepare_block(hplai_ctx *c, int j, int first, int q, bool simt, int side_ctas, cudaStream_t st, PhaseEvents &pe)
+{
+	const int n = c->n, b = c->b;
+	const int r1 = j * b, r2 = (j + 1) * b;
+	if (j > first) {
+		const Operands op = first_panel_operands(c, q, first);
+		HPLAI_TRY(schur_region(c, op, r1, n, r1, r2, side_ctas, st, pe));
+		HPLAI_TRY(schur_region(c, op, r1, r2, r2, n, side_ctas, st, pe));
+	}
+	if (c->deck && j > 0) {
+		HPLAI_TRY(pe.record(st, HPLAI_PH_LAZY_INIT));
+		if (f16_panel_form(c, simt)) {
+			HPLAI_TRY(launch_deck_apply(r1, r2, r1, r2, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
+		} else {
+			HPLAI_TRY(launch_deck_apply(r1, n, r1, r2, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
+			HPLAI_TRY(launch_deck_apply(r1, r2, r2, n, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
+		}
+		HPLAI_TRY(pe.end(st));
+	}
 	return HPLAI_OK;
 }
 
@@ -463,6 +604,8 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	if (!c) return HPLAI_EINVAL;
 	if (!c->have_inputs) return HPLAI_ESTATE;
 	const int n = c->n, b = c->b, nb = c->nb;
+	c->group = ((c->flags & HPLAI_FLAG_GROUP2) && c->gcap == 2) ? 2 : 1;
+	const int G = c->group;
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->kstatus, 0, 2 * sizeof(unsigned), c->st));
 	if (c->deck) HPLAI_CUDA_TRY(cudaMemsetAsync(c->deck, 0, sizeof(uint16_t) * static_cast<size_t>(c->lda) * n, c->st));
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->getrf_work, 0, sizeof(uint32_t), c->st));   // its status word
@@ -470,14 +613,16 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	const bool serial = (c->flags & HPLAI_FLAG_LOOKAHEAD) == 0;
 	for (double &v : c->phase_ms) v = 0.0;
 	PhaseEvents pe;
-	// Right-looking blocked LU without pivoting with one-step look-ahead
-	// (panel_lu_async / RDMAPanelLU::run, panel_trf.hpp:434-858).  The update
-	// of step k is split into the next panel's block column and block row
-	// (first) and the rest of the trailing matrix (after).  With
-	// HPLAI_FLAG_LOOKAHEAD step k+1's diagonal block and panels are formed on
-	// the side stream as soon as the first part is done, overlapping the
-	// second, which then leaves side_sms SMs to the side stream; otherwise
-	// everything runs in the same order on one stream.
+	// Right-looking blocked LU without pivoting with look-ahead
+	// (panel_lu_async / RDMAPanelLU::run, panel_trf.hpp:434-858), by groups
+	// of G panels.  The update by group [s, s+G) of the trailing matrix
+	// (rows and columns from e = s+G blocks on) is split into the next
+	// group's block columns and rows (first) and the rest (after).  The next
+	// group's panels are formed once the first part is done: block by block,
+	// the group's second block first receiving its first panel's update.
+	// With HPLAI_FLAG_LOOKAHEAD they are formed on the side stream while the
+	// main stream applies the rest, which then leaves side_sms SMs to the
+	// side stream; otherwise everything runs in the same order on one stream.
 	const int kSideSms = c->side_sms;
 	cudaStream_t st = c->st, sd = serial ? c->st : c->st2;
 	const int side_ctas = serial ? 0 : kSideSms;
@@ -487,35 +632,31 @@ extern "C" int hplai_factor(hplai_ctx *c)
 		if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	}
 	const int main_ctas = (serial || sms <= 2 * kSideSms) ? 0 : sms - kSideSms;
-	// the side stream starts from the generated matrix
+	// the side stream starts from the generated matrix: group 0's panels
 	HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));
 	HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_next, 0));
-	HPLAI_TRY(panel_step(c, 0, 0, simt, side_ctas, sd, pe));
-	for (int k = 0; k + 1 < nb; ++k) {
-		const int buf = k & 1;
-		const int r1 = (k + 1) * b, r2 = (k + 2) * b;
+	for (int j = 0; j < G && j < nb; ++j) {
+		HPLAI_TRY(prepare_block(c, j, 0, 0, simt, side_ctas, sd, pe));
+		HPLAI_TRY(panel_step(c, j, 0, j, simt, side_ctas, sd, pe));
+	}
+	for (int s = 0; s + G < nb; s += G) {
+		const int q = (s / G) & 1;
+		const int e = s + G, ne = std::min(G, nb - e);
+		const int r1 = e * b, r2 = (e + ne) * b;
+		const Operands op = group_operands(c, q, e);
 		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_panel, sd));
 		HPLAI_CUDA_TRY(cudaStreamWaitEvent(st, c->ev_panel, 0));
-		// the next panel's block column (rows r1..n) and block row (columns r2..n)
-		HPLAI_TRY(schur_region(c, buf, r1, r1, n, r1, r2, 0, st, pe));
-		HPLAI_TRY(schur_region(c, buf, r1, r1, r2, r2, n, 0, st, pe));
-		if (c->deck) {
-			// the next block column and block row become A + deck / dscale (the
-			// FP16 panel copies fold the deck in themselves: the diagonal block only)
-			HPLAI_TRY(pe.record(st, HPLAI_PH_LAZY_INIT));
-			if (f16_panel_form(c, simt)) {
-				HPLAI_TRY(launch_deck_apply(r1, r2, r1, r2, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
-			} else {
-				HPLAI_TRY(launch_deck_apply(r1, n, r1, r2, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
-				HPLAI_TRY(launch_deck_apply(r1, r2, r2, n, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
-			}
-			HPLAI_TRY(pe.end(st));
-		}
+		// the next group's block columns (rows r1..n) and block rows (columns r2..n)
+		HPLAI_TRY(schur_region(c, op, r1, n, r1, r2, 0, st, pe));
+		HPLAI_TRY(schur_region(c, op, r1, r2, r2, n, 0, st, pe));
 		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));
 		HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_next, 0));
-		HPLAI_TRY(panel_step(c, k + 1, buf ^ 1, simt, side_ctas, sd, pe));
+		for (int j = e; j < e + ne; ++j) {
+			HPLAI_TRY(prepare_block(c, j, e, q ^ 1, simt, side_ctas, sd, pe));
+			HPLAI_TRY(panel_step(c, j, q ^ 1, j - e, simt, side_ctas, sd, pe));
+		}
 		// the rest of the trailing matrix
-		HPLAI_TRY(schur_region(c, buf, r1, r2, n, r2, n, main_ctas, st, pe));
+		HPLAI_TRY(schur_region(c, op, r2, n, r2, n, main_ctas, st, pe));
 	}
 	HPLAI_CUDA_TRY(cudaEventRecord(c->ev_panel, sd));
 	HPLAI_CUDA_TRY(cudaStreamWaitEvent(st, c->ev_panel, 0));
@@ -793,10 +934,12 @@ int hplai_ctx_solve_stream_rhs(hplai_ctx *c, int col, double *x, int maxit, hpla
 
 // The project's own tuner in place of lda_tuner (lda_tuner.hpp:9-45, whose
 // call the reference leaves commented out): the factorisation is timed on
-// this context (regenerated from `seed` before each trial) serially and with
-// look-ahead at several side-stream SM counts; the fastest becomes the
-// context's schedule.  Tile shapes are compile-time constants of the kernels
-// (measured sweeps chose them), so the run-time choice is the schedule.
+// this context (regenerated from `seed` before each trial) under each
+// schedule -- one- or two-panel groups (the trailing update's K = b or 2b),
+// serial or with look-ahead at several side-stream SM counts -- after one
+// discarded warm-up factorisation; the two fastest are timed twice more and
+// the one with the lowest median becomes the context's schedule.  Every
+// trial is kept for hplai_get_autotune_log.
 extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, int *side_sms_out, double *ms_out)
 {
 	if (!c) return HPLAI_EINVAL;
@@ -805,35 +948,61 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 		int dev = 0;
 		if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	}
-	struct Trial {
-		bool lookahead;
+	struct Cand {
+		unsigned sched;   // HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2 bits
 		int side;
+		std::vector<double> ms;
 	};
-	const Trial trials[] = {{false, 20}, {true, 16}, {true, 24}, {true, 32}, {true, 48}};
-	const unsigned flags0 = c->flags, base_flags = c->flags & ~HPLAI_FLAG_LOOKAHEAD;
+	std::vector<Cand> cands;
+	for (int g = 1; g <= c->gcap; ++g) {
+		const unsigned gf = g == 2 ? HPLAI_FLAG_GROUP2 : 0u;
+		cands.push_back({gf, 20, {}});
+		for (int side : {16, 24, 32})
+			if (sms > 2 * side) cands.push_back({gf | HPLAI_FLAG_LOOKAHEAD, side, {}});
+	}
+	const unsigned sched_bits = HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2;
+	const unsigned flags0 = c->flags, base_flags = c->flags & ~sched_bits;
 	const int side0 = c->side_sms;
-	double best = -1.0;
-	Trial pick = trials[0];
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
 	HPLAI_CUDA_TRY(cudaEventCreate(&e0));
 	HPLAI_CUDA_TRY(cudaEventCreate(&e1));
-	int rc = HPLAI_OK;
-	for (const Trial &t : trials) {
-		if (t.lookahead && sms <= 2 * t.side) continue;
-		c->flags = base_flags | (t.lookahead ? HPLAI_FLAG_LOOKAHEAD : 0u);
+	c->tune_log.clear();
+	auto trial = [&](const Cand &t, double *ms) -> int {
+		c->flags = base_flags | t.sched;
 		c->side_sms = t.side;
-		rc = hplai_generate(c, seed);
-		if (rc == HPLAI_OK && cudaEventRecord(e0, c->st) != cudaSuccess) rc = HPLAI_ECUDA;
-		if (rc == HPLAI_OK) rc = hplai_factor(c);
-		if (rc == HPLAI_OK && cudaEventRecord(e1, c->st) != cudaSuccess) rc = HPLAI_ECUDA;
-		if (rc == HPLAI_OK && cudaEventSynchronize(e1) != cudaSuccess) rc = HPLAI_ECUDA;
-		float ms = 0.f;
-		if (rc == HPLAI_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = HPLAI_ECUDA;
-		if (rc != HPLAI_OK) break;
-		if (best < 0.0 || ms < best) {
-			best = ms;
-			pick = t;
-		}
+		HPLAI_TRY(hplai_generate(c, seed));
+		HPLAI_CUDA_TRY(cudaEventRecord(e0, c->st));
+		HPLAI_TRY(hplai_factor(c));
+		HPLAI_CUDA_TRY(cudaEventRecord(e1, c->st));
+		HPLAI_CUDA_TRY(cudaEventSynchronize(e1));
+		float f = 0.f;
+		HPLAI_CUDA_TRY(cudaEventElapsedTime(&f, e0, e1));
+		*ms = f;
+		c->tune_log.push_back({c->flags, t.side, f});
+		return HPLAI_OK;
+	};
+	auto median = [](std::vector<double> v) {
+		std::sort(v.begin(), v.end());
+		return v[v.size() / 2];
+	};
+	int rc = HPLAI_OK;
+	double warm = 0.0;
+	rc = trial(cands[0], &warm);   // discarded: first-touch and module loading
+	for (size_t i = 0; i < cands.size() && rc == HPLAI_OK; ++i) {
+		double ms = 0.0;
+		rc = trial(cands[i], &ms);
+		cands[i].ms.push_back(ms);
+	}
+	if (rc == HPLAI_OK) {
+		std::vector<size_t> order(cands.size());
+		for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+		std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cands[a].ms[0] < cands[b].ms[0]; });
+		for (size_t r = 0; r < std::min<size_t>(2, order.size()) && rc == HPLAI_OK; ++r)
+			for (int rep = 0; rep < 2 && rc == HPLAI_OK; ++rep) {
+				double ms = 0.0;
+				rc = trial(cands[order[r]], &ms);
+				cands[order[r]].ms.push_back(ms);
+			}
 	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
@@ -842,13 +1011,36 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 		c->side_sms = side0;
 		return rc;
 	}
-	c->flags = base_flags | (pick.lookahead ? HPLAI_FLAG_LOOKAHEAD : 0u);
-	c->side_sms = pick.side;
+	size_t pick = 0;
+	double best = -1.0;
+	for (size_t i = 0; i < cands.size(); ++i) {
+		if (cands[i].ms.size() < 3) continue;   // only the re-timed finalists
+		const double m = median(cands[i].ms);
+		if (best < 0.0 || m < best) {
+			best = m;
+			pick = i;
+		}
+	}
+	c->flags = base_flags | cands[pick].sched;
+	c->side_sms = cands[pick].side;
 	// the context is left generated and unfactored, as after hplai_generate
 	HPLAI_TRY(hplai_generate(c, seed));
 	if (flags_out) *flags_out = c->flags;
 	if (side_sms_out) *side_sms_out = c->side_sms;
 	if (ms_out) *ms_out = best;
+	return HPLAI_OK;
+}
+
+extern "C" int hplai_get_autotune_log(hplai_ctx *c, unsigned *flags, int *side_sms, double *ms, int cap, int *count)
+{
+	if (!c) return HPLAI_EINVAL;
+	const int m = static_cast<int>(c->tune_log.size());
+	for (int i = 0; i < m && i < cap; ++i) {
+		if (flags) flags[i] = c->tune_log[i].flags;
+		if (side_sms) side_sms[i] = c->tune_log[i].side_sms;
+		if (ms) ms[i] = c->tune_log[i].ms;
+	}
+	if (count) *count = m;
 	return HPLAI_OK;
 }
 

@@ -102,6 +102,8 @@ static int usage()
 		"   --fp8                   e4m3 Schur update with GMRES refinement.\n"
 		"   --gmres                 GMRES refinement instead of the classical correction.\n"
 		"   --lookahead             Factor the next panel while the trailing update runs.\n"
+		"   --group <g>             Panels per trailing update: 1 (default) or 2 (K = 2b; b %% 128 == 0).\n"
+		"   --autotune              Choose the schedule (groups, look-ahead) by timing it first.\n"
 		"   --checksum              Print sums of |diag|, |upper|, |lower| of the factors after the LU.\n"
 		"   --job-id <id>           Job number in the name of the Timerdump file (default 0).\n"
 		"   --help or -h            Print this message.\n"
@@ -117,7 +119,7 @@ int main(int argc, char **argv)
 	unsigned long long seed = 42;
 	int precision = HPLAI_F32_F16, mode = HPLAI_IR;
 	unsigned flags = 0;
-	bool checksum = false;
+	bool checksum = false, autotune = false;
 	int jobid = 0;
 	if (argc > 1) n = std::atoi(argv[1]);
 	if (argc > 2) b = std::atoi(argv[2]);
@@ -131,6 +133,10 @@ int main(int argc, char **argv)
 		else if (!std::strcmp(argv[i], "--fp8")) { precision = HPLAI_F32_F8; mode = HPLAI_GMRES; }
 		else if (!std::strcmp(argv[i], "--gmres")) mode = HPLAI_GMRES;
 		else if (!std::strcmp(argv[i], "--lookahead")) flags |= HPLAI_FLAG_LOOKAHEAD;
+		else if (!std::strcmp(argv[i], "--group") && i + 1 < argc) {
+			if (std::atoi(argv[++i]) == 2) flags |= HPLAI_FLAG_GROUP2;
+		}
+		else if (!std::strcmp(argv[i], "--autotune")) autotune = true;
 		else if (!std::strcmp(argv[i], "--checksum")) checksum = true;
 		else if (!std::strcmp(argv[i], "--numa") || !std::strcmp(argv[i], "--numa-map") ||
 			!std::strcmp(argv[i], "--nbuf")) ++i;
@@ -165,6 +171,20 @@ int main(int argc, char **argv)
 	if (rc != HPLAI_OK) {
 		std::fprintf(stderr, "hplai_create(n=%d, b=%d): %s\n", n, b, hplai_status_string(rc));
 		return 1;
+	}
+	if (autotune) {
+		unsigned tf = 0;
+		int side = 0;
+		double tms = 0.0;
+		rc = hplai_autotune(ctx, seed, &tf, &side, &tms);
+		if (rc != HPLAI_OK) {
+			std::fprintf(stderr, "hplai_autotune: %s\n", hplai_status_string(rc));
+			return 1;
+		}
+		flags = tf;
+		std::printf("autotune: %d panel(s) per update, %s, factorisation %.3f ms\n", (tf & HPLAI_FLAG_GROUP2) ? 2 : 1,
+			(tf & HPLAI_FLAG_LOOKAHEAD) ? "look-ahead" : "serial", tms);
+		if (tf & HPLAI_FLAG_LOOKAHEAD) std::printf("autotune: %d side-stream SMs\n", side);
 	}
 	auto tg0 = std::chrono::steady_clock::now();
 	rc = hplai_generate(ctx, seed);

@@ -127,7 +127,8 @@ __global__ void __launch_bounds__(256) split_n_kernel(int rows, int kdim, const 
 }
 
 // FP16 K-major copies of a panel for the precision form's panel products:
-// out[r*ldh + k] = half_rn(x(r, k)) for k < kdim, zero for kdim <= k < ldh.
+// out[r*pitch + k] = half_rn(x(r, k)) for k < kdim, zero for kdim <= k < width
+// (width <= pitch: a panel may be one slot of a wider group buffer).
 // (The precision form's Schur operands are e4m3, so FP16 operands, 11
 // significant bits, lose nothing that matters and run the panel products at
 // the FP16 tensor rate with half the bytes of TF32.)  With the FP16 deck,
@@ -154,7 +155,7 @@ __device__ __forceinline__ float4 load4_deck(const float *src, const __half *dec
 // through shared memory: float4 loads along r, half2 stores along k.
 __global__ void __launch_bounds__(256) panel_f16_t_kernel(int rows, int kdim, const float *__restrict__ src,
 	int64_t lds, const __half *__restrict__ deck, int64_t ldd, float inv_scale, __half *__restrict__ out,
-	int64_t ldh)
+	int64_t pitch, int width)
 {
 	__shared__ float tile[64][65];   // tile[k][r]
 	const int r0 = blockIdx.x * 64, k0 = blockIdx.y * 64;
@@ -177,8 +178,8 @@ __global__ void __launch_bounds__(256) panel_f16_t_kernel(int rows, int kdim, co
 	for (int q = 0; q < 8; ++q) {
 		const int idx = t + 256 * q, rr = idx >> 5, kp = (idx & 31) * 2;
 		const int r = r0 + rr, k = k0 + kp;
-		if (r < rows && k < ldh)
-			*reinterpret_cast<__half2 *>(out + static_cast<int64_t>(r) * ldh + k) =
+		if (r < rows && k < width)
+			*reinterpret_cast<__half2 *>(out + static_cast<int64_t>(r) * pitch + k) =
 				__floats2half2_rn(tile[kp][rr], tile[kp + 1][rr]);
 	}
 }
@@ -186,9 +187,9 @@ __global__ void __launch_bounds__(256) panel_f16_t_kernel(int rows, int kdim, co
 // A_row seen by columns: element (r, k) at src[r*lds + k]; no transpose.
 __global__ void __launch_bounds__(256) panel_f16_n_kernel(int rows, int kdim, const float *__restrict__ src,
 	int64_t lds, const __half *__restrict__ deck, int64_t ldd, float inv_scale, __half *__restrict__ out,
-	int64_t ldh)
+	int64_t pitch, int width)
 {
-	const int groups = static_cast<int>(ldh / 4);
+	const int groups = width / 4;
 	const int64_t total = static_cast<int64_t>(rows) * groups;
 	for (int64_t e = static_cast<int64_t>(blockIdx.x) * 256 + threadIdx.x; e < total;
 		e += static_cast<int64_t>(gridDim.x) * 256) {
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(256) panel_f16_n_kernel(int rows, int kdim, co
 		uint2 w;
 		w.x = *reinterpret_cast<const uint32_t *>(&h01);
 		w.y = *reinterpret_cast<const uint32_t *>(&h23);
-		*reinterpret_cast<uint2 *>(out + static_cast<int64_t>(r) * ldh + k) = w;
+		*reinterpret_cast<uint2 *>(out + static_cast<int64_t>(r) * pitch + k) = w;
 	}
 }
 
@@ -240,23 +241,24 @@ __device__ __forceinline__ float f16_tri_scale(unsigned bits)
 }
 
 // The inverted triangles as FP16 Schur operands, scaled by a power of two:
-//   uh[j*ldh + p] = half(s_u U11^{-1}(p, j))   (U operand of A_col U11^{-1})
-//   lh[i*ldh + p] = half(s_l L11^{-1}(i, p))   (L operand of L11^{-1} A_row)
-// and oscale[0..1] = 1/s_u, 1/s_l (exact) for the products' epilogues.
+//   uh[j*pitch + p] = half(s_u U11^{-1}(p, j))   (U operand of A_col U11^{-1})
+//   lh[i*pitch + p] = half(s_l L11^{-1}(i, p))   (L operand of L11^{-1} A_row)
+// for p < width (zero for b <= p), and oscale[0..1] = 1/s_u, 1/s_l (exact)
+// for the products' epilogues.
 __global__ void __launch_bounds__(256) tri_f16_kernel(int b, const float *__restrict__ xu,
 	const float *__restrict__ xl, int64_t ldp, const unsigned *__restrict__ amax, __half *__restrict__ uh,
-	__half *__restrict__ lh, int64_t ldh, float *__restrict__ oscale)
+	__half *__restrict__ lh, int64_t pitch, int width, float *__restrict__ oscale)
 {
 	const bool lower = blockIdx.y != 0;
 	const float *x = lower ? xl : xu;
 	__half *o = lower ? lh : uh;
 	const float sc = f16_tri_scale(amax[blockIdx.y]);
 	if (blockIdx.x == 0 && threadIdx.x == 0) oscale[blockIdx.y] = 1.f / sc;
-	const int64_t total = static_cast<int64_t>(b) * ldh;
+	const int64_t total = static_cast<int64_t>(b) * width;
 	for (int64_t e = blockIdx.x * 256 + threadIdx.x; e < total; e += static_cast<int64_t>(gridDim.x) * 256) {
-		const int pp = static_cast<int>(e % ldh), j = static_cast<int>(e / ldh);
+		const int pp = static_cast<int>(e % width), j = static_cast<int>(e / width);
 		const float v = (pp <= j && pp < b) ? x[static_cast<int64_t>(j) * ldp + pp] * sc : 0.f;
-		o[e] = __float2half_rn(v);
+		o[static_cast<int64_t>(j) * pitch + pp] = __float2half_rn(v);
 	}
 }
 
@@ -841,7 +843,9 @@ int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 	uint16_t *lh, uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st)
 {
 	if (rem <= 0) return HPLAI_OK;
-	if (!t.f16_amax || !t.f16_oscale || ldh % 64 || t.b % 4 || kb % 4 || rem % 4 || lda % 4) return HPLAI_EINVAL;
+	const int width = (t.b + 63) / 64 * 64;   // the panel's slot in a buffer of row pitch ldh
+	if (!t.f16_amax || !t.f16_oscale || ldh % 64 || ldh < width || t.b % 4 || kb % 4 || rem % 4 || lda % 4)
+		return HPLAI_EINVAL;
 	const int b = t.b;
 	// the inverted triangles into rows kb .. kb+b-1 of the FP16 panel buffers
 	// (rows the step's Schur update never reads)
@@ -852,15 +856,15 @@ int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	tri_f16_kernel<<<dim3(tb, 2), 256, 0, st>>>(b, t.xu, t.xl, t.ldp, t.f16_amax,
 		reinterpret_cast<__half *>(uh) + static_cast<int64_t>(kb) * ldh,
-		reinterpret_cast<__half *>(lh) + static_cast<int64_t>(kb) * ldh, ldh, t.f16_oscale);
+		reinterpret_cast<__half *>(lh) + static_cast<int64_t>(kb) * ldh, ldh, width, t.f16_oscale);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// A_col (rows kb+b.., columns kb..kb+b-1) -> FP16 K-major rows kb+b.. of lh
 	const int64_t kbl = kb;
 	float *acol = a + (kbl + b) + kbl * lda;
 	const __half *dcol = deck ? reinterpret_cast<const __half *>(deck) + (kbl + b) + kbl * lda : nullptr;
-	panel_f16_t_kernel<<<dim3((rem + 63) / 64, static_cast<unsigned>(ldh / 64)), 256, 0, st>>>(rem, b, acol, lda,
-		dcol, lda, inv_dscale, reinterpret_cast<__half *>(lh) + (kbl + b) * ldh, ldh);
+	panel_f16_t_kernel<<<dim3((rem + 63) / 64, static_cast<unsigned>(width / 64)), 256, 0, st>>>(rem, b, acol, lda,
+		dcol, lda, inv_dscale, reinterpret_cast<__half *>(lh) + (kbl + b) * ldh, ldh, width);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// A_col = (A_col (s_u U11^{-1})) / s_u
@@ -871,17 +875,18 @@ int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 	uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st)
 {
 	if (rem <= 0) return HPLAI_OK;
-	if (!t.f16_oscale || ldh % 64 || t.b % 4 || kb % 4 || rem % 4 || lda % 4) return HPLAI_EINVAL;
+	const int width = (t.b + 63) / 64 * 64;
+	if (!t.f16_oscale || ldh % 64 || ldh < width || t.b % 4 || kb % 4 || rem % 4 || lda % 4) return HPLAI_EINVAL;
 	const int b = t.b;
 	const int64_t kbl = kb;
 	// A_row (rows kb..kb+b-1, columns kb+b..): column j -> FP16 row kb+b+j of uh
 	float *arow = a + kbl + (kbl + b) * lda;
 	const __half *drow = deck ? reinterpret_cast<const __half *>(deck) + kbl + (kbl + b) * lda : nullptr;
 	{
-		const int64_t work = static_cast<int64_t>(rem) * (ldh / 4);
+		const int64_t work = static_cast<int64_t>(rem) * (width / 4);
 		const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((work + 255) / 256, 148 * 16));
 		panel_f16_n_kernel<<<blocks, 256, 0, st>>>(rem, b, arow, lda, drow, lda, inv_dscale,
-			reinterpret_cast<__half *>(uh) + (kbl + b) * ldh, ldh);
+			reinterpret_cast<__half *>(uh) + (kbl + b) * ldh, ldh, width);
 	}
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());

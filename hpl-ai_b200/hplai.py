@@ -30,6 +30,7 @@ F32_F16, F32_F8 = 0, 1
 FLAG_SIMT_PANELS = 1
 FLAG_LOOKAHEAD = 2
 FLAG_FP16_DECK = 4
+FLAG_GROUP2 = 8
 IR, GMRES = 0, 1
 PHASES = ("DIAG_LU", "TRSM_L", "TRSM_R", "GEMM_UPDATE", "IR_GEMV", "IR_TRSV", "TOTAL", "LAZY_INIT")
 
@@ -58,6 +59,7 @@ _generate = _proto("hplai_generate", _c_int, _vp, _c_u64)
 _upload = _proto("hplai_upload", _c_int, _vp, _vp, _c_i64, _vp, _vp, _c_u64)
 _factor = _proto("hplai_factor", _c_int, _vp)
 _autotune = _proto("hplai_autotune", _c_int, _vp, _c_u64, _vp, _vp, _vp)
+_autotune_log = _proto("hplai_get_autotune_log", _c_int, _vp, _vp, _vp, _vp, _c_int, ctypes.POINTER(_c_int))
 _refine = _proto("hplai_refine", _c_int, _vp, _c_int, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
 _get_x = _proto("hplai_get_x", _c_int, _vp, _vp)
 _get_lu = _proto("hplai_get_lu", _c_int, _vp, _vp, _c_i64)
@@ -204,6 +206,16 @@ class Solver:
         fl, side, ms = ctypes.c_uint(), _c_int(), ctypes.c_double()
         check(_autotune(self._h, seed, ctypes.byref(fl), ctypes.byref(side), ctypes.byref(ms)), "hplai_autotune")
         return fl.value, side.value, ms.value
+
+    def autotune_log(self):
+        """The last autotune's trials: [(flags, side_sms, ms)], warm-up first."""
+        cap = 64
+        fl = (ctypes.c_uint * cap)()
+        sd = (_c_int * cap)()
+        ms = (ctypes.c_double * cap)()
+        cnt = _c_int()
+        check(_autotune_log(self._h, fl, sd, ms, cap, ctypes.byref(cnt)), "hplai_get_autotune_log")
+        return [(fl[i], sd[i], ms[i]) for i in range(min(cnt.value, cap))]
 
     def iterative_refinement(self, maxit: int = 50, mode: int = IR) -> RefineResult:
         e = IRErrors()

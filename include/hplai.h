@@ -97,6 +97,15 @@ typedef enum hplai_phase {
  * Schur update's memory traffic; the FP32 matrix keeps the original
  * entries and receives the factors.  Requires b % 8 == 0. */
 #define HPLAI_FLAG_FP16_DECK 4u
+/* Two-panel groups: the trailing matrix is updated once per two panels,
+ * C -= [L_k L_k+1] [U_k; U_k+1] (K = 2b), after the group's second block has
+ * received the first panel's update alone -- the aggregated form of
+ * GemmControl's split update (schur_updator.hpp:108-269), which halves the
+ * passes over the trailing matrix.  With HPLAI_FLAG_LOOKAHEAD both panels of
+ * the next group are formed on the side stream.  Requires b % 128 == 0
+ * (hplai_create returns HPLAI_EINVAL otherwise); hplai_autotune may switch
+ * it on or off for contexts whose b allows it. */
+#define HPLAI_FLAG_GROUP2 8u
 
 typedef struct hplai_ctx hplai_ctx;
 
@@ -138,11 +147,19 @@ int hplai_factor(hplai_ctx *ctx);
 
 /* Schedule tuner in place of lda_tuner (lda_tuner.hpp:9-45): times
  * hplai_factor on this context (regenerated from seed before each trial)
- * serially and with HPLAI_FLAG_LOOKAHEAD at several side-stream SM counts,
- * keeps the fastest as the context's schedule, and leaves the context
- * generated and unfactored.  Outputs (may be NULL): the chosen flags, the
- * side-stream SM count and the best factorisation time in ms. */
+ * under each schedule -- one- or two-panel groups (HPLAI_FLAG_GROUP2, when
+ * b % 128 == 0), serial or with HPLAI_FLAG_LOOKAHEAD at several side-stream
+ * SM counts -- after one discarded warm-up factorisation, re-times the two
+ * fastest twice more, keeps the one with the lowest median as the context's
+ * schedule, and leaves the context generated and unfactored.  Outputs (may
+ * be NULL): the chosen flags, the side-stream SM count and the chosen
+ * schedule's median factorisation time in ms. */
 int hplai_autotune(hplai_ctx *ctx, uint64_t seed, unsigned *flags, int *side_sms, double *ms);
+/* The trials of the last hplai_autotune in the order they ran (the warm-up
+ * first): flags, side-stream SMs and factorisation ms of each; *count is
+ * the number of trials (at most cap are written).  No counterpart in the
+ * reference (lda_tuner prints its choice only). */
+int hplai_get_autotune_log(hplai_ctx *ctx, unsigned *flags, int *side_sms, double *ms, int cap, int *count);
 
 /* iterative_refinement (iterative_refinement.hpp:18-57) with maxit steps
  * (the driver uses 50).  Fills *err ({-1,-1} on failure) and *iters (the

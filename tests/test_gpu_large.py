@@ -81,16 +81,30 @@ def test_c2_lookahead_deck_residual_vs_oracle_rows(hplai, oracle, torch_cuda):
         _check_solution(hplai, oracle, torch_cuda, s, n, rep)
 
 
-@pytest.mark.parametrize("form", ["precision", "plain"])
+def test_c2_group2_residual_vs_oracle_rows(hplai, oracle, torch_cuda):
+    """The C2 size with two-panel groups (K = 1024 trailing updates)."""
+    n, b = 65536, 512
+    with hplai.Solver(n, b, flags=hplai.FLAG_GROUP2) as s:
+        s.generate(42)
+        s.factor()
+        rep = s.iterative_refinement(50)
+        assert rep.status == hplai.HPLAI_OK, rep
+        _check_solution(hplai, oracle, torch_cuda, s, n, rep)
+
+
+@pytest.mark.parametrize("form", ["precision", "plain", "precision-group2", "plain-group2"])
 def test_c3_residual_vs_oracle_rows(hplai, oracle, torch_cuda, form):
     """n = 131072, b = 1024: the precision form (e4m3 Schur into the FP16
     deck, GMRES-IR) and the plain form (FP16 Schur into the FP32 trailing
-    matrix, IR), one after the other."""
+    matrix, IR), with one- and two-panel trailing updates, one after the
+    other."""
     n, b = 131072, 1024
-    if form == "precision":
+    if form.startswith("precision"):
         prec, flags, mode = hplai.F32_F8, hplai.FLAG_FP16_DECK, hplai.GMRES
     else:
         prec, flags, mode = hplai.F32_F16, 0, hplai.IR
+    if form.endswith("group2"):
+        flags |= hplai.FLAG_GROUP2
     with hplai.Solver(n, b, precision=prec, flags=flags) as s:
         s.generate(42)
         s.factor()

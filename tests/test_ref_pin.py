@@ -9,10 +9,10 @@ built by oracle/build_ref.sh).
 * The refinement's step-0 residual and harness equal the reference's in every
   run; step 1 depends on the grid's TRSV summation order (the oracle follows a
   single process column), so it is compared to 1e-8.
-* Every solution -- the oracle's, the GPU's plain form, the GPU's FP16-deck
-  form, the GPU's precision form -- equals the reference's x from each of its
-  four runs (`-not -r`, `-not -d -r`, netlib and OpenBLAS builds) to FP64
-  relative error 1e-12.
+* Every solution -- the oracle's, the GPU's plain form, the GPU's precision
+  form (e4m3 Schur, GMRES-IR; the FP16 deck needs b % 8 == 0, which b = 60 is
+  not) -- equals the reference's x from each of its four runs (`-not -r`,
+  `-not -d -r`, netlib and OpenBLAS builds) to FP64 relative error 1e-12.
 """
 import hashlib
 import json
@@ -60,15 +60,13 @@ def test_oracle_x_matches_reference_x(oracle, run):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("form", ["plain", "deck", "precision"])
+@pytest.mark.parametrize("form", ["plain", "precision"])
 def test_gpu_x_matches_reference_x(hplai, torch_cuda, form):
     """C1's parity bar: x equals the reference's x to FP64 relative 1e-12,
     against all four of the reference's runs."""
     prec, flags, mode = hplai.F32_F16, 0, hplai.IR
-    if form == "deck":
-        flags = hplai.FLAG_FP16_DECK
-    elif form == "precision":
-        prec, flags, mode = hplai.F32_F8, hplai.FLAG_FP16_DECK, hplai.GMRES
+    if form == "precision":
+        prec, mode = hplai.F32_F8, hplai.GMRES
     with hplai.Solver(N, B, precision=prec, flags=flags) as s:
         s.generate(42)
         s.factor()
