@@ -603,6 +603,7 @@ def run_batch(args):
     launches = hplai.launch_count() - l0
     clocks = sampler.stop()
     worst = max(bt.result(s).hpl_harness for s in range(count))
+    graph_launches = bt.launches()
     bt.close()
     total_ms = sum(times)
     value, max_ms = replica_value(total_ms, args.steps * flops, world, device="cuda")
@@ -615,10 +616,15 @@ def run_batch(args):
             "data": f"synthetic (LCG matrices, system s seeded with s; sizes from host generator seed {args.batch_seed})",
             "config": {"workload": f"batched: {count} systems, n log-uniform 256..4096 (round 64), 1..8 "
                                    f"right-hand sides each, plain form + IR", "systems": count,
-                       "n_total": int(n.sum()), "rhs_total": int(nrhs.sum()), "workers": args.batch_workers,
+                       "n_total": int(n.sum()), "rhs_total": int(nrhs.sum()),
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "systems_per_s": world * count * args.steps / (max_ms / 1e3),
-            "worst_hpl_harness": worst, "context_create_s": create_s, "gpu_launches": int(launches),
+            "worst_hpl_harness": worst, "create_s": create_s, "gpu_launches": int(launches),
+            "launches_per_solve": int(launches) // max(args.steps, 1),
+            "graph_kernel_nodes": graph_launches,
+            "engine": "batched engine: every kernel over all systems (128-wide panels, identity padding), generation "
+                      "+ factorisation one CUDA graph, refinement steps until every right-hand side is below 16"
+            if graph_launches else "per-system contexts fed by host worker threads",
             "clocks": clocks,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(count * 16),
                     "d2h_bytes_per_step": xbytes,

@@ -599,12 +599,18 @@ int prepare_block(hplai_ctx *c, int j, int first, int q, bool simt, int side_cta
 
 } // namespace
 
-extern "C" int hplai_factor(hplai_ctx *c)
+namespace {
+
+// The factorisation of panels 0 .. kend-1 (kend = nb: the whole LU).  With
+// kend < nb (the benchmark warm-up) the updates of panels 0 .. kend-2 are
+// applied, as in the reference, whose loop applies panel k-1's update in
+// iteration k (RDMAPanelLU::run, panel_trf.hpp:726-850).
+int factor_impl(hplai_ctx *c, int kend)
 {
 	if (!c) return HPLAI_EINVAL;
 	if (!c->have_inputs) return HPLAI_ESTATE;
 	const int n = c->n, b = c->b, nb = c->nb;
-	c->group = ((c->flags & HPLAI_FLAG_GROUP2) && c->gcap == 2) ? 2 : 1;
+	c->group = ((c->flags & HPLAI_FLAG_GROUP2) && c->gcap == 2 && kend >= nb) ? 2 : 1;
 	const int G = c->group;
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->kstatus, 0, 2 * sizeof(unsigned), c->st));
 	if (c->deck) HPLAI_CUDA_TRY(cudaMemsetAsync(c->deck, 0, sizeof(uint16_t) * static_cast<size_t>(c->lda) * n, c->st));
@@ -635,11 +641,11 @@ extern "C" int hplai_factor(hplai_ctx *c)
 	// the side stream starts from the generated matrix: group 0's panels
 	HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));
 	HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_next, 0));
-	for (int j = 0; j < G && j < nb; ++j) {
+	for (int j = 0; j < G && j < nb && j < kend; ++j) {
 		HPLAI_TRY(prepare_block(c, j, 0, 0, simt, side_ctas, sd, pe));
 		HPLAI_TRY(panel_step(c, j, 0, j, simt, side_ctas, sd, pe));
 	}
-	for (int s = 0; s + G < nb; s += G) {
+	for (int s = 0; s + G < nb && (kend >= nb || s + 1 < kend); s += G) {
 		const int q = (s / G) & 1;
 		const int e = s + G, ne = std::min(G, nb - e);
 		const int r1 = e * b, r2 = (e + ne) * b;
@@ -651,7 +657,7 @@ extern "C" int hplai_factor(hplai_ctx *c)
 		HPLAI_TRY(schur_region(c, op, r1, r2, r2, n, 0, st, pe));
 		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));
 		HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_next, 0));
-		for (int j = e; j < e + ne; ++j) {
+		for (int j = e; j < e + ne && j < kend; ++j) {
 			HPLAI_TRY(prepare_block(c, j, e, q ^ 1, simt, side_ctas, sd, pe));
 			HPLAI_TRY(panel_step(c, j, q ^ 1, j - e, simt, side_ctas, sd, pe));
 		}
@@ -677,6 +683,28 @@ extern "C" int hplai_factor(hplai_ctx *c)
 		HPLAI_TRY(getrf_status(c->getrf_work, st, &gs));
 		HPLAI_TRY(gs);
 	}
+	c->factored = true;
+	return HPLAI_OK;
+}
+
+} // namespace
+
+extern "C" int hplai_factor(hplai_ctx *c) { return c ? factor_impl(c, c->nb) : HPLAI_EINVAL; }
+
+extern "C" int hplai_factor_steps(hplai_ctx *c, int steps)
+{
+	if (!c || steps < 0) return HPLAI_EINVAL;
+	return factor_impl(c, std::min(steps, c->nb));
+}
+
+extern "C" int hplai_l1est(hplai_ctx *c)
+{
+	if (!c) return HPLAI_EINVAL;
+	if (!c->have_inputs) return HPLAI_ESTATE;
+	for (double &v : c->phase_ms) v = 0.0;
+	HPLAI_TRY(launch_l1est(c->n, c->A, c->lda, c->d, c->st));
+	HPLAI_TRY(launch_trsv_dinv(c->n, c->A, c->lda, c->dinv, c->st));
+	HPLAI_CUDA_TRY(cudaStreamSynchronize(c->st));
 	c->factored = true;
 	return HPLAI_OK;
 }

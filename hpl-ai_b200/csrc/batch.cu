@@ -1,16 +1,17 @@
-// batch.cu -- many independent HPL-AI systems solved concurrently on one GPU.
+// batch.cu -- the batched C API: many independent HPL-AI systems on one GPU.
 //
 // The reference solves one system per run (main.cpp:144-492).  A batch holds
 // `count` systems; system s is the HPL-AI matrix of order n[s] generated from
 // seed[s] (state_0 = a*seed + 1, hpl_rand.hpp:35-57) with nrhs[s]
 // right-hand sides: columns n, n+1, ... of the same stream (pcolvgen,
-// matgen.hpp:193-207, extended past column n).  Each system has its own
-// context (buffers sized for it, its own streams), so the GPU runs the
-// kernels of several systems at once; a pool of host worker threads keeps
-// it fed.  The workers are persistent for the call and take systems
-// largest first (by n^3) from a shared counter, which balances the pool.
-// Every system is factored once and each right-hand side is refined with
-// the shared factors (IR for the plain form, GMRES-IR for F32_F8).
+// matgen.hpp:193-207, extended past column n).
+//
+// The plain form (F32_F16, IR; up to 8 right-hand sides per system) runs on
+// the batched engine of batched.cu: every kernel covers all systems, and
+// generation plus factorisation are one CUDA graph.  Other forms (the e4m3
+// precision form with GMRES-IR, the FP16 deck, more right-hand sides) give
+// each system its own context, fed by a pool of host worker threads that
+// take systems largest first (by n^3) from a shared counter.
 #include "common.cuh"
 #include "internal.h"
 
@@ -30,6 +31,7 @@ struct hplai_batch {
 	std::vector<hplai_ir_errors> worst;      // largest harness over the system's right-hand sides
 	std::vector<int> iters, status;
 	std::vector<int> order;                  // systems by decreasing n
+	hplai::BatchEngine *eng = nullptr;       // the batched engine (plain form), else per-system contexts
 };
 
 namespace {
@@ -46,6 +48,7 @@ int pick_block(int n)
 void destroy(hplai_batch *bt)
 {
 	if (!bt) return;
+	if (bt->eng) hplai::batched_destroy(bt->eng);
 	for (hplai_ctx *c : bt->ctx)
 		if (c) hplai_destroy(c);
 	delete bt;
@@ -97,6 +100,25 @@ extern "C" int hplai_batch_create(hplai_batch **out, int count, const int *n, co
 	bt->worst.assign(count, hplai_ir_errors{-1.0, -1.0});
 	bt->iters.assign(count, 0);
 	bt->status.assign(count, HPLAI_ESTATE);
+	bool engine = precision == HPLAI_F32_F16 && flags == 0;
+	for (int s = 0; s < count; ++s) {
+		if (n[s] < 1 || nrhs[s] < 1) {
+			destroy(bt);
+			return HPLAI_EINVAL;
+		}
+		if (nrhs[s] > 8) engine = false;
+	}
+	if (engine) {
+		std::vector<uint64_t> sd(seeds, seeds + count);
+		const int rc = hplai::batched_create(&bt->eng, count, n, nrhs, sd.data());
+		if (rc != HPLAI_OK) {
+			destroy(bt);
+			return rc;
+		}
+		for (int s = 0; s < count; ++s) bt->b[s] = 128;
+		*out = bt;
+		return HPLAI_OK;
+	}
 	for (int s = 0; s < count; ++s) {
 		const int bs = pick_block(n[s]);
 		if (bs == 0 || nrhs[s] < 1) {
@@ -127,6 +149,10 @@ extern "C" int hplai_batch_destroy(hplai_batch *bt)
 extern "C" int hplai_batch_solve(hplai_batch *bt, int maxit)
 {
 	if (!bt || maxit < 0) return HPLAI_EINVAL;
+	if (bt->eng) {
+		if (cudaSetDevice(bt->device) != cudaSuccess) return HPLAI_ECUDA;
+		return hplai::batched_solve(bt->eng, maxit, nullptr);
+	}
 	// the first (largest) system on this thread: every lazily initialised
 	// library setting is in place before the pool starts
 	solve_one(bt, bt->order[0], maxit);
@@ -152,6 +178,7 @@ extern "C" int hplai_batch_solve(hplai_batch *bt, int maxit)
 extern "C" int hplai_batch_result(hplai_batch *bt, int s, hplai_ir_errors *worst, int *iters, int *status)
 {
 	if (!bt || s < 0 || s >= bt->count) return HPLAI_EINVAL;
+	if (bt->eng) return hplai::batched_result(bt->eng, s, worst, iters, status);
 	if (worst) *worst = bt->worst[s];
 	if (iters) *iters = bt->iters[s];
 	if (status) *status = bt->status[s];
@@ -161,6 +188,7 @@ extern "C" int hplai_batch_result(hplai_batch *bt, int s, hplai_ir_errors *worst
 extern "C" int hplai_batch_get_x(hplai_batch *bt, int s, double *x, int64_t ldx)
 {
 	if (!bt || s < 0 || s >= bt->count || !x || ldx < bt->n[s]) return HPLAI_EINVAL;
+	if (bt->eng) return hplai::batched_get_x(bt->eng, s, x, ldx);
 	for (int r = 0; r < bt->nrhs[s]; ++r)
 		std::copy_n(bt->x[s].data() + static_cast<size_t>(r) * bt->n[s], bt->n[s], x + static_cast<size_t>(r) * ldx);
 	return HPLAI_OK;
@@ -170,4 +198,17 @@ extern "C" int hplai_batch_block(hplai_batch *bt, int s)
 {
 	if (!bt || s < 0 || s >= bt->count) return -1;
 	return bt->b[s];
+}
+
+extern "C" int hplai_batch_get_lu(hplai_batch *bt, int s, float *a, int64_t lda)
+{
+	if (!bt || s < 0 || s >= bt->count || !a || lda < bt->n[s]) return HPLAI_EINVAL;
+	if (bt->eng) return hplai::batched_get_lu(bt->eng, s, a, lda);
+	return hplai_get_lu(bt->ctx[s], a, lda);
+}
+
+extern "C" unsigned long long hplai_batch_launches(hplai_batch *bt)
+{
+	if (!bt) return 0;
+	return bt->eng ? hplai::batched_launches(bt->eng) : 0;
 }

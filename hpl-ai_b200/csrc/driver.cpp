@@ -6,8 +6,9 @@
 // (main.cpp:144-181, 437-453): n % b == 0, seed 42, LU + iterative
 // refinement timed as one region, then
 //   "%.9f sec. %.9f GFlop/s resid = %20.15e hpl-harness = %.9f".
-// P (the process-grid rows) is accepted and ignored: the whole matrix lives
-// on one GPU.  `-d`/`-l` (the double-decker layout with lazy
+// P (the process-grid rows) does not lay out anything -- the whole matrix
+// lives on one GPU -- but sets the length of the `-w` warm-up as in the
+// reference (the first P + 2 panels, main.cpp:57, panel_trf.hpp:726).  `-d`/`-l` (the double-decker layout with lazy
 // initialisation, main.cpp:52-53) select the FP16 trailing-update deck; `--fp8` the
 // precision form (e4m3 Schur update, GMRES-IR); `--gmres` GMRES-IR.  The
 // reference's layout/transport flags (-not, -r, -m, --pack, --numa, --nbuf,
@@ -33,7 +34,7 @@
 // so the items can add up to more than TOTAL: MISC is then clamped at 0 and
 // a comment line says that the items overlap.
 static void write_timerdump(int jobid, int n, int b, double total_s, const double *ms, long long matvecs,
-	bool overlapped)
+	bool overlapped, bool warmup)
 {
 	enum { DIAG_LU = 5, TRSM_L = 6, TRSM_R = 7, GEMM_UPDATE = 10, GEMM_PROGRESS = 11, LAZY_INIT = 12, IR_GEMV = 14,
 		IR_TRSV = 16, TOTAL = 19, MISC = 20, NUM_ITEMS = 21 };
@@ -62,7 +63,8 @@ static void write_timerdump(int jobid, int n, int b, double total_s, const doubl
 	for (int i = 0; i < NUM_ITEMS - 2; ++i) t[MISC] -= t[i];
 	if (t[MISC] < 0.0) t[MISC] = 0.0;
 	char fname[128];
-	std::snprintf(fname, sizeof fname, "Timerdump.%06d.%09d.%04d.%05d.%05d", jobid, n, b, 1, 0);
+	std::snprintf(fname, sizeof fname, warmup ? "Warmup.%06d.%09d.%04d.%05d.%05d" : "Timerdump.%06d.%09d.%04d.%05d.%05d",
+		jobid, n, b, 1, 0);
 	FILE *fp = std::fopen(fname, "w");
 	if (!fp) return;
 	char host[256] = "";
@@ -105,10 +107,12 @@ static int usage()
 		"   --group <g>             Panels per trailing update: 1 (default) or 2 (K = 2b; b %% 128 == 0).\n"
 		"   --autotune              Choose the schedule (groups, look-ahead) by timing it first.\n"
 		"   --checksum              Print sums of |diag|, |upper|, |lower| of the factors after the LU.\n"
+		"   -w, --warmup            Factor the first P+2 panels only, one refinement step (benchmark warm-up).\n"
+		"   --l1est                 Approximate the LU factors from the matrix instead of factoring it.\n"
 		"   --job-id <id>           Job number in the name of the Timerdump file (default 0).\n"
 		"   --help or -h            Print this message.\n"
-		"Layout and transport flags of the distributed reference (-not, -r, -m, -w, --pack,\n"
-		"--numa, --numa-map, --nbuf, --l1est, --highammat, --pwrtune)\n"
+		"Layout and transport flags of the distributed reference (-not, -r, -m, --pack,\n"
+		"--numa, --numa-map, --nbuf, --pwrtune)\n"
 		"are accepted and ignored.\n");
 	return 0;
 }
@@ -119,10 +123,12 @@ int main(int argc, char **argv)
 	unsigned long long seed = 42;
 	int precision = HPLAI_F32_F16, mode = HPLAI_IR;
 	unsigned flags = 0;
-	bool checksum = false, autotune = false;
+	bool checksum = false, autotune = false, warmup = false, l1est = false;
+	int nrow = 2;
 	int jobid = 0;
 	if (argc > 1) n = std::atoi(argv[1]);
 	if (argc > 2) b = std::atoi(argv[2]);
+	if (argc > 3) nrow = std::atoi(argv[3]);
 	for (int i = 4; i < argc; ++i) {
 		if (!std::strcmp(argv[i], "--help") || !std::strcmp(argv[i], "-h")) return usage();
 		else if (!std::strcmp(argv[i], "--maxit") && i + 1 < argc) maxit = std::atoi(argv[++i]);
@@ -138,6 +144,8 @@ int main(int argc, char **argv)
 		}
 		else if (!std::strcmp(argv[i], "--autotune")) autotune = true;
 		else if (!std::strcmp(argv[i], "--checksum")) checksum = true;
+		else if (!std::strcmp(argv[i], "-w") || !std::strcmp(argv[i], "--warmup")) warmup = true;
+		else if (!std::strcmp(argv[i], "--l1est")) l1est = true;
 		else if (!std::strcmp(argv[i], "--numa") || !std::strcmp(argv[i], "--numa-map") ||
 			!std::strcmp(argv[i], "--nbuf")) ++i;
 		else if (!std::strcmp(argv[i], "--job-id") && i + 1 < argc) jobid = std::atoi(argv[++i]);
@@ -200,8 +208,12 @@ int main(int argc, char **argv)
 
 	hplai_ir_errors er{-1.0, -1.0};
 	int iters = 0;
+	// with -w the refinement gets one step (main.cpp:322: maxit = warmup ? 1 : 50)
+	if (warmup) maxit = 1;
 	auto t0 = std::chrono::steady_clock::now();
-	rc = hplai_factor(ctx);
+	if (l1est) rc = hplai_l1est(ctx);
+	else if (warmup) rc = hplai_factor_steps(ctx, nrow + 2);
+	else rc = hplai_factor(ctx);
 	if (rc == HPLAI_OK && checksum) {
 		// inside the timed region, between the LU and the refinement (main.cpp:298-302)
 		double sigs[3];
@@ -228,7 +240,16 @@ int main(int argc, char **argv)
 	print_ctime("#END__: ");
 	char line[256];
 	const double secs = std::chrono::duration<double>(t1 - t0).count();
-	hplai_format_report(n, secs, er, line, sizeof line);
+	if (warmup) {
+		// the skipped trailing part leaves the flop count (main.cpp:441-446)
+		const double nn = static_cast<double>(n) - static_cast<double>(nrow + 2) * b;
+		const double flops = 2. / 3 * n * static_cast<double>(n) * n + 3. / 2 * n * static_cast<double>(n) -
+			(2. / 3 * nn * nn * nn + 3. / 2 * nn * nn);
+		std::snprintf(line, sizeof line, "%.9f sec. %.9f GFlop/s resid = %20.15e hpl-harness = %.9f", secs,
+			flops / secs * 1e-9, er.residual, er.hpl_harness);
+	} else {
+		hplai_format_report(n, secs, er, line, sizeof line);
+	}
 	std::printf("%s\n", line);
 	double ms[HPLAI_PH_COUNT];
 	hplai_get_phase_ms(ctx, ms, HPLAI_PH_COUNT);
@@ -239,11 +260,13 @@ int main(int argc, char **argv)
 	std::fflush(stdout);
 	int outer = 0, inner = 0;
 	hplai_get_refine_counts(ctx, &outer, &inner);
-	write_timerdump(jobid, n, b, secs, ms, static_cast<long long>(outer) + inner, (flags & HPLAI_FLAG_LOOKAHEAD) != 0);
+	write_timerdump(jobid, n, b, secs, ms, static_cast<long long>(outer) + inner, (flags & HPLAI_FLAG_LOOKAHEAD) != 0,
+		warmup);
 	hplai_destroy(ctx);
 	if (rr != HPLAI_OK && rr != HPLAI_ENOTCONV) {
 		std::fprintf(stderr, "hplai_refine: %s\n", hplai_status_string(rr));
 		return 1;
 	}
+	if (warmup) return 0;   // one refinement step of a partial factorisation: {-1, -1} by design
 	return rr == HPLAI_OK ? 0 : 2;
 }

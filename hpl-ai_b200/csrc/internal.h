@@ -20,6 +20,8 @@ int launch_diag(int n, int i0, int count, double *d, float *adiag, int64_t lda, 
 int launch_rhs(int n, double *rhs, uint64_t seed, cudaStream_t st);
 // columns n + col0 .. n + col0 + ncols - 1 of the stream, column-major with ld n
 int launch_rhs_cols(int n, int col0, int ncols, double *out, uint64_t seed, cudaStream_t st);
+// pmatl1est: strictly lower part of A (n x n, lda) times float(1/d_j) per column
+int launch_l1est(int n, float *a, int64_t lda, const double *d, cudaStream_t st);
 
 // panel.cu
 // getrf.cu: tile-parallel diagonal block LU (bit-exact with the sequential
@@ -46,7 +48,7 @@ struct SchurMaps {
 	// FP32 matrix holding C, for the TMA reduce-add epilogue (a map clipped to
 	// each launch's region is encoded per launch).
 	float *cbase = nullptr;
-	int64_t cld = 0;
+	int64_t cld = 0, crows = 0, ccols = 0;
 	bool has_cmap = false;
 	unsigned *status = nullptr;   // device word set on a wait timeout (null: the library's own)
 	// FP16 deck (trailing-matrix updates of the lazy form): base and leading
@@ -84,6 +86,12 @@ int launch_schur_store(const SchurMaps &maps, int lrow0, int urow0, int m, int n
 	int ccol0, const float *oscale, int max_ctas, cudaStream_t st);
 int launch_schur_deck(const SchurMaps &maps, bool fp8, const float *sl, int sl0, const float *su, int su0, int lrow0,
 	int urow0, int m, int n, int crow0, int ccol0, float dscale, int max_ctas, cudaStream_t st);
+// The batched form: `ntiles` 128 x 256 tiles, tile t updating C rows
+// tiles[t].z.. and columns tiles[t].w.. of the matrix given to
+// schur_set_cmap with L rows tiles[t].x.. and U rows tiles[t].y.. (FP16
+// maps); a tile may reach past the columns of its system into columns nobody
+// reads (or past the matrix, where it is clipped).
+int launch_schur_tiles(const SchurMaps &maps, const int4 *tiles, int ntiles, int max_ctas, cudaStream_t st);
 int schur_status();          // the library's word: HPLAI_ETIMEOUT if a device wait ran out since the last reset
 void schur_status_reset();
 
@@ -188,6 +196,17 @@ int launch_add_small(int nv, const double *a, double *b, cudaStream_t st);
 int launch_scale(int n, const double *w, const double *den, double *out, cudaStream_t st);
 // x += V y
 int launch_combine(int n, int nv, const double *v, int64_t ldv, const double *y, double *x, cudaStream_t st);
+
+// batched.cu: the step-synchronous batched engine (plain form, IR)
+struct BatchEngine;
+int batched_create(BatchEngine **out, int count, const int *n, const int *nrhs, const uint64_t *seeds);
+void batched_destroy(BatchEngine *e);
+int batched_solve(BatchEngine *e, int maxit, unsigned long long *launches);
+int batched_result(BatchEngine *e, int orig, hplai_ir_errors *worst, int *iters, int *status);
+int batched_get_x(BatchEngine *e, int orig, double *x, int64_t ldx);
+int batched_get_lu(BatchEngine *e, int orig, float *a, int64_t lda);
+int batched_pad(BatchEngine *e, int orig);
+unsigned long long batched_launches(const BatchEngine *e);
 
 } // namespace hplai
 

@@ -132,6 +132,11 @@ struct Params {
 	// Store form of the reduce epilogue (FP16 operands only): C = acc * *oscale
 	// written by TMA store instead of C -= acc (null: the update)
 	const float *oscale;
+	// Batched form (FP16 operands, reduce epilogue): `ntiles` tiles whose L
+	// row, U row, C row and C column come from this table instead of the
+	// region's tile grid -- the tiles of many systems' updates in one launch.
+	const int4 *tiles;
+	int ntiles;
 };
 
 __device__ unsigned int g_status;
@@ -259,7 +264,7 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 	tc_fence_after();
 	const uint32_t tmem_base = *tmem_holder;
 
-	const int total = p.tiles_m * p.tiles_n;
+	const int total = p.tiles ? p.ntiles : p.tiles_m * p.tiles_n;
 	int issued = 0;   // producer: stages issued
 
 	if (warp == 0) {
@@ -268,16 +273,25 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 		int stage = 0;
 		uint32_t phase = 0;
 		for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x) {
-			int tm, tn;
-			tile_coords(tile, p.tiles_m, p.tiles_n, tm, tn);
+			int lrow, urow;
+			if (p.tiles) {
+				const int4 t = p.tiles[tile];
+				lrow = t.x;
+				urow = t.y;
+			} else {
+				int tm, tn;
+				tile_coords(tile, p.tiles_m, p.tiles_n, tm, tn);
+				lrow = p.lrow0 + tm * BM;
+				urow = p.urow0 + tn * BN;
+			}
 			if (lane == 0) {
 				for (int kc = 0; kc < p.num_kc; ++kc) {
 					if (!mbar_wait(&empty[stage], phase ^ 1u)) { ok = false; break; }
 					mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
 					// K offset of this stage in elements: 64 FP16 or 128 FP8 per 128-byte row
 					const int kx = kc * (FP8 ? 2 * BK : BK);
-					tma_load_2d(sA + stage * A_BYTES, &lmap, &full[stage], kx, p.lrow0 + tm * BM);
-					tma_load_2d(sB + stage * B_BYTES, &umap, &full[stage], kx, p.urow0 + tn * BN);
+					tma_load_2d(sA + stage * A_BYTES, &lmap, &full[stage], kx, lrow);
+					tma_load_2d(sB + stage * B_BYTES, &umap, &full[stage], kx, urow);
 					++issued;
 					if (++stage == NST) { stage = 0; phase ^= 1u; }
 				}
@@ -441,8 +455,16 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 		uint32_t acc_phase = 0;
 		int epi_buf = 0;
 		for (int tile = blockIdx.x; tile < total; tile += gridDim.x) {
-			int tm, tn;
-			tile_coords(tile, p.tiles_m, p.tiles_n, tm, tn);
+			int tm = 0, tn = 0, crow, ccol;
+			if (p.tiles) {
+				const int4 t = p.tiles[tile];
+				crow = t.z;
+				ccol = t.w;
+			} else {
+				tile_coords(tile, p.tiles_m, p.tiles_n, tm, tn);
+				crow = p.crow0 + tm * BM;
+				ccol = p.ccol0 + tn * BN;
+			}
 			// the epilogue warps decide together (their named barriers must not split)
 			ok = epi_all(mbar_wait(&accf[acc], acc_phase));
 			if (!ok) break;
@@ -493,9 +515,9 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 					asm volatile("bar.sync 1, %0;" ::"n"(EPI_WARPS * 32) : "memory");
 					if (issuer) {
 						if (!FP8 && p.oscale)
-							tma_store_2d(&cmap, sb, p.crow0 + tm * BM, p.ccol0 + tn * BN + cc);
+							tma_store_2d(&cmap, sb, crow, ccol + cc);
 						else
-							tma_reduce_add_2d(&cmap, sb, p.crow0 + tm * BM, p.ccol0 + tn * BN + cc);
+							tma_reduce_add_2d(&cmap, sb, crow, ccol + cc);
 						asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 					}
 					++epi_buf;
@@ -656,6 +678,8 @@ int schur_set_cmap(SchurMaps *m, const float *c, int rows, int cols, int64_t ldc
 	if (!c || rows <= 0 || cols <= 0 || (reinterpret_cast<uintptr_t>(c) & 15u) || (ldc % 4)) return HPLAI_OK;
 	m->cbase = const_cast<float *>(c);
 	m->cld = ldc;
+	m->crows = rows;
+	m->ccols = cols;
 	m->has_cmap = true;
 	return HPLAI_OK;
 }
@@ -693,6 +717,8 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 	p.su0 = su0;
 	p.dscale = dscale;
 	p.oscale = oscale;
+	p.tiles = nullptr;
+	p.ntiles = 0;
 	p.status = maps.status;
 	if (!p.status) {
 		void *g = nullptr;
@@ -783,6 +809,47 @@ int launch_schur_deck(const SchurMaps &maps, bool fp8, const float *sl, int sl0,
 {
 	return launch_schur_any(maps, fp8, sl, sl0, su, su0, lrow0, urow0, m, n, maps.deck_base, maps.deck_ld, crow0, ccol0,
 		true, dscale, max_ctas, st);
+}
+
+int launch_schur_tiles(const SchurMaps &maps, const int4 *tiles, int ntiles, int max_ctas, cudaStream_t st)
+{
+	if (ntiles <= 0) return HPLAI_OK;
+	if (!maps.has_cmap || !TALL || !tiles) return HPLAI_EINVAL;
+	Params p;
+	std::memset(&p, 0, sizeof p);
+	p.c = maps.cbase;
+	p.ldc = maps.cld;
+	p.num_kc = (maps.k + BK - 1) / BK;
+	p.tiles = tiles;
+	p.ntiles = ntiles;
+	p.dscale = 0.f;
+	p.status = maps.status;
+	if (!p.status) {
+		void *g = nullptr;
+		HPLAI_CUDA_TRY(cudaGetSymbolAddress(&g, g_status));
+		p.status = static_cast<unsigned *>(g);
+	}
+	// one C map over the whole matrix holding every system's C: a tile past a
+	// system's last column lands in columns no system reads (the batched
+	// layout leaves them), past the matrix end it is clipped
+	alignas(64) unsigned char cmap[128];
+	HPLAI_TRY(make_map_2d(cmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, maps.cbase, static_cast<uint64_t>(maps.crows),
+		static_cast<uint64_t>(maps.ccols), static_cast<uint64_t>(maps.cld), BM, EPI_CHUNK, CU_TENSOR_MAP_SWIZZLE_NONE));
+	static bool attr_set = false;
+	if (!attr_set) {
+		HPLAI_TRY((set_smem_attr<1, false>()));
+		attr_set = true;
+	}
+	CUtensorMap lm, um, cm;
+	std::memcpy(&lm, maps.lmap, sizeof(lm));
+	std::memcpy(&um, maps.umap, sizeof(um));
+	std::memcpy(&cm, cmap, sizeof(cm));
+	int grid = (max_ctas > 0 && max_ctas < num_sms()) ? max_ctas : num_sms();
+	if (grid > ntiles) grid = ntiles;
+	schur_kernel<1, false><<<grid, threads_for(1), smem_bytes(1), st>>>(lm, um, cm, p);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
 }
 
 int schur_make_maps_fp8(SchurMaps *m, const uint8_t *l8, int lrows, int64_t ldl, const uint8_t *u8, int urows,

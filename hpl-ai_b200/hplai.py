@@ -58,6 +58,8 @@ _destroy = _proto("hplai_destroy", _c_int, _vp)
 _generate = _proto("hplai_generate", _c_int, _vp, _c_u64)
 _upload = _proto("hplai_upload", _c_int, _vp, _vp, _c_i64, _vp, _vp, _c_u64)
 _factor = _proto("hplai_factor", _c_int, _vp)
+_factor_steps = _proto("hplai_factor_steps", _c_int, _vp, _c_int)
+_l1est = _proto("hplai_l1est", _c_int, _vp)
 _autotune = _proto("hplai_autotune", _c_int, _vp, _c_u64, _vp, _vp, _vp)
 _autotune_log = _proto("hplai_get_autotune_log", _c_int, _vp, _vp, _vp, _vp, _c_int, ctypes.POINTER(_c_int))
 _refine = _proto("hplai_refine", _c_int, _vp, _c_int, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
@@ -118,6 +120,8 @@ _batch_create = _proto("hplai_batch_create", _c_int, ctypes.POINTER(_vp), _c_int
                        _c_int)
 _batch_destroy = _proto("hplai_batch_destroy", _c_int, _vp)
 _batch_solve = _proto("hplai_batch_solve", _c_int, _vp, _c_int)
+_batch_get_lu = _proto("hplai_batch_get_lu", _c_int, _vp, _c_int, _vp, _c_i64)
+_batch_launches = _proto("hplai_batch_launches", ctypes.c_ulonglong, _vp)
 _batch_result = _proto("hplai_batch_result", _c_int, _vp, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int),
                        ctypes.POINTER(_c_int))
 _batch_get_x = _proto("hplai_batch_get_x", _c_int, _vp, _c_int, _vp, _c_i64)
@@ -198,6 +202,14 @@ class Solver:
 
     def factor(self):
         check(_factor(self._h), "hplai_factor")
+
+    def factor_steps(self, steps: int):
+        """Panels 0 .. steps-1 only (the reference's -w warm-up)."""
+        check(_factor_steps(self._h, steps), "hplai_factor_steps")
+
+    def l1est(self):
+        """Approximate factors without a decomposition (the reference's --l1est)."""
+        check(_l1est(self._h), "hplai_l1est")
 
     def autotune(self, seed: int = 42):
         """Time the factorisation serially and with look-ahead at several
@@ -376,6 +388,17 @@ class Batch:
 
     def block(self, s: int) -> int:
         return _batch_block(self._h, s)
+
+    def lu(self, s: int) -> np.ndarray:
+        """System s's FP32 factors (unit L below the diagonal, U on and above)."""
+        m = int(self.n[s])
+        out = np.empty((m, m), dtype=np.float32, order="F")
+        check(_batch_get_lu(self._h, s, _ptr(out), m), "hplai_batch_get_lu")
+        return out
+
+    def launches(self) -> int:
+        """Kernel launches of the batched engine's generation + factorisation graph."""
+        return int(_batch_launches(self._h))
 
 
 def batch_sizes(count: int = 512, rng_seed: int = 20240611, lo: int = 256, hi: int = 4096):

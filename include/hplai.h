@@ -145,6 +145,20 @@ int hplai_upload(hplai_ctx *ctx, const float *a, int64_t lda, const double *rhs,
  * collapsed to one GPU.  Unit-L below and U on/above the diagonal, FP32. */
 int hplai_factor(hplai_ctx *ctx);
 
+/* The benchmark warm-up of the reference's driver (`-w`, main.cpp:57,
+ * RDMAPanelLU::run / panel_lu_async with warmup, panel_trf.hpp:458,726:
+ * kend = nrow + 2): only panels 0 .. steps-1 are factored, and -- as the
+ * reference's loop applies panel k-1's update in iteration k -- the updates
+ * of panels 0 .. steps-2 applied; the rest of the matrix is left partly
+ * updated.  steps >= n/b is hplai_factor.  One-panel trailing updates. */
+int hplai_factor_steps(hplai_ctx *ctx, int steps);
+
+/* Approximate factors without a decomposition (`--l1est`, pmatl1est,
+ * matgen.hpp:108-144, main.cpp:282-301): the strictly lower part of the
+ * generated matrix scaled column by column by float(1 / d_j), the upper part
+ * and the diagonal kept, then marked factored for the refinement. */
+int hplai_l1est(hplai_ctx *ctx);
+
 /* Schedule tuner in place of lda_tuner (lda_tuner.hpp:9-45): times
  * hplai_factor on this context (regenerated from seed before each trial)
  * under each schedule -- one- or two-panel groups (HPLAI_FLAG_GROUP2, when
@@ -225,9 +239,14 @@ typedef struct hplai_batch hplai_batch;
 
 /* `count` independent systems: system s is the HPL-AI matrix of order n[s]
  * from seeds[s] (as hplai_generate) with nrhs[s] >= 1 right-hand sides,
- * columns n[s], n[s]+1, ... of its stream.  The block size of each system is
- * the largest multiple of 16 up to 512 dividing n[s].  `workers` host
- * threads (0: 8) feed the GPU; every system gets its own context. */
+ * columns n[s], n[s]+1, ... of its stream -- the reference's one-system
+ * driver (main.cpp:144-492) over a batch.  The plain form (HPLAI_F32_F16,
+ * flags 0, at most 8 right-hand sides per system) runs on the batched
+ * engine: any n[s] >= 1 (padded with the identity to a multiple of 128,
+ * 128-wide panels), every kernel over all systems at once, generation and
+ * factorisation captured in one CUDA graph; `workers` is unused.  Other
+ * forms give every system its own context (block size: the largest multiple
+ * of 16 up to 512 dividing n[s]) fed by `workers` host threads (0: 8). */
 int hplai_batch_create(hplai_batch **batch, int count, const int *n, const int *nrhs, const uint64_t *seeds,
 	int precision, unsigned flags, int workers);
 int hplai_batch_destroy(hplai_batch *batch);
@@ -242,6 +261,14 @@ int hplai_batch_result(hplai_batch *batch, int s, hplai_ir_errors *worst, int *i
 int hplai_batch_get_x(hplai_batch *batch, int s, double *x, int64_t ldx);
 /* The block size chosen for system s. */
 int hplai_batch_block(hplai_batch *batch, int s);
+/* System s's factors after hplai_batch_solve: n[s] x n[s] FP32,
+ * column-major with leading dimension lda (unit L below the diagonal, U on
+ * and above) -- the reference's Panels after the LU (panel.hpp:20-60). */
+int hplai_batch_get_lu(hplai_batch *batch, int s, float *a, int64_t lda);
+/* Kernel launches per hplai_batch_solve of the batched engine's graph
+ * (generation and factorisation; 0 for per-system contexts).  No
+ * counterpart in the reference. */
+unsigned long long hplai_batch_launches(hplai_batch *batch);
 
 /* ---------------------------------------------------------------------- */
 /* Leaf kernels on caller-owned device buffers.                            */

@@ -148,6 +148,21 @@ ORC_EXPORT void orc_gen_rhs(int n, uint64_t seed, double *rhs)
 	}
 }
 
+/* Columns n + first .. n + first + count - 1 of the stream (pcolvgen's
+ * column n, then the further right-hand sides of a batch), column-major
+ * with leading dimension n. */
+ORC_EXPORT void orc_gen_rhs_cols(int n, uint64_t seed, int first, int count, double *out)
+{
+	orc_coeff inc1 = coeff_default();
+	for (int c = 0; c < count; c++) {
+		uint64_t s = state_at(n, 0, (int64_t)n + first + c, seed);
+		for (int i = 0; i < n; i++) {
+			out[(int64_t)c * n + i] = state_value(s);
+			s = coeff_apply(inc1, s);
+		}
+	}
+}
+
 /* pdiaggen                                      matgen.hpp:209-225 */
 ORC_EXPORT void orc_gen_diag(int n, uint64_t seed, double *d)
 {
@@ -295,10 +310,19 @@ ORC_EXPORT void orc_shgemm_minus(int m, int n, int k, const uint16_t *a, int64_t
  * above it (FP32), exactly like the reference's Panels after the LU.
  * scalea/scaleb are the FP16 down-cast scales (1 without lazy init,
  * panel_trf.hpp:446-447).                                              */
-ORC_EXPORT int orc_lu(int n, int b, float *a, int64_t lda)
+ORC_EXPORT int orc_lu_steps(int n, int b, float *a, int64_t lda, int kend);
+
+ORC_EXPORT int orc_lu(int n, int b, float *a, int64_t lda) { return orc_lu_steps(n, b, a, lda, n / (b > 0 ? b : 1)); }
+
+/* The first kend block steps only: the reference's benchmark warm-up (`-w`)
+ * stops its loop at kend = nrow + 2 (panel_trf.hpp:458,726).  Its loop
+ * applies panel k-1's update in iteration k, so panels 0 .. kend-1 are
+ * factored and the updates of panels 0 .. kend-2 applied. */
+ORC_EXPORT int orc_lu_steps(int n, int b, float *a, int64_t lda, int kend)
 {
 	if (n <= 0 || b <= 0 || n % b) return -1;
 	int nb = n / b;
+	if (kend < nb) nb = kend;
 	uint16_t *lh = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)n * b);
 	uint16_t *uh = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)n * b);
 	if (!lh || !uh) { free(lh); free(uh); return -2; }
@@ -308,7 +332,7 @@ ORC_EXPORT int orc_lu(int n, int b, float *a, int64_t lda)
 		/* diagonal block: getrf_nopiv (copy-first variant computes the same
 		 * numbers in a copy, getrf_nopiv.hpp:143-160)                       */
 		orc_getrf_nopiv(b, lu, lda);
-		if (k == nb - 1) break;
+		if (kb + b == n) break;
 		int64_t rem = n - kb - b;
 		/* update_left_panels: L = A_col * U^{-1}   panel_trf.hpp:143-157 */
 		orc_trsm_right_upper((int)rem, b, lu, lda, lu + b, lda);
@@ -319,6 +343,7 @@ ORC_EXPORT int orc_lu(int n, int b, float *a, int64_t lda)
 			orc_f32_to_f16(rem, lu + b + (int64_t)j * lda, lh + (size_t)j * rem);
 		for (int64_t j = 0; j < rem; j++)
 			orc_f32_to_f16(b, lu + (b + j) * lda, uh + (size_t)j * b);
+		if (k == kend - 1 && kend < n / b) break;   /* warm-up: the last panel's update is not applied */
 		/* Schur update of the trailing matrix       schur_updator.hpp:50-106 */
 		orc_shgemm_minus((int)rem, (int)rem, b, lh, rem, uh, b, lu + (int64_t)b * lda + b, lda);
 	}
@@ -638,5 +663,16 @@ ORC_EXPORT void orc_residual_rows(int n, uint64_t seed, const double *x, int nro
 		if (rhs) bi = rhs[i];
 		else bi = state_value(state_at(n, i, (int64_t)n + rhs_col, seed));
 		r[t] = (double)((long double)bi - acc);
+	}
+}
+
+/* pmatl1est (matgen.hpp:108-144): approximate factors without a
+ * decomposition: a_ij <- a_ij * (float)(1 / d_j) for i > j, with d_j the
+ * FP64 row sum (calc_diag); the upper part and the diagonal are kept. */
+ORC_EXPORT void orc_l1est(int n, float *a, int64_t lda, const double *d)
+{
+	for (int j = 0; j < n; j++) {
+		const float inv = (float)(1.0 / d[j]);
+		for (int i = j + 1; i < n; i++) a[(int64_t)j * lda + i] *= inv;
 	}
 }

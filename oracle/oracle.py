@@ -45,11 +45,14 @@ calc_diag = _proto("orc_calc_diag", _dbl, _int, _int, _u64)
 _fill_panel = _proto("orc_fill_panel", None, _int, _int, _int, _int, _int, _vp, _i64, _u64, _int)
 _gen_rhs = _proto("orc_gen_rhs", None, _int, _u64, _vp)
 _gen_diag = _proto("orc_gen_diag", None, _int, _u64, _vp)
+_gen_rhs_cols = _proto("orc_gen_rhs_cols", None, _int, _u64, _int, _int, _vp)
 _getrf = _proto("orc_getrf_nopiv", None, _int, _vp, _i64)
 _trsm_ru = _proto("orc_trsm_right_upper", None, _int, _int, _vp, _i64, _vp, _i64)
 _trsm_ll = _proto("orc_trsm_left_lower_unit", None, _int, _int, _vp, _i64, _vp, _i64)
 _shgemm = _proto("orc_shgemm_minus", None, _int, _int, _int, _vp, _i64, _vp, _i64, _vp, _i64)
 _lu = _proto("orc_lu", _int, _int, _int, _vp, _i64)
+_lu_steps = _proto("orc_lu_steps", _int, _int, _int, _vp, _i64, _int)
+_l1est = _proto("orc_l1est", None, _int, _vp, _i64, _vp)
 _otf_gemv = _proto("orc_otf_gemv", None, _int, _int, _int, _dbl, _vp, _vp, _u64, _vp)
 _trsv_l = _proto("orc_trsv_lower", None, _int, _int, _vp, _i64, _vp)
 _trsv_u = _proto("orc_trsv_upper", None, _int, _int, _vp, _i64, _vp)
@@ -88,6 +91,13 @@ def rhs(n, seed=42) -> np.ndarray:
     out = np.zeros(n)
     _gen_rhs(n, seed, _p(out))
     return out
+
+
+def rhs_cols(n, seed, first, count) -> np.ndarray:
+    """Columns n + first .. of the generator stream (n x count)."""
+    out = np.zeros((count, n))
+    _gen_rhs_cols(n, seed, first, count, _p(out))
+    return out.T
 
 
 def diag(n, seed=42) -> np.ndarray:
@@ -134,6 +144,23 @@ def lu(a: np.ndarray, b: int) -> np.ndarray:
     rc = _lu(a.shape[0], b, _p(a), a.shape[0])
     if rc:
         raise ValueError(f"orc_lu: {rc}")
+    return a
+
+
+def lu_steps(a: np.ndarray, b: int, kend: int) -> np.ndarray:
+    """The first kend block steps of the LU (the reference's -w warm-up):
+    panels 0..kend-1 factored, the updates of panels 0..kend-2 applied."""
+    a = np.array(a, dtype=np.float32, order="F", copy=True)
+    rc = _lu_steps(a.shape[0], b, _p(a), a.shape[0], kend)
+    if rc:
+        raise ValueError(f"orc_lu_steps: {rc}")
+    return a
+
+
+def l1est(a: np.ndarray, d: np.ndarray) -> np.ndarray:
+    """pmatl1est: approximate factors without a decomposition."""
+    a = np.array(a, dtype=np.float32, order="F", copy=True)
+    _l1est(a.shape[0], _p(a), a.shape[0], _p(np.ascontiguousarray(d, dtype=np.float64)))
     return a
 
 

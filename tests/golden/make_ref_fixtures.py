@@ -14,7 +14,10 @@ the printed refinement steps and report line, the solution vector x (the
 reference's refinement result, collected through TMPI_XDUMP) and, for the
 netlib build, the SHA-256 of the FP32 factors the LU left in memory
 (TMPI_LUDUMP), so that a test can pin a restatement of the LU bit for bit
-without a 5.8 MB fixture.
+without a 5.8 MB fixture.  Two more netlib runs cover the driver's other
+factor paths: `--l1est` (approximate factors without a decomposition) and
+`-w` (the benchmark warm-up: the first P + 2 = 4 block steps, one
+refinement step).
 
 Needs oracle/_ref (built from the reference tree on this machine); the
 fixture it writes is what the tests read.
@@ -52,10 +55,12 @@ def run(exe, flags, ludump):
             digest = hashlib.sha256(lu.tobytes()).hexdigest()
     steps = [{"residual": float(r), "hpl_harness": float(h)} for _, r, h in STEP.findall(out)]
     m = REPORT.search(out)
-    assert x.size == N and steps and m, out[-2000:]
+    assert (x.size == N or "-w" in flags) and steps and m, out[-2000:]
     rec = {"command": f"driver.out {N} {B} {P} " + " ".join(flags), "build": exe,
            "steps": steps, "resid": float(m.group(3)), "hpl_harness": float(m.group(4)),
-           "x": [float(v).hex() for v in x]}
+           "gflops": float(m.group(2)), "seconds": float(m.group(1))}
+    if "-w" not in flags:
+        rec["x"] = [float(v).hex() for v in x]
     if digest:
         rec["lu_sha256"] = digest
     return rec
@@ -64,6 +69,8 @@ def run(exe, flags, ludump):
 def main():
     runs = {
         "netlib_not_r": run("ref_driver_netlib.out", ["-not", "-r"], True),
+        "netlib_l1est": run("ref_driver_netlib.out", ["-not", "-r", "--l1est"], True),
+        "netlib_warmup": run("ref_driver_netlib.out", ["-not", "-r", "-w"], True),
         "netlib_not_d_r": run("ref_driver_netlib.out", ["-not", "-d", "-r"], False),
         "openblas_not_r": run("ref_driver.out", ["-not", "-r"], False),
         "openblas_not_d_r": run("ref_driver.out", ["-not", "-d", "-r"], False),

@@ -1,5 +1,7 @@
 """End-to-end solves through the context API against the oracle (B200)."""
 import json
+import re
+import subprocess
 import os
 
 import numpy as np
@@ -219,3 +221,27 @@ def test_checksum_after_lu_matches_oracle_and_driver(hplai, oracle, torch_cuda, 
     assert items["IR_GEMV"][2] > 0 and items["IR_GEMV"][2] % (2 * n * n) == 0
     assert items["GEMM_UPDATE"][0] > 0 and items["DIAG_BCAST"][0] == 0.0
     assert re.match(r"GEMM_TOTAL: \S+ Tflops$", dump[22])
+
+
+def test_driver_warmup_and_l1est(hplai, torch_cuda, tmp_path):
+    """driver.out -w (the first P + 2 panels, one refinement step, the
+    skipped part taken off the flop count, a Warmup.* phase file) and
+    --l1est (approximate factors, refinement to convergence), as the
+    reference's driver (main.cpp:57,84,282-301,441-446,474)."""
+    exe = os.path.abspath(os.path.join(HERE, "..", "hpl-ai_b200", "driver.out"))
+    n, b, p = 1200, 60, 2
+    out = subprocess.run([exe, str(n), str(b), str(p), "-w", "--job-id", "3"], capture_output=True, text=True,
+                         timeout=300, cwd=tmp_path)
+    assert out.returncode == 0, out.stderr
+    m = re.search(r"^(\S+) sec\. (\S+) GFlop/s resid = (\S+) hpl-harness = (\S+)$", out.stdout, re.M)
+    assert m and float(m.group(3)) == -1.0 and float(m.group(4)) == -1.0, out.stdout
+    nn = n - (p + 2) * b
+    flops = 2 / 3 * n ** 3 + 1.5 * n ** 2 - (2 / 3 * nn ** 3 + 1.5 * nn ** 2)
+    assert abs(float(m.group(2)) - flops / float(m.group(1)) * 1e-9) <= 1e-6 * float(m.group(2))
+    assert (tmp_path / "Warmup.000003.000001200.0060.00001.00000").exists()
+    assert len(re.findall(r"# iterative refinement: step=", out.stdout)) == 1
+    out = subprocess.run([exe, str(n), str(b), str(p), "--l1est"], capture_output=True, text=True, timeout=300,
+                         cwd=tmp_path)
+    assert out.returncode == 0, out.stderr
+    m = re.search(r"resid = (\S+) hpl-harness = (\S+)$", out.stdout, re.M)
+    assert m and 0 <= float(m.group(2)) < 16, out.stdout

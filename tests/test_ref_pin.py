@@ -9,6 +9,11 @@ built by oracle/build_ref.sh).
 * The refinement's step-0 residual and harness equal the reference's in every
   run; step 1 depends on the grid's TRSV summation order (the oracle follows a
   single process column), so it is compared to 1e-8.
+* The driver's two other factor paths pin the same way: `--l1est`
+  (approximate factors without a decomposition) bit for bit, and the `-w`
+  warm-up (the first P + 2 = 4 block steps) bit for bit against the oracle's
+  truncated LU; on the GPU, hplai_l1est is bit-exact and the refinement from
+  it reaches the reference's x.
 * Every solution -- the oracle's, the GPU's plain form, the GPU's precision
   form (e4m3 Schur, GMRES-IR; the FP16 deck needs b % 8 == 0, which b = 60 is
   not) -- equals the reference's x from each of its four runs (`-not -r`,
@@ -30,14 +35,45 @@ def ref_x(run):
     return np.array([float.fromhex(v) for v in FIX["runs"][run]["x"]])
 
 
+SOLVED = sorted(r for r in FIX["runs"] if "x" in FIX["runs"][r] and "l1est" not in r)
+
+
+def digest(a):
+    return hashlib.sha256(np.asfortranarray(a, dtype=np.float32).tobytes(order="F")).hexdigest()
+
+
 def rel(a, b):
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
 def test_oracle_lu_is_the_references_bit_for_bit(oracle):
     lu = oracle.lu(oracle.matrix(N), B)
-    digest = hashlib.sha256(np.asfortranarray(lu).tobytes(order="F")).hexdigest()
-    assert digest == FIX["runs"]["netlib_not_r"]["lu_sha256"]
+    assert digest(lu) == FIX["runs"]["netlib_not_r"]["lu_sha256"]
+
+
+def test_oracle_warmup_lu_is_the_references_bit_for_bit(oracle):
+    """-w: the first P + 2 = 4 block steps (panel_trf.hpp:726)."""
+    lu = oracle.lu_steps(oracle.matrix(N), B, 4)
+    assert digest(lu) == FIX["runs"]["netlib_warmup"]["lu_sha256"]
+
+
+def test_oracle_l1est_is_the_references_bit_for_bit(oracle):
+    a = oracle.l1est(oracle.matrix(N), oracle.diag(N))
+    assert digest(a) == FIX["runs"]["netlib_l1est"]["lu_sha256"]
+
+
+def test_oracle_l1est_refinement_vs_reference(oracle):
+    a = oracle.l1est(oracle.matrix(N), oracle.diag(N))
+    rc, x, res, har, steps = oracle.refine(a, B, 42, oracle.rhs(N), oracle.diag(N), q=2)
+    ref = FIX["runs"]["netlib_l1est"]
+    assert rc == 0 and len(steps) == len(ref["steps"])
+    assert steps[0][0] == ref["steps"][0]["residual"]
+    # the grid's TRSV sums in another order: while the residual is far above
+    # rounding level the steps agree to 1e-8; the last ones are rounding-level
+    for i, (got, want) in enumerate(zip(steps[1:], ref["steps"][1:]), 1):
+        tol = 1e-8 if i <= 2 else 1e-3
+        assert abs(got[0] - want["residual"]) <= tol * want["residual"], i
+    assert rel(x, ref_x("netlib_l1est")) <= 1e-12
 
 
 def test_oracle_refinement_vs_reference_steps(oracle):
@@ -52,7 +88,7 @@ def test_oracle_refinement_vs_reference_steps(oracle):
     assert 0 <= har < 16 and 0 <= FIX["runs"]["netlib_not_r"]["hpl_harness"] < 16
 
 
-@pytest.mark.parametrize("run", sorted(FIX["runs"]))
+@pytest.mark.parametrize("run", SOLVED)
 def test_oracle_x_matches_reference_x(oracle, run):
     rc, x, _, _, _ = oracle.solve(N, B, q=2)
     assert rc == 0
@@ -73,5 +109,41 @@ def test_gpu_x_matches_reference_x(hplai, torch_cuda, form):
         r = s.iterative_refinement(50, mode=mode)
         x = s.x()
     assert r.status == hplai.HPLAI_OK and 0 <= r.hpl_harness < 16
-    for run in FIX["runs"]:
+    for run in SOLVED:
         assert rel(x, ref_x(run)) <= 1e-12, run
+
+
+@pytest.mark.gpu
+def test_gpu_l1est_bit_exact_and_refines_to_reference_x(hplai, oracle, torch_cuda):
+    with hplai.Solver(N, B) as s:
+        s.generate(42)
+        s.l1est()
+        a = s.lu()
+        r = s.iterative_refinement(50)
+        x = s.x()
+        log = s.ir_log()
+    want = oracle.l1est(oracle.matrix(N), oracle.diag(N))
+    assert np.array_equal(a.view(np.uint32), want.view(np.uint32))
+    assert digest(a) == FIX["runs"]["netlib_l1est"]["lu_sha256"]
+    assert r.status == hplai.HPLAI_OK and 0 <= r.hpl_harness < 16
+    assert len(log) == len(FIX["runs"]["netlib_l1est"]["steps"])
+    assert rel(x, ref_x("netlib_l1est")) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_gpu_warmup_factor_steps(hplai, oracle, torch_cuda):
+    """hplai_factor_steps(4): panels 0..3 factored and applied; with the SIMT
+    panels the diagonal blocks and panels of step 0 are the reference's bit
+    for bit, and the whole truncated matrix is within the FP16 Schur
+    update's reordering of the oracle's (the reference's) truncated LU."""
+    with hplai.Solver(N, B, flags=hplai.FLAG_SIMT_PANELS) as s:
+        s.generate(42)
+        s.factor_steps(4)
+        lu = s.lu().astype(np.float64)
+        r = s.iterative_refinement(1)
+    ref = oracle.lu_steps(oracle.matrix(N), B, 4).astype(np.float64)
+    assert np.array_equal(lu[:, :B].astype(np.float32).view(np.uint32), ref[:, :B].astype(np.float32).view(np.uint32))
+    relerr = np.abs(lu - ref) / (np.abs(ref) + 1e-3 * np.abs(ref).max())
+    assert relerr.max() < 1e-3
+    assert r.status == hplai.HPLAI_ENOTCONV and r.hpl_harness == -1.0
+
