@@ -13,10 +13,12 @@
 //
 // Layout.  System s is padded with the identity to P_s = roundup(n_s, 128)
 // (the LU of [[A, 0], [0, I]] is [[L, 0], [0, I]] [[U, 0], [0, I]], exactly:
-// the padding receives only zero updates), and its P_s rows are stacked
-// under the previous system's in one FP32 matrix of `rows` = sum P_s rows
-// and P_max columns (ld = rows): system s's A(i, j) sits at row R_s + i,
-// column j.  Its L and U panels of step k are FP16 copies in two stacked
+// the padding receives only zero updates), and the systems sit side by side
+// in one FP32 matrix of P_max rows (ld = P_max): system s's A(i, j) is at
+// row i, column C_s + j, with 128 unused columns after each system (the
+// last 256-column Schur tile of a step may reach past a system's columns).
+// A system's columns are contiguous in memory, so a 128-column block spans a
+// few pages.  Its L and U panels of step k are FP16 copies in two stacked
 // K-major buffers (row R_s + i of L16 = row i of L, row R_s + j of U16 =
 // column j of U).  Systems are ordered by decreasing P_s, so the systems
 // still factoring at step k are a prefix.
@@ -80,7 +82,8 @@ __device__ __forceinline__ Coeff jump(const JumpT &t, uint64_t m)
 // Per-system descriptor (device copy), in factorisation order.
 struct BSys {
 	int n, P, nrhs, orig;   // order, padded order, right-hand sides, index in the caller's arrays
-	int64_t R;              // first stacked row
+	int64_t R;              // its first row in the stacked FP16 panel buffers
+	int64_t C;              // its first column in A (ld P_max; 128 unused columns after each system)
 	int64_t voff;           // its n x nrhs vectors (rhs, x, r), column-major with ld n
 	int64_t doff;           // its n diagonal entries
 	int64_t poff;           // its GEMV partial sums: ceil(n / kGemvCols) x nrhs x n
@@ -107,7 +110,7 @@ __global__ void __launch_bounds__(256) bfill_kernel(const BSys *__restrict__ sys
 	const int c0 = it.y, c1 = min(c0 + 32, S.P);
 	const Coeff jn = jump(tab, static_cast<uint64_t>(S.n));
 	for (int i = threadIdx.x; i < S.P; i += 256) {
-		float *col = A + S.R + i + static_cast<int64_t>(c0) * lda;
+		float *col = A + i + (S.C + c0) * lda;
 		if (i < S.n) {
 			uint64_t s = coeff_apply(jump(tab, static_cast<uint64_t>(i) + static_cast<uint64_t>(S.n) * c0), S.state0);
 			for (int c = c0; c < c1; ++c, col += lda) {
@@ -157,7 +160,7 @@ __global__ void __launch_bounds__(128) bdiag_kernel(const BSys *__restrict__ sys
 		s0 = coeff_apply(jn, s0);
 	}
 	d[S.doff + i] = sum;
-	A[S.R + i + static_cast<int64_t>(i) * lda] = __double2float_rn(sum);
+	A[i + (S.C + i) * lda] = __double2float_rn(sum);
 }
 
 // rhs column q = stream column n + q (item = (system, first row)).
@@ -180,6 +183,7 @@ __global__ void __launch_bounds__(128) brhs_kernel(const BSys *__restrict__ sys,
 // Factorisation step k.
 // ---------------------------------------------------------------------------
 constexpr int kLdS = kBB + 1;   // shared-memory column pitch (bank-conflict free)
+constexpr int kLdT = kBB + 4;   // pitch of the TRSM triangle: rows of 16-byte aligned float4
 
 // The diagonal block (k, k) of system blockIdx.x (the active prefix).
 __global__ void __launch_bounds__(512) bgetrf_kernel(const BSys *__restrict__ sys, float *__restrict__ A, int64_t lda,
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(512) bgetrf_kernel(const BSys *__restrict__ sy
 {
 	extern __shared__ float sm[];
 	const BSys S = sys[blockIdx.x];
-	float *blk = A + S.R + static_cast<int64_t>(k) * kBB + static_cast<int64_t>(k) * kBB * lda;
+	float *blk = A + static_cast<int64_t>(k) * kBB + (S.C + static_cast<int64_t>(k) * kBB) * lda;
 	for (int e = threadIdx.x; e < kBB * kBB; e += 512) {
 		const int r = e % kBB, c = e / kBB;
 		sm[c * kLdS + r] = blk[r + static_cast<int64_t>(c) * lda];
@@ -211,64 +215,118 @@ __global__ void __launch_bounds__(512) bgetrf_kernel(const BSys *__restrict__ sy
 	}
 }
 
-// blockIdx.y: active system; blockIdx.x: 128-row chunk of its panel below
-// (z = 0: L = A_col U^-1) or 128-column chunk right of (z = 1: U = L^-1 A_row)
-// the diagonal block.  One thread per panel row (column), netlib order:
+// One 128-row chunk of a system's L panel below the diagonal block (side 0:
+// L = A_col U^-1) or one 128-column chunk of its U panel (side 1:
+// U = L^-1 A_row); item = (system, chunk, side).  The netlib strsm order
 //   strsm("R","U","N","N"): for j: for i < j: b_j -= u_ij b_i; b_j *= 1/u_jj
-//   strsm("L","L","N","U"): for i: for r > i: b_r -= l_ri b_i
+//   strsm("L","L","N","U"): for i: if b_i != 0: for r > i: b_r -= l_ri b_i
 // with each multiply-add one fmaf (getrf_nopiv.hpp:14-28 as the reference's
-// -ffp-contract=fast build runs it).
-__global__ void __launch_bounds__(kBB) btrsm_kernel(const BSys *__restrict__ sys, float *__restrict__ A, int64_t lda,
-	__half *__restrict__ L16, __half *__restrict__ U16, int k)
+// -ffp-contract=fast build runs it), applied right-looking: at step i the
+// final b_i is published and every later element takes its update, so each
+// element sees the same updates in the same order as the netlib loops.
+// 256 threads; thread (lane, warp) holds 4 panel rows (side 0; columns for
+// side 1) 4 lane .. 4 lane + 3 times 16 elements 16 warp .. 16 warp + 15 in
+// registers, so the owner of step i is one warp and every other thread
+// updates 64 elements per step from two 16-byte shared-memory reads.
+// The 128 steps of one panel chunk.  Warp oi owns steps 16 oi .. 16 oi + 15
+// (its elements); within a warp's 16 steps the step index is a
+// compile-time constant, so the owner reads and scales its element directly
+// and a thread of a later warp updates all 16 of its elements unpredicated.
+template <bool UPPER>
+__device__ __forceinline__ void trsm_steps(float (&b)[4][16], const float *tri, float *pub, int p0, int e0, int wp)
 {
-	extern __shared__ float sm[];
-	float *tri = sm;                 // the diagonal block, [col][row] with pitch kLdS
-	float *pan = sm + kBB * kLdS;    // the chunk: pan[t * kLdS + e] = element e of this thread's row/column t
-	const BSys S = sys[blockIdx.y];
-	const int nchunks = S.P / kBB - k - 1;
-	if (static_cast<int>(blockIdx.x) >= nchunks) return;
-	const bool upper = blockIdx.z != 0;
-	const int64_t kb = static_cast<int64_t>(k) * kBB;
-	const int64_t off = kb + kBB + static_cast<int64_t>(blockIdx.x) * kBB;   // first panel row / column
-	const float *diag = A + S.R + kb + kb * lda;
-	for (int e = threadIdx.x; e < kBB * kBB; e += kBB) {
-		const int r = e % kBB, c = e / kBB;
-		tri[c * kLdS + r] = diag[r + static_cast<int64_t>(c) * lda];
-	}
-	const int t = threadIdx.x;
-	if (!upper) {
-		// rows off.. of block column k: element (t, e) at A[R + off + t, kb + e]
-		for (int e = 0; e < kBB; ++e) pan[t * kLdS + e] = A[S.R + off + t + (kb + e) * lda];
-	} else {
-		// columns off.. of block row k: element (e, t) at A[R + kb + e, off + t]
-		const float *col = A + S.R + kb + (off + t) * lda;
-		for (int e = 0; e < kBB; ++e) pan[t * kLdS + e] = col[e];
-	}
-	__syncthreads();
-	float *b = pan + t * kLdS;
-	if (!upper) {
-		for (int j = 0; j < kBB; ++j) {
-			float bj = b[j];
-			for (int i = 0; i < j; ++i) {
-				const float uij = tri[j * kLdS + i];
-				if (uij != 0.0f) bj = fmaf(-uij, b[i], bj);
+	for (int oi = 0; oi < 8; ++oi) {
+#pragma unroll
+		for (int li = 0; li < 16; ++li) {
+			const int i = 16 * oi + li;
+			float *pb = pub + (li & 1) * kBB;
+			if (wp == oi) {
+				if (!UPPER) {
+					const float inv = 1.0f / tri[i * kLdT + i];
+#pragma unroll
+					for (int r = 0; r < 4; ++r) b[r][li] = inv * b[r][li];
+				}
+				*reinterpret_cast<float4 *>(pb + p0) = make_float4(b[0][li], b[1][li], b[2][li], b[3][li]);
 			}
-			const float inv = 1.0f / tri[j * kLdS + j];
-			b[j] = inv * bj;
+			__syncthreads();
+			if (wp < oi) continue;
+			const float4 b4 = *reinterpret_cast<const float4 *>(pb + p0);
+			const float bi[4] = {b4.x, b4.y, b4.z, b4.w};
+			const float4 *row = reinterpret_cast<const float4 *>(tri + i * kLdT + e0);
+			const int cfirst = (wp > oi) ? 0 : li + 1;   // a later warp: all 16; the owner: after li
+#pragma unroll
+			for (int g = 0; g < 4; ++g) {
+				if (wp == oi && 4 * g + 3 <= li) continue;
+				const float4 m4 = row[g];
+				const float mg[4] = {m4.x, m4.y, m4.z, m4.w};
+#pragma unroll
+				for (int h = 0; h < 4; ++h) {
+					const int c = 4 * g + h;
+					if (c < cfirst) continue;
+					if (UPPER) {
+#pragma unroll
+						for (int r = 0; r < 4; ++r)
+							if (bi[r] != 0.0f) b[r][c] = fmaf(-bi[r], mg[h], b[r][c]);
+					} else if (mg[h] != 0.0f) {
+#pragma unroll
+						for (int r = 0; r < 4; ++r) b[r][c] = fmaf(-mg[h], bi[r], b[r][c]);
+					}
+				}
+			}
 		}
-		for (int e = 0; e < kBB; ++e) A[S.R + off + t + (kb + e) * lda] = b[e];
-		__half *o = L16 + (S.R + off + t) * kBB;
-		for (int e = 0; e < kBB; e += 2) *reinterpret_cast<__half2 *>(o + e) = __floats2half2_rn(b[e], b[e + 1]);
-	} else {
-		for (int i = 0; i < kBB; ++i) {
-			const float bi = b[i];
-			if (bi != 0.0f)
-				for (int r = i + 1; r < kBB; ++r) b[r] = fmaf(-bi, tri[i * kLdS + r], b[r]);
+	}
+}
+
+constexpr int kTrsmThreads = 256;
+__global__ void __launch_bounds__(kTrsmThreads, 2) btrsm_kernel(const BSys *__restrict__ sys,
+	const int4 *__restrict__ items, float *__restrict__ A, int64_t lda, __half *__restrict__ L16,
+	__half *__restrict__ U16, int k)
+{
+	extern __shared__ __align__(16) float sm[];
+	// side 0: tri[i * kLdT + j] = U(i, j) (rows of U); side 1: tri[i * kLdT + r] = L(r, i) (columns of L)
+	float *tri = sm;
+	float *pub = sm + kBB * kLdT;    // pub[2][128]: step i's final element of each panel row (column)
+	const int4 it = items[blockIdx.x];
+	const BSys S = sys[it.x];
+	const bool upper = it.z != 0;
+	const int64_t kb = static_cast<int64_t>(k) * kBB;
+	const int64_t off = kb + kBB + static_cast<int64_t>(it.y) * kBB;   // first panel row / column
+	const float *diag = A + kb + (S.C + kb) * lda;
+	for (int e = threadIdx.x; e < kBB * kBB; e += kTrsmThreads) {
+		const int r = e % kBB, c = e / kBB;   // diag(r, c)
+		tri[upper ? c * kLdT + r : r * kLdT + c] = diag[r + static_cast<int64_t>(c) * lda];
+	}
+	const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+	const int p0 = 4 * lane, e0 = 16 * wp;   // panel rows (columns) p0..p0+3, elements e0..e0+15
+	float b[4][16];
+	// element e of panel row p: side 0 A(off + p, kb + e); side 1 A(kb + e, off + p)
+#pragma unroll
+	for (int r = 0; r < 4; ++r)
+#pragma unroll
+		for (int c = 0; c < 16; ++c)
+			b[r][c] = upper ? A[kb + e0 + c + (S.C + off + p0 + r) * lda] : A[off + p0 + r + (S.C + kb + e0 + c) * lda];
+	__syncthreads();
+	if (upper) trsm_steps<true>(b, tri, pub, p0, e0, wp);
+	else trsm_steps<false>(b, tri, pub, p0, e0, wp);
+#pragma unroll
+	for (int r = 0; r < 4; ++r) {
+#pragma unroll
+		for (int c = 0; c < 16; ++c) {
+			if (upper) A[kb + e0 + c + (S.C + off + p0 + r) * lda] = b[r][c];
+			else A[off + p0 + r + (S.C + kb + e0 + c) * lda] = b[r][c];
 		}
-		float *col = A + S.R + kb + (off + t) * lda;
-		for (int e = 0; e < kBB; ++e) col[e] = b[e];
-		__half *o = U16 + (S.R + off + t) * kBB;
-		for (int e = 0; e < kBB; e += 2) *reinterpret_cast<__half2 *>(o + e) = __floats2half2_rn(b[e], b[e + 1]);
+		__half *o = (upper ? U16 : L16) + (S.R + off + p0 + r) * kBB + e0;
+#pragma unroll
+		for (int q = 0; q < 2; ++q) {
+			uint4 w;
+			uint32_t *wq = reinterpret_cast<uint32_t *>(&w);
+#pragma unroll
+			for (int h = 0; h < 4; ++h) {
+				const __half2 h2 = __floats2half2_rn(b[r][8 * q + 2 * h], b[r][8 * q + 2 * h + 1]);
+				wq[h] = *reinterpret_cast<const uint32_t *>(&h2);
+			}
+			*reinterpret_cast<uint4 *>(o + 8 * q) = w;
+		}
 	}
 }
 
@@ -402,101 +460,134 @@ __global__ void __launch_bounds__(256) bnorm_kernel(const BSys *__restrict__ sys
 	}
 }
 
-// r <- U^-1 L^-1 r for the refining pairs of one system (blockIdx.x), the
+// r <- U^-1 L^-1 r for the refining (system, right-hand side) pairs, the
 // FP32 factors applied to FP64 vectors (panel_trsvL / panel_trsvU,
-// panel_trsv.hpp:310-758): forward substitution with the unit L, then back
-// substitution with U, 128 rows at a time, all of the system's right-hand
-// sides together; then x += r for those pairs.
-__global__ void __launch_bounds__(256) btrsv_kernel(const BSys *__restrict__ sys, const float *__restrict__ A,
-	int64_t lda, const int *__restrict__ state, double *__restrict__ r, double *__restrict__ x)
+// panel_trsv.hpp:310-758), 128 rows at a time: at step t of the L pass each
+// system solves its diagonal block t (btrsv_diag_kernel) and then every
+// 128-row chunk below it is updated in parallel with that block column
+// (btrsv_off_kernel); the U pass does the same from each system's last block
+// up.  The steps of one correction are a CUDA graph.
+constexpr int kTrsvThreads = 256;   // 8 warps: one per right-hand side
+
+__device__ __forceinline__ bool any_live(const BSys &S, const int *__restrict__ state)
 {
+	for (int q = 0; q < S.nrhs; ++q)
+		if (state[S.pair0 + q] == 0) return true;
+	return false;
+}
+
+// One CTA per system: its diagonal block (L pass: block t; U pass: block
+// nbk-1-t) staged in shared memory and solved by one warp per right-hand
+// side, the solved entry broadcast by shuffle (no block barrier inside).
+__global__ void __launch_bounds__(kTrsvThreads) btrsv_diag_kernel(const BSys *__restrict__ sys,
+	const float *__restrict__ A, int64_t lda, const int *__restrict__ state, double *__restrict__ r, int t, int up)
+{
+	extern __shared__ __align__(16) float blk[];   // blk[j * kLdS + i] = T(j0 + i, j0 + j)
 	const BSys S = sys[blockIdx.x];
-	__shared__ double y[kMaxRhs][kBB];
-	__shared__ int live[kMaxRhs];
-	if (threadIdx.x < kMaxRhs) live[threadIdx.x] = threadIdx.x < S.nrhs && state[S.pair0 + threadIdx.x] == 0;
-	__syncthreads();
-	bool any = false;
-	for (int q = 0; q < S.nrhs; ++q) any |= live[q] != 0;
-	if (!any) return;
 	const int n = S.n, nbk = (n + kBB - 1) / kBB;
-	const float *a = A + S.R;
+	if (t >= nbk || !any_live(S, state)) return;
+	const int jb = up ? nbk - 1 - t : t;
+	const int j0 = jb * kBB, w = min(kBB, n - j0);
+	const float *a = A + S.C * lda;
+	for (int e = threadIdx.x; e < kBB * kBB; e += kTrsvThreads) {
+		const int i = e % kBB, j = e / kBB;
+		blk[j * kLdS + i] = (i < w && j < w) ? a[j0 + i + static_cast<int64_t>(j0 + j) * lda] : 0.f;
+	}
+	__syncthreads();
+	const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	if (q >= S.nrhs || state[S.pair0 + q] != 0) return;
+	double *rv = r + S.voff + static_cast<int64_t>(q) * n + j0;
+	double v[4];
+#pragma unroll
+	for (int m = 0; m < 4; ++m) {
+		const int i = lane + 32 * m;
+		v[m] = i < w ? rv[i] : 0.0;
+	}
+	if (!up) {
+		// unit lower: y_j final in order, then y_i -= L(i, j) y_j for i > j
+		for (int j = 0; j < w; ++j) {
+			double vj = 0.0;
+#pragma unroll
+			for (int m = 0; m < 4; ++m)
+				if (m == (j >> 5)) vj = __shfl_sync(0xffffffffu, v[m], j & 31);
+#pragma unroll
+			for (int m = 0; m < 4; ++m) {
+				const int i = lane + 32 * m;
+				if (i > j && i < w) v[m] = fma(-static_cast<double>(blk[j * kLdS + i]), vj, v[m]);
+			}
+		}
+	} else {
+		// upper: y_j = v_j / U(j, j) from the last row up, then y_i -= U(i, j) y_j for i < j
+		for (int j = w - 1; j >= 0; --j) {
+#pragma unroll
+			for (int m = 0; m < 4; ++m)
+				if (m == (j >> 5) && lane == (j & 31)) v[m] = v[m] / static_cast<double>(blk[j * kLdS + j]);
+			double vj = 0.0;
+#pragma unroll
+			for (int m = 0; m < 4; ++m)
+				if (m == (j >> 5)) vj = __shfl_sync(0xffffffffu, v[m], j & 31);
+#pragma unroll
+			for (int m = 0; m < 4; ++m) {
+				const int i = lane + 32 * m;
+				if (i < j) v[m] = fma(-static_cast<double>(blk[j * kLdS + i]), vj, v[m]);
+			}
+		}
+	}
+#pragma unroll
+	for (int m = 0; m < 4; ++m) {
+		const int i = lane + 32 * m;
+		if (i < w) rv[i] = v[m];
+	}
+}
+
+// item = (system, chunk): 128 rows below (L pass) or above (U pass) the
+// block solved at step t take its update, r_i -= sum_j T(i, j0 + j) y_j,
+// one thread per row, every refining right-hand side at once.
+__global__ void __launch_bounds__(kBB) btrsv_off_kernel(const BSys *__restrict__ sys, const int2 *__restrict__ items,
+	const float *__restrict__ A, int64_t lda, const int *__restrict__ state, double *__restrict__ r, int t, int up)
+{
+	__shared__ double y[kMaxRhs][kBB];
+	const int2 it = items[blockIdx.x];
+	const BSys S = sys[it.x];
+	const int n = S.n, nq = S.nrhs, nbk = (n + kBB - 1) / kBB;
+	if (!any_live(S, state)) return;
+	const int jb = up ? nbk - 1 - t : t;
+	const int j0 = jb * kBB, w = min(kBB, n - j0);
+	const int rbase = up ? it.y * kBB : j0 + kBB + it.y * kBB;
 	double *rv = r + S.voff;
-	// L: for each block column jb: solve the diagonal block, then update the rows below
-	for (int jb = 0; jb < nbk; ++jb) {
-		const int j0 = jb * kBB, j1 = min(j0 + kBB, n);
-		for (int e = threadIdx.x; e < kMaxRhs * kBB; e += 256) {
-			const int q = e / kBB, jj = e % kBB;
-			y[q][jj] = (q < S.nrhs && j0 + jj < j1) ? rv[static_cast<int64_t>(q) * n + j0 + jj] : 0.0;
-		}
-		__syncthreads();
-		for (int j = j0; j < j1; ++j) {
-			// rows j+1 .. j1-1 of the diagonal block
-			for (int e = threadIdx.x; e < (j1 - j - 1) * S.nrhs; e += 256) {
-				const int i = j + 1 + e % (j1 - j - 1), q = e / (j1 - j - 1);
-				y[q][i - j0] = fma(-static_cast<double>(a[i + static_cast<int64_t>(j) * lda]), y[q][j - j0], y[q][i - j0]);
-			}
-			__syncthreads();
-		}
-		for (int e = threadIdx.x; e < S.nrhs * (j1 - j0); e += 256) {
-			const int q = e / (j1 - j0), jj = e % (j1 - j0);
-			rv[static_cast<int64_t>(q) * n + j0 + jj] = y[q][jj];
-		}
-		// rows j1.. : r_i -= sum_j L_ij y_j over the block's columns
-		for (int i = j1 + threadIdx.x; i < n; i += 256) {
-			double acc[kMaxRhs];
-#pragma unroll
-			for (int q = 0; q < kMaxRhs; ++q) acc[q] = 0.0;
-			for (int j = j0; j < j1; ++j) {
-				const double l = a[i + static_cast<int64_t>(j) * lda];
-#pragma unroll
-				for (int q = 0; q < kMaxRhs; ++q)
-					if (q < S.nrhs) acc[q] = fma(l, y[q][j - j0], acc[q]);
-			}
-			for (int q = 0; q < S.nrhs; ++q) rv[static_cast<int64_t>(q) * n + i] -= acc[q];
-		}
-		__syncthreads();
+	for (int e = threadIdx.x; e < kMaxRhs * kBB; e += kBB) {
+		const int q = e / kBB, j = e % kBB;
+		y[q][j] = (q < nq && j < w) ? rv[static_cast<int64_t>(q) * n + j0 + j] : 0.0;
 	}
-	// U: block columns from the last one back
-	for (int jb = nbk - 1; jb >= 0; --jb) {
-		const int j0 = jb * kBB, j1 = min(j0 + kBB, n);
-		for (int e = threadIdx.x; e < kMaxRhs * kBB; e += 256) {
-			const int q = e / kBB, jj = e % kBB;
-			y[q][jj] = (q < S.nrhs && j0 + jj < j1) ? rv[static_cast<int64_t>(q) * n + j0 + jj] : 0.0;
-		}
-		__syncthreads();
-		for (int j = j1 - 1; j >= j0; --j) {
-			if (threadIdx.x < S.nrhs)
-				y[threadIdx.x][j - j0] /= static_cast<double>(a[j + static_cast<int64_t>(j) * lda]);
-			__syncthreads();
-			for (int e = threadIdx.x; e < (j - j0) * S.nrhs; e += 256) {
-				const int i = j0 + e % (j - j0), q = e / (j - j0);
-				y[q][i - j0] = fma(-static_cast<double>(a[i + static_cast<int64_t>(j) * lda]), y[q][j - j0], y[q][i - j0]);
-			}
-			__syncthreads();
-		}
-		for (int e = threadIdx.x; e < S.nrhs * (j1 - j0); e += 256) {
-			const int q = e / (j1 - j0), jj = e % (j1 - j0);
-			rv[static_cast<int64_t>(q) * n + j0 + jj] = y[q][jj];
-		}
-		// rows 0 .. j0-1: r_i -= sum_j U_ij y_j over the block's columns
-		for (int i = threadIdx.x; i < j0; i += 256) {
-			double acc[kMaxRhs];
+	__syncthreads();
+	const int i = rbase + threadIdx.x;
+	if (i >= (up ? j0 : n)) return;
+	const float *arow = A + i + (S.C + j0) * lda;
+	double acc[kMaxRhs];
 #pragma unroll
-			for (int q = 0; q < kMaxRhs; ++q) acc[q] = 0.0;
-			for (int j = j0; j < j1; ++j) {
-				const double u = a[i + static_cast<int64_t>(j) * lda];
+	for (int q = 0; q < kMaxRhs; ++q) acc[q] = 0.0;
+	for (int j = 0; j < w; ++j) {
+		const double l = arow[static_cast<int64_t>(j) * lda];
 #pragma unroll
-				for (int q = 0; q < kMaxRhs; ++q)
-					if (q < S.nrhs) acc[q] = fma(u, y[q][j - j0], acc[q]);
-			}
-			for (int q = 0; q < S.nrhs; ++q) rv[static_cast<int64_t>(q) * n + i] -= acc[q];
-		}
-		__syncthreads();
+		for (int q = 0; q < kMaxRhs; ++q)
+			if (q < nq) acc[q] = fma(l, y[q][j], acc[q]);
 	}
-	// x += correction for the pairs still refining
-	for (int e = threadIdx.x; e < S.nrhs * n; e += 256) {
-		const int q = e / n;
-		if (live[q]) x[S.voff + e] += rv[e];
+	for (int q = 0; q < nq; ++q)
+		if (state[S.pair0 + q] == 0) rv[static_cast<int64_t>(q) * n + i] -= acc[q];
+}
+
+// x += r for the pairs still refining; item = (system, first row)
+__global__ void __launch_bounds__(128) bxupd_kernel(const BSys *__restrict__ sys, const int2 *__restrict__ items,
+	const int *__restrict__ state, const double *__restrict__ r, double *__restrict__ x)
+{
+	const int2 it = items[blockIdx.x];
+	const BSys S = sys[it.x];
+	const int i = it.y + threadIdx.x;
+	if (i >= S.n) return;
+	for (int q = 0; q < S.nrhs; ++q) {
+		if (state[S.pair0 + q] != 0) continue;
+		const int64_t e = S.voff + static_cast<int64_t>(q) * S.n + i;
+		x[e] += r[e];
 	}
 }
 
@@ -507,14 +598,21 @@ __global__ void __launch_bounds__(256) btrsv_kernel(const BSys *__restrict__ sys
 // ---------------------------------------------------------------------------
 struct BatchEngine {
 	int count = 0, pmax = 0, nsteps = 0, npairs = 0;
-	int64_t rows = 0, lda = 0;
+	int64_t rows = 0, cols = 0, lda = 0;
 	std::vector<BSys> sys;                 // factorisation order
 	std::vector<int> active;               // systems still factoring at step k (a prefix)
 	std::vector<int> tile_off, tile_cnt;   // each step's slice of the tile table
+	std::vector<int> trsm_off, trsm_cnt;   // each step's slice of the panel-chunk list
+	std::vector<int> off_off, off_cnt;     // each refinement step's slice of the row-chunk list
+	int2 *off_items = nullptr;
+	cudaGraph_t cgraph = nullptr;          // one correction (both triangular solves and x += r)
+	cudaGraphExec_t cexec = nullptr;
+
 	int n_fill = 0, n_rows = 0, n_gemv = 0, max_chunks = 0;
 	float *A = nullptr;
 	__half *L16 = nullptr, *U16 = nullptr;
 	double *d = nullptr, *rhs = nullptr, *x = nullptr, *r = nullptr, *part = nullptr, *res = nullptr;
+	int4 *trsm_items = nullptr;
 	int *state = nullptr, *iters = nullptr, *counter = nullptr, *host_counter = nullptr;
 	BSys *dsys = nullptr;
 	int2 *fill_items = nullptr, *row_items = nullptr, *pairs = nullptr;
@@ -526,7 +624,7 @@ struct BatchEngine {
 	cudaGraphExec_t exec = nullptr;
 	std::vector<double> h_res;
 	std::vector<int> h_state, h_iters;
-	unsigned long long launches_per_solve = 0;
+	unsigned long long launches_per_solve = 0, correction_launches = 0;
 };
 
 namespace {
@@ -536,6 +634,9 @@ void engine_free(BatchEngine *e)
 	if (!e) return;
 	if (e->exec) cudaGraphExecDestroy(e->exec);
 	if (e->graph) cudaGraphDestroy(e->graph);
+	if (e->cexec) cudaGraphExecDestroy(e->cexec);
+	if (e->cgraph) cudaGraphDestroy(e->cgraph);
+	cudaFree(e->off_items);
 	cudaFree(e->A);
 	cudaFree(e->L16);
 	cudaFree(e->U16);
@@ -554,6 +655,7 @@ void engine_free(BatchEngine *e)
 	cudaFree(e->pairs);
 	cudaFree(e->gemv_items);
 	cudaFree(e->tiles);
+	cudaFree(e->trsm_items);
 	cudaFree(e->status);
 	if (e->host_counter) cudaFreeHost(e->host_counter);
 	if (e->st) cudaStreamDestroy(e->st);
@@ -570,7 +672,8 @@ int upload(T **dst, const std::vector<T> &v)
 }
 
 constexpr size_t kGetrfSmem = sizeof(float) * kBB * kLdS;
-constexpr size_t kTrsmSmem = 2 * sizeof(float) * kBB * kLdS;
+constexpr size_t kTrsmSmem = sizeof(float) * (kBB * kLdT + 2 * kBB);
+constexpr size_t kTrsvSmem = sizeof(float) * kBB * kLdS;
 
 // Generation and factorisation of every system, in stream order.
 int enqueue_factor(BatchEngine *e)
@@ -588,9 +691,9 @@ int enqueue_factor(BatchEngine *e)
 		bgetrf_kernel<<<m, 512, kGetrfSmem, st>>>(e->dsys, e->A, e->lda, k);
 		HPLAI_CUDA_TRY(cudaGetLastError());
 		++launches;
-		const int nch = e->pmax / kBB - k - 1;
-		if (nch <= 0) continue;
-		btrsm_kernel<<<dim3(nch, m, 2), kBB, kTrsmSmem, st>>>(e->dsys, e->A, e->lda, e->L16, e->U16, k);
+		if (e->trsm_cnt[k] <= 0) continue;
+		btrsm_kernel<<<e->trsm_cnt[k], kTrsmThreads, kTrsmSmem, st>>>(e->dsys, e->trsm_items + e->trsm_off[k], e->A, e->lda,
+			e->L16, e->U16, k);
 		HPLAI_CUDA_TRY(cudaGetLastError());
 		++launches;
 		if (e->tile_cnt[k] > 0) {
@@ -600,6 +703,48 @@ int enqueue_factor(BatchEngine *e)
 	}
 	e->launches_per_solve = launches;
 	return HPLAI_OK;
+}
+
+// One correction of every refining pair: U^-1 L^-1 r, then x += r.
+int enqueue_correction(BatchEngine *e, unsigned long long *launches)
+{
+	cudaStream_t st = e->st;
+	unsigned long long nl = 0;
+	for (int up = 0; up < 2; ++up)
+		for (int t = 0; t < e->nsteps; ++t) {
+			const int m = e->active[t];
+			if (m <= 0) break;
+			btrsv_diag_kernel<<<m, kTrsvThreads, kTrsvSmem, st>>>(e->dsys, e->A, e->lda, e->state, e->r, t, up);
+			HPLAI_CUDA_TRY(cudaGetLastError());
+			++nl;
+			if (e->off_cnt[t] > 0) {
+				btrsv_off_kernel<<<e->off_cnt[t], kBB, 0, st>>>(e->dsys, e->off_items + e->off_off[t], e->A, e->lda,
+					e->state, e->r, t, up);
+				HPLAI_CUDA_TRY(cudaGetLastError());
+				++nl;
+			}
+		}
+	bxupd_kernel<<<e->n_rows, 128, 0, st>>>(e->dsys, e->row_items, e->state, e->r, e->x);
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	*launches = nl + 1;
+	return HPLAI_OK;
+}
+
+// Captures the work enqueue() puts on e->st into a graph.
+template <typename F>
+int capture(BatchEngine *e, cudaGraph_t *graph, cudaGraphExec_t *exec, F enqueue)
+{
+	if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HPLAI_ECUDA;
+	const int er = enqueue();
+	cudaGraph_t g = nullptr;
+	const cudaError_t ce = cudaStreamEndCapture(e->st, &g);
+	(void)cudaGetLastError();
+	if (er != HPLAI_OK || ce != cudaSuccess) {
+		if (g) cudaGraphDestroy(g);
+		return er != HPLAI_OK ? er : HPLAI_ECUDA;
+	}
+	*graph = g;
+	return cudaGraphInstantiate(exec, g, 0) == cudaSuccess ? HPLAI_OK : HPLAI_ECUDA;
 }
 
 } // namespace
@@ -615,7 +760,7 @@ int batched_create(BatchEngine **out, int count, const int *n, const int *nrhs, 
 	std::vector<int> order(count);
 	std::iota(order.begin(), order.end(), 0);
 	std::stable_sort(order.begin(), order.end(), [&](int p, int q) { return n[p] > n[q]; });
-	int64_t rows = 0, voff = 0, doff = 0, poff = 0;
+	int64_t rows = 0, cols = 0, voff = 0, doff = 0, poff = 0;
 	int pair = 0;
 	std::vector<int2> pairs;
 	for (int s : order) {
@@ -625,12 +770,14 @@ int batched_create(BatchEngine **out, int count, const int *n, const int *nrhs, 
 		S.nrhs = nrhs[s];
 		S.orig = s;
 		S.R = rows;
+		S.C = cols;
 		S.voff = voff;
 		S.doff = doff;
 		S.poff = poff;
 		S.pair0 = pair;
 		S.state0 = state_initial(seeds[s]);
 		rows += S.P;
+		cols += S.P + kBB;
 		voff += static_cast<int64_t>(S.n) * S.nrhs;
 		doff += S.n;
 		poff += static_cast<int64_t>((S.n + kGemvCols - 1) / kGemvCols) * S.nrhs * S.n;
@@ -641,7 +788,8 @@ int batched_create(BatchEngine **out, int count, const int *n, const int *nrhs, 
 	}
 	e->npairs = pair;
 	e->rows = rows;
-	e->lda = (rows + 3) / 4 * 4;   // TMA strides are multiples of 16 bytes
+	e->cols = cols;
+	e->lda = e->pmax;   // a multiple of 128 floats: 16-byte TMA strides
 	e->nsteps = e->pmax / kBB;
 	for (int k = 0; k < e->nsteps; ++k) {
 		int m = 0;
@@ -650,13 +798,34 @@ int batched_create(BatchEngine **out, int count, const int *n, const int *nrhs, 
 	}
 	// work lists
 	std::vector<int2> fill, rowi;
-	std::vector<int4> gemv, tiles;
+	std::vector<int4> gemv, tiles, trsm;
 	for (int i = 0; i < count; ++i) {
 		const BSys &S = e->sys[i];
 		for (int c = 0; c < S.P; c += 32) fill.push_back(make_int2(i, c));
 		for (int r = 0; r < S.n; r += 128) rowi.push_back(make_int2(i, r));
 		for (int r = 0; r < S.n; r += kGemvRows)
 			for (int c = 0; c * kGemvCols < S.n; ++c) gemv.push_back(make_int4(i, r, c, 0));
+	}
+	// refinement step t: the 128-row chunks off the diagonal block (below it
+	// in the L pass, above it in the U pass: nbk - 1 - t either way)
+	std::vector<int2> offi;
+	for (int t = 0; t < e->nsteps; ++t) {
+		e->off_off.push_back(static_cast<int>(offi.size()));
+		for (int i = 0; i < e->active[t]; ++i) {
+			const int nbk = e->sys[i].P / kBB;
+			for (int c = 0; c < nbk - 1 - t; ++c) offi.push_back(make_int2(i, c));
+		}
+		e->off_cnt.push_back(static_cast<int>(offi.size()) - e->off_off.back());
+	}
+	// panel chunks of step k: 128 rows of L and 128 columns of U at a time
+	for (int k = 0; k < e->nsteps; ++k) {
+		e->trsm_off.push_back(static_cast<int>(trsm.size()));
+		for (int i = 0; i < e->active[k]; ++i) {
+			const int nch = e->sys[i].P / kBB - k - 1;
+			for (int c = 0; c < nch; ++c)
+				for (int side = 0; side < 2; ++side) trsm.push_back(make_int4(i, c, side, 0));
+		}
+		e->trsm_cnt.push_back(static_cast<int>(trsm.size()) - e->trsm_off.back());
 	}
 	// tiles of step k: the trailing rows and columns from (k + 1) * 128 of every
 	// system still factoring, 128-row x 256-column tiles
@@ -667,14 +836,15 @@ int batched_create(BatchEngine **out, int count, const int *n, const int *nrhs, 
 			const int t0 = (k + 1) * kBB;
 			for (int c = t0; c < S.P; c += 256)
 				for (int rr = t0; rr < S.P; rr += kBB)
-					tiles.push_back(make_int4(static_cast<int>(S.R + rr), static_cast<int>(S.R + c),
-						static_cast<int>(S.R + rr), c));
+					tiles.push_back(make_int4(static_cast<int>(S.R + rr), static_cast<int>(S.R + c), rr,
+						static_cast<int>(S.C + c)));
 		}
 		e->tile_cnt.push_back(static_cast<int>(tiles.size()) - e->tile_off.back());
 	}
 	e->n_fill = static_cast<int>(fill.size());
 	e->n_rows = static_cast<int>(rowi.size());
 	e->n_gemv = static_cast<int>(gemv.size());
+
 	int rc = HPLAI_OK;
 	auto alloc = [&](void **p, size_t bytes) {
 		if (rc == HPLAI_OK && cudaMalloc(p, bytes) != cudaSuccess) {
@@ -682,8 +852,8 @@ int batched_create(BatchEngine **out, int count, const int *n, const int *nrhs, 
 			rc = HPLAI_ENOMEM;
 		}
 	};
-	if (rows > (int64_t(1) << 31) - 1) rc = HPLAI_EUNSUPPORTED;   // int tile coordinates
-	alloc(reinterpret_cast<void **>(&e->A), sizeof(float) * static_cast<size_t>(e->lda) * e->pmax);
+	if (rows > (int64_t(1) << 31) - 1 || cols > (int64_t(1) << 31) - 1) rc = HPLAI_EUNSUPPORTED;   // int tile coordinates
+	alloc(reinterpret_cast<void **>(&e->A), sizeof(float) * static_cast<size_t>(e->lda) * e->cols);
 	alloc(reinterpret_cast<void **>(&e->L16), sizeof(__half) * static_cast<size_t>(rows) * kBB);
 	alloc(reinterpret_cast<void **>(&e->U16), sizeof(__half) * static_cast<size_t>(rows) * kBB);
 	alloc(reinterpret_cast<void **>(&e->d), sizeof(double) * static_cast<size_t>(doff));
@@ -691,6 +861,7 @@ int batched_create(BatchEngine **out, int count, const int *n, const int *nrhs, 
 	alloc(reinterpret_cast<void **>(&e->x), sizeof(double) * static_cast<size_t>(voff));
 	alloc(reinterpret_cast<void **>(&e->r), sizeof(double) * static_cast<size_t>(voff));
 	alloc(reinterpret_cast<void **>(&e->part), sizeof(double) * static_cast<size_t>(poff));
+
 	alloc(reinterpret_cast<void **>(&e->res), sizeof(double) * 2 * pair);
 	alloc(reinterpret_cast<void **>(&e->state), sizeof(int) * pair);
 	alloc(reinterpret_cast<void **>(&e->iters), sizeof(int) * pair);
@@ -698,39 +869,30 @@ int batched_create(BatchEngine **out, int count, const int *n, const int *nrhs, 
 	alloc(reinterpret_cast<void **>(&e->status), sizeof(unsigned));
 	if (rc == HPLAI_OK && (upload(&e->dsys, e->sys) != HPLAI_OK || upload(&e->fill_items, fill) != HPLAI_OK ||
 		upload(&e->row_items, rowi) != HPLAI_OK || upload(&e->pairs, pairs) != HPLAI_OK ||
-		upload(&e->gemv_items, gemv) != HPLAI_OK || upload(&e->tiles, tiles) != HPLAI_OK))
+		upload(&e->gemv_items, gemv) != HPLAI_OK || upload(&e->tiles, tiles) != HPLAI_OK ||
+		upload(&e->trsm_items, trsm) != HPLAI_OK || upload(&e->off_items, offi) != HPLAI_OK))
 		rc = HPLAI_ECUDA;
 	if (rc == HPLAI_OK && cudaHostAlloc(reinterpret_cast<void **>(&e->host_counter), sizeof(int), 0) != cudaSuccess)
 		rc = HPLAI_ENOMEM;
 	if (rc == HPLAI_OK && cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess) rc = HPLAI_ECUDA;
 	if (rc == HPLAI_OK && (cudaFuncSetAttribute(bgetrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(kGetrfSmem)) != cudaSuccess || cudaFuncSetAttribute(btrsm_kernel,
-		cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kTrsmSmem)) != cudaSuccess))
+		cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kTrsmSmem)) != cudaSuccess ||
+		cudaFuncSetAttribute(btrsv_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		static_cast<int>(kTrsvSmem)) != cudaSuccess))
 		rc = HPLAI_ECUDA;
 	if (rc == HPLAI_OK && cudaMemset(e->status, 0, sizeof(unsigned)) != cudaSuccess) rc = HPLAI_ECUDA;
 	if (rc == HPLAI_OK) rc = schur_make_maps(&e->maps, reinterpret_cast<const uint16_t *>(e->L16),
 		static_cast<int>(rows), kBB, reinterpret_cast<const uint16_t *>(e->U16), static_cast<int>(rows), kBB, kBB);
-	if (rc == HPLAI_OK) rc = schur_set_cmap(&e->maps, e->A, static_cast<int>(rows), e->pmax, e->lda);
+	if (rc == HPLAI_OK) rc = schur_set_cmap(&e->maps, e->A, e->pmax, static_cast<int>(e->cols), e->lda);
 	if (rc == HPLAI_OK && !e->maps.has_cmap) rc = HPLAI_EINVAL;
 	e->maps.status = e->status;
-	// the generation and the factorisation as one graph, replayed per solve
-	if (rc == HPLAI_OK) {
-		if (cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-			rc = HPLAI_ECUDA;
-		} else {
-			const int er = enqueue_factor(e);
-			cudaGraph_t g = nullptr;
-			const cudaError_t ce = cudaStreamEndCapture(e->st, &g);
-			if (er != HPLAI_OK || ce != cudaSuccess) {
-				if (g) cudaGraphDestroy(g);
-				rc = er != HPLAI_OK ? er : HPLAI_ECUDA;
-			} else {
-				e->graph = g;
-				if (cudaGraphInstantiate(&e->exec, g, 0) != cudaSuccess) rc = HPLAI_ECUDA;
-			}
-		}
-		(void)cudaGetLastError();
-	}
+	// the generation and the factorisation as one graph, replayed per solve,
+	// and one correction as another, replayed per refinement step
+	if (rc == HPLAI_OK) rc = capture(e, &e->graph, &e->exec, [&] { return enqueue_factor(e); });
+	unsigned long long cl = 0;
+	if (rc == HPLAI_OK) rc = capture(e, &e->cgraph, &e->cexec, [&] { return enqueue_correction(e, &cl); });
+	e->correction_launches = cl;
 	if (rc != HPLAI_OK) {
 		engine_free(e);
 		return rc;
@@ -766,9 +928,8 @@ int batched_solve(BatchEngine *e, int maxit, unsigned long long *launches)
 		HPLAI_CUDA_TRY(cudaMemcpyAsync(e->host_counter, e->counter, sizeof(int), cudaMemcpyDeviceToHost, st));
 		HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
 		if (*e->host_counter == 0) break;
-		btrsv_kernel<<<e->count, 256, 0, st>>>(e->dsys, e->A, e->lda, e->state, e->r, e->x);
-		HPLAI_CUDA_TRY(cudaGetLastError());
-		++nl;
+		HPLAI_CUDA_TRY(cudaGraphLaunch(e->cexec, st));
+		nl += e->correction_launches;
 	}
 	HPLAI_CUDA_TRY(cudaMemcpyAsync(e->h_res.data(), e->res, sizeof(double) * 2 * e->npairs, cudaMemcpyDeviceToHost,
 		st));
@@ -830,7 +991,7 @@ int batched_get_lu(BatchEngine *e, int orig, float *a, int64_t lda)
 	for (const BSys &S : e->sys) {
 		if (S.orig != orig) continue;
 		if (lda < S.n) return HPLAI_EINVAL;
-		HPLAI_CUDA_TRY(cudaMemcpy2D(a, sizeof(float) * lda, e->A + S.R, sizeof(float) * e->lda, sizeof(float) * S.n,
+		HPLAI_CUDA_TRY(cudaMemcpy2D(a, sizeof(float) * lda, e->A + S.C * e->lda, sizeof(float) * e->lda, sizeof(float) * S.n,
 			S.n, cudaMemcpyDeviceToHost));
 		return HPLAI_OK;
 	}
