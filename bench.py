@@ -343,7 +343,7 @@ class FormRun:
     hpl-harness < 16) after `warmup` untimed ones, the matrix regenerated on
     the device before each solve outside the timed window."""
 
-    def __init__(self, hplai, torch, form, n, b, seed, maxit, autotune, lookahead, barrier, group=1):
+    def __init__(self, hplai, torch, form, n, b, seed, maxit, autotune, lookahead, barrier, group=1, side_sms=32):
         self.hplai, self.torch, self.form = hplai, torch, form
         self.n, self.b, self.seed, self.maxit = n, b, seed, maxit
         self.fp8 = form["precision"] == "f8"
@@ -359,18 +359,24 @@ class FormRun:
         self.barrier = barrier
         self.tuned = None
         self.group = 2 if (flags & hplai.FLAG_GROUP2) else 1
-        self.schedule = {"lookahead": bool(lookahead), "side_sms": None, "panels_per_update": self.group,
-                         "source": "flags"}
+        if lookahead:
+            self.s.set_schedule(flags & (hplai.FLAG_LOOKAHEAD | hplai.FLAG_GROUP2), side_sms)
+        self.schedule = {"lookahead": bool(lookahead), "side_sms": side_sms if lookahead else None,
+                         "panels_per_update": self.group, "source": "flags"}
         if autotune:
             # outside the timed region: time the factorisation under each schedule, keep the fastest
             tflags, tside, tms = self.s.autotune(seed)
             la = bool(tflags & hplai.FLAG_LOOKAHEAD)
             self.group = 2 if (tflags & hplai.FLAG_GROUP2) else 1
+            def side_desc(f, sd):
+                if not (f & hplai.FLAG_LOOKAHEAD):
+                    return None
+                return sd if sd > 0 else f"share sms*c/(r+c), c={-sd} panels, r = trailing block columns"
             trials = [{"panels_per_update": 2 if (f & hplai.FLAG_GROUP2) else 1,
-                       "lookahead": bool(f & hplai.FLAG_LOOKAHEAD), "side_sms": sd if (f & hplai.FLAG_LOOKAHEAD) else None,
+                       "lookahead": bool(f & hplai.FLAG_LOOKAHEAD), "side_sms": side_desc(f, sd),
                        "factor_ms": round(ms, 2)} for f, sd, ms in self.s.autotune_log()]
             self.tuned = {"factor_ms_median": tms, "trials_warmup_first": trials}
-            self.schedule = {"lookahead": la, "side_sms": tside if la else None, "panels_per_update": self.group,
+            self.schedule = {"lookahead": la, "side_sms": side_desc(tflags, tside), "panels_per_update": self.group,
                              "source": "hplai_autotune"}
         self.results = []
 
@@ -502,7 +508,8 @@ def run_ours(args):
                               f"{'GMRES-IR' if head_form['refine'] == 'gmres' else 'IR'}")
 
     # the headline form: exactly `steps` timed solves after `warmup`
-    fr = FormRun(hplai, torch, head_form, n, b, seed, maxit, args.autotune, args.lookahead, barrier, args.group)
+    fr = FormRun(hplai, torch, head_form, n, b, seed, maxit, args.autotune, args.lookahead, barrier, args.group,
+                 args.side_sms)
     fr.run(0, args.warmup)
     sampler = ClockSampler(dev)
     sampler.start()
@@ -520,7 +527,7 @@ def run_ours(args):
     other = None
     if other_key:
         fo = FormRun(hplai, torch, FORMS[other_key], n, b, seed, maxit, args.autotune, args.lookahead, barrier,
-                     args.group)
+                     args.group, args.side_sms)
         fo.run(min(args.steps, args.compare_steps), min(args.warmup, args.compare_warmup))
         other = fo.summary(world)
         fo.close()
@@ -550,6 +557,7 @@ def run_ours(args):
             "dtype": "e4m3/fp16/fp32/fp64" if head_form["precision"] == "f8" else "fp16/fp32/fp64",
             "data": "synthetic (the reference's own LCG matrix, seed 42, regenerated on the device before each step)",
             "config": {"workload": wl, "n": n, "b": b, "form": head["form"], "schedule": head["schedule"],
+                       "autotuned": head["autotuned"],
                        "trailing_matrix": head["trailing_matrix"],
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": f"inputs {n * n * 4 / 1e9:.1f} GB FP32 > 126 MB L2, rewritten between steps"},
@@ -857,6 +865,7 @@ def main():
                     help="choose the schedule (serial or look-ahead, side-stream SMs) with hplai_autotune first "
                          "(the default for the solve workload unless --lookahead or --no-autotune is given)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the serial schedule (or --lookahead's)")
+    ap.add_argument("--side-sms", type=int, default=32, help="SMs of the side stream with --lookahead (no autotune)")
     ap.add_argument("--group", type=int, choices=(1, 2), default=1,
                     help="panels per trailing update without autotuning (2 = HPLAI_FLAG_GROUP2, b % 128 == 0)")
     ap.add_argument("--lookahead", action="store_true",

@@ -629,27 +629,43 @@ int factor_impl(hplai_ctx *c, int kend)
 	// With HPLAI_FLAG_LOOKAHEAD they are formed on the side stream while the
 	// main stream applies the rest, which then leaves side_sms SMs to the
 	// side stream; otherwise everything runs in the same order on one stream.
-	const int kSideSms = c->side_sms;
 	cudaStream_t st = c->st, sd = serial ? c->st : c->st2;
-	const int side_ctas = serial ? 0 : kSideSms;
 	int sms = 148;
 	{
 		int dev = 0;
 		if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	}
-	const int main_ctas = (serial || sms <= 2 * kSideSms) ? 0 : sms - kSideSms;
+	// SMs left to the side stream while it forms the panels of the group
+	// starting at block e: a fixed count (side_sms > 0) or, with side_sms < 0,
+	// a share of c = -side_sms panels against the remaining trailing blocks,
+	// sms * c / (rem / b + c): the panel work grows with rem, the update with
+	// rem^2, so the side stream needs more SMs as the matrix shrinks.  A share
+	// above one half forms the group's panels on the whole GPU before the
+	// rest of the update (no overlap).  0: no overlap.
+	auto side_for = [&](int e) -> int {
+		if (serial) return 0;
+		int side = c->side_sms;
+		if (side < 0) {
+			const double cp = -side, rb = static_cast<double>(n - e * b) / b;
+			side = static_cast<int>(std::lround(sms * cp / (rb + cp)));
+			if (side < 8) side = 8;
+		}
+		return (2 * side > sms) ? 0 : side;
+	};
 	// the side stream starts from the generated matrix: group 0's panels
 	HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));
 	HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_next, 0));
 	for (int j = 0; j < G && j < nb && j < kend; ++j) {
-		HPLAI_TRY(prepare_block(c, j, 0, 0, simt, side_ctas, sd, pe));
-		HPLAI_TRY(panel_step(c, j, 0, j, simt, side_ctas, sd, pe));
+		HPLAI_TRY(prepare_block(c, j, 0, 0, simt, 0, sd, pe));
+		HPLAI_TRY(panel_step(c, j, 0, j, simt, 0, sd, pe));
 	}
 	for (int s = 0; s + G < nb && (kend >= nb || s + 1 < kend); s += G) {
 		const int q = (s / G) & 1;
 		const int e = s + G, ne = std::min(G, nb - e);
 		const int r1 = e * b, r2 = (e + ne) * b;
 		const Operands op = group_operands(c, q, e);
+		const int side = side_for(e);
+		const int side_ctas = side, main_ctas = side ? sms - side : 0;
 		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_panel, sd));
 		HPLAI_CUDA_TRY(cudaStreamWaitEvent(st, c->ev_panel, 0));
 		// the next group's block columns (rows r1..n) and block rows (columns r2..n)
@@ -660,6 +676,11 @@ int factor_impl(hplai_ctx *c, int kend)
 		for (int j = e; j < e + ne && j < kend; ++j) {
 			HPLAI_TRY(prepare_block(c, j, e, q ^ 1, simt, side_ctas, sd, pe));
 			HPLAI_TRY(panel_step(c, j, q ^ 1, j - e, simt, side_ctas, sd, pe));
+		}
+		if (!serial && side == 0) {
+			// no overlap for this group: its panels first, on the whole GPU
+			HPLAI_CUDA_TRY(cudaEventRecord(c->ev_panel, sd));
+			HPLAI_CUDA_TRY(cudaStreamWaitEvent(st, c->ev_panel, 0));
 		}
 		// the rest of the trailing matrix
 		HPLAI_TRY(schur_region(c, op, r2, n, r2, n, main_ctas, st, pe));
@@ -985,8 +1006,10 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 	for (int g = 1; g <= c->gcap; ++g) {
 		const unsigned gf = g == 2 ? HPLAI_FLAG_GROUP2 : 0u;
 		cands.push_back({gf, 20, {}});
-		for (int side : {16, 24, 32})
+		for (int side : {16, 32})
 			if (sms > 2 * side) cands.push_back({gf | HPLAI_FLAG_LOOKAHEAD, side, {}});
+		// side-stream share growing as the trailing matrix shrinks
+		for (int share : {8, 16, 24}) cands.push_back({gf | HPLAI_FLAG_LOOKAHEAD, -share, {}});
 	}
 	const unsigned sched_bits = HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2;
 	const unsigned flags0 = c->flags, base_flags = c->flags & ~sched_bits;
@@ -1056,6 +1079,16 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 	if (flags_out) *flags_out = c->flags;
 	if (side_sms_out) *side_sms_out = c->side_sms;
 	if (ms_out) *ms_out = best;
+	return HPLAI_OK;
+}
+
+extern "C" int hplai_set_schedule(hplai_ctx *c, unsigned flags, int side_sms)
+{
+	const unsigned sched = HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2;
+	if (!c || (flags & ~sched) || side_sms == 0 || side_sms > 64 || side_sms < -256) return HPLAI_EINVAL;
+	if ((flags & HPLAI_FLAG_GROUP2) && c->gcap != 2) return HPLAI_EINVAL;
+	c->flags = (c->flags & ~sched) | flags;
+	c->side_sms = side_sms;
 	return HPLAI_OK;
 }
 

@@ -61,6 +61,7 @@ _factor = _proto("hplai_factor", _c_int, _vp)
 _factor_steps = _proto("hplai_factor_steps", _c_int, _vp, _c_int)
 _l1est = _proto("hplai_l1est", _c_int, _vp)
 _autotune = _proto("hplai_autotune", _c_int, _vp, _c_u64, _vp, _vp, _vp)
+_set_schedule = _proto("hplai_set_schedule", _c_int, _vp, ctypes.c_uint, _c_int)
 _autotune_log = _proto("hplai_get_autotune_log", _c_int, _vp, _vp, _vp, _vp, _c_int, ctypes.POINTER(_c_int))
 _refine = _proto("hplai_refine", _c_int, _vp, _c_int, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
 _get_x = _proto("hplai_get_x", _c_int, _vp, _vp)
@@ -218,6 +219,10 @@ class Solver:
         fl, side, ms = ctypes.c_uint(), _c_int(), ctypes.c_double()
         check(_autotune(self._h, seed, ctypes.byref(fl), ctypes.byref(side), ctypes.byref(ms)), "hplai_autotune")
         return fl.value, side.value, ms.value
+
+    def set_schedule(self, flags: int, side_sms: int = 32):
+        """Look-ahead / two-panel groups and the side stream's SMs, by hand."""
+        check(_set_schedule(self._h, flags, side_sms), "hplai_set_schedule")
 
     def autotune_log(self):
         """The last autotune's trials: [(flags, side_sms, ms)], warm-up first."""

@@ -162,13 +162,25 @@ int hplai_l1est(hplai_ctx *ctx);
 /* Schedule tuner in place of lda_tuner (lda_tuner.hpp:9-45): times
  * hplai_factor on this context (regenerated from seed before each trial)
  * under each schedule -- one- or two-panel groups (HPLAI_FLAG_GROUP2, when
- * b % 128 == 0), serial or with HPLAI_FLAG_LOOKAHEAD at several side-stream
- * SM counts -- after one discarded warm-up factorisation, re-times the two
+ * b % 128 == 0), serial or with HPLAI_FLAG_LOOKAHEAD at fixed side-stream SM
+ * counts or at shares growing as the trailing matrix shrinks (negative
+ * side_sms, see hplai_set_schedule) -- after one discarded warm-up
+ * factorisation, re-times the two
  * fastest twice more, keeps the one with the lowest median as the context's
  * schedule, and leaves the context generated and unfactored.  Outputs (may
  * be NULL): the chosen flags, the side-stream SM count and the chosen
  * schedule's median factorisation time in ms. */
 int hplai_autotune(hplai_ctx *ctx, uint64_t seed, unsigned *flags, int *side_sms, double *ms);
+/* Sets the schedule by hand, as hplai_autotune would: `flags` a combination
+ * of HPLAI_FLAG_LOOKAHEAD and HPLAI_FLAG_GROUP2 (the other flags of the
+ * context are kept), side_sms the SMs left to the side stream with
+ * look-ahead: a fixed count (1 .. 64), or, negative, a share growing as the
+ * trailing matrix shrinks -- with c = -side_sms (1 .. 256) the group whose
+ * trailing matrix has r block columns left gets sms * c / (r + c) SMs, and
+ * forms its panels on the whole GPU, without overlap, once that is more
+ * than half of them.  The reference's schedule is fixed at build time
+ * (panel_lu_async / RDMAPanelLU::run, panel_trf.hpp:434-858). */
+int hplai_set_schedule(hplai_ctx *ctx, unsigned flags, int side_sms);
 /* The trials of the last hplai_autotune in the order they ran (the warm-up
  * first): flags, side-stream SMs and factorisation ms of each; *count is
  * the number of trials (at most cap are written).  No counterpart in the

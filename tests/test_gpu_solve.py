@@ -167,7 +167,7 @@ def test_autotune_picks_a_schedule_and_solves(hplai, oracle, torch_cuda):
     n, b = 4096, 512
     with hplai.Solver(n, b) as s:
         flags, side, ms = s.autotune(42)
-        assert ms > 0.0 and side in (16, 20, 24, 32, 48)
+        assert ms > 0.0 and (side in (16, 20, 24, 32, 48) or -24 <= side <= -8)
         assert flags & ~(hplai.FLAG_LOOKAHEAD | hplai.FLAG_GROUP2) == 0
         s.factor()
         res = s.iterative_refinement(50)
