@@ -101,6 +101,11 @@ struct hplai_ctx {
 	cudaStream_t st = nullptr;    // main stream: Schur updates, refinement, everything else
 	cudaStream_t st2 = nullptr;   // side stream (high priority): diagonal block + panels
 	cudaEvent_t ev_panel = nullptr, ev_next = nullptr;
+	// host -> device copies of the matrix streamed behind the factorisation
+	// (hplai_solve_host with the FP16 deck): one event per panel's block
+	// column and row, created on first use
+	cudaStream_t st3 = nullptr;
+	std::vector<cudaEvent_t> ev_copy;
 	uint64_t seed = 0;
 	bool have_inputs = false, factored = false;
 	double norma = 0.0, normb = 0.0;
@@ -166,6 +171,8 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->x2);
 	if (c->ev_panel) cudaEventDestroy(c->ev_panel);
 	if (c->ev_next) cudaEventDestroy(c->ev_next);
+	for (cudaEvent_t e : c->ev_copy) cudaEventDestroy(e);
+	if (c->st3) cudaStreamDestroy(c->st3);
 	if (c->st) cudaStreamDestroy(c->st);
 	if (c->st2) cudaStreamDestroy(c->st2);
 	delete c;
@@ -605,7 +612,7 @@ namespace {
 // kend < nb (the benchmark warm-up) the updates of panels 0 .. kend-2 are
 // applied, as in the reference, whose loop applies panel k-1's update in
 // iteration k (RDMAPanelLU::run, panel_trf.hpp:726-850).
-int factor_impl(hplai_ctx *c, int kend)
+int factor_impl(hplai_ctx *c, int kend, const float *host_a = nullptr, int64_t host_lda = 0)
 {
 	if (!c) return HPLAI_EINVAL;
 	if (!c->have_inputs) return HPLAI_ESTATE;
@@ -652,10 +659,35 @@ int factor_impl(hplai_ctx *c, int kend)
 		}
 		return (2 * side > sms) ? 0 : side;
 	};
+	// With a host source (the FP16 deck form only: the updates go to the deck,
+	// so block column and row j of A are first read when panel j is formed)
+	// the matrix is copied panel by panel on a copy stream, block column j
+	// (rows jb..n) and block row j (columns (j+1)b..n) before event j, and
+	// panel j's preparation waits for that event.
+	if (host_a) {
+		const int64_t lda = c->lda;
+		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));   // the deck's zeroing and the step's inputs
+		HPLAI_CUDA_TRY(cudaStreamWaitEvent(c->st3, c->ev_next, 0));
+		for (int j = 0; j < nb; ++j) {
+			const int64_t jb = static_cast<int64_t>(j) * b;
+			HPLAI_CUDA_TRY(cudaMemcpy2DAsync(c->A + jb + jb * lda, sizeof(float) * lda, host_a + jb + jb * host_lda,
+				sizeof(float) * host_lda, sizeof(float) * (n - jb), b, cudaMemcpyHostToDevice, c->st3));
+			if (jb + b < n)
+				HPLAI_CUDA_TRY(cudaMemcpy2DAsync(c->A + jb + (jb + b) * lda, sizeof(float) * lda,
+					host_a + jb + (jb + b) * host_lda, sizeof(float) * host_lda, sizeof(float) * b, n - jb - b,
+					cudaMemcpyHostToDevice, c->st3));
+			HPLAI_CUDA_TRY(cudaEventRecord(c->ev_copy[j], c->st3));
+		}
+	}
+	auto wait_copy = [&](int j) -> int {
+		if (host_a) HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_copy[j], 0));
+		return HPLAI_OK;
+	};
 	// the side stream starts from the generated matrix: group 0's panels
 	HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));
 	HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_next, 0));
 	for (int j = 0; j < G && j < nb && j < kend; ++j) {
+		HPLAI_TRY(wait_copy(j));
 		HPLAI_TRY(prepare_block(c, j, 0, 0, simt, 0, sd, pe));
 		HPLAI_TRY(panel_step(c, j, 0, j, simt, 0, sd, pe));
 	}
@@ -674,6 +706,7 @@ int factor_impl(hplai_ctx *c, int kend)
 		HPLAI_CUDA_TRY(cudaEventRecord(c->ev_next, st));
 		HPLAI_CUDA_TRY(cudaStreamWaitEvent(sd, c->ev_next, 0));
 		for (int j = e; j < e + ne && j < kend; ++j) {
+			HPLAI_TRY(wait_copy(j));
 			HPLAI_TRY(prepare_block(c, j, e, q ^ 1, simt, side_ctas, sd, pe));
 			HPLAI_TRY(panel_step(c, j, q ^ 1, j - e, simt, side_ctas, sd, pe));
 		}
@@ -1202,8 +1235,32 @@ extern "C" int hplai_get_norms(hplai_ctx *c, double *norma, double *normb)
 extern "C" int hplai_solve_host(hplai_ctx *c, const float *a, int64_t lda, const double *rhs, const double *diag,
 	uint64_t seed, int maxit, double *x, hplai_ir_errors *err, int *iters)
 {
-	HPLAI_TRY(hplai_upload(c, a, lda, rhs, diag, seed));
-	HPLAI_TRY(hplai_factor(c));
+	if (!c || !a || !rhs || !diag || !x || lda < c->n) return HPLAI_EINVAL;
+	// With the FP16 deck and a page-locked matrix the copy runs behind the
+	// factorisation (each panel waits for its own block column and row);
+	// otherwise the whole matrix is copied first.
+	cudaPointerAttributes pa{};
+	const bool pinned = cudaPointerGetAttributes(&pa, a) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+	(void)cudaGetLastError();
+	if (c->deck && pinned) {
+		const int n = c->n;
+		if (!c->st3) HPLAI_CUDA_TRY(cudaStreamCreateWithFlags(&c->st3, cudaStreamNonBlocking));
+		while (static_cast<int>(c->ev_copy.size()) < c->nb) {
+			cudaEvent_t e;
+			HPLAI_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+			c->ev_copy.push_back(e);
+		}
+		HPLAI_CUDA_TRY(cudaMemcpyAsync(c->rhs, rhs, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+		HPLAI_CUDA_TRY(cudaMemcpyAsync(c->d, diag, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+		c->seed = seed;
+		HPLAI_TRY(compute_norms(c));
+		c->have_inputs = true;
+		c->factored = false;
+		HPLAI_TRY(factor_impl(c, c->nb, a, lda));
+	} else {
+		HPLAI_TRY(hplai_upload(c, a, lda, rhs, diag, seed));
+		HPLAI_TRY(hplai_factor(c));
+	}
 	const int rc = hplai_refine(c, c->precision == HPLAI_F32_F8 ? HPLAI_GMRES : HPLAI_IR, maxit, err, iters);
 	if (rc != HPLAI_OK && rc != HPLAI_ENOTCONV) return rc;
 	HPLAI_TRY(hplai_get_x(c, x));

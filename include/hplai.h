@@ -235,7 +235,12 @@ int hplai_get_norms(hplai_ctx *ctx, double *norma, double *normb);
 
 /* One end-to-end solve through host buffers: upload, factor, refine and
  * copy x back (the whole of main.cpp's timed region plus the transfers).
- * Refines with HPLAI_IR, or HPLAI_GMRES for an HPLAI_F32_F8 context. */
+ * Refines with HPLAI_IR, or HPLAI_GMRES for an HPLAI_F32_F8 context.  With
+ * HPLAI_FLAG_FP16_DECK and a page-locked `a` (cudaHostAlloc / registered),
+ * the matrix is copied panel by panel on a copy stream behind the
+ * factorisation -- block column and row j arrive before panel j is formed,
+ * which is the first time the deck form reads them -- so the transfer
+ * overlaps the trailing updates; results are identical to the device path. */
 int hplai_solve_host(hplai_ctx *ctx, const float *a, int64_t lda, const double *rhs,
 	const double *diag, uint64_t seed, int maxit, double *x, hplai_ir_errors *err, int *iters);
 

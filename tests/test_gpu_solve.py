@@ -145,6 +145,30 @@ def test_solve_host_matches_device_path(hplai, oracle, torch_cuda):
         assert np.array_equal(s.x(), x)
 
 
+@pytest.mark.parametrize("precision,flags,n,b", [(0, 4, 4096, 256), (1, 4 | 8, 4096, 512), (1, 4 | 8 | 2, 8192, 1024)])
+def test_streamed_host_solve_matches_device_path(hplai, oracle, torch_cuda, precision, flags, n, b):
+    """hplai_solve_host with the FP16 deck and page-locked buffers copies the
+    matrix panel by panel behind the factorisation: x equals the device
+    path's bit for bit (the same kernels on the same values), twice in a row
+    (the second solve overwrites the first one's factors)."""
+    torch = torch_cuda
+    with hplai.Solver(n, b, precision=precision, flags=flags) as s:
+        s.generate(42)
+        a_h = torch.empty(n * n, dtype=torch.float32, pin_memory=True)
+        hplai.check(hplai._get_lu(s._h, a_h.data_ptr(), n), "hplai_get_lu")
+        rhs_h = torch.from_numpy(s.rhs()).pin_memory()
+        d_h = torch.from_numpy(s.diag()).pin_memory()
+        x_h = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        mode = hplai.GMRES if precision == hplai.F32_F8 else hplai.IR
+        s.factor()
+        s.iterative_refinement(50, mode=mode)
+        x_dev = s.x()
+        for _ in range(2):
+            r = s.solve_host_ptrs(a_h.data_ptr(), n, rhs_h.data_ptr(), d_h.data_ptr(), 42, 50, x_h.data_ptr())
+            assert r.status == hplai.HPLAI_OK and r.hpl_harness < 16
+            assert np.array_equal(x_h.numpy(), x_dev)
+
+
 def test_call_order_and_nonconvergence(hplai, torch_cuda):
     with hplai.Solver(480, 60) as s:
         with pytest.raises(hplai.HplaiError) as e:
