@@ -255,19 +255,19 @@ def schur_algorithmic(n, b, panel_bytes=2, c_bytes=8, group=1):
     return acc["flops"], acc["bytes"], acc["launches"]
 
 
-def schur_traffic_per_launch(n, b, group=1):
+def schur_traffic_per_launch(n, b, group=1, kind="fp16_fp32c"):
     """DRAM bytes per average launch from the committed ncu summary (DRAM
-    bytes per C element of the FP32-C kernel), times the C elements of one
-    factorisation's launches (traffic grows with the C area), per launch."""
+    bytes per updated C element of the kernel at K = 2048), times the C
+    elements of one factorisation's launches (traffic grows with the C
+    area), per launch."""
     p = os.path.join(ROOT, "profiles", "schur_kernel_traffic.json")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p))
-    per_elem = d.get("dram_bytes_per_c_element")
-    if not per_elem:
+    d = json.load(open(p)).get("kernels", {}).get(kind)
+    if not d:
         return None
     _, byts, launches = schur_algorithmic(n, b, 0, 1, group)   # bytes = C elements
-    return per_elem * byts / launches
+    return d["dram_bytes_per_c_element"] * byts / launches
 
 
 FORMS = {
@@ -309,7 +309,8 @@ def schur_roofline(hplai, n, b, fp8, deck, gemm_ms, group=1):
         roof = {"bound": "tensor", "achieved": ach_tf, "peak": tc_sus, "unit": "TFLOP/s", "frac": ach_tf / tc_sus}
     cdesc = "FP16 deck, deck -= s*L*U" if deck else "FP32 C, C -= L*U"
     kname = f"schur_kernel (tcgen05 {'e4m3 x e4m3' if fp8 else 'FP16 x FP16'} -> FP32 accumulator; {cdesc})"
-    traffic = schur_traffic_per_launch(n, b, group) if (not fp8 and not deck) else None
+    kind = "e4m3_deck" if (fp8 and deck) else ("fp16_fp32c" if (not fp8 and not deck) else None)
+    traffic = schur_traffic_per_launch(n, b, group, kind) if kind else None
     roof.update({"traffic": traffic, "kernel": kname,
                  "launches_per_step": slaunch, "avg_launch_ms": avg_launch_s * 1e3,
                  "algorithmic_bytes_per_launch": sbytes / slaunch, "algorithmic_flops_per_launch": sflops / slaunch,
