@@ -11,6 +11,7 @@
 #include <cstddef>
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
+#include <mutex>
 
 #include "../../include/hplai.h"
 
@@ -33,6 +34,32 @@ namespace hplai {
 
 void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int line);
 void set_last_error_message(const char *msg);
+
+// Kernel attributes and occupancy belong to one device: a call site's
+// set-up runs the first time the site is reached with each device current
+// (under a lock, so concurrent first calls do it once), and its int result
+// is cached per device.
+struct DeviceOnce {
+	static constexpr int kMax = 64;
+	std::mutex mu;
+	int value[kMax] = {};
+	bool done[kMax] = {};
+	template <class F> int get(F &&init, int *out = nullptr)
+	{
+		int dev = 0;
+		HPLAI_CUDA_TRY(cudaGetDevice(&dev));
+		if (dev < 0 || dev >= kMax) return HPLAI_EUNSUPPORTED;
+		std::lock_guard<std::mutex> lk(mu);
+		if (!done[dev]) {
+			int v = 0;
+			HPLAI_TRY(init(dev, &v));
+			value[dev] = v;
+			done[dev] = true;
+		}
+		if (out) *out = value[dev];
+		return HPLAI_OK;
+	}
+};
 
 // ---------------------------------------------------------------------------
 // LCG x <- a*x + c mod 2^64 (hpl_rand.hpp:8-57).

@@ -396,18 +396,19 @@ uint32_t g_static_epoch = 0;
 
 int max_coresident_ctas()
 {
-	static int cached = 0;
-	if (!cached) {
-		int per_sm = 0, dev = 0, sms = 0;
+	static DeviceOnce once;
+	int n = 0;
+	if (once.get([](int dev, int *v) -> int {
+		int per_sm = 0, sms = 0;
 		HPLAI_CUDA_TRY(cudaFuncSetAttribute(getrf_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			static_cast<int>(kSmemBytes)));
 		HPLAI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, getrf_tiles_kernel, kWarps * 32,
 			kSmemBytes));
-		HPLAI_CUDA_TRY(cudaGetDevice(&dev));
 		HPLAI_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-		cached = per_sm * sms;
-	}
-	return cached;
+		*v = per_sm * sms;
+		return HPLAI_OK;
+	}, &n) != HPLAI_OK) return 0;
+	return n;
 }
 
 } // namespace

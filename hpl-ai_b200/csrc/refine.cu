@@ -649,20 +649,22 @@ int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void 
 	if (n <= 0) return HPLAI_OK;
 	if (!work || work_bytes < trsv_workspace(n)) return HPLAI_EINVAL;
 	constexpr size_t dsmem = sizeof(float) * (TB * (TB + 1) + 3 + 4 + 2 * TB * TB);
-	static int max_blocks = 0;
-	if (!max_blocks) {
-		int per_sm = 0, per_sm_t = 0, dev = 0, sms = 0;
+	// co-resident CTAs of the cooperative launch on this device
+	static DeviceOnce grid_once;
+	int max_blocks = 0;
+	HPLAI_TRY(grid_once.get([&](int dev, int *v) -> int {
+		int per_sm = 0, per_sm_t = 0, sms = 0;
 		HPLAI_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			static_cast<int>(dsmem)));
 		HPLAI_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			static_cast<int>(dsmem)));
 		HPLAI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_kernel<false>, TRSV_THREADS, dsmem));
 		HPLAI_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, trsv_kernel<true>, TRSV_THREADS, dsmem));
-		HPLAI_CUDA_TRY(cudaGetDevice(&dev));
 		HPLAI_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-		max_blocks = (per_sm < per_sm_t ? per_sm : per_sm_t) * sms;
-		if (max_blocks <= 0) return HPLAI_EUNSUPPORTED;
-	}
+		*v = (per_sm < per_sm_t ? per_sm : per_sm_t) * sms;
+		return HPLAI_OK;
+	}, &max_blocks));
+	if (max_blocks <= 0) return HPLAI_EUNSUPPORTED;
 	// the transposed solve reads rows of the stored matrix as float4
 	if (trans && ((reinterpret_cast<uintptr_t>(a) & 15u) || (lda & 3))) return HPLAI_EINVAL;
 	TrsvWork *w = static_cast<TrsvWork *>(work);
@@ -689,12 +691,12 @@ int launch_trsv_dinv(int n, const float *a, int64_t lda, double *dinv, cudaStrea
 {
 	if (n <= 0) return HPLAI_OK;
 	constexpr size_t smem = sizeof(float) * (TB * (TB + 1) + 3) + sizeof(double) * TB * TB;
-	static bool attr = false;
-	if (!attr) {
+	static DeviceOnce attr;
+	HPLAI_TRY(attr.get([&](int, int *) -> int {
 		HPLAI_CUDA_TRY(cudaFuncSetAttribute(trsv_dinv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			static_cast<int>(smem)));
-		attr = true;
-	}
+		return HPLAI_OK;
+	}));
 	trsv_dinv_kernel<<<dim3((n + TB - 1) / TB, 2), TB, smem, st>>>(n, a, lda, dinv);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());

@@ -753,16 +753,16 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 	// The store form writes whole 16-byte units of a column, so its region
 	// starts and ends on multiples of 4 rows; it needs the tall-box reduce path.
 	if (oscale && (fp8 || deck || epi != 1 || !TALL || (m % 4))) return HPLAI_EINVAL;
-	static bool attr_set = false;
-	if (!attr_set) {
+	static DeviceOnce attr;
+	HPLAI_TRY(attr.get([](int, int *) -> int {
 		HPLAI_TRY((set_smem_attr<0, false>()));
 		HPLAI_TRY((set_smem_attr<1, false>()));
 		HPLAI_TRY((set_smem_attr<2, false>()));
 		HPLAI_TRY((set_smem_attr<0, true>()));
 		HPLAI_TRY((set_smem_attr<1, true>()));
 		HPLAI_TRY((set_smem_attr<2, true>()));
-		attr_set = true;
-	}
+		return HPLAI_OK;
+	}));
 	CUtensorMap lm, um, cm;
 	std::memcpy(&lm, maps.lmap, sizeof(lm));
 	std::memcpy(&um, maps.umap, sizeof(um));
@@ -835,11 +835,11 @@ int launch_schur_tiles(const SchurMaps &maps, const int4 *tiles, int ntiles, int
 	alignas(64) unsigned char cmap[128];
 	HPLAI_TRY(make_map_2d(cmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, maps.cbase, static_cast<uint64_t>(maps.crows),
 		static_cast<uint64_t>(maps.ccols), static_cast<uint64_t>(maps.cld), BM, EPI_CHUNK, CU_TENSOR_MAP_SWIZZLE_NONE));
-	static bool attr_set = false;
-	if (!attr_set) {
+	static DeviceOnce attr;
+	HPLAI_TRY(attr.get([](int, int *) -> int {
 		HPLAI_TRY((set_smem_attr<1, false>()));
-		attr_set = true;
-	}
+		return HPLAI_OK;
+	}));
 	CUtensorMap lm, um, cm;
 	std::memcpy(&lm, maps.lmap, sizeof(lm));
 	std::memcpy(&um, maps.umap, sizeof(um));

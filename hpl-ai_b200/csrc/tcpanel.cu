@@ -715,12 +715,12 @@ int launch_tf32x3(const unsigned char *m_ahi, const unsigned char *m_alo, const 
 	p.s16m = s16m;
 	p.s16n = s16n;
 	p.scale = scale;
-	static bool attr = false;
-	if (!attr) {
+	static DeviceOnce attr;
+	HPLAI_TRY(attr.get([](int, int *) -> int {
 		HPLAI_CUDA_TRY(cudaFuncSetAttribute(tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			static_cast<int>(TSMEM_BYTES)));
-		attr = true;
-	}
+		return HPLAI_OK;
+	}));
 	const int total = p.tiles_m * p.tiles_n;
 	int grid = max_ctas > 0 ? max_ctas : sm_count();
 	if (grid > total) grid = total;
