@@ -53,6 +53,8 @@ _shgemm = _proto("orc_shgemm_minus", None, _int, _int, _int, _vp, _i64, _vp, _i6
 _lu = _proto("orc_lu", _int, _int, _int, _vp, _i64)
 _lu_steps = _proto("orc_lu_steps", _int, _int, _int, _vp, _i64, _int)
 _l1est = _proto("orc_l1est", None, _int, _vp, _i64, _vp)
+_lu_deck_steps = _proto("orc_lu_deck_steps", _int, _int, _int, _u64, _vp, _vp, _i64, _int, _vp)
+_deck_scales = _proto("orc_deck_scales", None, _int, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float))
 _otf_gemv = _proto("orc_otf_gemv", None, _int, _int, _int, _dbl, _vp, _vp, _u64, _vp)
 _trsv_l = _proto("orc_trsv_lower", None, _int, _int, _vp, _i64, _vp)
 _trsv_u = _proto("orc_trsv_upper", None, _int, _int, _vp, _i64, _vp)
@@ -155,6 +157,28 @@ def lu_steps(a: np.ndarray, b: int, kend: int) -> np.ndarray:
     if rc:
         raise ValueError(f"orc_lu_steps: {rc}")
     return a
+
+
+def lu_deck(n: int, b: int, seed: int = 42, kend: int = None, with_deck: bool = False):
+    """The reference's lazy-initialised double-decker LU (`-d`): A never
+    stored, trailing updates into an FP16 deck by the FP16-accumulating
+    hgemm_opt, blocks formed as fma(downscale, deck, a_ij) when they join a
+    panel.  Returns the FP32 factors (and the final deck, n x n FP16 bits)."""
+    a = np.zeros((n, n), dtype=np.float32, order="F")
+    dk = np.zeros((n, n), dtype=np.uint16, order="F") if with_deck else None
+    df = np.ascontiguousarray(diag(n, seed).astype(np.float32))
+    rc = _lu_deck_steps(n, b, seed, _p(df), _p(a), n, n // b if kend is None else kend,
+                        _p(dk) if with_deck else None)
+    if rc:
+        raise ValueError(f"orc_lu_deck_steps: {rc}")
+    return (a, dk) if with_deck else a
+
+
+def deck_scales(n: int):
+    """(scalea, downscale) of the `-d` LU as FP32: n^0.75 and 1 / n^0.75."""
+    sa, ds = ctypes.c_float(), ctypes.c_float()
+    _deck_scales(n, ctypes.byref(sa), ctypes.byref(ds))
+    return sa.value, ds.value
 
 
 def l1est(a: np.ndarray, d: np.ndarray) -> np.ndarray:

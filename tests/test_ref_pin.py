@@ -14,6 +14,11 @@ built by oracle/build_ref.sh).
   warm-up (the first P + 2 = 4 block steps) bit for bit against the oracle's
   truncated LU; on the GPU, hplai_l1est is bit-exact and the refinement from
   it reaches the reference's x.
+* The `-d` path (lazy initialisation, FP16 deck, FP16-accumulating Schur
+  update in k-chunks of 100): the oracle's factors are the reference's bit
+  for bit at C1 and at n = 2400, b = 120 (two chunks per panel); on the GPU,
+  HPLAI_FLAG_REF_DECK reproduces them bit for bit and refines to the
+  reference's x.
 * Every solution -- the oracle's, the GPU's plain form, the GPU's precision
   form (e4m3 Schur, GMRES-IR; the FP16 deck needs b % 8 == 0, which b = 60 is
   not) -- equals the reference's x from each of its four runs (`-not -r`,
@@ -57,6 +62,25 @@ def test_oracle_warmup_lu_is_the_references_bit_for_bit(oracle):
     assert digest(lu) == FIX["runs"]["netlib_warmup"]["lu_sha256"]
 
 
+@pytest.mark.parametrize("run", ["netlib_not_d_r", "netlib_not_d_r_2400"])
+def test_oracle_deck_lu_is_the_references_bit_for_bit(oracle, run):
+    """-d: lazy init + FP16 deck + hgemm_opt numerics (lazy_init.hpp:92-227,
+    kernels/avx2.cpp:82-189)."""
+    n, b = (N, B) if run == "netlib_not_d_r" else (2400, 120)
+    assert FIX["runs"][run]["command"] == f"driver.out {n} {b} 2 -not -d -r"
+    assert digest(oracle.lu_deck(n, b)) == FIX["runs"][run]["lu_sha256"]
+
+
+def test_oracle_deck_refinement_vs_reference(oracle):
+    lu = oracle.lu_deck(N, B)
+    rc, x, res, har, steps = oracle.refine(lu, B, 42, oracle.rhs(N), oracle.diag(N), q=2)
+    ref = FIX["runs"]["netlib_not_d_r"]
+    assert rc == 0 and len(steps) == len(ref["steps"])
+    assert steps[0][0] == ref["steps"][0]["residual"]
+    assert abs(steps[1][0] - ref["steps"][1]["residual"]) <= 1e-8 * ref["steps"][1]["residual"]
+    assert rel(x, ref_x("netlib_not_d_r")) <= 1e-12
+
+
 def test_oracle_l1est_is_the_references_bit_for_bit(oracle):
     a = oracle.l1est(oracle.matrix(N), oracle.diag(N))
     assert digest(a) == FIX["runs"]["netlib_l1est"]["lu_sha256"]
@@ -80,6 +104,8 @@ def test_oracle_refinement_vs_reference_steps(oracle):
     rc, x, res, har, steps = oracle.solve(N, B, q=2)
     assert rc == 0
     for run in FIX["runs"].values():
+        if not run["command"].startswith(f"driver.out {N} {B} "):
+            continue
         assert steps[0][0] == run["steps"][0]["residual"]
         assert abs(steps[0][1] - run["steps"][0]["hpl_harness"]) <= 1e-12 * steps[0][1]
     ref = FIX["runs"]["netlib_not_r"]["steps"]
