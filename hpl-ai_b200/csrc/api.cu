@@ -82,6 +82,12 @@ struct hplai_ctx {
 	// dscale x (accumulated update)
 	uint16_t *deck = nullptr;
 	float dscale = 1.f;
+	// HPLAI_FLAG_REF_DECK: the reference's `-d` deck (n x lda halves), its
+	// FP16 L-panel scale n^0.75 and the lazy-init downscale; regen_a: A is
+	// not stored (hplai_generate) and the lazy initialisation regenerates it
+	uint16_t *rdeck = nullptr;
+	float rscalea = 1.f, rdownscale = 1.f;
+	bool regen_a = false;
 	SchurMaps maps8[2];           // [buffer]: K = b
 	SchurMaps maps8g[2];          // [buffer]: K = 2b (gcap 2)
 	SchurMaps maps8s;             // the single panel copy, K = b
@@ -151,6 +157,7 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->sus);
 	cudaFree(c->qbits);
 	cudaFree(c->deck);
+	cudaFree(c->rdeck);
 	cudaFree(c->tcbuf);
 	cudaFree(c->rhs);
 	cudaFree(c->d);
@@ -270,6 +277,9 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	if (precision != HPLAI_F32_F16 && precision != HPLAI_F32_F8) return HPLAI_EUNSUPPORTED;
 	if ((flags & HPLAI_FLAG_FP16_DECK) && (b % 8)) return HPLAI_EINVAL;
 	if ((flags & HPLAI_FLAG_GROUP2) && (b % 128)) return HPLAI_EINVAL;
+	if ((flags & HPLAI_FLAG_REF_DECK) &&
+		(precision != HPLAI_F32_F16 || (flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_LOOKAHEAD))))
+		return HPLAI_EINVAL;
 	hplai_ctx *c = new hplai_ctx;
 	c->n = n;
 	c->b = b;
@@ -326,6 +336,13 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		CTX_ALLOC(c->deck, sizeof(uint16_t) * static_cast<size_t>(c->lda) * n);
 		// a power of two near n^0.75, the reference's scalea (hpl_rand.hpp:154)
 		c->dscale = std::ldexp(1.0f, static_cast<int>(std::lround(0.75 * std::log2(static_cast<double>(n)))));
+	}
+	if (flags & HPLAI_FLAG_REF_DECK) {
+		CTX_ALLOC(c->rdeck, sizeof(uint16_t) * static_cast<size_t>(c->lda) * n);
+		// scalea = sqrt(n sqrt(n)) in FP64, then FP32; downscale = FP32(1 / (scalea * scaleb)), scaleb = 1
+		// (hpl_rand.hpp:154-155, panel_trf.hpp:717-719)
+		c->rscalea = static_cast<float>(std::sqrt(n * std::sqrt(static_cast<double>(n))));
+		c->rdownscale = static_cast<float>(1. / static_cast<double>(c->rscalea * 1.0f));
 	}
 	const int64_t ldp = round_up(b, 32);
 	const size_t tc_elems = static_cast<size_t>(ldp) * (2 * static_cast<size_t>(n) + 4 * static_cast<size_t>(b)) +
@@ -407,9 +424,12 @@ extern "C" int hplai_generate(hplai_ctx *c, uint64_t seed)
 	if (!c) return HPLAI_EINVAL;
 	const int n = c->n;
 	// pmatgen (matgen.hpp:7-22): the whole matrix, then the diagonal as the
-	// FP32 rounding of the sequential FP64 row sums (which are also d).
-	HPLAI_TRY(launch_fill(n, 0, 0, n, n, c->A, c->lda, seed, 0, c->st));
-	HPLAI_TRY(launch_diag(n, 0, n, c->d, c->A, c->lda, seed, c->st));
+	// FP32 rounding of the sequential FP64 row sums (which are also d).  The
+	// `-d` parity mode stores no A (pmatgen0, main.cpp:260-261): its lazy
+	// initialisation regenerates each block when it joins a panel.
+	c->regen_a = (c->flags & HPLAI_FLAG_REF_DECK) != 0;
+	if (!c->regen_a) HPLAI_TRY(launch_fill(n, 0, 0, n, n, c->A, c->lda, seed, 0, c->st));
+	HPLAI_TRY(launch_diag(n, 0, n, c->d, c->regen_a ? nullptr : c->A, c->lda, seed, c->st));
 	HPLAI_TRY(launch_rhs(n, c->rhs, seed, c->st));
 	c->seed = seed;
 	HPLAI_TRY(compute_norms(c));
@@ -428,6 +448,7 @@ extern "C" int hplai_upload(hplai_ctx *c, const float *a, int64_t lda, const dou
 	HPLAI_CUDA_TRY(cudaMemcpyAsync(c->rhs, rhs, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
 	HPLAI_CUDA_TRY(cudaMemcpyAsync(c->d, diag, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
 	c->seed = seed;
+	c->regen_a = false;
 	HPLAI_TRY(compute_norms(c));
 	c->have_inputs = true;
 	c->factored = false;
@@ -608,6 +629,68 @@ int prepare_block(hplai_ctx *c, int j, int first, int q, bool simt, int side_cta
 
 namespace {
 
+// The reference's `-d` LU bit for bit (HPLAI_FLAG_REF_DECK): the steps of
+// RDMAPanelLU::run<Matgen, 1, true, false> (panel_trf.hpp:703-856) on one
+// stream.  Step k: lazy initialisation of the diagonal block, its LU, lazy
+// initialisation + TRSM of the block column (FP16 copy scaled by scalea) and
+// of the block row (scale 1), then the FP16-accumulating update of the deck
+// by panel k.  Every element sees the updates of the panels before it in
+// panel order, as in the reference's split schedule.  With kend < nb the
+// last panel's update is not applied (the warm-up, panel_trf.hpp:726).
+int factor_refdeck(hplai_ctx *c, int kend)
+{
+	const int n = c->n, b = c->b, nb = c->nb;
+	const int64_t lda = c->lda, ldg = c->ldg;
+	cudaStream_t st = c->st;
+	for (double &v : c->phase_ms) v = 0.0;
+	PhaseEvents pe;
+	HPLAI_CUDA_TRY(cudaMemsetAsync(c->rdeck, 0, sizeof(uint16_t) * static_cast<size_t>(lda) * n, st));
+	HPLAI_CUDA_TRY(cudaMemsetAsync(c->getrf_work, 0, sizeof(uint32_t), st));   // its status word
+	// pmatgen0 (matgen.hpp:81-105): the blocks a warm-up leaves unformed hold zero
+	if (c->regen_a) HPLAI_CUDA_TRY(cudaMemsetAsync(c->A, 0, sizeof(float) * static_cast<size_t>(lda) * n, st));
+	auto lazy = [&](int r0, int r1, int c0, int c1) -> int {
+		HPLAI_TRY(pe.record(st, HPLAI_PH_LAZY_INIT));
+		HPLAI_TRY(launch_lazy_init(n, r0, r1, c0, c1, c->A, lda, c->rdeck, lda, c->rdownscale, c->seed, c->d, c->regen_a,
+			st));
+		return pe.end(st);
+	};
+	const int steps = std::min(kend, nb);
+	for (int k = 0; k < steps; ++k) {
+		const int kb = k * b;
+		float *diag = c->A + kb + static_cast<int64_t>(kb) * lda;
+		HPLAI_TRY(lazy(kb, kb + b, kb, kb + b));
+		HPLAI_TRY(pe.record(st, HPLAI_PH_DIAG_LU));
+		HPLAI_TRY(launch_getrf_tiles(b, diag, lda, c->getrf_work, &c->getrf_epoch, 0, st));
+		HPLAI_TRY(pe.end(st));
+		if (k == nb - 1) break;
+		const int rem = n - kb - b;
+		uint16_t *lh = c->Lh[0] + static_cast<int64_t>(kb + b) * ldg, *uh = c->Uh[0] + static_cast<int64_t>(kb + b) * ldg;
+		HPLAI_TRY(lazy(kb + b, n, kb, kb + b));
+		HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_L));
+		HPLAI_TRY(launch_trsm_right_upper(rem, b, diag, lda, diag + b, lda, lh, ldg, c->rscalea, st));
+		HPLAI_TRY(pe.end(st));
+		HPLAI_TRY(lazy(kb, kb + b, kb + b, n));
+		HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_R));
+		HPLAI_TRY(launch_trsm_left_lower(b, rem, diag, lda, diag + static_cast<int64_t>(b) * lda, lda, uh, ldg, 1.0f, st));
+		HPLAI_TRY(pe.end(st));
+		if (k == kend - 1 && kend < nb) break;
+		HPLAI_TRY(pe.record(st, HPLAI_PH_GEMM_UPDATE));
+		HPLAI_TRY(launch_hgemm_deck(rem, rem, b, lh, ldg, uh, ldg, c->rdeck + (kb + b) + static_cast<int64_t>(kb + b) * lda,
+			lda, st));
+		HPLAI_TRY(pe.end(st));
+	}
+	HPLAI_TRY(pe.record(st, HPLAI_PH_IR_TRSV));
+	HPLAI_TRY(launch_trsv_dinv(n, c->A, lda, c->dinv, st));
+	HPLAI_TRY(pe.end(st));
+	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
+	pe.collect(c->phase_ms);
+	int gs = HPLAI_OK;
+	HPLAI_TRY(getrf_status(c->getrf_work, st, &gs));
+	HPLAI_TRY(gs);
+	c->factored = true;
+	return HPLAI_OK;
+}
+
 // The factorisation of panels 0 .. kend-1 (kend = nb: the whole LU).  With
 // kend < nb (the benchmark warm-up) the updates of panels 0 .. kend-2 are
 // applied, as in the reference, whose loop applies panel k-1's update in
@@ -616,6 +699,7 @@ int factor_impl(hplai_ctx *c, int kend, const float *host_a = nullptr, int64_t h
 {
 	if (!c) return HPLAI_EINVAL;
 	if (!c->have_inputs) return HPLAI_ESTATE;
+	if (c->flags & HPLAI_FLAG_REF_DECK) return factor_refdeck(c, kend);
 	const int n = c->n, b = c->b, nb = c->nb;
 	c->group = ((c->flags & HPLAI_FLAG_GROUP2) && c->gcap == 2 && kend >= nb) ? 2 : 1;
 	const int G = c->group;
@@ -756,6 +840,11 @@ extern "C" int hplai_l1est(hplai_ctx *c)
 	if (!c) return HPLAI_EINVAL;
 	if (!c->have_inputs) return HPLAI_ESTATE;
 	for (double &v : c->phase_ms) v = 0.0;
+	if (c->regen_a) {
+		// --l1est stores A even with `-d` (pmatgen, main.cpp:260-263)
+		HPLAI_TRY(launch_fill(c->n, 0, 0, c->n, c->n, c->A, c->lda, c->seed, 0, c->st));
+		HPLAI_TRY(launch_diag(c->n, 0, c->n, nullptr, c->A, c->lda, c->seed, c->st));
+	}
 	HPLAI_TRY(launch_l1est(c->n, c->A, c->lda, c->d, c->st));
 	HPLAI_TRY(launch_trsv_dinv(c->n, c->A, c->lda, c->dinv, c->st));
 	HPLAI_CUDA_TRY(cudaStreamSynchronize(c->st));
@@ -1025,6 +1114,7 @@ int hplai_ctx_solve_stream_rhs(hplai_ctx *c, int col, double *x, int maxit, hpla
 extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, int *side_sms_out, double *ms_out)
 {
 	if (!c) return HPLAI_EINVAL;
+	if (c->flags & HPLAI_FLAG_REF_DECK) return HPLAI_EUNSUPPORTED;   // one fixed schedule
 	int sms = 148;
 	{
 		int dev = 0;
@@ -1120,6 +1210,7 @@ extern "C" int hplai_set_schedule(hplai_ctx *c, unsigned flags, int side_sms)
 	const unsigned sched = HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2;
 	if (!c || (flags & ~sched) || side_sms == 0 || side_sms > 64 || side_sms < -256) return HPLAI_EINVAL;
 	if ((flags & HPLAI_FLAG_GROUP2) && c->gcap != 2) return HPLAI_EINVAL;
+	if ((c->flags & HPLAI_FLAG_REF_DECK) && flags) return HPLAI_EINVAL;
 	c->flags = (c->flags & ~sched) | flags;
 	c->side_sms = side_sms;
 	return HPLAI_OK;

@@ -101,6 +101,8 @@ static int usage()
 		"   --seed <s>              LCG seed (default 42, as the reference).\n"
 		"   -d, -l, --delayed, --lazy-init\n"
 		"                           Keep the trailing updates in an FP16 deck (double-decker form).\n"
+		"   --ref-deck              The reference's -d arithmetic bit for bit: A regenerated at panel\n"
+		"                           time, FP16-accumulating Schur update on CUDA cores (parity mode).\n"
 		"   --fp8                   e4m3 Schur update with GMRES refinement.\n"
 		"   --gmres                 GMRES refinement instead of the classical correction.\n"
 		"   --lookahead             Factor the next panel while the trailing update runs.\n"
@@ -136,6 +138,7 @@ int main(int argc, char **argv)
 		else if (!std::strcmp(argv[i], "-d") || !std::strcmp(argv[i], "--delayed") || !std::strcmp(argv[i], "-l") ||
 			!std::strcmp(argv[i], "--lazy-init"))
 			flags |= HPLAI_FLAG_FP16_DECK;
+		else if (!std::strcmp(argv[i], "--ref-deck")) flags |= HPLAI_FLAG_REF_DECK;
 		else if (!std::strcmp(argv[i], "--fp8")) { precision = HPLAI_F32_F8; mode = HPLAI_GMRES; }
 		else if (!std::strcmp(argv[i], "--gmres")) mode = HPLAI_GMRES;
 		else if (!std::strcmp(argv[i], "--lookahead")) flags |= HPLAI_FLAG_LOOKAHEAD;
@@ -153,10 +156,16 @@ int main(int argc, char **argv)
 		else std::printf("Ignoring unknown option: %s\n", argv[i]);
 	}
 	if (argc > 1 && (!std::strcmp(argv[1], "-h") || !std::strcmp(argv[1], "--help"))) return usage();
+	if (flags & HPLAI_FLAG_REF_DECK) {
+		// one fixed schedule: nothing to tune
+		flags &= ~(HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_LOOKAHEAD);
+		autotune = false;
+	}
 
 	std::printf("n=%d b=%d r=1 c=1\n", n, b);
-	std::printf("1gpu precomp full fp32/%s%s\n", precision == HPLAI_F32_F8 ? "e4m3" : "fp16",
-		(flags & HPLAI_FLAG_FP16_DECK) ? " fp16-deck" : " ddmat");
+	std::printf("1gpu %s full fp32/%s%s\n", (flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_REF_DECK)) ? "lazy" : "precomp",
+		precision == HPLAI_F32_F8 ? "e4m3" : "fp16",
+		(flags & HPLAI_FLAG_REF_DECK) ? " fp16-deck-ref" : (flags & HPLAI_FLAG_FP16_DECK) ? " fp16-deck" : " ddmat");
 
 	// Warm-up on a small system with the same block size so that every kernel
 	// is loaded before the timed region (the reference warms BLAS up the same

@@ -146,6 +146,52 @@ int launch_l1est(int n, float *a, int64_t lda, const double *d, cudaStream_t st)
 	return HPLAI_OK;
 }
 
+// Lazy initialisation of the double-decker LU (`-d`,
+// LazyInitializer<FLow,1,true>::update/update_diag, lazy_init.hpp:92-227):
+// a block's FP32 value is formed only when it joins a panel, as
+//     a(i, j) = fma(downscale, deck(i, j), a0(i, j)),
+// one fused multiply-add like the reference's x86 build, with the initial
+// value a0 regenerated from the LCG (float(d_i) on the diagonal, d the FP64
+// row sums) when `regen`, or read from a (an uploaded matrix) otherwise.
+// Rows [r0, r1) x columns [c0, c1), one thread per row.
+__global__ void __launch_bounds__(kFillRows) lazy_init_kernel(int n, int r0, int r1, int c0, int c1,
+	float *__restrict__ a, int64_t lda, const __half *__restrict__ deck, int64_t ldd, float downscale, uint64_t seed,
+	const double *__restrict__ d, int regen, JumpTable tab)
+{
+	const int i = r0 + blockIdx.x * kFillRows + threadIdx.x;
+	const int j0 = c0 + blockIdx.y * kFillCols;
+	if (i >= r1) return;
+	const Coeff jn = jump_of(tab, static_cast<uint64_t>(n));
+	uint64_t s = regen ? coeff_apply(jump_of(tab, static_cast<uint64_t>(i) +
+	                                               static_cast<uint64_t>(n) * static_cast<uint64_t>(j0)),
+	                         state_initial(seed))
+	                   : 0;
+	const int j1 = min(j0 + kFillCols, c1);
+	for (int j = j0; j < j1; ++j) {
+		const int64_t o = static_cast<int64_t>(j) * lda + i;
+		float a0;
+		if (regen) {
+			a0 = (i == j) ? __double2float_rn(d[i]) : __double2float_rn(state_value(s));
+			s = coeff_apply(jn, s);
+		} else {
+			a0 = a[o];
+		}
+		a[o] = __fmaf_rn(downscale, __half2float(deck[static_cast<int64_t>(j) * ldd + i]), a0);
+	}
+}
+
+int launch_lazy_init(int n, int r0, int r1, int c0, int c1, float *a, int64_t lda, const uint16_t *deck, int64_t ldd,
+	float downscale, uint64_t seed, const double *d, bool regen, cudaStream_t st)
+{
+	if (r1 <= r0 || c1 <= c0) return HPLAI_OK;
+	dim3 grid((r1 - r0 + kFillRows - 1) / kFillRows, (c1 - c0 + kFillCols - 1) / kFillCols);
+	lazy_init_kernel<<<grid, kFillRows, 0, st>>>(n, r0, r1, c0, c1, a, lda, reinterpret_cast<const __half *>(deck), ldd,
+		downscale, seed, d, regen ? 1 : 0, jump_table());
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
 int launch_fill(int n, int i0, int j0, int nrow, int ncol, float *a, int64_t lda, uint64_t seed, int calc_diag,
 	cudaStream_t st)
 {

@@ -22,6 +22,16 @@ int launch_rhs(int n, double *rhs, uint64_t seed, cudaStream_t st);
 int launch_rhs_cols(int n, int col0, int ncols, double *out, uint64_t seed, cudaStream_t st);
 // pmatl1est: strictly lower part of A (n x n, lda) times float(1/d_j) per column
 int launch_l1est(int n, float *a, int64_t lda, const double *d, cudaStream_t st);
+// The `-d` lazy initialisation a = fma(downscale, deck, a0) on rows [r0, r1)
+// x columns [c0, c1), a0 regenerated (regen) or read from a.
+int launch_lazy_init(int n, int r0, int r1, int c0, int c1, float *a, int64_t lda, const uint16_t *deck, int64_t ldd,
+	float downscale, uint64_t seed, const double *d, bool regen, cudaStream_t st);
+// The reference's FP16-accumulating Schur update of the deck (hgemm_opt,
+// alpha = -1): D(m x n) -= L(m x k) U(k x n) with an FP16 accumulator per
+// element over k-chunks of 100.  L row i at l + i ldl, U column j at
+// u + j ldu (both K-major), D column-major.
+int launch_hgemm_deck(int m, int n, int k, const uint16_t *l, int64_t ldl, const uint16_t *u, int64_t ldu,
+	uint16_t *d, int64_t ldd, cudaStream_t st);
 
 // panel.cu
 // getrf.cu: tile-parallel diagonal block LU (bit-exact with the sequential

@@ -1,0 +1,102 @@
+// refdeck.cu -- the reference's FP16-accumulating Schur update of the `-d`
+// (lazy-init, double-decker) LU, bit for bit.
+//
+// The reference's x86 build updates its FP16 deck with hgemm_opt
+// (kernels/avx2.cpp:82-189, fp16sim.hpp:185-213) with alpha = -1: for every
+// element, over k-chunks of 100 (bk), an FP16 accumulator
+//     t <- fp16(fp32(l_iq * u_qj + t))
+// (the FP16 x FP16 product is exact in FP32, so the FP32 FMA and the
+// reference's FMA give the same value), and after each chunk
+//     d_ij <- fp16(fp32(d_ij - t)),
+// every FP32 -> FP16 conversion rounding to nearest even.  Tensor cores
+// cannot round an accumulator to FP16 after every product, so this parity
+// mode runs on CUDA cores: a 64 x 64 tile per CTA, 4 x 4 elements per thread,
+// FP16 operand slabs converted to FP32 in shared memory.  It is a numerics
+// mode (the reference's `-d` arithmetic), not the fast path: the fast deck
+// form accumulates in FP32 on tcgen05 and rounds once per update.
+#include "common.cuh"
+#include "internal.h"
+
+namespace hplai {
+namespace {
+
+constexpr int kHt = 64;       // tile rows and columns
+constexpr int kHk = 20;       // k-slab staged per pass (divides the chunk of 100)
+constexpr int kChunk = 100;   // hgemm_opt's bk
+
+__device__ __forceinline__ float round_f16(float x) { return __half2float(__float2half_rn(x)); }
+
+__global__ void __launch_bounds__(256) hgemm_deck_kernel(int m, int n, int k, const __half *__restrict__ l,
+	int64_t ldl, const __half *__restrict__ u, int64_t ldu, __half *__restrict__ d, int64_t ldd)
+{
+	__shared__ float ls[kHk][kHt + 4];
+	__shared__ float us[kHk][kHt + 4];
+	const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+	const int row0 = blockIdx.x * kHt, col0 = blockIdx.y * kHt;
+	float acc[4][4], dv[4][4];
+#pragma unroll
+	for (int r = 0; r < 4; ++r)
+#pragma unroll
+		for (int c = 0; c < 4; ++c) {
+			const int i = row0 + tx + 16 * r, j = col0 + ty + 16 * c;
+			dv[r][c] = (i < m && j < n) ? __half2float(d[static_cast<int64_t>(j) * ldd + i]) : 0.f;
+			acc[r][c] = 0.f;
+		}
+	for (int q0 = 0; q0 < k; q0 += kHk) {
+		__syncthreads();
+		for (int e = threadIdx.x; e < kHt * kHk; e += 256) {
+			const int r = e / kHk, qq = e % kHk, q = q0 + qq;
+			const int i = row0 + r, j = col0 + r;
+			ls[qq][r] = (i < m && q < k) ? __half2float(l[static_cast<int64_t>(i) * ldl + q]) : 0.f;
+			us[qq][r] = (j < n && q < k) ? __half2float(u[static_cast<int64_t>(j) * ldu + q]) : 0.f;
+		}
+		__syncthreads();
+		const int qn = min(kHk, k - q0);
+		for (int qq = 0; qq < qn; ++qq) {
+			float a[4], bq[4];
+#pragma unroll
+			for (int r = 0; r < 4; ++r) a[r] = ls[qq][tx + 16 * r];
+#pragma unroll
+			for (int c = 0; c < 4; ++c) bq[c] = us[qq][ty + 16 * c];
+#pragma unroll
+			for (int r = 0; r < 4; ++r)
+#pragma unroll
+				for (int c = 0; c < 4; ++c) acc[r][c] = round_f16(__fmaf_rn(a[r], bq[c], acc[r][c]));
+			const int q = q0 + qq;
+			if ((q + 1) % kChunk == 0 || q + 1 == k) {
+#pragma unroll
+				for (int r = 0; r < 4; ++r)
+#pragma unroll
+					for (int c = 0; c < 4; ++c) {
+						dv[r][c] = round_f16(__fsub_rn(dv[r][c], acc[r][c]));
+						acc[r][c] = 0.f;
+					}
+			}
+		}
+	}
+#pragma unroll
+	for (int r = 0; r < 4; ++r)
+#pragma unroll
+		for (int c = 0; c < 4; ++c) {
+			const int i = row0 + tx + 16 * r, j = col0 + ty + 16 * c;
+			if (i < m && j < n) d[static_cast<int64_t>(j) * ldd + i] = __float2half_rn(dv[r][c]);
+		}
+}
+
+} // namespace
+
+int launch_hgemm_deck(int m, int n, int k, const uint16_t *l, int64_t ldl, const uint16_t *u, int64_t ldu,
+	uint16_t *d, int64_t ldd, cudaStream_t st)
+{
+	if (m <= 0 || n <= 0 || k <= 0) return HPLAI_OK;
+	if (!l || !u || !d || ldl < k || ldu < k || ldd < m) return HPLAI_EINVAL;
+	const dim3 grid((m + kHt - 1) / kHt, (n + kHt - 1) / kHt);
+	if (grid.y > 65535) return HPLAI_EINVAL;
+	hgemm_deck_kernel<<<grid, 256, 0, st>>>(m, n, k, reinterpret_cast<const __half *>(l), ldl,
+		reinterpret_cast<const __half *>(u), ldu, reinterpret_cast<__half *>(d), ldd);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+} // namespace hplai

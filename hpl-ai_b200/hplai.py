@@ -31,6 +31,7 @@ FLAG_SIMT_PANELS = 1
 FLAG_LOOKAHEAD = 2
 FLAG_FP16_DECK = 4
 FLAG_GROUP2 = 8
+FLAG_REF_DECK = 16
 IR, GMRES = 0, 1
 PHASES = ("DIAG_LU", "TRSM_L", "TRSM_R", "GEMM_UPDATE", "IR_GEMV", "IR_TRSV", "TOTAL", "LAZY_INIT")
 

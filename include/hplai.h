@@ -85,9 +85,10 @@ typedef enum hplai_phase {
 #define HPLAI_FLAG_SIMT_PANELS 1u
 /* One-step look-ahead on two streams: the next diagonal block and panels are
  * formed on a high-priority side stream while the main stream applies the
- * rest of the trailing update (which then leaves 20 SMs free).  Off by
- * default: on B200 the diagonal-block kernels slow down more under the
- * concurrent update than the overlap saves.  Results are bit-identical. */
+ * rest of the trailing update, leaving the side stream a fixed SM count or a
+ * share that grows as the trailing matrix shrinks (hplai_set_schedule;
+ * hplai_autotune picks one).  Results are bit-identical to the one-stream
+ * schedule. */
 #define HPLAI_FLAG_LOOKAHEAD 2u
 /* The trailing matrix's updates accumulate in an FP16 "deck" (the
  * double-decker lazy form, lazy_init.hpp:92-227): each step adds
@@ -106,6 +107,18 @@ typedef enum hplai_phase {
  * (hplai_create returns HPLAI_EINVAL otherwise); hplai_autotune may switch
  * it on or off for contexts whose b allows it. */
 #define HPLAI_FLAG_GROUP2 8u
+/* The reference's `-d` arithmetic bit for bit (a parity mode, CUDA cores):
+ * A is never stored -- a block is formed when it joins a panel as
+ * fma(downscale, deck, a_ij) with a_ij regenerated from the LCG
+ * (lazy_init.hpp:92-227; read from the matrix instead after hplai_upload);
+ * the L panel's FP16 copy is scaled by scalea = n^0.75 (hpl_rand.hpp:154) and
+ * downscale = 1 / scalea; the trailing updates go to an FP16 deck through the
+ * reference's FP16-accumulating GEMM (hgemm_opt, kernels/avx2.cpp:82-189: an
+ * FP16 accumulator rounded after every product, folded into the deck every
+ * 100 products); panels in netlib order (as HPLAI_FLAG_SIMT_PANELS), one
+ * stream.  Only with HPLAI_F32_F16 and without HPLAI_FLAG_FP16_DECK,
+ * HPLAI_FLAG_GROUP2 and HPLAI_FLAG_LOOKAHEAD (HPLAI_EINVAL otherwise). */
+#define HPLAI_FLAG_REF_DECK 16u
 
 typedef struct hplai_ctx hplai_ctx;
 

@@ -269,3 +269,23 @@ def test_driver_warmup_and_l1est(hplai, torch_cuda, tmp_path):
     assert out.returncode == 0, out.stderr
     m = re.search(r"resid = (\S+) hpl-harness = (\S+)$", out.stdout, re.M)
     assert m and 0 <= float(m.group(2)) < 16, out.stdout
+
+
+def test_driver_ref_deck_reproduces_the_references_steps(hplai, torch_cuda, tmp_path):
+    """driver.out ... -not -d -r --ref-deck: the reference's `-d` factors, so
+    the refinement log has the reference's number of steps, its step-0
+    residual to 1e-13 (the device GEMV's summation order) and its step-1
+    residual to 1e-8 (tests/golden/ref_c1.json,
+    the C1 command run by the reference's own driver)."""
+    fix = json.load(open(os.path.join(HERE, "golden", "ref_c1.json")))["runs"]["netlib_not_d_r"]
+    exe = os.path.abspath(os.path.join(HERE, "..", "hpl-ai_b200", "driver.out"))
+    out = subprocess.run([exe, "1200", "60", "2", "-not", "-d", "-r", "--ref-deck"], capture_output=True, text=True,
+                         timeout=300, cwd=tmp_path)
+    assert out.returncode == 0, out.stderr
+    assert "1gpu lazy full fp32/fp16 fp16-deck-ref" in out.stdout
+    steps = re.findall(r"# iterative refinement: step=\s*(\d+), residual=(\S+) hpl-harness=(\S+)", out.stdout)
+    assert len(steps) == len(fix["steps"]), out.stdout
+    assert abs(float(steps[0][1]) - fix["steps"][0]["residual"]) <= 1e-13 * fix["steps"][0]["residual"]
+    assert abs(float(steps[1][1]) - fix["steps"][1]["residual"]) <= 1e-8 * fix["steps"][1]["residual"]
+    m = re.search(r"resid = (\S+) hpl-harness = (\S+)$", out.stdout, re.M)
+    assert m and 0 <= float(m.group(2)) < 16, out.stdout
