@@ -88,6 +88,10 @@ struct hplai_ctx {
 	uint16_t *rdeck = nullptr;
 	float rscalea = 1.f, rdownscale = 1.f;
 	bool regen_a = false;
+	// the matrix family (hplai_set_matrix): the LCG benchmark matrix or
+	// Higham's, with its parameters
+	int matrix = HPLAI_MATRIX_LCG;
+	double h_alpha = 0.0, h_beta = 0.0;
 	SchurMaps maps8[2];           // [buffer]: K = b
 	SchurMaps maps8g[2];          // [buffer]: K = 2b (gcap 2)
 	SchurMaps maps8s;             // the single panel copy, K = b
@@ -234,8 +238,21 @@ int compute_norms(hplai_ctx *c)
 	HPLAI_CUDA_TRY(cudaMemcpyAsync(h, c->scal, sizeof h, cudaMemcpyDeviceToHost, c->st));
 	HPLAI_CUDA_TRY(cudaStreamSynchronize(c->st));
 	c->normb = h[0];
-	c->norma = 2.0 * h[1];   // hpl_infnorm: the diagonal is the off-diagonal row 1-norm
+	if (c->matrix == HPLAI_MATRIX_HIGHAM)
+		c->norma = higham_norm(c->n, c->h_alpha, c->h_beta);   // higham_infnorm (panel_norm.hpp:86-141)
+	else
+		c->norma = 2.0 * h[1];   // hpl_infnorm: the diagonal is the off-diagonal row 1-norm
 	return HPLAI_OK;
+}
+
+// y <- beta y + alpha A x (A^T x with trans), A regenerated in FP64
+// (panel_gemv with Matgen<double> or HMGen<double>, panel_gemv.hpp:57-132)
+int matvec(hplai_ctx *c, double alpha, const double *x, double beta, double *y, cudaStream_t st, bool trans)
+{
+	if (c->matrix == HPLAI_MATRIX_HIGHAM)
+		return launch_higham_gemv(c->n, alpha, x, beta, y, c->h_alpha, c->h_beta, c->d, c->gemv_work, c->gemv_bytes, st,
+			trans);
+	return launch_otf_gemv(c->n, alpha, x, beta, y, c->seed, c->d, c->gemv_work, c->gemv_bytes, st, trans);
 }
 
 } // namespace
@@ -428,8 +445,14 @@ extern "C" int hplai_generate(hplai_ctx *c, uint64_t seed)
 	// `-d` parity mode stores no A (pmatgen0, main.cpp:260-261): its lazy
 	// initialisation regenerates each block when it joins a panel.
 	c->regen_a = (c->flags & HPLAI_FLAG_REF_DECK) != 0;
-	if (!c->regen_a) HPLAI_TRY(launch_fill(n, 0, 0, n, n, c->A, c->lda, seed, 0, c->st));
-	HPLAI_TRY(launch_diag(n, 0, n, c->d, c->regen_a ? nullptr : c->A, c->lda, seed, c->st));
+	if (c->matrix == HPLAI_MATRIX_HIGHAM) {
+		// pmatgen / pdiaggen with HMGen (matgen.hpp:25-77, 227-243); the
+		// right-hand side stays the LCG's column n (main.cpp:266)
+		HPLAI_TRY(launch_higham_fill(n, c->h_alpha, c->h_beta, c->A, c->lda, c->d, false, c->st));
+	} else {
+		if (!c->regen_a) HPLAI_TRY(launch_fill(n, 0, 0, n, n, c->A, c->lda, seed, 0, c->st));
+		HPLAI_TRY(launch_diag(n, 0, n, c->d, c->regen_a ? nullptr : c->A, c->lda, seed, c->st));
+	}
 	HPLAI_TRY(launch_rhs(n, c->rhs, seed, c->st));
 	c->seed = seed;
 	HPLAI_TRY(compute_norms(c));
@@ -840,6 +863,15 @@ extern "C" int hplai_l1est(hplai_ctx *c)
 	if (!c) return HPLAI_EINVAL;
 	if (!c->have_inputs) return HPLAI_ESTATE;
 	for (double &v : c->phase_ms) v = 0.0;
+	if (c->matrix == HPLAI_MATRIX_HIGHAM) {
+		// pmatl1est with HMGen (matgen.hpp:147-192): Higham's matrix is L U with
+		// constant strictly triangular parts, so the "approximation" is exact
+		HPLAI_TRY(launch_higham_fill(c->n, c->h_alpha, c->h_beta, c->A, c->lda, nullptr, true, c->st));
+		HPLAI_TRY(launch_trsv_dinv(c->n, c->A, c->lda, c->dinv, c->st));
+		HPLAI_CUDA_TRY(cudaStreamSynchronize(c->st));
+		c->factored = true;
+		return HPLAI_OK;
+	}
 	if (c->regen_a) {
 		// --l1est stores A even with `-d` (pmatgen, main.cpp:260-263)
 		HPLAI_TRY(launch_fill(c->n, 0, 0, c->n, c->n, c->A, c->lda, c->seed, 0, c->st));
@@ -920,7 +952,7 @@ int correct_gmres(hplai_ctx *c, double *x, PhaseEvents &pe, int *inner, bool tra
 		double *vj = V + j * ldv, *vn = V + (j + 1) * ldv, *hc = H + j * kMaxBasis;
 		// w = M^{-1} A v_j, A regenerated in FP64
 		HPLAI_TRY(pe.record(st, HPLAI_PH_IR_GEMV));
-		HPLAI_TRY(launch_otf_gemv(n, 1.0, vj, 0.0, w, c->seed, c->d, c->gemv_work, c->gemv_bytes, st, trans));
+		HPLAI_TRY(matvec(c, 1.0, vj, 0.0, w, st, trans));
 		HPLAI_TRY(pe.end(st));
 		HPLAI_TRY(apply_lu_inverse(c, w, pe, trans));
 		// two Gram-Schmidt sweeps against v_0..v_j; ||w|| after the second
@@ -1008,7 +1040,7 @@ int refine_core(hplai_ctx *c, int mode, bool trans, const double *rhs, double no
 		HPLAI_TRY(launch_infnorm(n, x, c->scal + 2, st));
 		// r = b - A x with A regenerated in FP64 (panel_gemv(-1, ..., 1, r))
 		HPLAI_TRY(pe.record(st, HPLAI_PH_IR_GEMV));
-		HPLAI_TRY(launch_otf_gemv(n, -1.0, x, 1.0, c->r, c->seed, c->d, c->gemv_work, c->gemv_bytes, st, trans));
+		HPLAI_TRY(matvec(c, -1.0, x, 1.0, c->r, st, trans));
 		HPLAI_TRY(pe.end(st));
 		HPLAI_TRY(launch_infnorm(n, c->r, c->scal + 3, st));
 		double h[2];
@@ -1213,6 +1245,37 @@ extern "C" int hplai_set_schedule(hplai_ctx *c, unsigned flags, int side_sms)
 	if ((c->flags & HPLAI_FLAG_REF_DECK) && flags) return HPLAI_EINVAL;
 	c->flags = (c->flags & ~sched) | flags;
 	c->side_sms = side_sms;
+	return HPLAI_OK;
+}
+
+extern "C" int hplai_higham_params(int n, double cond, double rho, double *alpha, double *beta)
+{
+	if (!alpha || !beta) return HPLAI_EINVAL;
+	const double b = higham_beta(n, cond, rho);
+	if (!std::isfinite(b) || !(b > 0.)) return HPLAI_EINVAL;
+	*beta = b;
+	*alpha = rho * b;
+	return HPLAI_OK;
+}
+
+extern "C" int hplai_set_matrix(hplai_ctx *c, int kind, double cond, double rho)
+{
+	if (!c) return HPLAI_EINVAL;
+	if (kind == HPLAI_MATRIX_LCG) {
+		c->matrix = kind;
+	} else if (kind == HPLAI_MATRIX_HIGHAM) {
+		// the `-d` parity mode regenerates the LCG matrix at panel time
+		if (c->flags & HPLAI_FLAG_REF_DECK) return HPLAI_EUNSUPPORTED;
+		double a = 0.0, b = 0.0;
+		HPLAI_TRY(hplai_higham_params(c->n, cond, rho, &a, &b));
+		c->matrix = kind;
+		c->h_alpha = a;
+		c->h_beta = b;
+	} else {
+		return HPLAI_EINVAL;
+	}
+	c->have_inputs = false;
+	c->factored = false;
 	return HPLAI_OK;
 }
 

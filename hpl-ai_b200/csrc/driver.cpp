@@ -103,6 +103,7 @@ static int usage()
 		"                           Keep the trailing updates in an FP16 deck (double-decker form).\n"
 		"   --ref-deck              The reference's -d arithmetic bit for bit: A regenerated at panel\n"
 		"                           time, FP16-accumulating Schur update on CUDA cores (parity mode).\n"
+		"   --highammat             Higham's HPL-AI matrix (cond 1000) instead of the LCG matrix.\n"
 		"   --fp8                   e4m3 Schur update with GMRES refinement.\n"
 		"   --gmres                 GMRES refinement instead of the classical correction.\n"
 		"   --lookahead             Factor the next panel while the trailing update runs.\n"
@@ -125,7 +126,7 @@ int main(int argc, char **argv)
 	unsigned long long seed = 42;
 	int precision = HPLAI_F32_F16, mode = HPLAI_IR;
 	unsigned flags = 0;
-	bool checksum = false, autotune = false, warmup = false, l1est = false;
+	bool checksum = false, autotune = false, warmup = false, l1est = false, higham = false;
 	int nrow = 2;
 	int jobid = 0;
 	if (argc > 1) n = std::atoi(argv[1]);
@@ -139,6 +140,7 @@ int main(int argc, char **argv)
 			!std::strcmp(argv[i], "--lazy-init"))
 			flags |= HPLAI_FLAG_FP16_DECK;
 		else if (!std::strcmp(argv[i], "--ref-deck")) flags |= HPLAI_FLAG_REF_DECK;
+		else if (!std::strcmp(argv[i], "--highammat")) higham = true;
 		else if (!std::strcmp(argv[i], "--fp8")) { precision = HPLAI_F32_F8; mode = HPLAI_GMRES; }
 		else if (!std::strcmp(argv[i], "--gmres")) mode = HPLAI_GMRES;
 		else if (!std::strcmp(argv[i], "--lookahead")) flags |= HPLAI_FLAG_LOOKAHEAD;
@@ -163,9 +165,10 @@ int main(int argc, char **argv)
 	}
 
 	std::printf("n=%d b=%d r=1 c=1\n", n, b);
-	std::printf("1gpu %s full fp32/%s%s\n", (flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_REF_DECK)) ? "lazy" : "precomp",
+	std::printf("1gpu %s full fp32/%s%s%s\n", (flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_REF_DECK)) ? "lazy" : "precomp",
 		precision == HPLAI_F32_F8 ? "e4m3" : "fp16",
-		(flags & HPLAI_FLAG_REF_DECK) ? " fp16-deck-ref" : (flags & HPLAI_FLAG_FP16_DECK) ? " fp16-deck" : " ddmat");
+		(flags & HPLAI_FLAG_REF_DECK) ? " fp16-deck-ref" : (flags & HPLAI_FLAG_FP16_DECK) ? " fp16-deck" : "",
+		higham ? " hmat" : " ddmat");
 
 	// Warm-up on a small system with the same block size so that every kernel
 	// is loaded before the timed region (the reference warms BLAS up the same
@@ -176,6 +179,7 @@ int main(int argc, char **argv)
 		if (rc == HPLAI_OK) {
 			hplai_ir_errors e;
 			int it;
+			if (higham) hplai_set_matrix(w, HPLAI_MATRIX_HIGHAM, 1000., 0.5);
 			hplai_generate(w, seed);
 			hplai_factor(w);
 			hplai_refine(w, mode, maxit, &e, &it);
@@ -188,6 +192,14 @@ int main(int argc, char **argv)
 	if (rc != HPLAI_OK) {
 		std::fprintf(stderr, "hplai_create(n=%d, b=%d): %s\n", n, b, hplai_status_string(rc));
 		return 1;
+	}
+	if (higham) {
+		// HMGen(n, 1000., 0.5, ...) (main.cpp:258-259)
+		rc = hplai_set_matrix(ctx, HPLAI_MATRIX_HIGHAM, 1000., 0.5);
+		if (rc != HPLAI_OK) {
+			std::fprintf(stderr, "hplai_set_matrix(higham): %s\n", hplai_status_string(rc));
+			return 1;
+		}
 	}
 	if (autotune) {
 		unsigned tf = 0;

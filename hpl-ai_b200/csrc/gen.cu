@@ -10,6 +10,10 @@
 #include "common.cuh"
 #include "internal.h"
 
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+
 namespace hplai {
 
 // inc1^(2^k) for k < 64, passed by value as a kernel parameter.
@@ -187,6 +191,130 @@ int launch_lazy_init(int n, int r0, int r1, int c0, int c1, float *a, int64_t ld
 	dim3 grid((r1 - r0 + kFillRows - 1) / kFillRows, (c1 - c0 + kFillCols - 1) / kFillCols);
 	lazy_init_kernel<<<grid, kFillRows, 0, st>>>(n, r0, r1, c0, c1, a, lda, reinterpret_cast<const __half *>(deck), ldd,
 		downscale, seed, d, regen ? 1 : 0, jump_table());
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Higham's HPL-AI matrix (--highammat; higham_mat_impl.cpp, from Higham's
+// hpl-ai-matrix): A = L U with L unit lower triangular with every strictly
+// lower entry -alpha and U unit upper triangular with every strictly upper
+// entry -beta, so a_ij = -beta + ab i above the diagonal, 1 + ab i on it and
+// -alpha + ab j below it (ab = alpha beta).  beta is found by bisection so
+// that an estimate of cond(A, inf) equals kappa, alpha = rho beta.
+// ---------------------------------------------------------------------------
+namespace {
+
+// 32-bit int arithmetic with wrap-around: the reference evaluates the
+// estimate's integer terms in int, which wraps from about n = 46341 on, and
+// alpha and beta are kept identical to its values for every n.
+int32_t wrap32(int64_t v) { return static_cast<int32_t>(static_cast<uint32_t>(static_cast<uint64_t>(v))); }
+int32_t imul(int32_t a, int32_t b) { return wrap32(static_cast<int64_t>(a) * b); }
+
+// the condition-number estimate for (a, b) (fhpl, higham_mat_impl.cpp:38-61)
+double cond_estimate(int n, double a, double b)
+{
+	if (std::isnan(a)) a = b / 2;
+	const double l1 = 1 + (n - 1) * b;
+	const int id = std::min(static_cast<int>(std::floor(1. / a)), n);
+	const int k = std::min(static_cast<int>(std::floor((1 + b) / b)), n - 1);
+	int32_t t = wrap32(static_cast<int64_t>(imul(-k, k)) + k);
+	t = wrap32(static_cast<int64_t>(t) + imul(imul(3, id), id - 1) / 2);
+	t = wrap32(static_cast<int64_t>(t) - imul(n, id));
+	t = wrap32(static_cast<int64_t>(t) + n);
+	const double lid = 1 + (2 * k - id + 1) * a + (n - id) * b + static_cast<double>(t) * a * b;
+	const int32_t u = wrap32(static_cast<int64_t>(wrap32(static_cast<int64_t>(imul(-k, k)) + k)) + imul(n, n - 1) / 2);
+	const double ln = 1 + (2 * k - n + 1) * a + static_cast<double>(u) * a * b;
+	const double na = std::max(std::max(l1, lid), ln);
+	const double r = (1 + a) * (1 + b);
+	const double d1 = (1 + a) * (1. / (1 + a) + (r == 0. ? 0. : b * (1 - std::pow(r, n - 1)) / (1 - r)));
+	const double dn = std::pow(1 + a, n) * (1. / (1 + a));
+	const double ret = na * std::max(d1, dn);
+	return std::isinf(ret) ? DBL_MAX : ret;
+}
+
+// bisection on cond_estimate(rho x, x) - kappa (zero_find, higham_mat_impl.cpp:63-84)
+double bisect_beta(int n, double kappa, double rho, double lo, double hi)
+{
+	auto f = [&](double x) { return cond_estimate(n, rho * x, x) - kappa; };
+	if (f(lo) > 0. || f(hi) < 0.) return std::nan("");
+	for (;;) {
+		if (hi - lo < (2. * std::fabs(hi) + 0.5) * DBL_EPSILON) break;
+		const double mid = (lo + hi) / 2;
+		if (mid == lo || mid == hi) break;
+		const double fm = f(mid);
+		if (fm == 0.) return mid;
+		(fm < 0. ? lo : hi) = mid;
+	}
+	return hi;
+}
+
+// The FP32 matrix as the reference forms it in float (lazy_init.hpp:331-440:
+// one fused multiply-add of alpha_f beta_f, the index and -beta_f / -alpha_f
+// / 1) and the FP64 diagonal fma(ab, i, 1) (pdiaggen, matgen.hpp:227-243).
+__global__ void __launch_bounds__(kFillRows) higham_fill_kernel(int n, float abf, float mb, float ma,
+	float *__restrict__ a, int64_t lda, double ab, double *__restrict__ d)
+{
+	const int i = blockIdx.x * kFillRows + threadIdx.x;
+	const int j0 = blockIdx.y * kFillCols;
+	if (i >= n) return;
+	const float fi = static_cast<float>(i);
+	const float up = __fmaf_rn(abf, fi, mb);
+	const int j1 = min(j0 + kFillCols, n);
+	for (int j = j0; j < j1; ++j) {
+		const float v = i < j ? up : (i > j ? __fmaf_rn(abf, static_cast<float>(j), ma) : __fmaf_rn(abf, fi, 1.0f));
+		a[static_cast<int64_t>(j) * lda + i] = v;
+	}
+	if (blockIdx.y == 0 && d) d[i] = fma(ab, static_cast<double>(i), 1.0);
+}
+
+} // namespace
+
+double higham_beta(int n, double kappa, double rho)
+{
+	if (n < 2 || !(kappa > 1.) || !(rho > 0.)) return std::nan("");
+	// higham_mat_comp_beta (higham_mat_impl.cpp:87-113)
+	const double lo = DBL_EPSILON;
+	double hi = 1. / rho;
+	for (int k = 1;;) {
+		const double v = cond_estimate(n, rho * hi, hi) - kappa;
+		if (std::isfinite(v) && v > 0.) break;
+		hi *= 0.5;
+		if (++k == 100) break;
+	}
+	double beta = bisect_beta(n, kappa, rho, lo, hi);
+	while (rho * beta > 1.) {
+		hi *= 0.25;
+		beta = bisect_beta(n, kappa, rho, lo, hi);
+	}
+	return beta;
+}
+
+double higham_norm(int n, double alpha, double beta)
+{
+	// largest row sum of |a_ij|: the lower constants of the columns before the
+	// row, the diagonal, the row's upper constant n - 1 - i times
+	const double ab = alpha * beta;
+	long double best = 0, lower = 0;
+	for (int i = 0; i < n; ++i) {
+		const long double row = lower + std::fabs(std::fma(ab, static_cast<double>(i), 1.0)) +
+			static_cast<long double>(n - 1 - i) * std::fabs(std::fma(ab, static_cast<double>(i), -beta));
+		best = std::max(best, row);
+		lower += std::fabs(std::fma(ab, static_cast<double>(i), -alpha));
+	}
+	return static_cast<double>(best);
+}
+
+int launch_higham_fill(int n, double alpha, double beta, float *a, int64_t lda, double *d, bool factors, cudaStream_t st)
+{
+	if (n <= 0) return HPLAI_OK;
+	const float af = static_cast<float>(alpha), bf = static_cast<float>(beta);
+	dim3 grid((n + kFillRows - 1) / kFillRows, (n + kFillCols - 1) / kFillCols);
+	// factors: ab = 0 leaves -beta above, 1 on and -alpha below the diagonal,
+	// the exact unit-L / U factors in the one-array layout
+	higham_fill_kernel<<<grid, kFillRows, 0, st>>>(n, factors ? 0.0f : af * bf, -bf, -af, a, lda, alpha * beta,
+		factors ? nullptr : d);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;

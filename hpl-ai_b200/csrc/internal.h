@@ -22,6 +22,13 @@ int launch_rhs(int n, double *rhs, uint64_t seed, cudaStream_t st);
 int launch_rhs_cols(int n, int col0, int ncols, double *out, uint64_t seed, cudaStream_t st);
 // pmatl1est: strictly lower part of A (n x n, lda) times float(1/d_j) per column
 int launch_l1est(int n, float *a, int64_t lda, const double *d, cudaStream_t st);
+// Higham's HPL-AI matrix: beta for cond(A, inf) = kappa and alpha = rho beta
+// (NaN if the bisection fails), the FP32 matrix and the FP64 diagonal.
+double higham_beta(int n, double kappa, double rho);
+// With `factors`, the exact factors instead (-beta above, 1 on and -alpha
+// below the diagonal; d untouched).
+int launch_higham_fill(int n, double alpha, double beta, float *a, int64_t lda, double *d, bool factors, cudaStream_t st);
+double higham_norm(int n, double alpha, double beta);
 // The `-d` lazy initialisation a = fma(downscale, deck, a0) on rows [r0, r1)
 // x columns [c0, c1), a0 regenerated (regen) or read from a.
 int launch_lazy_init(int n, int r0, int r1, int c0, int c1, float *a, int64_t lda, const uint16_t *deck, int64_t ldd,
@@ -171,6 +178,10 @@ size_t otf_gemv_workspace(int n);
 // trans: y <- beta*y + alpha*A^T x
 int launch_otf_gemv(int n, double alpha, const double *x, double beta, double *y, uint64_t seed,
 	const double *diag, void *work, size_t work_bytes, cudaStream_t st, bool trans = false);
+// y <- beta y + alpha A x (A^T x with trans) over Higham's matrix with
+// parameters (halpha, hbeta), entries computed on the fly in FP64.
+int launch_higham_gemv(int n, double alpha, const double *x, double beta, double *y, double halpha, double hbeta,
+	const double *diag, void *work, size_t work_bytes, cudaStream_t st, bool trans);
 int launch_otf_gemv_block(int64_t n, int mb, int nb, double alpha, const double *x, double *y, uint64_t state00,
 	void *work, size_t work_bytes, cudaStream_t st);
 size_t trsv_workspace(int n);

@@ -148,6 +148,47 @@ int otf_launch(int64_t n, int mb, int nb, double alpha, const double *x, double 
 }
 
 // ---------------------------------------------------------------------------
+// On-the-fly GEMV over Higham's HPL-AI matrix (hmg_gemv_up/low/diag,
+// otf_gemv.cpp:133-314): the entries of row i are the lower constants
+// fma(ab, j, cl) of the columns j < i, the diagonal d_i and the upper
+// constant fma(ab, i, cu) of the row; A^T swaps the two constants.  Same
+// CTA shape, accumulators and fixed-order fold as the LCG GEMV.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(GEMV_ROWS) higham_partial_kernel(int n, double alpha, const double *__restrict__ x,
+	double ab, double cu, double cl, const double *__restrict__ diag, double *__restrict__ part)
+{
+	__shared__ double xs[GEMV_COLS];
+	__shared__ double ls[GEMV_COLS];
+	const int j0 = blockIdx.y * GEMV_COLS;
+	const int j1 = min(j0 + GEMV_COLS, n);
+	for (int j = threadIdx.x; j < j1 - j0; j += GEMV_ROWS) {
+		xs[j] = x[j0 + j];
+		ls[j] = fma(ab, static_cast<double>(j0 + j), cl);
+	}
+	__syncthreads();
+	const int i = blockIdx.x * GEMV_ROWS + threadIdx.x;
+	if (i >= n) return;
+	const double up = fma(ab, static_cast<double>(i), cu);
+	const int len = j1 - j0;
+	double a0 = 0.0, a1 = 0.0;
+	int j = 0;
+	for (; j + 1 < len; j += 2) {
+		const int g = j0 + j;
+		const double v0 = g < i ? ls[j] : (g > i ? up : 0.0);
+		const double v1 = g + 1 < i ? ls[j + 1] : (g + 1 > i ? up : 0.0);
+		a0 = fma(v0, xs[j], a0);
+		a1 = fma(v1, xs[j + 1], a1);
+	}
+	if (j < len) {
+		const int g = j0 + j;
+		a0 = fma(g < i ? ls[j] : (g > i ? up : 0.0), xs[j], a0);
+	}
+	double r = (a0 + a1) * alpha;
+	if (i >= j0 && i < j1) r = fma(alpha * diag[i], xs[i - j0], r);
+	part[static_cast<int64_t>(blockIdx.y) * n + i] = r;
+}
+
+// ---------------------------------------------------------------------------
 // Triangular solves.  Block rows of TB; CTA c handles block rows c, c+G, ...
 // in solve order, accumulating the off-diagonal products as the block
 // columns it depends on are published (flag[cb] == epoch), then solving its
@@ -629,6 +670,26 @@ int launch_otf_gemv(int n, double alpha, const double *x, double beta, double *y
 	void *work, size_t work_bytes, cudaStream_t st, bool trans)
 {
 	return otf_launch(n, n, n, alpha, x, beta, y, state_initial(seed), 1, diag, work, work_bytes, st, trans);
+}
+
+int launch_higham_gemv(int n, double alpha, const double *x, double beta, double *y, double halpha, double hbeta,
+	const double *diag, void *work, size_t work_bytes, cudaStream_t st, bool trans)
+{
+	if (n <= 0) return HPLAI_OK;
+	const int nchunks = (n + GEMV_COLS - 1) / GEMV_COLS;
+	if (work_bytes < static_cast<size_t>(nchunks) * n * sizeof(double)) return HPLAI_EINVAL;
+	double *part = static_cast<double *>(work);
+	const double ab = halpha * hbeta;
+	// A: upper constants -beta + ab i, lower -alpha + ab j; A^T the other way round
+	const double cu = trans ? -halpha : -hbeta, cl = trans ? -hbeta : -halpha;
+	higham_partial_kernel<<<dim3((n + GEMV_ROWS - 1) / GEMV_ROWS, nchunks), GEMV_ROWS, 0, st>>>(n, alpha, x, ab, cu, cl,
+		diag, part);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	otf_reduce_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, nchunks, beta, part, y, beta == 0.0 ? 1 : 0);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
 }
 
 int launch_otf_gemv_block(int64_t n, int mb, int nb, double alpha, const double *x, double *y, uint64_t state00,

@@ -32,6 +32,8 @@ FLAG_LOOKAHEAD = 2
 FLAG_FP16_DECK = 4
 FLAG_GROUP2 = 8
 FLAG_REF_DECK = 16
+MATRIX_LCG = 0
+MATRIX_HIGHAM = 1
 IR, GMRES = 0, 1
 PHASES = ("DIAG_LU", "TRSM_L", "TRSM_R", "GEMM_UPDATE", "IR_GEMV", "IR_TRSV", "TOTAL", "LAZY_INIT")
 
@@ -59,6 +61,9 @@ _destroy = _proto("hplai_destroy", _c_int, _vp)
 _generate = _proto("hplai_generate", _c_int, _vp, _c_u64)
 _upload = _proto("hplai_upload", _c_int, _vp, _vp, _c_i64, _vp, _vp, _c_u64)
 _factor = _proto("hplai_factor", _c_int, _vp)
+_set_matrix = _proto("hplai_set_matrix", _c_int, _vp, _c_int, ctypes.c_double, ctypes.c_double)
+_higham_params = _proto("hplai_higham_params", _c_int, _c_int, ctypes.c_double, ctypes.c_double,
+                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double))
 _factor_steps = _proto("hplai_factor_steps", _c_int, _vp, _c_int)
 _l1est = _proto("hplai_l1est", _c_int, _vp)
 _autotune = _proto("hplai_autotune", _c_int, _vp, _c_u64, _vp, _vp, _vp)
@@ -167,6 +172,13 @@ class RefineResult:
     status: int
 
 
+def higham_params(n: int, cond: float = 1000.0, rho: float = 0.5):
+    """(alpha, beta) of Higham's HPL-AI matrix of order n."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    check(_higham_params(n, cond, rho, ctypes.byref(a), ctypes.byref(b)), "hplai_higham_params")
+    return a.value, b.value
+
+
 class Solver:
     """One solve context: the single-GPU collapse of the reference driver."""
 
@@ -195,6 +207,10 @@ class Solver:
 
     def generate(self, seed: int = 42):
         check(_generate(self._h, seed), "hplai_generate")
+
+    def set_matrix(self, kind: int, cond: float = 1000.0, rho: float = 0.5):
+        """MATRIX_LCG (the benchmark matrix) or MATRIX_HIGHAM (--highammat)."""
+        check(_set_matrix(self._h, kind, cond, rho), "hplai_set_matrix")
 
     def upload(self, a: np.ndarray, rhs: np.ndarray, diag: np.ndarray, seed: int = 42):
         a = np.asfortranarray(a, dtype=np.float32)

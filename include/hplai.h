@@ -147,6 +147,32 @@ int hplai_destroy(hplai_ctx *ctx);
  * reference driver uses seed 42 (main.cpp:174). */
 int hplai_generate(hplai_ctx *ctx, uint64_t seed);
 
+/* Matrix families.  HPLAI_MATRIX_LCG: the HPL-AI benchmark matrix (LCG
+ * entries, row-sum diagonal; the default).  HPLAI_MATRIX_HIGHAM: Higham's
+ * HPL-AI matrix (the reference's --highammat, HMGen, highammgen.hpp:5-28,
+ * higham_mat_impl.cpp:116-128): A = L U with L unit lower triangular, every
+ * strictly lower entry -alpha, and U unit upper triangular, every strictly
+ * upper entry -beta, i.e. a_ij = -beta + alpha beta i above the diagonal,
+ * 1 + alpha beta i on it, -alpha + alpha beta j below it; beta is chosen by
+ * bisection so that an estimate of cond(A, inf) equals `cond` and
+ * alpha = rho beta (the reference's driver: cond 1000, rho 0.5). */
+#define HPLAI_MATRIX_LCG 0
+#define HPLAI_MATRIX_HIGHAM 1
+/* The matrix that hplai_generate produces and that the refinement's FP64
+ * GEMV regenerates (also after hplai_upload): kind HPLAI_MATRIX_LCG (cond and
+ * rho ignored) or HPLAI_MATRIX_HIGHAM with its condition number and ratio.
+ * The right-hand side stays column n of the LCG stream (main.cpp:266).
+ * hplai_l1est on Higham's matrix writes its exact factors (pmatl1est with
+ * HMGen, matgen.hpp:147-192).  Clears the inputs (call hplai_generate or
+ * hplai_upload next).  HPLAI_EUNSUPPORTED for Higham's matrix with
+ * HPLAI_FLAG_REF_DECK; HPLAI_EINVAL when the bisection finds no beta. */
+int hplai_set_matrix(hplai_ctx *ctx, int kind, double cond, double rho);
+/* alpha and beta of Higham's matrix of order n (higham_mat_comp_beta,
+ * higham_mat_impl.cpp:87-113; the estimate's integer terms in 32-bit int as
+ * the reference computes them, so that the values are the reference's for
+ * every n). */
+int hplai_higham_params(int n, double cond, double rho, double *alpha, double *beta);
+
 /* Host-supplied inputs: FP32 matrix (lda >= n), FP64 right-hand side and
  * FP64 diagonal, plus the LCG seed they came from (refinement regenerates
  * A in FP64 from it, as Matgen<double> does, main.cpp:257).  Copies

@@ -10,6 +10,9 @@
 #   ref_driver_netlib.out  linked with tmpi/netlib_blas.cpp (netlib loop
 #                          order, fused multiply-adds): a deterministic LU for
 #                          pinning the oracle bit for bit
+#   libref_higham.so       the reference's higham_mat_impl.cpp alone, so that
+#                          the fixture script can record the alpha and beta
+#                          of Higham's matrix (--highammat) it computes
 #
 # MPI is replaced by the thread-rank runtime in tmpi/ (TMPI_NP ranks as
 # threads of one process); main.cpp is compiled through tmpi/ref_xdump.cpp so
@@ -40,7 +43,7 @@ mkdir -p "$OBJ"
 
 stamp="$OUT/.stamp"
 newest_src=$(find "$REF" "$HERE/tmpi" "$HERE/build_ref.sh" -newer "$stamp" -type f 2>/dev/null | head -1 || true)
-if [ -f "$stamp" ] && [ -z "$newest_src" ] && [ -x "$OUT/ref_driver_netlib.out" ]; then
+if [ -f "$stamp" ] && [ -z "$newest_src" ] && [ -x "$OUT/ref_driver_netlib.out" ] && [ -f "$OUT/libref_higham.so" ]; then
 	exit 0
 fi
 
@@ -61,5 +64,6 @@ else
 	echo "build_ref.sh: no OpenBLAS found; the CPU baseline uses the netlib-order build" >&2
 	cp "$OUT/ref_driver_netlib.out" "$OUT/ref_driver.out"
 fi
+"$CXX" -shared -o "$OUT/libref_higham.so" "$OBJ/higham_mat_impl.o" -lm
 touch "$stamp"
 echo "build_ref.sh: built $OUT/ref_driver.out and $OUT/ref_driver_netlib.out"

@@ -54,6 +54,12 @@ _lu = _proto("orc_lu", _int, _int, _int, _vp, _i64)
 _lu_steps = _proto("orc_lu_steps", _int, _int, _int, _vp, _i64, _int)
 _l1est = _proto("orc_l1est", None, _int, _vp, _i64, _vp)
 _lu_deck_steps = _proto("orc_lu_deck_steps", _int, _int, _int, _u64, _vp, _vp, _i64, _int, _vp)
+_higham_beta = _proto("orc_higham_beta", _dbl, _int, _dbl, _dbl)
+_higham_fill = _proto("orc_higham_fill", None, _int, _int, _int, _int, _dbl, _dbl, _vp, _i64)
+_higham_elem = _proto("orc_higham_elem", _dbl, _i64, _i64, _dbl, _dbl)
+_higham_diag = _proto("orc_higham_diag", None, _int, _dbl, _dbl, _vp)
+_higham_norm = _proto("orc_higham_norm", _dbl, _int, _dbl, _dbl)
+_higham_resid = _proto("orc_higham_residual_rows", None, _int, _dbl, _dbl, _vp, _vp, _int, _vp, _vp)
 _deck_scales = _proto("orc_deck_scales", None, _int, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float))
 _otf_gemv = _proto("orc_otf_gemv", None, _int, _int, _int, _dbl, _vp, _vp, _u64, _vp)
 _trsv_l = _proto("orc_trsv_lower", None, _int, _int, _vp, _i64, _vp)
@@ -318,3 +324,50 @@ def residual_rows(n, x, rows, seed=42, trans=False, rhs_col=0, rhs_v=None) -> np
     _residual_rows(n, seed, _p(x), len(rows), _p(rows), 1 if trans else 0, rhs_col,
                    None if rv is None else _p(rv), _p(out))
     return out
+
+
+# ---- Higham's HPL-AI matrix (--highammat) --------------------------------
+
+def higham_params(n, cond=1000.0, rho=0.5):
+    """(alpha, beta): higham_mat_comp_beta restated (32-bit int terms)."""
+    b = _higham_beta(n, cond, rho)
+    return rho * b, b
+
+
+def higham_matrix(n, alpha, beta, i0=0, j0=0, nrow=None, ncol=None) -> np.ndarray:
+    """The FP32 matrix (or a sub-matrix) as the reference forms it in float."""
+    nrow = n if nrow is None else nrow
+    ncol = n if ncol is None else ncol
+    a = np.zeros((nrow, ncol), dtype=np.float32, order="F")
+    _higham_fill(i0, j0, nrow, ncol, alpha, beta, _p(a), nrow)
+    return a
+
+
+def higham_dense_f64(n, alpha, beta) -> np.ndarray:
+    """The FP64 matrix: row constants above the diagonal, column constants
+    below it, each one fused multiply-add as orc_higham_elem."""
+    up = np.array([_higham_elem(k, k + 1, alpha, beta) for k in range(n)])
+    lo = np.array([_higham_elem(k + 1, k, alpha, beta) for k in range(n)])
+    i = np.arange(n)
+    a = np.where(i[:, None] < i[None, :], up[:, None], lo[None, :])
+    np.fill_diagonal(a, higham_diag(n, alpha, beta))
+    return a
+
+
+def higham_diag(n, alpha, beta) -> np.ndarray:
+    d = np.zeros(n)
+    _higham_diag(n, alpha, beta, _p(d))
+    return d
+
+
+def higham_norm(n, alpha, beta) -> float:
+    return _higham_norm(n, alpha, beta)
+
+
+def higham_residual_rows(n, alpha, beta, x, rows, rhs_v) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    rhs_v = np.ascontiguousarray(rhs_v, dtype=np.float64)
+    r = np.zeros(rows.size)
+    _higham_resid(n, alpha, beta, _p(x), _p(rows), rows.size, _p(rhs_v), _p(r))
+    return r

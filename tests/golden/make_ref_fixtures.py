@@ -22,9 +22,21 @@ initialisation the LU runs through the FP16-accumulating Schur update
 (hgemm_opt), which the oracle restates in oracle/hplai_oracle_deck.c; one more
 `-d` run at n = 2400, b = 120 covers its k-chunks of 100 (two per panel).
 
+Higham's matrix (`--highammat`): the alpha and beta that the reference's
+higham_mat_comp_beta returns for a list of orders (oracle/_ref/libref_higham.so,
+its higham_mat_impl.cpp compiled alone), and the first refinement steps of
+its driver with `--highammat` (with and without `-d`), which diverge: its
+pmatgen drops the signs of Higham's matrix (matgen.hpp:25-77; the lazy
+initialisation keeps them, lazy_init.hpp:331-440) and its FP64 GEMV swaps
+alpha and beta inside the diagonal blocks (hmg_gemv_diag,
+otf_gemv.cpp:296-314), so the residual it refines against is of neither
+matrix.  The tests use the step-0 numbers to pin alpha, beta, the diagonal
+and the right-hand side through the reference's own residual evaluation.
+
 Needs oracle/_ref (built from the reference tree on this machine); the
 fixture it writes is what the tests read.
 """
+import ctypes
 import hashlib
 import json
 import os
@@ -69,6 +81,29 @@ def run(exe, flags, ludump, n=N, b=B, keep_x=True):
     return rec
 
 
+def higham():
+    lib = ctypes.CDLL(os.path.join(REF, "libref_higham.so"))
+    lib.higham_mat_comp_beta.restype = ctypes.c_double
+    lib.higham_mat_comp_beta.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
+    betas = []
+    for n in [64, 120, 1200, 2400, 4096, 8192, 16384, 46340, 46341, 50000, 65536, 98304, 131072, 196608]:
+        for cond, rho in [(1000.0, 0.5), (100.0, 0.5), (1.0e4, 0.25)]:
+            betas.append({"n": n, "cond": cond, "rho": rho, "beta": lib.higham_mat_comp_beta(n, cond, rho).hex()})
+    runs = {}
+    for key, flags in [("not_r", ["-not", "-r", "--highammat"]), ("not_d_r", ["-not", "-d", "-r", "--highammat"])]:
+        with tempfile.TemporaryDirectory() as td:
+            env = dict(os.environ, TMPI_NP="4", OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
+            out = subprocess.run([os.path.join(REF, "ref_driver_netlib.out"), str(N), str(B), str(P)] + flags,
+                                 capture_output=True, text=True, env=env, cwd=td, timeout=600, check=True).stdout
+        steps = [{"residual": float(r), "hpl_harness": float(h)} for _, r, h in STEP.findall(out)]
+        m = REPORT.search(out)
+        runs[key] = {"command": f"driver.out {N} {B} {P} " + " ".join(flags), "build": "ref_driver_netlib.out",
+                     "first_steps": steps[:3], "steps": len(steps), "resid": float(m.group(3)),
+                     "hpl_harness": float(m.group(4))}
+    return {"betas": betas, "runs": runs,
+            "note": "the reference's --highammat refinement diverges (IRErrors {-1,-1}); see make_ref_fixtures.py"}
+
+
 def main():
     runs = {
         "netlib_not_r": run("ref_driver_netlib.out", ["-not", "-r"], True),
@@ -81,7 +116,7 @@ def main():
     }
     doc = {"n": N, "b": B, "seed": 42, "ranks": "4 threads (2 x 2 grid), OMP_NUM_THREADS=1",
            "generator": "tests/golden/make_ref_fixtures.py (reference built by oracle/build_ref.sh)",
-           "x_format": "float.hex() per entry", "runs": runs}
+           "x_format": "float.hex() per entry", "runs": runs, "higham": higham()}
     with open(os.path.join(HERE, "ref_c1.json"), "w") as f:
         json.dump(doc, f, indent=1)
         f.write("\n")
