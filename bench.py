@@ -344,7 +344,8 @@ class FormRun:
     hpl-harness < 16) after `warmup` untimed ones, the matrix regenerated on
     the device before each solve outside the timed window."""
 
-    def __init__(self, hplai, torch, form, n, b, seed, maxit, autotune, lookahead, barrier, group=1, side_sms=32):
+    def __init__(self, hplai, torch, form, n, b, seed, maxit, autotune, lookahead, barrier, group=1, side_sms=32,
+                 matrix="lcg"):
         self.hplai, self.torch, self.form = hplai, torch, form
         self.n, self.b, self.seed, self.maxit = n, b, seed, maxit
         self.fp8 = form["precision"] == "f8"
@@ -356,6 +357,8 @@ class FormRun:
         if group == 2:
             flags |= hplai.FLAG_GROUP2
         self.s = hplai.Solver(n, b, precision=hplai.F32_F8 if self.fp8 else hplai.F32_F16, flags=flags)
+        if matrix == "higham":
+            self.s.set_matrix(hplai.MATRIX_HIGHAM, 1000.0, 0.5)
         self.ext = torch.cuda.ExternalStream(self.s.stream())
         self.barrier = barrier
         self.tuned = None
@@ -510,7 +513,7 @@ def run_ours(args):
 
     # the headline form: exactly `steps` timed solves after `warmup`
     fr = FormRun(hplai, torch, head_form, n, b, seed, maxit, args.autotune, args.lookahead, barrier, args.group,
-                 args.side_sms)
+                 args.side_sms, args.matrix)
     fr.run(0, args.warmup)
     sampler = ClockSampler(dev)
     sampler.start()
@@ -528,7 +531,7 @@ def run_ours(args):
     other = None
     if other_key:
         fo = FormRun(hplai, torch, FORMS[other_key], n, b, seed, maxit, args.autotune, args.lookahead, barrier,
-                     args.group, args.side_sms)
+                     args.group, args.side_sms, args.matrix)
         fo.run(min(args.steps, args.compare_steps), min(args.warmup, args.compare_warmup))
         other = fo.summary(world)
         fo.close()
@@ -556,8 +559,12 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "e4m3/fp16/fp32/fp64" if head_form["precision"] == "f8" else "fp16/fp32/fp64",
-            "data": "synthetic (the reference's own LCG matrix, seed 42, regenerated on the device before each step)",
-            "config": {"workload": wl, "n": n, "b": b, "form": head["form"], "schedule": head["schedule"],
+            "data": ("synthetic (the reference's own LCG matrix, seed 42, regenerated on the device before each step)"
+                     if args.matrix == "lcg" else
+                     "synthetic (Higham's HPL-AI matrix, cond 1000, rho 0.5, as --highammat; LCG right-hand side, "
+                     "seed 42; regenerated on the device before each step)"),
+            "config": {"workload": wl, "n": n, "b": b, "matrix": args.matrix, "form": head["form"],
+                       "schedule": head["schedule"],
                        "autotuned": head["autotuned"],
                        "trailing_matrix": head["trailing_matrix"],
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
@@ -854,6 +861,8 @@ def main():
                     help="solve: one system (default n=131072 b=1024, precision and plain forms); batch: many "
                          "systems; adjoint: forward + transposed solves; gemm / check: the Schur GEMM or the "
                          "factor checksum leaf alone; peak: cuBLAS bf16/e4m3 dense rates (the roofline denominators)")
+    ap.add_argument("--matrix", choices=("lcg", "higham"), default="lcg",
+                    help="solve workload: the benchmark's LCG matrix or Higham's (the reference's --highammat)")
     ap.add_argument("--m", type=int, default=16384, help="gemm workload: rows of C")
     ap.add_argument("--n-cols", type=int, default=16384, help="gemm workload: columns of C")
     ap.add_argument("--k", type=int, default=512, help="gemm workload: panel width")
@@ -868,7 +877,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the serial schedule (or --lookahead's)")
     ap.add_argument("--side-sms", type=int, default=32, help="SMs of the side stream with --lookahead (no autotune)")
     ap.add_argument("--group", type=int, choices=(1, 2), default=1,
-                    help="panels per trailing update without autotuning (2 = HPLAI_FLAG_GROUP2, b % 128 == 0)")
+                    help="panels per trailing update without autotuning (2 = HPLAI_FLAG_GROUP2, b %% 128 == 0)")
     ap.add_argument("--lookahead", action="store_true",
                     help="form the next step's diagonal block and panels on a side stream (HPLAI_FLAG_LOOKAHEAD)")
     ap.add_argument("--refine", choices=("ir", "gmres"), default=None,
