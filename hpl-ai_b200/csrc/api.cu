@@ -85,7 +85,7 @@ struct hplai_ctx {
 	// HPLAI_FLAG_REF_DECK: the reference's `-d` deck (n x lda halves), its
 	// FP16 L-panel scale n^0.75 and the lazy-init downscale; regen_a: A is
 	// not stored (hplai_generate) and the lazy initialisation regenerates it
-	uint16_t *rdeck = nullptr;
+	uint16_t *rdeck = nullptr, *rback = nullptr;   // rback: HPLAI_FLAG_REF_BACKBUF
 	float rscalea = 1.f, rdownscale = 1.f;
 	bool regen_a = false;
 	// the matrix family (hplai_set_matrix): the LCG benchmark matrix or
@@ -162,6 +162,7 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->qbits);
 	cudaFree(c->deck);
 	cudaFree(c->rdeck);
+	cudaFree(c->rback);
 	cudaFree(c->tcbuf);
 	cudaFree(c->rhs);
 	cudaFree(c->d);
@@ -297,6 +298,7 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	if ((flags & HPLAI_FLAG_REF_DECK) &&
 		(precision != HPLAI_F32_F16 || (flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_LOOKAHEAD))))
 		return HPLAI_EINVAL;
+	if ((flags & HPLAI_FLAG_REF_BACKBUF) && !(flags & HPLAI_FLAG_REF_DECK)) return HPLAI_EINVAL;
 	hplai_ctx *c = new hplai_ctx;
 	c->n = n;
 	c->b = b;
@@ -356,6 +358,7 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	}
 	if (flags & HPLAI_FLAG_REF_DECK) {
 		CTX_ALLOC(c->rdeck, sizeof(uint16_t) * static_cast<size_t>(c->lda) * n);
+		if (flags & HPLAI_FLAG_REF_BACKBUF) CTX_ALLOC(c->rback, sizeof(uint16_t) * static_cast<size_t>(c->lda) * n);
 		// scalea = sqrt(n sqrt(n)) in FP64, then FP32; downscale = FP32(1 / (scalea * scaleb)), scaleb = 1
 		// (hpl_rand.hpp:154-155, panel_trf.hpp:717-719)
 		c->rscalea = static_cast<float>(std::sqrt(n * std::sqrt(static_cast<double>(n))));
@@ -668,13 +671,14 @@ int factor_refdeck(hplai_ctx *c, int kend)
 	for (double &v : c->phase_ms) v = 0.0;
 	PhaseEvents pe;
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->rdeck, 0, sizeof(uint16_t) * static_cast<size_t>(lda) * n, st));
+	if (c->rback) HPLAI_CUDA_TRY(cudaMemsetAsync(c->rback, 0, sizeof(uint16_t) * static_cast<size_t>(lda) * n, st));
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->getrf_work, 0, sizeof(uint32_t), st));   // its status word
 	// pmatgen0 (matgen.hpp:81-105): the blocks a warm-up leaves unformed hold zero
 	if (c->regen_a) HPLAI_CUDA_TRY(cudaMemsetAsync(c->A, 0, sizeof(float) * static_cast<size_t>(lda) * n, st));
 	auto lazy = [&](int r0, int r1, int c0, int c1) -> int {
 		HPLAI_TRY(pe.record(st, HPLAI_PH_LAZY_INIT));
-		HPLAI_TRY(launch_lazy_init(n, r0, r1, c0, c1, c->A, lda, c->rdeck, lda, c->rdownscale, c->seed, c->d, c->regen_a,
-			st));
+		HPLAI_TRY(launch_lazy_init(n, r0, r1, c0, c1, c->A, lda, c->rdeck, c->rback, lda, c->rdownscale, c->seed, c->d,
+			c->regen_a, st));
 		return pe.end(st);
 	};
 	const int steps = std::min(kend, nb);
@@ -697,6 +701,13 @@ int factor_refdeck(hplai_ctx *c, int kend)
 		HPLAI_TRY(launch_trsm_left_lower(b, rem, diag, lda, diag + static_cast<int64_t>(b) * lda, lda, uh, ldg, 1.0f, st));
 		HPLAI_TRY(pe.end(st));
 		if (k == kend - 1 && kend < nb) break;
+		// BackBuffer::write_back at the end of the reference's iteration k
+		// (BB_NCYCLE = 32), before panel k's update, which it applies in k+1
+		if (c->rback && k >= 1 && (k - 1) % 32 == 31) {
+			HPLAI_TRY(pe.record(st, HPLAI_PH_WRITE_BACK));
+			HPLAI_TRY(launch_backbuf_writeback(n, kb + b, c->rdeck, c->rback, lda, st));
+			HPLAI_TRY(pe.end(st));
+		}
 		HPLAI_TRY(pe.record(st, HPLAI_PH_GEMM_UPDATE));
 		HPLAI_TRY(launch_hgemm_deck(rem, rem, b, lh, ldg, uh, ldg, c->rdeck + (kb + b) + static_cast<int64_t>(kb + b) * lda,
 			lda, st));

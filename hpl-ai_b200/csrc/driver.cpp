@@ -36,7 +36,7 @@
 static void write_timerdump(int jobid, int n, int b, double total_s, const double *ms, long long matvecs,
 	bool overlapped, bool warmup)
 {
-	enum { DIAG_LU = 5, TRSM_L = 6, TRSM_R = 7, GEMM_UPDATE = 10, GEMM_PROGRESS = 11, LAZY_INIT = 12, IR_GEMV = 14,
+	enum { DIAG_LU = 5, TRSM_L = 6, TRSM_R = 7, GEMM_UPDATE = 10, GEMM_PROGRESS = 11, LAZY_INIT = 12, WRITE_BACK = 13, IR_GEMV = 14,
 		IR_TRSV = 16, TOTAL = 19, MISC = 20, NUM_ITEMS = 21 };
 	static const char *names[NUM_ITEMS] = {"DIAG_BCAST", "LCOL_BCAST", "RROW_BCAST", "TEST", "WAIT", "DIAG_LU",
 		"TRSM_L", "TRSM_R", "CONV_L", "CONV_R", "GEMM_UPDATE", "GEMM_PROGRESS", "LAZY_INIT", "WRITE_BACK", "IR_GEMV",
@@ -49,6 +49,7 @@ static void write_timerdump(int jobid, int n, int b, double total_s, const doubl
 	t[TRSM_R] = 1e-3 * ms[HPLAI_PH_TRSM_R];
 	t[GEMM_UPDATE] = 1e-3 * ms[HPLAI_PH_GEMM_UPDATE];
 	t[LAZY_INIT] = 1e-3 * ms[HPLAI_PH_LAZY_INIT];
+	t[WRITE_BACK] = 1e-3 * ms[HPLAI_PH_WRITE_BACK];
 	t[IR_GEMV] = 1e-3 * ms[HPLAI_PH_IR_GEMV];
 	t[IR_TRSV] = 1e-3 * ms[HPLAI_PH_IR_TRSV];
 	t[TOTAL] = total_s;
@@ -103,6 +104,7 @@ static int usage()
 		"                           Keep the trailing updates in an FP16 deck (double-decker form).\n"
 		"   --ref-deck              The reference's -d arithmetic bit for bit: A regenerated at panel\n"
 		"                           time, FP16-accumulating Schur update on CUDA cores (parity mode).\n"
+		"   --back_buffer           With --ref-deck (implied): the reference's back-buffer form bit for bit.\n"
 		"   --highammat             Higham's HPL-AI matrix (cond 1000) instead of the LCG matrix.\n"
 		"   --fp8                   e4m3 Schur update with GMRES refinement.\n"
 		"   --gmres                 GMRES refinement instead of the classical correction.\n"
@@ -140,6 +142,7 @@ int main(int argc, char **argv)
 			!std::strcmp(argv[i], "--lazy-init"))
 			flags |= HPLAI_FLAG_FP16_DECK;
 		else if (!std::strcmp(argv[i], "--ref-deck")) flags |= HPLAI_FLAG_REF_DECK;
+		else if (!std::strcmp(argv[i], "--back_buffer")) flags |= HPLAI_FLAG_REF_DECK | HPLAI_FLAG_REF_BACKBUF;
 		else if (!std::strcmp(argv[i], "--highammat")) higham = true;
 		else if (!std::strcmp(argv[i], "--fp8")) { precision = HPLAI_F32_F8; mode = HPLAI_GMRES; }
 		else if (!std::strcmp(argv[i], "--gmres")) mode = HPLAI_GMRES;
@@ -167,7 +170,8 @@ int main(int argc, char **argv)
 	std::printf("n=%d b=%d r=1 c=1\n", n, b);
 	std::printf("1gpu %s full fp32/%s%s%s\n", (flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_REF_DECK)) ? "lazy" : "precomp",
 		precision == HPLAI_F32_F8 ? "e4m3" : "fp16",
-		(flags & HPLAI_FLAG_REF_DECK) ? " fp16-deck-ref" : (flags & HPLAI_FLAG_FP16_DECK) ? " fp16-deck" : "",
+		(flags & HPLAI_FLAG_REF_BACKBUF) ? " fp16-deck-ref back_buffer"
+		: (flags & HPLAI_FLAG_REF_DECK) ? " fp16-deck-ref" : (flags & HPLAI_FLAG_FP16_DECK) ? " fp16-deck" : "",
 		higham ? " hmat" : " ddmat");
 
 	// Warm-up on a small system with the same block size so that every kernel

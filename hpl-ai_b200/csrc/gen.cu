@@ -156,11 +156,12 @@ int launch_l1est(int n, float *a, int64_t lda, const double *d, cudaStream_t st)
 //     a(i, j) = fma(downscale, deck(i, j), a0(i, j)),
 // one fused multiply-add like the reference's x86 build, with the initial
 // value a0 regenerated from the LCG (float(d_i) on the diagonal, d the FP64
-// row sums) when `regen`, or read from a (an uploaded matrix) otherwise.
-// Rows [r0, r1) x columns [c0, c1), one thread per row.
+// row sums) when `regen`, or read from a (an uploaded matrix) otherwise;
+// with a back buffer the deck value is deck + 32 back.  Rows [r0, r1) x
+// columns [c0, c1), one thread per row.
 __global__ void __launch_bounds__(kFillRows) lazy_init_kernel(int n, int r0, int r1, int c0, int c1,
-	float *__restrict__ a, int64_t lda, const __half *__restrict__ deck, int64_t ldd, float downscale, uint64_t seed,
-	const double *__restrict__ d, int regen, JumpTable tab)
+	float *__restrict__ a, int64_t lda, const __half *__restrict__ deck, const __half *__restrict__ back, int64_t ldd,
+	float downscale, uint64_t seed, const double *__restrict__ d, int regen, JumpTable tab)
 {
 	const int i = r0 + blockIdx.x * kFillRows + threadIdx.x;
 	const int j0 = c0 + blockIdx.y * kFillCols;
@@ -180,17 +181,20 @@ __global__ void __launch_bounds__(kFillRows) lazy_init_kernel(int n, int r0, int
 		} else {
 			a0 = a[o];
 		}
-		a[o] = __fmaf_rn(downscale, __half2float(deck[static_cast<int64_t>(j) * ldd + i]), a0);
+		const int64_t od = static_cast<int64_t>(j) * ldd + i;
+		// with the back buffer: deck + 32 back (lazy_init_omp.cpp:704-760)
+		const float x = back ? __fmaf_rn(32.0f, __half2float(back[od]), __half2float(deck[od])) : __half2float(deck[od]);
+		a[o] = __fmaf_rn(downscale, x, a0);
 	}
 }
 
-int launch_lazy_init(int n, int r0, int r1, int c0, int c1, float *a, int64_t lda, const uint16_t *deck, int64_t ldd,
-	float downscale, uint64_t seed, const double *d, bool regen, cudaStream_t st)
+int launch_lazy_init(int n, int r0, int r1, int c0, int c1, float *a, int64_t lda, const uint16_t *deck,
+	const uint16_t *back, int64_t ldd, float downscale, uint64_t seed, const double *d, bool regen, cudaStream_t st)
 {
 	if (r1 <= r0 || c1 <= c0) return HPLAI_OK;
 	dim3 grid((r1 - r0 + kFillRows - 1) / kFillRows, (c1 - c0 + kFillCols - 1) / kFillCols);
-	lazy_init_kernel<<<grid, kFillRows, 0, st>>>(n, r0, r1, c0, c1, a, lda, reinterpret_cast<const __half *>(deck), ldd,
-		downscale, seed, d, regen ? 1 : 0, jump_table());
+	lazy_init_kernel<<<grid, kFillRows, 0, st>>>(n, r0, r1, c0, c1, a, lda, reinterpret_cast<const __half *>(deck),
+		reinterpret_cast<const __half *>(back), ldd, downscale, seed, d, regen ? 1 : 0, jump_table());
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;

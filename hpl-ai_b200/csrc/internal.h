@@ -31,8 +31,11 @@ int launch_higham_fill(int n, double alpha, double beta, float *a, int64_t lda, 
 double higham_norm(int n, double alpha, double beta);
 // The `-d` lazy initialisation a = fma(downscale, deck, a0) on rows [r0, r1)
 // x columns [c0, c1), a0 regenerated (regen) or read from a.
-int launch_lazy_init(int n, int r0, int r1, int c0, int c1, float *a, int64_t lda, const uint16_t *deck, int64_t ldd,
-	float downscale, uint64_t seed, const double *d, bool regen, cudaStream_t st);
+int launch_lazy_init(int n, int r0, int r1, int c0, int c1, float *a, int64_t lda, const uint16_t *deck,
+	const uint16_t *back, int64_t ldd, float downscale, uint64_t seed, const double *d, bool regen, cudaStream_t st);
+// The back buffer's write-back of the deck over rows and columns [r0, n)
+// (bb_writeback_b_impl_fp16, back_buffer.cpp:53-100).
+int launch_backbuf_writeback(int n, int r0, uint16_t *deck, uint16_t *back, int64_t ld, cudaStream_t st);
 // The reference's FP16-accumulating Schur update of the deck (hgemm_opt,
 // alpha = -1): D(m x n) -= L(m x k) U(k x n) with an FP16 accumulator per
 // element over k-chunks of 100.  L row i at l + i ldl, U column j at

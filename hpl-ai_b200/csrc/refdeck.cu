@@ -17,6 +17,8 @@
 #include "common.cuh"
 #include "internal.h"
 
+#include <algorithm>
+
 namespace hplai {
 namespace {
 
@@ -83,7 +85,41 @@ __global__ void __launch_bounds__(256) hgemm_deck_kernel(int m, int n, int k, co
 		}
 }
 
+// The back buffer (`--back_buffer`, back_buffer.hpp:81-170): every 32 steps
+// the deck's value moves into a second FP16 array with a compensated sum,
+// each operation rounded to FP16 through FP32 (the reference's FP16
+// arithmetic, svesim.hpp:190-262):
+//     p = h(y / 32), t2 = h(x + p), t3 = h(t2 - x), t4 = h(p - t3),
+//     back = t2, deck = h(32 t4).
+__global__ void __launch_bounds__(256) backbuf_kernel(int n, int r0, __half *__restrict__ deck,
+	__half *__restrict__ back, int64_t ld)
+{
+	const int i = r0 + blockIdx.x * 256 + threadIdx.x;
+	if (i >= n) return;
+	for (int j = r0 + blockIdx.y; j < n; j += gridDim.y) {
+		const int64_t o = static_cast<int64_t>(j) * ld + i;
+		const float x = __half2float(back[o]);
+		const float p = round_f16(__fmul_rn(__half2float(deck[o]), 0.03125f));
+		const float t2 = round_f16(__fadd_rn(x, p));
+		const float t3 = round_f16(__fsub_rn(t2, x));
+		const float t4 = round_f16(__fsub_rn(p, t3));
+		back[o] = __float2half_rn(t2);
+		deck[o] = __float2half_rn(__fmul_rn(t4, 32.0f));
+	}
+}
+
 } // namespace
+
+int launch_backbuf_writeback(int n, int r0, uint16_t *deck, uint16_t *back, int64_t ld, cudaStream_t st)
+{
+	if (r0 >= n) return HPLAI_OK;
+	if (!deck || !back || ld < n) return HPLAI_EINVAL;
+	const dim3 grid((n - r0 + 255) / 256, std::min(n - r0, 4096));
+	backbuf_kernel<<<grid, 256, 0, st>>>(n, r0, reinterpret_cast<__half *>(deck), reinterpret_cast<__half *>(back), ld);
+	count_launches();
+	HPLAI_CUDA_TRY(cudaGetLastError());
+	return HPLAI_OK;
+}
 
 int launch_hgemm_deck(int m, int n, int k, const uint16_t *l, int64_t ldl, const uint16_t *u, int64_t ldu,
 	uint16_t *d, int64_t ldd, cudaStream_t st)

@@ -32,10 +32,11 @@ FLAG_LOOKAHEAD = 2
 FLAG_FP16_DECK = 4
 FLAG_GROUP2 = 8
 FLAG_REF_DECK = 16
+FLAG_REF_BACKBUF = 32
 MATRIX_LCG = 0
 MATRIX_HIGHAM = 1
 IR, GMRES = 0, 1
-PHASES = ("DIAG_LU", "TRSM_L", "TRSM_R", "GEMM_UPDATE", "IR_GEMV", "IR_TRSV", "TOTAL", "LAZY_INIT")
+PHASES = ("DIAG_LU", "TRSM_L", "TRSM_R", "GEMM_UPDATE", "IR_GEMV", "IR_TRSV", "TOTAL", "LAZY_INIT", "WRITE_BACK")
 
 _c_int, _c_i64, _c_u64, _c_dbl, _c_flt, _c_sz, _vp = (
     ctypes.c_int, ctypes.c_int64, ctypes.c_uint64, ctypes.c_double, ctypes.c_float, ctypes.c_size_t,

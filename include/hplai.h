@@ -75,7 +75,8 @@ typedef enum hplai_phase {
 	HPLAI_PH_IR_TRSV = 5,
 	HPLAI_PH_TOTAL = 6,      /* sum of the other items (overlapping side-stream items included) */
 	HPLAI_PH_LAZY_INIT = 7,  /* FP16 deck folded into the next block column/row (lazy_init.hpp:92-227) */
-	HPLAI_PH_COUNT = 8
+	HPLAI_PH_WRITE_BACK = 8, /* the back buffer's write-backs (back_buffer.hpp:125-169) */
+	HPLAI_PH_COUNT = 9
 } hplai_phase;
 
 /* hplai_create flags. */
@@ -119,6 +120,13 @@ typedef enum hplai_phase {
  * stream.  Only with HPLAI_F32_F16 and without HPLAI_FLAG_FP16_DECK,
  * HPLAI_FLAG_GROUP2 and HPLAI_FLAG_LOOKAHEAD (HPLAI_EINVAL otherwise). */
 #define HPLAI_FLAG_REF_DECK 16u
+/* With HPLAI_FLAG_REF_DECK: the reference's `--back_buffer` form bit for bit
+ * (dd_layout = 2, back_buffer.hpp:81-170): every 32 steps the deck is written
+ * back into a second FP16 array with a compensated FP16 sum (deck / 32 moved
+ * into it, the remainder kept), and the lazy initialisation forms
+ * fma(downscale, deck + 32 back, a_ij).  HPLAI_EINVAL without
+ * HPLAI_FLAG_REF_DECK. */
+#define HPLAI_FLAG_REF_BACKBUF 32u
 
 typedef struct hplai_ctx hplai_ctx;
 

@@ -24,6 +24,18 @@
  * The lazy-init sum scale * deck + a_ij is one FMA in the reference's x86
  * build (g++ -O2 contracts it), written here as fmaf().  Compiled with
  * -ffp-contract=off, like hplai_oracle.c.
+ *
+ * The back buffer (`--back_buffer`, dd_layout = 2, back_buffer.hpp:81-170,
+ * back_buffer.cpp:53-191): a second FP16 array per element.  At the end of
+ * step k with (k - 1) % 32 == 31 (BB_NCYCLE = 32) every element of the
+ * trailing blocks (rows and columns from (k+1) b on; panel k's update not yet
+ * applied) moves its deck value into the back buffer with a compensated sum,
+ * in FP16 arithmetic (each operation rounded to FP16 through FP32, the x86
+ * build's emulation of the SVE FP16 instructions, svesim.hpp:190-262):
+ *     p = h(y / 32),  t2 = h(x + p),  t3 = h(t2 - x),  t4 = h(p - t3),
+ *     back = t2,  deck = h(32 t4);
+ * the lazy initialisation then forms fma(scale, deck + 32 back, a_ij)
+ * (lazy_init_omp.cpp:600-630, 704-760).
  */
 #include <stdint.h>
 #include <stdlib.h>
@@ -70,8 +82,8 @@ ORC_EXPORT void orc_deck_scales(int n, float *scalea, float *downscale)
 /* LazyInitializer<FLow,1,true>::update / update_diag over the rectangle
  * rows r0..r1, cols c0..c1 (block-aligned): A = fma(downscale, deck, a_ij),
  * a_ii = diag_f[i]. */
-static void lazy_init(int n, uint64_t seed, const float *diag_f, float downscale, const uint16_t *deck, float *a,
-	int64_t lda, int r0, int r1, int c0, int c1)
+static void lazy_init(int n, uint64_t seed, const float *diag_f, float downscale, const uint16_t *deck,
+	const uint16_t *back, float *a, int64_t lda, int r0, int r1, int c0, int c1)
 {
 	uint64_t ia, ic;
 	orc_coeff_pow(1, &ia, &ic);
@@ -81,7 +93,9 @@ static void lazy_init(int n, uint64_t seed, const float *diag_f, float downscale
 		for (int i = r0; i < r1; i++) {
 			const float aij = i == j ? diag_f[i] : lcg_float(s);
 			const int64_t o = (int64_t)j * lda + i;
-			a[o] = fmaf(downscale, from_f16(deck[o]), aij);
+			/* with the back buffer: deck + 32 back in FP32 (exact scaling, one rounding) */
+			const float x = back ? fmaf(32.0f, from_f16(back[o]), from_f16(deck[o])) : from_f16(deck[o]);
+			a[o] = fmaf(downscale, x, aij);
 			s = ia * s + ic;
 		}
 	}
@@ -115,15 +129,34 @@ static void hgemm_deck(int m, int n, int k, const uint16_t *l, int64_t ldl, cons
 	}
 }
 
+/* bb_writeback_b_impl_fp16 over rows and columns [r0, n) */
+static void back_buffer_writeback(int n, int r0, uint16_t *deck, uint16_t *back, int64_t ld)
+{
+	#pragma omp parallel for schedule(static)
+	for (int j = r0; j < n; j++)
+		for (int i = r0; i < n; i++) {
+			const int64_t o = (int64_t)j * ld + i;
+			const float x = from_f16(back[o]);
+			const float p = from_f16(to_f16(from_f16(deck[o]) * (1.0f / 32.0f)));
+			const float t2 = from_f16(to_f16(x + p));
+			const float t3 = from_f16(to_f16(t2 - x));
+			const float t4 = from_f16(to_f16(p - t3));
+			back[o] = to_f16(t2);
+			deck[o] = to_f16(t4 * 32.0f);
+		}
+}
+
 /* The first kend block steps of RDMAPanelLU::run<Matgen, 1, true, false>
  * (panel_trf.hpp:703-856) collapsed onto one process.  On return `a` holds
  * the FP32 factors of the factored blocks (unit L below the diagonal, U on
  * and above) and, when kend < n/b, the not-yet-factored blocks hold zero
  * (their value lives in the deck, returned in `deck_out` if not NULL, n x n
  * FP16 with leading dimension lda).  diag_f is the FP32 diagonal (pdiaggen,
- * then FHigh).  Returns 0, or -1 on bad sizes, -2 on allocation failure. */
+ * then FHigh).  back_buffer: the `--back_buffer` form (RDMAPanelLU::run
+ * <Matgen, 2, true, false>).  Returns 0, or -1 on bad sizes, -2 on
+ * allocation failure. */
 ORC_EXPORT int orc_lu_deck_steps(int n, int b, uint64_t seed, const float *diag_f, float *a, int64_t lda, int kend,
-	uint16_t *deck_out)
+	uint16_t *deck_out, int back_buffer)
 {
 	if (n <= 0 || b <= 0 || n % b || lda < n) return -1;
 	int nb = n / b;
@@ -131,9 +164,11 @@ ORC_EXPORT int orc_lu_deck_steps(int n, int b, uint64_t seed, const float *diag_
 	float scalea, downscale;
 	orc_deck_scales(n, &scalea, &downscale);
 	uint16_t *deck = (uint16_t *)calloc((size_t)lda * n, sizeof(uint16_t));
+	uint16_t *back = back_buffer ? (uint16_t *)calloc((size_t)lda * n, sizeof(uint16_t)) : NULL;
 	uint16_t *lh = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)n * b);
 	uint16_t *uh = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)n * b);
-	if (!deck || !lh || !uh) {
+	if (!deck || !lh || !uh || (back_buffer && !back)) {
+		free(back);
 		free(deck);
 		free(lh);
 		free(uh);
@@ -143,24 +178,28 @@ ORC_EXPORT int orc_lu_deck_steps(int n, int b, uint64_t seed, const float *diag_
 	for (int k = 0; k < nb; k++) {
 		const int kb = k * b;
 		float *lu = a + (int64_t)kb * lda + kb;
-		lazy_init(n, seed, diag_f, downscale, deck, a, lda, kb, kb + b, kb, kb + b);
+		lazy_init(n, seed, diag_f, downscale, deck, back, a, lda, kb, kb + b, kb, kb + b);
 		orc_getrf_nopiv(b, lu, lda);
 		if (kb + b == n) break;
 		const int rem = n - kb - b;
 		/* column panel: lazy init, TRSM, down-cast with scalea */
-		lazy_init(n, seed, diag_f, downscale, deck, a, lda, kb + b, n, kb, kb + b);
+		lazy_init(n, seed, diag_f, downscale, deck, back, a, lda, kb + b, n, kb, kb + b);
 		orc_trsm_right_upper(rem, b, lu, lda, lu + b, lda);
 		for (int j = 0; j < b; j++)
 			for (int i = 0; i < rem; i++) lh[(size_t)j * rem + i] = to_f16(scalea * lu[b + (int64_t)j * lda + i]);
 		/* row panel: lazy init, TRSM, down-cast with scaleb = 1 */
-		lazy_init(n, seed, diag_f, downscale, deck, a, lda, kb, kb + b, kb + b, n);
+		lazy_init(n, seed, diag_f, downscale, deck, back, a, lda, kb, kb + b, kb + b, n);
 		orc_trsm_left_lower_unit(b, rem, lu, lda, lu + (int64_t)b * lda, lda);
 		for (int j = 0; j < rem; j++)
 			for (int i = 0; i < b; i++) uh[(size_t)j * b + i] = to_f16(1.0f * lu[(int64_t)(b + j) * lda + i]);
 		if (k == kend - 1 && kend < n / b) break;   /* warm-up: the last panel's update is not applied */
+		/* BackBuffer::write_back at the end of the reference's iteration k,
+		 * before panel k's update (applied in its iteration k+1) */
+		if (back && k >= 1 && (k - 1) % 32 == 31) back_buffer_writeback(n, kb + b, deck, back, lda);
 		hgemm_deck(rem, rem, b, lh, rem, uh, b, deck + (int64_t)(kb + b) * lda + kb + b, lda);
 	}
 	if (deck_out) memcpy(deck_out, deck, sizeof(uint16_t) * (size_t)lda * n);
+	free(back);
 	free(deck);
 	free(lh);
 	free(uh);
@@ -169,5 +208,5 @@ ORC_EXPORT int orc_lu_deck_steps(int n, int b, uint64_t seed, const float *diag_
 
 ORC_EXPORT int orc_lu_deck(int n, int b, uint64_t seed, const float *diag_f, float *a, int64_t lda)
 {
-	return orc_lu_deck_steps(n, b, seed, diag_f, a, lda, n / (b > 0 ? b : 1), NULL);
+	return orc_lu_deck_steps(n, b, seed, diag_f, a, lda, n / (b > 0 ? b : 1), NULL, 0);
 }

@@ -53,7 +53,7 @@ _shgemm = _proto("orc_shgemm_minus", None, _int, _int, _int, _vp, _i64, _vp, _i6
 _lu = _proto("orc_lu", _int, _int, _int, _vp, _i64)
 _lu_steps = _proto("orc_lu_steps", _int, _int, _int, _vp, _i64, _int)
 _l1est = _proto("orc_l1est", None, _int, _vp, _i64, _vp)
-_lu_deck_steps = _proto("orc_lu_deck_steps", _int, _int, _int, _u64, _vp, _vp, _i64, _int, _vp)
+_lu_deck_steps = _proto("orc_lu_deck_steps", _int, _int, _int, _u64, _vp, _vp, _i64, _int, _vp, _int)
 _higham_beta = _proto("orc_higham_beta", _dbl, _int, _dbl, _dbl)
 _higham_fill = _proto("orc_higham_fill", None, _int, _int, _int, _int, _dbl, _dbl, _vp, _i64)
 _higham_elem = _proto("orc_higham_elem", _dbl, _i64, _i64, _dbl, _dbl)
@@ -165,16 +165,17 @@ def lu_steps(a: np.ndarray, b: int, kend: int) -> np.ndarray:
     return a
 
 
-def lu_deck(n: int, b: int, seed: int = 42, kend: int = None, with_deck: bool = False):
+def lu_deck(n: int, b: int, seed: int = 42, kend: int = None, with_deck: bool = False, back_buffer: bool = False):
     """The reference's lazy-initialised double-decker LU (`-d`): A never
     stored, trailing updates into an FP16 deck by the FP16-accumulating
     hgemm_opt, blocks formed as fma(downscale, deck, a_ij) when they join a
-    panel.  Returns the FP32 factors (and the final deck, n x n FP16 bits)."""
+    panel; back_buffer: the `--back_buffer` form.  Returns the FP32 factors
+    (and the final deck, n x n FP16 bits)."""
     a = np.zeros((n, n), dtype=np.float32, order="F")
     dk = np.zeros((n, n), dtype=np.uint16, order="F") if with_deck else None
     df = np.ascontiguousarray(diag(n, seed).astype(np.float32))
     rc = _lu_deck_steps(n, b, seed, _p(df), _p(a), n, n // b if kend is None else kend,
-                        _p(dk) if with_deck else None)
+                        _p(dk) if with_deck else None, 1 if back_buffer else 0)
     if rc:
         raise ValueError(f"orc_lu_deck_steps: {rc}")
     return (a, dk) if with_deck else a

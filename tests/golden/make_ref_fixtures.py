@@ -21,6 +21,9 @@ refinement step).  The `-d` runs also record the factors' digest: with lazy
 initialisation the LU runs through the FP16-accumulating Schur update
 (hgemm_opt), which the oracle restates in oracle/hplai_oracle_deck.c; one more
 `-d` run at n = 2400, b = 120 covers its k-chunks of 100 (two per panel).
+Two `--back_buffer` runs (n = 2400 and 4800, b = 60: one and two write-backs
+of the deck into the back buffer, at steps 32 and 64) record the factors'
+digest of that form too.
 
 Higham's matrix (`--highammat`): the alpha and beta that the reference's
 higham_mat_comp_beta returns for a list of orders (oracle/_ref/libref_higham.so,
@@ -111,6 +114,10 @@ def main():
         "netlib_warmup": run("ref_driver_netlib.out", ["-not", "-r", "-w"], True),
         "netlib_not_d_r": run("ref_driver_netlib.out", ["-not", "-d", "-r"], True),
         "netlib_not_d_r_2400": run("ref_driver_netlib.out", ["-not", "-d", "-r"], True, n=2400, b=120, keep_x=False),
+        "netlib_not_r_bb_2400": run("ref_driver_netlib.out", ["-not", "-r", "--back_buffer"], True, n=2400, b=60,
+                                    keep_x=False),
+        "netlib_not_r_bb_4800": run("ref_driver_netlib.out", ["-not", "-r", "--back_buffer"], True, n=4800, b=60,
+                                    keep_x=False),
         "openblas_not_r": run("ref_driver.out", ["-not", "-r"], False),
         "openblas_not_d_r": run("ref_driver.out", ["-not", "-d", "-r"], False),
     }

@@ -62,13 +62,22 @@ def test_oracle_warmup_lu_is_the_references_bit_for_bit(oracle):
     assert digest(lu) == FIX["runs"]["netlib_warmup"]["lu_sha256"]
 
 
-@pytest.mark.parametrize("run", ["netlib_not_d_r", "netlib_not_d_r_2400"])
+DECK_RUNS = {"netlib_not_d_r": (N, B, False), "netlib_not_d_r_2400": (2400, 120, False),
+             "netlib_not_r_bb_2400": (2400, 60, True), "netlib_not_r_bb_4800": (4800, 60, True)}
+
+
+def _deck_command(n, b, bb):
+    return f"driver.out {n} {b} 2 " + ("-not -r --back_buffer" if bb else "-not -d -r")
+
+
+@pytest.mark.parametrize("run", ["netlib_not_d_r", "netlib_not_d_r_2400", "netlib_not_r_bb_2400"])
 def test_oracle_deck_lu_is_the_references_bit_for_bit(oracle, run):
     """-d: lazy init + FP16 deck + hgemm_opt numerics (lazy_init.hpp:92-227,
-    kernels/avx2.cpp:82-189)."""
-    n, b = (N, B) if run == "netlib_not_d_r" else (2400, 120)
-    assert FIX["runs"][run]["command"] == f"driver.out {n} {b} 2 -not -d -r"
-    assert digest(oracle.lu_deck(n, b)) == FIX["runs"][run]["lu_sha256"]
+    kernels/avx2.cpp:82-189); --back_buffer: the deck written back every 32
+    steps (back_buffer.hpp:81-170) -- one write-back at n = 2400, b = 60."""
+    n, b, bb = DECK_RUNS[run]
+    assert FIX["runs"][run]["command"] == _deck_command(n, b, bb)
+    assert digest(oracle.lu_deck(n, b, back_buffer=bb)) == FIX["runs"][run]["lu_sha256"]
 
 
 def test_oracle_deck_refinement_vs_reference(oracle):
@@ -176,13 +185,17 @@ def test_gpu_warmup_factor_steps(hplai, oracle, torch_cuda):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("run", ["netlib_not_d_r", "netlib_not_d_r_2400"])
+@pytest.mark.parametrize("run", sorted(DECK_RUNS))
 def test_gpu_ref_deck_lu_is_the_references_bit_for_bit(hplai, torch_cuda, run):
     """HPLAI_FLAG_REF_DECK: A regenerated at panel time, the FP16-accumulating
     deck update on CUDA cores -- the reference's `-d` factors bit for bit
-    (C1 and n = 2400, b = 120: two k-chunks of 100 per panel)."""
-    n, b = (N, B) if run == "netlib_not_d_r" else (2400, 120)
-    with hplai.Solver(n, b, flags=hplai.FLAG_REF_DECK) as s:
+    (C1 and n = 2400, b = 120: two k-chunks of 100 per panel); with
+    HPLAI_FLAG_REF_BACKBUF its `--back_buffer` factors (one and two
+    write-backs at n = 2400 and 4800, b = 60)."""
+    n, b, bb = DECK_RUNS[run]
+    assert FIX["runs"][run]["command"] == _deck_command(n, b, bb)
+    flags = hplai.FLAG_REF_DECK | (hplai.FLAG_REF_BACKBUF if bb else 0)
+    with hplai.Solver(n, b, flags=flags) as s:
         s.generate(42)
         s.factor()
         assert digest(s.lu()) == FIX["runs"][run]["lu_sha256"]
@@ -219,6 +232,6 @@ def test_gpu_ref_deck_matches_oracle_beyond_c1(hplai, oracle, torch_cuda):
 
 def test_ref_deck_flag_combinations(hplai):
     for flags, prec in [(hplai.FLAG_REF_DECK | hplai.FLAG_FP16_DECK, 0), (hplai.FLAG_REF_DECK | hplai.FLAG_LOOKAHEAD, 0),
-                        (hplai.FLAG_REF_DECK, 1)]:
+                        (hplai.FLAG_REF_DECK, 1), (hplai.FLAG_REF_BACKBUF, 0)]:
         with pytest.raises(hplai.HplaiError):
             hplai.Solver(1200, 60, precision=prec, flags=flags)
