@@ -378,10 +378,10 @@ class FormRun:
                 return sd if sd > 0 else f"share sms*c/(r+c), c={-sd} panels, r = trailing block columns"
             trials = [{"panels_per_update": 2 if (f & hplai.FLAG_GROUP2) else 1,
                        "lookahead": bool(f & hplai.FLAG_LOOKAHEAD), "side_sms": side_desc(f, sd),
-                       "factor_ms": round(ms, 2)} for f, sd, ms in self.s.autotune_log()]
-            self.tuned = {"factor_ms_median": tms, "trials_warmup_first": trials}
+                       "tile_group": tg, "factor_ms": round(ms, 2)} for f, sd, tg, ms in self.s.autotune_trials()]
+            self.tuned = {"factor_ms": tms, "trials_warmup_first": trials}
             self.schedule = {"lookahead": la, "side_sms": side_desc(tflags, tside), "panels_per_update": self.group,
-                             "source": "hplai_autotune"}
+                             "tile_group": self.s.tile_group(), "source": "hplai_autotune"}
         self.results = []
 
     def step(self, timed):

@@ -126,7 +126,9 @@ struct hplai_ctx {
 		unsigned flags;
 		int side_sms;
 		double ms;
+		int tile_group;
 	};
+	int tile_group = 0;   // tile rows per group of the Schur kernel's tile order (0: its default)
 	std::vector<Trial> tune_log;
 	// GMRES correction: restart length, relative tolerance on the
 	// preconditioned residual, basis and scratch (allocated on first use)
@@ -1154,6 +1156,38 @@ int hplai_ctx_solve_stream_rhs(hplai_ctx *c, int col, double *x, int maxit, hpla
 // discarded warm-up factorisation; the two fastest are timed twice more and
 // the one with the lowest median becomes the context's schedule.  Every
 // trial is kept for hplai_get_autotune_log.
+namespace {
+
+// The tile order of every Schur launch of the context (trailing updates and
+// panel products): groups of `gm` tile rows (0: the kernel's default).
+void apply_tile_group(hplai_ctx *c, int gm)
+{
+	c->tile_group = gm;
+	for (int i = 0; i < 2; ++i) {
+		for (auto &m : c->maps[i]) m.group_m = gm;
+		c->mapsg[i].group_m = gm;
+		c->maps8[i].group_m = gm;
+		c->maps8g[i].group_m = gm;
+	}
+	c->maps8s.group_m = gm;
+}
+
+} // namespace
+
+extern "C" int hplai_set_tile_group(hplai_ctx *c, int group_m)
+{
+	if (!c || group_m < 0 || group_m > 1024) return HPLAI_EINVAL;
+	apply_tile_group(c, group_m);
+	return HPLAI_OK;
+}
+
+extern "C" int hplai_get_tile_group(hplai_ctx *c, int *group_m)
+{
+	if (!c || !group_m) return HPLAI_EINVAL;
+	*group_m = c->tile_group > 0 ? c->tile_group : 32;
+	return HPLAI_OK;
+}
+
 extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, int *side_sms_out, double *ms_out)
 {
 	if (!c) return HPLAI_EINVAL;
@@ -1167,6 +1201,7 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 		unsigned sched;   // HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2 bits
 		int side;
 		std::vector<double> ms;
+		int tg = 0;       // tile group (0: the kernel's default)
 	};
 	std::vector<Cand> cands;
 	for (int g = 1; g <= c->gcap; ++g) {
@@ -1177,6 +1212,7 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 		// side-stream share growing as the trailing matrix shrinks
 		for (int share : {8, 16, 24}) cands.push_back({gf | HPLAI_FLAG_LOOKAHEAD, -share, {}});
 	}
+	const int tg0 = c->tile_group;
 	const unsigned sched_bits = HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2;
 	const unsigned flags0 = c->flags, base_flags = c->flags & ~sched_bits;
 	const int side0 = c->side_sms;
@@ -1187,6 +1223,7 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 	auto trial = [&](const Cand &t, double *ms) -> int {
 		c->flags = base_flags | t.sched;
 		c->side_sms = t.side;
+		apply_tile_group(c, t.tg);
 		HPLAI_TRY(hplai_generate(c, seed));
 		HPLAI_CUDA_TRY(cudaEventRecord(e0, c->st));
 		HPLAI_TRY(hplai_factor(c));
@@ -1195,7 +1232,7 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 		float f = 0.f;
 		HPLAI_CUDA_TRY(cudaEventElapsedTime(&f, e0, e1));
 		*ms = f;
-		c->tune_log.push_back({c->flags, t.side, f});
+		c->tune_log.push_back({c->flags, t.side, f, t.tg > 0 ? t.tg : 32});
 		return HPLAI_OK;
 	};
 	auto median = [](std::vector<double> v) {
@@ -1221,16 +1258,9 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 				cands[order[r]].ms.push_back(ms);
 			}
 	}
-	cudaEventDestroy(e0);
-	cudaEventDestroy(e1);
-	if (rc != HPLAI_OK) {
-		c->flags = flags0;
-		c->side_sms = side0;
-		return rc;
-	}
 	size_t pick = 0;
 	double best = -1.0;
-	for (size_t i = 0; i < cands.size(); ++i) {
+	for (size_t i = 0; rc == HPLAI_OK && i < cands.size(); ++i) {
 		if (cands[i].ms.size() < 3) continue;   // only the re-timed finalists
 		const double m = median(cands[i].ms);
 		if (best < 0.0 || m < best) {
@@ -1238,8 +1268,33 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 			pick = i;
 		}
 	}
+	// then the tile order of the chosen schedule: groups of 16 or 64 tile rows
+	// instead of 32, kept only when both of their trials beat the schedule's
+	// median by half a percent
+	int tg_pick = 0;
+	for (int tg : {16, 64}) {
+		if (rc != HPLAI_OK) break;
+		Cand t = cands[pick];
+		t.tg = tg;
+		double a = 0.0, b2 = 0.0;
+		rc = trial(t, &a);
+		if (rc == HPLAI_OK) rc = trial(t, &b2);
+		if (rc == HPLAI_OK && std::max(a, b2) < 0.995 * best) {
+			best = std::max(a, b2);
+			tg_pick = tg;
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	if (rc != HPLAI_OK) {
+		c->flags = flags0;
+		c->side_sms = side0;
+		apply_tile_group(c, tg0);
+		return rc;
+	}
 	c->flags = base_flags | cands[pick].sched;
 	c->side_sms = cands[pick].side;
+	apply_tile_group(c, tg_pick);
 	// the context is left generated and unfactored, as after hplai_generate
 	HPLAI_TRY(hplai_generate(c, seed));
 	if (flags_out) *flags_out = c->flags;
@@ -1256,6 +1311,20 @@ extern "C" int hplai_set_schedule(hplai_ctx *c, unsigned flags, int side_sms)
 	if ((c->flags & HPLAI_FLAG_REF_DECK) && flags) return HPLAI_EINVAL;
 	c->flags = (c->flags & ~sched) | flags;
 	c->side_sms = side_sms;
+	return HPLAI_OK;
+}
+
+extern "C" int hplai_get_autotune_trials(hplai_ctx *c, unsigned *flags, int *side_sms, int *tile_group, double *ms,
+	int cap, int *count)
+{
+	if (!c || !count || cap < 0) return HPLAI_EINVAL;
+	*count = static_cast<int>(c->tune_log.size());
+	for (int i = 0; i < cap && i < *count; ++i) {
+		if (flags) flags[i] = c->tune_log[i].flags;
+		if (side_sms) side_sms[i] = c->tune_log[i].side_sms;
+		if (tile_group) tile_group[i] = c->tune_log[i].tile_group;
+		if (ms) ms[i] = c->tune_log[i].ms;
+	}
 	return HPLAI_OK;
 }
 

@@ -75,6 +75,9 @@ struct SchurMaps {
 	// dimension in halves
 	void *deck_base = nullptr;
 	int64_t deck_ld = 0;
+	// tile rows per group of the persistent kernel's tile order (0: the
+	// default, 32); hplai_set_tile_group / hplai_autotune set it
+	int group_m = 0;
 };
 // L: lrows x k FP16, row-major with ldl; U: urows x k FP16 (row j = column j
 // of U), ldu.  Rows beyond lrows/urows read as zero.

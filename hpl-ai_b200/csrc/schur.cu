@@ -137,23 +137,25 @@ struct Params {
 	// region's tile grid -- the tiles of many systems' updates in one launch.
 	const int4 *tiles;
 	int ntiles;
+	int group_m;        // tile rows per group of the tile order (tile_coords)
 };
 
 __device__ unsigned int g_status;
 
-// Tile order: groups of kGroupM tile rows, each group swept column by column
-// (tile rows fastest).  The CTAs in flight then share a few U blocks and the
-// group's L blocks stay in L2 while the group crosses all tile columns, so
-// each panel is read from HBM about once per group instead of once per tile
-// column (the L panel alone is 256 MB at n = 131072, b = 1024).
+// Tile order: groups of group_m tile rows (kGroupM unless the context's
+// tuner chose another), each group swept column by column (tile rows
+// fastest).  The CTAs in flight then share a few U blocks and the group's L
+// blocks stay in L2 while the group crosses all tile columns, so each panel
+// is read from HBM about once per group instead of once per tile column (the
+// L panel alone is 256 MB at n = 131072, b = 1024).
 constexpr int kGroupM = 32;
 
-__device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, int &tm, int &tn)
+__device__ __forceinline__ void tile_coords(int tile, int tiles_m, int tiles_n, int group_m, int &tm, int &tn)
 {
-	const int per_group = kGroupM * tiles_n;
+	const int per_group = group_m * tiles_n;
 	const int g = tile / per_group;
-	const int first = g * kGroupM;
-	const int gm = min(kGroupM, tiles_m - first);
+	const int first = g * group_m;
+	const int gm = min(group_m, tiles_m - first);
 	const int in = tile - g * per_group;
 	tm = first + in % gm;
 	tn = in / gm;
@@ -280,7 +282,7 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 				urow = t.y;
 			} else {
 				int tm, tn;
-				tile_coords(tile, p.tiles_m, p.tiles_n, tm, tn);
+				tile_coords(tile, p.tiles_m, p.tiles_n, p.group_m, tm, tn);
 				lrow = p.lrow0 + tm * BM;
 				urow = p.urow0 + tn * BN;
 			}
@@ -356,7 +358,7 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 		const int nseq = my_tiles * CPT;
 		auto chunk_xy = [&](int sidx, int &x, int &y) {
 			int tm, tn;
-			tile_coords(blockIdx.x + (sidx / CPT) * gridDim.x, p.tiles_m, p.tiles_n, tm, tn);
+			tile_coords(blockIdx.x + (sidx / CPT) * gridDim.x, p.tiles_m, p.tiles_n, p.group_m, tm, tn);
 			x = p.crow0 + tm * BM;
 			y = p.ccol0 + tn * BN + (sidx % CPT) * DECK_CH;
 		};
@@ -375,7 +377,7 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 		int sidx = 0;
 		for (int it = 0; it < my_tiles && ok; ++it) {
 			int tm, tn;
-			tile_coords(blockIdx.x + it * gridDim.x, p.tiles_m, p.tiles_n, tm, tn);
+			tile_coords(blockIdx.x + it * gridDim.x, p.tiles_m, p.tiles_n, p.group_m, tm, tn);
 			ok = epi_all<NW>(mbar_wait(&accf[acc], acc_phase));
 			if (!ok) break;
 			tc_fence_after();
@@ -461,7 +463,7 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 				crow = t.z;
 				ccol = t.w;
 			} else {
-				tile_coords(tile, p.tiles_m, p.tiles_n, tm, tn);
+				tile_coords(tile, p.tiles_m, p.tiles_n, p.group_m, tm, tn);
 				crow = p.crow0 + tm * BM;
 				ccol = p.ccol0 + tn * BN;
 			}
@@ -719,6 +721,7 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 	p.oscale = oscale;
 	p.tiles = nullptr;
 	p.ntiles = 0;
+	p.group_m = maps.group_m > 0 ? maps.group_m : kGroupM;
 	p.status = maps.status;
 	if (!p.status) {
 		void *g = nullptr;
@@ -822,6 +825,7 @@ int launch_schur_tiles(const SchurMaps &maps, const int4 *tiles, int ntiles, int
 	p.num_kc = (maps.k + BK - 1) / BK;
 	p.tiles = tiles;
 	p.ntiles = ntiles;
+	p.group_m = kGroupM;
 	p.dscale = 0.f;
 	p.status = maps.status;
 	if (!p.status) {

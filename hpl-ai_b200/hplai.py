@@ -70,6 +70,10 @@ _l1est = _proto("hplai_l1est", _c_int, _vp)
 _autotune = _proto("hplai_autotune", _c_int, _vp, _c_u64, _vp, _vp, _vp)
 _set_schedule = _proto("hplai_set_schedule", _c_int, _vp, ctypes.c_uint, _c_int)
 _autotune_log = _proto("hplai_get_autotune_log", _c_int, _vp, _vp, _vp, _vp, _c_int, ctypes.POINTER(_c_int))
+_autotune_trials = _proto("hplai_get_autotune_trials", _c_int, _vp, _vp, _vp, _vp, _vp, _c_int,
+                          ctypes.POINTER(_c_int))
+_set_tile_group = _proto("hplai_set_tile_group", _c_int, _vp, _c_int)
+_get_tile_group = _proto("hplai_get_tile_group", _c_int, _vp, ctypes.POINTER(_c_int))
 _refine = _proto("hplai_refine", _c_int, _vp, _c_int, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
 _get_x = _proto("hplai_get_x", _c_int, _vp, _vp)
 _get_lu = _proto("hplai_get_lu", _c_int, _vp, _vp, _c_i64)
@@ -251,6 +255,25 @@ class Solver:
         cnt = _c_int()
         check(_autotune_log(self._h, fl, sd, ms, cap, ctypes.byref(cnt)), "hplai_get_autotune_log")
         return [(fl[i], sd[i], ms[i]) for i in range(min(cnt.value, cap))]
+
+    def autotune_trials(self):
+        """The last autotune's trials: [(flags, side_sms, tile_group, ms)], warm-up first."""
+        cap = 64
+        fl = (ctypes.c_uint * cap)()
+        sd = (_c_int * cap)()
+        tg = (_c_int * cap)()
+        ms = (ctypes.c_double * cap)()
+        cnt = _c_int()
+        check(_autotune_trials(self._h, fl, sd, tg, ms, cap, ctypes.byref(cnt)), "hplai_get_autotune_trials")
+        return [(fl[i], sd[i], tg[i], ms[i]) for i in range(min(cnt.value, cap))]
+
+    def set_tile_group(self, group_m: int):
+        check(_set_tile_group(self._h, group_m), "hplai_set_tile_group")
+
+    def tile_group(self) -> int:
+        g = _c_int()
+        check(_get_tile_group(self._h, ctypes.byref(g)), "hplai_get_tile_group")
+        return g.value
 
     def iterative_refinement(self, maxit: int = 50, mode: int = IR) -> RefineResult:
         e = IRErrors()

@@ -214,9 +214,12 @@ int hplai_l1est(hplai_ctx *ctx);
  * side_sms, see hplai_set_schedule) -- after one discarded warm-up
  * factorisation, re-times the two
  * fastest twice more, keeps the one with the lowest median as the context's
- * schedule, and leaves the context generated and unfactored.  Outputs (may
- * be NULL): the chosen flags, the side-stream SM count and the chosen
- * schedule's median factorisation time in ms. */
+ * schedule, then times that schedule twice under each of two other tile
+ * orders of the Schur kernel (groups of 16 and 64 tile rows instead of 32,
+ * hplai_set_tile_group) and keeps one only if both of its trials beat the
+ * median by 0.5 %; leaves the context generated and unfactored.  Outputs
+ * (may be NULL): the chosen flags, the side-stream SM count and the chosen
+ * configuration's factorisation time in ms. */
 int hplai_autotune(hplai_ctx *ctx, uint64_t seed, unsigned *flags, int *side_sms, double *ms);
 /* Sets the schedule by hand, as hplai_autotune would: `flags` a combination
  * of HPLAI_FLAG_LOOKAHEAD and HPLAI_FLAG_GROUP2 (the other flags of the
@@ -233,6 +236,15 @@ int hplai_set_schedule(hplai_ctx *ctx, unsigned flags, int side_sms);
  * the number of trials (at most cap are written).  No counterpart in the
  * reference (lda_tuner prints its choice only). */
 int hplai_get_autotune_log(hplai_ctx *ctx, unsigned *flags, int *side_sms, double *ms, int cap, int *count);
+/* The same trials with the tile group each ran with (any output may be NULL). */
+int hplai_get_autotune_trials(hplai_ctx *ctx, unsigned *flags, int *side_sms, int *tile_group, double *ms, int cap,
+	int *count);
+/* Tile order of the context's Schur launches: the persistent kernel sweeps
+ * its tiles in groups of group_m tile rows (1 .. 1024; 0 restores the
+ * default, 32), each group column by column, so that a group's L rows stay
+ * in L2 while it crosses the trailing matrix.  Results do not depend on it. */
+int hplai_set_tile_group(hplai_ctx *ctx, int group_m);
+int hplai_get_tile_group(hplai_ctx *ctx, int *group_m);
 
 /* iterative_refinement (iterative_refinement.hpp:18-57) with maxit steps
  * (the driver uses 50).  Fills *err ({-1,-1} on failure) and *iters (the

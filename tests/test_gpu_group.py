@@ -86,3 +86,32 @@ def test_autotune_considers_groups(hplai, oracle, torch_cuda):
     assert res.status == hplai.HPLAI_OK and res.hpl_harness < 16.0
     xs = _dense_x(oracle, n)
     assert np.max(np.abs(x - xs)) / np.max(np.abs(xs)) < 1e-12
+
+
+@pytest.mark.parametrize("precision,flags", [(0, 0), (0, 8), (1, 4 | 8)])
+def test_tile_group_does_not_change_results(hplai, torch_cuda, precision, flags):
+    """The tile order only decides which CTA computes which tile when: every
+    C element still receives each update once, so the factors are
+    bit-identical under any tile group."""
+    n, b = 4096, 512
+    out = []
+    for gm in (0, 1, 16, 64, 1024):
+        with hplai.Solver(n, b, precision=precision, flags=flags) as s:
+            s.set_tile_group(gm)
+            assert s.tile_group() == (gm if gm else 32)
+            s.generate(42)
+            s.factor()
+            out.append(s.lu().view(np.uint32))
+    for o in out[1:]:
+        assert np.array_equal(out[0], o)
+
+
+def test_autotune_trials_cover_tile_groups(hplai, torch_cuda):
+    with hplai.Solver(4096, 512) as s:
+        s.autotune(42)
+        trials = s.autotune_trials()
+        assert {tg for _, _, tg, _ in trials} >= {16, 32, 64}
+        assert len(trials) == len(s.autotune_log())
+        assert s.tile_group() in (16, 32, 64)
+        with pytest.raises(hplai.HplaiError):
+            s.set_tile_group(-1)
