@@ -134,17 +134,19 @@ __global__ void rhs_kernel(int n, int col0, int ncols, double *out, uint64_t see
 __global__ void __launch_bounds__(256) l1est_kernel(int n, float *__restrict__ a, int64_t lda,
 	const double *__restrict__ d)
 {
-	const int j = blockIdx.y;
-	const float inv = static_cast<float>(1.0 / d[j]);
-	float *col = a + static_cast<int64_t>(j) * lda;
-	for (int i = j + 1 + blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) col[i] *= inv;
+	for (int j = blockIdx.y; j < n; j += gridDim.y) {
+		const float inv = static_cast<float>(1.0 / d[j]);
+		float *col = a + static_cast<int64_t>(j) * lda;
+		for (int i = j + 1 + blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) col[i] *= inv;
+	}
 }
 
 int launch_l1est(int n, float *a, int64_t lda, const double *d, cudaStream_t st)
 {
 	if (n <= 1) return HPLAI_OK;
-	l1est_kernel<<<dim3(static_cast<unsigned>((n + 255) / 256 < 8 ? (n + 255) / 256 : 8), static_cast<unsigned>(n)), 256, 0,
-		st>>>(n, a, lda, d);
+	// grid.y is limited to 65535: columns beyond it are taken in a grid stride
+	l1est_kernel<<<dim3(static_cast<unsigned>((n + 255) / 256 < 8 ? (n + 255) / 256 : 8),
+		static_cast<unsigned>(n < 65535 ? n : 65535)), 256, 0, st>>>(n, a, lda, d);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;

@@ -260,9 +260,16 @@ __global__ void __launch_bounds__(TB) trsv_dinv_kernel(int n, const float *__res
 // else 4-byte copies.  The matrix is read-only for the whole solve.
 template <bool TRANS>
 __device__ __forceinline__ void stage_block(float *blk, const float *a, int64_t lda, int r0, int c0, int rows,
-	int cols, bool vec)
+	int cols, bool vec, const double *xsrc = nullptr, double *xdst = nullptr)
 {
 	const int t = threadIdx.x;
+	// x of the block column in the same copy group (its values are published)
+	if (xsrc && t < TB / 2) {
+		int bytes = (cols - 2 * t) * 8;
+		bytes = bytes < 0 ? 0 : (bytes > 16 ? 16 : bytes);
+		asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(xdst + 2 * t)),
+			"l"(xsrc + (bytes ? 2 * t : 0)), "r"(bytes) : "memory");
+	}
 	// contiguous index of the stored matrix: rows for M = stored, columns for M^T
 	const int ncont = TRANS ? cols : rows, nline = TRANS ? rows : cols;
 	if (vec) {
@@ -305,9 +312,15 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) trsv_kernel(int lower, int n,
 	float (*dblk)[TB + 1] = reinterpret_cast<float (*)[TB + 1]>(dyn_smem);   // dblk[i][j] = M[r0+i][r0+j]
 	float *bufs = dyn_smem + TB * (TB + 1) + 3;   // two TB x TB blocks, 16-byte aligned
 	bufs = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(bufs) + 15) & ~static_cast<uintptr_t>(15));
+	// With the diagonal inverses the staged diagonal block is not needed and
+	// its space becomes a third block buffer: two blocks in flight while one
+	// is applied.
+	const int NB = dinv ? 3 : 2;
+	float *const bufp[3] = {bufs, bufs + TB * TB, dyn_smem};
 	const bool unit = TRANS ? !lower : lower;
 	const bool vec = ((reinterpret_cast<uintptr_t>(a) & 15u) == 0) && ((lda & 3) == 0);
-	__shared__ double xs[TB];            // x of the block column being applied
+	const bool xvec = (reinterpret_cast<uintptr_t>(x) & 15u) == 0;   // x copies of 16 bytes
+	__shared__ __align__(16) double xsb[3][TB];   // x of the staged block columns, one per block buffer
 	__shared__ double part[2][TB];       // partial sums of the two column halves
 	__shared__ double rhs[TB];
 	__shared__ int ready_upto;
@@ -319,17 +332,36 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) trsv_kernel(int lower, int n,
 	const int t = threadIdx.x;
 	const int lr = t % TB, grp = t / TB;   // row within the block, column half
 
-	if (t == 0) abort_flag = 0;
+	// the published prefix seen so far: flags only advance during a launch,
+	// so it carries over from one block row of this CTA to its next
+	if (t == 0) {
+		abort_flag = 0;
+		ready_upto = lower ? 0 : nbt - 1;
+	}
+	__syncthreads();
 	for (int idx = blockIdx.x; idx < nbt; idx += gridDim.x) {
 		const int r = lower ? idx : nbt - 1 - idx;
 		const int r0 = r * TB;
 		const int rows = min(TB, n - r0);
 		const int nblk = lower ? r : nbt - 1 - r;
-		// first off-diagonal block in flight before anything waits
-		if (nblk > 0) {
-			const int cb0 = lower ? 0 : nbt - 1;
-			stage_block<TRANS>(bufs, a, lda, r0, cb0 * TB, rows, min(TB, n - cb0 * TB), vec);
-		}
+		// the first NB - 1 off-diagonal blocks in flight before anything waits;
+		// one copy group per block (empty past the last) keeps the count fixed
+		// With the block goes its x when the block column is already known to
+		// be solved (the published prefix warp 0 has seen; the same for every
+		// thread between two barriers), so that applying it waits on nothing
+		// but its copy group.
+		bool xpre[3] = {false, false, false};
+		auto stage_q = [&](int q) {
+			if (q < nblk) {
+				const int cb = lower ? q : nbt - 1 - q;
+				const bool known = xvec && (lower ? (cb < ready_upto) : (cb > ready_upto));
+				xpre[q % NB] = known;
+				stage_block<TRANS>(bufp[q % NB], a, lda, r0, cb * TB, rows, min(TB, n - cb * TB), vec,
+					known ? x + static_cast<int64_t>(cb) * TB : nullptr, xsb[q % NB]);
+			} else {
+				asm volatile("cp.async.commit_group;" ::: "memory");
+			}
+		};
 		// the diagonal block's inverse (M^{-1} = T^{-1} or its transpose) into L2
 		const double *dblock = nullptr;
 		if (dinv) {
@@ -357,23 +389,24 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) trsv_kernel(int lower, int n,
 			const int64_t off = TRANS ? static_cast<int64_t>(r0 + i) * lda + r0 + jj : static_cast<int64_t>(r0 + jj) * lda + r0 + i;
 			dblk[i][jj] = (i < rows && jj < rows) ? a[off] : 0.f;
 		}
-		if (t == 0) ready_upto = lower ? 0 : nbt - 1;
-		double acc = 0.0;
+		double acc4[4] = {0.0, 0.0, 0.0, 0.0};
 		// TRANS: warp `wv` takes rows wv, wv + 8, ...; lane takes 4 columns
 		double tacc[TB / 8];
 #pragma unroll
 		for (int q = 0; q < TB / 8; ++q) tacc[q] = 0.0;
 		__syncthreads();
-		// Off-diagonal block columns in dependency order.
+		for (int q = 0; q < NB - 1; ++q) stage_q(q);
+		// Off-diagonal block columns in dependency order: one barrier per
+		// block.  Before it, warp 0 makes sure x of the block is published and
+		// loads it, and every thread waits for its own copies of the block;
+		// after it, the buffer of the previous block (every thread is done
+		// with it) receives the block NB - 1 ahead, and the block is applied.
 		for (int q = 0; q < nblk; ++q) {
 			const int cb = lower ? q : nbt - 1 - q;
 			const int cols = min(TB, n - cb * TB);
-			float *cur = bufs + (q & 1) * TB * TB;
-			if (q + 1 < nblk) {
-				const int cn = lower ? q + 1 : nbt - 2 - q;
-				stage_block<TRANS>(bufs + ((q + 1) & 1) * TB * TB, a, lda, r0, cn * TB, rows, min(TB, n - cn * TB), vec);
-			}
-			if (t < 32) {
+			const float *cur = bufp[q % NB];
+			double *xs = xsb[q % NB];
+			if (t < 32 && !xpre[q % NB]) {
 				// Learn how far the published prefix reaches, 32 flags at a time.
 				bool have = lower ? (cb < ready_upto) : (cb > ready_upto);
 				if (!have) {
@@ -397,19 +430,21 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) trsv_kernel(int lower, int n,
 						__nanosleep(100);
 					}
 				}
+				// x of this block column, published by another CTA: bypass L1
+#pragma unroll
+				for (int k = 0; k < TB / 32; ++k) {
+					const int j = cb * TB + t + 32 * k;
+					xs[t + 32 * k] = (j < n) ? __ldcg(&x[j]) : 0.0;
+				}
 			}
-			__syncthreads();
-			if (abort_flag) break;
-			if (t < TB) {
-				const int j = cb * TB + t;
-				xs[t] = (j < n) ? __ldcg(&x[j]) : 0.0;   // published by another CTA: bypass L1
-			}
-			// block q has landed (block q+1 may still be in flight)
-			if (q + 1 < nblk)
+			// block q has landed (the NB - 2 blocks after it may still be in flight)
+			if (NB == 3)
 				asm volatile("cp.async.wait_group 1;" ::: "memory");
 			else
 				asm volatile("cp.async.wait_group 0;" ::: "memory");
 			__syncthreads();
+			if (abort_flag) break;
+			stage_q(q + NB - 1);
 			if (TRANS) {
 				const int wv = t >> 5, ln = t & 31;
 				const int j = 4 * ln;
@@ -428,11 +463,18 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) trsv_kernel(int lower, int n,
 					}
 				}
 			} else if (lr < rows) {
+				// four independent FMA chains: one chain of 64 dependent FMAs per
+				// block left the FP64 pipe waiting on its own latency
 				const int jb = grp * (TB / 2), je = min(jb + TB / 2, cols);
-#pragma unroll 8
-				for (int j = jb; j < je; ++j) acc = fma(static_cast<double>(cur[j * TB + lr]), xs[j], acc);
+				int j = jb;
+				for (; j + 3 < je; j += 4) {
+					acc4[0] = fma(static_cast<double>(cur[j * TB + lr]), xs[j], acc4[0]);
+					acc4[1] = fma(static_cast<double>(cur[(j + 1) * TB + lr]), xs[j + 1], acc4[1]);
+					acc4[2] = fma(static_cast<double>(cur[(j + 2) * TB + lr]), xs[j + 2], acc4[2]);
+					acc4[3] = fma(static_cast<double>(cur[(j + 3) * TB + lr]), xs[j + 3], acc4[3]);
+				}
+				for (; j < je; ++j) acc4[0] = fma(static_cast<double>(cur[j * TB + lr]), xs[j], acc4[0]);
 			}
-			__syncthreads();   // this buffer is refilled two blocks later
 		}
 		if (abort_flag) break;
 		if (TRANS) {
@@ -448,7 +490,7 @@ __global__ void __launch_bounds__(TRSV_THREADS, 1) trsv_kernel(int lower, int n,
 				}
 			}
 		} else {
-			part[grp][lr] = acc;
+			part[grp][lr] = (acc4[0] + acc4[1]) + (acc4[2] + acc4[3]);
 		}
 		__syncthreads();
 		if (t < TB) rhs[t] = (t < rows) ? xr - (part[0][t] + part[1][t]) : 0.0;

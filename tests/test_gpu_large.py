@@ -113,3 +113,15 @@ def test_c3_residual_vs_oracle_rows(hplai, oracle, torch_cuda, form):
         outer, inner = s.refine_counts()
         assert outer <= 5 and (mode == hplai.IR or inner <= 30)
         _check_solution(hplai, oracle, torch_cuda, s, n, rep)
+
+
+def test_l1est_beyond_the_grid_y_limit(hplai, torch_cuda):
+    """--l1est at an order above 65535 (one CTA row per column no longer
+    fits a launch's y dimension): the scaling covers every column, and the
+    refinement from those approximate factors converges."""
+    n, b = 65664, 128
+    with hplai.Solver(n, b) as s:
+        s.generate(42)
+        s.l1est()
+        res = s.iterative_refinement(50)
+        assert res.status == hplai.HPLAI_OK and res.hpl_harness < 16.0, res
