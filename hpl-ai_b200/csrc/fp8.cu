@@ -10,8 +10,9 @@
 // (exact, powers of two) before the update.
 //
 // amax_kernel: per-block max |x| (atomicMax on the float bits, which order
-// like the values for x >= 0).  cast8_kernel: x * 2^-e rounded to e4m3 (RN,
-// saturating), row-major with K contiguous, plus the factor 2^e per block.
+// like the values for x >= 0).  cast8_cols_kernel / cast8_rows_kernel: x *
+// 2^-e rounded to e4m3 (RN, saturating), row-major with K contiguous, plus
+// the factor 2^e per block.
 #include "common.cuh"
 #include "internal.h"
 
@@ -58,36 +59,70 @@ __device__ __forceinline__ int block_exponent(unsigned amax_bits)
 	return e;
 }
 
-// Tile of 32 rows x 128 k: load (coalesced along the source's contiguous
-// index), then write 4 e4m3 bytes per thread along k.
-template <bool RCONTIG>
-__global__ void __launch_bounds__(256) cast8_kernel(int rows, int kdim, const float *__restrict__ src, int64_t ld,
+// Four values times the block factor to e4m3 (RN, saturating), packed little-endian.
+__device__ __forceinline__ uint32_t pack_e4m3(float v0, float v1, float v2, float v3, float inv)
+{
+	const uint32_t lo = __nv_cvt_float2_to_fp8x2(make_float2(v0 * inv, v1 * inv), __NV_SATFINITE, __NV_E4M3);
+	const uint32_t hi = __nv_cvt_float2_to_fp8x2(make_float2(v2 * inv, v3 * inv), __NV_SATFINITE, __NV_E4M3);
+	return lo | (hi << 16);
+}
+
+// L panel (element (r, k) at src[r + k*ld]): tile of 32 rows x 128 k loaded
+// coalesced along r, then 4 e4m3 bytes per thread written along k.  The 32
+// rows lie in one 128-row block: one factor per CTA.
+__global__ void __launch_bounds__(256) cast8_cols_kernel(int rows, int kdim, const float *__restrict__ src, int64_t ld,
 	const unsigned *__restrict__ bits, uint8_t *__restrict__ dst, int64_t ld8, float *__restrict__ scale)
 {
 	__shared__ float tile[32][129];
+	__shared__ float s_inv;
 	const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 128;
+	if (threadIdx.x == 0) {
+		const int ex = block_exponent(bits[r0 >> 7]);
+		s_inv = ldexpf(1.f, -ex);
+		if ((r0 & 127) == 0 && k0 == 0) scale[r0 >> 7] = ldexpf(1.f, ex);
+	}
 	for (int e = threadIdx.x; e < 32 * 128; e += 256) {
-		const int r = RCONTIG ? (e & 31) : (e >> 7), k = RCONTIG ? (e >> 5) : (e & 127);
-		float v = 0.f;
-		if (r0 + r < rows && k0 + k < kdim)
-			v = RCONTIG ? src[static_cast<int64_t>(k0 + k) * ld + r0 + r] : src[static_cast<int64_t>(r0 + r) * ld + k0 + k];
-		tile[r][k] = v;
+		const int r = e & 31, k = e >> 5;
+		tile[r][k] = (r0 + r < rows && k0 + k < kdim) ? src[static_cast<int64_t>(k0 + k) * ld + r0 + r] : 0.f;
 	}
 	__syncthreads();
+	const float inv = s_inv;
 	for (int e = threadIdx.x; e < 32 * 32; e += 256) {
 		const int r = e >> 5, w = e & 31;
 		const int row = r0 + r;
-		if (row >= rows) continue;
-		const int ex = block_exponent(bits[row >> 7]);
+		if (row >= rows || k0 + 4 * w >= ld8) continue;
+		*reinterpret_cast<uint32_t *>(dst + static_cast<int64_t>(row) * ld8 + k0 + 4 * w) =
+			pack_e4m3(tile[r][4 * w], tile[r][4 * w + 1], tile[r][4 * w + 2], tile[r][4 * w + 3], inv);
+	}
+}
+
+// U panel (element (r, k) at src[r*ld + k]): source and copy are both
+// contiguous along k, so each thread converts four consecutive k of a row
+// with no staging (16-byte loads when src and ld allow them).
+__global__ void __launch_bounds__(256) cast8_rows_kernel(int rows, int kdim, const float *__restrict__ src, int64_t ld,
+	const unsigned *__restrict__ bits, uint8_t *__restrict__ dst, int64_t ld8, float *__restrict__ scale, int vec)
+{
+	const int k = 4 * (blockIdx.x * 256 + threadIdx.x);
+	if (k >= ld8) return;
+	for (int r = blockIdx.y; r < rows; r += gridDim.y) {
+		const int ex = block_exponent(bits[r >> 7]);
 		const float inv = ldexpf(1.f, -ex);
-		uint32_t packed = 0;
-#pragma unroll
-		for (int q = 0; q < 4; ++q) {
-			const __nv_fp8_storage_t b8 = __nv_cvt_float_to_fp8(tile[r][4 * w + q] * inv, __NV_SATFINITE, __NV_E4M3);
-			packed |= static_cast<uint32_t>(b8) << (8 * q);
+		const float *row = src + static_cast<int64_t>(r) * ld;
+		float v0, v1, v2, v3;
+		if (vec && k + 3 < kdim) {
+			const float4 q = __ldg(reinterpret_cast<const float4 *>(row + k));
+			v0 = q.x;
+			v1 = q.y;
+			v2 = q.z;
+			v3 = q.w;
+		} else {
+			v0 = (k < kdim) ? row[k] : 0.f;
+			v1 = (k + 1 < kdim) ? row[k + 1] : 0.f;
+			v2 = (k + 2 < kdim) ? row[k + 2] : 0.f;
+			v3 = (k + 3 < kdim) ? row[k + 3] : 0.f;
 		}
-		if (k0 + 4 * w < ld8) *reinterpret_cast<uint32_t *>(dst + static_cast<int64_t>(row) * ld8 + k0 + 4 * w) = packed;
-		if ((row & 127) == 0 && k0 == 0 && w == 0) scale[row >> 7] = ldexpf(1.f, ex);
+		*reinterpret_cast<uint32_t *>(dst + static_cast<int64_t>(r) * ld8 + k) = pack_e4m3(v0, v1, v2, v3, inv);
+		if ((r & 127) == 0 && k == 0) scale[r >> 7] = ldexpf(1.f, ex);
 	}
 }
 
@@ -101,8 +136,14 @@ int quantize(int rows, int kdim, const float *src, int64_t ld, unsigned *bits, u
 	amax_kernel<RCONTIG><<<dim3(nblk, (kdim + 63) / 64), 256, 0, st>>>(rows, kdim, src, ld, bits);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
-	cast8_kernel<RCONTIG><<<dim3((rows + 31) / 32, static_cast<unsigned>((ld8 + 127) / 128)), 256, 0, st>>>(rows, kdim,
-		src, ld, bits, dst, ld8, scale);
+	if (RCONTIG) {
+		cast8_cols_kernel<<<dim3((rows + 31) / 32, static_cast<unsigned>((ld8 + 127) / 128)), 256, 0, st>>>(rows, kdim,
+			src, ld, bits, dst, ld8, scale);
+	} else {
+		const int vec = ((reinterpret_cast<uintptr_t>(src) & 15u) == 0 && (ld & 3) == 0) ? 1 : 0;
+		cast8_rows_kernel<<<dim3(static_cast<unsigned>((ld8 / 4 + 255) / 256), static_cast<unsigned>(rows < 8192 ? rows : 8192)),
+			256, 0, st>>>(rows, kdim, src, ld, bits, dst, ld8, scale, vec);
+	}
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
