@@ -117,8 +117,8 @@ static int usage()
 		"   --job-id <id>           Job number in the name of the Timerdump file (default 0).\n"
 		"   --help or -h            Print this message.\n"
 		"Layout and transport flags of the distributed reference (-not, -r, -m, --pack,\n"
-		"--numa, --numa-map, --nbuf, --pwrtune)\n"
-		"are accepted and ignored.\n");
+		"--numa, --numa-map, --nbuf, --pwrtune) are accepted, echoed in the settings lines\n"
+		"and have no effect on one GPU.\n");
 	return 0;
 }
 
@@ -131,6 +131,11 @@ int main(int argc, char **argv)
 	bool checksum = false, autotune = false, warmup = false, l1est = false, higham = false;
 	int nrow = 2;
 	int jobid = 0;
+	// layout and transport settings of the distributed reference: accepted,
+	// echoed in its settings lines, without effect on one GPU
+	bool tile = true, rdma = false, pack = false;
+	int numasize = 0, nbuf = 2;
+	const char *numamap = "ROWDIST";
 	if (argc > 1) n = std::atoi(argv[1]);
 	if (argc > 2) b = std::atoi(argv[2]);
 	if (argc > 3) nrow = std::atoi(argv[3]);
@@ -154,8 +159,23 @@ int main(int argc, char **argv)
 		else if (!std::strcmp(argv[i], "--checksum")) checksum = true;
 		else if (!std::strcmp(argv[i], "-w") || !std::strcmp(argv[i], "--warmup")) warmup = true;
 		else if (!std::strcmp(argv[i], "--l1est")) l1est = true;
-		else if (!std::strcmp(argv[i], "--numa") || !std::strcmp(argv[i], "--numa-map") ||
-			!std::strcmp(argv[i], "--nbuf")) ++i;
+		else if (!std::strcmp(argv[i], "-not") || !std::strcmp(argv[i], "-nt") || !std::strcmp(argv[i], "--notile"))
+			tile = false;
+		else if (!std::strcmp(argv[i], "-r") || !std::strcmp(argv[i], "--rdma")) rdma = true;
+		else if (!std::strcmp(argv[i], "--pack")) pack = true;
+		else if (!std::strcmp(argv[i], "-m") || !std::strcmp(argv[i], "--manual-progress") ||
+			!std::strcmp(argv[i], "--pwrtune")) continue;
+		else if (!std::strcmp(argv[i], "--numa")) {
+			if (i + 1 < argc) numasize = std::atoi(argv[++i]);
+		} else if (!std::strcmp(argv[i], "--numa-map")) {
+			if (i + 1 < argc) {
+				++i;
+				for (const char *m : {"ROWCONT", "COLCONT", "ROWDIST", "COLDIST"})
+					if (!std::strcmp(argv[i], m)) numamap = m;
+			}
+		} else if (!std::strcmp(argv[i], "--nbuf")) {
+			if (i + 1 < argc) nbuf = std::atoi(argv[++i]);
+		}
 		else if (!std::strcmp(argv[i], "--job-id") && i + 1 < argc) jobid = std::atoi(argv[++i]);
 		else if (argv[i][0] == '-') std::printf("Ignoring option not applicable on one GPU: %s\n", argv[i]);
 		else std::printf("Ignoring unknown option: %s\n", argv[i]);
@@ -167,7 +187,15 @@ int main(int argc, char **argv)
 		autotune = false;
 	}
 
+	// the reference's settings lines (main.cpp:214-232), then this build's
+	const bool lazy = (flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_REF_DECK)) != 0;
+	std::printf("jobid=%d\n", jobid);
 	std::printf("n=%d b=%d r=1 c=1\n", n, b);
+	std::printf("%s %s %s %s %s %s %s %s\n", tile ? "tile" : "2dbc",
+		(flags & HPLAI_FLAG_REF_BACKBUF) ? "back_buffer" : lazy ? "lazy" : "precomp", rdma ? "rdma" : "mpi",
+		warmup ? "warmup" : "full", pack ? "pack" : "nopack", checksum ? "checksum" : "nocheck",
+		l1est ? "skiplu" : "noskiplu", higham ? "hmat" : "ddmat");
+	std::printf("numasize=%d numamap=%s nbuf=%d\n", numasize, numamap, nbuf);
 	std::printf("1gpu %s full fp32/%s%s%s\n", (flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_REF_DECK)) ? "lazy" : "precomp",
 		precision == HPLAI_F32_F8 ? "e4m3" : "fp16",
 		(flags & HPLAI_FLAG_REF_BACKBUF) ? " fp16-deck-ref back_buffer"

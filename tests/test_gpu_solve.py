@@ -283,6 +283,9 @@ def test_driver_ref_deck_reproduces_the_references_steps(hplai, torch_cuda, tmp_
                          timeout=300, cwd=tmp_path)
     assert out.returncode == 0, out.stderr
     assert "1gpu lazy full fp32/fp16 fp16-deck-ref" in out.stdout
+    # the reference's settings lines for the same flags (main.cpp:214-232)
+    assert "jobid=0\nn=1200 b=60 r=1 c=1\n2dbc lazy rdma full nopack nocheck noskiplu ddmat\n" in out.stdout
+    assert "numasize=0 numamap=ROWDIST nbuf=2" in out.stdout
     steps = re.findall(r"# iterative refinement: step=\s*(\d+), residual=(\S+) hpl-harness=(\S+)", out.stdout)
     assert len(steps) == len(fix["steps"]), out.stdout
     assert abs(float(steps[0][1]) - fix["steps"][0]["residual"]) <= 1e-13 * fix["steps"][0]["residual"]
