@@ -82,6 +82,13 @@ struct hplai_ctx {
 	// dscale x (accumulated update)
 	uint16_t *deck = nullptr;
 	float dscale = 1.f;
+	// HPLAI_FLAG_LAZY_A: A is not stored; the deck lives in the upper half of
+	// each FP32 column (FP16 element (i, j) at ((uint16_t*)A)[2 lda j + lda + i],
+	// FP32 rows lda/2 .. (lda + n)/2), so deck_ld = 2 lda halves; dstage holds
+	// a diagonal block's deck while the block is formed over it
+	int64_t deck_ld = 0;
+	bool deck_aliased = false;
+	uint16_t *dstage = nullptr;
 	// HPLAI_FLAG_REF_DECK: the reference's `-d` deck (n x lda halves), its
 	// FP16 L-panel scale n^0.75 and the lazy-init downscale; regen_a: A is
 	// not stored (hplai_generate) and the lazy initialisation regenerates it
@@ -162,7 +169,8 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->sls);
 	cudaFree(c->sus);
 	cudaFree(c->qbits);
-	cudaFree(c->deck);
+	if (!c->deck_aliased) cudaFree(c->deck);
+	cudaFree(c->dstage);
 	cudaFree(c->rdeck);
 	cudaFree(c->rback);
 	cudaFree(c->tcbuf);
@@ -301,6 +309,10 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		(precision != HPLAI_F32_F16 || (flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_LOOKAHEAD))))
 		return HPLAI_EINVAL;
 	if ((flags & HPLAI_FLAG_REF_BACKBUF) && !(flags & HPLAI_FLAG_REF_DECK)) return HPLAI_EINVAL;
+	// A regenerated at panel time: the precision form's FP16 panel copies fold it in
+	if ((flags & HPLAI_FLAG_LAZY_A) && (!(flags & HPLAI_FLAG_FP16_DECK) || precision != HPLAI_F32_F8 || b % 4 ||
+		(flags & (HPLAI_FLAG_SIMT_PANELS | HPLAI_FLAG_REF_DECK))))
+		return HPLAI_EINVAL;
 	hplai_ctx *c = new hplai_ctx;
 	c->n = n;
 	c->b = b;
@@ -353,7 +365,14 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		}
 		CTX_ALLOC(c->qbits, sizeof(unsigned) * nblk128);
 	}
-	if (flags & HPLAI_FLAG_FP16_DECK) {
+	c->deck_ld = c->lda;
+	if (flags & HPLAI_FLAG_LAZY_A) {
+		c->deck = reinterpret_cast<uint16_t *>(c->A) + c->lda;
+		c->deck_ld = 2 * c->lda;
+		c->deck_aliased = true;
+		CTX_ALLOC(c->dstage, sizeof(uint16_t) * static_cast<size_t>(b) * b);
+		c->dscale = std::ldexp(1.0f, static_cast<int>(std::lround(0.75 * std::log2(static_cast<double>(n)))));
+	} else if (flags & HPLAI_FLAG_FP16_DECK) {
 		CTX_ALLOC(c->deck, sizeof(uint16_t) * static_cast<size_t>(c->lda) * n);
 		// a power of two near n^0.75, the reference's scalea (hpl_rand.hpp:154)
 		c->dscale = std::ldexp(1.0f, static_cast<int>(std::lround(0.75 * std::log2(static_cast<double>(n)))));
@@ -396,7 +415,7 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 		if (s == HPLAI_OK) s = schur_set_cmap(&m, c->A, n, n, c->lda);
 		m.status = c->kstatus;
 		m.deck_base = c->deck;
-		m.deck_ld = c->lda;
+		m.deck_ld = c->deck_ld;
 	};
 	for (int i = 0; i < 2 && s == HPLAI_OK; ++i) {
 		for (int h = 0; h < c->gcap && s == HPLAI_OK; ++h) {
@@ -449,7 +468,7 @@ extern "C" int hplai_generate(hplai_ctx *c, uint64_t seed)
 	// FP32 rounding of the sequential FP64 row sums (which are also d).  The
 	// `-d` parity mode stores no A (pmatgen0, main.cpp:260-261): its lazy
 	// initialisation regenerates each block when it joins a panel.
-	c->regen_a = (c->flags & HPLAI_FLAG_REF_DECK) != 0;
+	c->regen_a = (c->flags & (HPLAI_FLAG_REF_DECK | HPLAI_FLAG_LAZY_A)) != 0;
 	if (c->matrix == HPLAI_MATRIX_HIGHAM) {
 		// pmatgen / pdiaggen with HMGen (matgen.hpp:25-77, 227-243); the
 		// right-hand side stays the LCG's column n (main.cpp:266)
@@ -470,6 +489,7 @@ extern "C" int hplai_upload(hplai_ctx *c, const float *a, int64_t lda, const dou
 	uint64_t seed)
 {
 	if (!c || !a || !rhs || !diag || lda < c->n) return HPLAI_EINVAL;
+	if (c->flags & HPLAI_FLAG_LAZY_A) return HPLAI_EUNSUPPORTED;   // the matrix is regenerated, not stored
 	const int n = c->n;
 	HPLAI_CUDA_TRY(cudaMemcpy2DAsync(c->A, sizeof(float) * c->lda, a, sizeof(float) * lda, sizeof(float) * n, n,
 		cudaMemcpyHostToDevice, c->st));
@@ -520,8 +540,15 @@ int panel_step(hplai_ctx *c, int k, int buf, int slot, bool simt, int side_ctas,
 	} else if (f16_panels) {
 		// FP16 panel products (the Schur update reads only the e4m3 copies made below)
 		HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st, false));
+		// A not stored: the block column regenerated into the (otherwise unused)
+		// TF32 split buffer, column-major with leading dimension n
+		const float *src = nullptr;
+		if (c->deck_aliased) {
+			HPLAI_TRY(launch_fill(n, static_cast<int>(kb) + b, static_cast<int>(kb), rem, b, c->tcbuf, n, c->seed, 0, st));
+			src = c->tcbuf;
+		}
 		HPLAI_TRY(launch_lpanel_f16(c->tc, c->maps[buf][slot], static_cast<int>(kb), rem, c->A, lda, lslot, uslot, ldg,
-			deck, inv_dscale, side_ctas, st));
+			deck, c->deck_ld, inv_dscale, side_ctas, st, src, n));
 	} else {
 		HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st));
 		// the precision form's Schur update reads the e4m3 copies only: no FP16 copy
@@ -534,8 +561,15 @@ int panel_step(hplai_ctx *c, int k, int buf, int slot, bool simt, int side_ctas,
 		HPLAI_TRY(launch_trsm_left_lower(b, rem, diag, lda, diag + static_cast<int64_t>(b) * lda, lda,
 			uslot + (kb + b) * ldg, ldg, 1.0f, st));
 	} else if (f16_panels) {
+		// the block row likewise (b x rem, leading dimension the split buffer's ldp)
+		const float *src = nullptr;
+		const int64_t ldp = (b + 31) / 32 * 32;
+		if (c->deck_aliased) {
+			HPLAI_TRY(launch_fill(n, static_cast<int>(kb), static_cast<int>(kb) + b, b, rem, c->tcbuf, ldp, c->seed, 0, st));
+			src = c->tcbuf;
+		}
 		HPLAI_TRY(launch_upanel_f16(c->tc, c->maps[buf][slot], static_cast<int>(kb), rem, c->A, lda, uslot, ldg, deck,
-			inv_dscale, side_ctas, st));
+			c->deck_ld, inv_dscale, side_ctas, st, src, ldp));
 	} else {
 		uint16_t *uh = c->precision == HPLAI_F32_F8 ? nullptr : uslot + (kb + b) * ldg;
 		HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, uh, ldg, 1.0f, side_ctas, st));
@@ -640,7 +674,16 @@ int prepare_block(hplai_ctx *c, int j, int first, int q, bool simt, int side_cta
 		HPLAI_TRY(schur_region(c, op, r1, n, r1, r2, side_ctas, st, pe));
 		HPLAI_TRY(schur_region(c, op, r1, r2, r2, n, side_ctas, st, pe));
 	}
-	if (c->deck && j > 0) {
+	if (c->deck_aliased) {
+		// the diagonal block formed from the LCG and its deck, staged first:
+		// near the matrix end its FP32 rows overlay its own deck rows
+		HPLAI_TRY(pe.record(st, HPLAI_PH_LAZY_INIT));
+		HPLAI_CUDA_TRY(cudaMemcpy2DAsync(c->dstage, sizeof(uint16_t) * b, c->deck + r1 + static_cast<int64_t>(r1) * c->deck_ld,
+			sizeof(uint16_t) * c->deck_ld, sizeof(uint16_t) * b, b, cudaMemcpyDeviceToDevice, st));
+		HPLAI_TRY(launch_lazy_init(n, r1, r2, r1, r2, c->A, c->lda, c->dstage, nullptr, b, r1, r1, 1.0f / c->dscale,
+			c->seed, c->d, true, st));
+		HPLAI_TRY(pe.end(st));
+	} else if (c->deck && j > 0) {
 		HPLAI_TRY(pe.record(st, HPLAI_PH_LAZY_INIT));
 		if (f16_panel_form(c, simt)) {
 			HPLAI_TRY(launch_deck_apply(r1, r2, r1, r2, c->A, c->lda, c->deck, c->lda, 1.0f / c->dscale, st));
@@ -679,8 +722,8 @@ int factor_refdeck(hplai_ctx *c, int kend)
 	if (c->regen_a) HPLAI_CUDA_TRY(cudaMemsetAsync(c->A, 0, sizeof(float) * static_cast<size_t>(lda) * n, st));
 	auto lazy = [&](int r0, int r1, int c0, int c1) -> int {
 		HPLAI_TRY(pe.record(st, HPLAI_PH_LAZY_INIT));
-		HPLAI_TRY(launch_lazy_init(n, r0, r1, c0, c1, c->A, lda, c->rdeck, c->rback, lda, c->rdownscale, c->seed, c->d,
-			c->regen_a, st));
+		HPLAI_TRY(launch_lazy_init(n, r0, r1, c0, c1, c->A, lda, c->rdeck, c->rback, lda, 0, 0, c->rdownscale, c->seed,
+			c->d, c->regen_a, st));
 		return pe.end(st);
 	};
 	const int steps = std::min(kend, nb);
@@ -740,7 +783,10 @@ int factor_impl(hplai_ctx *c, int kend, const float *host_a = nullptr, int64_t h
 	c->group = ((c->flags & HPLAI_FLAG_GROUP2) && c->gcap == 2 && kend >= nb) ? 2 : 1;
 	const int G = c->group;
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->kstatus, 0, 2 * sizeof(unsigned), c->st));
-	if (c->deck) HPLAI_CUDA_TRY(cudaMemsetAsync(c->deck, 0, sizeof(uint16_t) * static_cast<size_t>(c->lda) * n, c->st));
+	if (c->deck_aliased)
+		HPLAI_CUDA_TRY(cudaMemset2DAsync(c->deck, sizeof(uint16_t) * c->deck_ld, 0, sizeof(uint16_t) * n, n, c->st));
+	else if (c->deck)
+		HPLAI_CUDA_TRY(cudaMemsetAsync(c->deck, 0, sizeof(uint16_t) * static_cast<size_t>(c->lda) * n, c->st));
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->getrf_work, 0, sizeof(uint32_t), c->st));   // its status word
 	const bool simt = (c->flags & HPLAI_FLAG_SIMT_PANELS) != 0;
 	const bool serial = (c->flags & HPLAI_FLAG_LOOKAHEAD) == 0;
@@ -1470,6 +1516,7 @@ extern "C" int hplai_solve_host(hplai_ctx *c, const float *a, int64_t lda, const
 	uint64_t seed, int maxit, double *x, hplai_ir_errors *err, int *iters)
 {
 	if (!c || !a || !rhs || !diag || !x || lda < c->n) return HPLAI_EINVAL;
+	if (c->flags & HPLAI_FLAG_LAZY_A) return HPLAI_EUNSUPPORTED;   // the matrix is regenerated, not stored
 	// With the FP16 deck and a page-locked matrix the copy runs behind the
 	// factorisation (each panel waits for its own block column and row);
 	// otherwise the whole matrix is copied first.

@@ -160,10 +160,11 @@ int launch_l1est(int n, float *a, int64_t lda, const double *d, cudaStream_t st)
 // value a0 regenerated from the LCG (float(d_i) on the diagonal, d the FP64
 // row sums) when `regen`, or read from a (an uploaded matrix) otherwise;
 // with a back buffer the deck value is deck + 32 back.  Rows [r0, r1) x
-// columns [c0, c1), one thread per row.
+// columns [c0, c1), one thread per row; deck (and back) element (i, j) at
+// [(j - dc0) * ldd + (i - dr0)].
 __global__ void __launch_bounds__(kFillRows) lazy_init_kernel(int n, int r0, int r1, int c0, int c1,
 	float *__restrict__ a, int64_t lda, const __half *__restrict__ deck, const __half *__restrict__ back, int64_t ldd,
-	float downscale, uint64_t seed, const double *__restrict__ d, int regen, JumpTable tab)
+	int dr0, int dc0, float downscale, uint64_t seed, const double *__restrict__ d, int regen, JumpTable tab)
 {
 	const int i = r0 + blockIdx.x * kFillRows + threadIdx.x;
 	const int j0 = c0 + blockIdx.y * kFillCols;
@@ -183,7 +184,7 @@ __global__ void __launch_bounds__(kFillRows) lazy_init_kernel(int n, int r0, int
 		} else {
 			a0 = a[o];
 		}
-		const int64_t od = static_cast<int64_t>(j) * ldd + i;
+		const int64_t od = static_cast<int64_t>(j - dc0) * ldd + (i - dr0);
 		// with the back buffer: deck + 32 back (lazy_init_omp.cpp:704-760)
 		const float x = back ? __fmaf_rn(32.0f, __half2float(back[od]), __half2float(deck[od])) : __half2float(deck[od]);
 		a[o] = __fmaf_rn(downscale, x, a0);
@@ -191,12 +192,13 @@ __global__ void __launch_bounds__(kFillRows) lazy_init_kernel(int n, int r0, int
 }
 
 int launch_lazy_init(int n, int r0, int r1, int c0, int c1, float *a, int64_t lda, const uint16_t *deck,
-	const uint16_t *back, int64_t ldd, float downscale, uint64_t seed, const double *d, bool regen, cudaStream_t st)
+	const uint16_t *back, int64_t ldd, int dr0, int dc0, float downscale, uint64_t seed, const double *d, bool regen,
+	cudaStream_t st)
 {
 	if (r1 <= r0 || c1 <= c0) return HPLAI_OK;
 	dim3 grid((r1 - r0 + kFillRows - 1) / kFillRows, (c1 - c0 + kFillCols - 1) / kFillCols);
 	lazy_init_kernel<<<grid, kFillRows, 0, st>>>(n, r0, r1, c0, c1, a, lda, reinterpret_cast<const __half *>(deck),
-		reinterpret_cast<const __half *>(back), ldd, downscale, seed, d, regen ? 1 : 0, jump_table());
+		reinterpret_cast<const __half *>(back), ldd, dr0, dc0, downscale, seed, d, regen ? 1 : 0, jump_table());
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;

@@ -30,9 +30,11 @@ double higham_beta(int n, double kappa, double rho);
 int launch_higham_fill(int n, double alpha, double beta, float *a, int64_t lda, double *d, bool factors, cudaStream_t st);
 double higham_norm(int n, double alpha, double beta);
 // The `-d` lazy initialisation a = fma(downscale, deck, a0) on rows [r0, r1)
-// x columns [c0, c1), a0 regenerated (regen) or read from a.
+// x columns [c0, c1), a0 regenerated (regen) or read from a; the deck's
+// element (i, j) at deck[(j - dc0) * ldd + (i - dr0)].
 int launch_lazy_init(int n, int r0, int r1, int c0, int c1, float *a, int64_t lda, const uint16_t *deck,
-	const uint16_t *back, int64_t ldd, float downscale, uint64_t seed, const double *d, bool regen, cudaStream_t st);
+	const uint16_t *back, int64_t ldd, int dr0, int dc0, float downscale, uint64_t seed, const double *d, bool regen,
+	cudaStream_t st);
 // The back buffer's write-back of the deck over rows and columns [r0, n)
 // (bb_writeback_b_impl_fp16, back_buffer.cpp:53-100).
 int launch_backbuf_writeback(int n, int r0, uint16_t *deck, uint16_t *back, int64_t ld, cudaStream_t st);
@@ -150,12 +152,18 @@ int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStr
 // copied to FP16 (rows kb+b..), and A_col <- A_col U11^{-1},
 // A_row <- L11^{-1} A_row are written back into A by the Schur kernel's store
 // form.  `maps` are the FP16 maps over lh/uh with the C map over A.  With
-// the FP16 deck (same layout as A; null if none) the panels are read as
-// A + deck * inv_dscale, so only the diagonal block needs deck_apply.
+// the FP16 deck (element (i, j) at deck[j*ldd + i]; null if none) the panels
+// are read as A + deck * inv_dscale, so only the diagonal block needs
+// deck_apply.  src (null: A itself) holds the panel's A values instead of A
+// (column-major, leading dimension lds; element (r, k) of A_col at
+// src[k*lds + r], of A_row at src[r*lds + k]) -- the matrix regenerated into
+// a scratch panel when A is not stored.
 int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
-	uint16_t *lh, uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st);
+	uint16_t *lh, uint16_t *uh, int64_t ldh, const uint16_t *deck, int64_t ldd, float inv_dscale, int max_ctas,
+	cudaStream_t st, const float *src = nullptr, int64_t lds = 0);
 int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
-	uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st);
+	uint16_t *uh, int64_t ldh, const uint16_t *deck, int64_t ldd, float inv_dscale, int max_ctas, cudaStream_t st,
+	const float *src = nullptr, int64_t lds = 0);
 // A_col (rem x b) <- A_col U11^{-1}; lh row i = half(scale * A_col row i)
 int launch_lpanel_tc(const TcPanels &t, int rem, float *acol, int64_t lda, uint16_t *lh, int64_t ldh, float scale,
 	int max_ctas, cudaStream_t st);

@@ -840,11 +840,13 @@ int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint1
 }
 
 int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
-	uint16_t *lh, uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st)
+	uint16_t *lh, uint16_t *uh, int64_t ldh, const uint16_t *deck, int64_t ldd, float inv_dscale, int max_ctas,
+	cudaStream_t st, const float *src, int64_t lds)
 {
 	if (rem <= 0) return HPLAI_OK;
 	const int width = (t.b + 63) / 64 * 64;   // the panel's slot in a buffer of row pitch ldh
-	if (!t.f16_amax || !t.f16_oscale || ldh % 64 || ldh < width || t.b % 4 || kb % 4 || rem % 4 || lda % 4)
+	if (!t.f16_amax || !t.f16_oscale || ldh % 64 || ldh < width || t.b % 4 || kb % 4 || rem % 4 || lda % 4 ||
+		ldd % 4 || (src && (lds % 4 || lds < rem || reinterpret_cast<uintptr_t>(src) % 16)))
 		return HPLAI_EINVAL;
 	const int b = t.b;
 	// the inverted triangles into rows kb .. kb+b-1 of the FP16 panel buffers
@@ -861,10 +863,10 @@ int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// A_col (rows kb+b.., columns kb..kb+b-1) -> FP16 K-major rows kb+b.. of lh
 	const int64_t kbl = kb;
-	float *acol = a + (kbl + b) + kbl * lda;
-	const __half *dcol = deck ? reinterpret_cast<const __half *>(deck) + (kbl + b) + kbl * lda : nullptr;
-	panel_f16_t_kernel<<<dim3((rem + 63) / 64, static_cast<unsigned>(width / 64)), 256, 0, st>>>(rem, b, acol, lda,
-		dcol, lda, inv_dscale, reinterpret_cast<__half *>(lh) + (kbl + b) * ldh, ldh, width);
+	const float *acol = src ? src : a + (kbl + b) + kbl * lda;
+	const __half *dcol = deck ? reinterpret_cast<const __half *>(deck) + (kbl + b) + kbl * ldd : nullptr;
+	panel_f16_t_kernel<<<dim3((rem + 63) / 64, static_cast<unsigned>(width / 64)), 256, 0, st>>>(rem, b, acol,
+		src ? lds : lda, dcol, ldd, inv_dscale, reinterpret_cast<__half *>(lh) + (kbl + b) * ldh, ldh, width);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// A_col = (A_col (s_u U11^{-1})) / s_u
@@ -872,20 +874,23 @@ int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 }
 
 int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
-	uint16_t *uh, int64_t ldh, const uint16_t *deck, float inv_dscale, int max_ctas, cudaStream_t st)
+	uint16_t *uh, int64_t ldh, const uint16_t *deck, int64_t ldd, float inv_dscale, int max_ctas, cudaStream_t st,
+	const float *src, int64_t lds)
 {
 	if (rem <= 0) return HPLAI_OK;
 	const int width = (t.b + 63) / 64 * 64;
-	if (!t.f16_oscale || ldh % 64 || ldh < width || t.b % 4 || kb % 4 || rem % 4 || lda % 4) return HPLAI_EINVAL;
+	if (!t.f16_oscale || ldh % 64 || ldh < width || t.b % 4 || kb % 4 || rem % 4 || lda % 4 || ldd % 4 ||
+		(src && (lds % 4 || lds < t.b || reinterpret_cast<uintptr_t>(src) % 16)))
+		return HPLAI_EINVAL;
 	const int b = t.b;
 	const int64_t kbl = kb;
 	// A_row (rows kb..kb+b-1, columns kb+b..): column j -> FP16 row kb+b+j of uh
-	float *arow = a + kbl + (kbl + b) * lda;
-	const __half *drow = deck ? reinterpret_cast<const __half *>(deck) + kbl + (kbl + b) * lda : nullptr;
+	const float *arow = src ? src : a + kbl + (kbl + b) * lda;
+	const __half *drow = deck ? reinterpret_cast<const __half *>(deck) + kbl + (kbl + b) * ldd : nullptr;
 	{
 		const int64_t work = static_cast<int64_t>(rem) * (width / 4);
 		const unsigned blocks = static_cast<unsigned>(std::min<int64_t>((work + 255) / 256, 148 * 16));
-		panel_f16_n_kernel<<<blocks, 256, 0, st>>>(rem, b, arow, lda, drow, lda, inv_dscale,
+		panel_f16_n_kernel<<<blocks, 256, 0, st>>>(rem, b, arow, src ? lds : lda, drow, ldd, inv_dscale,
 			reinterpret_cast<__half *>(uh) + (kbl + b) * ldh, ldh, width);
 	}
 	count_launches();

@@ -33,6 +33,7 @@ FLAG_FP16_DECK = 4
 FLAG_GROUP2 = 8
 FLAG_REF_DECK = 16
 FLAG_REF_BACKBUF = 32
+FLAG_LAZY_A = 64
 MATRIX_LCG = 0
 MATRIX_HIGHAM = 1
 IR, GMRES = 0, 1

@@ -127,6 +127,18 @@ typedef enum hplai_phase {
  * fma(downscale, deck + 32 back, a_ij).  HPLAI_EINVAL without
  * HPLAI_FLAG_REF_DECK. */
 #define HPLAI_FLAG_REF_BACKBUF 32u
+/* With HPLAI_FLAG_FP16_DECK and HPLAI_F32_F8: A is never stored.  A block's
+ * entries are regenerated from the LCG when it joins a panel (the reference's
+ * lazy initialisation, lazy_init.hpp:92-227), and the FP16 deck shares the
+ * factors' storage -- it lives in the upper half of each FP32 column, where
+ * the factors arrive only after the deck entries there are consumed -- so a
+ * solve holds 4 n^2 bytes of matrix instead of 6 n^2 (n = 196608 fits in
+ * 180 GB).  The factors are bit-identical to the stored-A deck form.
+ * hplai_upload and hplai_solve_host return HPLAI_EUNSUPPORTED (nothing to
+ * regenerate a caller's matrix from).  HPLAI_EINVAL without
+ * HPLAI_FLAG_FP16_DECK, with another precision, b % 4 != 0,
+ * HPLAI_FLAG_SIMT_PANELS or HPLAI_FLAG_REF_DECK. */
+#define HPLAI_FLAG_LAZY_A 64u
 
 typedef struct hplai_ctx hplai_ctx;
 
