@@ -345,7 +345,7 @@ class FormRun:
     the device before each solve outside the timed window."""
 
     def __init__(self, hplai, torch, form, n, b, seed, maxit, autotune, lookahead, barrier, group=1, side_sms=32,
-                 matrix="lcg"):
+                 matrix="lcg", lazy_a=False):
         self.hplai, self.torch, self.form = hplai, torch, form
         self.n, self.b, self.seed, self.maxit = n, b, seed, maxit
         self.fp8 = form["precision"] == "f8"
@@ -354,6 +354,9 @@ class FormRun:
         flags = hplai.FLAG_LOOKAHEAD if lookahead else 0
         if self.deck:
             flags |= hplai.FLAG_FP16_DECK
+        self.lazy_a = bool(lazy_a and self.deck and self.fp8)
+        if self.lazy_a:
+            flags |= hplai.FLAG_LAZY_A
         if group == 2:
             flags |= hplai.FLAG_GROUP2
         self.s = hplai.Solver(n, b, precision=hplai.F32_F8 if self.fp8 else hplai.F32_F16, flags=flags)
@@ -423,7 +426,9 @@ class FormRun:
             "ms_per_step": max_ms / steps, "ms_min": min(r[0] for r in self.results),
             "ms_max": max(r[0] for r in self.results),
             "schedule": self.schedule, "autotuned": self.tuned,
-            "trailing_matrix": "FP16 deck (updates rounded to FP16 once per step, folded in per panel)"
+            "trailing_matrix": ("FP16 deck (updates rounded to FP16 once per step, folded in per panel)"
+                                + ("; A not stored: each block regenerated from the LCG when it joins a panel, "
+                                   "the deck in the upper half of each FP32 column" if self.lazy_a else ""))
             if self.deck else "FP32",
             "hpl_harness": last[1].hpl_harness, "resid": last[1].residual,
             "residual_evaluations": last[1].iters,
@@ -516,8 +521,10 @@ def run_ours(args):
                               f"{'GMRES-IR' if head_form['refine'] == 'gmres' else 'IR'}")
 
     # the headline form: exactly `steps` timed solves after `warmup`
+    if args.lazy_a and not (head_form["precision"] == "f8" and head_form["deck"] and args.matrix == "lcg"):
+        raise SystemExit("--lazy-a needs the e4m3 form with the FP16 deck and the LCG matrix")
     fr = FormRun(hplai, torch, head_form, n, b, seed, maxit, args.autotune, args.lookahead, barrier, args.group,
-                 args.side_sms, args.matrix)
+                 args.side_sms, args.matrix, args.lazy_a)
     fr.run(0, args.warmup)
     sampler = ClockSampler(dev)
     sampler.start()
@@ -527,7 +534,9 @@ def run_ours(args):
     clocks = sampler.stop()
     head = fr.summary(world)
     e2e = None
-    if not args.no_e2e:
+    if args.lazy_a:
+        e2e = {"unavailable": "HPLAI_FLAG_LAZY_A takes no host matrix: A is regenerated from its seed on the device"}
+    elif not args.no_e2e:
         e2e = e2e_run(hplai, torch, fr, min(args.steps, args.e2e_steps), args.e2e_warmup, world, barrier)
     fr.close()
 
@@ -865,6 +874,8 @@ def main():
                     help="solve: one system (default n=131072 b=1024, precision and plain forms); batch: many "
                          "systems; adjoint: forward + transposed solves; gemm / check: the Schur GEMM or the "
                          "factor checksum leaf alone; peak: cuBLAS bf16/e4m3 dense rates (the roofline denominators)")
+    ap.add_argument("--lazy-a", action="store_true",
+                    help="headline form without a stored A (HPLAI_FLAG_LAZY_A; e4m3 + FP16 deck, LCG matrix)")
     ap.add_argument("--matrix", choices=("lcg", "higham"), default="lcg",
                     help="solve workload: the benchmark's LCG matrix or Higham's (the reference's --highammat)")
     ap.add_argument("--m", type=int, default=16384, help="gemm workload: rows of C")

@@ -1390,8 +1390,8 @@ extern "C" int hplai_set_matrix(hplai_ctx *c, int kind, double cond, double rho)
 	if (kind == HPLAI_MATRIX_LCG) {
 		c->matrix = kind;
 	} else if (kind == HPLAI_MATRIX_HIGHAM) {
-		// the `-d` parity mode regenerates the LCG matrix at panel time
-		if (c->flags & HPLAI_FLAG_REF_DECK) return HPLAI_EUNSUPPORTED;
+		// the `-d` parity mode and the lazy form regenerate the LCG matrix at panel time
+		if (c->flags & (HPLAI_FLAG_REF_DECK | HPLAI_FLAG_LAZY_A)) return HPLAI_EUNSUPPORTED;
 		double a = 0.0, b = 0.0;
 		HPLAI_TRY(hplai_higham_params(c->n, cond, rho, &a, &b));
 		c->matrix = kind;

@@ -105,6 +105,8 @@ static int usage()
 		"   --ref-deck              The reference's -d arithmetic bit for bit: A regenerated at panel\n"
 		"                           time, FP16-accumulating Schur update on CUDA cores (parity mode).\n"
 		"   --back_buffer           With --ref-deck (implied): the reference's back-buffer form bit for bit.\n"
+		"   --lazy-a                With --fp8 (implies -d): store no A; each block is regenerated from the\n"
+		"                           LCG when it joins a panel and the deck shares the factors' storage.\n"
 		"   --highammat             Higham's HPL-AI matrix (cond 1000) instead of the LCG matrix.\n"
 		"   --fp8                   e4m3 Schur update with GMRES refinement.\n"
 		"   --gmres                 GMRES refinement instead of the classical correction.\n"
@@ -147,6 +149,7 @@ int main(int argc, char **argv)
 			!std::strcmp(argv[i], "--lazy-init"))
 			flags |= HPLAI_FLAG_FP16_DECK;
 		else if (!std::strcmp(argv[i], "--ref-deck")) flags |= HPLAI_FLAG_REF_DECK;
+		else if (!std::strcmp(argv[i], "--lazy-a")) flags |= HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_LAZY_A;
 		else if (!std::strcmp(argv[i], "--back_buffer")) flags |= HPLAI_FLAG_REF_DECK | HPLAI_FLAG_REF_BACKBUF;
 		else if (!std::strcmp(argv[i], "--highammat")) higham = true;
 		else if (!std::strcmp(argv[i], "--fp8")) { precision = HPLAI_F32_F8; mode = HPLAI_GMRES; }
@@ -183,7 +186,7 @@ int main(int argc, char **argv)
 	if (argc > 1 && (!std::strcmp(argv[1], "-h") || !std::strcmp(argv[1], "--help"))) return usage();
 	if (flags & HPLAI_FLAG_REF_DECK) {
 		// one fixed schedule: nothing to tune
-		flags &= ~(HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_LOOKAHEAD);
+		flags &= ~(HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_LAZY_A);
 		autotune = false;
 	}
 
@@ -199,7 +202,8 @@ int main(int argc, char **argv)
 	std::printf("1gpu %s full fp32/%s%s%s\n", (flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_REF_DECK)) ? "lazy" : "precomp",
 		precision == HPLAI_F32_F8 ? "e4m3" : "fp16",
 		(flags & HPLAI_FLAG_REF_BACKBUF) ? " fp16-deck-ref back_buffer"
-		: (flags & HPLAI_FLAG_REF_DECK) ? " fp16-deck-ref" : (flags & HPLAI_FLAG_FP16_DECK) ? " fp16-deck" : "",
+		: (flags & HPLAI_FLAG_REF_DECK) ? " fp16-deck-ref"
+		: (flags & HPLAI_FLAG_LAZY_A) ? " fp16-deck no-stored-A" : (flags & HPLAI_FLAG_FP16_DECK) ? " fp16-deck" : "",
 		higham ? " hmat" : " ddmat");
 
 	// Warm-up on a small system with the same block size so that every kernel

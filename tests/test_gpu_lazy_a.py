@@ -49,3 +49,26 @@ def test_lazy_a_flag_combinations(hplai):
     for prec, flags in [(1, 64), (0, 4 | 64), (1, 4 | 1 | 64)]:
         with pytest.raises(hplai.HplaiError):
             hplai.Solver(1024, 128, precision=prec, flags=flags)
+    # the lazy form regenerates the LCG matrix: Higham's matrix is refused
+    with hplai.Solver(1024, 128, precision=hplai.F32_F8, flags=DECK | hplai.FLAG_LAZY_A) as s:
+        with pytest.raises(hplai.HplaiError):
+            s.set_matrix(hplai.MATRIX_HIGHAM, 1000.0, 0.5)
+
+
+def test_lazy_a_l1est_and_checksum(hplai, torch_cuda):
+    """--l1est regenerates the whole matrix into the factors' storage (the
+    deck is cleared again by the next factorisation) and gives the stored-A
+    form's approximation; the checksum of the lazy factors equals the
+    stored-A form's."""
+    n, b = 2048, 256
+    sig = []
+    for flags in (DECK, DECK | hplai.FLAG_LAZY_A):
+        with hplai.Solver(n, b, precision=hplai.F32_F8, flags=flags) as s:
+            s.generate(42)
+            s.l1est()
+            e0 = s.lu()
+            s.generate(42)
+            s.factor()
+            sig.append((e0, s.checksum()))
+    assert np.array_equal(sig[0][0].view(np.uint32), sig[1][0].view(np.uint32))
+    assert np.array_equal(sig[0][1], sig[1][1])
