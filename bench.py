@@ -495,6 +495,7 @@ def run_ours(args):
     else:
         torch.cuda.set_device(0)
     import hplai
+    hplai.set_cta_pairs_default(args.pairs != "off")
 
     n, b, seed, maxit = args.n, args.b, 42, 50
     dev = torch.cuda.current_device()
@@ -718,6 +719,7 @@ def run_gemm(args):
     import hplai
     m, n, k = args.m, args.n_cols, args.k
     fp8 = args.precision == "f8"
+    hplai.set_cta_pairs_default(args.pairs != "off")
     torch.manual_seed(0)
     ldc = (m + 63) // 64 * 64 + 64   # the solver's padded leading dimension (no power-of-two stride)
     deck = args.deck == "on"
@@ -753,19 +755,24 @@ def run_gemm(args):
     for _ in range(args.warmup):
         call()
     torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
         call()
     e1.record()
     e1.synchronize()
+    clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / args.steps
     flops = 2.0 * m * n * k
     byts = (4.0 if deck else 8.0) * m * n + (m + n) * k * (1 if fp8 else 2)
     cform = "FP16 deck" if deck else "FP32 C"
+    if deck:
+        cform += ", CTA pairs" if args.pairs != "off" else ", single CTAs"
     print(json.dumps({"workload": f"schur GEMM leaf m={m} n={n} k={k} {'e4m3' if fp8 else 'fp16'} {cform}",
                       "ms_per_launch": ms, "tflops": flops / ms / 1e9, "gbs": byts / ms / 1e6,
-                      "algorithmic_bytes": byts, "flops": flops}), flush=True)
+                      "algorithmic_bytes": byts, "flops": flops, "clocks": clocks}), flush=True)
     return 0
 
 
@@ -874,6 +881,8 @@ def main():
                     help="solve: one system (default n=131072 b=1024, precision and plain forms); batch: many "
                          "systems; adjoint: forward + transposed solves; gemm / check: the Schur GEMM or the "
                          "factor checksum leaf alone; peak: cuBLAS bf16/e4m3 dense rates (the roofline denominators)")
+    ap.add_argument("--pairs", choices=("on", "off"), default="off",
+                    help="deck updates on CTA pairs (tcgen05 cta_group::2) or single CTAs")
     ap.add_argument("--lazy-a", action="store_true",
                     help="headline form without a stored A (HPLAI_FLAG_LAZY_A; e4m3 + FP16 deck, LCG matrix)")
     ap.add_argument("--matrix", choices=("lcg", "higham"), default="lcg",

@@ -136,6 +136,7 @@ struct hplai_ctx {
 		int tile_group;
 	};
 	int tile_group = 0;   // tile rows per group of the Schur kernel's tile order (0: its default)
+	int cta_pairs = -1;   // deck updates on CTA pairs: 1 on, 0 off, -1 the library default
 	std::vector<Trial> tune_log;
 	// GMRES correction: restart length, relative tolerance on the
 	// preconditioned residual, basis and scratch (allocated on first use)
@@ -1224,6 +1225,26 @@ extern "C" int hplai_set_tile_group(hplai_ctx *c, int group_m)
 {
 	if (!c || group_m < 0 || group_m > 1024) return HPLAI_EINVAL;
 	apply_tile_group(c, group_m);
+	return HPLAI_OK;
+}
+
+extern "C" int hplai_set_cta_pairs(hplai_ctx *c, int on)
+{
+	if (!c) {
+		// the library default, for contexts left at -1 and the leaf calls
+		if (on < 0) return HPLAI_EINVAL;
+		schur_set_pairs_default(on != 0);
+		return HPLAI_OK;
+	}
+	if (on < -1) return HPLAI_EINVAL;
+	c->cta_pairs = on > 0 ? 1 : on;
+	for (int i = 0; i < 2; ++i) {
+		for (auto &m : c->maps[i]) m.pairs = c->cta_pairs;
+		c->mapsg[i].pairs = c->cta_pairs;
+		c->maps8[i].pairs = c->cta_pairs;
+		c->maps8g[i].pairs = c->cta_pairs;
+	}
+	c->maps8s.pairs = c->cta_pairs;
 	return HPLAI_OK;
 }
 

@@ -66,6 +66,7 @@ int launch_trsm_left_lower(int b, int ncols, const float *l, int64_t ldl, float 
 struct SchurMaps {
 	alignas(64) unsigned char lmap[128];
 	alignas(64) unsigned char umap[128];
+	alignas(64) unsigned char umap2[128];   // U with 128-row boxes (CTA-pair kernel)
 	int k;         // inner dimension (panel width)
 	// FP32 matrix holding C, for the TMA reduce-add epilogue (a map clipped to
 	// each launch's region is encoded per launch).
@@ -80,11 +81,16 @@ struct SchurMaps {
 	// tile rows per group of the persistent kernel's tile order (0: the
 	// default, 32); hplai_set_tile_group / hplai_autotune set it
 	int group_m = 0;
+	// deck updates on CTA pairs (256 x 256 tiles, tcgen05 cta_group::2):
+	// 1 on, 0 off, -1 the library default (hplai_set_cta_pairs)
+	int pairs = -1;
 };
 // L: lrows x k FP16, row-major with ldl; U: urows x k FP16 (row j = column j
 // of U), ldu.  Rows beyond lrows/urows read as zero.
 int schur_make_maps(SchurMaps *m, const uint16_t *lh, int lrows, int64_t ldl, const uint16_t *uh, int urows,
 	int64_t ldu, int k);
+// The library default for deck updates on CTA pairs (SchurMaps::pairs < 0).
+void schur_set_pairs_default(bool on);
 // Matrix holding C for the TMA reduce-add epilogue; left unset (plain
 // epilogue) when c or ldc is not 16-byte aligned.
 int schur_set_cmap(SchurMaps *m, const float *c, int rows, int cols, int64_t ldc);

@@ -25,6 +25,7 @@
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <atomic>
 #include <cstring>
 
 namespace hplai {
@@ -610,6 +611,267 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 	}
 }
 
+// ---------------------------------------------------------------------------
+// The deck update on CTA pairs (tcgen05 cta_group::2).  A cluster of two CTAs
+// owns a 256 x 256 tile: CTA r loads rows 128 r .. 128 r + 127 of the tile's
+// L block and of its U block (16 KB each per stage), the leader (r = 0)
+// issues M = 256, N = 256 MMAs that read both CTAs' shared memory, and each
+// CTA's tensor memory receives its 128 rows of the accumulator.  Per stage an
+// SM then loads 32 KB for the MMA work that costs 48 KB in the single-CTA
+// kernel (128 x 256 tile), which is what bounds that kernel's e4m3 rate: the
+// operand stream from L2, not the tensor pipe.  Both CTAs' loads count on the
+// leader's `full` barrier; the leader's commits arrive on both CTAs' `empty`
+// and `accf` barriers; the epilogue warps of both CTAs arrive on the leader's
+// `acce` barrier.  Every wait is bounded as in schur_kernel.
+// ---------------------------------------------------------------------------
+#ifndef HPLAI_PAIR_STAGES
+#define HPLAI_PAIR_STAGES 4
+#endif
+constexpr int PAIR_STAGES = HPLAI_PAIR_STAGES;
+constexpr int PAIR_BM = 2 * BM;                       // tile rows of a pair
+constexpr int PAIR_HALF = BM * 128;                   // 16 KB: 128 rows x 128 bytes of one operand
+constexpr int PAIR_STAGE_BYTES = 2 * PAIR_HALF;       // per CTA: its L rows and its U rows
+constexpr size_t pair_smem_bytes()
+{
+	return static_cast<size_t>(PAIR_STAGES) * PAIR_STAGE_BYTES + DECK_BYTES + 1024 + 256;
+}
+static_assert(pair_smem_bytes() <= 232448, "shared memory per CTA of a pair");
+
+template <bool FP8>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(threads_for(2), 1) schur_pair_kernel(
+	const __grid_constant__ CUtensorMap lmap, const __grid_constant__ CUtensorMap umap,
+	const __grid_constant__ CUtensorMap cmap, const Params p)
+{
+	constexpr int NST = PAIR_STAGES;
+	constexpr int NW = DECK_EPI_WARPS;
+	extern __shared__ uint8_t smem_raw[];
+	const uint32_t raw_addr = smem_u32(smem_raw);
+	uint8_t *smem = smem_raw + ((1024u - (raw_addr & 1023u)) & 1023u);
+	uint8_t *sA = smem;
+	uint8_t *sB = smem + NST * PAIR_HALF;
+	__half *dbuf = reinterpret_cast<__half *>(smem + NST * PAIR_STAGE_BYTES);
+	uint64_t *bars = reinterpret_cast<uint64_t *>(smem + NST * PAIR_STAGE_BYTES + DECK_BYTES);
+	uint64_t *full = bars;          // leader: both CTAs' loads of a stage
+	uint64_t *empty = bars + NST;   // both: the stage's MMAs completed
+	uint64_t *accf = bars + 2 * NST;
+	uint64_t *acce = accf + 2;      // leader: both CTAs' epilogues drained the accumulator
+	uint64_t *drain = acce + 2;
+	uint64_t *dbar = drain + 1;
+	uint32_t *tmem_holder = reinterpret_cast<uint32_t *>(dbar + DECK_BUFS);
+
+	const int warp = threadIdx.x >> 5;
+	const int lane = threadIdx.x & 31;
+	const uint32_t rank = cluster_rank();
+	const bool leader = rank == 0;
+	const int cl = static_cast<int>(blockIdx.x >> 1), ncl = static_cast<int>(gridDim.x >> 1);
+
+	if (threadIdx.x == 0) {
+		for (int s = 0; s < NST; ++s) {
+			mbar_init(&full[s], 1);
+			mbar_init(&empty[s], 1);
+		}
+		for (int a = 0; a < 2; ++a) {
+			mbar_init(&accf[a], 1);
+			mbar_init(&acce[a], 2 * NW);
+		}
+		mbar_init(drain, 1);
+		for (int b = 0; b < DECK_BUFS; ++b) mbar_init(&dbar[b], 1);
+		fence_mbar_init();
+	}
+	if (warp == 1) {
+		tmem_alloc_pair(tmem_holder, TMEM_COLS);
+		tmem_relinquish_pair();
+	}
+	if (warp == 0 && lane == 0) {
+		tma_prefetch_desc(&lmap);
+		tma_prefetch_desc(&umap);
+		tma_prefetch_desc(&cmap);
+	}
+	__syncwarp();
+	tc_fence_before();
+	cluster_sync();
+	tc_fence_after();
+	const uint32_t tmem_base = *tmem_holder;
+	const int total = p.tiles_m * p.tiles_n;   // pair tiles (tiles_m counts 256-row tiles)
+	bool ok = true;
+
+	if (warp == 0) {
+		// ---------------- TMA producer (both CTAs) ----------------
+		if (lane == 0) {
+			int stage = 0;
+			uint32_t phase = 0;
+			for (int tile = cl; tile < total && ok; tile += ncl) {
+				int tm, tn;
+				tile_coords(tile, p.tiles_m, p.tiles_n, p.group_m, tm, tn);
+				const int lrow = p.lrow0 + tm * PAIR_BM + static_cast<int>(rank) * BM;
+				const int urow = p.urow0 + tn * BN + static_cast<int>(rank) * BM;
+				for (int kc = 0; kc < p.num_kc; ++kc) {
+					if (!mbar_wait(&empty[stage], phase ^ 1u)) { ok = false; break; }
+					if (leader) mbar_arrive_expect_tx(&full[stage], 2 * PAIR_STAGE_BYTES);
+					const uint32_t fb = smem_peer_u32(&full[stage], 0);
+					const int kx = kc * (FP8 ? 2 * BK : BK);
+					tma_load_2d_pair(sA + stage * PAIR_HALF, &lmap, fb, kx, lrow);
+					tma_load_2d_pair(sB + stage * PAIR_HALF, &umap, fb, kx, urow);
+					if (++stage == NST) { stage = 0; phase ^= 1u; }
+				}
+			}
+			if (!ok) atomicOr(p.status, 1u);
+		}
+	} else if (warp == 1) {
+		// ---------------- MMA issuer (leader) ----------------
+		if (leader && lane == 0) {
+			int stage = 0;
+			uint32_t phase = 0;
+			int acc = 0;
+			uint32_t acc_phase = 0;
+			const uint32_t idesc = FP8 ? umma_idesc_e4m3(PAIR_BM, BN) : umma_idesc_f16(PAIR_BM, BN);
+			for (int tile = cl; tile < total && ok; tile += ncl) {
+				if (!mbar_wait(&acce[acc], acc_phase ^ 1u)) { ok = false; break; }
+				tc_fence_after();
+				const uint32_t d_tmem = tmem_base + static_cast<uint32_t>(acc * BN);
+				for (int kc = 0; kc < p.num_kc; ++kc) {
+					if (!mbar_wait(&full[stage], phase)) { ok = false; break; }
+					tc_fence_after();
+					const uint64_t adesc = umma_desc_k_sw128(smem_u32(sA + stage * PAIR_HALF));
+					const uint64_t bdesc = umma_desc_k_sw128(smem_u32(sB + stage * PAIR_HALF));
+#pragma unroll
+					for (int kk = 0; kk < 4; ++kk) {
+						if (FP8)
+							umma_f8_pair(d_tmem, adesc + 2u * kk, bdesc + 2u * kk, idesc, (kc | kk) != 0 ? 1u : 0u);
+						else
+							umma_f16_pair(d_tmem, adesc + 2u * kk, bdesc + 2u * kk, idesc, (kc | kk) != 0 ? 1u : 0u);
+					}
+					umma_commit_pair_both(&empty[stage]);
+					if (++stage == NST) { stage = 0; phase ^= 1u; }
+				}
+				if (!ok) break;
+				umma_commit_pair_both(&accf[acc]);
+				if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+			}
+			// every MMA completes before the pair releases its shared and tensor memory
+			umma_commit_pair(drain);
+			if (!mbar_wait(drain, 0)) ok = false;
+			if (!ok) atomicOr(p.status, 1u);
+		}
+	} else {
+		// ---------------- FP16 deck epilogue (both CTAs, their own 128 rows) ----------------
+		constexpr int CPT = BN / DECK_CH;
+		const int q = warp & 3;
+		const int cw0 = ((warp - 2) >> 2) * DECK_CW;
+		const bool lead = (warp == 2 && lane == 0);
+		const int my_tiles = (cl < total) ? (total - cl + ncl - 1) / ncl : 0;
+		const int nseq = my_tiles * CPT;
+		const int r0 = static_cast<int>(rank) * BM;   // first tile row of this CTA
+		const uint32_t acce_leader[2] = {smem_peer_u32(&acce[0], 0), smem_peer_u32(&acce[1], 0)};
+		auto chunk_xy = [&](int sidx, int &x, int &y, bool &rows_in) {
+			int tm, tn;
+			tile_coords(cl + (sidx / CPT) * ncl, p.tiles_m, p.tiles_n, p.group_m, tm, tn);
+			x = p.crow0 + tm * PAIR_BM + r0;
+			y = p.ccol0 + tn * BN + (sidx % CPT) * DECK_CH;
+			rows_in = tm * PAIR_BM + r0 < p.m;
+		};
+		int issued = 0;
+		if (lead) {
+			for (; issued < DECK_BUFS - 1 && issued < nseq; ++issued) {
+				int x, y;
+				bool in;
+				chunk_xy(issued, x, y, in);
+				mbar_arrive_expect_tx(&dbar[issued % DECK_BUFS], DECK_CHUNK_BYTES);
+				tma_load_2d(dbuf + (issued % DECK_BUFS) * (BM * DECK_CH), &cmap, &dbar[issued % DECK_BUFS], x, y);
+			}
+		}
+		int acc = 0;
+		uint32_t acc_phase = 0;
+		int sidx = 0;
+		for (int it = 0; it < my_tiles && ok; ++it) {
+			int tm, tn;
+			tile_coords(cl + it * ncl, p.tiles_m, p.tiles_n, p.group_m, tm, tn);
+			ok = epi_all<NW>(mbar_wait(&accf[acc], acc_phase));
+			if (!ok) break;
+			tc_fence_after();
+			const uint32_t tbase = tmem_base + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(acc * BN);
+			float rf = p.dscale;
+			if (FP8) rf *= p.sl[(p.lrow0 + min(tm * PAIR_BM + r0 + q * 32 + lane, p.m - 1) - p.sl0) >> 7];
+#pragma unroll 1
+			for (int ch = 0; ch < CPT; ++ch, ++sidx) {
+				const int bi = sidx % DECK_BUFS;
+				ok = epi_all<NW>(mbar_wait(&dbar[bi], static_cast<uint32_t>((sidx / DECK_BUFS) & 1)));
+				if (!ok) break;
+#pragma unroll
+				for (int g = 0; g < DECK_CW / 32; ++g) {
+					const int cc = ch * DECK_CH + cw0 + 32 * g;
+					uint32_t r[32];
+					tmem_ld_32x32b_x32(tbase + static_cast<uint32_t>(cc), r);
+					__half *sb = dbuf + bi * (BM * DECK_CH) + (cw0 + 32 * g) * BM + q * 32 + lane;
+					float d[32];
+#pragma unroll
+					for (int j = 0; j < 32; ++j) d[j] = __half2float(sb[j * BM]);
+					float fu = rf, fl = 0.f;
+					const bool uni = FP8 ? col_factors(p, tn * BN + cc, lane, fu, fl) : true;
+					if (FP8 && uni) fu *= rf;
+					tmem_ld_wait();
+					if (uni) {
+#pragma unroll
+						for (int j = 0; j < 32; ++j) sb[j * BM] = __float2half_rn(d[j] - __uint_as_float(r[j]) * fu);
+					} else {
+#pragma unroll
+						for (int j = 0; j < 32; ++j) {
+							const float f = rf * __shfl_sync(0xffffffffu, fl, j);
+							sb[j * BM] = __float2half_rn(d[j] - __uint_as_float(r[j]) * f);
+						}
+					}
+				}
+				asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+				asm volatile("bar.sync 1, %0;" ::"n"(NW * 32) : "memory");
+				if (lead) {
+					int x, y;
+					bool in;
+					chunk_xy(sidx, x, y, in);
+					// a half tile wholly below the region's last row stores nothing
+					if (in) tma_store_2d(&cmap, dbuf + bi * (BM * DECK_CH), x, y);
+					asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+					if (issued < nseq) {
+						const int nb2 = issued % DECK_BUFS;
+						asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+						chunk_xy(issued, x, y, in);
+						mbar_arrive_expect_tx(&dbar[nb2], DECK_CHUNK_BYTES);
+						tma_load_2d(dbuf + nb2 * (BM * DECK_CH), &cmap, &dbar[nb2], x, y);
+						++issued;
+					}
+				}
+			}
+			if (!ok) break;
+			tc_fence_before();
+			__syncwarp();
+			if (lane == 0) mbar_arrive_cluster(acce_leader[acc]);
+			if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+		}
+		if (lead) {
+			asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+			for (int s2 = sidx; s2 < issued; ++s2)
+				(void)mbar_wait(&dbar[s2 % DECK_BUFS], static_cast<uint32_t>((s2 / DECK_BUFS) & 1));
+		}
+		if (lane == 0 && !ok) atomicOr(p.status, 1u);
+	}
+
+	__syncwarp();
+	tc_fence_before();
+	cluster_sync();
+	if (warp == 0 && lane == 0 && *static_cast<volatile unsigned *>(p.status)) {
+		// After a timeout, operand loads of either CTA may still be in flight
+		// (their completion is counted on the leader's barriers): give them
+		// 100 us to land before the pair's shared memory is released.
+		const uint64_t t0 = global_ns();
+		while (global_ns() - t0 < 100000ULL) {
+		}
+	}
+	cluster_sync();
+	if (warp == 1) {
+		tc_fence_after();
+		tmem_dealloc_pair(tmem_base, TMEM_COLS);
+	}
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
 	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -669,6 +931,8 @@ int schur_make_maps(SchurMaps *m, const uint16_t *lh, int lrows, int64_t ldl, co
 		static_cast<uint64_t>(ldl), BK, BM));
 	HPLAI_TRY(make_map_f16(m->umap, uh, static_cast<uint64_t>(k), static_cast<uint64_t>(urows),
 		static_cast<uint64_t>(ldu), BK, BN));
+	HPLAI_TRY(make_map_f16(m->umap2, uh, static_cast<uint64_t>(k), static_cast<uint64_t>(urows),
+		static_cast<uint64_t>(ldu), BK, BM));
 	m->k = k;
 	m->has_cmap = false;
 	return HPLAI_OK;
@@ -692,6 +956,40 @@ int set_smem_attr()
 	HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_kernel<EPI, FP8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 		static_cast<int>(smem_bytes(EPI))));
 	return HPLAI_OK;
+}
+
+// Off by default: in the solves the trailing update runs under the 1000 W
+// cap, where the pairs' lighter operand stream gave 2 % more throughput on
+// long leaf runs (32768^2 e4m3 deck, K = 2048: 2112 against 2064 TFLOP/s at
+// 1.27 against 1.24 GHz) but nothing measurable in a serial C3 solve, and
+// under look-ahead the pairs, which need two free SMs of one TPC, lost
+// 1 % to the side stream's scattered CTAs.
+std::atomic<int> g_pairs_default{0};
+
+// Shared memory of the pair kernel, and the most clusters of two that the
+// device keeps resident at once (the persistent pair kernel launches no more:
+// its clusters stride over the tiles and none waits for another).
+int pair_cluster_limit(int *limit)
+{
+	static DeviceOnce once;
+	return once.get([](int, int *v) -> int {
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_pair_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(pair_smem_bytes())));
+		HPLAI_CUDA_TRY(cudaFuncSetAttribute(schur_pair_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			static_cast<int>(pair_smem_bytes())));
+		cudaLaunchConfig_t cfg;
+		std::memset(&cfg, 0, sizeof cfg);
+		cfg.gridDim = dim3(2 * (num_sms() / 2), 1, 1);
+		cfg.blockDim = dim3(threads_for(2), 1, 1);
+		cfg.dynamicSmemBytes = pair_smem_bytes();
+		int n = 0;
+		if (cudaOccupancyMaxActiveClusters(&n, schur_pair_kernel<true>, &cfg) != cudaSuccess || n <= 0) {
+			(void)cudaGetLastError();
+			n = num_sms() / 2;
+		}
+		*v = n;
+		return HPLAI_OK;
+	}, limit);
 }
 
 // deck: C is the FP16 deck (c = its base, ldc its leading dimension in
@@ -756,6 +1054,34 @@ static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, in
 	// The store form writes whole 16-byte units of a column, so its region
 	// starts and ends on multiples of 4 rows; it needs the tall-box reduce path.
 	if (oscale && (fp8 || deck || epi != 1 || !TALL || (m % 4))) return HPLAI_EINVAL;
+	// 256-row tiles on CTA pairs for the updates of K >= 2048 (two-panel groups
+	// at b = 1024), where the single-CTA kernel's operand stream from L2 limits
+	// it (16384^2 e4m3 deck, short runs: 2518 against 2375 TFLOP/s); at
+	// K = 1024 the deck epilogue bounds both and the pairs' coupled tile steps
+	// measured 17 % slower (1506 against 1817 TFLOP/s)
+	if (epi == 2 && m > BM && maps.k >= 2048 && (maps.pairs > 0 || (maps.pairs < 0 && g_pairs_default.load() != 0))) {
+		p.tiles_m = (m + PAIR_BM - 1) / PAIR_BM;
+		const int ptotal = p.tiles_m * p.tiles_n;
+		int limit = 0;
+		HPLAI_TRY(pair_cluster_limit(&limit));
+		int ncl = ((max_ctas > 0 && max_ctas < num_sms()) ? max_ctas : num_sms()) / 2;
+		if (ncl > limit) ncl = limit;
+		if (ncl > ptotal) ncl = ptotal;
+		if (ncl >= 1) {
+			CUtensorMap lm, um, cm;
+			std::memcpy(&lm, maps.lmap, sizeof(lm));
+			std::memcpy(&um, maps.umap2, sizeof(um));
+			std::memcpy(&cm, cmap, sizeof(cm));
+			if (fp8)
+				schur_pair_kernel<true><<<2 * ncl, threads_for(2), pair_smem_bytes(), st>>>(lm, um, cm, p);
+			else
+				schur_pair_kernel<false><<<2 * ncl, threads_for(2), pair_smem_bytes(), st>>>(lm, um, cm, p);
+			count_launches();
+			HPLAI_CUDA_TRY(cudaGetLastError());
+			return HPLAI_OK;
+		}
+		p.tiles_m = (m + BM - 1) / BM;
+	}
 	static DeviceOnce attr;
 	HPLAI_TRY(attr.get([](int, int *) -> int {
 		HPLAI_TRY((set_smem_attr<0, false>()));
@@ -865,10 +1191,14 @@ int schur_make_maps_fp8(SchurMaps *m, const uint8_t *l8, int lrows, int64_t ldl,
 		static_cast<uint64_t>(lrows), static_cast<uint64_t>(ldl), 128, BM, CU_TENSOR_MAP_SWIZZLE_128B));
 	HPLAI_TRY(make_map_2d(m->umap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, u8, static_cast<uint64_t>(k),
 		static_cast<uint64_t>(urows), static_cast<uint64_t>(ldu), 128, BN, CU_TENSOR_MAP_SWIZZLE_128B));
+	HPLAI_TRY(make_map_2d(m->umap2, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, u8, static_cast<uint64_t>(k),
+		static_cast<uint64_t>(urows), static_cast<uint64_t>(ldu), 128, BM, CU_TENSOR_MAP_SWIZZLE_128B));
 	m->k = k;
 	m->has_cmap = false;
 	return HPLAI_OK;
 }
+
+void schur_set_pairs_default(bool on) { g_pairs_default.store(on ? 1 : 0); }
 
 int schur_status()
 {

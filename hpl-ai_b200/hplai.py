@@ -75,6 +75,7 @@ _autotune_trials = _proto("hplai_get_autotune_trials", _c_int, _vp, _vp, _vp, _v
                           ctypes.POINTER(_c_int))
 _set_tile_group = _proto("hplai_set_tile_group", _c_int, _vp, _c_int)
 _get_tile_group = _proto("hplai_get_tile_group", _c_int, _vp, ctypes.POINTER(_c_int))
+_set_cta_pairs = _proto("hplai_set_cta_pairs", _c_int, _vp, _c_int)
 _refine = _proto("hplai_refine", _c_int, _vp, _c_int, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
 _get_x = _proto("hplai_get_x", _c_int, _vp, _vp)
 _get_lu = _proto("hplai_get_lu", _c_int, _vp, _vp, _c_i64)
@@ -178,6 +179,11 @@ class RefineResult:
     status: int
 
 
+def set_cta_pairs_default(on: bool):
+    """The library default for deck updates on CTA pairs (contexts at -1 and the leaf calls)."""
+    check(_set_cta_pairs(None, 1 if on else 0), "hplai_set_cta_pairs")
+
+
 def higham_params(n: int, cond: float = 1000.0, rho: float = 0.5):
     """(alpha, beta) of Higham's HPL-AI matrix of order n."""
     a, b = ctypes.c_double(), ctypes.c_double()
@@ -267,6 +273,10 @@ class Solver:
         cnt = _c_int()
         check(_autotune_trials(self._h, fl, sd, tg, ms, cap, ctypes.byref(cnt)), "hplai_get_autotune_trials")
         return [(fl[i], sd[i], tg[i], ms[i]) for i in range(min(cnt.value, cap))]
+
+    def set_cta_pairs(self, on: int):
+        """Deck updates on CTA pairs (1), single CTAs (0) or the library default (-1)."""
+        check(_set_cta_pairs(self._h, on), "hplai_set_cta_pairs")
 
     def set_tile_group(self, group_m: int):
         check(_set_tile_group(self._h, group_m), "hplai_set_tile_group")

@@ -258,6 +258,16 @@ int hplai_get_autotune_trials(hplai_ctx *ctx, unsigned *flags, int *side_sms, in
 int hplai_set_tile_group(hplai_ctx *ctx, int group_m);
 int hplai_get_tile_group(hplai_ctx *ctx, int *group_m);
 
+/* The FP16-deck trailing update on CTA pairs: a cluster of two CTAs per
+ * 256 x 256 tile, the leader issuing tcgen05 MMAs of M = 256 (cta_group::2)
+ * over both CTAs' shared memory, so that each SM streams 32 KB of operands per
+ * stage instead of 48 KB.  on = 1 or 0 for the context (-1: follow the
+ * library default); with ctx = NULL, sets the library default (off at start),
+ * which the leaf calls (hplai_f8gemm_deck_minus, hplai_shgemm_deck_minus)
+ * follow.  Replaces nothing in the reference (its GEMM is a CPU kernel,
+ * kernels/avx2.cpp:82-302); a performance setting, results are unchanged. */
+int hplai_set_cta_pairs(hplai_ctx *ctx, int on);
+
 /* iterative_refinement (iterative_refinement.hpp:18-57) with maxit steps
  * (the driver uses 50).  Fills *err ({-1,-1} on failure) and *iters (the
  * number of residual evaluations).  Returns HPLAI_ENOTCONV on failure.
