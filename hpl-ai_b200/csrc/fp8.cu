@@ -18,6 +18,8 @@
 
 #include <cuda_fp8.h>
 
+#include <algorithm>
+
 namespace hplai {
 
 namespace {
@@ -25,19 +27,36 @@ namespace {
 constexpr float kE4M3Max = 448.f;
 
 // X (rows x kdim), element (r, k) at src[r + k*ld] (RCONTIG, column-major L
-// panel) or at src[k + r*ld] (the U panel read by columns).
+// panel) or at src[k + r*ld] (the U panel read by columns).  A CTA covers
+// 128 rows x 64 k with 16-byte loads along the contiguous index when vec
+// (src 16-byte aligned, ld and the contiguous extent multiples of 4).
 template <bool RCONTIG>
 __global__ void __launch_bounds__(256) amax_kernel(int rows, int kdim, const float *__restrict__ src, int64_t ld,
-	unsigned *__restrict__ bits)
+	unsigned *__restrict__ bits, int vec)
 {
 	const int r0 = blockIdx.x * 128, k0 = blockIdx.y * 64;
 	float m = 0.f;
-	for (int e = threadIdx.x; e < 128 * 64; e += 256) {
-		const int r = RCONTIG ? (e & 127) : (e >> 6), k = RCONTIG ? (e >> 7) : (e & 63);
-		if (r0 + r < rows && k0 + k < kdim) {
-			const float v = RCONTIG ? src[static_cast<int64_t>(k0 + k) * ld + r0 + r]
-			                        : src[static_cast<int64_t>(r0 + r) * ld + k0 + k];
-			m = fmaxf(m, fabsf(v));
+	if (vec) {
+#pragma unroll
+		for (int q = 0; q < 8; ++q) {
+			const int e = threadIdx.x + 256 * q;
+			// RCONTIG: 32 float4 along r per k; else 16 float4 along k per r
+			const int r = RCONTIG ? 4 * (e & 31) : (e >> 4), k = RCONTIG ? (e >> 5) : 4 * (e & 15);
+			if (r0 + r < rows && k0 + k < kdim) {
+				const float4 v = __ldg(reinterpret_cast<const float4 *>(
+					RCONTIG ? src + static_cast<int64_t>(k0 + k) * ld + r0 + r
+					        : src + static_cast<int64_t>(r0 + r) * ld + k0 + k));
+				m = fmaxf(m, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+			}
+		}
+	} else {
+		for (int e = threadIdx.x; e < 128 * 64; e += 256) {
+			const int r = RCONTIG ? (e & 127) : (e >> 6), k = RCONTIG ? (e >> 7) : (e & 63);
+			if (r0 + r < rows && k0 + k < kdim) {
+				const float v = RCONTIG ? src[static_cast<int64_t>(k0 + k) * ld + r0 + r]
+				                        : src[static_cast<int64_t>(r0 + r) * ld + k0 + k];
+				m = fmaxf(m, fabsf(v));
+			}
 		}
 	}
 	for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -67,43 +86,63 @@ __device__ __forceinline__ uint32_t pack_e4m3(float v0, float v1, float v2, floa
 	return lo | (hi << 16);
 }
 
-// L panel (element (r, k) at src[r + k*ld]): tile of 32 rows x 128 k loaded
-// coalesced along r, then 4 e4m3 bytes per thread written along k.  The 32
-// rows lie in one 128-row block: one factor per CTA.
-__global__ void __launch_bounds__(256) cast8_cols_kernel(int rows, int kdim, const float *__restrict__ src, int64_t ld,
-	const unsigned *__restrict__ bits, uint8_t *__restrict__ dst, int64_t ld8, float *__restrict__ scale)
+// L panel (element (r, k) at src[r + k*ld]): a CTA converts 64 rows (inside
+// one 128-row factor block: one factor per CTA) x 128 k.  The tile is read
+// along r, 256 bytes per column (16-byte loads when src, ld and rows allow
+// them), staged in shared memory and written along k, one warp per row's 128
+// bytes.  (32-row tiles, 128 bytes per column, ran at a quarter of the copy
+// bandwidth.)  Bytes past kdim up to kend are written as zeros.
+constexpr int kC8Rows = 64, kC8K = 128;
+__global__ void __launch_bounds__(256) cast8_cols_kernel(int rows, int kdim, int kend, const float *__restrict__ src,
+	int64_t ld, const unsigned *__restrict__ bits, uint8_t *__restrict__ dst, int64_t ld8, float *__restrict__ scale,
+	int vec)
 {
-	__shared__ float tile[32][129];
-	__shared__ float s_inv;
-	const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 128;
-	if (threadIdx.x == 0) {
-		const int ex = block_exponent(bits[r0 >> 7]);
-		s_inv = ldexpf(1.f, -ex);
-		if ((r0 & 127) == 0 && k0 == 0) scale[r0 >> 7] = ldexpf(1.f, ex);
-	}
-	for (int e = threadIdx.x; e < 32 * 128; e += 256) {
-		const int r = e & 31, k = e >> 5;
-		tile[r][k] = (r0 + r < rows && k0 + k < kdim) ? src[static_cast<int64_t>(k0 + k) * ld + r0 + r] : 0.f;
+	__shared__ float tile[kC8K][kC8Rows + 1];   // tile[k][r]
+	const int r0 = blockIdx.x * kC8Rows, k0 = blockIdx.y * kC8K;
+	const int ex = block_exponent(bits[r0 >> 7]);
+	const float inv = ldexpf(1.f, -ex);
+	if (threadIdx.x == 0 && (r0 & 127) == 0 && k0 == 0) scale[r0 >> 7] = ldexpf(1.f, ex);
+#pragma unroll
+	for (int q = 0; q < (kC8K * kC8Rows / 4) / 256; ++q) {
+		const int idx = threadIdx.x + 256 * q, kk = idx >> 4, rr = (idx & 15) * 4;
+		const int k = k0 + kk, r = r0 + rr;
+		float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+		if (k < kdim) {
+			const float *col = src + static_cast<int64_t>(k) * ld + r;
+			if (vec) {
+				if (r < rows) v = __ldg(reinterpret_cast<const float4 *>(col));
+			} else {
+				if (r < rows) v.x = col[0];
+				if (r + 1 < rows) v.y = col[1];
+				if (r + 2 < rows) v.z = col[2];
+				if (r + 3 < rows) v.w = col[3];
+			}
+		}
+		tile[kk][rr] = v.x;
+		tile[kk][rr + 1] = v.y;
+		tile[kk][rr + 2] = v.z;
+		tile[kk][rr + 3] = v.w;
 	}
 	__syncthreads();
-	const float inv = s_inv;
-	for (int e = threadIdx.x; e < 32 * 32; e += 256) {
-		const int r = e >> 5, w = e & 31;
-		const int row = r0 + r;
-		if (row >= rows || k0 + 4 * w >= ld8) continue;
-		*reinterpret_cast<uint32_t *>(dst + static_cast<int64_t>(row) * ld8 + k0 + 4 * w) =
-			pack_e4m3(tile[r][4 * w], tile[r][4 * w + 1], tile[r][4 * w + 2], tile[r][4 * w + 3], inv);
+#pragma unroll
+	for (int q = 0; q < (kC8K / 4 * kC8Rows) / 256; ++q) {
+		const int idx = threadIdx.x + 256 * q, rr = idx >> 5, w = idx & 31;
+		const int row = r0 + rr, k = k0 + 4 * w;
+		if (row < rows && k < kend)
+			*reinterpret_cast<uint32_t *>(dst + static_cast<int64_t>(row) * ld8 + k) =
+				pack_e4m3(tile[4 * w][rr], tile[4 * w + 1][rr], tile[4 * w + 2][rr], tile[4 * w + 3][rr], inv);
 	}
 }
 
 // U panel (element (r, k) at src[r*ld + k]): source and copy are both
 // contiguous along k, so each thread converts four consecutive k of a row
 // with no staging (16-byte loads when src and ld allow them).
-__global__ void __launch_bounds__(256) cast8_rows_kernel(int rows, int kdim, const float *__restrict__ src, int64_t ld,
-	const unsigned *__restrict__ bits, uint8_t *__restrict__ dst, int64_t ld8, float *__restrict__ scale, int vec)
+__global__ void __launch_bounds__(256) cast8_rows_kernel(int rows, int kdim, int kend, const float *__restrict__ src,
+	int64_t ld, const unsigned *__restrict__ bits, uint8_t *__restrict__ dst, int64_t ld8, float *__restrict__ scale,
+	int vec)
 {
 	const int k = 4 * (blockIdx.x * 256 + threadIdx.x);
-	if (k >= ld8) return;
+	if (k >= kend) return;
 	for (int r = blockIdx.y; r < rows; r += gridDim.y) {
 		const int ex = block_exponent(bits[r >> 7]);
 		const float inv = ldexpf(1.f, -ex);
@@ -128,21 +167,26 @@ __global__ void __launch_bounds__(256) cast8_rows_kernel(int rows, int kdim, con
 
 template <bool RCONTIG>
 int quantize(int rows, int kdim, const float *src, int64_t ld, unsigned *bits, uint8_t *dst, int64_t ld8,
-	float *scale, cudaStream_t st)
+	float *scale, cudaStream_t st, bool pad_row)
 {
 	if (rows <= 0) return HPLAI_OK;
 	const int nblk = (rows + 127) / 128;
+	const bool aligned = (reinterpret_cast<uintptr_t>(src) & 15u) == 0 && (ld & 3) == 0;
 	HPLAI_CUDA_TRY(cudaMemsetAsync(bits, 0, sizeof(unsigned) * nblk, st));
-	amax_kernel<RCONTIG><<<dim3(nblk, (kdim + 63) / 64), 256, 0, st>>>(rows, kdim, src, ld, bits);
+	amax_kernel<RCONTIG><<<dim3(nblk, (kdim + 63) / 64), 256, 0, st>>>(rows, kdim, src, ld, bits,
+		(aligned && (RCONTIG ? rows : kdim) % 4 == 0) ? 1 : 0);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
+	// the Schur kernel reads the copy in 128-byte K chunks: zeros up to the
+	// chunk's end (pad_row: up to ld8)
+	const int kend = pad_row ? static_cast<int>(ld8) : static_cast<int>(std::min<int64_t>(ld8, (kdim + 127) / 128 * 128));
 	if (RCONTIG) {
-		cast8_cols_kernel<<<dim3((rows + 31) / 32, static_cast<unsigned>((ld8 + 127) / 128)), 256, 0, st>>>(rows, kdim,
-			src, ld, bits, dst, ld8, scale);
+		const int vec = (aligned && rows % 4 == 0) ? 1 : 0;
+		cast8_cols_kernel<<<dim3((rows + kC8Rows - 1) / kC8Rows, static_cast<unsigned>((kend + kC8K - 1) / kC8K)), 256, 0,
+			st>>>(rows, kdim, kend, src, ld, bits, dst, ld8, scale, vec);
 	} else {
-		const int vec = ((reinterpret_cast<uintptr_t>(src) & 15u) == 0 && (ld & 3) == 0) ? 1 : 0;
-		cast8_rows_kernel<<<dim3(static_cast<unsigned>((ld8 / 4 + 255) / 256), static_cast<unsigned>(rows < 8192 ? rows : 8192)),
-			256, 0, st>>>(rows, kdim, src, ld, bits, dst, ld8, scale, vec);
+		cast8_rows_kernel<<<dim3(static_cast<unsigned>((kend / 4 + 255) / 256), static_cast<unsigned>(rows < 8192 ? rows : 8192)),
+			256, 0, st>>>(rows, kdim, kend, src, ld, bits, dst, ld8, scale, aligned ? 1 : 0);
 	}
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
@@ -152,17 +196,17 @@ int quantize(int rows, int kdim, const float *src, int64_t ld, unsigned *bits, u
 } // namespace
 
 int launch_quantize_lpanel(int rows, int b, const float *acol, int64_t lda, unsigned *bits, uint8_t *l8, int64_t ld8,
-	float *scale, cudaStream_t st)
+	float *scale, cudaStream_t st, bool pad_row)
 {
 	if (ld8 % 128) return HPLAI_EINVAL;
-	return quantize<true>(rows, b, acol, lda, bits, l8, ld8, scale, st);
+	return quantize<true>(rows, b, acol, lda, bits, l8, ld8, scale, st, pad_row);
 }
 
 int launch_quantize_upanel(int cols, int b, const float *arow, int64_t lda, unsigned *bits, uint8_t *u8, int64_t ld8,
-	float *scale, cudaStream_t st)
+	float *scale, cudaStream_t st, bool pad_row)
 {
 	if (ld8 % 128) return HPLAI_EINVAL;
-	return quantize<false>(cols, b, arow, lda, bits, u8, ld8, scale, st);
+	return quantize<false>(cols, b, arow, lda, bits, u8, ld8, scale, st, pad_row);
 }
 
 namespace {
@@ -206,6 +250,6 @@ extern "C" int hplai_quantize_e4m3(int rows, int k, const float *src, int64_t ld
 	if (reinterpret_cast<uintptr_t>(dst) % 16) return HPLAI_EINVAL;   // rows are written as 4-byte words
 	if (col_major ? lds < rows : lds < k) return HPLAI_EINVAL;
 	cudaStream_t st = static_cast<cudaStream_t>(stream);
-	return col_major ? hplai::launch_quantize_lpanel(rows, k, src, lds, bits, dst, ld8, scale, st)
-	                 : hplai::launch_quantize_upanel(rows, k, src, lds, bits, dst, ld8, scale, st);
+	return col_major ? hplai::launch_quantize_lpanel(rows, k, src, lds, bits, dst, ld8, scale, st, true)
+	                 : hplai::launch_quantize_upanel(rows, k, src, lds, bits, dst, ld8, scale, st, true);
 }

@@ -184,10 +184,12 @@ void tc_status_reset();
 // U panel (read by columns), row-major with K contiguous (ld8 a multiple of
 // 128 bytes), and one power-of-two factor per 128 rows/columns in `scale`
 // (block 0 = the first row).  `bits` is rows/128 + 1 words of scratch.
+// Row bytes past b are zero up to the next multiple of 128 (the Schur
+// kernel's K chunk), or up to ld8 with pad_row.
 int launch_quantize_lpanel(int rows, int b, const float *acol, int64_t lda, unsigned *bits, uint8_t *l8, int64_t ld8,
-	float *scale, cudaStream_t st);
+	float *scale, cudaStream_t st, bool pad_row = false);
 int launch_quantize_upanel(int cols, int b, const float *arow, int64_t lda, unsigned *bits, uint8_t *u8, int64_t ld8,
-	float *scale, cudaStream_t st);
+	float *scale, cudaStream_t st, bool pad_row = false);
 
 // A[i][j] += deck[i][j] * inv_scale on rows [r0, r1) x cols [c0, c1) (FP16 deck, ld ldd)
 int launch_deck_apply(int r0, int r1, int c0, int c1, float *a, int64_t lda, const void *deck, int64_t ldd,
