@@ -407,19 +407,22 @@ __device__ __forceinline__ void umma_f8_pair(uint32_t d_tmem, uint64_t adesc, ui
 		: "memory");
 }
 
-// Arrive on the mbarrier at this shared-memory offset in both CTAs of the
-// pair once the pair's previously issued MMAs have completed.
-__device__ __forceinline__ void umma_commit_pair_both(uint64_t *bar)
-{
-	asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
-		::"r"(smem_u32(bar)), "h"(static_cast<uint16_t>(3)) : "memory");
-}
-
-// The same, on this CTA's mbarrier only.
-__device__ __forceinline__ void umma_commit_pair(uint64_t *bar)
+// Arrive on an mbarrier (shared::cluster address: this CTA's or the peer's)
+// once the pair's previously issued MMAs have completed.
+__device__ __forceinline__ void umma_commit_pair_at(uint32_t bar)
 {
 	asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-		::"r"(smem_u32(bar)) : "memory");
+		::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void umma_commit_pair(uint64_t *bar) { umma_commit_pair_at(smem_u32(bar)); }
+
+// The same on the mbarrier at this shared-memory offset in both CTAs of the
+// pair (two commits, one per CTA).
+__device__ __forceinline__ void umma_commit_pair_both(uint64_t *bar)
+{
+	umma_commit_pair_at(smem_peer_u32(bar, 0));
+	umma_commit_pair_at(smem_peer_u32(bar, 1));
 }
 
 // Memory-model helpers for flags exchanged between CTAs of one launch.
