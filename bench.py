@@ -220,8 +220,9 @@ def schur_algorithmic(n, b, panel_bytes=2, c_bytes=8, group=1):
     in the order hplai_factor issues them.  The update by a group of `group`
     panels (K = group * b) of the trailing matrix from block e on is split
     into the next group's block columns, its block rows and the rest; with
-    two-panel groups a group's second block first receives its first panel's
-    update alone (K = b).  A region of m x n C elements with panel width K
+    panel groups a group's block e + j first receives the updates of the
+    group's panels e .. e + j - 1, each alone (K = b).  A region of m x n C
+    elements with panel width K
     does 2 m n K flops and moves c_bytes per C element (8: FP32 read +
     write; 4: the FP16 deck) plus (m + n) K panel elements of panel_bytes
     (2 for FP16, 1 for e4m3)."""
@@ -235,12 +236,13 @@ def schur_algorithmic(n, b, panel_bytes=2, c_bytes=8, group=1):
         acc["bytes"] += float(c_bytes) * m * nn + float(panel_bytes) * (m + nn) * k
         acc["launches"] += 1
 
-    def first_panel_update(j):
-        region(n - j * b, b, b)
-        region(b, n - (j + 1) * b, b)
+    def panel_updates(j, first):
+        for _ in range(j - first):
+            region(n - j * b, b, b)
+            region(b, n - (j + 1) * b, b)
 
     for j in range(1, min(group, nb)):
-        first_panel_update(j)
+        panel_updates(j, 0)
     s = 0
     while s + group < nb:
         e = s + group
@@ -249,7 +251,7 @@ def schur_algorithmic(n, b, panel_bytes=2, c_bytes=8, group=1):
         region(n - r1, r2 - r1, k)
         region(r2 - r1, n - r2, k)
         for j in range(e + 1, e + ne):
-            first_panel_update(j)
+            panel_updates(j, e)
         region(n - r2, n - r2, k)
         s += group
     return acc["flops"], acc["bytes"], acc["launches"]
@@ -359,27 +361,43 @@ class FormRun:
             flags |= hplai.FLAG_LAZY_A
         if group == 2:
             flags |= hplai.FLAG_GROUP2
-        self.s = hplai.Solver(n, b, precision=hplai.F32_F8 if self.fp8 else hplai.F32_F16, flags=flags)
+        elif group == 4:
+            flags |= hplai.FLAG_GROUP4
+        prec = hplai.F32_F8 if self.fp8 else hplai.F32_F16
+        self.s = None
+        if autotune and b % 128 == 0 and group != 4:
+            # buffers for four-panel groups, so that the tuner can choose them
+            # (skipped when they do not fit)
+            try:
+                self.s = hplai.Solver(n, b, precision=prec, flags=flags | hplai.FLAG_GROUP4)
+                self.s.set_schedule(flags & (hplai.FLAG_LOOKAHEAD | hplai.FLAG_GROUP2), side_sms)
+            except hplai.HplaiError:
+                self.s = None
+        if self.s is None:
+            self.s = hplai.Solver(n, b, precision=prec, flags=flags)
         if matrix == "higham":
             self.s.set_matrix(hplai.MATRIX_HIGHAM, 1000.0, 0.5)
         self.ext = torch.cuda.ExternalStream(self.s.stream())
         self.barrier = barrier
         self.tuned = None
-        self.group = 2 if (flags & hplai.FLAG_GROUP2) else 1
+        def group_of(f):
+            return 4 if (f & hplai.FLAG_GROUP4) else 2 if (f & hplai.FLAG_GROUP2) else 1
+        self.group = group_of(flags)
+        sched_bits = hplai.FLAG_LOOKAHEAD | hplai.FLAG_GROUP2 | hplai.FLAG_GROUP4
         if lookahead:
-            self.s.set_schedule(flags & (hplai.FLAG_LOOKAHEAD | hplai.FLAG_GROUP2), side_sms)
+            self.s.set_schedule(flags & sched_bits, side_sms)
         self.schedule = {"lookahead": bool(lookahead), "side_sms": side_sms if lookahead else None,
                          "panels_per_update": self.group, "source": "flags"}
         if autotune:
             # outside the timed region: time the factorisation under each schedule, keep the fastest
             tflags, tside, tms = self.s.autotune(seed)
             la = bool(tflags & hplai.FLAG_LOOKAHEAD)
-            self.group = 2 if (tflags & hplai.FLAG_GROUP2) else 1
+            self.group = group_of(tflags)
             def side_desc(f, sd):
                 if not (f & hplai.FLAG_LOOKAHEAD):
                     return None
                 return sd if sd > 0 else f"share sms*c/(r+c), c={-sd} panels, r = trailing block columns"
-            trials = [{"panels_per_update": 2 if (f & hplai.FLAG_GROUP2) else 1,
+            trials = [{"panels_per_update": group_of(f),
                        "lookahead": bool(f & hplai.FLAG_LOOKAHEAD), "side_sms": side_desc(f, sd),
                        "tile_group": tg, "factor_ms": round(ms, 2)} for f, sd, tg, ms in self.s.autotune_trials()]
             self.tuned = {"factor_ms": tms, "trials_warmup_first": trials}
@@ -900,8 +918,9 @@ def main():
                          "(the default for the solve workload unless --lookahead or --no-autotune is given)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the serial schedule (or --lookahead's)")
     ap.add_argument("--side-sms", type=int, default=32, help="SMs of the side stream with --lookahead (no autotune)")
-    ap.add_argument("--group", type=int, choices=(1, 2), default=1,
-                    help="panels per trailing update without autotuning (2 = HPLAI_FLAG_GROUP2, b %% 128 == 0)")
+    ap.add_argument("--group", type=int, choices=(1, 2, 4), default=1,
+                    help="panels per trailing update without autotuning (2 = HPLAI_FLAG_GROUP2, 4 = HPLAI_FLAG_GROUP4; "
+                         "b %% 128 == 0)")
     ap.add_argument("--lookahead", action="store_true",
                     help="form the next step's diagonal block and panels on a side stream (HPLAI_FLAG_LOOKAHEAD)")
     ap.add_argument("--refine", choices=("ir", "gmres"), default=None,

@@ -55,27 +55,30 @@ struct hplai_ctx {
 	int64_t lda = 0, ldh = 0;
 	float *A = nullptr;
 	// Panel copies for the trailing updates.  A group of `group` consecutive
-	// panels (1, or 2 with HPLAI_FLAG_GROUP2) updates the trailing matrix in
-	// one pass with K = group * b (C -= [L_k L_k+1] [U_k; U_k+1]), which halves
-	// the passes over the trailing matrix.  FP16 group buffers, double
+	// panels (1, 2 with HPLAI_FLAG_GROUP2, 4 with HPLAI_FLAG_GROUP4) updates
+	// the trailing matrix in one pass with K = group * b
+	// (C -= [L_k .. L_k+g-1] [U_k; ..; U_k+g-1]), which divides the passes over
+	// the trailing matrix by the group size.  FP16 group buffers, double
 	// buffered (the next group is formed on the side stream while the main
 	// stream's update still reads the current one): row i of Lh[q] holds row i
 	// of the group's L panels side by side (slot h at column h * ldh, row
 	// pitch ldg = gcap * ldh), row j of Uh[q] column j of its U panels (the
 	// reference's nbuf = 2 rotating LRPanels, panel.hpp:236-268).
+	static constexpr int kMaxGroup = 4;
 	int group = 1, gcap = 1;      // panels per update now / that the buffers hold
 	int64_t ldg = 0;
 	uint16_t *Lh[2] = {nullptr, nullptr}, *Uh[2] = {nullptr, nullptr};
-	SchurMaps maps[2][2];         // [buffer][slot]: one panel, K = b
-	SchurMaps mapsg[2];           // [buffer]: both slots, K = 2b (gcap 2)
+	SchurMaps maps[2][kMaxGroup]; // [buffer][slot]: one panel, K = b
+	SchurMaps mapsg[2][2];        // [buffer][0: K = 2b, 1: K = 4b]: the group's slots together
 	// precision form: e4m3 group copies with one power-of-two factor per 128
 	// rows shared by the group's panels (row pitch ld8g = gcap * ld8), and,
-	// for the update of a group's second block by its first panel alone, an
-	// e4m3 copy of that panel (L8s, U8s)
+	// for the updates of a group's later blocks by its earlier panels (block
+	// e + j receives panels e .. e + j - 1 before it is factored), an e4m3
+	// copy of each panel but the group's last (L8s[h], U8s[h] for slot h)
 	uint8_t *L8[2] = {nullptr, nullptr}, *U8[2] = {nullptr, nullptr};
 	float *sl[2] = {nullptr, nullptr}, *su[2] = {nullptr, nullptr};
-	uint8_t *L8s = nullptr, *U8s = nullptr;
-	float *sls = nullptr, *sus = nullptr;
+	uint8_t *L8s[kMaxGroup - 1] = {}, *U8s[kMaxGroup - 1] = {};
+	float *sls[kMaxGroup - 1] = {}, *sus[kMaxGroup - 1] = {};
 	unsigned *qbits = nullptr;
 	int64_t ld8 = 0, ld8g = 0;
 	// HPLAI_FLAG_FP16_DECK: FP16 trailing-update deck (n x lda halves), holding
@@ -100,8 +103,8 @@ struct hplai_ctx {
 	int matrix = HPLAI_MATRIX_LCG;
 	double h_alpha = 0.0, h_beta = 0.0;
 	SchurMaps maps8[2];           // [buffer]: K = b
-	SchurMaps maps8g[2];          // [buffer]: K = 2b (gcap 2)
-	SchurMaps maps8s;             // the single panel copy, K = b
+	SchurMaps maps8g[2][2];       // [buffer][0: K = 2b, 1: K = 4b]
+	SchurMaps maps8s[kMaxGroup - 1];   // the single panel copies, K = b
 	TcPanels tc;
 	float *tcbuf = nullptr;   // phi, plo (n x ldp), the four b x ldp inverse buffers, the inversion work
 	double *rhs = nullptr, *d = nullptr, *x = nullptr, *r = nullptr, *scal = nullptr;
@@ -165,10 +168,12 @@ int ctx_free(hplai_ctx *c)
 		cudaFree(c->sl[i]);
 		cudaFree(c->su[i]);
 	}
-	cudaFree(c->L8s);
-	cudaFree(c->U8s);
-	cudaFree(c->sls);
-	cudaFree(c->sus);
+	for (int h = 0; h < hplai_ctx::kMaxGroup - 1; ++h) {
+		cudaFree(c->L8s[h]);
+		cudaFree(c->U8s[h]);
+		cudaFree(c->sls[h]);
+		cudaFree(c->sus[h]);
+	}
 	cudaFree(c->qbits);
 	if (!c->deck_aliased) cudaFree(c->deck);
 	cudaFree(c->dstage);
@@ -305,9 +310,10 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	if (n <= 0 || b < 16 || b > 1024 || n % b) return HPLAI_EINVAL;
 	if (precision != HPLAI_F32_F16 && precision != HPLAI_F32_F8) return HPLAI_EUNSUPPORTED;
 	if ((flags & HPLAI_FLAG_FP16_DECK) && (b % 8)) return HPLAI_EINVAL;
-	if ((flags & HPLAI_FLAG_GROUP2) && (b % 128)) return HPLAI_EINVAL;
-	if ((flags & HPLAI_FLAG_REF_DECK) &&
-		(precision != HPLAI_F32_F16 || (flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_LOOKAHEAD))))
+	if ((flags & (HPLAI_FLAG_GROUP2 | HPLAI_FLAG_GROUP4)) && (b % 128)) return HPLAI_EINVAL;
+	if ((flags & HPLAI_FLAG_GROUP2) && (flags & HPLAI_FLAG_GROUP4)) return HPLAI_EINVAL;
+	if ((flags & HPLAI_FLAG_REF_DECK) && (precision != HPLAI_F32_F16 ||
+		(flags & (HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_GROUP4 | HPLAI_FLAG_LOOKAHEAD))))
 		return HPLAI_EINVAL;
 	if ((flags & HPLAI_FLAG_REF_BACKBUF) && !(flags & HPLAI_FLAG_REF_DECK)) return HPLAI_EINVAL;
 	// A regenerated at panel time: the precision form's FP16 panel copies fold it in
@@ -324,9 +330,10 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 	// power-of-two stride (the reference's calc_lda_c, panel.hpp:10-18, for HBM).
 	c->lda = round_up(n, 64) + 64;
 	c->ldh = round_up(b, 64);
-	// two-panel groups need whole 128-byte e4m3 rows and 64-half FP16 rows per panel
-	c->gcap = (b % 128 == 0) ? 2 : 1;
-	c->group = (flags & HPLAI_FLAG_GROUP2) ? 2 : 1;
+	// panel groups need whole 128-byte e4m3 rows and 64-half FP16 rows per
+	// panel; buffers for four panels only when asked for (HPLAI_FLAG_GROUP4)
+	c->gcap = (b % 128 == 0) ? ((flags & HPLAI_FLAG_GROUP4) ? 4 : 2) : 1;
+	c->group = (flags & HPLAI_FLAG_GROUP4) ? 4 : (flags & HPLAI_FLAG_GROUP2) ? 2 : 1;
 	c->ldg = c->gcap * c->ldh;
 	{
 		int lo = 0, hi = 0;
@@ -358,11 +365,11 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 			CTX_ALLOC(c->sl[i], sizeof(float) * nblk128);
 			CTX_ALLOC(c->su[i], sizeof(float) * nblk128);
 		}
-		if (c->gcap == 2) {
-			CTX_ALLOC(c->L8s, static_cast<size_t>(c->ld8) * n);
-			CTX_ALLOC(c->U8s, static_cast<size_t>(c->ld8) * n);
-			CTX_ALLOC(c->sls, sizeof(float) * nblk128);
-			CTX_ALLOC(c->sus, sizeof(float) * nblk128);
+		for (int h = 0; h < c->gcap - 1; ++h) {
+			CTX_ALLOC(c->L8s[h], static_cast<size_t>(c->ld8) * n);
+			CTX_ALLOC(c->U8s[h], static_cast<size_t>(c->ld8) * n);
+			CTX_ALLOC(c->sls[h], sizeof(float) * nblk128);
+			CTX_ALLOC(c->sus[h], sizeof(float) * nblk128);
 		}
 		CTX_ALLOC(c->qbits, sizeof(unsigned) * nblk128);
 	}
@@ -423,22 +430,26 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 			s = schur_make_maps(&c->maps[i][h], c->Lh[i] + h * c->ldh, n, c->ldg, c->Uh[i] + h * c->ldh, n, c->ldg, b);
 			finish(c->maps[i][h]);
 		}
-		if (s == HPLAI_OK && c->gcap == 2) {
-			s = schur_make_maps(&c->mapsg[i], c->Lh[i], n, c->ldg, c->Uh[i], n, c->ldg, 2 * b);
-			finish(c->mapsg[i]);
+		for (int g = 0; g < 2 && s == HPLAI_OK; ++g) {
+			const int gk = 2 << g;   // panels of the group: 2, 4
+			if (gk > c->gcap) break;
+			s = schur_make_maps(&c->mapsg[i][g], c->Lh[i], n, c->ldg, c->Uh[i], n, c->ldg, gk * b);
+			finish(c->mapsg[i][g]);
 		}
 		if (s == HPLAI_OK && precision == HPLAI_F32_F8) {
 			s = schur_make_maps_fp8(&c->maps8[i], c->L8[i], n, c->ld8g, c->U8[i], n, c->ld8g, b);
 			finish(c->maps8[i]);
-			if (s == HPLAI_OK && c->gcap == 2) {
-				s = schur_make_maps_fp8(&c->maps8g[i], c->L8[i], n, c->ld8g, c->U8[i], n, c->ld8g, 2 * b);
-				finish(c->maps8g[i]);
+			for (int g = 0; g < 2 && s == HPLAI_OK; ++g) {
+				const int gk = 2 << g;
+				if (gk > c->gcap) break;
+				s = schur_make_maps_fp8(&c->maps8g[i][g], c->L8[i], n, c->ld8g, c->U8[i], n, c->ld8g, gk * b);
+				finish(c->maps8g[i][g]);
 			}
 		}
 	}
-	if (s == HPLAI_OK && precision == HPLAI_F32_F8 && c->gcap == 2) {
-		s = schur_make_maps_fp8(&c->maps8s, c->L8s, n, c->ld8, c->U8s, n, c->ld8, b);
-		finish(c->maps8s);
+	for (int h = 0; h < c->gcap - 1 && s == HPLAI_OK && precision == HPLAI_F32_F8; ++h) {
+		s = schur_make_maps_fp8(&c->maps8s[h], c->L8s[h], n, c->ld8, c->U8s[h], n, c->ld8, b);
+		finish(c->maps8s[h]);
 	}
 	if (s == HPLAI_OK) {
 		float *base = c->tcbuf;
@@ -517,9 +528,10 @@ bool f16_panel_form(const hplai_ctx *c, bool simt)
 // FP16 copies in slot `slot` of group buffer `buf` (getrf_nopiv +
 // update_left/right_panels + convert_left/right_panels,
 // panel_trf.hpp:143-233).  Precision form: the e4m3 copies for the next
-// update that reads this panel -- with one-panel groups this panel's own, in
-// a group's first slot the single copy for the update of the group's second
-// block, in its second slot the group's shared copy of both panels.
+// update that reads this panel -- with one-panel groups this panel's own; in
+// a group's earlier slots the panel's single copy, for the updates of the
+// group's later blocks; in its last slot the group's shared copy of all its
+// panels.
 int panel_step(hplai_ctx *c, int k, int buf, int slot, bool simt, int side_ctas, cudaStream_t st, PhaseEvents &pe)
 {
 	const int n = c->n, b = c->b;
@@ -576,22 +588,26 @@ int panel_step(hplai_ctx *c, int k, int buf, int slot, bool simt, int side_ctas,
 		HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, uh, ldg, 1.0f, side_ctas, st));
 	}
 	if (c->precision == HPLAI_F32_F8) {
-		if (c->group == 1) {
+		const int G = c->group;
+		if (G == 1) {
 			HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, c->qbits, c->L8[buf] + (kb + b) * c->ld8g, c->ld8g,
 				c->sl[buf], st));
 			HPLAI_TRY(launch_quantize_upanel(rem, b, diag + static_cast<int64_t>(b) * lda, lda, c->qbits,
 				c->U8[buf] + (kb + b) * c->ld8g, c->ld8g, c->su[buf], st));
-		} else if (slot == 0) {
-			HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, c->qbits, c->L8s + (kb + b) * c->ld8, c->ld8, c->sls,
-				st));
+		} else if (slot < G - 1) {
+			// the panel alone, for the updates of the group's later blocks
+			HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, c->qbits, c->L8s[slot] + (kb + b) * c->ld8, c->ld8,
+				c->sls[slot], st));
 			HPLAI_TRY(launch_quantize_upanel(rem, b, diag + static_cast<int64_t>(b) * lda, lda, c->qbits,
-				c->U8s + (kb + b) * c->ld8, c->ld8, c->sus, st));
+				c->U8s[slot] + (kb + b) * c->ld8, c->ld8, c->sus[slot], st));
 		} else {
-			// [L_k-1 L_k] (rows kb+b.., A columns kb-b .. kb+b-1) and [U_k-1; U_k]
-			// (A rows kb-b .. kb+b-1, columns kb+b..) with factors over both panels
-			HPLAI_TRY(launch_quantize_lpanel(rem, 2 * b, diag + b - static_cast<int64_t>(b) * lda, lda, c->qbits,
+			// the group's last panel: [L_k-G+1 .. L_k] (rows kb+b.., A columns
+			// kb-(G-1)b .. kb+b-1) and [U_k-G+1; ..; U_k] (A rows kb-(G-1)b ..
+			// kb+b-1, columns kb+b..) with factors over all the group's panels
+			const int64_t back = static_cast<int64_t>(G - 1) * b;
+			HPLAI_TRY(launch_quantize_lpanel(rem, G * b, diag + b - back * lda, lda, c->qbits,
 				c->L8[buf] + (kb + b) * c->ld8g, c->ld8g, c->sl[buf], st));
-			HPLAI_TRY(launch_quantize_upanel(rem, 2 * b, diag - b + static_cast<int64_t>(b) * lda, lda, c->qbits,
+			HPLAI_TRY(launch_quantize_upanel(rem, G * b, diag - back + static_cast<int64_t>(b) * lda, lda, c->qbits,
 				c->U8[buf] + (kb + b) * c->ld8g, c->ld8g, c->su[buf], st));
 		}
 	}
@@ -633,45 +649,48 @@ Operands group_operands(const hplai_ctx *c, int q, int e)
 {
 	Operands op;
 	op.fp8 = c->precision == HPLAI_F32_F8;
+	const int g = c->group == 4 ? 1 : 0;
 	if (op.fp8) {
-		op.m = c->group == 2 ? &c->maps8g[q] : &c->maps8[q];
+		op.m = c->group > 1 ? &c->maps8g[q][g] : &c->maps8[q];
 		op.sl = c->sl[q];
 		op.su = c->su[q];
 		op.s0 = e * c->b;
 	} else {
-		op.m = c->group == 2 ? &c->mapsg[q] : &c->maps[q][0];
+		op.m = c->group > 1 ? &c->mapsg[q][g] : &c->maps[q][0];
 	}
 	return op;
 }
 
-// The operands of the update of a group's second block by its first panel
-// alone (panel e in slot 0 of buffer q).
-Operands first_panel_operands(const hplai_ctx *c, int q, int e)
+// The operands of the update by one panel of a group alone: the panel in
+// slot h of buffer q, of the group whose first block is e (its e4m3 copy's
+// rows start below its own block, at (e + h + 1) b).
+Operands slot_operands(const hplai_ctx *c, int q, int e, int h)
 {
 	Operands op;
 	op.fp8 = c->precision == HPLAI_F32_F8;
 	if (op.fp8) {
-		op.m = &c->maps8s;
-		op.sl = c->sls;
-		op.su = c->sus;
-		op.s0 = (e + 1) * c->b;
+		op.m = &c->maps8s[h];
+		op.sl = c->sls[h];
+		op.su = c->sus[h];
+		op.s0 = (e + h + 1) * c->b;
 	} else {
-		op.m = &c->maps[q][0];
+		op.m = &c->maps[q][h];
 	}
 	return op;
 }
 
 // Everything block j needs before it is factored, on the side stream: with
-// two-panel groups the update of a group's second block by the group's first
-// panel; then, with the FP16 deck, the deck folded into the block column and
+// panel groups the updates of the group's block j by the group's earlier
+// panels (first .. j-1, each alone); then, with the FP16 deck, the deck folded into the block column and
 // row (A + deck / dscale; the FP16 panel copies fold the off-diagonal part
 // themselves, so then only the diagonal block).
 int prepare_block(hplai_ctx *c, int j, int first, int q, bool simt, int side_ctas, cudaStream_t st, PhaseEvents &pe)
 {
 	const int n = c->n, b = c->b;
 	const int r1 = j * b, r2 = (j + 1) * b;
-	if (j > first) {
-		const Operands op = first_panel_operands(c, q, first);
+	// the updates of block j by the group's earlier panels, in panel order
+	for (int h = 0; h < j - first; ++h) {
+		const Operands op = slot_operands(c, q, first, h);
 		HPLAI_TRY(schur_region(c, op, r1, n, r1, r2, side_ctas, st, pe));
 		HPLAI_TRY(schur_region(c, op, r1, r2, r2, n, side_ctas, st, pe));
 	}
@@ -781,7 +800,9 @@ int factor_impl(hplai_ctx *c, int kend, const float *host_a = nullptr, int64_t h
 	if (!c->have_inputs) return HPLAI_ESTATE;
 	if (c->flags & HPLAI_FLAG_REF_DECK) return factor_refdeck(c, kend);
 	const int n = c->n, b = c->b, nb = c->nb;
-	c->group = ((c->flags & HPLAI_FLAG_GROUP2) && c->gcap == 2 && kend >= nb) ? 2 : 1;
+	c->group = kend < nb ? 1
+		: ((c->flags & HPLAI_FLAG_GROUP4) && c->gcap >= 4) ? 4
+		: ((c->flags & HPLAI_FLAG_GROUP2) && c->gcap >= 2) ? 2 : 1;
 	const int G = c->group;
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->kstatus, 0, 2 * sizeof(unsigned), c->st));
 	if (c->deck_aliased)
@@ -1205,18 +1226,25 @@ int hplai_ctx_solve_stream_rhs(hplai_ctx *c, int col, double *x, int maxit, hpla
 // trial is kept for hplai_get_autotune_log.
 namespace {
 
+// Every set of Schur maps of the context.
+template <class F>
+void for_each_maps(hplai_ctx *c, F &&f)
+{
+	for (int i = 0; i < 2; ++i) {
+		for (auto &m : c->maps[i]) f(m);
+		for (auto &m : c->mapsg[i]) f(m);
+		f(c->maps8[i]);
+		for (auto &m : c->maps8g[i]) f(m);
+	}
+	for (auto &m : c->maps8s) f(m);
+}
+
 // The tile order of every Schur launch of the context (trailing updates and
 // panel products): groups of `gm` tile rows (0: the kernel's default).
 void apply_tile_group(hplai_ctx *c, int gm)
 {
 	c->tile_group = gm;
-	for (int i = 0; i < 2; ++i) {
-		for (auto &m : c->maps[i]) m.group_m = gm;
-		c->mapsg[i].group_m = gm;
-		c->maps8[i].group_m = gm;
-		c->maps8g[i].group_m = gm;
-	}
-	c->maps8s.group_m = gm;
+	for_each_maps(c, [gm](SchurMaps &m) { m.group_m = gm; });
 }
 
 } // namespace
@@ -1238,13 +1266,8 @@ extern "C" int hplai_set_cta_pairs(hplai_ctx *c, int on)
 	}
 	if (on < -1) return HPLAI_EINVAL;
 	c->cta_pairs = on > 0 ? 1 : on;
-	for (int i = 0; i < 2; ++i) {
-		for (auto &m : c->maps[i]) m.pairs = c->cta_pairs;
-		c->mapsg[i].pairs = c->cta_pairs;
-		c->maps8[i].pairs = c->cta_pairs;
-		c->maps8g[i].pairs = c->cta_pairs;
-	}
-	c->maps8s.pairs = c->cta_pairs;
+	const int v = c->cta_pairs;
+	for_each_maps(c, [v](SchurMaps &m) { m.pairs = v; });
 	return HPLAI_OK;
 }
 
@@ -1265,22 +1288,25 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 		if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	}
 	struct Cand {
-		unsigned sched;   // HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2 bits
+		unsigned sched;   // HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_GROUP4 bits
 		int side;
 		std::vector<double> ms;
 		int tg = 0;       // tile group (0: the kernel's default)
 	};
 	std::vector<Cand> cands;
-	for (int g = 1; g <= c->gcap; ++g) {
-		const unsigned gf = g == 2 ? HPLAI_FLAG_GROUP2 : 0u;
+	for (int g : {1, 2, 4}) {
+		if (g > c->gcap) break;
+		const unsigned gf = g == 4 ? HPLAI_FLAG_GROUP4 : g == 2 ? HPLAI_FLAG_GROUP2 : 0u;
 		cands.push_back({gf, 20, {}});
 		for (int side : {16, 32})
 			if (sms > 2 * side) cands.push_back({gf | HPLAI_FLAG_LOOKAHEAD, side, {}});
-		// side-stream share growing as the trailing matrix shrinks
-		for (int share : {8, 16, 24}) cands.push_back({gf | HPLAI_FLAG_LOOKAHEAD, -share, {}});
+		// side-stream share growing as the trailing matrix shrinks (four-panel
+		// groups give the side stream twice the panels per update: larger shares)
+		const int shares2[3] = {8, 16, 24}, shares4[3] = {16, 24, 32};
+		for (int share : (g == 4 ? shares4 : shares2)) cands.push_back({gf | HPLAI_FLAG_LOOKAHEAD, -share, {}});
 	}
 	const int tg0 = c->tile_group;
-	const unsigned sched_bits = HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2;
+	const unsigned sched_bits = HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_GROUP4;
 	const unsigned flags0 = c->flags, base_flags = c->flags & ~sched_bits;
 	const int side0 = c->side_sms;
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1372,9 +1398,11 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 
 extern "C" int hplai_set_schedule(hplai_ctx *c, unsigned flags, int side_sms)
 {
-	const unsigned sched = HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2;
+	const unsigned sched = HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_GROUP4;
 	if (!c || (flags & ~sched) || side_sms == 0 || side_sms > 64 || side_sms < -256) return HPLAI_EINVAL;
-	if ((flags & HPLAI_FLAG_GROUP2) && c->gcap != 2) return HPLAI_EINVAL;
+	if ((flags & HPLAI_FLAG_GROUP2) && (flags & HPLAI_FLAG_GROUP4)) return HPLAI_EINVAL;
+	if ((flags & HPLAI_FLAG_GROUP2) && c->gcap < 2) return HPLAI_EINVAL;
+	if ((flags & HPLAI_FLAG_GROUP4) && c->gcap < 4) return HPLAI_EINVAL;
 	if ((c->flags & HPLAI_FLAG_REF_DECK) && flags) return HPLAI_EINVAL;
 	c->flags = (c->flags & ~sched) | flags;
 	c->side_sms = side_sms;

@@ -111,7 +111,7 @@ static int usage()
 		"   --fp8                   e4m3 Schur update with GMRES refinement.\n"
 		"   --gmres                 GMRES refinement instead of the classical correction.\n"
 		"   --lookahead             Factor the next panel while the trailing update runs.\n"
-		"   --group <g>             Panels per trailing update: 1 (default) or 2 (K = 2b; b %% 128 == 0).\n"
+		"   --group <g>             Panels per trailing update: 1 (default), 2 or 4 (K = g b; b %% 128 == 0).\n"
 		"   --autotune              Choose the schedule (groups, look-ahead) by timing it first.\n"
 		"   --checksum              Print sums of |diag|, |upper|, |lower| of the factors after the LU.\n"
 		"   -w, --warmup            Factor the first P+2 panels only, one refinement step (benchmark warm-up).\n"
@@ -156,7 +156,9 @@ int main(int argc, char **argv)
 		else if (!std::strcmp(argv[i], "--gmres")) mode = HPLAI_GMRES;
 		else if (!std::strcmp(argv[i], "--lookahead")) flags |= HPLAI_FLAG_LOOKAHEAD;
 		else if (!std::strcmp(argv[i], "--group") && i + 1 < argc) {
-			if (std::atoi(argv[++i]) == 2) flags |= HPLAI_FLAG_GROUP2;
+			const int g = std::atoi(argv[++i]);
+			if (g == 2) flags |= HPLAI_FLAG_GROUP2;
+			else if (g == 4) flags |= HPLAI_FLAG_GROUP4;
 		}
 		else if (!std::strcmp(argv[i], "--autotune")) autotune = true;
 		else if (!std::strcmp(argv[i], "--checksum")) checksum = true;
@@ -186,7 +188,7 @@ int main(int argc, char **argv)
 	if (argc > 1 && (!std::strcmp(argv[1], "-h") || !std::strcmp(argv[1], "--help"))) return usage();
 	if (flags & HPLAI_FLAG_REF_DECK) {
 		// one fixed schedule: nothing to tune
-		flags &= ~(HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_LAZY_A);
+		flags &= ~(HPLAI_FLAG_FP16_DECK | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_GROUP4 | HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_LAZY_A);
 		autotune = false;
 	}
 
@@ -224,7 +226,17 @@ int main(int argc, char **argv)
 	}
 
 	hplai_ctx *ctx = nullptr;
-	int rc = hplai_create(&ctx, n, b, precision, flags);
+	int rc = HPLAI_OK;
+	if (autotune && b % 128 == 0 && !(flags & (HPLAI_FLAG_GROUP2 | HPLAI_FLAG_GROUP4 | HPLAI_FLAG_REF_DECK))) {
+		// buffers for four-panel groups, so that the tuner can choose them (skipped when they do not fit)
+		rc = hplai_create(&ctx, n, b, precision, flags | HPLAI_FLAG_GROUP4);
+		if (rc == HPLAI_OK) rc = hplai_set_schedule(ctx, flags & HPLAI_FLAG_LOOKAHEAD, 32);
+		if (rc != HPLAI_OK && ctx) {
+			hplai_destroy(ctx);
+			ctx = nullptr;
+		}
+	}
+	if (!ctx) rc = hplai_create(&ctx, n, b, precision, flags);
 	if (rc != HPLAI_OK) {
 		std::fprintf(stderr, "hplai_create(n=%d, b=%d): %s\n", n, b, hplai_status_string(rc));
 		return 1;
@@ -247,7 +259,8 @@ int main(int argc, char **argv)
 			return 1;
 		}
 		flags = tf;
-		std::printf("autotune: %d panel(s) per update, %s, factorisation %.3f ms\n", (tf & HPLAI_FLAG_GROUP2) ? 2 : 1,
+		std::printf("autotune: %d panel(s) per update, %s, factorisation %.3f ms\n",
+			(tf & HPLAI_FLAG_GROUP4) ? 4 : (tf & HPLAI_FLAG_GROUP2) ? 2 : 1,
 			(tf & HPLAI_FLAG_LOOKAHEAD) ? "look-ahead" : "serial", tms);
 		if (tf & HPLAI_FLAG_LOOKAHEAD) std::printf("autotune: %d side-stream SMs\n", side);
 	}

@@ -31,6 +31,7 @@ FLAG_SIMT_PANELS = 1
 FLAG_LOOKAHEAD = 2
 FLAG_FP16_DECK = 4
 FLAG_GROUP2 = 8
+FLAG_GROUP4 = 128
 FLAG_REF_DECK = 16
 FLAG_REF_BACKBUF = 32
 FLAG_LAZY_A = 64

@@ -108,6 +108,15 @@ typedef enum hplai_phase {
  * (hplai_create returns HPLAI_EINVAL otherwise); hplai_autotune may switch
  * it on or off for contexts whose b allows it. */
 #define HPLAI_FLAG_GROUP2 8u
+/* Four-panel groups: as HPLAI_FLAG_GROUP2 with K = 4b -- the group's block
+ * e + j receives the updates of the group's panels e .. e + j - 1 (each
+ * alone) before it is factored, and the trailing matrix is updated once per
+ * four panels, which quarters the passes over it (at the 1000 W cap of a
+ * B200 the e4m3 deck update sustains 11 % more at K = 4096 than at 2048).
+ * At creation it also sizes the group buffers for four panels (28 n b bytes
+ * more than two-panel buffers with HPLAI_F32_F8, 16 n b with HPLAI_F32_F16),
+ * which hplai_autotune and hplai_set_schedule need to choose it later.  Requires b % 128 == 0; not with HPLAI_FLAG_GROUP2. */
+#define HPLAI_FLAG_GROUP4 128u
 /* The reference's `-d` arithmetic bit for bit (a parity mode, CUDA cores):
  * A is never stored -- a block is formed when it joins a panel as
  * fma(downscale, deck, a_ij) with a_ij regenerated from the LCG
@@ -118,7 +127,8 @@ typedef enum hplai_phase {
  * FP16 accumulator rounded after every product, folded into the deck every
  * 100 products); panels in netlib order (as HPLAI_FLAG_SIMT_PANELS), one
  * stream.  Only with HPLAI_F32_F16 and without HPLAI_FLAG_FP16_DECK,
- * HPLAI_FLAG_GROUP2 and HPLAI_FLAG_LOOKAHEAD (HPLAI_EINVAL otherwise). */
+ * HPLAI_FLAG_GROUP2, HPLAI_FLAG_GROUP4 and HPLAI_FLAG_LOOKAHEAD (HPLAI_EINVAL
+ * otherwise). */
 #define HPLAI_FLAG_REF_DECK 16u
 /* With HPLAI_FLAG_REF_DECK: the reference's `--back_buffer` form bit for bit
  * (dd_layout = 2, back_buffer.hpp:81-170): every 32 steps the deck is written
@@ -220,10 +230,12 @@ int hplai_l1est(hplai_ctx *ctx);
 
 /* Schedule tuner in place of lda_tuner (lda_tuner.hpp:9-45): times
  * hplai_factor on this context (regenerated from seed before each trial)
- * under each schedule -- one- or two-panel groups (HPLAI_FLAG_GROUP2, when
- * b % 128 == 0), serial or with HPLAI_FLAG_LOOKAHEAD at fixed side-stream SM
- * counts or at shares growing as the trailing matrix shrinks (negative
- * side_sms, see hplai_set_schedule) -- after one discarded warm-up
+ * under each schedule -- one-, two- or four-panel groups (HPLAI_FLAG_GROUP2
+ * when b % 128 == 0, HPLAI_FLAG_GROUP4 when the context was created with
+ * it), serial or with HPLAI_FLAG_LOOKAHEAD at fixed side-stream SM
+ * counts (16, 32) or at shares growing as the trailing matrix shrinks
+ * (negative side_sms, see hplai_set_schedule: c = 8, 16, 24; 16, 24, 32 for
+ * four-panel groups) -- after one discarded warm-up
  * factorisation, re-times the two
  * fastest twice more, keeps the one with the lowest median as the context's
  * schedule, then times that schedule twice under each of two other tile
@@ -234,7 +246,8 @@ int hplai_l1est(hplai_ctx *ctx);
  * configuration's factorisation time in ms. */
 int hplai_autotune(hplai_ctx *ctx, uint64_t seed, unsigned *flags, int *side_sms, double *ms);
 /* Sets the schedule by hand, as hplai_autotune would: `flags` a combination
- * of HPLAI_FLAG_LOOKAHEAD and HPLAI_FLAG_GROUP2 (the other flags of the
+ * of HPLAI_FLAG_LOOKAHEAD and HPLAI_FLAG_GROUP2 or HPLAI_FLAG_GROUP4 (the
+ * latter for contexts created with it; the other flags of the
  * context are kept), side_sms the SMs left to the side stream with
  * look-ahead: a fixed count (1 .. 64), or, negative, a share growing as the
  * trailing matrix shrinks -- with c = -side_sms (1 .. 256) the group whose
