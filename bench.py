@@ -258,14 +258,16 @@ def schur_algorithmic(n, b, panel_bytes=2, c_bytes=8, group=1):
 
 
 def schur_traffic_per_launch(n, b, group=1, kind="fp16_fp32c"):
-    """DRAM bytes per average launch from the committed ncu summary (DRAM
-    bytes per updated C element of the kernel at K = 2048), times the C
-    elements of one factorisation's launches (traffic grows with the C
-    area), per launch."""
+    """DRAM bytes per average launch from the committed ncu summaries (DRAM
+    bytes per updated C element of the kernel at the group's K: 2048 or 4096),
+    times the C elements of one factorisation's launches (traffic grows with
+    the C area), per launch."""
     p = os.path.join(ROOT, "profiles", "schur_kernel_traffic.json")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p)).get("kernels", {}).get(kind)
+    kernels = json.load(open(p)).get("kernels", {})
+    d = kernels.get(kind + "_k4096") if group * b >= 4096 else None
+    d = d or kernels.get(kind)
     if not d:
         return None
     _, byts, launches = schur_algorithmic(n, b, 0, 1, group)   # bytes = C elements
