@@ -102,3 +102,19 @@ def test_autotune_considers_four_panel_groups(hplai, torch_cuda):
         s.factor()
         res = s.iterative_refinement(50, mode=1)
         assert res.status == hplai.HPLAI_OK and res.hpl_harness < 16.0
+
+
+@pytest.mark.parametrize("args", [["--fp8", "-d", "--group", "4", "--lookahead"], ["--group", "4"],
+                                  ["--fp8", "--lazy-a", "--autotune"]])
+def test_driver_four_panel_groups(hplai, torch_cuda, tmp_path, args):
+    """driver.out with --group 4 (and the tuner, which may pick it) converges
+    and prints the reference's report line."""
+    import os
+    import re
+    import subprocess
+    exe = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", "hpl-ai_b200", "driver.out"))
+    out = subprocess.run([exe, "8192", "1024", "2"] + args, capture_output=True, text=True, timeout=300,
+                         cwd=tmp_path)
+    assert out.returncode == 0, out.stderr
+    m = re.search(r"^(\S+) sec\. (\S+) GFlop/s resid = (\S+) hpl-harness = (\S+)$", out.stdout, re.M)
+    assert m and 0 <= float(m.group(4)) < 16, out.stdout
