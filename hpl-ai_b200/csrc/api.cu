@@ -1302,7 +1302,7 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 			if (sms > 2 * side) cands.push_back({gf | HPLAI_FLAG_LOOKAHEAD, side, {}});
 		// side-stream share growing as the trailing matrix shrinks (four-panel
 		// groups give the side stream twice the panels per update: larger shares)
-		const int shares2[3] = {8, 16, 24}, shares4[3] = {16, 24, 32};
+		static const std::vector<int> shares2 = {8, 16, 24}, shares4 = {16, 20, 24, 28, 32};
 		for (int share : (g == 4 ? shares4 : shares2)) cands.push_back({gf | HPLAI_FLAG_LOOKAHEAD, -share, {}});
 	}
 	const int tg0 = c->tile_group;

@@ -234,8 +234,8 @@ int hplai_l1est(hplai_ctx *ctx);
  * when b % 128 == 0, HPLAI_FLAG_GROUP4 when the context was created with
  * it), serial or with HPLAI_FLAG_LOOKAHEAD at fixed side-stream SM
  * counts (16, 32) or at shares growing as the trailing matrix shrinks
- * (negative side_sms, see hplai_set_schedule: c = 8, 16, 24; 16, 24, 32 for
- * four-panel groups) -- after one discarded warm-up
+ * (negative side_sms, see hplai_set_schedule: c = 8, 16, 24; 16, 20, 24,
+ * 28, 32 for four-panel groups, whose optimum is sharper) -- after one discarded warm-up
  * factorisation, re-times the two
  * fastest twice more, keeps the one with the lowest median as the context's
  * schedule, then times that schedule twice under each of two other tile
