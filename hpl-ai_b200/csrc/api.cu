@@ -80,6 +80,10 @@ struct hplai_ctx {
 	uint8_t *L8s[kMaxGroup - 1] = {}, *U8s[kMaxGroup - 1] = {};
 	float *sls[kMaxGroup - 1] = {}, *sus[kMaxGroup - 1] = {};
 	unsigned *qbits = nullptr;
+	// precision form with FP16 panel products: the e4m3 copies' block maxima,
+	// gathered by the panel stores (L and U of the panel's own copy, L and U
+	// of the group's shared copy)
+	unsigned *qb[4] = {nullptr, nullptr, nullptr, nullptr};
 	int64_t ld8 = 0, ld8g = 0;
 	// HPLAI_FLAG_FP16_DECK: FP16 trailing-update deck (n x lda halves), holding
 	// dscale x (accumulated update)
@@ -175,6 +179,7 @@ int ctx_free(hplai_ctx *c)
 		cudaFree(c->sus[h]);
 	}
 	cudaFree(c->qbits);
+	cudaFree(c->qb[0]);
 	if (!c->deck_aliased) cudaFree(c->deck);
 	cudaFree(c->dstage);
 	cudaFree(c->rdeck);
@@ -372,6 +377,8 @@ extern "C" int hplai_create(hplai_ctx **out, int n, int b, int precision, unsign
 			CTX_ALLOC(c->sus[h], sizeof(float) * nblk128);
 		}
 		CTX_ALLOC(c->qbits, sizeof(unsigned) * nblk128);
+		CTX_ALLOC(c->qb[0], sizeof(unsigned) * 4 * nblk128);
+		for (int i = 1; i < 4; ++i) c->qb[i] = c->qb[0] + i * nblk128;
 	}
 	c->deck_ld = c->lda;
 	if (flags & HPLAI_FLAG_LAZY_A) {
@@ -547,6 +554,32 @@ int panel_step(hplai_ctx *c, int k, int buf, int slot, bool simt, int side_ctas,
 	const uint16_t *deck = f16_panels ? c->deck : nullptr;   // folded into the FP16 panel copies
 	const float inv_dscale = c->deck ? 1.0f / c->dscale : 0.f;
 	uint16_t *lslot = c->Lh[buf] + slot * c->ldh, *uslot = c->Uh[buf] + slot * c->ldh;
+	// FP16 panel products: their stores gather the e4m3 copies' block maxima
+	// (this panel's own copy; with groups also the group's shared copy, whose
+	// blocks start (G - 1 - slot) b below this panel's first row / column)
+	const int G = c->group;
+	AmaxTargets al, au;
+	al.dim = 0;
+	au.dim = 1;
+	if (f16_panels) {
+		const size_t nbw = sizeof(unsigned) * (n / 128 + 2);
+		const bool own = G == 1 || slot < G - 1;
+		if (own) {
+			HPLAI_CUDA_TRY(cudaMemsetAsync(c->qb[0], 0, nbw, st));
+			HPLAI_CUDA_TRY(cudaMemsetAsync(c->qb[1], 0, nbw, st));
+			al.bits[0] = c->qb[0];
+			au.bits[0] = c->qb[1];
+		}
+		if (G > 1) {
+			if (slot == 0) {
+				HPLAI_CUDA_TRY(cudaMemsetAsync(c->qb[2], 0, nbw, st));
+				HPLAI_CUDA_TRY(cudaMemsetAsync(c->qb[3], 0, nbw, st));
+			}
+			al.bits[1] = c->qb[2];
+			au.bits[1] = c->qb[3];
+			al.base[1] = au.base[1] = (G - 1 - slot) * b;
+		}
+	}
 	HPLAI_TRY(pe.record(st, HPLAI_PH_TRSM_L));
 	if (simt) {
 		HPLAI_TRY(launch_trsm_right_upper(rem, b, diag, lda, diag + b, lda, lslot + (kb + b) * ldg, ldg, 1.0f, st));
@@ -561,7 +594,7 @@ int panel_step(hplai_ctx *c, int k, int buf, int slot, bool simt, int side_ctas,
 			src = c->tcbuf;
 		}
 		HPLAI_TRY(launch_lpanel_f16(c->tc, c->maps[buf][slot], static_cast<int>(kb), rem, c->A, lda, lslot, uslot, ldg,
-			deck, c->deck_ld, inv_dscale, side_ctas, st, src, n));
+			deck, c->deck_ld, inv_dscale, side_ctas, st, src, n, &al));
 	} else {
 		HPLAI_TRY(launch_tri_inverses(c->tc, diag, lda, st));
 		// the precision form's Schur update reads the e4m3 copies only: no FP16 copy
@@ -582,33 +615,35 @@ int panel_step(hplai_ctx *c, int k, int buf, int slot, bool simt, int side_ctas,
 			src = c->tcbuf;
 		}
 		HPLAI_TRY(launch_upanel_f16(c->tc, c->maps[buf][slot], static_cast<int>(kb), rem, c->A, lda, uslot, ldg, deck,
-			c->deck_ld, inv_dscale, side_ctas, st, src, ldp));
+			c->deck_ld, inv_dscale, side_ctas, st, src, ldp, &au));
 	} else {
 		uint16_t *uh = c->precision == HPLAI_F32_F8 ? nullptr : uslot + (kb + b) * ldg;
 		HPLAI_TRY(launch_upanel_tc(c->tc, rem, diag + static_cast<int64_t>(b) * lda, lda, uh, ldg, 1.0f, side_ctas, st));
 	}
 	if (c->precision == HPLAI_F32_F8) {
-		const int G = c->group;
+		// the block maxima: gathered by the FP16 panel stores, else the copy's own pass
+		const bool ready = f16_panels;
+		unsigned *bl = ready ? c->qb[0] : c->qbits, *bu = ready ? c->qb[1] : c->qbits;
 		if (G == 1) {
-			HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, c->qbits, c->L8[buf] + (kb + b) * c->ld8g, c->ld8g,
-				c->sl[buf], st));
-			HPLAI_TRY(launch_quantize_upanel(rem, b, diag + static_cast<int64_t>(b) * lda, lda, c->qbits,
-				c->U8[buf] + (kb + b) * c->ld8g, c->ld8g, c->su[buf], st));
+			HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, bl, c->L8[buf] + (kb + b) * c->ld8g, c->ld8g,
+				c->sl[buf], st, false, ready));
+			HPLAI_TRY(launch_quantize_upanel(rem, b, diag + static_cast<int64_t>(b) * lda, lda, bu,
+				c->U8[buf] + (kb + b) * c->ld8g, c->ld8g, c->su[buf], st, false, ready));
 		} else if (slot < G - 1) {
 			// the panel alone, for the updates of the group's later blocks
-			HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, c->qbits, c->L8s[slot] + (kb + b) * c->ld8, c->ld8,
-				c->sls[slot], st));
-			HPLAI_TRY(launch_quantize_upanel(rem, b, diag + static_cast<int64_t>(b) * lda, lda, c->qbits,
-				c->U8s[slot] + (kb + b) * c->ld8, c->ld8, c->sus[slot], st));
+			HPLAI_TRY(launch_quantize_lpanel(rem, b, diag + b, lda, bl, c->L8s[slot] + (kb + b) * c->ld8, c->ld8,
+				c->sls[slot], st, false, ready));
+			HPLAI_TRY(launch_quantize_upanel(rem, b, diag + static_cast<int64_t>(b) * lda, lda, bu,
+				c->U8s[slot] + (kb + b) * c->ld8, c->ld8, c->sus[slot], st, false, ready));
 		} else {
 			// the group's last panel: [L_k-G+1 .. L_k] (rows kb+b.., A columns
 			// kb-(G-1)b .. kb+b-1) and [U_k-G+1; ..; U_k] (A rows kb-(G-1)b ..
 			// kb+b-1, columns kb+b..) with factors over all the group's panels
 			const int64_t back = static_cast<int64_t>(G - 1) * b;
-			HPLAI_TRY(launch_quantize_lpanel(rem, G * b, diag + b - back * lda, lda, c->qbits,
-				c->L8[buf] + (kb + b) * c->ld8g, c->ld8g, c->sl[buf], st));
-			HPLAI_TRY(launch_quantize_upanel(rem, G * b, diag - back + static_cast<int64_t>(b) * lda, lda, c->qbits,
-				c->U8[buf] + (kb + b) * c->ld8g, c->ld8g, c->su[buf], st));
+			HPLAI_TRY(launch_quantize_lpanel(rem, G * b, diag + b - back * lda, lda, ready ? c->qb[2] : c->qbits,
+				c->L8[buf] + (kb + b) * c->ld8g, c->ld8g, c->sl[buf], st, false, ready));
+			HPLAI_TRY(launch_quantize_upanel(rem, G * b, diag - back + static_cast<int64_t>(b) * lda, lda,
+				ready ? c->qb[3] : c->qbits, c->U8[buf] + (kb + b) * c->ld8g, c->ld8g, c->su[buf], st, false, ready));
 		}
 	}
 	HPLAI_TRY(pe.end(st));

@@ -167,16 +167,18 @@ __global__ void __launch_bounds__(256) cast8_rows_kernel(int rows, int kdim, int
 
 template <bool RCONTIG>
 int quantize(int rows, int kdim, const float *src, int64_t ld, unsigned *bits, uint8_t *dst, int64_t ld8,
-	float *scale, cudaStream_t st, bool pad_row)
+	float *scale, cudaStream_t st, bool pad_row, bool bits_ready)
 {
 	if (rows <= 0) return HPLAI_OK;
 	const int nblk = (rows + 127) / 128;
 	const bool aligned = (reinterpret_cast<uintptr_t>(src) & 15u) == 0 && (ld & 3) == 0;
-	HPLAI_CUDA_TRY(cudaMemsetAsync(bits, 0, sizeof(unsigned) * nblk, st));
-	amax_kernel<RCONTIG><<<dim3(nblk, (kdim + 63) / 64), 256, 0, st>>>(rows, kdim, src, ld, bits,
-		(aligned && (RCONTIG ? rows : kdim) % 4 == 0) ? 1 : 0);
-	count_launches();
-	HPLAI_CUDA_TRY(cudaGetLastError());
+	if (!bits_ready) {
+		HPLAI_CUDA_TRY(cudaMemsetAsync(bits, 0, sizeof(unsigned) * nblk, st));
+		amax_kernel<RCONTIG><<<dim3(nblk, (kdim + 63) / 64), 256, 0, st>>>(rows, kdim, src, ld, bits,
+			(aligned && (RCONTIG ? rows : kdim) % 4 == 0) ? 1 : 0);
+		count_launches();
+		HPLAI_CUDA_TRY(cudaGetLastError());
+	}
 	// the Schur kernel reads the copy in 128-byte K chunks: zeros up to the
 	// chunk's end (pad_row: up to ld8)
 	const int kend = pad_row ? static_cast<int>(ld8) : static_cast<int>(std::min<int64_t>(ld8, (kdim + 127) / 128 * 128));
@@ -196,17 +198,17 @@ int quantize(int rows, int kdim, const float *src, int64_t ld, unsigned *bits, u
 } // namespace
 
 int launch_quantize_lpanel(int rows, int b, const float *acol, int64_t lda, unsigned *bits, uint8_t *l8, int64_t ld8,
-	float *scale, cudaStream_t st, bool pad_row)
+	float *scale, cudaStream_t st, bool pad_row, bool bits_ready)
 {
 	if (ld8 % 128) return HPLAI_EINVAL;
-	return quantize<true>(rows, b, acol, lda, bits, l8, ld8, scale, st, pad_row);
+	return quantize<true>(rows, b, acol, lda, bits, l8, ld8, scale, st, pad_row, bits_ready);
 }
 
 int launch_quantize_upanel(int cols, int b, const float *arow, int64_t lda, unsigned *bits, uint8_t *u8, int64_t ld8,
-	float *scale, cudaStream_t st, bool pad_row)
+	float *scale, cudaStream_t st, bool pad_row, bool bits_ready)
 {
 	if (ld8 % 128) return HPLAI_EINVAL;
-	return quantize<false>(cols, b, arow, lda, bits, u8, ld8, scale, st, pad_row);
+	return quantize<false>(cols, b, arow, lda, bits, u8, ld8, scale, st, pad_row, bits_ready);
 }
 
 namespace {

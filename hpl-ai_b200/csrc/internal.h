@@ -111,10 +111,21 @@ int launch_schur_fp8(const SchurMaps &maps8, const float *sl, int sl0, const flo
 	int m, int n, float *c, int64_t ldc, int crow0, int ccol0, int max_ctas, cudaStream_t st);
 // deck -= dscale * L U on the FP16 deck of `maps` (rows crow0.., cols ccol0..;
 // crow0 a multiple of 8), FP16 (fp8 = false) or e4m3 operands.
+// Block maxima of a panel written by the store form, for its e4m3 copies:
+// atomicMax of |value| bits into bits[t][(index - base[t]) / 128] for the
+// region's rows (dim 0: an L panel, blocks of 128 rows) or columns (dim 1: a
+// U panel, blocks of 128 columns) from base[t] on (region-relative, a
+// multiple of 128); a null bits[t] is skipped.
+struct AmaxTargets {
+	unsigned *bits[2] = {nullptr, nullptr};
+	int base[2] = {0, 0};
+	int dim = 0;
+};
 // C (m x n FP32 region of the map's matrix) = (L U) * *oscale, written by TMA
-// store (FP16 operands; crow0 and m multiples of 4).
+// store (FP16 operands; crow0 and m multiples of 4); with amax, the written
+// values' block maxima as well.
 int launch_schur_store(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
-	int ccol0, const float *oscale, int max_ctas, cudaStream_t st);
+	int ccol0, const float *oscale, int max_ctas, cudaStream_t st, const AmaxTargets *amax = nullptr);
 int launch_schur_deck(const SchurMaps &maps, bool fp8, const float *sl, int sl0, const float *su, int su0, int lrow0,
 	int urow0, int m, int n, int crow0, int ccol0, float dscale, int max_ctas, cudaStream_t st);
 // The batched form: `ntiles` 128 x 256 tiles, tile t updating C rows
@@ -164,12 +175,14 @@ int launch_tri_inverses(const TcPanels &t, const float *lu, int64_t lda, cudaStr
 // (column-major, leading dimension lds; element (r, k) of A_col at
 // src[k*lds + r], of A_row at src[r*lds + k]) -- the matrix regenerated into
 // a scratch panel when A is not stored.
+// amax: the block maxima of the panel written (AmaxTargets, dim 0 for
+// the L panel, 1 for the U panel), for its e4m3 copies.
 int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
 	uint16_t *lh, uint16_t *uh, int64_t ldh, const uint16_t *deck, int64_t ldd, float inv_dscale, int max_ctas,
-	cudaStream_t st, const float *src = nullptr, int64_t lds = 0);
+	cudaStream_t st, const float *src = nullptr, int64_t lds = 0, const AmaxTargets *amax = nullptr);
 int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
 	uint16_t *uh, int64_t ldh, const uint16_t *deck, int64_t ldd, float inv_dscale, int max_ctas, cudaStream_t st,
-	const float *src = nullptr, int64_t lds = 0);
+	const float *src = nullptr, int64_t lds = 0, const AmaxTargets *amax = nullptr);
 // A_col (rem x b) <- A_col U11^{-1}; lh row i = half(scale * A_col row i)
 int launch_lpanel_tc(const TcPanels &t, int rem, float *acol, int64_t lda, uint16_t *lh, int64_t ldh, float scale,
 	int max_ctas, cudaStream_t st);
@@ -185,11 +198,12 @@ void tc_status_reset();
 // 128 bytes), and one power-of-two factor per 128 rows/columns in `scale`
 // (block 0 = the first row).  `bits` is rows/128 + 1 words of scratch.
 // Row bytes past b are zero up to the next multiple of 128 (the Schur
-// kernel's K chunk), or up to ld8 with pad_row.
+// kernel's K chunk), or up to ld8 with pad_row.  bits_ready: `bits` already
+// holds the blocks' maxima (the store form's AmaxTargets), so no pass of its own.
 int launch_quantize_lpanel(int rows, int b, const float *acol, int64_t lda, unsigned *bits, uint8_t *l8, int64_t ld8,
-	float *scale, cudaStream_t st, bool pad_row = false);
+	float *scale, cudaStream_t st, bool pad_row = false, bool bits_ready = false);
 int launch_quantize_upanel(int cols, int b, const float *arow, int64_t lda, unsigned *bits, uint8_t *u8, int64_t ld8,
-	float *scale, cudaStream_t st, bool pad_row = false);
+	float *scale, cudaStream_t st, bool pad_row = false, bool bits_ready = false);
 
 // A[i][j] += deck[i][j] * inv_scale on rows [r0, r1) x cols [c0, c1) (FP16 deck, ld ldd)
 int launch_deck_apply(int r0, int r1, int c0, int c1, float *a, int64_t lda, const void *deck, int64_t ldd,

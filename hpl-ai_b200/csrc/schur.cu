@@ -139,6 +139,10 @@ struct Params {
 	const int4 *tiles;
 	int ntiles;
 	int group_m;        // tile rows per group of the tile order (tile_coords)
+	// Store form: block maxima of the written values (AmaxTargets)
+	unsigned *amax_bits[2];
+	int amax_base[2];
+	int amax_dim;
 };
 
 __device__ unsigned int g_status;
@@ -481,6 +485,9 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 			}
 			if (RED && TALL) {
 				const bool issuer = (warp == 2 && lane == 0);
+				// store form: |value| maxima of this lane's row over the tile's
+				// two 128-column halves (values past the region are exact zeros)
+				float vmax[2] = {0.f, 0.f};
 #pragma unroll 1
 				for (int ch = 0; ch < BN / EPI_CHUNK; ++ch) {
 					const int cc = ch * EPI_CHUNK;
@@ -507,8 +514,14 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 							}
 						} else if (p.oscale) {
 							const float os = *p.oscale;
+							float m = 0.f;
 #pragma unroll
-							for (int j = 0; j < 32; ++j) sb[(32 * half + j) * BM + q * 32 + lane] = __uint_as_float(r[j]) * os;
+							for (int j = 0; j < 32; ++j) {
+								const float v = __uint_as_float(r[j]) * os;
+								sb[(32 * half + j) * BM + q * 32 + lane] = v;
+								m = fmaxf(m, fabsf(v));
+							}
+							vmax[(cc + 32 * half) >> 7] = fmaxf(vmax[(cc + 32 * half) >> 7], m);
 						} else {
 #pragma unroll
 							for (int j = 0; j < 32; ++j) sb[(32 * half + j) * BM + q * 32 + lane] = -__uint_as_float(r[j]);
@@ -524,6 +537,34 @@ __global__ void __launch_bounds__(threads_for(EPI), 1) schur_kernel(const __grid
 						asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 					}
 					++epi_buf;
+				}
+				if (!FP8 && p.oscale && (p.amax_bits[0] || p.amax_bits[1])) {
+					// dim 0: the tile's 128 rows are one block, every lane's row
+					// max over both halves; dim 1: one block per 128-column half,
+					// the max over this warp's 32 rows
+					if (p.amax_dim == 0) vmax[0] = fmaxf(vmax[0], vmax[1]);
+#pragma unroll
+					for (int o = 16; o; o >>= 1) {
+						vmax[0] = fmaxf(vmax[0], __shfl_xor_sync(0xffffffffu, vmax[0], o));
+						vmax[1] = fmaxf(vmax[1], __shfl_xor_sync(0xffffffffu, vmax[1], o));
+					}
+					if (lane == 0) {
+#pragma unroll
+						for (int t2 = 0; t2 < 2; ++t2) {
+							if (!p.amax_bits[t2]) continue;
+							if (p.amax_dim == 0) {
+								const int r0 = tm * BM - p.amax_base[t2];
+								if (r0 >= 0) atomicMax(&p.amax_bits[t2][r0 >> 7], __float_as_uint(vmax[0]));
+							} else {
+#pragma unroll
+								for (int h = 0; h < 2; ++h) {
+									const int c0 = tn * BN + 128 * h - p.amax_base[t2];
+									if (c0 >= 0 && tn * BN + 128 * h < p.n)
+										atomicMax(&p.amax_bits[t2][c0 >> 7], __float_as_uint(vmax[h]));
+								}
+							}
+						}
+					}
 				}
 			} else if (RED) {
 				float *mybuf = sEpi + (warp - 2) * EPI_BUFS * (EPI_BUF_BYTES / 4);
@@ -996,10 +1037,16 @@ int pair_cluster_limit(int *limit)
 // halves) updated as deck - dscale * acc; otherwise FP32 C.
 static int launch_schur_any(const SchurMaps &maps, bool fp8, const float *sl, int sl0, const float *su, int su0,
 	int lrow0, int urow0, int m, int n, void *c, int64_t ldc, int crow0, int ccol0, bool deck, float dscale,
-	int max_ctas, cudaStream_t st, const float *oscale = nullptr)
+	int max_ctas, cudaStream_t st, const float *oscale = nullptr, const AmaxTargets *amax = nullptr)
 {
 	if (m <= 0 || n <= 0) return HPLAI_OK;
 	Params p;
+	for (int t = 0; t < 2; ++t) {
+		p.amax_bits[t] = amax ? amax->bits[t] : nullptr;
+		p.amax_base[t] = amax ? amax->base[t] : 0;
+	}
+	p.amax_dim = amax ? amax->dim : 0;
+	if (amax && (!oscale || amax->base[0] % 128 || amax->base[1] % 128)) return HPLAI_EINVAL;
 	p.c = static_cast<float *>(c);
 	p.ldc = ldc;
 	p.m = m;
@@ -1126,11 +1173,11 @@ int launch_schur_fp8(const SchurMaps &maps8, const float *sl, int sl0, const flo
 }
 
 int launch_schur_store(const SchurMaps &maps, int lrow0, int urow0, int m, int n, float *c, int64_t ldc, int crow0,
-	int ccol0, const float *oscale, int max_ctas, cudaStream_t st)
+	int ccol0, const float *oscale, int max_ctas, cudaStream_t st, const AmaxTargets *amax)
 {
 	if (!oscale) return HPLAI_EINVAL;
 	return launch_schur_any(maps, false, nullptr, 0, nullptr, 0, lrow0, urow0, m, n, c, ldc, crow0, ccol0, false, 0.f,
-		max_ctas, st, oscale);
+		max_ctas, st, oscale, amax);
 }
 
 int launch_schur_deck(const SchurMaps &maps, bool fp8, const float *sl, int sl0, const float *su, int su0, int lrow0,

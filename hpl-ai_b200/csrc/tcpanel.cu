@@ -841,7 +841,7 @@ int launch_upanel_tc(const TcPanels &t, int rem, float *arow, int64_t lda, uint1
 
 int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
 	uint16_t *lh, uint16_t *uh, int64_t ldh, const uint16_t *deck, int64_t ldd, float inv_dscale, int max_ctas,
-	cudaStream_t st, const float *src, int64_t lds)
+	cudaStream_t st, const float *src, int64_t lds, const AmaxTargets *amax)
 {
 	if (rem <= 0) return HPLAI_OK;
 	const int width = (t.b + 63) / 64 * 64;   // the panel's slot in a buffer of row pitch ldh
@@ -870,12 +870,12 @@ int launch_lpanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// A_col = (A_col (s_u U11^{-1})) / s_u
-	return launch_schur_store(maps, kb + b, kb, rem, b, a, lda, kb + b, kb, t.f16_oscale, max_ctas, st);
+	return launch_schur_store(maps, kb + b, kb, rem, b, a, lda, kb + b, kb, t.f16_oscale, max_ctas, st, amax);
 }
 
 int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem, float *a, int64_t lda,
 	uint16_t *uh, int64_t ldh, const uint16_t *deck, int64_t ldd, float inv_dscale, int max_ctas, cudaStream_t st,
-	const float *src, int64_t lds)
+	const float *src, int64_t lds, const AmaxTargets *amax)
 {
 	if (rem <= 0) return HPLAI_OK;
 	const int width = (t.b + 63) / 64 * 64;
@@ -896,7 +896,7 @@ int launch_upanel_f16(const TcPanels &t, const SchurMaps &maps, int kb, int rem,
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	// A_row = ((s_l L11^{-1}) A_row) / s_l, the triangle in rows kb.. of the L buffer
-	return launch_schur_store(maps, kb, kb + b, b, rem, a, lda, kb, kb + b, t.f16_oscale + 1, max_ctas, st);
+	return launch_schur_store(maps, kb, kb + b, b, rem, a, lda, kb, kb + b, t.f16_oscale + 1, max_ctas, st, amax);
 }
 
 int tc_status()
