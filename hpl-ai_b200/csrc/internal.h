@@ -228,7 +228,8 @@ size_t trsv_workspace(int n);
 int launch_trsv(bool lower, int n, const float *a, int64_t lda, double *x, void *work, size_t work_bytes,
 	cudaStream_t st, bool trans = false, const double *dinv = nullptr);
 size_t trsv_dinv_doubles(int n);
-int launch_trsv_dinv(int n, const float *a, int64_t lda, double *dinv, cudaStream_t st);
+// blocks blk0 .. blk0 + nblk - 1 of 128 rows (nblk < 0: to the last)
+int launch_trsv_dinv(int n, const float *a, int64_t lda, double *dinv, cudaStream_t st, int blk0 = 0, int nblk = -1);
 int trsv_status(void *work, cudaStream_t st, int *status);
 int launch_infnorm(int n, const double *x, double *out, cudaStream_t st);
 // panel_check: sigs (device, 3 doubles) = FP64 sums of |a_ij| over the

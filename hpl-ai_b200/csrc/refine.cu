@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(GEMV_ROWS) otf_partial_kernel(int64_t n, int m
 	const double *__restrict__ x, uint64_t state00, int with_diag, const double *__restrict__ diag,
 	double *__restrict__ part, JumpTable64 tab)
 {
-	__shared__ double xs[GEMV_COLS];
+	__shared__ __align__(16) double xs[GEMV_COLS];
 	const int j0 = blockIdx.y * GEMV_COLS;
 	const int j1 = min(j0 + GEMV_COLS, nb);
 	for (int j = threadIdx.x; j < j1 - j0; j += GEMV_ROWS) xs[j] = x[j0 + j];
@@ -81,25 +81,42 @@ __global__ void __launch_bounds__(GEMV_ROWS) otf_partial_kernel(int64_t n, int m
 	const int len = j1 - j0;
 	const int dj = (with_diag && i >= j0 && i < j1) ? i - j0 : -1;   // diagonal column inside the chunk
 	int j = 0;
-	for (; j + 3 < len; j += 4) {
-		double v0 = __ll2double_rn(static_cast<long long>(s0));
-		double v1 = __ll2double_rn(static_cast<long long>(s1));
-		double v2 = __ll2double_rn(static_cast<long long>(s2));
-		double v3 = __ll2double_rn(static_cast<long long>(s3));
-		if (dj >= j && dj < j + 4) {
-			if (dj == j) v0 = 0.0;
-			if (dj == j + 1) v1 = 0.0;
-			if (dj == j + 2) v2 = 0.0;
-			if (dj == j + 3) v3 = 0.0;
+	if (dj < 0) {
+		// no diagonal in this chunk (every CTA but those on the diagonal):
+		// the same sums without the per-group test, x read two at a time
+		for (; j + 3 < len; j += 4) {
+			const double2 x01 = *reinterpret_cast<const double2 *>(&xs[j]);
+			const double2 x23 = *reinterpret_cast<const double2 *>(&xs[j + 2]);
+			a0 = fma(__ll2double_rn(static_cast<long long>(s0)), x01.x, a0);
+			a1 = fma(__ll2double_rn(static_cast<long long>(s1)), x01.y, a1);
+			a0 = fma(__ll2double_rn(static_cast<long long>(s2)), x23.x, a0);
+			a1 = fma(__ll2double_rn(static_cast<long long>(s3)), x23.y, a1);
+			s0 = coeff_apply(jn4, s0);
+			s1 = coeff_apply(jn4, s1);
+			s2 = coeff_apply(jn4, s2);
+			s3 = coeff_apply(jn4, s3);
 		}
-		a0 = fma(v0, xs[j], a0);
-		a1 = fma(v1, xs[j + 1], a1);
-		a0 = fma(v2, xs[j + 2], a0);
-		a1 = fma(v3, xs[j + 3], a1);
-		s0 = coeff_apply(jn4, s0);
-		s1 = coeff_apply(jn4, s1);
-		s2 = coeff_apply(jn4, s2);
-		s3 = coeff_apply(jn4, s3);
+	} else {
+		for (; j + 3 < len; j += 4) {
+			double v0 = __ll2double_rn(static_cast<long long>(s0));
+			double v1 = __ll2double_rn(static_cast<long long>(s1));
+			double v2 = __ll2double_rn(static_cast<long long>(s2));
+			double v3 = __ll2double_rn(static_cast<long long>(s3));
+			if (dj >= j && dj < j + 4) {
+				if (dj == j) v0 = 0.0;
+				if (dj == j + 1) v1 = 0.0;
+				if (dj == j + 2) v2 = 0.0;
+				if (dj == j + 3) v3 = 0.0;
+			}
+			a0 = fma(v0, xs[j], a0);
+			a1 = fma(v1, xs[j + 1], a1);
+			a0 = fma(v2, xs[j + 2], a0);
+			a1 = fma(v3, xs[j + 3], a1);
+			s0 = coeff_apply(jn4, s0);
+			s1 = coeff_apply(jn4, s1);
+			s2 = coeff_apply(jn4, s2);
+			s3 = coeff_apply(jn4, s3);
+		}
 	}
 	for (; j < len; ++j) {
 		const double v = (j == dj) ? 0.0 : __ll2double_rn(static_cast<long long>(s0));
@@ -220,13 +237,13 @@ __global__ void trsv_epoch_kernel(TrsvWork *w)
 // FP64 (the FP32 factor entries convert exactly).  Computed once per
 // factorisation; the triangular solves then apply a block as one product.
 __global__ void __launch_bounds__(TB) trsv_dinv_kernel(int n, const float *__restrict__ a, int64_t lda,
-	double *__restrict__ dinv)
+	double *__restrict__ dinv, int blk0)
 {
 	extern __shared__ __align__(16) float dyn_smem[];
 	float (*tb)[TB + 1] = reinterpret_cast<float (*)[TB + 1]>(dyn_smem);                 // tb[i][j] = A[r0+i][r0+j]
 	double *xc = reinterpret_cast<double *>(dyn_smem + TB * (TB + 1) + 1);             // xc[i * TB + c], 8-aligned
 	xc = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(xc) + 7) & ~static_cast<uintptr_t>(7));
-	const int r = blockIdx.x, upper = blockIdx.y;
+	const int r = blk0 + blockIdx.x, upper = blockIdx.y;
 	const int r0 = r * TB, rows = min(TB, n - r0);
 	const int c = threadIdx.x;
 	for (int e = c; e < TB * TB; e += TB) {
@@ -790,9 +807,12 @@ size_t trsv_dinv_doubles(int n)
 	return 2 * nbt * TB * TB;
 }
 
-int launch_trsv_dinv(int n, const float *a, int64_t lda, double *dinv, cudaStream_t st)
+int launch_trsv_dinv(int n, const float *a, int64_t lda, double *dinv, cudaStream_t st, int blk0, int nblk)
 {
 	if (n <= 0) return HPLAI_OK;
+	const int nbt = (n + TB - 1) / TB;
+	if (nblk < 0) nblk = nbt - blk0;
+	if (blk0 < 0 || nblk <= 0 || blk0 + nblk > nbt) return nblk == 0 ? HPLAI_OK : HPLAI_EINVAL;
 	constexpr size_t smem = sizeof(float) * (TB * (TB + 1) + 3) + sizeof(double) * TB * TB;
 	static DeviceOnce attr;
 	HPLAI_TRY(attr.get([&](int, int *) -> int {
@@ -800,7 +820,7 @@ int launch_trsv_dinv(int n, const float *a, int64_t lda, double *dinv, cudaStrea
 			static_cast<int>(smem)));
 		return HPLAI_OK;
 	}));
-	trsv_dinv_kernel<<<dim3((n + TB - 1) / TB, 2), TB, smem, st>>>(n, a, lda, dinv);
+	trsv_dinv_kernel<<<dim3(nblk, 2), TB, smem, st>>>(n, a, lda, dinv, blk0);
 	count_launches();
 	HPLAI_CUDA_TRY(cudaGetLastError());
 	return HPLAI_OK;
