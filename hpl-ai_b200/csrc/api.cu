@@ -153,7 +153,13 @@ struct hplai_ctx {
 	// preconditioned residual, basis and scratch (allocated on first use)
 	int gm_restart = 30;
 	double gm_tol = 1e-12;
+	// right (flexible) preconditioning: the basis of A M^{-1}, with the
+	// preconditioned vectors z_j = M^{-1} v_j kept (gm_z) so that the
+	// correction is Z y -- one application of M^{-1} per inner step and none
+	// before or after; left: M^{-1} A, one more application for M^{-1} r
+	int gm_right = 1;
 	double *gm_v = nullptr;     // n x (gm_restart + 1), ld = gm_ldv
+	double *gm_z = nullptr;     // n x gm_restart (right preconditioning), ld = gm_ldv
 	double *gm_w = nullptr;     // n
 	double *gm_small = nullptr; // part (kDotBlocks x kMaxBasis), H (kMaxBasis^2), tmp, y
 	double *rhs2 = nullptr, *x2 = nullptr;   // caller right-hand sides (hplai_solve_rhs / _transpose)
@@ -202,6 +208,7 @@ int ctx_free(hplai_ctx *c)
 	cudaFree(c->kstatus);
 	cudaFree(c->f16s);
 	cudaFree(c->gm_v);
+	cudaFree(c->gm_z);
 	cudaFree(c->gm_w);
 	cudaFree(c->gm_small);
 	cudaFree(c->rhs2);
@@ -1018,11 +1025,13 @@ int ensure_gmres_buffers(hplai_ctx *c)
 	const int m = c->gm_restart;
 	if (c->gm_v && c->gm_cap >= m) return HPLAI_OK;
 	cudaFree(c->gm_v);
+	cudaFree(c->gm_z);
 	cudaFree(c->gm_w);
 	cudaFree(c->gm_small);
-	c->gm_v = c->gm_w = c->gm_small = nullptr;
+	c->gm_v = c->gm_z = c->gm_w = c->gm_small = nullptr;
 	c->gm_ldv = round_up(c->n, 32);
 	HPLAI_CUDA_TRY(cudaMalloc(&c->gm_v, sizeof(double) * c->gm_ldv * (m + 1)));
+	HPLAI_CUDA_TRY(cudaMalloc(&c->gm_z, sizeof(double) * c->gm_ldv * m));
 	HPLAI_CUDA_TRY(cudaMalloc(&c->gm_w, sizeof(double) * c->gm_ldv));
 	HPLAI_CUDA_TRY(cudaMalloc(&c->gm_small, sizeof(double) * (kDotBlocks * kMaxBasis + kMaxBasis * kMaxBasis +
 		2 * kMaxBasis)));
@@ -1051,10 +1060,12 @@ int correct_ir(hplai_ctx *c, double *x, PhaseEvents &pe, bool trans)
 	return HPLAI_OK;
 }
 
-// The GMRES correction: one cycle of left-preconditioned GMRES(m) on
-// M^{-1} A d = M^{-1} r from d = 0, x += d.  CGS2 orthogonalisation on the
-// device, Givens rotations and the small triangular solve on the host.
-// Stops at |g_{j+1}| <= tol * ||M^{-1} r||_2 or after m steps.
+// The GMRES correction: one cycle of GMRES(m) from d = 0, x += d, either
+// right-preconditioned (flexible: A M^{-1} u = r with the vectors
+// z_j = M^{-1} v_j kept, d = Z y) or left-preconditioned (M^{-1} A d =
+// M^{-1} r).  CGS2 orthogonalisation on the device, Givens rotations and the
+// small triangular solve on the host.  Stops at |g_{j+1}| <= tol * beta
+// (beta = ||r||_2, or ||M^{-1} r||_2 when left) or after m steps.
 int correct_gmres(hplai_ctx *c, double *x, PhaseEvents &pe, int *inner, bool trans)
 {
 	const int n = c->n, m = c->gm_restart;
@@ -1062,10 +1073,11 @@ int correct_gmres(hplai_ctx *c, double *x, PhaseEvents &pe, int *inner, bool tra
 	cudaStream_t st = c->st;
 	double *part = c->gm_small, *H = part + kDotBlocks * kMaxBasis, *tmp = H + kMaxBasis * kMaxBasis,
 	       *yd = tmp + kMaxBasis;
-	double *V = c->gm_v, *w = c->gm_w;
+	double *V = c->gm_v, *w = c->gm_w, *Z = c->gm_z;
+	const bool right = c->gm_right != 0;
 	*inner = 0;
-	// z = M^{-1} r, beta = ||z||, v_0 = z / beta
-	HPLAI_TRY(apply_lu_inverse(c, c->r, pe, trans));
+	// left: z = M^{-1} r, beta = ||z||, v_0 = z / beta; right: beta = ||r||, v_0 = r / beta
+	if (!right) HPLAI_TRY(apply_lu_inverse(c, c->r, pe, trans));
 	HPLAI_TRY(launch_dots(n, 1, c->r, ldv, c->r, part, tmp, 2, st));
 	HPLAI_TRY(launch_scale(n, c->r, tmp, V, st));
 	double beta = 0.0;
@@ -1077,11 +1089,21 @@ int correct_gmres(hplai_ctx *c, double *x, PhaseEvents &pe, int *inner, bool tra
 	int k = 0;
 	for (int j = 0; j < m; ++j) {
 		double *vj = V + j * ldv, *vn = V + (j + 1) * ldv, *hc = H + j * kMaxBasis;
-		// w = M^{-1} A v_j, A regenerated in FP64
-		HPLAI_TRY(pe.record(st, HPLAI_PH_IR_GEMV));
-		HPLAI_TRY(matvec(c, 1.0, vj, 0.0, w, st, trans));
-		HPLAI_TRY(pe.end(st));
-		HPLAI_TRY(apply_lu_inverse(c, w, pe, trans));
+		if (right) {
+			// z_j = M^{-1} v_j, w = A z_j (A regenerated in FP64)
+			double *zj = Z + j * ldv;
+			HPLAI_CUDA_TRY(cudaMemcpyAsync(zj, vj, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+			HPLAI_TRY(apply_lu_inverse(c, zj, pe, trans));
+			HPLAI_TRY(pe.record(st, HPLAI_PH_IR_GEMV));
+			HPLAI_TRY(matvec(c, 1.0, zj, 0.0, w, st, trans));
+			HPLAI_TRY(pe.end(st));
+		} else {
+			// w = M^{-1} A v_j, A regenerated in FP64
+			HPLAI_TRY(pe.record(st, HPLAI_PH_IR_GEMV));
+			HPLAI_TRY(matvec(c, 1.0, vj, 0.0, w, st, trans));
+			HPLAI_TRY(pe.end(st));
+			HPLAI_TRY(apply_lu_inverse(c, w, pe, trans));
+		}
 		// two Gram-Schmidt sweeps against v_0..v_j; ||w|| after the second
 		HPLAI_TRY(launch_dots(n, j + 1, V, ldv, w, part, hc, 0, st));
 		HPLAI_TRY(launch_gs_update(n, j + 1, V, ldv, hc, w, part, nullptr, st));
@@ -1117,7 +1139,7 @@ int correct_gmres(hplai_ctx *c, double *x, PhaseEvents &pe, int *inner, bool tra
 		y[i] = s / R[static_cast<size_t>(i) * m + i];
 	}
 	HPLAI_CUDA_TRY(cudaMemcpyAsync(yd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
-	HPLAI_TRY(launch_combine(n, k, V, ldv, yd, x, st));
+	HPLAI_TRY(launch_combine(n, k, right ? Z : V, ldv, yd, x, st));
 	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
 	return HPLAI_OK;
 }
@@ -1129,6 +1151,13 @@ extern "C" int hplai_set_gmres(hplai_ctx *c, int restart, double tol)
 	if (!c || restart < 1 || restart > kMaxBasis - 1 || !(tol > 0.0) || !(tol < 1.0)) return HPLAI_EINVAL;
 	c->gm_restart = restart;
 	c->gm_tol = tol;
+	return HPLAI_OK;
+}
+
+extern "C" int hplai_set_gmres_side(hplai_ctx *c, int right)
+{
+	if (!c || (right != 0 && right != 1)) return HPLAI_EINVAL;
+	c->gm_right = right;
 	return HPLAI_OK;
 }
 

@@ -91,6 +91,7 @@ _solve_rhs = _proto("hplai_solve_rhs", _c_int, _vp, _vp, _vp, _c_int, ctypes.POI
 _solve_transpose = _proto("hplai_solve_transpose", _c_int, _vp, _vp, _vp, _c_int, ctypes.POINTER(IRErrors),
                           ctypes.POINTER(_c_int))
 _set_gmres = _proto("hplai_set_gmres", _c_int, _vp, _c_int, _c_dbl)
+_set_gmres_side = _proto("hplai_set_gmres_side", _c_int, _vp, _c_int)
 _get_refine_counts = _proto("hplai_get_refine_counts", _c_int, _vp, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int))
 _get_norms = _proto("hplai_get_norms", _c_int, _vp, ctypes.POINTER(_c_dbl), ctypes.POINTER(_c_dbl))
 _solve_host = _proto("hplai_solve_host", _c_int, _vp, _vp, _c_i64, _vp, _vp, _c_u64, _c_int, _vp,
@@ -317,6 +318,10 @@ class Solver:
 
     def set_gmres(self, restart: int = 30, tol: float = 1e-12):
         check(_set_gmres(self._h, restart, tol), "hplai_set_gmres")
+
+    def set_gmres_side(self, right: bool):
+        """GMRES preconditioning: right (flexible, the default) or left."""
+        check(_set_gmres_side(self._h, 1 if right else 0), "hplai_set_gmres_side")
 
     def refine_counts(self):
         """(residual evaluations, GMRES inner steps) of the last refinement."""

@@ -302,6 +302,12 @@ int hplai_solve_transpose(hplai_ctx *ctx, const double *g, double *lambda, int m
 /* GMRES parameters: restart length (1..31, default 30) and the relative
  * reduction of the preconditioned residual that ends a cycle (default 1e-12). */
 int hplai_set_gmres(hplai_ctx *ctx, int restart, double tol);
+/* GMRES preconditioning side: 1 (default) right / flexible -- the basis of
+ * A M^{-1} with the vectors z_j = M^{-1} v_j kept and the correction Z y, one
+ * application of M^{-1} = (L U)^{-1} per inner step; 0 left -- the basis of
+ * M^{-1} A, one more application (M^{-1} r) per cycle.  Both end a cycle
+ * when the residual of their own system has fallen by the tolerance. */
+int hplai_set_gmres_side(hplai_ctx *ctx, int right);
 /* Residual evaluations and GMRES inner steps of the last hplai_refine. */
 int hplai_get_refine_counts(hplai_ctx *ctx, int *outer, int *inner);
 
