@@ -399,12 +399,13 @@ class FormRun:
                 if not (f & hplai.FLAG_LOOKAHEAD):
                     return None
                 return sd if sd > 0 else f"share sms*c/(r+c), c={-sd} panels, r = trailing block columns"
-            trials = [{"panels_per_update": group_of(f),
+            trials = [{"panels_per_update": group_of(f), "cta_pairs": bool(f & hplai.TRIAL_CTA_PAIRS),
                        "lookahead": bool(f & hplai.FLAG_LOOKAHEAD), "side_sms": side_desc(f, sd),
                        "tile_group": tg, "factor_ms": round(ms, 2)} for f, sd, tg, ms in self.s.autotune_trials()]
             self.tuned = {"factor_ms": tms, "trials_warmup_first": trials}
             self.schedule = {"lookahead": la, "side_sms": side_desc(tflags, tside), "panels_per_update": self.group,
-                             "tile_group": self.s.tile_group(), "source": "hplai_autotune"}
+                             "tile_group": self.s.tile_group(), "cta_pairs": self.s.cta_pairs() == 1,
+                             "source": "hplai_autotune"}
         self.results = []
 
     def step(self, timed):

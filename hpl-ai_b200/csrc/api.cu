@@ -1322,6 +1322,14 @@ void apply_tile_group(hplai_ctx *c, int gm)
 	for_each_maps(c, [gm](SchurMaps &m) { m.group_m = gm; });
 }
 
+// Deck updates on CTA pairs for every Schur launch of the context (1 on, 0
+// off, -1 the library default).
+void apply_cta_pairs(hplai_ctx *c, int v)
+{
+	c->cta_pairs = v;
+	for_each_maps(c, [v](SchurMaps &m) { m.pairs = v; });
+}
+
 } // namespace
 
 extern "C" int hplai_set_tile_group(hplai_ctx *c, int group_m)
@@ -1340,9 +1348,14 @@ extern "C" int hplai_set_cta_pairs(hplai_ctx *c, int on)
 		return HPLAI_OK;
 	}
 	if (on < -1) return HPLAI_EINVAL;
-	c->cta_pairs = on > 0 ? 1 : on;
-	const int v = c->cta_pairs;
-	for_each_maps(c, [v](SchurMaps &m) { m.pairs = v; });
+	apply_cta_pairs(c, on > 0 ? 1 : on);
+	return HPLAI_OK;
+}
+
+extern "C" int hplai_get_cta_pairs(hplai_ctx *c, int *on)
+{
+	if (!c || !on) return HPLAI_EINVAL;
+	*on = c->cta_pairs;
 	return HPLAI_OK;
 }
 
@@ -1367,6 +1380,7 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 		int side;
 		std::vector<double> ms;
 		int tg = 0;       // tile group (0: the kernel's default)
+		int pairs = -2;   // deck updates on CTA pairs for the trial (-2: the context's setting)
 	};
 	std::vector<Cand> cands;
 	for (int g : {1, 2, 4}) {
@@ -1380,7 +1394,7 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 		static const std::vector<int> shares2 = {8, 16, 24}, shares4 = {16, 20, 24, 28, 32};
 		for (int share : (g == 4 ? shares4 : shares2)) cands.push_back({gf | HPLAI_FLAG_LOOKAHEAD, -share, {}});
 	}
-	const int tg0 = c->tile_group;
+	const int tg0 = c->tile_group, pairs0 = c->cta_pairs;
 	const unsigned sched_bits = HPLAI_FLAG_LOOKAHEAD | HPLAI_FLAG_GROUP2 | HPLAI_FLAG_GROUP4;
 	const unsigned flags0 = c->flags, base_flags = c->flags & ~sched_bits;
 	const int side0 = c->side_sms;
@@ -1392,6 +1406,7 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 		c->flags = base_flags | t.sched;
 		c->side_sms = t.side;
 		apply_tile_group(c, t.tg);
+		apply_cta_pairs(c, t.pairs == -2 ? pairs0 : t.pairs);
 		HPLAI_TRY(hplai_generate(c, seed));
 		HPLAI_CUDA_TRY(cudaEventRecord(e0, c->st));
 		HPLAI_TRY(hplai_factor(c));
@@ -1400,7 +1415,7 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 		float f = 0.f;
 		HPLAI_CUDA_TRY(cudaEventElapsedTime(&f, e0, e1));
 		*ms = f;
-		c->tune_log.push_back({c->flags, t.side, f, t.tg > 0 ? t.tg : 32});
+		c->tune_log.push_back({c->flags | (t.pairs == 1 ? HPLAI_TRIAL_CTA_PAIRS : 0u), t.side, f, t.tg > 0 ? t.tg : 32});
 		return HPLAI_OK;
 	};
 	auto median = [](std::vector<double> v) {
@@ -1452,17 +1467,36 @@ extern "C" int hplai_autotune(hplai_ctx *c, uint64_t seed, unsigned *flags_out, 
 			tg_pick = tg;
 		}
 	}
+	// then the tile shape of the deck updates with K >= 2048: 256 x 256 tiles
+	// on CTA pairs instead of 128 x 256 on single CTAs, by the same rule
+	bool pairs_pick = false;
+	const bool deck_k2048 = c->deck && (cands[pick].sched & (HPLAI_FLAG_GROUP2 | HPLAI_FLAG_GROUP4)) &&
+		(((cands[pick].sched & HPLAI_FLAG_GROUP4) ? 4 : 2) * c->b >= 2048);
+	if (rc == HPLAI_OK && deck_k2048) {
+		Cand t = cands[pick];
+		t.tg = tg_pick;
+		t.pairs = 1;
+		double a = 0.0, b2 = 0.0;
+		rc = trial(t, &a);
+		if (rc == HPLAI_OK) rc = trial(t, &b2);
+		if (rc == HPLAI_OK && std::max(a, b2) < 0.995 * best) {
+			best = std::max(a, b2);
+			pairs_pick = true;
+		}
+	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	if (rc != HPLAI_OK) {
 		c->flags = flags0;
 		c->side_sms = side0;
 		apply_tile_group(c, tg0);
+		apply_cta_pairs(c, pairs0);
 		return rc;
 	}
 	c->flags = base_flags | cands[pick].sched;
 	c->side_sms = cands[pick].side;
 	apply_tile_group(c, tg_pick);
+	apply_cta_pairs(c, pairs_pick ? 1 : pairs0);
 	// the context is left generated and unfactored, as after hplai_generate
 	HPLAI_TRY(hplai_generate(c, seed));
 	if (flags_out) *flags_out = c->flags;

@@ -32,6 +32,7 @@ FLAG_LOOKAHEAD = 2
 FLAG_FP16_DECK = 4
 FLAG_GROUP2 = 8
 FLAG_GROUP4 = 128
+TRIAL_CTA_PAIRS = 0x80000000
 FLAG_REF_DECK = 16
 FLAG_REF_BACKBUF = 32
 FLAG_LAZY_A = 64
@@ -77,6 +78,7 @@ _autotune_trials = _proto("hplai_get_autotune_trials", _c_int, _vp, _vp, _vp, _v
 _set_tile_group = _proto("hplai_set_tile_group", _c_int, _vp, _c_int)
 _get_tile_group = _proto("hplai_get_tile_group", _c_int, _vp, ctypes.POINTER(_c_int))
 _set_cta_pairs = _proto("hplai_set_cta_pairs", _c_int, _vp, _c_int)
+_get_cta_pairs = _proto("hplai_get_cta_pairs", _c_int, _vp, ctypes.POINTER(_c_int))
 _refine = _proto("hplai_refine", _c_int, _vp, _c_int, _c_int, ctypes.POINTER(IRErrors), ctypes.POINTER(_c_int))
 _get_x = _proto("hplai_get_x", _c_int, _vp, _vp)
 _get_lu = _proto("hplai_get_lu", _c_int, _vp, _vp, _c_i64)
@@ -279,6 +281,11 @@ class Solver:
     def set_cta_pairs(self, on: int):
         """Deck updates on CTA pairs (1), single CTAs (0) or the library default (-1)."""
         check(_set_cta_pairs(self._h, on), "hplai_set_cta_pairs")
+
+    def cta_pairs(self) -> int:
+        v = _c_int()
+        check(_get_cta_pairs(self._h, ctypes.byref(v)), "hplai_get_cta_pairs")
+        return v.value
 
     def set_tile_group(self, group_m: int):
         check(_set_tile_group(self._h, group_m), "hplai_set_tile_group")

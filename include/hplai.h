@@ -241,10 +241,16 @@ int hplai_l1est(hplai_ctx *ctx);
  * schedule, then times that schedule twice under each of two other tile
  * orders of the Schur kernel (groups of 16 and 64 tile rows instead of 32,
  * hplai_set_tile_group) and keeps one only if both of its trials beat the
- * median by 0.5 %; leaves the context generated and unfactored.  Outputs
+ * median by 0.5 %, then -- for the FP16 deck with groups of K >= 2048 --
+ * the deck update's 256 x 256 tiles on CTA pairs instead of 128 x 256
+ * (hplai_set_cta_pairs) by the same rule; leaves the context generated and
+ * unfactored.  Outputs
  * (may be NULL): the chosen flags, the side-stream SM count and the chosen
  * configuration's factorisation time in ms. */
 int hplai_autotune(hplai_ctx *ctx, uint64_t seed, unsigned *flags, int *side_sms, double *ms);
+/* In the flags of hplai_get_autotune_trials / hplai_get_autotune_log: the
+ * trial ran the deck update on CTA pairs. */
+#define HPLAI_TRIAL_CTA_PAIRS 0x80000000u
 /* Sets the schedule by hand, as hplai_autotune would: `flags` a combination
  * of HPLAI_FLAG_LOOKAHEAD and HPLAI_FLAG_GROUP2 or HPLAI_FLAG_GROUP4 (the
  * latter for contexts created with it; the other flags of the
@@ -280,6 +286,8 @@ int hplai_get_tile_group(hplai_ctx *ctx, int *group_m);
  * follow.  Replaces nothing in the reference (its GEMM is a CPU kernel,
  * kernels/avx2.cpp:82-302); a performance setting, results are unchanged. */
 int hplai_set_cta_pairs(hplai_ctx *ctx, int on);
+/* The context's setting: 1, 0 or -1 (the library default). */
+int hplai_get_cta_pairs(hplai_ctx *ctx, int *on);
 
 /* iterative_refinement (iterative_refinement.hpp:18-57) with maxit steps
  * (the driver uses 50).  Fills *err ({-1,-1} on failure) and *iters (the

@@ -82,3 +82,21 @@ def test_pair_switch_arguments(hplai):
             s.set_cta_pairs(v)
         with pytest.raises(hplai.HplaiError):
             s.set_cta_pairs(-2)
+
+
+def test_autotune_tries_cta_pairs(hplai, torch_cuda):
+    """For the deck with four-panel groups (K = 4096) the tuner times the
+    chosen schedule once more on CTA pairs and keeps the faster tile shape;
+    the chosen configuration solves."""
+    with hplai.Solver(8192, 1024, precision=hplai.F32_F8, flags=DECK | 128) as s:
+        flags, side, ms = s.autotune(42)
+        trials = s.autotune_trials()
+        paired = [t for t in trials if t[0] & hplai.TRIAL_CTA_PAIRS]
+        if flags & (8 | 128):   # a grouped schedule: K >= 2048
+            assert len(paired) == 2 and all(t[0] & (8 | 128) for t in paired)
+        else:
+            assert not paired
+        assert s.cta_pairs() in (-1, 1)
+        s.factor()
+        res = s.iterative_refinement(50, mode=hplai.GMRES)
+        assert res.status == hplai.HPLAI_OK and res.hpl_harness < 16.0
