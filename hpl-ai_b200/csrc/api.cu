@@ -143,10 +143,6 @@ struct hplai_ctx {
 		int tile_group;
 	};
 	int tile_group = 0;   // tile rows per group of the Schur kernel's tile order (0: its default)
-	// the refinement's FP64 inverses of 128 x 128 diagonal blocks computed
-	// right after each diagonal block's LU (b % 128 == 0, whole factorisation)
-	// instead of at the end
-	bool dinv_per_panel = false;
 	int cta_pairs = -1;   // deck updates on CTA pairs: 1 on, 0 off, -1 the library default
 	std::vector<Trial> tune_log;
 	// GMRES correction: restart length, relative tolerance on the
@@ -558,8 +554,6 @@ int panel_step(hplai_ctx *c, int k, int buf, int slot, bool simt, int side_ctas,
 	float *diag = c->A + kb + kb * lda;
 	HPLAI_TRY(pe.record(st, HPLAI_PH_DIAG_LU));
 	HPLAI_TRY(launch_getrf_tiles(b, diag, lda, c->getrf_work, &c->getrf_epoch, side_ctas, st));
-	if (c->dinv_per_panel)   // the block's entries are final: its 128-row blocks' inverses, off the end's path
-		HPLAI_TRY(launch_trsv_dinv(n, c->A, lda, c->dinv, st, static_cast<int>(kb / 128), b / 128));
 	HPLAI_TRY(pe.end(st));
 	if (k == c->nb - 1) return HPLAI_OK;
 	const int rem = n - static_cast<int>(kb) - b;
@@ -860,7 +854,6 @@ int factor_impl(hplai_ctx *c, int kend, const float *host_a = nullptr, int64_t h
 	HPLAI_CUDA_TRY(cudaMemsetAsync(c->getrf_work, 0, sizeof(uint32_t), c->st));   // its status word
 	const bool simt = (c->flags & HPLAI_FLAG_SIMT_PANELS) != 0;
 	const bool serial = (c->flags & HPLAI_FLAG_LOOKAHEAD) == 0;
-	c->dinv_per_panel = (b % 128 == 0) && kend >= nb;
 	for (double &v : c->phase_ms) v = 0.0;
 	PhaseEvents pe;
 	// Right-looking blocked LU without pivoting with look-ahead
@@ -958,13 +951,13 @@ int factor_impl(hplai_ctx *c, int kend, const float *host_a = nullptr, int64_t h
 	HPLAI_CUDA_TRY(cudaEventRecord(c->ev_panel, sd));
 	HPLAI_CUDA_TRY(cudaStreamWaitEvent(st, c->ev_panel, 0));
 	// inverses of the factors' 128 x 128 diagonal blocks for the refinement's
-	// solves, unless each panel step made its own
-	if (!c->dinv_per_panel) {
-		HPLAI_TRY(pe.record(st, HPLAI_PH_IR_TRSV));
-		HPLAI_TRY(launch_trsv_dinv(n, c->A, c->lda, c->dinv, st));
-		HPLAI_TRY(pe.end(st));
-	}
-	c->dinv_per_panel = false;
+	// solves, in one launch of all blocks (made per panel instead, each
+	// block's ~0.2 ms substitution lengthened the panel chain: 7 ms more at
+	// n = 8192, b = 256 and 11 ms at n = 65536, b = 1024 with look-ahead,
+	// against 0.24 and 1.5 ms here)
+	HPLAI_TRY(pe.record(st, HPLAI_PH_IR_TRSV));
+	HPLAI_TRY(launch_trsv_dinv(n, c->A, c->lda, c->dinv, st));
+	HPLAI_TRY(pe.end(st));
 	HPLAI_CUDA_TRY(cudaStreamSynchronize(st));
 	pe.collect(c->phase_ms);
 	{
