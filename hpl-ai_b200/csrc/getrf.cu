@@ -339,7 +339,11 @@ __global__ void __launch_bounds__(kWarps * 32) getrf_tiles_kernel(int b, float *
 	}
 
 	// ---------------- worker warps ----------------
-	const int wid = (blockIdx.x - 1) * kWarps + warp, nwarps = (gridDim.x - 1) * kWarps;
+	// worker warp w owns tiles w, w + nwarps, ... (column-major tile index);
+	// warp numbers run across the CTAs first, so that neighbouring tiles sit
+	// on different SMs (b = 1024: 0.57 ms against 0.62 with them on one SM;
+	// ordering each warp's tiles nearest-the-diagonal first was slower)
+	const int wid = warp * (gridDim.x - 1) + (blockIdx.x - 1), nwarps = (gridDim.x - 1) * kWarps;
 	for (int r = 0; r < nt && ok; ++r) {
 		const int k0 = r * T, kv = min(T, b - k0);
 		const uint32_t diag_final = base + r + 1;
