@@ -166,10 +166,12 @@ __device__ __noinline__ void op_solve_l(float *x, const float *d, int kv)
 	float v[T];
 #pragma unroll
 	for (int j = 0; j < T; ++j) v[j] = x[j * kLd + lane];
+	// 1/u_jj, lane j's (the staged tile is zero past kv: those lanes' values go unused)
+	const float inv = 1.0f / d[lane * kLd + lane];
 #pragma unroll 1
 	for (int j = 0; j < kv; ++j) {
 		// v[t] = element (lane, j + t); U(j, j + t) at d[(j + t) * kLd + j]
-		v[0] *= 1.0f / d[j * kLd + j];
+		v[0] *= __shfl_sync(0xffffffffu, inv, j);
 		const float *urow = d + j * kLd + j;
 #pragma unroll
 		for (int t = 1; t < T; ++t)
@@ -211,21 +213,42 @@ __device__ __noinline__ void op_solve_u(float *x, const float *d, int kv)
 	__syncwarp();
 }
 
-// x -= l u (K = T); row `lane` of x in registers.
+// x -= l u (K = T); column `lane` of x in registers: per k, u_kj from the
+// lane's own column of u and column k of l as eight 16-byte broadcasts
+// (columns are 16-byte aligned: kLd * 4 = 144 bytes).
 __device__ __noinline__ void op_update(float *x, const float *l, const float *u)
 {
 	const int lane = threadIdx.x & 31;
 	float v[T];
+	float4 *xc = reinterpret_cast<float4 *>(x + lane * kLd);
 #pragma unroll
-	for (int j = 0; j < T; ++j) v[j] = x[j * kLd + lane];
+	for (int q = 0; q < T / 4; ++q) {
+		const float4 c = xc[q];
+		v[4 * q] = c.x;
+		v[4 * q + 1] = c.y;
+		v[4 * q + 2] = c.z;
+		v[4 * q + 3] = c.w;
+	}
+	const float4 *uc = reinterpret_cast<const float4 *>(u + lane * kLd);
 #pragma unroll 1
-	for (int k = 0; k < T; ++k) {
-		const float lk = l[k * kLd + lane];
+	for (int k4 = 0; k4 < T / 4; ++k4) {
+		const float4 u4 = uc[k4];
+		const float uk[4] = {u4.x, u4.y, u4.z, u4.w};
 #pragma unroll
-		for (int j = 0; j < T; ++j) v[j] = fmaf(-lk, u[j * kLd + k], v[j]);
+		for (int kk = 0; kk < 4; ++kk) {
+			const float4 *lc = reinterpret_cast<const float4 *>(l + (4 * k4 + kk) * kLd);
+#pragma unroll
+			for (int q = 0; q < T / 4; ++q) {
+				const float4 l4 = lc[q];
+				v[4 * q] = fmaf(-l4.x, uk[kk], v[4 * q]);
+				v[4 * q + 1] = fmaf(-l4.y, uk[kk], v[4 * q + 1]);
+				v[4 * q + 2] = fmaf(-l4.z, uk[kk], v[4 * q + 2]);
+				v[4 * q + 3] = fmaf(-l4.w, uk[kk], v[4 * q + 3]);
+			}
+		}
 	}
 #pragma unroll
-	for (int j = 0; j < T; ++j) x[j * kLd + lane] = v[j];
+	for (int q = 0; q < T / 4; ++q) xc[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
 	__syncwarp();
 }
 
