@@ -11,12 +11,13 @@
 // tile with min(ti, tj) = r is final at r + 1; consumers wait for the value
 // they need.
 //
-// The diagonal is the critical chain, so one warp (CTA 0) does nothing
+// The diagonal is the critical chain, so one CTA (CTA 0) does nothing
 // else: at step r it takes L(r+1, r) and U(r, r+1) once their owners have
 // applied their first r updates, solves them with the factored tile (r, r)
-// it still holds, publishes them, applies the last update to tile
-// (r+1, r+1) and factors it.  There is no flag hop between two diagonal
-// tiles, and its code stays hot in its SM's instruction cache.  Worker
+// it still holds (four warps each, a step per named barrier), publishes
+// them, applies the last update to tile (r+1, r+1) and factors it (all
+// eight warps).  There is no flag hop between two diagonal tiles, and its
+// code stays hot in its SM's instruction cache.  Worker
 // warps (the other CTAs) own every other tile and walk them step by step,
 // panel tiles before updates.  Every wait is on work the producer reaches
 // without waiting on the waiter, so the dataflow always completes (all
@@ -124,40 +125,13 @@ __device__ __forceinline__ void store_tile(const float *t, float *a, int64_t lda
 	}
 }
 
-// Tile operations on staged tiles.  Each keeps a row (or column) of its tile
-// in registers and walks the pivots with a runtime loop: the element of the
-// current pivot column is always v[0] and the row shifts left by one after
-// each step, so every register index is static while the loop body stays a
-// few hundred bytes of code (instruction-cache resident; a fully unrolled
-// 32-step elimination is tens of KB and runs from L2 once per step).
-
-// Unblocked LU (getrf_nopiv_small order) of the kv x kv tile x; row `lane`
-// in registers, the pivot row broadcast from its lane.
-__device__ __noinline__ void op_factor(float *x, int kv)
-{
-	const int lane = threadIdx.x & 31;
-	float v[T];
-#pragma unroll
-	for (int j = 0; j < T; ++j) v[j] = x[j * kLd + lane];
-#pragma unroll 1
-	for (int k = 0; k < kv; ++k) {
-		// v[t] = element (lane, k + t)
-		const float inv = 1.0f / __shfl_sync(0xffffffffu, v[0], k);
-		const bool below = lane > k;
-		const float lik = v[0] * inv;
-		if (below) v[0] = lik;
-#pragma unroll
-		for (int t = 1; t < T; ++t) {
-			const float ukj = __shfl_sync(0xffffffffu, v[t], k);
-			if (below) v[t] = fmaf(-lik, ukj, v[t]);
-		}
-		x[k * kLd + lane] = v[0];   // column k of row `lane` is final
-#pragma unroll
-		for (int t = 0; t < T - 1; ++t) v[t] = v[t + 1];
-		v[T - 1] = 0.f;
-	}
-	__syncwarp();
-}
+// One-warp tile operations on staged tiles (the worker warps').  The solves
+// keep a row (or column) of the tile in registers and walk the pivots with a
+// runtime loop: the element of the current pivot column is always v[0] and
+// the row shifts left by one after each step, so every register index is
+// static while the loop body stays a few hundred bytes of code
+// (instruction-cache resident; a fully unrolled 32-step elimination is tens
+// of KB and runs from L2 once per step).
 
 // L tile x <- x U^{-1}, U = upper part of the factored tile d (kv x kv); row `lane`.
 __device__ __noinline__ void op_solve_l(float *x, const float *d, int kv)
@@ -252,7 +226,7 @@ __device__ __noinline__ void op_update(float *x, const float *l, const float *u)
 	__syncwarp();
 }
 
-constexpr int kDiagWarps = 4;
+constexpr int kDiagWarps = kWarps;
 
 // Barrier and AND-vote of the diagonal CTA's warps (named barrier 1).
 __device__ __forceinline__ void diag_sync()
@@ -287,6 +261,116 @@ __device__ __noinline__ void op_update_cols(float *x, const float *l, const floa
 	for (int j = 0; j < C; ++j) x[(c0 + j) * kLd + lane] = v[j];
 }
 
+// The diagonal CTA's tile operations over several warps: warp w of a group
+// owns C = T / (warps in the group) columns (rows for the U solve), lane =
+// row (column); the value each step broadcasts (a multiplier column or a
+// solved row) goes through shared memory, double-buffered, one named
+// barrier per step.  Every element receives the same operations in the same
+// order as in an unblocked one-warp factorisation and in the workers'
+// op_solve_l / op_solve_u.
+__device__ __forceinline__ void group_sync(int id, int threads)
+{
+	asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+// Unblocked LU of the kv x kv tile x, all kDiagWarps warps (barrier 1).
+__device__ __noinline__ void coop_factor(float *x, int kv, float *mbuf, int warp)
+{
+	constexpr int C = T / kDiagWarps;
+	const int lane = threadIdx.x & 31, c0 = warp * C;
+	float v[C];
+#pragma unroll
+	for (int c = 0; c < C; ++c) v[c] = x[(c0 + c) * kLd + lane];
+#pragma unroll 1
+	for (int k = 0; k < kv; ++k) {
+		float *m = mbuf + (k & 1) * T;
+		const bool own = k >= c0 && k < c0 + C;
+		float lreg = 0.f;
+#pragma unroll
+		for (int c = 0; c < C; ++c)
+			if (k == c0 + c) {
+				const float inv = 1.0f / __shfl_sync(0xffffffffu, v[c], k);
+				const float lik = v[c] * inv;
+				if (lane > k) v[c] = lik;
+				m[lane] = lik;
+				lreg = lik;
+			}
+		group_sync(1, kDiagWarps * 32);
+		const float l = own ? lreg : m[lane];
+#pragma unroll
+		for (int c = 0; c < C; ++c) {
+			const float ukj = __shfl_sync(0xffffffffu, v[c], k);
+			if (lane > k && c0 + c > k) v[c] = fmaf(-l, ukj, v[c]);
+		}
+	}
+#pragma unroll
+	for (int c = 0; c < C; ++c) x[(c0 + c) * kLd + lane] = v[c];
+}
+
+// L tile x <- x U^{-1} (T columns), warps w = 0 .. kSolveWarps - 1 of the
+// group on barrier `bar`; row `lane`.
+constexpr int kSolveWarps = kDiagWarps / 2;
+__device__ __noinline__ void coop_solve_l(float *x, const float *d, float *mbuf, int w, int bar)
+{
+	constexpr int C = T / kSolveWarps;
+	const int lane = threadIdx.x & 31, c0 = w * C;
+	float v[C];
+#pragma unroll
+	for (int c = 0; c < C; ++c) v[c] = x[(c0 + c) * kLd + lane];
+	const float inv = 1.0f / d[lane * kLd + lane];   // lane j: 1/u_jj
+#pragma unroll 1
+	for (int j = 0; j < T; ++j) {
+		float *m = mbuf + (j & 1) * T;
+		const bool own = j >= c0 && j < c0 + C;
+		const float invj = __shfl_sync(0xffffffffu, inv, j);
+		float xreg = 0.f;
+#pragma unroll
+		for (int c = 0; c < C; ++c)
+			if (j == c0 + c) {
+				v[c] *= invj;
+				m[lane] = v[c];
+				xreg = v[c];
+			}
+		group_sync(bar, kSolveWarps * 32);
+		const float xij = own ? xreg : m[lane];
+#pragma unroll
+		for (int c = 0; c < C; ++c)
+			if (c0 + c > j) v[c] = fmaf(-xij, d[(c0 + c) * kLd + j], v[c]);
+	}
+#pragma unroll
+	for (int c = 0; c < C; ++c) x[(c0 + c) * kLd + lane] = v[c];
+}
+
+// U tile x <- L^{-1} x (T rows, L unit lower), warp w of its group owning
+// rows w * C ..; column `lane`.
+__device__ __noinline__ void coop_solve_u(float *x, const float *d, float *mbuf, int w, int bar)
+{
+	constexpr int C = T / kSolveWarps;
+	const int lane = threadIdx.x & 31, r0 = w * C;
+	float v[C];
+#pragma unroll
+	for (int r = 0; r < C; ++r) v[r] = x[lane * kLd + r0 + r];
+#pragma unroll 1
+	for (int k = 0; k < T; ++k) {
+		float *m = mbuf + (k & 1) * T;
+		const bool own = k >= r0 && k < r0 + C;
+		float xreg = 0.f;
+#pragma unroll
+		for (int r = 0; r < C; ++r)
+			if (k == r0 + r) {
+				m[lane] = v[r];
+				xreg = v[r];
+			}
+		group_sync(bar, kSolveWarps * 32);
+		const float xkj = own ? xreg : m[lane];
+#pragma unroll
+		for (int r = 0; r < C; ++r)
+			if (r0 + r > k) v[r] = fmaf(-xkj, d[k * kLd + r0 + r], v[r]);
+	}
+#pragma unroll
+	for (int r = 0; r < C; ++r) x[lane * kLd + r0 + r] = v[r];
+}
+
 __global__ void __launch_bounds__(kWarps * 32) getrf_tiles_kernel(int b, float *a, int64_t lda, GetrfWork *w,
 	uint32_t epoch)
 {
@@ -304,19 +388,25 @@ __global__ void __launch_bounds__(kWarps * 32) getrf_tiles_kernel(int b, float *
 	bool ok = true;
 
 	if (blockIdx.x == 0) {
-		// ---------------- the diagonal chain (4 warps) ----------------
-		// warp 0 solves L(r+1, r) while warp 1 solves U(r, r+1); the four
-		// warps share the update of tile (r+1, r+1), 8 columns each; warp 0
-		// factors it.  Their tiles are warp 0's four staging buffers.
-		if (warp >= kDiagWarps) return;
+		// ---------------- the diagonal chain (all kDiagWarps warps) ----------------
+		// warps 0 .. 3 solve L(r+1, r) while warps 4 .. 7 solve U(r, r+1);
+		// all share the update of tile (r+1, r+1) and its factorisation.
+		// Their tiles are warp 0's four staging buffers; the broadcast rows
+		// sit in warp 1's.
 		float *Dd = dyn, *Xd = dyn + kTileFloats, *Ld = dyn + 2 * kTileFloats, *Ud = dyn + 3 * kTileFloats;
-		if (warp == 0) {
+		float *mF = dyn + 4 * kTileFloats, *mL = mF + 2 * T, *mU = mL + 2 * T;
+		const bool lgroup = warp < kSolveWarps;
+		{
 			const int kv = min(T, b);
-			stage_tile(Dd, a, lda, 0, 0, kv, kv, vec, lane);
+			if (warp == 0) stage_tile(Dd, a, lda, 0, 0, kv, kv, vec, lane);
 			stage_wait();
-			op_factor(Dd, kv);
-			store_tile(Dd, a, lda, 0, 0, kv, kv, lane);
-			publish(&prog[0], base + 1);
+			diag_sync();
+			coop_factor(Dd, kv, mF, warp);
+			diag_sync();
+			if (warp == 0) {
+				store_tile(Dd, a, lda, 0, 0, kv, kv, lane);
+				publish(&prog[0], base + 1);
+			}
 		}
 		diag_sync();
 		for (int r = 0; r + 1 < nt && ok; ++r) {
@@ -332,13 +422,16 @@ __global__ void __launch_bounds__(kWarps * 32) getrf_tiles_kernel(int b, float *
 			if (warp == 1) stage_tile(Ud, a, lda, k0, r1, T, v1, vec, lane);   // U(r, r+1) before its solve
 			if (warp == 2) stage_tile(Xd, a, lda, r1, r1, v1, v1, vec, lane);  // tile (r+1, r+1)
 			stage_wait();
-			if (warp == 0) {
-				op_solve_l(Ld, Dd, T);
+			diag_sync();
+			if (lgroup)
+				coop_solve_l(Ld, Dd, mL, warp, 2);
+			else
+				coop_solve_u(Ud, Dd, mU, warp - kSolveWarps, 3);
+			diag_sync();
+			if (warp == 0)
 				store_tile(Ld, a, lda, r1, k0, v1, T, lane);
-			} else if (warp == 1) {
-				op_solve_u(Ud, Dd, T);
+			else if (warp == 1)
 				store_tile(Ud, a, lda, k0, r1, T, v1, lane);
-			}
 			__threadfence();
 			diag_sync();
 			if (warp == 0 && lane == 0) {
@@ -347,12 +440,12 @@ __global__ void __launch_bounds__(kWarps * 32) getrf_tiles_kernel(int b, float *
 			}
 			op_update_cols(Xd, Ld, Ud, warp * (T / kDiagWarps));
 			diag_sync();
+			coop_factor(Xd, v1, mF, warp);
+			diag_sync();
 			if (warp == 0) {
-				op_factor(Xd, v1);
 				store_tile(Xd, a, lda, r1, r1, v1, v1, lane);
 				publish(&prog[pidx(r + 1, r + 1)], base + r + 2);
 			}
-			diag_sync();
 			// the new diagonal tile is the next step's factor
 			for (int e = threadIdx.x; e < kTileFloats; e += kDiagWarps * 32) Dd[e] = Xd[e];
 			diag_sync();
@@ -375,8 +468,8 @@ __global__ void __launch_bounds__(kWarps * 32) getrf_tiles_kernel(int b, float *
 			for (int t = wid; t < ntiles && ok; t += nwarps) {
 				const int ti = t % nt, tj = t / nt;
 				const int mn = min(ti, tj);
-				if (mn < r || ti == tj && ti <= r + 1) continue;                     // done, or the diagonal warp's
-				if ((ti == r + 1 && tj == r) || (ti == r && tj == r + 1)) continue;  // the diagonal warp's
+				if (mn < r || ti == tj && ti <= r + 1) continue;                     // done, or the diagonal CTA's
+				if ((ti == r + 1 && tj == r) || (ti == r && tj == r + 1)) continue;  // the diagonal CTA's
 				if ((mn == r ? 0 : 1) != pass) continue;
 				const int r0 = ti * T, c0 = tj * T;
 				const int rv = min(T, b - r0), cv = min(T, b - c0);
@@ -447,7 +540,7 @@ int launch_getrf_tiles(int b, float *a, int64_t lda, void *work, uint32_t *epoch
 	if (b <= 0) return HPLAI_OK;
 	if (b > T * kMaxTiles || !a || lda < b || !work || !epoch) return HPLAI_EINVAL;
 	const int nt = (b + T - 1) / T;
-	// CTA 0: the diagonal warp; then enough worker CTAs for one tile per warp
+	// CTA 0: the diagonal chain; then enough worker CTAs for one tile per warp
 	int grid = 1 + (nt > 1 ? (nt * nt + kWarps - 1) / kWarps : 0);
 	const int cap = max_coresident_ctas();
 	if (cap < 2) return HPLAI_EUNSUPPORTED;
