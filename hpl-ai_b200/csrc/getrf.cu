@@ -126,12 +126,9 @@ __device__ __forceinline__ void store_tile(const float *t, float *a, int64_t lda
 }
 
 // One-warp tile operations on staged tiles (the worker warps').  The solves
-// keep a row (or column) of the tile in registers and walk the pivots with a
-// runtime loop: the element of the current pivot column is always v[0] and
-// the row shifts left by one after each step, so every register index is
-// static while the loop body stays a few hundred bytes of code
-// (instruction-cache resident; a fully unrolled 32-step elimination is tens
-// of KB and runs from L2 once per step).
+// keep a row (or column) of the tile in registers, fully unrolled so that
+// every register index is static: 496 FMAs and their loads per lane, with no
+// register moves between pivots.
 
 // L tile x <- x U^{-1}, U = upper part of the factored tile d (kv x kv); row `lane`.
 __device__ __noinline__ void op_solve_l(float *x, const float *d, int kv)
@@ -142,19 +139,18 @@ __device__ __noinline__ void op_solve_l(float *x, const float *d, int kv)
 	for (int j = 0; j < T; ++j) v[j] = x[j * kLd + lane];
 	// 1/u_jj, lane j's (the staged tile is zero past kv: those lanes' values go unused)
 	const float inv = 1.0f / d[lane * kLd + lane];
-#pragma unroll 1
-	for (int j = 0; j < kv; ++j) {
-		// v[t] = element (lane, j + t); U(j, j + t) at d[(j + t) * kLd + j]
-		v[0] *= __shfl_sync(0xffffffffu, inv, j);
-		const float *urow = d + j * kLd + j;
 #pragma unroll
-		for (int t = 1; t < T; ++t)
-			if (j + t < T) v[t] = fmaf(-v[0], urow[t * kLd], v[t]);
-		x[j * kLd + lane] = v[0];
+	for (int j = 0; j < T; ++j) {
+		if (j < kv) {
+			v[j] *= __shfl_sync(0xffffffffu, inv, j);
+			// U(j, t) at d[t * kLd + j]
 #pragma unroll
-		for (int t = 0; t < T - 1; ++t) v[t] = v[t + 1];
-		v[T - 1] = 0.f;
+			for (int t = j + 1; t < T; ++t) v[t] = fmaf(-v[j], d[t * kLd + j], v[t]);
+		}
 	}
+#pragma unroll
+	for (int j = 0; j < T; ++j)
+		if (j < kv) x[j * kLd + lane] = v[j];
 	__syncwarp();
 }
 
@@ -172,18 +168,17 @@ __device__ __noinline__ void op_solve_u(float *x, const float *d, int kv)
 		v[4 * q + 2] = c.z;
 		v[4 * q + 3] = c.w;
 	}
-#pragma unroll 1
-	for (int k = 0; k < kv; ++k) {
-		// v[t] = element (k + t, lane); L(k + t, k) at d[k * kLd + k + t]
-		const float *lcol = d + k * kLd + k;
 #pragma unroll
-		for (int t = 1; t < T; ++t)
-			if (k + t < T) v[t] = fmaf(-v[0], lcol[t], v[t]);
-		col[k] = v[0];
+	for (int k = 0; k < T; ++k) {
+		if (k < kv) {
+			// L(i, k) at d[k * kLd + i]
 #pragma unroll
-		for (int t = 0; t < T - 1; ++t) v[t] = v[t + 1];
-		v[T - 1] = 0.f;
+			for (int i = k + 1; i < T; ++i) v[i] = fmaf(-v[k], d[k * kLd + i], v[i]);
+		}
 	}
+#pragma unroll
+	for (int k = 0; k < T; ++k)
+		if (k < kv) col[k] = v[k];
 	__syncwarp();
 }
 
