@@ -17,9 +17,9 @@
 // it still holds (four warps each, a step per named barrier), publishes
 // them, applies the last update to tile (r+1, r+1) and factors it (all
 // eight warps).  There is no flag hop between two diagonal tiles, and its
-// code stays hot in its SM's instruction cache.  Worker
-// warps (the other CTAs) own every other tile and walk them step by step,
-// panel tiles before updates.  Every wait is on work the producer reaches
+// code stays hot in its SM's instruction cache.  Worker warps (the other
+// CTAs) own every other tile and walk them step by step, panel tiles before
+// updates.  Every wait is on work the producer reaches
 // without waiting on the waiter, so the dataflow always completes (all
 // warps are resident: cooperative launch); every wait is bounded, and a
 // timeout sets the status word and the warp stops.
