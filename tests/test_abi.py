@@ -52,3 +52,30 @@ def test_invalid_arguments_rejected_without_gpu(hplai):
     assert hplai.panel_check(100, 16, 99, 16, 16, 1 << 20, None) == hplai.HPLAI_EINVAL
     assert hplai.panel_check(100, 16, 100, None, 16, 1 << 20, None) == hplai.HPLAI_EINVAL
     assert hplai.panel_check(100, 16, 100, 16, 16, hplai.panel_check_workspace(100) - 1, None) == hplai.HPLAI_EINVAL
+
+
+def test_create_rejects_invalid_schedules_without_gpu(hplai):
+    """hplai_create checks sizes, precision and flag combinations before any
+    CUDA call, so each refusal is visible on a machine without a GPU."""
+    import pytest
+    F = hplai
+    cases = [
+        (1024, 8, F.F32_F16, 0, F.HPLAI_EINVAL),                                        # b < 16
+        (4096, 2048, F.F32_F16, 0, F.HPLAI_EINVAL),                                     # b > 1024
+        (4096, 256, 7, 0, F.HPLAI_EUNSUPPORTED),                                        # precision
+        (4080, 60, F.F32_F16, F.FLAG_FP16_DECK, F.HPLAI_EINVAL),                        # deck: b % 8
+        (4096, 64, F.F32_F16, F.FLAG_GROUP2, F.HPLAI_EINVAL),                           # groups: b % 128
+        (4096, 64, F.F32_F8, F.FLAG_GROUP4, F.HPLAI_EINVAL),
+        (4096, 256, F.F32_F16, F.FLAG_GROUP2 | F.FLAG_GROUP4, F.HPLAI_EINVAL),          # both group sizes
+        (4096, 256, F.F32_F8, F.FLAG_REF_DECK, F.HPLAI_EINVAL),                         # -d arithmetic: FP16 form only
+        (4096, 256, F.F32_F16, F.FLAG_REF_DECK | F.FLAG_LOOKAHEAD, F.HPLAI_EINVAL),
+        (4096, 256, F.F32_F16, F.FLAG_REF_DECK | F.FLAG_GROUP2, F.HPLAI_EINVAL),
+        (4096, 256, F.F32_F16, F.FLAG_REF_BACKBUF, F.HPLAI_EINVAL),                     # back buffer needs -d
+        (4096, 256, F.F32_F8, F.FLAG_LAZY_A, F.HPLAI_EINVAL),                           # no stored A: deck form
+        (4096, 256, F.F32_F16, F.FLAG_LAZY_A | F.FLAG_FP16_DECK, F.HPLAI_EINVAL),       # ... and e4m3
+        (4096, 256, F.F32_F8, F.FLAG_LAZY_A | F.FLAG_FP16_DECK | F.FLAG_SIMT_PANELS, F.HPLAI_EINVAL),
+    ]
+    for n, b, prec, flags, status in cases:
+        with pytest.raises(F.HplaiError) as e:
+            F.Solver(n, b, precision=prec, flags=flags)
+        assert e.value.status == status, (n, b, prec, flags)
